@@ -1,0 +1,217 @@
+"""CPU oracle for the ERI path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests, ``__graft_entry__.smoke()`` (as the checker) and ``bench.py``'s CPU-baseline and
+reference arms may import this module.  The product (``molecularintegrals.jl_b200``) never
+does.  It wraps ``molints_oracle.c``, a plain-C FP64 restatement of the reference Julia
+HGP / Boys / Huzinaga code of MolecularIntegrals.jl (file:line citations are in that file),
+and adds an mpmath Boys function used to pin the C series.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD_DIR = HERE / "_build"
+LIB_PATH = BUILD_DIR / "libmolints_oracle.so"
+SRC = HERE / "molints_oracle.c"
+
+_lib = None
+
+_D = ctypes.c_double
+_I = ctypes.c_int
+_P = ctypes.c_void_p
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle with gcc (-O3, OpenMP) into oracle/_build/."""
+    if LIB_PATH.exists() and not force and LIB_PATH.stat().st_mtime >= SRC.stat().st_mtime:
+        return LIB_PATH
+    BUILD_DIR.mkdir(exist_ok=True)
+    tmp = LIB_PATH.with_suffix(f".{os.getpid()}.tmp.so")
+    cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-Wall",
+           "-o", str(tmp), str(SRC), "-lm"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.oracle_boys.restype = _D
+        L.oracle_boys.argtypes = [_I, _D]
+        L.oracle_boys_asymp.restype = _D
+        L.oracle_boys_asymp.argtypes = [_I, _D]
+        L.oracle_farray.argtypes = [_I, _D, _P]
+        L.oracle_vrr.argtypes = [_I, _I, _D, _D, _D, _D, _P, _P, _P, _P, _I, _P]
+        L.oracle_hrr.argtypes = [_I, _I, _I, _I, _D, _D, _D, _D, _P, _P, _P, _P, _I, _P]
+        L.oracle_hrr_size.restype = ctypes.c_size_t
+        L.oracle_hrr_size.argtypes = [_I, _I, _I, _I]
+        L.oracle_nao.restype = _I
+        L.oracle_nao.argtypes = [_I]
+        L.oracle_ao_index.restype = _I
+        L.oracle_ao_index.argtypes = [_I, _I, _I]
+        L.oracle_ao2m.argtypes = [_I, _P]
+        L.oracle_pgbf_norm.restype = _D
+        L.oracle_pgbf_norm.argtypes = [_D, _I, _I, _I]
+        L.oracle_cgbf_norm.restype = _D
+        L.oracle_cgbf_norm.argtypes = [_I, _I, _P, _P]
+        L.oracle_iindex.restype = ctypes.c_int64
+        L.oracle_iindex.argtypes = [ctypes.c_int64] * 4
+        L.oracle_npacked.restype = ctypes.c_int64
+        L.oracle_npacked.argtypes = [ctypes.c_int64]
+        drv = [_I, _P, _P, _P, _P, _P, _P, _P, _I]
+        L.oracle_eri_packed_hgp.restype = _I
+        L.oracle_eri_packed_hgp.argtypes = drv
+        L.oracle_eri_packed_huzinaga.restype = _I
+        L.oracle_eri_packed_huzinaga.argtypes = drv
+        L.oracle_shell_quartet.restype = _I
+        L.oracle_shell_quartet.argtypes = [_I, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]
+        L.oracle_coulomb_prim.restype = _D
+        L.oracle_coulomb_prim.argtypes = ([_D, _D, _D, _D, _I, _I, _I] * 4)
+        L.oracle_set_boys_tmax.argtypes = [_D]
+        L.oracle_get_boys_tmax.restype = _D
+        L.oracle_init()
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ------------------------------------------------------------------ Boys
+def boys(m: int, T: float) -> float:
+    """Fm(m,T) (src/Boys.jl:29-34)."""
+    return lib().oracle_boys(m, T)
+
+
+def farray(mmax: int, T: float) -> np.ndarray:
+    """farray(mmax,T) (src/Boys.jl:19-27): F_0..F_{mmax-1}."""
+    out = np.zeros(mmax)
+    lib().oracle_farray(mmax, T, _ptr(out))
+    return out
+
+
+def set_boys_tmax(tmax: float = 30.0) -> None:
+    """Move farray's switch to the asymptotic form (30 in src/Boys.jl:19)."""
+    lib().oracle_set_boys_tmax(tmax)
+
+
+class exact_boys:
+    """Context manager: the oracle uses the exact F_m(T) at every T (no asymptotic branch)."""
+
+    def __enter__(self):
+        self._old = lib().oracle_get_boys_tmax()
+        set_boys_tmax(1e300)
+
+    def __exit__(self, *exc):
+        set_boys_tmax(self._old)
+
+
+def boys_mpmath(m: int, T: float, dps: int = 40) -> float:
+    """Exact F_m(T) = 1/2 T^-(m+1/2) gamma_lower(m+1/2, T), in mpmath."""
+    import mpmath
+    with mpmath.workdps(dps):
+        if T == 0:
+            return float(mpmath.mpf(1) / (2 * m + 1))
+        a = mpmath.mpf(m) + mpmath.mpf(1) / 2
+        t = mpmath.mpf(T)
+        return float(mpmath.gammainc(a, 0, t) / (2 * t ** a))
+
+
+# ------------------------------------------------------------------ tables
+def nao(l: int) -> int:
+    return lib().oracle_nao(l)
+
+
+def ao_index(i: int, j: int, k: int) -> int:
+    """0-based m2ao (src/Basis.jl:295-316)."""
+    return lib().oracle_ao_index(i, j, k)
+
+
+# ------------------------------------------------------------------ primitive VRR/HRR
+def vrr(amax, cmax, aexp, bexp, cexp, dexp, A, B, C, D, prefactor_mode=0) -> np.ndarray:
+    """vrr(amax,cmax,...) (src/HGP.jl:371-376): array [mmax, nao(amax), nao(cmax)]."""
+    mmax = amax + cmax + 1
+    out = np.zeros((mmax, nao(amax), nao(cmax)))
+    cs = [np.ascontiguousarray(x, dtype=np.float64) for x in (A, B, C, D)]
+    lib().oracle_vrr(amax, cmax, aexp, bexp, cexp, dexp, *[_ptr(c) for c in cs],
+                     prefactor_mode, _ptr(out))
+    return out
+
+
+def hrr(la, lb, lc, ld, aexp, bexp, cexp, dexp, A, B, C, D, prefactor_mode=0) -> np.ndarray:
+    """hrr(...) (src/HGP.jl:392-424): [nao(la+lb), nao(lb), nao(lc+ld), nao(ld)]."""
+    out = np.zeros((nao(la + lb), nao(lb), nao(lc + ld), nao(ld)))
+    cs = [np.ascontiguousarray(x, dtype=np.float64) for x in (A, B, C, D)]
+    lib().oracle_hrr(la, lb, lc, ld, aexp, bexp, cexp, dexp, *[_ptr(c) for c in cs],
+                     prefactor_mode, _ptr(out))
+    return out
+
+
+def coulomb_prim(a, b, c, d) -> float:
+    """Raw primitive Huzinaga coulomb (src/ERI.jl:15-46); each arg (expn, (x,y,z), (I,J,K))."""
+    args = []
+    for expn, xyz, ijk in (a, b, c, d):
+        args += [float(expn), *map(float, xyz), *map(int, ijk)]
+    return lib().oracle_coulomb_prim(*args)
+
+
+def pgbf_norm(expn, I, J, K) -> float:
+    return lib().oracle_pgbf_norm(expn, I, J, K)
+
+
+# ------------------------------------------------------------------ whole basis
+def _shell_arrays(shells):
+    xyz = np.ascontiguousarray(shells.xyz, dtype=np.float64)
+    L = np.ascontiguousarray(shells.L, dtype=np.int32)
+    nprim = np.ascontiguousarray(shells.nprim, dtype=np.int32)
+    poff = np.ascontiguousarray(shells.prim_off, dtype=np.int32)
+    expn = np.ascontiguousarray(shells.expn, dtype=np.float64)
+    coef = np.ascontiguousarray(shells.coef, dtype=np.float64)
+    return xyz, L, nprim, poff, expn, coef
+
+
+def eri_packed_hgp(shells, nthreads: int = 1) -> np.ndarray:
+    """all_twoe_ints_chrr with D1-D3, D5 fixed: the normalised packed iindex vector."""
+    arrs = _shell_arrays(shells)
+    n = shells.nbf
+    out = np.zeros(n * (n + 1) * (n * n + n + 2) // 8)
+    rc = lib().oracle_eri_packed_hgp(len(arrs[1]), *[_ptr(a) for a in arrs], _ptr(out), nthreads)
+    if rc != 0:
+        raise ValueError("oracle_eri_packed_hgp: unsupported shell")
+    return out
+
+
+def eri_packed_huzinaga(shells, nthreads: int = 1) -> np.ndarray:
+    """all_twoe_ints(bfs, coulomb) (src/ERI.jl:104-112): normalised packed iindex vector."""
+    arrs = _shell_arrays(shells)
+    n = shells.nbf
+    out = np.zeros(n * (n + 1) * (n * n + n + 2) // 8)
+    rc = lib().oracle_eri_packed_huzinaga(len(arrs[1]), *[_ptr(a) for a in arrs], _ptr(out),
+                                          nthreads)
+    if rc != 0:
+        raise ValueError("oracle_eri_packed_huzinaga: unsupported shell")
+    return out
+
+
+def shell_quartet(shells, sa, sb, sc, sd) -> np.ndarray:
+    """Normalised contracted (ab|cd) block [na, nb, nc, nd] for four shells."""
+    arrs = _shell_arrays(shells)
+    nc = [(int(shells.L[s]) + 1) * (int(shells.L[s]) + 2) // 2 for s in (sa, sb, sc, sd)]
+    out = np.zeros(nc)
+    lib().oracle_shell_quartet(len(arrs[1]), *[_ptr(a) for a in arrs], sa, sb, sc, sd, _ptr(out))
+    return out
+
+
+def iindex(i, j, k, l) -> int:
+    """0-based iindex (src/Utils.jl:19 minus one)."""
+    return lib().oracle_iindex(i, j, k, l)
