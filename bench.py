@@ -1,0 +1,323 @@
+"""Benchmark of the ERI engine: unique ERIs per second on B200.
+
+Workload: the 24-atom split-valence molecule (8 heavy atoms with s6 s3 p3 s1 p1 shells,
+16 H with s3 s1; exponents log-uniform in [0.1, 5e3], seed 1; 104 cartesian functions,
+14,908,530 unique integrals, 3,454,506 shell quartets, 124.8 M primitive quartets).
+
+A step is one plan execute: primitive-pair build, Schwarz bounds and every shell quartet,
+writing the packed iindex vector into HBM.  ``value`` is the mixed-precision rate (FP32 VRR
+for quartets whose Schwarz bound is below ``fp32_cutoff``) whose max abs error against the
+FP64 path is reported beside it; ``fp64`` is the plain FP64 rate.  The packed output (119 MB)
+fits in L2, so a 256 MB buffer is written between timed steps (outside the timed events).
+``e2e`` is the same metric through the public call with host buffers (basis upload, device
+path, 119 MB device-to-host copy into pinned memory).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import __graft_entry__  # noqa: E402
+
+mi = __graft_entry__.load_package()
+
+METRIC = "ERIs/sec on 1 B200 (mixed vs plain FP64, max err <=1e-9); serve p50/p99 ms"
+UNIT = "ERI/s"
+WORKLOAD = "split_valence_24 (8 heavy s6s3p3s1p1 + 16 H s3s1, seed 1, 104 cart. functions)"
+FP32_CUTOFF = 1e-4
+CPU_SAMPLE_SECONDS = 10.0
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_reference_rate(shells, threads: int, min_seconds: float):
+    """The oracle's HGP driver (restatement of the reference's all_twoe_ints_chrr) over the
+    whole workload on `threads` host threads, repeated until min_seconds have passed:
+    (ERI/s, seconds, passes)."""
+    from oracle import oracle as orc
+    out = np.zeros(shells.npacked)
+    t0 = time.perf_counter()
+    n = passes = 0
+    while True:
+        n += orc.eri_packed_hgp_sample(shells, threads, 1, out)
+        passes += 1
+        dt = time.perf_counter() - t0
+        if dt >= min_seconds or passes >= 1000:
+            return n / dt, dt, passes
+
+
+def run_reference(args):
+    rank, world, _ = _dist()
+    if rank != 0:
+        return 0
+    sh = mi.config1()
+    threads = os.cpu_count() or 1
+    cpu_reference_rate(sh, threads, 0.0)  # builds the oracle, warms caches
+    for _ in range(max(args.warmup, 0)):
+        cpu_reference_rate(sh, threads, 0.0)
+    t0 = time.perf_counter()
+    passes = 0
+    for _ in range(args.steps):
+        _, _, p = cpu_reference_rate(sh, threads, 0.0)
+        passes += p
+    wall = time.perf_counter() - t0
+    value = passes * sh.npacked / wall
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "algorithm": "HGP (restated all_twoe_ints_chrr, C, OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"one full pass over the workload per step ({sh.npacked} integrals)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from molints_b200 import engine as E
+    from molints_b200 import flops as F
+
+    rank, world, local = _dist()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    eng = E.Engine(local)
+    eng.set_stream(stream.cuda_stream)
+    sh = mi.config1()
+    npacked = sh.npacked
+    per_class, tot = F.workload(sh)
+
+    out = torch.empty(npacked, dtype=torch.float64, device=dev)
+    flush = torch.zeros(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    plan64 = eng.plan(sh, precision=E.FP64)
+    planmx = eng.plan(sh, precision=E.MIXED, fp32_cutoff=FP32_CUTOFF)
+
+    # accuracy of the mixed path against the FP64 path on the same device
+    plan64.execute(out.data_ptr())
+    ref = out.clone()
+    planmx.execute(out.data_ptr())
+    max_err = (out - ref).abs().max().item()
+    mx_stats = planmx.stats()
+    del ref
+
+    def timed(plan, k):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        for a, b in ev:
+            flush_l2(flush)
+            a.record(stream)
+            plan.execute(out.data_ptr())
+            b.record(stream)
+        torch.cuda.synchronize(dev)
+        return sum(a.elapsed_time(b) for a, b in ev)
+
+    for plan in (plan64, planmx):
+        timed(plan, max(args.warmup, 3))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        ms64 = timed(plan64, args.steps)
+        msmx = timed(planmx, args.steps)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([ms64, msmx], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms64, msmx = t.tolist()
+    clocks = clk.summary()
+    value64 = world * args.steps * npacked / (ms64 * 1e-3)
+    valuemx = world * args.steps * npacked / (msmx * 1e-3)
+
+    # per-launch times of one FP64 execute -> dominant kernel and its roofline
+    plan64.set_profiling(True)
+    flush_l2(flush)
+    plan64.execute(out.data_ptr())
+    launches = plan64.launch_times()
+    plan64.set_profiling(False)
+    eri_l = [(n, ms) for n, ms in launches if n.startswith("eri_")]
+    top_name, top_ms = max(eri_l, key=lambda x: x[1])
+    top_flop = per_class[top_name[4:]]["flop"]
+    peak_fp64 = measure_fp64_peak(dev)
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(top_name)
+    roofline = {
+        "bound": "fp64", "kernel": top_name, "achieved": top_flop / (top_ms * 1e-3) / 1e12,
+        "peak": peak_fp64, "unit": "TFLOP/s",
+        "frac": top_flop / (top_ms * 1e-3) / 1e12 / peak_fp64,
+        "traffic": traffic,
+        "peak_source": "measured in this run: torch float64 8192^3 matmul (cuBLAS DGEMM), "
+                       "MEASURED_PEAKS.json has no FP64 figure",
+        "whole_step_tflops": tot["flop"] / (ms64 / args.steps * 1e-3) / 1e12,
+        "launch_share": {n: ms for n, ms in launches},
+    }
+
+    # end to end through the public call: host basis in, pinned host vector out
+    host_out = torch.empty(npacked, dtype=torch.float64, pin_memory=True).numpy()
+    eng_e2e = E.Engine(local)
+    eng_e2e.eri_packed(sh, precision=E.MIXED, fp32_cutoff=FP32_CUTOFF, out=host_out)
+    e2e_t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        eng_e2e.eri_packed(sh, precision=E.MIXED, fp32_cutoff=FP32_CUTOFF, out=host_out)
+        e2e_t.append(time.perf_counter() - t0)
+    h2d = int(sh.xyz.nbytes + sh.L.nbytes + sh.nprim.nbytes + sh.prim_off.nbytes +
+              sh.expn.nbytes + sh.coef.nbytes)
+    e2e = {"value": world * npacked * len(e2e_t) / sum(e2e_t), "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": npacked * 8,
+           "timing": "host wall clock around molints_eri_packed (synchronous call)"}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        r, dt, passes = cpu_reference_rate(sh, os.cpu_count() or 1, CPU_SAMPLE_SECONDS)
+        cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"{passes} full passes over the workload in {dt:.1f} s (oracle HGP, OpenMP)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": valuemx, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": msmx / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (FP32 VRR below the Schwarz cutoff)", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_eri_per_step": npacked,
+                       "shell_quartets": tot["quartets"], "prim_quartets": tot["prim_quartets"],
+                       "fp32_cutoff": FP32_CUTOFF, "fp32_quartets": mx_stats["n_fp32_quartets"],
+                       "l2": "256 MB buffer written between timed steps",
+                       "parallelism": f"replicas x{world}"},
+            "max_abs_err_mixed_vs_fp64": max_err,
+            "fp64": {"value": value64, "ms_per_step": ms64 / args.steps},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * 2 * plan64.stats()["n_kernel_launches"],
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    plan64.close()
+    planmx.close()
+    eng_e2e.close()
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def measure_fp64_peak(dev) -> float:
+    import torch
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize(dev)
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

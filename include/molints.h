@@ -1,0 +1,151 @@
+/*
+ * molints.h -- C ABI of libmolints_cuda.so, a B200 (sm_100a) engine for the two-electron
+ * repulsion integrals (ERIs) of contracted cartesian Gaussian basis sets.
+ *
+ * It replaces the ERI drivers of MolecularIntegrals.jl (paths relative to that project):
+ *   all_twoe_ints(bfs, ERI=coulomb)   src/ERI.jl:104-112
+ *   all_twoe_ints_chrr(bfs::Basis)    src/HGP.jl:22-34
+ *   all_twoe_ints_rys(bfs)            src/Rys.jl:16-24
+ * All three return the unique integrals (ij|kl), i>=j, k>=l, ij>=kl, of normalised
+ * functions in one packed vector indexed by iindex (src/Utils.jl:14-19); this library
+ * writes exactly that vector (0-based: element iindex(i,j,k,l)-1).
+ *
+ * Conventions: every function returns an int status (MOLINTS_OK = 0, negative on error);
+ * no C++ exception crosses the ABI; molints_last_error() describes the last failure of a
+ * context.  A context belongs to one host thread at a time.  Pointers are plain host
+ * pointers unless a name or comment says "device".
+ */
+#ifndef MOLINTS_H
+#define MOLINTS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOLINTS_ABI_VERSION 1
+
+enum molints_status {
+    MOLINTS_OK = 0,
+    MOLINTS_ERR_INVALID = -1,      /* bad argument or malformed basis */
+    MOLINTS_ERR_UNSUPPORTED = -2,  /* angular momentum or size beyond the engine's limits */
+    MOLINTS_ERR_BUDGET = -3,       /* the request does not fit the context's HBM budget */
+    MOLINTS_ERR_CUDA = -4,         /* a CUDA runtime call failed */
+    MOLINTS_ERR_TIMEOUT = -5,      /* a bounded device or host wait gave up */
+    MOLINTS_ERR_NOMEM = -6         /* host allocation failed */
+};
+
+enum molints_method { MOLINTS_METHOD_AUTO = 0, MOLINTS_METHOD_HGP = 1 };
+enum molints_precision { MOLINTS_FP64 = 0, MOLINTS_MIXED = 1 };
+enum molints_boys {
+    /* farray of src/Boys.jl:19-27: exact F_m below T = 30, the asymptotic form (without the
+     * e^-T terms) from T = 30 up.  Matches the reference HGP bit for bit up to rounding. */
+    MOLINTS_BOYS_REFERENCE = 0,
+    /* exact F_m (table + Taylor + downward recursion) up to T = 40, asymptotic beyond. */
+    MOLINTS_BOYS_EXACT = 1
+};
+
+/* Largest shell angular momentum the engine accepts (d = 2). */
+#define MOLINTS_LMAX 2
+
+/* A basis set as flat shell arrays: what the reference's Basis/Shell hold
+ * (src/Basis.jl:147-177).  Functions are numbered shell by shell, components in the
+ * reference's shell_indices order (src/Basis.jl:269-279). */
+typedef struct molints_basis {
+    int32_t nshell;
+    const double *xyz;       /* [3*nshell] centres, bohr */
+    const int32_t *L;        /* [nshell] angular momentum, 0..MOLINTS_LMAX */
+    const int32_t *nprim;    /* [nshell] primitives per shell, >= 1 */
+    const int32_t *prim_off; /* [nshell] offset of the shell's first primitive */
+    const double *expn;      /* primitive exponents (Shell.expns) */
+    const double *coef;      /* raw contraction coefficients (Shell.coefs); the engine
+                                applies primitive and contracted norms (src/Basis.jl:42-98) */
+} molints_basis;
+
+typedef struct molints_options {
+    int32_t method;          /* enum molints_method */
+    int32_t precision;       /* enum molints_precision */
+    int32_t boys;            /* enum molints_boys */
+    int32_t reserved;
+    double fp32_cutoff;      /* MIXED: quartets whose Schwarz bound Q_ab*Q_cd is below this
+                                run the VRR in FP32 (FP64 Boys, prefactors, accumulation) */
+    double screen_cutoff;    /* quartets with Q_ab*Q_cd below this are written as 0 */
+} molints_options;
+
+typedef struct molints_stats {
+    int64_t n_eri;            /* packed integrals written */
+    int64_t n_shell_quartets; /* unique shell quartets */
+    int64_t n_prim_quartets;  /* primitive quartets in those */
+    int64_t n_fp32_quartets;  /* quartets that took the FP32 VRR (counted on the host) */
+    int64_t n_screened;       /* quartets skipped by screen_cutoff (counted on the host) */
+    int32_t n_kernel_launches;
+    int32_t reserved;
+    double device_ms;         /* device time of the last execute (CUDA events) */
+} molints_stats;
+
+typedef struct molints_ctx molints_ctx;
+typedef struct molints_plan molints_plan;
+
+/* Library version / ABI check. */
+int molints_abi_version(void);
+
+/* Fill opts with the defaults: AUTO, FP64, reference Boys, fp32_cutoff 0, screen 0. */
+void molints_default_options(molints_options *opts);
+
+/* Number of basis functions of a basis, or a negative status. */
+int64_t molints_nbf(const molints_basis *basis);
+/* Length of the packed vector for n functions: n(n+1)(n^2+n+2)/8 (src/ERI.jl:106). */
+int64_t molints_npacked(int64_t nbf);
+
+/* Create a context on a CUDA device.  hbm_budget_bytes bounds the device memory the
+ * context may hold (0 = no bound).  flags is reserved (0). */
+int molints_create(molints_ctx **ctx, int device, int64_t hbm_budget_bytes, uint32_t flags);
+int molints_destroy(molints_ctx *ctx);
+const char *molints_last_error(const molints_ctx *ctx);
+
+/* Set the CUDA stream (a cudaStream_t passed as void*) the context launches on.
+ * NULL selects the context's own stream. */
+int molints_set_stream(molints_ctx *ctx, void *stream);
+
+/* One call, the drop-in for all_twoe_ints / all_twoe_ints_chrr: computes every unique
+ * integral of the basis into out[molints_npacked(nbf)].  out is a host pointer (pinned or
+ * pageable) when out_is_device == 0, a device pointer on the context's device otherwise.
+ * The call returns when the result is in out.  stats may be NULL. */
+int molints_eri_packed(molints_ctx *ctx, const molints_basis *basis,
+                       const molints_options *opts, double *out, int out_is_device,
+                       molints_stats *stats);
+
+/* Plans: the device-resident form of one basis.  plan_create normalises the basis, orders
+ * the shell pairs by class and contraction length, uploads them and sizes every buffer;
+ * plan_execute then runs the whole device path -- primitive-pair data, Schwarz bounds and
+ * all shell quartets -- into a device vector of molints_npacked(nbf) doubles, on the
+ * context's stream, without host synchronisation. */
+int molints_plan_create(molints_ctx *ctx, const molints_basis *basis,
+                        const molints_options *opts, molints_plan **plan);
+int molints_plan_execute(molints_plan *plan, double *out_device);
+int molints_plan_stats(const molints_plan *plan, molints_stats *stats);
+int molints_plan_destroy(molints_plan *plan);
+
+/* Schwarz bounds Q_ab = sqrt(max |(ab|ab)|) of the plan's shell pairs after an execute,
+ * in the reference's pair order (shell i >= shell j, row-major): out[nshell*(nshell+1)/2]. */
+int molints_plan_schwarz(molints_plan *plan, double *out_host);
+
+/* Per-launch device times.  After molints_plan_set_profiling(plan, 1), every execute records
+ * a CUDA event pair around each kernel launch; molints_plan_launch_times then waits for the
+ * last execute and returns up to cap entries: names[k] (static strings such as
+ * "eri_ssss", "schwarz_pp", "build_pairs") and ms[k].  Returns the number of launches of the
+ * last execute, or a negative status. */
+int molints_plan_set_profiling(molints_plan *plan, int enable);
+int molints_plan_launch_times(molints_plan *plan, const char **names, float *ms, int cap);
+
+/* F_m(T) for m = 0..mmax-1 at n values of T, evaluated by the device Boys function
+ * (src/Boys.jl:19-27) in the given mode.  T and out are host arrays; out is [n][mmax]. */
+int molints_boys_eval(molints_ctx *ctx, int32_t boys_mode, int32_t mmax, const double *T,
+                      int64_t n, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOLINTS_H */

@@ -1,0 +1,142 @@
+// eri_common.cuh -- device data layout and shared device functions of the ERI engine.
+//
+// Layout in HBM (all arrays are owned by a plan, see molints.cu):
+//   * shell pairs, canonical orientation (L_A >= L_B), sorted by pair class and then by
+//     contraction length; structure of arrays:
+//       info[p] = {first primitive pair, number of primitive pairs, first function of A,
+//                  first function of B}                      (int4, 16 B)
+//       geo[p]  = {A-B (x,y,z), Schwarz bound Q_p}          (double4, 32 B)
+//   * primitive pairs, 80 B each (5 x 16 B vector loads): PrimPair below;
+//   * the Boys table (T = 0..40 step 1/16, F_0..F_22 and e^-T per row);
+//   * the packed output vector, 0-based iindex order (src/Utils.jl:14-19).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace molints {
+
+constexpr int kBoysRows = 641;            // T_n = n/16, n = 0..640 (T up to 40)
+constexpr int kBoysCols = 24;             // F_0..F_22 at T_n, then e^-T_n
+constexpr int kBoysTaylor = 8;            // Taylor terms about T_n; |T - T_n| <= 1/32
+constexpr double kBoysStepInv = 16.0;
+constexpr double kBoysStep = 0.0625;
+constexpr double kBoysTableMax = 40.0;    // exact-mode switch to the asymptotic form
+constexpr double kBoysReferenceSwitch = 30.0;  // farray's Tmax, src/Boys.jl:19
+
+// Record of one primitive pair (a, b) of a canonical shell pair (A, B):
+//   zeta = a + b
+//   kab  = sqrt(2) pi^(5/4) c_a c_b exp(-a b |A-B|^2 / zeta) / zeta, with c_a, c_b the
+//          fully normalised contraction coefficients (radial primitive norm x CGBF norm)
+//   oo2z = 1 / (2 zeta)
+//   P    = (a A + b B) / zeta (gaussian_product_center, src/OneInts.jl:78-83)
+//   PA   = P - A
+// so that kab_bra * kab_ket / sqrt(zeta+eta) is the [00|00] prefactor of HGP eq. 12,
+// 2 pi^(5/2) / (zeta eta sqrt(zeta+eta)) x exp(...) x coefficients.
+struct PrimPair {
+    double zeta, kab, oo2z, px, py, pz, pax, pay, paz, pad;
+};
+static_assert(sizeof(PrimPair) == 80, "PrimPair is 5 x 16 bytes");
+
+struct PairTab {
+    const int4 *info;
+    const double4 *geo;
+    const PrimPair *pp;
+};
+
+struct BoysTab {
+    const double *tab;  // [kBoysRows][kBoysCols]
+    double t_switch;    // asymptotic form at T >= t_switch
+};
+
+// One launch of a class-pair kernel: a rectangle (bra pairs x ket pairs) or, when both
+// come from the same pair class, the triangle q <= p of it.
+struct EriLaunch {
+    PairTab pairs;
+    BoysTab boys;
+    double *out;              // packed output (device)
+    int bra0, nbra;           // bra shell pairs [bra0, bra0 + nbra)
+    int ket0, nket;           // ket shell pairs [ket0, ket0 + nket)
+    int tri;                  // 1: same class on both sides, only q <= p
+    int pad;
+    long long nquart;         // nbra * nket or nbra * (nbra + 1) / 2
+    double screen_cut;        // Q_p Q_q below this: written as 0
+    double fp32_cut;          // Q_p Q_q below this (MIXED kernels): FP32 VRR
+};
+
+__device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {
+    const double2 *v = reinterpret_cast<const double2 *>(base + k);
+    const double2 a = __ldg(v), b = __ldg(v + 1), c = __ldg(v + 2), d = __ldg(v + 3),
+                  e = __ldg(v + 4);
+    PrimPair r;
+    r.zeta = a.x; r.kab = a.y; r.oo2z = b.x; r.px = b.y; r.py = c.x; r.pz = c.y;
+    r.pax = d.x; r.pay = d.y; r.paz = e.x; r.pad = e.y;
+    return r;
+}
+
+// F_0..F_M at T: the farray structure of src/Boys.jl:19-27.
+//   T <  t_switch: F_M by an 8-term Taylor expansion about the nearest table point
+//                  (F_m(T_n - d) = sum_k F_{m+k}(T_n) d^k / k!), e^-T = e^-T_n e^d, then
+//                  the downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1).
+//   T >= t_switch: the asymptotic family F_m = (2m-1)!! / (2T)^m * sqrt(pi/T)/2, the values
+//                  farray's Fm_asymp top order and e^-T-free recursion produce.
+template <int M>
+__device__ __forceinline__ void boys_fm(double T, const BoysTab &bt, double *F) {
+    if (T < bt.t_switch) {
+        const int n = __double2int_rn(T * kBoysStepInv);
+        const double d = n * kBoysStep - T;
+        const double *__restrict__ row = bt.tab + n * kBoysCols;
+        double f = __ldg(row + M + kBoysTaylor - 1);
+#pragma unroll
+        for (int k = kBoysTaylor - 1; k >= 1; --k) f = fma(f, d * (1.0 / k), __ldg(row + M + k - 1));
+        F[M] = f;
+        if (M > 0) {
+            double ed = 1.0;
+#pragma unroll
+            for (int k = kBoysTaylor - 1; k >= 1; --k) ed = fma(ed, d * (1.0 / k), 1.0);
+            const double emt = __ldg(row + kBoysCols - 1) * ed;
+            const double t2 = 2.0 * T;
+#pragma unroll
+            for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], emt) * (1.0 / (2 * m + 1));
+        }
+    } else {
+        const double r = rsqrt(T);
+        F[0] = 0.88622692545275801365 * r;  // sqrt(pi)/2
+        const double oo2t = 0.5 * r * r;
+#pragma unroll
+        for (int m = 1; m <= M; ++m) F[m] = F[m - 1] * ((2 * m - 1) * oo2t);
+    }
+}
+
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+    const double2 *v = reinterpret_cast<const double2 *>(p);
+    const double2 a = __ldg(v), b = __ldg(v + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ long long tri_ll(long long i) { return i * (i + 1) / 2; }
+
+// 0-based packed index of the function-pair indices ij, kl (iindex, src/Utils.jl:19).
+__device__ __forceinline__ long long packed_index(long long ij, long long kl) {
+    return ij >= kl ? tri_ll(ij) + kl : tri_ll(kl) + ij;
+}
+__device__ __forceinline__ long long pair_index(int i, int j) {
+    return i >= j ? tri_ll(i) + j : tri_ll(j) + i;
+}
+
+// Decode a quartet's linear index in a launch into (bra pair, ket pair).
+__device__ __forceinline__ void decode_quartet(const EriLaunch &L, long long t, int &p, int &q) {
+    if (L.tri) {
+        long long pp = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while (tri_ll(pp) > t) --pp;
+        while (tri_ll(pp + 1) <= t) ++pp;
+        p = (int)pp;
+        q = (int)(t - tri_ll(pp));
+    } else {
+        p = (int)(t / L.nket);
+        q = (int)(t - (long long)p * L.nket);
+    }
+    p += L.bra0;
+    q += L.ket0;
+}
+
+}  // namespace molints

@@ -1,0 +1,457 @@
+"""Generate the per-class ERI kernels (CUDA C for sm_100a).
+
+This is the engine's counterpart of the reference's ``vrr_autogen`` (src/HGP.jl:432-534),
+which emits unrolled, branch-free Julia VRR code per (amax, cmax).  Here one kernel is
+emitted per class pair (la lb | lc ld) with la >= lb, lc >= ld and the bra class at or
+above the ket class.  Each kernel evaluates one contracted shell quartet per thread:
+
+  * the HGP vertical recurrence of src/HGP.jl:135-242 -- the a-build (eq. 6a with c = 0,
+    :180-197) and the c-build (eq. 6d, :204-240) -- unrolled and pruned to the
+    [a0|c0]^(m) entries the class needs, in registers (FP64, or FP32 for MIXED quartets);
+  * contraction over the primitive quartets in FP64 after the VRR (cvrr, :50-68);
+  * the horizontal recurrences of chrr (:87-114) on the contracted block, bra then ket;
+  * the component norms 1/sqrt((2I-1)!!(2J-1)!!(2K-1)!!) and the packed iindex store of
+    the quartet's unique integrals.
+
+Run ``python gen_eri.py`` to (re)write ``generated/``; the build does it automatically.
+"""
+from __future__ import annotations
+
+import math
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT_DIR = HERE / "generated"
+LMAX = 2            # shell angular momentum supported by the generated kernels
+LTAB = 2 * LMAX     # AO tables must reach la + lb
+
+
+# ------------------------------------------------------------------ AO tables
+def shell_components(l):
+    """src/Basis.jl:269-279 order (x-power descending, then y), l=3 with xzz before xyz."""
+    comps = [(i, j, l - i - j) for i in range(l, -1, -1) for j in range(l - i, -1, -1)]
+    if l == 3:
+        comps[4], comps[5] = comps[5], comps[4]
+    return comps
+
+
+AO = []           # cumulative AO list (ao2m, src/Basis.jl:306-314), 0-based
+NAO = []          # cumulative counts (nao, src/Basis.jl:320-321)
+for _l in range(LTAB + 1):
+    AO.extend(shell_components(_l))
+    NAO.append(len(AO))
+AO_INDEX = {c: i for i, c in enumerate(AO)}
+
+
+def lof(a):
+    return sum(AO[a])
+
+
+def shell_range(l):
+    return range(NAO[l - 1] if l > 0 else 0, NAO[l])
+
+
+def shift_dir(a):
+    """First argmax of the powers (shift_direction, src/Basis.jl:346-354)."""
+    m = AO[a]
+    return max(range(3), key=lambda i: (m[i], -i))
+
+
+def shift_minus(a, i):
+    m = list(AO[a])
+    if m[i] == 0:
+        return -1
+    m[i] -= 1
+    return AO_INDEX[tuple(m)]
+
+
+def shift_plus(a, i):
+    m = list(AO[a])
+    m[i] += 1
+    return AO_INDEX[tuple(m)]
+
+
+def dfact2(n):
+    r = 1
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def comp_norm(a):
+    I, J, K = AO[a]
+    return 1.0 / math.sqrt(dfact2(2 * I - 1) * dfact2(2 * J - 1) * dfact2(2 * K - 1))
+
+
+XYZ = "xyz"
+
+
+# ------------------------------------------------------------------ classes
+def pair_classes(lmax=LMAX):
+    """Shell-pair classes (la, lb), la >= lb, ordered by la+lb then la."""
+    cls = [(la, lb) for la in range(lmax + 1) for lb in range(la + 1)]
+    return sorted(cls, key=lambda c: (c[0] + c[1], c[0]))
+
+
+def class_pairs(lmax=LMAX):
+    cls = pair_classes(lmax)
+    out = []
+    for i, X in enumerate(cls):
+        for j in range(i + 1):
+            out.append((X, cls[j]))
+    return out
+
+
+def tag_of(X, Y):
+    L = "spdfg"
+    return f"{L[X[0]]}{L[X[1]]}{L[Y[0]]}{L[Y[1]]}"
+
+
+# ------------------------------------------------------------------ VRR plan
+def vrr_entries(e_lo, e_hi, f_lo, f_hi):
+    """Needed [a0|c0]^(m) entries, in an order where every entry follows its inputs."""
+    need = set()
+    stack = [(a, c, 0) for a in range(NAO[e_lo - 1] if e_lo else 0, NAO[e_hi])
+             for c in range(NAO[f_lo - 1] if f_lo else 0, NAO[f_hi])]
+    while stack:
+        key = stack.pop()
+        if key in need:
+            continue
+        need.add(key)
+        stack.extend(vrr_deps(*key))
+    return sorted(need, key=lambda k: (k[1], k[0], k[2]))
+
+
+def vrr_deps(a, c, m):
+    if c == 0:
+        if a == 0:
+            return []
+        i = shift_dir(a)
+        am = shift_minus(a, i)
+        amm = shift_minus(am, i)
+        d = [(am, 0, m), (am, 0, m + 1)]
+        if amm >= 0:
+            d += [(amm, 0, m), (amm, 0, m + 1)]
+        return d
+    i = shift_dir(c)
+    cm = shift_minus(c, i)
+    cmm = shift_minus(cm, i)
+    am = shift_minus(a, i)
+    d = [(a, cm, m), (a, cm, m + 1)]
+    if am >= 0:
+        d.append((am, cm, m + 1))
+    if cmm >= 0:
+        d += [(a, cmm, m), (a, cmm, m + 1)]
+    return d
+
+
+def vname(a, c, m):
+    return f"v{a}_{c}_{m}"
+
+
+def vrr_line(a, c, m):
+    """The recurrence of src/HGP.jl:189-190 / :218-236 for one entry."""
+    if c == 0:
+        if a == 0:
+            return f"const VT {vname(0, 0, m)} = (VT)(pref * F[{m}]);"
+        i = shift_dir(a)
+        am = shift_minus(a, i)
+        amm = shift_minus(am, i)
+        x = XYZ[i]
+        s = f"PA{x} * {vname(am, 0, m)} + WP{x} * {vname(am, 0, m + 1)}"
+        if amm >= 0:
+            k = AO[am][i]
+            s += (f" + (VT){k}.0 * oo2z * ({vname(amm, 0, m)} - rho_z * "
+                  f"{vname(amm, 0, m + 1)})")
+        return f"const VT {vname(a, 0, m)} = {s};"
+    i = shift_dir(c)
+    cm = shift_minus(c, i)
+    cmm = shift_minus(cm, i)
+    am = shift_minus(a, i)
+    x = XYZ[i]
+    s = f"QC{x} * {vname(a, cm, m)} + WQ{x} * {vname(a, cm, m + 1)}"
+    if am >= 0:
+        s += f" + (VT){AO[a][i]}.0 * oo2ze * {vname(am, cm, m + 1)}"
+    if cmm >= 0:
+        k = AO[cm][i]
+        s += f" + (VT){k}.0 * oo2e * ({vname(a, cmm, m)} - rho_e * {vname(a, cmm, m + 1)})"
+    return f"const VT {vname(a, c, m)} = {s};"
+
+
+# ------------------------------------------------------------------ HRR plan
+class HrrPlan:
+    """(ab|cd) from the contracted [a0|c0] block: bra HRR then ket HRR (src/HGP.jl:92-114)."""
+
+    def __init__(self, la, lb, lc, ld):
+        self.la, self.lb, self.lc, self.ld = la, lb, lc, ld
+        self.lines = []
+        self.done = {}
+        e, f = la + lb, lc + ld
+        self.acc_a = [a for l in range(la, e + 1) for a in shell_range(l)]
+        self.acc_c = [c for l in range(lc, f + 1) for c in shell_range(l)]
+        self.acc_index = {(a, c): i * len(self.acc_c) + j
+                          for i, a in enumerate(self.acc_a) for j, c in enumerate(self.acc_c)}
+        self.targets = []
+        for a in shell_range(la):
+            for b in shell_range(lb):
+                for c in shell_range(lc):
+                    for d in shell_range(ld):
+                        self.targets.append((a, b, c, d, self.ket(a, b, c, d)))
+
+    def bra(self, a, b, c):
+        if b == 0:
+            return f"acc[{self.acc_index[(a, c)]}]"
+        key = ("h", a, b, c)
+        if key in self.done:
+            return self.done[key]
+        j = shift_dir(b)
+        bm = shift_minus(b, j)
+        t1 = self.bra(shift_plus(a, j), bm, c)
+        t2 = self.bra(a, bm, c)
+        name = f"h{a}_{b}_{c}"
+        self.lines.append(f"const double {name} = {t1} + AB{XYZ[j]} * {t2};")
+        self.done[key] = name
+        return name
+
+    def ket(self, a, b, c, d):
+        if d == 0:
+            return self.bra(a, b, c)
+        key = ("k", a, b, c, d)
+        if key in self.done:
+            return self.done[key]
+        j = shift_dir(d)
+        dm = shift_minus(d, j)
+        t1 = self.ket(a, b, shift_plus(c, j), dm)
+        t2 = self.ket(a, b, c, dm)
+        name = f"k{a}_{b}_{c}_{d}"
+        self.lines.append(f"const double {name} = {t1} + CD{XYZ[j]} * {t2};")
+        self.done[key] = name
+        return name
+
+
+# ------------------------------------------------------------------ emit
+def emit_class_pair(X, Y):
+    (la, lb), (lc, ld) = X, Y
+    tag = tag_of(X, Y)
+    e, f = la + lb, lc + ld
+    M = e + f
+    entries = vrr_entries(la, e, lc, f)
+    hp = HrrPlan(la, lb, lc, ld)
+    nacc = len(hp.acc_a) * len(hp.acc_c)
+    na, nb, nc, nd = [len(shell_range(l)) for l in (la, lb, lc, ld)]
+    nout = na * nb * nc * nd
+    ind = "        "
+    vrr_code = "\n".join(ind + "    " + vrr_line(*k) for k in entries)
+    acc_code = "\n".join(
+        f"{ind}    acc[{hp.acc_index[(a, c)]}] += (double){vname(a, c, 0)};"
+        for a in hp.acc_a for c in hp.acc_c)
+    hrr_code = "\n".join("    " + ln for ln in hp.lines)
+    out_code = []
+    for x, (a, b, c, d, expr) in enumerate(hp.targets):
+        g = comp_norm(a) * comp_norm(b) * comp_norm(c) * comp_norm(d)
+        if abs(g - 1.0) < 1e-15:
+            out_code.append(f"    res[{x}] = {expr};")
+        else:
+            out_code.append(f"    res[{x}] = {expr} * {g!r};")
+    out_code = "\n".join(out_code)
+    stores = []
+    for ia in range(na):
+        for ib in range(nb):
+            for ic in range(nc):
+                for id_ in range(nd):
+                    x = ((ia * nb + ib) * nc + ic) * nd + id_
+                    conds = []
+                    if la == lb:
+                        conds.append(f"(!dab || {ia} >= {ib})")
+                    if lc == ld:
+                        conds.append(f"(!dcd || {ic} >= {id_})")
+                    cond = " && ".join(conds) if conds else "true"
+                    stores.append(
+                        f"    {{ const long long ij = ij_{ia}_{ib}, kl = kl_{ic}_{id_};\n"
+                        f"      if ({cond} && (!same || ij >= kl)) "
+                        f"out[packed_index(ij, kl)] = res[{x}]; }}")
+    ij_code = "\n".join(f"    const long long ij_{ia}_{ib} = pair_index(ib_.z + {ia}, ib_.w + {ib});"
+                        for ia in range(na) for ib in range(nb))
+    kl_code = "\n".join(f"    const long long kl_{ic}_{id_} = pair_index(ik_.z + {ic}, ik_.w + {id_});"
+                        for ic in range(nc) for id_ in range(nd))
+    store_code = "\n".join(stores)
+    schwarz = ""
+    if X == Y:
+        diag = []
+        for ia in range(na):
+            for ib in range(nb):
+                x = ((ia * nb + ib) * nc + ia) * nd + ib
+                diag.append(f"    m = fmax(m, fabs(res[{x}]));")
+        diag = "\n".join(diag)
+        schwarz = f"""
+// Schwarz bound Q_p = sqrt(max over components of |(ab|ab)|) for the pairs of one class.
+__global__ void __launch_bounds__(128) schwarz_kernel_{tag}(PairTab P, BoysTab B, int p0, int np,
+                                                          double4 *geo_rw) {{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int p = p0 + t;
+    double res[{nout}];
+    quartet_{tag}<double>(P, B, p, p, res);
+    double m = 0.0;
+{diag}
+    geo_rw[p].w = sqrt(m);
+}}
+
+void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw,
+                          cudaStream_t s) {{
+    if (np <= 0) return;
+    schwarz_kernel_{tag}<<<(np + 127) / 128, 128, 0, s>>>(P, B, p0, np, geo_rw);
+}}
+"""
+    return f"""// Generated by gen_eri.py -- class ({'spdfg'[la]}{'spdfg'[lb]}|{'spdfg'[lc]}{'spdfg'[ld]}).  Do not edit.
+// VRR entries: {len(entries)}, contracted block: {nacc}, HRR lines: {len(hp.lines)}, outputs: {nout}.
+#include "../eri_common.cuh"
+
+namespace molints {{
+
+// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[{nout}]
+// (ma, mb, mc, md row-major).  VT is the VRR arithmetic type (double, or float for MIXED).
+template <typename VT>
+__device__ __forceinline__ void quartet_{tag}(const PairTab &P, const BoysTab &B, int p, int q,
+                                              double *__restrict__ res) {{
+    const int4 ib_ = __ldg(&P.info[p]);
+    const int4 ik_ = __ldg(&P.info[q]);
+    double acc[{nacc}];
+#pragma unroll
+    for (int x = 0; x < {nacc}; ++x) acc[x] = 0.0;
+    for (int i = 0; i < ib_.y; ++i) {{
+        const PrimPair bra = load_pp(P.pp, ib_.x + i);
+        for (int j = 0; j < ik_.y; ++j) {{
+            const PrimPair ket = load_pp(P.pp, ik_.x + j);
+            const double r = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = r * r;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double T = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = bra.kab * ket.kab * r;
+            double F[{M + 1}];
+            boys_fm<{M}>(T, B, F);
+            const VT PAx = (VT)bra.pax, PAy = (VT)bra.pay, PAz = (VT)bra.paz;
+            const VT QCx = (VT)ket.pax, QCy = (VT)ket.pay, QCz = (VT)ket.paz;
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const VT WPx = (VT)(-ez * PQx), WPy = (VT)(-ez * PQy), WPz = (VT)(-ez * PQz);
+            const VT WQx = (VT)(zz * PQx), WQy = (VT)(zz * PQy), WQz = (VT)(zz * PQz);
+            const VT oo2z = (VT)bra.oo2z, oo2e = (VT)ket.oo2z, oo2ze = (VT)(0.5 * r2);
+            const VT rho_z = (VT)ez, rho_e = (VT)zz;
+            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz;
+            (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;
+            (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;
+{vrr_code}
+{acc_code}
+        }}
+    }}
+    const double4 gb = ldg4(&P.geo[p]);
+    const double4 gk = ldg4(&P.geo[q]);
+    const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
+    const double CDx = gk.x, CDy = gk.y, CDz = gk.z;
+    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
+{hrr_code}
+{out_code}
+}}
+
+__device__ __forceinline__ void store_{tag}(double *__restrict__ out, const int4 ib_, const int4 ik_,
+                                            bool same, const double *__restrict__ res) {{
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    (void)dab; (void)dcd;
+{ij_code}
+{kl_code}
+{store_code}
+}}
+
+template <int MIXED>
+__global__ void __launch_bounds__(128) eri_kernel_{tag}(const EriLaunch L) {{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.nquart) return;
+    int p, q;
+    decode_quartet(L, t, p, q);
+    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    double res[{nout}];
+    if (bound < L.screen_cut) {{
+#pragma unroll
+        for (int x = 0; x < {nout}; ++x) res[x] = 0.0;
+    }} else if (MIXED && bound < L.fp32_cut) {{
+        quartet_{tag}<float>(L.pairs, L.boys, p, q, res);
+    }} else {{
+        quartet_{tag}<double>(L.pairs, L.boys, p, q, res);
+    }}
+    store_{tag}(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
+}}
+
+void launch_eri_{tag}(const EriLaunch &L, int mixed, cudaStream_t s) {{
+    if (L.nquart <= 0) return;
+    const long long blocks = (L.nquart + 127) / 128;
+    if (mixed) eri_kernel_{tag}<1><<<(unsigned)blocks, 128, 0, s>>>(L);
+    else eri_kernel_{tag}<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+}}
+{schwarz}
+}}  // namespace molints
+"""
+
+
+def emit_dispatch(pairs):
+    cls = pair_classes()
+    lines = ["// Generated by gen_eri.py.  Do not edit.", "#pragma once",
+             '#include "eri_common.cuh"', "namespace molints {"]
+    for X, Y in pairs:
+        t = tag_of(X, Y)
+        lines.append(f"void launch_eri_{t}(const EriLaunch &L, int mixed, cudaStream_t s);")
+        if X == Y:
+            lines.append(f"void launch_schwarz_{t}(const PairTab &P, const BoysTab &B, int p0, "
+                         f"int np, double4 *geo_rw, cudaStream_t s);")
+    lines.append("typedef void (*EriLauncher)(const EriLaunch &, int, cudaStream_t);")
+    lines.append("typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, "
+                 "double4 *, cudaStream_t);")
+    lines.append(f"constexpr int kLmax = {LMAX};")
+    lines.append(f"constexpr int kNumPairClasses = {len(cls)};")
+    lines.append("// pair class c = (kPairClassLa[c], kPairClassLb[c]), ordered by la+lb then la")
+    lines.append("constexpr int kPairClassLa[] = {" + ", ".join(str(c[0]) for c in cls) + "};")
+    lines.append("constexpr int kPairClassLb[] = {" + ", ".join(str(c[1]) for c in cls) + "};")
+    lines.append("// kEriLaunchers[x][y], x >= y (bra class x, ket class y)")
+    lines.append(f"static const EriLauncher kEriLaunchers[{len(cls)}][{len(cls)}] = {{")
+    for i, X in enumerate(cls):
+        row = []
+        for j, Y in enumerate(cls):
+            row.append(f"launch_eri_{tag_of(X, Y)}" if j <= i else "nullptr")
+        lines.append("    {" + ", ".join(row) + "},")
+    lines.append("};")
+    lines.append(f"static const char *const kEriNames[{len(cls)}][{len(cls)}] = {{")
+    for i, X in enumerate(cls):
+        row = [f'"eri_{tag_of(X, Y)}"' if j <= i else "nullptr" for j, Y in enumerate(cls)]
+        lines.append("    {" + ", ".join(row) + "},")
+    lines.append("};")
+    lines.append(f"static const char *const kSchwarzNames[{len(cls)}] = {{")
+    lines.append("    " + ", ".join(f'"schwarz_{tag_of(X, X)[:2]}"' for X in cls))
+    lines.append("};")
+    lines.append(f"static const SchwarzLauncher kSchwarzLaunchers[{len(cls)}] = {{")
+    lines.append("    " + ", ".join(f"launch_schwarz_{tag_of(X, X)}" for X in cls))
+    lines.append("};")
+    lines.append("}  // namespace molints")
+    return "\n".join(lines) + "\n"
+
+
+def generate(out_dir: Path = OUT_DIR):
+    out_dir.mkdir(parents=True, exist_ok=True)
+    pairs = class_pairs()
+    written = []
+    for X, Y in pairs:
+        p = out_dir / f"eri_{tag_of(X, Y)}.cu"
+        src = emit_class_pair(X, Y)
+        if not p.exists() or p.read_text() != src:
+            p.write_text(src)
+        written.append(p)
+    d = HERE / "eri_dispatch.h"
+    src = emit_dispatch(pairs)
+    if not d.exists() or d.read_text() != src:
+        d.write_text(src)
+    return written
+
+
+if __name__ == "__main__":
+    files = generate()
+    print(f"{len(files)} class-pair kernels in {OUT_DIR}", file=sys.stderr)

@@ -1,0 +1,404 @@
+// Generated by gen_eri.py -- class (dd|ss).  Do not edit.
+// VRR entries: 70, contracted block: 31, HRR lines: 79, outputs: 36.
+#include "../eri_common.cuh"
+
+namespace molints {
+
+// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[36]
+// (ma, mb, mc, md row-major).  VT is the VRR arithmetic type (double, or float for MIXED).
+template <typename VT>
+__device__ __forceinline__ void quartet_ddss(const PairTab &P, const BoysTab &B, int p, int q,
+                                              double *__restrict__ res) {
+    const int4 ib_ = __ldg(&P.info[p]);
+    const int4 ik_ = __ldg(&P.info[q]);
+    double acc[31];
+#pragma unroll
+    for (int x = 0; x < 31; ++x) acc[x] = 0.0;
+    for (int i = 0; i < ib_.y; ++i) {
+        const PrimPair bra = load_pp(P.pp, ib_.x + i);
+        for (int j = 0; j < ik_.y; ++j) {
+            const PrimPair ket = load_pp(P.pp, ik_.x + j);
+            const double r = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = r * r;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double T = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = bra.kab * ket.kab * r;
+            double F[5];
+            boys_fm<4>(T, B, F);
+            const VT PAx = (VT)bra.pax, PAy = (VT)bra.pay, PAz = (VT)bra.paz;
+            const VT QCx = (VT)ket.pax, QCy = (VT)ket.pay, QCz = (VT)ket.paz;
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const VT WPx = (VT)(-ez * PQx), WPy = (VT)(-ez * PQy), WPz = (VT)(-ez * PQz);
+            const VT WQx = (VT)(zz * PQx), WQy = (VT)(zz * PQy), WQz = (VT)(zz * PQz);
+            const VT oo2z = (VT)bra.oo2z, oo2e = (VT)ket.oo2z, oo2ze = (VT)(0.5 * r2);
+            const VT rho_z = (VT)ez, rho_e = (VT)zz;
+            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz;
+            (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;
+            (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;
+            const VT v0_0_0 = (VT)(pref * F[0]);
+            const VT v0_0_1 = (VT)(pref * F[1]);
+            const VT v0_0_2 = (VT)(pref * F[2]);
+            const VT v0_0_3 = (VT)(pref * F[3]);
+            const VT v0_0_4 = (VT)(pref * F[4]);
+            const VT v1_0_0 = PAx * v0_0_0 + WPx * v0_0_1;
+            const VT v1_0_1 = PAx * v0_0_1 + WPx * v0_0_2;
+            const VT v1_0_2 = PAx * v0_0_2 + WPx * v0_0_3;
+            const VT v1_0_3 = PAx * v0_0_3 + WPx * v0_0_4;
+            const VT v2_0_0 = PAy * v0_0_0 + WPy * v0_0_1;
+            const VT v2_0_1 = PAy * v0_0_1 + WPy * v0_0_2;
+            const VT v2_0_2 = PAy * v0_0_2 + WPy * v0_0_3;
+            const VT v2_0_3 = PAy * v0_0_3 + WPy * v0_0_4;
+            const VT v3_0_0 = PAz * v0_0_0 + WPz * v0_0_1;
+            const VT v3_0_1 = PAz * v0_0_1 + WPz * v0_0_2;
+            const VT v3_0_2 = PAz * v0_0_2 + WPz * v0_0_3;
+            const VT v3_0_3 = PAz * v0_0_3 + WPz * v0_0_4;
+            const VT v4_0_0 = PAx * v1_0_0 + WPx * v1_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v4_0_1 = PAx * v1_0_1 + WPx * v1_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v4_0_2 = PAx * v1_0_2 + WPx * v1_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v5_0_0 = PAx * v2_0_0 + WPx * v2_0_1;
+            const VT v5_0_1 = PAx * v2_0_1 + WPx * v2_0_2;
+            const VT v5_0_2 = PAx * v2_0_2 + WPx * v2_0_3;
+            const VT v6_0_0 = PAx * v3_0_0 + WPx * v3_0_1;
+            const VT v6_0_1 = PAx * v3_0_1 + WPx * v3_0_2;
+            const VT v6_0_2 = PAx * v3_0_2 + WPx * v3_0_3;
+            const VT v7_0_0 = PAy * v2_0_0 + WPy * v2_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v7_0_1 = PAy * v2_0_1 + WPy * v2_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v7_0_2 = PAy * v2_0_2 + WPy * v2_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v8_0_0 = PAy * v3_0_0 + WPy * v3_0_1;
+            const VT v8_0_1 = PAy * v3_0_1 + WPy * v3_0_2;
+            const VT v8_0_2 = PAy * v3_0_2 + WPy * v3_0_3;
+            const VT v9_0_0 = PAz * v3_0_0 + WPz * v3_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v9_0_1 = PAz * v3_0_1 + WPz * v3_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v9_0_2 = PAz * v3_0_2 + WPz * v3_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v10_0_0 = PAx * v4_0_0 + WPx * v4_0_1 + (VT)2.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v10_0_1 = PAx * v4_0_1 + WPx * v4_0_2 + (VT)2.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v11_0_0 = PAx * v5_0_0 + WPx * v5_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v11_0_1 = PAx * v5_0_1 + WPx * v5_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v12_0_0 = PAx * v6_0_0 + WPx * v6_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v12_0_1 = PAx * v6_0_1 + WPx * v6_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v13_0_0 = PAy * v5_0_0 + WPy * v5_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v13_0_1 = PAy * v5_0_1 + WPy * v5_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v14_0_0 = PAz * v6_0_0 + WPz * v6_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v14_0_1 = PAz * v6_0_1 + WPz * v6_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v15_0_0 = PAx * v8_0_0 + WPx * v8_0_1;
+            const VT v15_0_1 = PAx * v8_0_1 + WPx * v8_0_2;
+            const VT v16_0_0 = PAy * v7_0_0 + WPy * v7_0_1 + (VT)2.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v16_0_1 = PAy * v7_0_1 + WPy * v7_0_2 + (VT)2.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v17_0_0 = PAy * v8_0_0 + WPy * v8_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v17_0_1 = PAy * v8_0_1 + WPy * v8_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v18_0_0 = PAz * v8_0_0 + WPz * v8_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v18_0_1 = PAz * v8_0_1 + WPz * v8_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v19_0_0 = PAz * v9_0_0 + WPz * v9_0_1 + (VT)2.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v19_0_1 = PAz * v9_0_1 + WPz * v9_0_2 + (VT)2.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v20_0_0 = PAx * v10_0_0 + WPx * v10_0_1 + (VT)3.0 * oo2z * (v4_0_0 - rho_z * v4_0_1);
+            const VT v21_0_0 = PAx * v11_0_0 + WPx * v11_0_1 + (VT)2.0 * oo2z * (v5_0_0 - rho_z * v5_0_1);
+            const VT v22_0_0 = PAx * v12_0_0 + WPx * v12_0_1 + (VT)2.0 * oo2z * (v6_0_0 - rho_z * v6_0_1);
+            const VT v23_0_0 = PAx * v13_0_0 + WPx * v13_0_1 + (VT)1.0 * oo2z * (v7_0_0 - rho_z * v7_0_1);
+            const VT v24_0_0 = PAx * v15_0_0 + WPx * v15_0_1 + (VT)1.0 * oo2z * (v8_0_0 - rho_z * v8_0_1);
+            const VT v25_0_0 = PAx * v14_0_0 + WPx * v14_0_1 + (VT)1.0 * oo2z * (v9_0_0 - rho_z * v9_0_1);
+            const VT v26_0_0 = PAy * v13_0_0 + WPy * v13_0_1 + (VT)2.0 * oo2z * (v5_0_0 - rho_z * v5_0_1);
+            const VT v27_0_0 = PAy * v15_0_0 + WPy * v15_0_1 + (VT)1.0 * oo2z * (v6_0_0 - rho_z * v6_0_1);
+            const VT v28_0_0 = PAz * v15_0_0 + WPz * v15_0_1 + (VT)1.0 * oo2z * (v5_0_0 - rho_z * v5_0_1);
+            const VT v29_0_0 = PAz * v14_0_0 + WPz * v14_0_1 + (VT)2.0 * oo2z * (v6_0_0 - rho_z * v6_0_1);
+            const VT v30_0_0 = PAy * v16_0_0 + WPy * v16_0_1 + (VT)3.0 * oo2z * (v7_0_0 - rho_z * v7_0_1);
+            const VT v31_0_0 = PAy * v17_0_0 + WPy * v17_0_1 + (VT)2.0 * oo2z * (v8_0_0 - rho_z * v8_0_1);
+            const VT v32_0_0 = PAy * v18_0_0 + WPy * v18_0_1 + (VT)1.0 * oo2z * (v9_0_0 - rho_z * v9_0_1);
+            const VT v33_0_0 = PAz * v18_0_0 + WPz * v18_0_1 + (VT)2.0 * oo2z * (v8_0_0 - rho_z * v8_0_1);
+            const VT v34_0_0 = PAz * v19_0_0 + WPz * v19_0_1 + (VT)3.0 * oo2z * (v9_0_0 - rho_z * v9_0_1);
+            acc[0] += (double)v4_0_0;
+            acc[1] += (double)v5_0_0;
+            acc[2] += (double)v6_0_0;
+            acc[3] += (double)v7_0_0;
+            acc[4] += (double)v8_0_0;
+            acc[5] += (double)v9_0_0;
+            acc[6] += (double)v10_0_0;
+            acc[7] += (double)v11_0_0;
+            acc[8] += (double)v12_0_0;
+            acc[9] += (double)v13_0_0;
+            acc[10] += (double)v14_0_0;
+            acc[11] += (double)v15_0_0;
+            acc[12] += (double)v16_0_0;
+            acc[13] += (double)v17_0_0;
+            acc[14] += (double)v18_0_0;
+            acc[15] += (double)v19_0_0;
+            acc[16] += (double)v20_0_0;
+            acc[17] += (double)v21_0_0;
+            acc[18] += (double)v22_0_0;
+            acc[19] += (double)v23_0_0;
+            acc[20] += (double)v24_0_0;
+            acc[21] += (double)v25_0_0;
+            acc[22] += (double)v26_0_0;
+            acc[23] += (double)v27_0_0;
+            acc[24] += (double)v28_0_0;
+            acc[25] += (double)v29_0_0;
+            acc[26] += (double)v30_0_0;
+            acc[27] += (double)v31_0_0;
+            acc[28] += (double)v32_0_0;
+            acc[29] += (double)v33_0_0;
+            acc[30] += (double)v34_0_0;
+        }
+    }
+    const double4 gb = ldg4(&P.geo[p]);
+    const double4 gk = ldg4(&P.geo[q]);
+    const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
+    const double CDx = gk.x, CDy = gk.y, CDz = gk.z;
+    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
+    const double h10_1_0 = acc[16] + ABx * acc[6];
+    const double h4_1_0 = acc[6] + ABx * acc[0];
+    const double h4_4_0 = h10_1_0 + ABx * h4_1_0;
+    const double h10_2_0 = acc[17] + ABy * acc[6];
+    const double h4_2_0 = acc[7] + ABy * acc[0];
+    const double h4_5_0 = h10_2_0 + ABx * h4_2_0;
+    const double h10_3_0 = acc[18] + ABz * acc[6];
+    const double h4_3_0 = acc[8] + ABz * acc[0];
+    const double h4_6_0 = h10_3_0 + ABx * h4_3_0;
+    const double h11_2_0 = acc[19] + ABy * acc[7];
+    const double h4_7_0 = h11_2_0 + ABy * h4_2_0;
+    const double h11_3_0 = acc[20] + ABz * acc[7];
+    const double h4_8_0 = h11_3_0 + ABy * h4_3_0;
+    const double h12_3_0 = acc[21] + ABz * acc[8];
+    const double h4_9_0 = h12_3_0 + ABz * h4_3_0;
+    const double h11_1_0 = acc[17] + ABx * acc[7];
+    const double h5_1_0 = acc[7] + ABx * acc[1];
+    const double h5_4_0 = h11_1_0 + ABx * h5_1_0;
+    const double h5_2_0 = acc[9] + ABy * acc[1];
+    const double h5_5_0 = h11_2_0 + ABx * h5_2_0;
+    const double h5_3_0 = acc[11] + ABz * acc[1];
+    const double h5_6_0 = h11_3_0 + ABx * h5_3_0;
+    const double h13_2_0 = acc[22] + ABy * acc[9];
+    const double h5_7_0 = h13_2_0 + ABy * h5_2_0;
+    const double h13_3_0 = acc[23] + ABz * acc[9];
+    const double h5_8_0 = h13_3_0 + ABy * h5_3_0;
+    const double h15_3_0 = acc[24] + ABz * acc[11];
+    const double h5_9_0 = h15_3_0 + ABz * h5_3_0;
+    const double h12_1_0 = acc[18] + ABx * acc[8];
+    const double h6_1_0 = acc[8] + ABx * acc[2];
+    const double h6_4_0 = h12_1_0 + ABx * h6_1_0;
+    const double h12_2_0 = acc[20] + ABy * acc[8];
+    const double h6_2_0 = acc[11] + ABy * acc[2];
+    const double h6_5_0 = h12_2_0 + ABx * h6_2_0;
+    const double h6_3_0 = acc[10] + ABz * acc[2];
+    const double h6_6_0 = h12_3_0 + ABx * h6_3_0;
+    const double h15_2_0 = acc[23] + ABy * acc[11];
+    const double h6_7_0 = h15_2_0 + ABy * h6_2_0;
+    const double h6_8_0 = h15_3_0 + ABy * h6_3_0;
+    const double h14_3_0 = acc[25] + ABz * acc[10];
+    const double h6_9_0 = h14_3_0 + ABz * h6_3_0;
+    const double h13_1_0 = acc[19] + ABx * acc[9];
+    const double h7_1_0 = acc[9] + ABx * acc[3];
+    const double h7_4_0 = h13_1_0 + ABx * h7_1_0;
+    const double h7_2_0 = acc[12] + ABy * acc[3];
+    const double h7_5_0 = h13_2_0 + ABx * h7_2_0;
+    const double h7_3_0 = acc[13] + ABz * acc[3];
+    const double h7_6_0 = h13_3_0 + ABx * h7_3_0;
+    const double h16_2_0 = acc[26] + ABy * acc[12];
+    const double h7_7_0 = h16_2_0 + ABy * h7_2_0;
+    const double h16_3_0 = acc[27] + ABz * acc[12];
+    const double h7_8_0 = h16_3_0 + ABy * h7_3_0;
+    const double h17_3_0 = acc[28] + ABz * acc[13];
+    const double h7_9_0 = h17_3_0 + ABz * h7_3_0;
+    const double h15_1_0 = acc[20] + ABx * acc[11];
+    const double h8_1_0 = acc[11] + ABx * acc[4];
+    const double h8_4_0 = h15_1_0 + ABx * h8_1_0;
+    const double h8_2_0 = acc[13] + ABy * acc[4];
+    const double h8_5_0 = h15_2_0 + ABx * h8_2_0;
+    const double h8_3_0 = acc[14] + ABz * acc[4];
+    const double h8_6_0 = h15_3_0 + ABx * h8_3_0;
+    const double h17_2_0 = acc[27] + ABy * acc[13];
+    const double h8_7_0 = h17_2_0 + ABy * h8_2_0;
+    const double h8_8_0 = h17_3_0 + ABy * h8_3_0;
+    const double h18_3_0 = acc[29] + ABz * acc[14];
+    const double h8_9_0 = h18_3_0 + ABz * h8_3_0;
+    const double h14_1_0 = acc[21] + ABx * acc[10];
+    const double h9_1_0 = acc[10] + ABx * acc[5];
+    const double h9_4_0 = h14_1_0 + ABx * h9_1_0;
+    const double h14_2_0 = acc[24] + ABy * acc[10];
+    const double h9_2_0 = acc[14] + ABy * acc[5];
+    const double h9_5_0 = h14_2_0 + ABx * h9_2_0;
+    const double h9_3_0 = acc[15] + ABz * acc[5];
+    const double h9_6_0 = h14_3_0 + ABx * h9_3_0;
+    const double h18_2_0 = acc[28] + ABy * acc[14];
+    const double h9_7_0 = h18_2_0 + ABy * h9_2_0;
+    const double h9_8_0 = h18_3_0 + ABy * h9_3_0;
+    const double h19_3_0 = acc[30] + ABz * acc[15];
+    const double h9_9_0 = h19_3_0 + ABz * h9_3_0;
+    res[0] = h4_4_0 * 0.3333333333333334;
+    res[1] = h4_5_0 * 0.5773502691896258;
+    res[2] = h4_6_0 * 0.5773502691896258;
+    res[3] = h4_7_0 * 0.3333333333333334;
+    res[4] = h4_8_0 * 0.5773502691896258;
+    res[5] = h4_9_0 * 0.3333333333333334;
+    res[6] = h5_4_0 * 0.5773502691896258;
+    res[7] = h5_5_0;
+    res[8] = h5_6_0;
+    res[9] = h5_7_0 * 0.5773502691896258;
+    res[10] = h5_8_0;
+    res[11] = h5_9_0 * 0.5773502691896258;
+    res[12] = h6_4_0 * 0.5773502691896258;
+    res[13] = h6_5_0;
+    res[14] = h6_6_0;
+    res[15] = h6_7_0 * 0.5773502691896258;
+    res[16] = h6_8_0;
+    res[17] = h6_9_0 * 0.5773502691896258;
+    res[18] = h7_4_0 * 0.3333333333333334;
+    res[19] = h7_5_0 * 0.5773502691896258;
+    res[20] = h7_6_0 * 0.5773502691896258;
+    res[21] = h7_7_0 * 0.3333333333333334;
+    res[22] = h7_8_0 * 0.5773502691896258;
+    res[23] = h7_9_0 * 0.3333333333333334;
+    res[24] = h8_4_0 * 0.5773502691896258;
+    res[25] = h8_5_0;
+    res[26] = h8_6_0;
+    res[27] = h8_7_0 * 0.5773502691896258;
+    res[28] = h8_8_0;
+    res[29] = h8_9_0 * 0.5773502691896258;
+    res[30] = h9_4_0 * 0.3333333333333334;
+    res[31] = h9_5_0 * 0.5773502691896258;
+    res[32] = h9_6_0 * 0.5773502691896258;
+    res[33] = h9_7_0 * 0.3333333333333334;
+    res[34] = h9_8_0 * 0.5773502691896258;
+    res[35] = h9_9_0 * 0.3333333333333334;
+}
+
+__device__ __forceinline__ void store_ddss(double *__restrict__ out, const int4 ib_, const int4 ik_,
+                                            bool same, const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    (void)dab; (void)dcd;
+    const long long ij_0_0 = pair_index(ib_.z + 0, ib_.w + 0);
+    const long long ij_0_1 = pair_index(ib_.z + 0, ib_.w + 1);
+    const long long ij_0_2 = pair_index(ib_.z + 0, ib_.w + 2);
+    const long long ij_0_3 = pair_index(ib_.z + 0, ib_.w + 3);
+    const long long ij_0_4 = pair_index(ib_.z + 0, ib_.w + 4);
+    const long long ij_0_5 = pair_index(ib_.z + 0, ib_.w + 5);
+    const long long ij_1_0 = pair_index(ib_.z + 1, ib_.w + 0);
+    const long long ij_1_1 = pair_index(ib_.z + 1, ib_.w + 1);
+    const long long ij_1_2 = pair_index(ib_.z + 1, ib_.w + 2);
+    const long long ij_1_3 = pair_index(ib_.z + 1, ib_.w + 3);
+    const long long ij_1_4 = pair_index(ib_.z + 1, ib_.w + 4);
+    const long long ij_1_5 = pair_index(ib_.z + 1, ib_.w + 5);
+    const long long ij_2_0 = pair_index(ib_.z + 2, ib_.w + 0);
+    const long long ij_2_1 = pair_index(ib_.z + 2, ib_.w + 1);
+    const long long ij_2_2 = pair_index(ib_.z + 2, ib_.w + 2);
+    const long long ij_2_3 = pair_index(ib_.z + 2, ib_.w + 3);
+    const long long ij_2_4 = pair_index(ib_.z + 2, ib_.w + 4);
+    const long long ij_2_5 = pair_index(ib_.z + 2, ib_.w + 5);
+    const long long ij_3_0 = pair_index(ib_.z + 3, ib_.w + 0);
+    const long long ij_3_1 = pair_index(ib_.z + 3, ib_.w + 1);
+    const long long ij_3_2 = pair_index(ib_.z + 3, ib_.w + 2);
+    const long long ij_3_3 = pair_index(ib_.z + 3, ib_.w + 3);
+    const long long ij_3_4 = pair_index(ib_.z + 3, ib_.w + 4);
+    const long long ij_3_5 = pair_index(ib_.z + 3, ib_.w + 5);
+    const long long ij_4_0 = pair_index(ib_.z + 4, ib_.w + 0);
+    const long long ij_4_1 = pair_index(ib_.z + 4, ib_.w + 1);
+    const long long ij_4_2 = pair_index(ib_.z + 4, ib_.w + 2);
+    const long long ij_4_3 = pair_index(ib_.z + 4, ib_.w + 3);
+    const long long ij_4_4 = pair_index(ib_.z + 4, ib_.w + 4);
+    const long long ij_4_5 = pair_index(ib_.z + 4, ib_.w + 5);
+    const long long ij_5_0 = pair_index(ib_.z + 5, ib_.w + 0);
+    const long long ij_5_1 = pair_index(ib_.z + 5, ib_.w + 1);
+    const long long ij_5_2 = pair_index(ib_.z + 5, ib_.w + 2);
+    const long long ij_5_3 = pair_index(ib_.z + 5, ib_.w + 3);
+    const long long ij_5_4 = pair_index(ib_.z + 5, ib_.w + 4);
+    const long long ij_5_5 = pair_index(ib_.z + 5, ib_.w + 5);
+    const long long kl_0_0 = pair_index(ik_.z + 0, ik_.w + 0);
+    { const long long ij = ij_0_0, kl = kl_0_0;
+      if ((!dab || 0 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[0]; }
+    { const long long ij = ij_0_1, kl = kl_0_0;
+      if ((!dab || 0 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[1]; }
+    { const long long ij = ij_0_2, kl = kl_0_0;
+      if ((!dab || 0 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[2]; }
+    { const long long ij = ij_0_3, kl = kl_0_0;
+      if ((!dab || 0 >= 3) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[3]; }
+    { const long long ij = ij_0_4, kl = kl_0_0;
+      if ((!dab || 0 >= 4) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[4]; }
+    { const long long ij = ij_0_5, kl = kl_0_0;
+      if ((!dab || 0 >= 5) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[5]; }
+    { const long long ij = ij_1_0, kl = kl_0_0;
+      if ((!dab || 1 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[6]; }
+    { const long long ij = ij_1_1, kl = kl_0_0;
+      if ((!dab || 1 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[7]; }
+    { const long long ij = ij_1_2, kl = kl_0_0;
+      if ((!dab || 1 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[8]; }
+    { const long long ij = ij_1_3, kl = kl_0_0;
+      if ((!dab || 1 >= 3) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[9]; }
+    { const long long ij = ij_1_4, kl = kl_0_0;
+      if ((!dab || 1 >= 4) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[10]; }
+    { const long long ij = ij_1_5, kl = kl_0_0;
+      if ((!dab || 1 >= 5) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[11]; }
+    { const long long ij = ij_2_0, kl = kl_0_0;
+      if ((!dab || 2 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[12]; }
+    { const long long ij = ij_2_1, kl = kl_0_0;
+      if ((!dab || 2 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[13]; }
+    { const long long ij = ij_2_2, kl = kl_0_0;
+      if ((!dab || 2 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[14]; }
+    { const long long ij = ij_2_3, kl = kl_0_0;
+      if ((!dab || 2 >= 3) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[15]; }
+    { const long long ij = ij_2_4, kl = kl_0_0;
+      if ((!dab || 2 >= 4) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[16]; }
+    { const long long ij = ij_2_5, kl = kl_0_0;
+      if ((!dab || 2 >= 5) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[17]; }
+    { const long long ij = ij_3_0, kl = kl_0_0;
+      if ((!dab || 3 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[18]; }
+    { const long long ij = ij_3_1, kl = kl_0_0;
+      if ((!dab || 3 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[19]; }
+    { const long long ij = ij_3_2, kl = kl_0_0;
+      if ((!dab || 3 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[20]; }
+    { const long long ij = ij_3_3, kl = kl_0_0;
+      if ((!dab || 3 >= 3) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[21]; }
+    { const long long ij = ij_3_4, kl = kl_0_0;
+      if ((!dab || 3 >= 4) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[22]; }
+    { const long long ij = ij_3_5, kl = kl_0_0;
+      if ((!dab || 3 >= 5) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[23]; }
+    { const long long ij = ij_4_0, kl = kl_0_0;
+      if ((!dab || 4 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[24]; }
+    { const long long ij = ij_4_1, kl = kl_0_0;
+      if ((!dab || 4 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[25]; }
+    { const long long ij = ij_4_2, kl = kl_0_0;
+      if ((!dab || 4 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[26]; }
+    { const long long ij = ij_4_3, kl = kl_0_0;
+      if ((!dab || 4 >= 3) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[27]; }
+    { const long long ij = ij_4_4, kl = kl_0_0;
+      if ((!dab || 4 >= 4) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[28]; }
+    { const long long ij = ij_4_5, kl = kl_0_0;
+      if ((!dab || 4 >= 5) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[29]; }
+    { const long long ij = ij_5_0, kl = kl_0_0;
+      if ((!dab || 5 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[30]; }
+    { const long long ij = ij_5_1, kl = kl_0_0;
+      if ((!dab || 5 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[31]; }
+    { const long long ij = ij_5_2, kl = kl_0_0;
+      if ((!dab || 5 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[32]; }
+    { const long long ij = ij_5_3, kl = kl_0_0;
+      if ((!dab || 5 >= 3) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[33]; }
+    { const long long ij = ij_5_4, kl = kl_0_0;
+      if ((!dab || 5 >= 4) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[34]; }
+    { const long long ij = ij_5_5, kl = kl_0_0;
+      if ((!dab || 5 >= 5) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[35]; }
+}
+
+template <int MIXED>
+__global__ void __launch_bounds__(128) eri_kernel_ddss(const EriLaunch L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.nquart) return;
+    int p, q;
+    decode_quartet(L, t, p, q);
+    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    double res[36];
+    if (bound < L.screen_cut) {
+#pragma unroll
+        for (int x = 0; x < 36; ++x) res[x] = 0.0;
+    } else if (MIXED && bound < L.fp32_cut) {
+        quartet_ddss<float>(L.pairs, L.boys, p, q, res);
+    } else {
+        quartet_ddss<double>(L.pairs, L.boys, p, q, res);
+    }
+    store_ddss(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
+}
+
+void launch_eri_ddss(const EriLaunch &L, int mixed, cudaStream_t s) {
+    if (L.nquart <= 0) return;
+    const long long blocks = (L.nquart + 127) / 128;
+    if (mixed) eri_kernel_ddss<1><<<(unsigned)blocks, 128, 0, s>>>(L);
+    else eri_kernel_ddss<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+}
+
+}  // namespace molints

@@ -1,0 +1,1336 @@
+// Generated by gen_eri.py -- class (dp|pp).  Do not edit.
+// VRR entries: 276, contracted block: 144, HRR lines: 324, outputs: 162.
+#include "../eri_common.cuh"
+
+namespace molints {
+
+// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[162]
+// (ma, mb, mc, md row-major).  VT is the VRR arithmetic type (double, or float for MIXED).
+template <typename VT>
+__device__ __forceinline__ void quartet_dppp(const PairTab &P, const BoysTab &B, int p, int q,
+                                              double *__restrict__ res) {
+    const int4 ib_ = __ldg(&P.info[p]);
+    const int4 ik_ = __ldg(&P.info[q]);
+    double acc[144];
+#pragma unroll
+    for (int x = 0; x < 144; ++x) acc[x] = 0.0;
+    for (int i = 0; i < ib_.y; ++i) {
+        const PrimPair bra = load_pp(P.pp, ib_.x + i);
+        for (int j = 0; j < ik_.y; ++j) {
+            const PrimPair ket = load_pp(P.pp, ik_.x + j);
+            const double r = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = r * r;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double T = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = bra.kab * ket.kab * r;
+            double F[6];
+            boys_fm<5>(T, B, F);
+            const VT PAx = (VT)bra.pax, PAy = (VT)bra.pay, PAz = (VT)bra.paz;
+            const VT QCx = (VT)ket.pax, QCy = (VT)ket.pay, QCz = (VT)ket.paz;
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const VT WPx = (VT)(-ez * PQx), WPy = (VT)(-ez * PQy), WPz = (VT)(-ez * PQz);
+            const VT WQx = (VT)(zz * PQx), WQy = (VT)(zz * PQy), WQz = (VT)(zz * PQz);
+            const VT oo2z = (VT)bra.oo2z, oo2e = (VT)ket.oo2z, oo2ze = (VT)(0.5 * r2);
+            const VT rho_z = (VT)ez, rho_e = (VT)zz;
+            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz;
+            (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;
+            (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;
+            const VT v0_0_0 = (VT)(pref * F[0]);
+            const VT v0_0_1 = (VT)(pref * F[1]);
+            const VT v0_0_2 = (VT)(pref * F[2]);
+            const VT v0_0_3 = (VT)(pref * F[3]);
+            const VT v0_0_4 = (VT)(pref * F[4]);
+            const VT v0_0_5 = (VT)(pref * F[5]);
+            const VT v1_0_0 = PAx * v0_0_0 + WPx * v0_0_1;
+            const VT v1_0_1 = PAx * v0_0_1 + WPx * v0_0_2;
+            const VT v1_0_2 = PAx * v0_0_2 + WPx * v0_0_3;
+            const VT v1_0_3 = PAx * v0_0_3 + WPx * v0_0_4;
+            const VT v1_0_4 = PAx * v0_0_4 + WPx * v0_0_5;
+            const VT v2_0_0 = PAy * v0_0_0 + WPy * v0_0_1;
+            const VT v2_0_1 = PAy * v0_0_1 + WPy * v0_0_2;
+            const VT v2_0_2 = PAy * v0_0_2 + WPy * v0_0_3;
+            const VT v2_0_3 = PAy * v0_0_3 + WPy * v0_0_4;
+            const VT v2_0_4 = PAy * v0_0_4 + WPy * v0_0_5;
+            const VT v3_0_0 = PAz * v0_0_0 + WPz * v0_0_1;
+            const VT v3_0_1 = PAz * v0_0_1 + WPz * v0_0_2;
+            const VT v3_0_2 = PAz * v0_0_2 + WPz * v0_0_3;
+            const VT v3_0_3 = PAz * v0_0_3 + WPz * v0_0_4;
+            const VT v3_0_4 = PAz * v0_0_4 + WPz * v0_0_5;
+            const VT v4_0_0 = PAx * v1_0_0 + WPx * v1_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v4_0_1 = PAx * v1_0_1 + WPx * v1_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v4_0_2 = PAx * v1_0_2 + WPx * v1_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v4_0_3 = PAx * v1_0_3 + WPx * v1_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v5_0_0 = PAx * v2_0_0 + WPx * v2_0_1;
+            const VT v5_0_1 = PAx * v2_0_1 + WPx * v2_0_2;
+            const VT v5_0_2 = PAx * v2_0_2 + WPx * v2_0_3;
+            const VT v5_0_3 = PAx * v2_0_3 + WPx * v2_0_4;
+            const VT v6_0_0 = PAx * v3_0_0 + WPx * v3_0_1;
+            const VT v6_0_1 = PAx * v3_0_1 + WPx * v3_0_2;
+            const VT v6_0_2 = PAx * v3_0_2 + WPx * v3_0_3;
+            const VT v6_0_3 = PAx * v3_0_3 + WPx * v3_0_4;
+            const VT v7_0_0 = PAy * v2_0_0 + WPy * v2_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v7_0_1 = PAy * v2_0_1 + WPy * v2_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v7_0_2 = PAy * v2_0_2 + WPy * v2_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v7_0_3 = PAy * v2_0_3 + WPy * v2_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v8_0_0 = PAy * v3_0_0 + WPy * v3_0_1;
+            const VT v8_0_1 = PAy * v3_0_1 + WPy * v3_0_2;
+            const VT v8_0_2 = PAy * v3_0_2 + WPy * v3_0_3;
+            const VT v8_0_3 = PAy * v3_0_3 + WPy * v3_0_4;
+            const VT v9_0_0 = PAz * v3_0_0 + WPz * v3_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v9_0_1 = PAz * v3_0_1 + WPz * v3_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v9_0_2 = PAz * v3_0_2 + WPz * v3_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v9_0_3 = PAz * v3_0_3 + WPz * v3_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v10_0_0 = PAx * v4_0_0 + WPx * v4_0_1 + (VT)2.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v10_0_1 = PAx * v4_0_1 + WPx * v4_0_2 + (VT)2.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v10_0_2 = PAx * v4_0_2 + WPx * v4_0_3 + (VT)2.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v11_0_0 = PAx * v5_0_0 + WPx * v5_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v11_0_1 = PAx * v5_0_1 + WPx * v5_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v11_0_2 = PAx * v5_0_2 + WPx * v5_0_3 + (VT)1.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v12_0_0 = PAx * v6_0_0 + WPx * v6_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v12_0_1 = PAx * v6_0_1 + WPx * v6_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v12_0_2 = PAx * v6_0_2 + WPx * v6_0_3 + (VT)1.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v13_0_0 = PAy * v5_0_0 + WPy * v5_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v13_0_1 = PAy * v5_0_1 + WPy * v5_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v13_0_2 = PAy * v5_0_2 + WPy * v5_0_3 + (VT)1.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v14_0_0 = PAz * v6_0_0 + WPz * v6_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v14_0_1 = PAz * v6_0_1 + WPz * v6_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v14_0_2 = PAz * v6_0_2 + WPz * v6_0_3 + (VT)1.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v15_0_0 = PAx * v8_0_0 + WPx * v8_0_1;
+            const VT v15_0_1 = PAx * v8_0_1 + WPx * v8_0_2;
+            const VT v15_0_2 = PAx * v8_0_2 + WPx * v8_0_3;
+            const VT v16_0_0 = PAy * v7_0_0 + WPy * v7_0_1 + (VT)2.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v16_0_1 = PAy * v7_0_1 + WPy * v7_0_2 + (VT)2.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v16_0_2 = PAy * v7_0_2 + WPy * v7_0_3 + (VT)2.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v17_0_0 = PAy * v8_0_0 + WPy * v8_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v17_0_1 = PAy * v8_0_1 + WPy * v8_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v17_0_2 = PAy * v8_0_2 + WPy * v8_0_3 + (VT)1.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v18_0_0 = PAz * v8_0_0 + WPz * v8_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v18_0_1 = PAz * v8_0_1 + WPz * v8_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v18_0_2 = PAz * v8_0_2 + WPz * v8_0_3 + (VT)1.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v19_0_0 = PAz * v9_0_0 + WPz * v9_0_1 + (VT)2.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v19_0_1 = PAz * v9_0_1 + WPz * v9_0_2 + (VT)2.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v19_0_2 = PAz * v9_0_2 + WPz * v9_0_3 + (VT)2.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v1_1_1 = QCx * v1_0_1 + WQx * v1_0_2 + (VT)1.0 * oo2ze * v0_0_2;
+            const VT v2_1_1 = QCx * v2_0_1 + WQx * v2_0_2;
+            const VT v3_1_1 = QCx * v3_0_1 + WQx * v3_0_2;
+            const VT v4_1_0 = QCx * v4_0_0 + WQx * v4_0_1 + (VT)2.0 * oo2ze * v1_0_1;
+            const VT v4_1_1 = QCx * v4_0_1 + WQx * v4_0_2 + (VT)2.0 * oo2ze * v1_0_2;
+            const VT v5_1_0 = QCx * v5_0_0 + WQx * v5_0_1 + (VT)1.0 * oo2ze * v2_0_1;
+            const VT v5_1_1 = QCx * v5_0_1 + WQx * v5_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v6_1_0 = QCx * v6_0_0 + WQx * v6_0_1 + (VT)1.0 * oo2ze * v3_0_1;
+            const VT v6_1_1 = QCx * v6_0_1 + WQx * v6_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v7_1_0 = QCx * v7_0_0 + WQx * v7_0_1;
+            const VT v7_1_1 = QCx * v7_0_1 + WQx * v7_0_2;
+            const VT v8_1_0 = QCx * v8_0_0 + WQx * v8_0_1;
+            const VT v8_1_1 = QCx * v8_0_1 + WQx * v8_0_2;
+            const VT v9_1_0 = QCx * v9_0_0 + WQx * v9_0_1;
+            const VT v9_1_1 = QCx * v9_0_1 + WQx * v9_0_2;
+            const VT v10_1_0 = QCx * v10_0_0 + WQx * v10_0_1 + (VT)3.0 * oo2ze * v4_0_1;
+            const VT v10_1_1 = QCx * v10_0_1 + WQx * v10_0_2 + (VT)3.0 * oo2ze * v4_0_2;
+            const VT v11_1_0 = QCx * v11_0_0 + WQx * v11_0_1 + (VT)2.0 * oo2ze * v5_0_1;
+            const VT v11_1_1 = QCx * v11_0_1 + WQx * v11_0_2 + (VT)2.0 * oo2ze * v5_0_2;
+            const VT v12_1_0 = QCx * v12_0_0 + WQx * v12_0_1 + (VT)2.0 * oo2ze * v6_0_1;
+            const VT v12_1_1 = QCx * v12_0_1 + WQx * v12_0_2 + (VT)2.0 * oo2ze * v6_0_2;
+            const VT v13_1_0 = QCx * v13_0_0 + WQx * v13_0_1 + (VT)1.0 * oo2ze * v7_0_1;
+            const VT v13_1_1 = QCx * v13_0_1 + WQx * v13_0_2 + (VT)1.0 * oo2ze * v7_0_2;
+            const VT v14_1_0 = QCx * v14_0_0 + WQx * v14_0_1 + (VT)1.0 * oo2ze * v9_0_1;
+            const VT v14_1_1 = QCx * v14_0_1 + WQx * v14_0_2 + (VT)1.0 * oo2ze * v9_0_2;
+            const VT v15_1_0 = QCx * v15_0_0 + WQx * v15_0_1 + (VT)1.0 * oo2ze * v8_0_1;
+            const VT v15_1_1 = QCx * v15_0_1 + WQx * v15_0_2 + (VT)1.0 * oo2ze * v8_0_2;
+            const VT v16_1_0 = QCx * v16_0_0 + WQx * v16_0_1;
+            const VT v16_1_1 = QCx * v16_0_1 + WQx * v16_0_2;
+            const VT v17_1_0 = QCx * v17_0_0 + WQx * v17_0_1;
+            const VT v17_1_1 = QCx * v17_0_1 + WQx * v17_0_2;
+            const VT v18_1_0 = QCx * v18_0_0 + WQx * v18_0_1;
+            const VT v18_1_1 = QCx * v18_0_1 + WQx * v18_0_2;
+            const VT v19_1_0 = QCx * v19_0_0 + WQx * v19_0_1;
+            const VT v19_1_1 = QCx * v19_0_1 + WQx * v19_0_2;
+            const VT v1_2_1 = QCy * v1_0_1 + WQy * v1_0_2;
+            const VT v2_2_1 = QCy * v2_0_1 + WQy * v2_0_2 + (VT)1.0 * oo2ze * v0_0_2;
+            const VT v3_2_1 = QCy * v3_0_1 + WQy * v3_0_2;
+            const VT v4_2_0 = QCy * v4_0_0 + WQy * v4_0_1;
+            const VT v4_2_1 = QCy * v4_0_1 + WQy * v4_0_2;
+            const VT v5_2_0 = QCy * v5_0_0 + WQy * v5_0_1 + (VT)1.0 * oo2ze * v1_0_1;
+            const VT v5_2_1 = QCy * v5_0_1 + WQy * v5_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v6_2_0 = QCy * v6_0_0 + WQy * v6_0_1;
+            const VT v6_2_1 = QCy * v6_0_1 + WQy * v6_0_2;
+            const VT v7_2_0 = QCy * v7_0_0 + WQy * v7_0_1 + (VT)2.0 * oo2ze * v2_0_1;
+            const VT v7_2_1 = QCy * v7_0_1 + WQy * v7_0_2 + (VT)2.0 * oo2ze * v2_0_2;
+            const VT v8_2_0 = QCy * v8_0_0 + WQy * v8_0_1 + (VT)1.0 * oo2ze * v3_0_1;
+            const VT v8_2_1 = QCy * v8_0_1 + WQy * v8_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v9_2_0 = QCy * v9_0_0 + WQy * v9_0_1;
+            const VT v9_2_1 = QCy * v9_0_1 + WQy * v9_0_2;
+            const VT v10_2_0 = QCy * v10_0_0 + WQy * v10_0_1;
+            const VT v10_2_1 = QCy * v10_0_1 + WQy * v10_0_2;
+            const VT v11_2_0 = QCy * v11_0_0 + WQy * v11_0_1 + (VT)1.0 * oo2ze * v4_0_1;
+            const VT v11_2_1 = QCy * v11_0_1 + WQy * v11_0_2 + (VT)1.0 * oo2ze * v4_0_2;
+            const VT v12_2_0 = QCy * v12_0_0 + WQy * v12_0_1;
+            const VT v12_2_1 = QCy * v12_0_1 + WQy * v12_0_2;
+            const VT v13_2_0 = QCy * v13_0_0 + WQy * v13_0_1 + (VT)2.0 * oo2ze * v5_0_1;
+            const VT v13_2_1 = QCy * v13_0_1 + WQy * v13_0_2 + (VT)2.0 * oo2ze * v5_0_2;
+            const VT v14_2_0 = QCy * v14_0_0 + WQy * v14_0_1;
+            const VT v14_2_1 = QCy * v14_0_1 + WQy * v14_0_2;
+            const VT v15_2_0 = QCy * v15_0_0 + WQy * v15_0_1 + (VT)1.0 * oo2ze * v6_0_1;
+            const VT v15_2_1 = QCy * v15_0_1 + WQy * v15_0_2 + (VT)1.0 * oo2ze * v6_0_2;
+            const VT v16_2_0 = QCy * v16_0_0 + WQy * v16_0_1 + (VT)3.0 * oo2ze * v7_0_1;
+            const VT v16_2_1 = QCy * v16_0_1 + WQy * v16_0_2 + (VT)3.0 * oo2ze * v7_0_2;
+            const VT v17_2_0 = QCy * v17_0_0 + WQy * v17_0_1 + (VT)2.0 * oo2ze * v8_0_1;
+            const VT v17_2_1 = QCy * v17_0_1 + WQy * v17_0_2 + (VT)2.0 * oo2ze * v8_0_2;
+            const VT v18_2_0 = QCy * v18_0_0 + WQy * v18_0_1 + (VT)1.0 * oo2ze * v9_0_1;
+            const VT v18_2_1 = QCy * v18_0_1 + WQy * v18_0_2 + (VT)1.0 * oo2ze * v9_0_2;
+            const VT v19_2_0 = QCy * v19_0_0 + WQy * v19_0_1;
+            const VT v19_2_1 = QCy * v19_0_1 + WQy * v19_0_2;
+            const VT v1_3_1 = QCz * v1_0_1 + WQz * v1_0_2;
+            const VT v2_3_1 = QCz * v2_0_1 + WQz * v2_0_2;
+            const VT v3_3_1 = QCz * v3_0_1 + WQz * v3_0_2 + (VT)1.0 * oo2ze * v0_0_2;
+            const VT v4_3_0 = QCz * v4_0_0 + WQz * v4_0_1;
+            const VT v4_3_1 = QCz * v4_0_1 + WQz * v4_0_2;
+            const VT v5_3_0 = QCz * v5_0_0 + WQz * v5_0_1;
+            const VT v5_3_1 = QCz * v5_0_1 + WQz * v5_0_2;
+            const VT v6_3_0 = QCz * v6_0_0 + WQz * v6_0_1 + (VT)1.0 * oo2ze * v1_0_1;
+            const VT v6_3_1 = QCz * v6_0_1 + WQz * v6_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v7_3_0 = QCz * v7_0_0 + WQz * v7_0_1;
+            const VT v7_3_1 = QCz * v7_0_1 + WQz * v7_0_2;
+            const VT v8_3_0 = QCz * v8_0_0 + WQz * v8_0_1 + (VT)1.0 * oo2ze * v2_0_1;
+            const VT v8_3_1 = QCz * v8_0_1 + WQz * v8_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v9_3_0 = QCz * v9_0_0 + WQz * v9_0_1 + (VT)2.0 * oo2ze * v3_0_1;
+            const VT v9_3_1 = QCz * v9_0_1 + WQz * v9_0_2 + (VT)2.0 * oo2ze * v3_0_2;
+            const VT v10_3_0 = QCz * v10_0_0 + WQz * v10_0_1;
+            const VT v10_3_1 = QCz * v10_0_1 + WQz * v10_0_2;
+            const VT v11_3_0 = QCz * v11_0_0 + WQz * v11_0_1;
+            const VT v11_3_1 = QCz * v11_0_1 + WQz * v11_0_2;
+            const VT v12_3_0 = QCz * v12_0_0 + WQz * v12_0_1 + (VT)1.0 * oo2ze * v4_0_1;
+            const VT v12_3_1 = QCz * v12_0_1 + WQz * v12_0_2 + (VT)1.0 * oo2ze * v4_0_2;
+            const VT v13_3_0 = QCz * v13_0_0 + WQz * v13_0_1;
+            const VT v13_3_1 = QCz * v13_0_1 + WQz * v13_0_2;
+            const VT v14_3_0 = QCz * v14_0_0 + WQz * v14_0_1 + (VT)2.0 * oo2ze * v6_0_1;
+            const VT v14_3_1 = QCz * v14_0_1 + WQz * v14_0_2 + (VT)2.0 * oo2ze * v6_0_2;
+            const VT v15_3_0 = QCz * v15_0_0 + WQz * v15_0_1 + (VT)1.0 * oo2ze * v5_0_1;
+            const VT v15_3_1 = QCz * v15_0_1 + WQz * v15_0_2 + (VT)1.0 * oo2ze * v5_0_2;
+            const VT v16_3_0 = QCz * v16_0_0 + WQz * v16_0_1;
+            const VT v16_3_1 = QCz * v16_0_1 + WQz * v16_0_2;
+            const VT v17_3_0 = QCz * v17_0_0 + WQz * v17_0_1 + (VT)1.0 * oo2ze * v7_0_1;
+            const VT v17_3_1 = QCz * v17_0_1 + WQz * v17_0_2 + (VT)1.0 * oo2ze * v7_0_2;
+            const VT v18_3_0 = QCz * v18_0_0 + WQz * v18_0_1 + (VT)2.0 * oo2ze * v8_0_1;
+            const VT v18_3_1 = QCz * v18_0_1 + WQz * v18_0_2 + (VT)2.0 * oo2ze * v8_0_2;
+            const VT v19_3_0 = QCz * v19_0_0 + WQz * v19_0_1 + (VT)3.0 * oo2ze * v9_0_1;
+            const VT v19_3_1 = QCz * v19_0_1 + WQz * v19_0_2 + (VT)3.0 * oo2ze * v9_0_2;
+            const VT v4_4_0 = QCx * v4_1_0 + WQx * v4_1_1 + (VT)2.0 * oo2ze * v1_1_1 + (VT)1.0 * oo2e * (v4_0_0 - rho_e * v4_0_1);
+            const VT v5_4_0 = QCx * v5_1_0 + WQx * v5_1_1 + (VT)1.0 * oo2ze * v2_1_1 + (VT)1.0 * oo2e * (v5_0_0 - rho_e * v5_0_1);
+            const VT v6_4_0 = QCx * v6_1_0 + WQx * v6_1_1 + (VT)1.0 * oo2ze * v3_1_1 + (VT)1.0 * oo2e * (v6_0_0 - rho_e * v6_0_1);
+            const VT v7_4_0 = QCx * v7_1_0 + WQx * v7_1_1 + (VT)1.0 * oo2e * (v7_0_0 - rho_e * v7_0_1);
+            const VT v8_4_0 = QCx * v8_1_0 + WQx * v8_1_1 + (VT)1.0 * oo2e * (v8_0_0 - rho_e * v8_0_1);
+            const VT v9_4_0 = QCx * v9_1_0 + WQx * v9_1_1 + (VT)1.0 * oo2e * (v9_0_0 - rho_e * v9_0_1);
+            const VT v10_4_0 = QCx * v10_1_0 + WQx * v10_1_1 + (VT)3.0 * oo2ze * v4_1_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v11_4_0 = QCx * v11_1_0 + WQx * v11_1_1 + (VT)2.0 * oo2ze * v5_1_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v12_4_0 = QCx * v12_1_0 + WQx * v12_1_1 + (VT)2.0 * oo2ze * v6_1_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v13_4_0 = QCx * v13_1_0 + WQx * v13_1_1 + (VT)1.0 * oo2ze * v7_1_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v14_4_0 = QCx * v14_1_0 + WQx * v14_1_1 + (VT)1.0 * oo2ze * v9_1_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v15_4_0 = QCx * v15_1_0 + WQx * v15_1_1 + (VT)1.0 * oo2ze * v8_1_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v16_4_0 = QCx * v16_1_0 + WQx * v16_1_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v17_4_0 = QCx * v17_1_0 + WQx * v17_1_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v18_4_0 = QCx * v18_1_0 + WQx * v18_1_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v19_4_0 = QCx * v19_1_0 + WQx * v19_1_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v4_5_0 = QCx * v4_2_0 + WQx * v4_2_1 + (VT)2.0 * oo2ze * v1_2_1;
+            const VT v5_5_0 = QCx * v5_2_0 + WQx * v5_2_1 + (VT)1.0 * oo2ze * v2_2_1;
+            const VT v6_5_0 = QCx * v6_2_0 + WQx * v6_2_1 + (VT)1.0 * oo2ze * v3_2_1;
+            const VT v7_5_0 = QCx * v7_2_0 + WQx * v7_2_1;
+            const VT v8_5_0 = QCx * v8_2_0 + WQx * v8_2_1;
+            const VT v9_5_0 = QCx * v9_2_0 + WQx * v9_2_1;
+            const VT v10_5_0 = QCx * v10_2_0 + WQx * v10_2_1 + (VT)3.0 * oo2ze * v4_2_1;
+            const VT v11_5_0 = QCx * v11_2_0 + WQx * v11_2_1 + (VT)2.0 * oo2ze * v5_2_1;
+            const VT v12_5_0 = QCx * v12_2_0 + WQx * v12_2_1 + (VT)2.0 * oo2ze * v6_2_1;
+            const VT v13_5_0 = QCx * v13_2_0 + WQx * v13_2_1 + (VT)1.0 * oo2ze * v7_2_1;
+            const VT v14_5_0 = QCx * v14_2_0 + WQx * v14_2_1 + (VT)1.0 * oo2ze * v9_2_1;
+            const VT v15_5_0 = QCx * v15_2_0 + WQx * v15_2_1 + (VT)1.0 * oo2ze * v8_2_1;
+            const VT v16_5_0 = QCx * v16_2_0 + WQx * v16_2_1;
+            const VT v17_5_0 = QCx * v17_2_0 + WQx * v17_2_1;
+            const VT v18_5_0 = QCx * v18_2_0 + WQx * v18_2_1;
+            const VT v19_5_0 = QCx * v19_2_0 + WQx * v19_2_1;
+            const VT v4_6_0 = QCx * v4_3_0 + WQx * v4_3_1 + (VT)2.0 * oo2ze * v1_3_1;
+            const VT v5_6_0 = QCx * v5_3_0 + WQx * v5_3_1 + (VT)1.0 * oo2ze * v2_3_1;
+            const VT v6_6_0 = QCx * v6_3_0 + WQx * v6_3_1 + (VT)1.0 * oo2ze * v3_3_1;
+            const VT v7_6_0 = QCx * v7_3_0 + WQx * v7_3_1;
+            const VT v8_6_0 = QCx * v8_3_0 + WQx * v8_3_1;
+            const VT v9_6_0 = QCx * v9_3_0 + WQx * v9_3_1;
+            const VT v10_6_0 = QCx * v10_3_0 + WQx * v10_3_1 + (VT)3.0 * oo2ze * v4_3_1;
+            const VT v11_6_0 = QCx * v11_3_0 + WQx * v11_3_1 + (VT)2.0 * oo2ze * v5_3_1;
+            const VT v12_6_0 = QCx * v12_3_0 + WQx * v12_3_1 + (VT)2.0 * oo2ze * v6_3_1;
+            const VT v13_6_0 = QCx * v13_3_0 + WQx * v13_3_1 + (VT)1.0 * oo2ze * v7_3_1;
+            const VT v14_6_0 = QCx * v14_3_0 + WQx * v14_3_1 + (VT)1.0 * oo2ze * v9_3_1;
+            const VT v15_6_0 = QCx * v15_3_0 + WQx * v15_3_1 + (VT)1.0 * oo2ze * v8_3_1;
+            const VT v16_6_0 = QCx * v16_3_0 + WQx * v16_3_1;
+            const VT v17_6_0 = QCx * v17_3_0 + WQx * v17_3_1;
+            const VT v18_6_0 = QCx * v18_3_0 + WQx * v18_3_1;
+            const VT v19_6_0 = QCx * v19_3_0 + WQx * v19_3_1;
+            const VT v4_7_0 = QCy * v4_2_0 + WQy * v4_2_1 + (VT)1.0 * oo2e * (v4_0_0 - rho_e * v4_0_1);
+            const VT v5_7_0 = QCy * v5_2_0 + WQy * v5_2_1 + (VT)1.0 * oo2ze * v1_2_1 + (VT)1.0 * oo2e * (v5_0_0 - rho_e * v5_0_1);
+            const VT v6_7_0 = QCy * v6_2_0 + WQy * v6_2_1 + (VT)1.0 * oo2e * (v6_0_0 - rho_e * v6_0_1);
+            const VT v7_7_0 = QCy * v7_2_0 + WQy * v7_2_1 + (VT)2.0 * oo2ze * v2_2_1 + (VT)1.0 * oo2e * (v7_0_0 - rho_e * v7_0_1);
+            const VT v8_7_0 = QCy * v8_2_0 + WQy * v8_2_1 + (VT)1.0 * oo2ze * v3_2_1 + (VT)1.0 * oo2e * (v8_0_0 - rho_e * v8_0_1);
+            const VT v9_7_0 = QCy * v9_2_0 + WQy * v9_2_1 + (VT)1.0 * oo2e * (v9_0_0 - rho_e * v9_0_1);
+            const VT v10_7_0 = QCy * v10_2_0 + WQy * v10_2_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v11_7_0 = QCy * v11_2_0 + WQy * v11_2_1 + (VT)1.0 * oo2ze * v4_2_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v12_7_0 = QCy * v12_2_0 + WQy * v12_2_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v13_7_0 = QCy * v13_2_0 + WQy * v13_2_1 + (VT)2.0 * oo2ze * v5_2_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v14_7_0 = QCy * v14_2_0 + WQy * v14_2_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v15_7_0 = QCy * v15_2_0 + WQy * v15_2_1 + (VT)1.0 * oo2ze * v6_2_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v16_7_0 = QCy * v16_2_0 + WQy * v16_2_1 + (VT)3.0 * oo2ze * v7_2_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v17_7_0 = QCy * v17_2_0 + WQy * v17_2_1 + (VT)2.0 * oo2ze * v8_2_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v18_7_0 = QCy * v18_2_0 + WQy * v18_2_1 + (VT)1.0 * oo2ze * v9_2_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v19_7_0 = QCy * v19_2_0 + WQy * v19_2_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v4_8_0 = QCy * v4_3_0 + WQy * v4_3_1;
+            const VT v5_8_0 = QCy * v5_3_0 + WQy * v5_3_1 + (VT)1.0 * oo2ze * v1_3_1;
+            const VT v6_8_0 = QCy * v6_3_0 + WQy * v6_3_1;
+            const VT v7_8_0 = QCy * v7_3_0 + WQy * v7_3_1 + (VT)2.0 * oo2ze * v2_3_1;
+            const VT v8_8_0 = QCy * v8_3_0 + WQy * v8_3_1 + (VT)1.0 * oo2ze * v3_3_1;
+            const VT v9_8_0 = QCy * v9_3_0 + WQy * v9_3_1;
+            const VT v10_8_0 = QCy * v10_3_0 + WQy * v10_3_1;
+            const VT v11_8_0 = QCy * v11_3_0 + WQy * v11_3_1 + (VT)1.0 * oo2ze * v4_3_1;
+            const VT v12_8_0 = QCy * v12_3_0 + WQy * v12_3_1;
+            const VT v13_8_0 = QCy * v13_3_0 + WQy * v13_3_1 + (VT)2.0 * oo2ze * v5_3_1;
+            const VT v14_8_0 = QCy * v14_3_0 + WQy * v14_3_1;
+            const VT v15_8_0 = QCy * v15_3_0 + WQy * v15_3_1 + (VT)1.0 * oo2ze * v6_3_1;
+            const VT v16_8_0 = QCy * v16_3_0 + WQy * v16_3_1 + (VT)3.0 * oo2ze * v7_3_1;
+            const VT v17_8_0 = QCy * v17_3_0 + WQy * v17_3_1 + (VT)2.0 * oo2ze * v8_3_1;
+            const VT v18_8_0 = QCy * v18_3_0 + WQy * v18_3_1 + (VT)1.0 * oo2ze * v9_3_1;
+            const VT v19_8_0 = QCy * v19_3_0 + WQy * v19_3_1;
+            const VT v4_9_0 = QCz * v4_3_0 + WQz * v4_3_1 + (VT)1.0 * oo2e * (v4_0_0 - rho_e * v4_0_1);
+            const VT v5_9_0 = QCz * v5_3_0 + WQz * v5_3_1 + (VT)1.0 * oo2e * (v5_0_0 - rho_e * v5_0_1);
+            const VT v6_9_0 = QCz * v6_3_0 + WQz * v6_3_1 + (VT)1.0 * oo2ze * v1_3_1 + (VT)1.0 * oo2e * (v6_0_0 - rho_e * v6_0_1);
+            const VT v7_9_0 = QCz * v7_3_0 + WQz * v7_3_1 + (VT)1.0 * oo2e * (v7_0_0 - rho_e * v7_0_1);
+            const VT v8_9_0 = QCz * v8_3_0 + WQz * v8_3_1 + (VT)1.0 * oo2ze * v2_3_1 + (VT)1.0 * oo2e * (v8_0_0 - rho_e * v8_0_1);
+            const VT v9_9_0 = QCz * v9_3_0 + WQz * v9_3_1 + (VT)2.0 * oo2ze * v3_3_1 + (VT)1.0 * oo2e * (v9_0_0 - rho_e * v9_0_1);
+            const VT v10_9_0 = QCz * v10_3_0 + WQz * v10_3_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v11_9_0 = QCz * v11_3_0 + WQz * v11_3_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v12_9_0 = QCz * v12_3_0 + WQz * v12_3_1 + (VT)1.0 * oo2ze * v4_3_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v13_9_0 = QCz * v13_3_0 + WQz * v13_3_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v14_9_0 = QCz * v14_3_0 + WQz * v14_3_1 + (VT)2.0 * oo2ze * v6_3_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v15_9_0 = QCz * v15_3_0 + WQz * v15_3_1 + (VT)1.0 * oo2ze * v5_3_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v16_9_0 = QCz * v16_3_0 + WQz * v16_3_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v17_9_0 = QCz * v17_3_0 + WQz * v17_3_1 + (VT)1.0 * oo2ze * v7_3_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v18_9_0 = QCz * v18_3_0 + WQz * v18_3_1 + (VT)2.0 * oo2ze * v8_3_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v19_9_0 = QCz * v19_3_0 + WQz * v19_3_1 + (VT)3.0 * oo2ze * v9_3_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            acc[0] += (double)v4_1_0;
+            acc[1] += (double)v4_2_0;
+            acc[2] += (double)v4_3_0;
+            acc[3] += (double)v4_4_0;
+            acc[4] += (double)v4_5_0;
+            acc[5] += (double)v4_6_0;
+            acc[6] += (double)v4_7_0;
+            acc[7] += (double)v4_8_0;
+            acc[8] += (double)v4_9_0;
+            acc[9] += (double)v5_1_0;
+            acc[10] += (double)v5_2_0;
+            acc[11] += (double)v5_3_0;
+            acc[12] += (double)v5_4_0;
+            acc[13] += (double)v5_5_0;
+            acc[14] += (double)v5_6_0;
+            acc[15] += (double)v5_7_0;
+            acc[16] += (double)v5_8_0;
+            acc[17] += (double)v5_9_0;
+            acc[18] += (double)v6_1_0;
+            acc[19] += (double)v6_2_0;
+            acc[20] += (double)v6_3_0;
+            acc[21] += (double)v6_4_0;
+            acc[22] += (double)v6_5_0;
+            acc[23] += (double)v6_6_0;
+            acc[24] += (double)v6_7_0;
+            acc[25] += (double)v6_8_0;
+            acc[26] += (double)v6_9_0;
+            acc[27] += (double)v7_1_0;
+            acc[28] += (double)v7_2_0;
+            acc[29] += (double)v7_3_0;
+            acc[30] += (double)v7_4_0;
+            acc[31] += (double)v7_5_0;
+            acc[32] += (double)v7_6_0;
+            acc[33] += (double)v7_7_0;
+            acc[34] += (double)v7_8_0;
+            acc[35] += (double)v7_9_0;
+            acc[36] += (double)v8_1_0;
+            acc[37] += (double)v8_2_0;
+            acc[38] += (double)v8_3_0;
+            acc[39] += (double)v8_4_0;
+            acc[40] += (double)v8_5_0;
+            acc[41] += (double)v8_6_0;
+            acc[42] += (double)v8_7_0;
+            acc[43] += (double)v8_8_0;
+            acc[44] += (double)v8_9_0;
+            acc[45] += (double)v9_1_0;
+            acc[46] += (double)v9_2_0;
+            acc[47] += (double)v9_3_0;
+            acc[48] += (double)v9_4_0;
+            acc[49] += (double)v9_5_0;
+            acc[50] += (double)v9_6_0;
+            acc[51] += (double)v9_7_0;
+            acc[52] += (double)v9_8_0;
+            acc[53] += (double)v9_9_0;
+            acc[54] += (double)v10_1_0;
+            acc[55] += (double)v10_2_0;
+            acc[56] += (double)v10_3_0;
+            acc[57] += (double)v10_4_0;
+            acc[58] += (double)v10_5_0;
+            acc[59] += (double)v10_6_0;
+            acc[60] += (double)v10_7_0;
+            acc[61] += (double)v10_8_0;
+            acc[62] += (double)v10_9_0;
+            acc[63] += (double)v11_1_0;
+            acc[64] += (double)v11_2_0;
+            acc[65] += (double)v11_3_0;
+            acc[66] += (double)v11_4_0;
+            acc[67] += (double)v11_5_0;
+            acc[68] += (double)v11_6_0;
+            acc[69] += (double)v11_7_0;
+            acc[70] += (double)v11_8_0;
+            acc[71] += (double)v11_9_0;
+            acc[72] += (double)v12_1_0;
+            acc[73] += (double)v12_2_0;
+            acc[74] += (double)v12_3_0;
+            acc[75] += (double)v12_4_0;
+            acc[76] += (double)v12_5_0;
+            acc[77] += (double)v12_6_0;
+            acc[78] += (double)v12_7_0;
+            acc[79] += (double)v12_8_0;
+            acc[80] += (double)v12_9_0;
+            acc[81] += (double)v13_1_0;
+            acc[82] += (double)v13_2_0;
+            acc[83] += (double)v13_3_0;
+            acc[84] += (double)v13_4_0;
+            acc[85] += (double)v13_5_0;
+            acc[86] += (double)v13_6_0;
+            acc[87] += (double)v13_7_0;
+            acc[88] += (double)v13_8_0;
+            acc[89] += (double)v13_9_0;
+            acc[90] += (double)v14_1_0;
+            acc[91] += (double)v14_2_0;
+            acc[92] += (double)v14_3_0;
+            acc[93] += (double)v14_4_0;
+            acc[94] += (double)v14_5_0;
+            acc[95] += (double)v14_6_0;
+            acc[96] += (double)v14_7_0;
+            acc[97] += (double)v14_8_0;
+            acc[98] += (double)v14_9_0;
+            acc[99] += (double)v15_1_0;
+            acc[100] += (double)v15_2_0;
+            acc[101] += (double)v15_3_0;
+            acc[102] += (double)v15_4_0;
+            acc[103] += (double)v15_5_0;
+            acc[104] += (double)v15_6_0;
+            acc[105] += (double)v15_7_0;
+            acc[106] += (double)v15_8_0;
+            acc[107] += (double)v15_9_0;
+            acc[108] += (double)v16_1_0;
+            acc[109] += (double)v16_2_0;
+            acc[110] += (double)v16_3_0;
+            acc[111] += (double)v16_4_0;
+            acc[112] += (double)v16_5_0;
+            acc[113] += (double)v16_6_0;
+            acc[114] += (double)v16_7_0;
+            acc[115] += (double)v16_8_0;
+            acc[116] += (double)v16_9_0;
+            acc[117] += (double)v17_1_0;
+            acc[118] += (double)v17_2_0;
+            acc[119] += (double)v17_3_0;
+            acc[120] += (double)v17_4_0;
+            acc[121] += (double)v17_5_0;
+            acc[122] += (double)v17_6_0;
+            acc[123] += (double)v17_7_0;
+            acc[124] += (double)v17_8_0;
+            acc[125] += (double)v17_9_0;
+            acc[126] += (double)v18_1_0;
+            acc[127] += (double)v18_2_0;
+            acc[128] += (double)v18_3_0;
+            acc[129] += (double)v18_4_0;
+            acc[130] += (double)v18_5_0;
+            acc[131] += (double)v18_6_0;
+            acc[132] += (double)v18_7_0;
+            acc[133] += (double)v18_8_0;
+            acc[134] += (double)v18_9_0;
+            acc[135] += (double)v19_1_0;
+            acc[136] += (double)v19_2_0;
+            acc[137] += (double)v19_3_0;
+            acc[138] += (double)v19_4_0;
+            acc[139] += (double)v19_5_0;
+            acc[140] += (double)v19_6_0;
+            acc[141] += (double)v19_7_0;
+            acc[142] += (double)v19_8_0;
+            acc[143] += (double)v19_9_0;
+        }
+    }
+    const double4 gb = ldg4(&P.geo[p]);
+    const double4 gk = ldg4(&P.geo[q]);
+    const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
+    const double CDx = gk.x, CDy = gk.y, CDz = gk.z;
+    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
+    const double h4_1_4 = acc[57] + ABx * acc[3];
+    const double h4_1_1 = acc[54] + ABx * acc[0];
+    const double k4_1_1_1 = h4_1_4 + CDx * h4_1_1;
+    const double h4_1_5 = acc[58] + ABx * acc[4];
+    const double k4_1_1_2 = h4_1_5 + CDy * h4_1_1;
+    const double h4_1_6 = acc[59] + ABx * acc[5];
+    const double k4_1_1_3 = h4_1_6 + CDz * h4_1_1;
+    const double h4_1_2 = acc[55] + ABx * acc[1];
+    const double k4_1_2_1 = h4_1_5 + CDx * h4_1_2;
+    const double h4_1_7 = acc[60] + ABx * acc[6];
+    const double k4_1_2_2 = h4_1_7 + CDy * h4_1_2;
+    const double h4_1_8 = acc[61] + ABx * acc[7];
+    const double k4_1_2_3 = h4_1_8 + CDz * h4_1_2;
+    const double h4_1_3 = acc[56] + ABx * acc[2];
+    const double k4_1_3_1 = h4_1_6 + CDx * h4_1_3;
+    const double k4_1_3_2 = h4_1_8 + CDy * h4_1_3;
+    const double h4_1_9 = acc[62] + ABx * acc[8];
+    const double k4_1_3_3 = h4_1_9 + CDz * h4_1_3;
+    const double h4_2_4 = acc[66] + ABy * acc[3];
+    const double h4_2_1 = acc[63] + ABy * acc[0];
+    const double k4_2_1_1 = h4_2_4 + CDx * h4_2_1;
+    const double h4_2_5 = acc[67] + ABy * acc[4];
+    const double k4_2_1_2 = h4_2_5 + CDy * h4_2_1;
+    const double h4_2_6 = acc[68] + ABy * acc[5];
+    const double k4_2_1_3 = h4_2_6 + CDz * h4_2_1;
+    const double h4_2_2 = acc[64] + ABy * acc[1];
+    const double k4_2_2_1 = h4_2_5 + CDx * h4_2_2;
+    const double h4_2_7 = acc[69] + ABy * acc[6];
+    const double k4_2_2_2 = h4_2_7 + CDy * h4_2_2;
+    const double h4_2_8 = acc[70] + ABy * acc[7];
+    const double k4_2_2_3 = h4_2_8 + CDz * h4_2_2;
+    const double h4_2_3 = acc[65] + ABy * acc[2];
+    const double k4_2_3_1 = h4_2_6 + CDx * h4_2_3;
+    const double k4_2_3_2 = h4_2_8 + CDy * h4_2_3;
+    const double h4_2_9 = acc[71] + ABy * acc[8];
+    const double k4_2_3_3 = h4_2_9 + CDz * h4_2_3;
+    const double h4_3_4 = acc[75] + ABz * acc[3];
+    const double h4_3_1 = acc[72] + ABz * acc[0];
+    const double k4_3_1_1 = h4_3_4 + CDx * h4_3_1;
+    const double h4_3_5 = acc[76] + ABz * acc[4];
+    const double k4_3_1_2 = h4_3_5 + CDy * h4_3_1;
+    const double h4_3_6 = acc[77] + ABz * acc[5];
+    const double k4_3_1_3 = h4_3_6 + CDz * h4_3_1;
+    const double h4_3_2 = acc[73] + ABz * acc[1];
+    const double k4_3_2_1 = h4_3_5 + CDx * h4_3_2;
+    const double h4_3_7 = acc[78] + ABz * acc[6];
+    const double k4_3_2_2 = h4_3_7 + CDy * h4_3_2;
+    const double h4_3_8 = acc[79] + ABz * acc[7];
+    const double k4_3_2_3 = h4_3_8 + CDz * h4_3_2;
+    const double h4_3_3 = acc[74] + ABz * acc[2];
+    const double k4_3_3_1 = h4_3_6 + CDx * h4_3_3;
+    const double k4_3_3_2 = h4_3_8 + CDy * h4_3_3;
+    const double h4_3_9 = acc[80] + ABz * acc[8];
+    const double k4_3_3_3 = h4_3_9 + CDz * h4_3_3;
+    const double h5_1_4 = acc[66] + ABx * acc[12];
+    const double h5_1_1 = acc[63] + ABx * acc[9];
+    const double k5_1_1_1 = h5_1_4 + CDx * h5_1_1;
+    const double h5_1_5 = acc[67] + ABx * acc[13];
+    const double k5_1_1_2 = h5_1_5 + CDy * h5_1_1;
+    const double h5_1_6 = acc[68] + ABx * acc[14];
+    const double k5_1_1_3 = h5_1_6 + CDz * h5_1_1;
+    const double h5_1_2 = acc[64] + ABx * acc[10];
+    const double k5_1_2_1 = h5_1_5 + CDx * h5_1_2;
+    const double h5_1_7 = acc[69] + ABx * acc[15];
+    const double k5_1_2_2 = h5_1_7 + CDy * h5_1_2;
+    const double h5_1_8 = acc[70] + ABx * acc[16];
+    const double k5_1_2_3 = h5_1_8 + CDz * h5_1_2;
+    const double h5_1_3 = acc[65] + ABx * acc[11];
+    const double k5_1_3_1 = h5_1_6 + CDx * h5_1_3;
+    const double k5_1_3_2 = h5_1_8 + CDy * h5_1_3;
+    const double h5_1_9 = acc[71] + ABx * acc[17];
+    const double k5_1_3_3 = h5_1_9 + CDz * h5_1_3;
+    const double h5_2_4 = acc[84] + ABy * acc[12];
+    const double h5_2_1 = acc[81] + ABy * acc[9];
+    const double k5_2_1_1 = h5_2_4 + CDx * h5_2_1;
+    const double h5_2_5 = acc[85] + ABy * acc[13];
+    const double k5_2_1_2 = h5_2_5 + CDy * h5_2_1;
+    const double h5_2_6 = acc[86] + ABy * acc[14];
+    const double k5_2_1_3 = h5_2_6 + CDz * h5_2_1;
+    const double h5_2_2 = acc[82] + ABy * acc[10];
+    const double k5_2_2_1 = h5_2_5 + CDx * h5_2_2;
+    const double h5_2_7 = acc[87] + ABy * acc[15];
+    const double k5_2_2_2 = h5_2_7 + CDy * h5_2_2;
+    const double h5_2_8 = acc[88] + ABy * acc[16];
+    const double k5_2_2_3 = h5_2_8 + CDz * h5_2_2;
+    const double h5_2_3 = acc[83] + ABy * acc[11];
+    const double k5_2_3_1 = h5_2_6 + CDx * h5_2_3;
+    const double k5_2_3_2 = h5_2_8 + CDy * h5_2_3;
+    const double h5_2_9 = acc[89] + ABy * acc[17];
+    const double k5_2_3_3 = h5_2_9 + CDz * h5_2_3;
+    const double h5_3_4 = acc[102] + ABz * acc[12];
+    const double h5_3_1 = acc[99] + ABz * acc[9];
+    const double k5_3_1_1 = h5_3_4 + CDx * h5_3_1;
+    const double h5_3_5 = acc[103] + ABz * acc[13];
+    const double k5_3_1_2 = h5_3_5 + CDy * h5_3_1;
+    const double h5_3_6 = acc[104] + ABz * acc[14];
+    const double k5_3_1_3 = h5_3_6 + CDz * h5_3_1;
+    const double h5_3_2 = acc[100] + ABz * acc[10];
+    const double k5_3_2_1 = h5_3_5 + CDx * h5_3_2;
+    const double h5_3_7 = acc[105] + ABz * acc[15];
+    const double k5_3_2_2 = h5_3_7 + CDy * h5_3_2;
+    const double h5_3_8 = acc[106] + ABz * acc[16];
+    const double k5_3_2_3 = h5_3_8 + CDz * h5_3_2;
+    const double h5_3_3 = acc[101] + ABz * acc[11];
+    const double k5_3_3_1 = h5_3_6 + CDx * h5_3_3;
+    const double k5_3_3_2 = h5_3_8 + CDy * h5_3_3;
+    const double h5_3_9 = acc[107] + ABz * acc[17];
+    const double k5_3_3_3 = h5_3_9 + CDz * h5_3_3;
+    const double h6_1_4 = acc[75] + ABx * acc[21];
+    const double h6_1_1 = acc[72] + ABx * acc[18];
+    const double k6_1_1_1 = h6_1_4 + CDx * h6_1_1;
+    const double h6_1_5 = acc[76] + ABx * acc[22];
+    const double k6_1_1_2 = h6_1_5 + CDy * h6_1_1;
+    const double h6_1_6 = acc[77] + ABx * acc[23];
+    const double k6_1_1_3 = h6_1_6 + CDz * h6_1_1;
+    const double h6_1_2 = acc[73] + ABx * acc[19];
+    const double k6_1_2_1 = h6_1_5 + CDx * h6_1_2;
+    const double h6_1_7 = acc[78] + ABx * acc[24];
+    const double k6_1_2_2 = h6_1_7 + CDy * h6_1_2;
+    const double h6_1_8 = acc[79] + ABx * acc[25];
+    const double k6_1_2_3 = h6_1_8 + CDz * h6_1_2;
+    const double h6_1_3 = acc[74] + ABx * acc[20];
+    const double k6_1_3_1 = h6_1_6 + CDx * h6_1_3;
+    const double k6_1_3_2 = h6_1_8 + CDy * h6_1_3;
+    const double h6_1_9 = acc[80] + ABx * acc[26];
+    const double k6_1_3_3 = h6_1_9 + CDz * h6_1_3;
+    const double h6_2_4 = acc[102] + ABy * acc[21];
+    const double h6_2_1 = acc[99] + ABy * acc[18];
+    const double k6_2_1_1 = h6_2_4 + CDx * h6_2_1;
+    const double h6_2_5 = acc[103] + ABy * acc[22];
+    const double k6_2_1_2 = h6_2_5 + CDy * h6_2_1;
+    const double h6_2_6 = acc[104] + ABy * acc[23];
+    const double k6_2_1_3 = h6_2_6 + CDz * h6_2_1;
+    const double h6_2_2 = acc[100] + ABy * acc[19];
+    const double k6_2_2_1 = h6_2_5 + CDx * h6_2_2;
+    const double h6_2_7 = acc[105] + ABy * acc[24];
+    const double k6_2_2_2 = h6_2_7 + CDy * h6_2_2;
+    const double h6_2_8 = acc[106] + ABy * acc[25];
+    const double k6_2_2_3 = h6_2_8 + CDz * h6_2_2;
+    const double h6_2_3 = acc[101] + ABy * acc[20];
+    const double k6_2_3_1 = h6_2_6 + CDx * h6_2_3;
+    const double k6_2_3_2 = h6_2_8 + CDy * h6_2_3;
+    const double h6_2_9 = acc[107] + ABy * acc[26];
+    const double k6_2_3_3 = h6_2_9 + CDz * h6_2_3;
+    const double h6_3_4 = acc[93] + ABz * acc[21];
+    const double h6_3_1 = acc[90] + ABz * acc[18];
+    const double k6_3_1_1 = h6_3_4 + CDx * h6_3_1;
+    const double h6_3_5 = acc[94] + ABz * acc[22];
+    const double k6_3_1_2 = h6_3_5 + CDy * h6_3_1;
+    const double h6_3_6 = acc[95] + ABz * acc[23];
+    const double k6_3_1_3 = h6_3_6 + CDz * h6_3_1;
+    const double h6_3_2 = acc[91] + ABz * acc[19];
+    const double k6_3_2_1 = h6_3_5 + CDx * h6_3_2;
+    const double h6_3_7 = acc[96] + ABz * acc[24];
+    const double k6_3_2_2 = h6_3_7 + CDy * h6_3_2;
+    const double h6_3_8 = acc[97] + ABz * acc[25];
+    const double k6_3_2_3 = h6_3_8 + CDz * h6_3_2;
+    const double h6_3_3 = acc[92] + ABz * acc[20];
+    const double k6_3_3_1 = h6_3_6 + CDx * h6_3_3;
+    const double k6_3_3_2 = h6_3_8 + CDy * h6_3_3;
+    const double h6_3_9 = acc[98] + ABz * acc[26];
+    const double k6_3_3_3 = h6_3_9 + CDz * h6_3_3;
+    const double h7_1_4 = acc[84] + ABx * acc[30];
+    const double h7_1_1 = acc[81] + ABx * acc[27];
+    const double k7_1_1_1 = h7_1_4 + CDx * h7_1_1;
+    const double h7_1_5 = acc[85] + ABx * acc[31];
+    const double k7_1_1_2 = h7_1_5 + CDy * h7_1_1;
+    const double h7_1_6 = acc[86] + ABx * acc[32];
+    const double k7_1_1_3 = h7_1_6 + CDz * h7_1_1;
+    const double h7_1_2 = acc[82] + ABx * acc[28];
+    const double k7_1_2_1 = h7_1_5 + CDx * h7_1_2;
+    const double h7_1_7 = acc[87] + ABx * acc[33];
+    const double k7_1_2_2 = h7_1_7 + CDy * h7_1_2;
+    const double h7_1_8 = acc[88] + ABx * acc[34];
+    const double k7_1_2_3 = h7_1_8 + CDz * h7_1_2;
+    const double h7_1_3 = acc[83] + ABx * acc[29];
+    const double k7_1_3_1 = h7_1_6 + CDx * h7_1_3;
+    const double k7_1_3_2 = h7_1_8 + CDy * h7_1_3;
+    const double h7_1_9 = acc[89] + ABx * acc[35];
+    const double k7_1_3_3 = h7_1_9 + CDz * h7_1_3;
+    const double h7_2_4 = acc[111] + ABy * acc[30];
+    const double h7_2_1 = acc[108] + ABy * acc[27];
+    const double k7_2_1_1 = h7_2_4 + CDx * h7_2_1;
+    const double h7_2_5 = acc[112] + ABy * acc[31];
+    const double k7_2_1_2 = h7_2_5 + CDy * h7_2_1;
+    const double h7_2_6 = acc[113] + ABy * acc[32];
+    const double k7_2_1_3 = h7_2_6 + CDz * h7_2_1;
+    const double h7_2_2 = acc[109] + ABy * acc[28];
+    const double k7_2_2_1 = h7_2_5 + CDx * h7_2_2;
+    const double h7_2_7 = acc[114] + ABy * acc[33];
+    const double k7_2_2_2 = h7_2_7 + CDy * h7_2_2;
+    const double h7_2_8 = acc[115] + ABy * acc[34];
+    const double k7_2_2_3 = h7_2_8 + CDz * h7_2_2;
+    const double h7_2_3 = acc[110] + ABy * acc[29];
+    const double k7_2_3_1 = h7_2_6 + CDx * h7_2_3;
+    const double k7_2_3_2 = h7_2_8 + CDy * h7_2_3;
+    const double h7_2_9 = acc[116] + ABy * acc[35];
+    const double k7_2_3_3 = h7_2_9 + CDz * h7_2_3;
+    const double h7_3_4 = acc[120] + ABz * acc[30];
+    const double h7_3_1 = acc[117] + ABz * acc[27];
+    const double k7_3_1_1 = h7_3_4 + CDx * h7_3_1;
+    const double h7_3_5 = acc[121] + ABz * acc[31];
+    const double k7_3_1_2 = h7_3_5 + CDy * h7_3_1;
+    const double h7_3_6 = acc[122] + ABz * acc[32];
+    const double k7_3_1_3 = h7_3_6 + CDz * h7_3_1;
+    const double h7_3_2 = acc[118] + ABz * acc[28];
+    const double k7_3_2_1 = h7_3_5 + CDx * h7_3_2;
+    const double h7_3_7 = acc[123] + ABz * acc[33];
+    const double k7_3_2_2 = h7_3_7 + CDy * h7_3_2;
+    const double h7_3_8 = acc[124] + ABz * acc[34];
+    const double k7_3_2_3 = h7_3_8 + CDz * h7_3_2;
+    const double h7_3_3 = acc[119] + ABz * acc[29];
+    const double k7_3_3_1 = h7_3_6 + CDx * h7_3_3;
+    const double k7_3_3_2 = h7_3_8 + CDy * h7_3_3;
+    const double h7_3_9 = acc[125] + ABz * acc[35];
+    const double k7_3_3_3 = h7_3_9 + CDz * h7_3_3;
+    const double h8_1_4 = acc[102] + ABx * acc[39];
+    const double h8_1_1 = acc[99] + ABx * acc[36];
+    const double k8_1_1_1 = h8_1_4 + CDx * h8_1_1;
+    const double h8_1_5 = acc[103] + ABx * acc[40];
+    const double k8_1_1_2 = h8_1_5 + CDy * h8_1_1;
+    const double h8_1_6 = acc[104] + ABx * acc[41];
+    const double k8_1_1_3 = h8_1_6 + CDz * h8_1_1;
+    const double h8_1_2 = acc[100] + ABx * acc[37];
+    const double k8_1_2_1 = h8_1_5 + CDx * h8_1_2;
+    const double h8_1_7 = acc[105] + ABx * acc[42];
+    const double k8_1_2_2 = h8_1_7 + CDy * h8_1_2;
+    const double h8_1_8 = acc[106] + ABx * acc[43];
+    const double k8_1_2_3 = h8_1_8 + CDz * h8_1_2;
+    const double h8_1_3 = acc[101] + ABx * acc[38];
+    const double k8_1_3_1 = h8_1_6 + CDx * h8_1_3;
+    const double k8_1_3_2 = h8_1_8 + CDy * h8_1_3;
+    const double h8_1_9 = acc[107] + ABx * acc[44];
+    const double k8_1_3_3 = h8_1_9 + CDz * h8_1_3;
+    const double h8_2_4 = acc[120] + ABy * acc[39];
+    const double h8_2_1 = acc[117] + ABy * acc[36];
+    const double k8_2_1_1 = h8_2_4 + CDx * h8_2_1;
+    const double h8_2_5 = acc[121] + ABy * acc[40];
+    const double k8_2_1_2 = h8_2_5 + CDy * h8_2_1;
+    const double h8_2_6 = acc[122] + ABy * acc[41];
+    const double k8_2_1_3 = h8_2_6 + CDz * h8_2_1;
+    const double h8_2_2 = acc[118] + ABy * acc[37];
+    const double k8_2_2_1 = h8_2_5 + CDx * h8_2_2;
+    const double h8_2_7 = acc[123] + ABy * acc[42];
+    const double k8_2_2_2 = h8_2_7 + CDy * h8_2_2;
+    const double h8_2_8 = acc[124] + ABy * acc[43];
+    const double k8_2_2_3 = h8_2_8 + CDz * h8_2_2;
+    const double h8_2_3 = acc[119] + ABy * acc[38];
+    const double k8_2_3_1 = h8_2_6 + CDx * h8_2_3;
+    const double k8_2_3_2 = h8_2_8 + CDy * h8_2_3;
+    const double h8_2_9 = acc[125] + ABy * acc[44];
+    const double k8_2_3_3 = h8_2_9 + CDz * h8_2_3;
+    const double h8_3_4 = acc[129] + ABz * acc[39];
+    const double h8_3_1 = acc[126] + ABz * acc[36];
+    const double k8_3_1_1 = h8_3_4 + CDx * h8_3_1;
+    const double h8_3_5 = acc[130] + ABz * acc[40];
+    const double k8_3_1_2 = h8_3_5 + CDy * h8_3_1;
+    const double h8_3_6 = acc[131] + ABz * acc[41];
+    const double k8_3_1_3 = h8_3_6 + CDz * h8_3_1;
+    const double h8_3_2 = acc[127] + ABz * acc[37];
+    const double k8_3_2_1 = h8_3_5 + CDx * h8_3_2;
+    const double h8_3_7 = acc[132] + ABz * acc[42];
+    const double k8_3_2_2 = h8_3_7 + CDy * h8_3_2;
+    const double h8_3_8 = acc[133] + ABz * acc[43];
+    const double k8_3_2_3 = h8_3_8 + CDz * h8_3_2;
+    const double h8_3_3 = acc[128] + ABz * acc[38];
+    const double k8_3_3_1 = h8_3_6 + CDx * h8_3_3;
+    const double k8_3_3_2 = h8_3_8 + CDy * h8_3_3;
+    const double h8_3_9 = acc[134] + ABz * acc[44];
+    const double k8_3_3_3 = h8_3_9 + CDz * h8_3_3;
+    const double h9_1_4 = acc[93] + ABx * acc[48];
+    const double h9_1_1 = acc[90] + ABx * acc[45];
+    const double k9_1_1_1 = h9_1_4 + CDx * h9_1_1;
+    const double h9_1_5 = acc[94] + ABx * acc[49];
+    const double k9_1_1_2 = h9_1_5 + CDy * h9_1_1;
+    const double h9_1_6 = acc[95] + ABx * acc[50];
+    const double k9_1_1_3 = h9_1_6 + CDz * h9_1_1;
+    const double h9_1_2 = acc[91] + ABx * acc[46];
+    const double k9_1_2_1 = h9_1_5 + CDx * h9_1_2;
+    const double h9_1_7 = acc[96] + ABx * acc[51];
+    const double k9_1_2_2 = h9_1_7 + CDy * h9_1_2;
+    const double h9_1_8 = acc[97] + ABx * acc[52];
+    const double k9_1_2_3 = h9_1_8 + CDz * h9_1_2;
+    const double h9_1_3 = acc[92] + ABx * acc[47];
+    const double k9_1_3_1 = h9_1_6 + CDx * h9_1_3;
+    const double k9_1_3_2 = h9_1_8 + CDy * h9_1_3;
+    const double h9_1_9 = acc[98] + ABx * acc[53];
+    const double k9_1_3_3 = h9_1_9 + CDz * h9_1_3;
+    const double h9_2_4 = acc[129] + ABy * acc[48];
+    const double h9_2_1 = acc[126] + ABy * acc[45];
+    const double k9_2_1_1 = h9_2_4 + CDx * h9_2_1;
+    const double h9_2_5 = acc[130] + ABy * acc[49];
+    const double k9_2_1_2 = h9_2_5 + CDy * h9_2_1;
+    const double h9_2_6 = acc[131] + ABy * acc[50];
+    const double k9_2_1_3 = h9_2_6 + CDz * h9_2_1;
+    const double h9_2_2 = acc[127] + ABy * acc[46];
+    const double k9_2_2_1 = h9_2_5 + CDx * h9_2_2;
+    const double h9_2_7 = acc[132] + ABy * acc[51];
+    const double k9_2_2_2 = h9_2_7 + CDy * h9_2_2;
+    const double h9_2_8 = acc[133] + ABy * acc[52];
+    const double k9_2_2_3 = h9_2_8 + CDz * h9_2_2;
+    const double h9_2_3 = acc[128] + ABy * acc[47];
+    const double k9_2_3_1 = h9_2_6 + CDx * h9_2_3;
+    const double k9_2_3_2 = h9_2_8 + CDy * h9_2_3;
+    const double h9_2_9 = acc[134] + ABy * acc[53];
+    const double k9_2_3_3 = h9_2_9 + CDz * h9_2_3;
+    const double h9_3_4 = acc[138] + ABz * acc[48];
+    const double h9_3_1 = acc[135] + ABz * acc[45];
+    const double k9_3_1_1 = h9_3_4 + CDx * h9_3_1;
+    const double h9_3_5 = acc[139] + ABz * acc[49];
+    const double k9_3_1_2 = h9_3_5 + CDy * h9_3_1;
+    const double h9_3_6 = acc[140] + ABz * acc[50];
+    const double k9_3_1_3 = h9_3_6 + CDz * h9_3_1;
+    const double h9_3_2 = acc[136] + ABz * acc[46];
+    const double k9_3_2_1 = h9_3_5 + CDx * h9_3_2;
+    const double h9_3_7 = acc[141] + ABz * acc[51];
+    const double k9_3_2_2 = h9_3_7 + CDy * h9_3_2;
+    const double h9_3_8 = acc[142] + ABz * acc[52];
+    const double k9_3_2_3 = h9_3_8 + CDz * h9_3_2;
+    const double h9_3_3 = acc[137] + ABz * acc[47];
+    const double k9_3_3_1 = h9_3_6 + CDx * h9_3_3;
+    const double k9_3_3_2 = h9_3_8 + CDy * h9_3_3;
+    const double h9_3_9 = acc[143] + ABz * acc[53];
+    const double k9_3_3_3 = h9_3_9 + CDz * h9_3_3;
+    res[0] = k4_1_1_1 * 0.5773502691896258;
+    res[1] = k4_1_1_2 * 0.5773502691896258;
+    res[2] = k4_1_1_3 * 0.5773502691896258;
+    res[3] = k4_1_2_1 * 0.5773502691896258;
+    res[4] = k4_1_2_2 * 0.5773502691896258;
+    res[5] = k4_1_2_3 * 0.5773502691896258;
+    res[6] = k4_1_3_1 * 0.5773502691896258;
+    res[7] = k4_1_3_2 * 0.5773502691896258;
+    res[8] = k4_1_3_3 * 0.5773502691896258;
+    res[9] = k4_2_1_1 * 0.5773502691896258;
+    res[10] = k4_2_1_2 * 0.5773502691896258;
+    res[11] = k4_2_1_3 * 0.5773502691896258;
+    res[12] = k4_2_2_1 * 0.5773502691896258;
+    res[13] = k4_2_2_2 * 0.5773502691896258;
+    res[14] = k4_2_2_3 * 0.5773502691896258;
+    res[15] = k4_2_3_1 * 0.5773502691896258;
+    res[16] = k4_2_3_2 * 0.5773502691896258;
+    res[17] = k4_2_3_3 * 0.5773502691896258;
+    res[18] = k4_3_1_1 * 0.5773502691896258;
+    res[19] = k4_3_1_2 * 0.5773502691896258;
+    res[20] = k4_3_1_3 * 0.5773502691896258;
+    res[21] = k4_3_2_1 * 0.5773502691896258;
+    res[22] = k4_3_2_2 * 0.5773502691896258;
+    res[23] = k4_3_2_3 * 0.5773502691896258;
+    res[24] = k4_3_3_1 * 0.5773502691896258;
+    res[25] = k4_3_3_2 * 0.5773502691896258;
+    res[26] = k4_3_3_3 * 0.5773502691896258;
+    res[27] = k5_1_1_1;
+    res[28] = k5_1_1_2;
+    res[29] = k5_1_1_3;
+    res[30] = k5_1_2_1;
+    res[31] = k5_1_2_2;
+    res[32] = k5_1_2_3;
+    res[33] = k5_1_3_1;
+    res[34] = k5_1_3_2;
+    res[35] = k5_1_3_3;
+    res[36] = k5_2_1_1;
+    res[37] = k5_2_1_2;
+    res[38] = k5_2_1_3;
+    res[39] = k5_2_2_1;
+    res[40] = k5_2_2_2;
+    res[41] = k5_2_2_3;
+    res[42] = k5_2_3_1;
+    res[43] = k5_2_3_2;
+    res[44] = k5_2_3_3;
+    res[45] = k5_3_1_1;
+    res[46] = k5_3_1_2;
+    res[47] = k5_3_1_3;
+    res[48] = k5_3_2_1;
+    res[49] = k5_3_2_2;
+    res[50] = k5_3_2_3;
+    res[51] = k5_3_3_1;
+    res[52] = k5_3_3_2;
+    res[53] = k5_3_3_3;
+    res[54] = k6_1_1_1;
+    res[55] = k6_1_1_2;
+    res[56] = k6_1_1_3;
+    res[57] = k6_1_2_1;
+    res[58] = k6_1_2_2;
+    res[59] = k6_1_2_3;
+    res[60] = k6_1_3_1;
+    res[61] = k6_1_3_2;
+    res[62] = k6_1_3_3;
+    res[63] = k6_2_1_1;
+    res[64] = k6_2_1_2;
+    res[65] = k6_2_1_3;
+    res[66] = k6_2_2_1;
+    res[67] = k6_2_2_2;
+    res[68] = k6_2_2_3;
+    res[69] = k6_2_3_1;
+    res[70] = k6_2_3_2;
+    res[71] = k6_2_3_3;
+    res[72] = k6_3_1_1;
+    res[73] = k6_3_1_2;
+    res[74] = k6_3_1_3;
+    res[75] = k6_3_2_1;
+    res[76] = k6_3_2_2;
+    res[77] = k6_3_2_3;
+    res[78] = k6_3_3_1;
+    res[79] = k6_3_3_2;
+    res[80] = k6_3_3_3;
+    res[81] = k7_1_1_1 * 0.5773502691896258;
+    res[82] = k7_1_1_2 * 0.5773502691896258;
+    res[83] = k7_1_1_3 * 0.5773502691896258;
+    res[84] = k7_1_2_1 * 0.5773502691896258;
+    res[85] = k7_1_2_2 * 0.5773502691896258;
+    res[86] = k7_1_2_3 * 0.5773502691896258;
+    res[87] = k7_1_3_1 * 0.5773502691896258;
+    res[88] = k7_1_3_2 * 0.5773502691896258;
+    res[89] = k7_1_3_3 * 0.5773502691896258;
+    res[90] = k7_2_1_1 * 0.5773502691896258;
+    res[91] = k7_2_1_2 * 0.5773502691896258;
+    res[92] = k7_2_1_3 * 0.5773502691896258;
+    res[93] = k7_2_2_1 * 0.5773502691896258;
+    res[94] = k7_2_2_2 * 0.5773502691896258;
+    res[95] = k7_2_2_3 * 0.5773502691896258;
+    res[96] = k7_2_3_1 * 0.5773502691896258;
+    res[97] = k7_2_3_2 * 0.5773502691896258;
+    res[98] = k7_2_3_3 * 0.5773502691896258;
+    res[99] = k7_3_1_1 * 0.5773502691896258;
+    res[100] = k7_3_1_2 * 0.5773502691896258;
+    res[101] = k7_3_1_3 * 0.5773502691896258;
+    res[102] = k7_3_2_1 * 0.5773502691896258;
+    res[103] = k7_3_2_2 * 0.5773502691896258;
+    res[104] = k7_3_2_3 * 0.5773502691896258;
+    res[105] = k7_3_3_1 * 0.5773502691896258;
+    res[106] = k7_3_3_2 * 0.5773502691896258;
+    res[107] = k7_3_3_3 * 0.5773502691896258;
+    res[108] = k8_1_1_1;
+    res[109] = k8_1_1_2;
+    res[110] = k8_1_1_3;
+    res[111] = k8_1_2_1;
+    res[112] = k8_1_2_2;
+    res[113] = k8_1_2_3;
+    res[114] = k8_1_3_1;
+    res[115] = k8_1_3_2;
+    res[116] = k8_1_3_3;
+    res[117] = k8_2_1_1;
+    res[118] = k8_2_1_2;
+    res[119] = k8_2_1_3;
+    res[120] = k8_2_2_1;
+    res[121] = k8_2_2_2;
+    res[122] = k8_2_2_3;
+    res[123] = k8_2_3_1;
+    res[124] = k8_2_3_2;
+    res[125] = k8_2_3_3;
+    res[126] = k8_3_1_1;
+    res[127] = k8_3_1_2;
+    res[128] = k8_3_1_3;
+    res[129] = k8_3_2_1;
+    res[130] = k8_3_2_2;
+    res[131] = k8_3_2_3;
+    res[132] = k8_3_3_1;
+    res[133] = k8_3_3_2;
+    res[134] = k8_3_3_3;
+    res[135] = k9_1_1_1 * 0.5773502691896258;
+    res[136] = k9_1_1_2 * 0.5773502691896258;
+    res[137] = k9_1_1_3 * 0.5773502691896258;
+    res[138] = k9_1_2_1 * 0.5773502691896258;
+    res[139] = k9_1_2_2 * 0.5773502691896258;
+    res[140] = k9_1_2_3 * 0.5773502691896258;
+    res[141] = k9_1_3_1 * 0.5773502691896258;
+    res[142] = k9_1_3_2 * 0.5773502691896258;
+    res[143] = k9_1_3_3 * 0.5773502691896258;
+    res[144] = k9_2_1_1 * 0.5773502691896258;
+    res[145] = k9_2_1_2 * 0.5773502691896258;
+    res[146] = k9_2_1_3 * 0.5773502691896258;
+    res[147] = k9_2_2_1 * 0.5773502691896258;
+    res[148] = k9_2_2_2 * 0.5773502691896258;
+    res[149] = k9_2_2_3 * 0.5773502691896258;
+    res[150] = k9_2_3_1 * 0.5773502691896258;
+    res[151] = k9_2_3_2 * 0.5773502691896258;
+    res[152] = k9_2_3_3 * 0.5773502691896258;
+    res[153] = k9_3_1_1 * 0.5773502691896258;
+    res[154] = k9_3_1_2 * 0.5773502691896258;
+    res[155] = k9_3_1_3 * 0.5773502691896258;
+    res[156] = k9_3_2_1 * 0.5773502691896258;
+    res[157] = k9_3_2_2 * 0.5773502691896258;
+    res[158] = k9_3_2_3 * 0.5773502691896258;
+    res[159] = k9_3_3_1 * 0.5773502691896258;
+    res[160] = k9_3_3_2 * 0.5773502691896258;
+    res[161] = k9_3_3_3 * 0.5773502691896258;
+}
+
+__device__ __forceinline__ void store_dppp(double *__restrict__ out, const int4 ib_, const int4 ik_,
+                                            bool same, const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    (void)dab; (void)dcd;
+    const long long ij_0_0 = pair_index(ib_.z + 0, ib_.w + 0);
+    const long long ij_0_1 = pair_index(ib_.z + 0, ib_.w + 1);
+    const long long ij_0_2 = pair_index(ib_.z + 0, ib_.w + 2);
+    const long long ij_1_0 = pair_index(ib_.z + 1, ib_.w + 0);
+    const long long ij_1_1 = pair_index(ib_.z + 1, ib_.w + 1);
+    const long long ij_1_2 = pair_index(ib_.z + 1, ib_.w + 2);
+    const long long ij_2_0 = pair_index(ib_.z + 2, ib_.w + 0);
+    const long long ij_2_1 = pair_index(ib_.z + 2, ib_.w + 1);
+    const long long ij_2_2 = pair_index(ib_.z + 2, ib_.w + 2);
+    const long long ij_3_0 = pair_index(ib_.z + 3, ib_.w + 0);
+    const long long ij_3_1 = pair_index(ib_.z + 3, ib_.w + 1);
+    const long long ij_3_2 = pair_index(ib_.z + 3, ib_.w + 2);
+    const long long ij_4_0 = pair_index(ib_.z + 4, ib_.w + 0);
+    const long long ij_4_1 = pair_index(ib_.z + 4, ib_.w + 1);
+    const long long ij_4_2 = pair_index(ib_.z + 4, ib_.w + 2);
+    const long long ij_5_0 = pair_index(ib_.z + 5, ib_.w + 0);
+    const long long ij_5_1 = pair_index(ib_.z + 5, ib_.w + 1);
+    const long long ij_5_2 = pair_index(ib_.z + 5, ib_.w + 2);
+    const long long kl_0_0 = pair_index(ik_.z + 0, ik_.w + 0);
+    const long long kl_0_1 = pair_index(ik_.z + 0, ik_.w + 1);
+    const long long kl_0_2 = pair_index(ik_.z + 0, ik_.w + 2);
+    const long long kl_1_0 = pair_index(ik_.z + 1, ik_.w + 0);
+    const long long kl_1_1 = pair_index(ik_.z + 1, ik_.w + 1);
+    const long long kl_1_2 = pair_index(ik_.z + 1, ik_.w + 2);
+    const long long kl_2_0 = pair_index(ik_.z + 2, ik_.w + 0);
+    const long long kl_2_1 = pair_index(ik_.z + 2, ik_.w + 1);
+    const long long kl_2_2 = pair_index(ik_.z + 2, ik_.w + 2);
+    { const long long ij = ij_0_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[0]; }
+    { const long long ij = ij_0_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[1]; }
+    { const long long ij = ij_0_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[2]; }
+    { const long long ij = ij_0_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[3]; }
+    { const long long ij = ij_0_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[4]; }
+    { const long long ij = ij_0_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[5]; }
+    { const long long ij = ij_0_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[6]; }
+    { const long long ij = ij_0_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[7]; }
+    { const long long ij = ij_0_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[8]; }
+    { const long long ij = ij_0_1, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[9]; }
+    { const long long ij = ij_0_1, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[10]; }
+    { const long long ij = ij_0_1, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[11]; }
+    { const long long ij = ij_0_1, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[12]; }
+    { const long long ij = ij_0_1, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[13]; }
+    { const long long ij = ij_0_1, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[14]; }
+    { const long long ij = ij_0_1, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[15]; }
+    { const long long ij = ij_0_1, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[16]; }
+    { const long long ij = ij_0_1, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[17]; }
+    { const long long ij = ij_0_2, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[18]; }
+    { const long long ij = ij_0_2, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[19]; }
+    { const long long ij = ij_0_2, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[20]; }
+    { const long long ij = ij_0_2, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[21]; }
+    { const long long ij = ij_0_2, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[22]; }
+    { const long long ij = ij_0_2, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[23]; }
+    { const long long ij = ij_0_2, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[24]; }
+    { const long long ij = ij_0_2, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[25]; }
+    { const long long ij = ij_0_2, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[26]; }
+    { const long long ij = ij_1_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[27]; }
+    { const long long ij = ij_1_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[28]; }
+    { const long long ij = ij_1_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[29]; }
+    { const long long ij = ij_1_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[30]; }
+    { const long long ij = ij_1_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[31]; }
+    { const long long ij = ij_1_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[32]; }
+    { const long long ij = ij_1_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[33]; }
+    { const long long ij = ij_1_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[34]; }
+    { const long long ij = ij_1_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[35]; }
+    { const long long ij = ij_1_1, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[36]; }
+    { const long long ij = ij_1_1, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[37]; }
+    { const long long ij = ij_1_1, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[38]; }
+    { const long long ij = ij_1_1, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[39]; }
+    { const long long ij = ij_1_1, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[40]; }
+    { const long long ij = ij_1_1, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[41]; }
+    { const long long ij = ij_1_1, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[42]; }
+    { const long long ij = ij_1_1, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[43]; }
+    { const long long ij = ij_1_1, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[44]; }
+    { const long long ij = ij_1_2, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[45]; }
+    { const long long ij = ij_1_2, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[46]; }
+    { const long long ij = ij_1_2, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[47]; }
+    { const long long ij = ij_1_2, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[48]; }
+    { const long long ij = ij_1_2, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[49]; }
+    { const long long ij = ij_1_2, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[50]; }
+    { const long long ij = ij_1_2, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[51]; }
+    { const long long ij = ij_1_2, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[52]; }
+    { const long long ij = ij_1_2, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[53]; }
+    { const long long ij = ij_2_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[54]; }
+    { const long long ij = ij_2_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[55]; }
+    { const long long ij = ij_2_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[56]; }
+    { const long long ij = ij_2_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[57]; }
+    { const long long ij = ij_2_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[58]; }
+    { const long long ij = ij_2_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[59]; }
+    { const long long ij = ij_2_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[60]; }
+    { const long long ij = ij_2_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[61]; }
+    { const long long ij = ij_2_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[62]; }
+    { const long long ij = ij_2_1, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[63]; }
+    { const long long ij = ij_2_1, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[64]; }
+    { const long long ij = ij_2_1, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[65]; }
+    { const long long ij = ij_2_1, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[66]; }
+    { const long long ij = ij_2_1, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[67]; }
+    { const long long ij = ij_2_1, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[68]; }
+    { const long long ij = ij_2_1, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[69]; }
+    { const long long ij = ij_2_1, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[70]; }
+    { const long long ij = ij_2_1, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[71]; }
+    { const long long ij = ij_2_2, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[72]; }
+    { const long long ij = ij_2_2, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[73]; }
+    { const long long ij = ij_2_2, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[74]; }
+    { const long long ij = ij_2_2, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[75]; }
+    { const long long ij = ij_2_2, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[76]; }
+    { const long long ij = ij_2_2, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[77]; }
+    { const long long ij = ij_2_2, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[78]; }
+    { const long long ij = ij_2_2, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[79]; }
+    { const long long ij = ij_2_2, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[80]; }
+    { const long long ij = ij_3_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[81]; }
+    { const long long ij = ij_3_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[82]; }
+    { const long long ij = ij_3_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[83]; }
+    { const long long ij = ij_3_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[84]; }
+    { const long long ij = ij_3_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[85]; }
+    { const long long ij = ij_3_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[86]; }
+    { const long long ij = ij_3_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[87]; }
+    { const long long ij = ij_3_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[88]; }
+    { const long long ij = ij_3_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[89]; }
+    { const long long ij = ij_3_1, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[90]; }
+    { const long long ij = ij_3_1, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[91]; }
+    { const long long ij = ij_3_1, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[92]; }
+    { const long long ij = ij_3_1, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[93]; }
+    { const long long ij = ij_3_1, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[94]; }
+    { const long long ij = ij_3_1, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[95]; }
+    { const long long ij = ij_3_1, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[96]; }
+    { const long long ij = ij_3_1, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[97]; }
+    { const long long ij = ij_3_1, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[98]; }
+    { const long long ij = ij_3_2, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[99]; }
+    { const long long ij = ij_3_2, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[100]; }
+    { const long long ij = ij_3_2, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[101]; }
+    { const long long ij = ij_3_2, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[102]; }
+    { const long long ij = ij_3_2, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[103]; }
+    { const long long ij = ij_3_2, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[104]; }
+    { const long long ij = ij_3_2, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[105]; }
+    { const long long ij = ij_3_2, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[106]; }
+    { const long long ij = ij_3_2, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[107]; }
+    { const long long ij = ij_4_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[108]; }
+    { const long long ij = ij_4_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[109]; }
+    { const long long ij = ij_4_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[110]; }
+    { const long long ij = ij_4_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[111]; }
+    { const long long ij = ij_4_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[112]; }
+    { const long long ij = ij_4_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[113]; }
+    { const long long ij = ij_4_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[114]; }
+    { const long long ij = ij_4_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[115]; }
+    { const long long ij = ij_4_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[116]; }
+    { const long long ij = ij_4_1, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[117]; }
+    { const long long ij = ij_4_1, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[118]; }
+    { const long long ij = ij_4_1, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[119]; }
+    { const long long ij = ij_4_1, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[120]; }
+    { const long long ij = ij_4_1, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[121]; }
+    { const long long ij = ij_4_1, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[122]; }
+    { const long long ij = ij_4_1, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[123]; }
+    { const long long ij = ij_4_1, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[124]; }
+    { const long long ij = ij_4_1, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[125]; }
+    { const long long ij = ij_4_2, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[126]; }
+    { const long long ij = ij_4_2, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[127]; }
+    { const long long ij = ij_4_2, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[128]; }
+    { const long long ij = ij_4_2, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[129]; }
+    { const long long ij = ij_4_2, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[130]; }
+    { const long long ij = ij_4_2, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[131]; }
+    { const long long ij = ij_4_2, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[132]; }
+    { const long long ij = ij_4_2, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[133]; }
+    { const long long ij = ij_4_2, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[134]; }
+    { const long long ij = ij_5_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[135]; }
+    { const long long ij = ij_5_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[136]; }
+    { const long long ij = ij_5_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[137]; }
+    { const long long ij = ij_5_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[138]; }
+    { const long long ij = ij_5_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[139]; }
+    { const long long ij = ij_5_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[140]; }
+    { const long long ij = ij_5_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[141]; }
+    { const long long ij = ij_5_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[142]; }
+    { const long long ij = ij_5_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[143]; }
+    { const long long ij = ij_5_1, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[144]; }
+    { const long long ij = ij_5_1, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[145]; }
+    { const long long ij = ij_5_1, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[146]; }
+    { const long long ij = ij_5_1, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[147]; }
+    { const long long ij = ij_5_1, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[148]; }
+    { const long long ij = ij_5_1, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[149]; }
+    { const long long ij = ij_5_1, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[150]; }
+    { const long long ij = ij_5_1, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[151]; }
+    { const long long ij = ij_5_1, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[152]; }
+    { const long long ij = ij_5_2, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[153]; }
+    { const long long ij = ij_5_2, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[154]; }
+    { const long long ij = ij_5_2, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[155]; }
+    { const long long ij = ij_5_2, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[156]; }
+    { const long long ij = ij_5_2, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[157]; }
+    { const long long ij = ij_5_2, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[158]; }
+    { const long long ij = ij_5_2, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[159]; }
+    { const long long ij = ij_5_2, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[160]; }
+    { const long long ij = ij_5_2, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[161]; }
+}
+
+template <int MIXED>
+__global__ void __launch_bounds__(128) eri_kernel_dppp(const EriLaunch L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.nquart) return;
+    int p, q;
+    decode_quartet(L, t, p, q);
+    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    double res[162];
+    if (bound < L.screen_cut) {
+#pragma unroll
+        for (int x = 0; x < 162; ++x) res[x] = 0.0;
+    } else if (MIXED && bound < L.fp32_cut) {
+        quartet_dppp<float>(L.pairs, L.boys, p, q, res);
+    } else {
+        quartet_dppp<double>(L.pairs, L.boys, p, q, res);
+    }
+    store_dppp(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
+}
+
+void launch_eri_dppp(const EriLaunch &L, int mixed, cudaStream_t s) {
+    if (L.nquart <= 0) return;
+    const long long blocks = (L.nquart + 127) / 128;
+    if (mixed) eri_kernel_dppp<1><<<(unsigned)blocks, 128, 0, s>>>(L);
+    else eri_kernel_dppp<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+}
+
+}  // namespace molints

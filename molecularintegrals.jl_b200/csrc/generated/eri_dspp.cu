@@ -1,0 +1,480 @@
+// Generated by gen_eri.py -- class (ds|pp).  Do not edit.
+// VRR entries: 116, contracted block: 54, HRR lines: 54, outputs: 54.
+#include "../eri_common.cuh"
+
+namespace molints {
+
+// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[54]
+// (ma, mb, mc, md row-major).  VT is the VRR arithmetic type (double, or float for MIXED).
+template <typename VT>
+__device__ __forceinline__ void quartet_dspp(const PairTab &P, const BoysTab &B, int p, int q,
+                                              double *__restrict__ res) {
+    const int4 ib_ = __ldg(&P.info[p]);
+    const int4 ik_ = __ldg(&P.info[q]);
+    double acc[54];
+#pragma unroll
+    for (int x = 0; x < 54; ++x) acc[x] = 0.0;
+    for (int i = 0; i < ib_.y; ++i) {
+        const PrimPair bra = load_pp(P.pp, ib_.x + i);
+        for (int j = 0; j < ik_.y; ++j) {
+            const PrimPair ket = load_pp(P.pp, ik_.x + j);
+            const double r = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = r * r;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double T = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = bra.kab * ket.kab * r;
+            double F[5];
+            boys_fm<4>(T, B, F);
+            const VT PAx = (VT)bra.pax, PAy = (VT)bra.pay, PAz = (VT)bra.paz;
+            const VT QCx = (VT)ket.pax, QCy = (VT)ket.pay, QCz = (VT)ket.paz;
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const VT WPx = (VT)(-ez * PQx), WPy = (VT)(-ez * PQy), WPz = (VT)(-ez * PQz);
+            const VT WQx = (VT)(zz * PQx), WQy = (VT)(zz * PQy), WQz = (VT)(zz * PQz);
+            const VT oo2z = (VT)bra.oo2z, oo2e = (VT)ket.oo2z, oo2ze = (VT)(0.5 * r2);
+            const VT rho_z = (VT)ez, rho_e = (VT)zz;
+            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz;
+            (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;
+            (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;
+            const VT v0_0_0 = (VT)(pref * F[0]);
+            const VT v0_0_1 = (VT)(pref * F[1]);
+            const VT v0_0_2 = (VT)(pref * F[2]);
+            const VT v0_0_3 = (VT)(pref * F[3]);
+            const VT v0_0_4 = (VT)(pref * F[4]);
+            const VT v1_0_0 = PAx * v0_0_0 + WPx * v0_0_1;
+            const VT v1_0_1 = PAx * v0_0_1 + WPx * v0_0_2;
+            const VT v1_0_2 = PAx * v0_0_2 + WPx * v0_0_3;
+            const VT v1_0_3 = PAx * v0_0_3 + WPx * v0_0_4;
+            const VT v2_0_0 = PAy * v0_0_0 + WPy * v0_0_1;
+            const VT v2_0_1 = PAy * v0_0_1 + WPy * v0_0_2;
+            const VT v2_0_2 = PAy * v0_0_2 + WPy * v0_0_3;
+            const VT v2_0_3 = PAy * v0_0_3 + WPy * v0_0_4;
+            const VT v3_0_0 = PAz * v0_0_0 + WPz * v0_0_1;
+            const VT v3_0_1 = PAz * v0_0_1 + WPz * v0_0_2;
+            const VT v3_0_2 = PAz * v0_0_2 + WPz * v0_0_3;
+            const VT v3_0_3 = PAz * v0_0_3 + WPz * v0_0_4;
+            const VT v4_0_0 = PAx * v1_0_0 + WPx * v1_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v4_0_1 = PAx * v1_0_1 + WPx * v1_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v4_0_2 = PAx * v1_0_2 + WPx * v1_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v5_0_0 = PAx * v2_0_0 + WPx * v2_0_1;
+            const VT v5_0_1 = PAx * v2_0_1 + WPx * v2_0_2;
+            const VT v5_0_2 = PAx * v2_0_2 + WPx * v2_0_3;
+            const VT v6_0_0 = PAx * v3_0_0 + WPx * v3_0_1;
+            const VT v6_0_1 = PAx * v3_0_1 + WPx * v3_0_2;
+            const VT v6_0_2 = PAx * v3_0_2 + WPx * v3_0_3;
+            const VT v7_0_0 = PAy * v2_0_0 + WPy * v2_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v7_0_1 = PAy * v2_0_1 + WPy * v2_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v7_0_2 = PAy * v2_0_2 + WPy * v2_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v8_0_0 = PAy * v3_0_0 + WPy * v3_0_1;
+            const VT v8_0_1 = PAy * v3_0_1 + WPy * v3_0_2;
+            const VT v8_0_2 = PAy * v3_0_2 + WPy * v3_0_3;
+            const VT v9_0_0 = PAz * v3_0_0 + WPz * v3_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v9_0_1 = PAz * v3_0_1 + WPz * v3_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v9_0_2 = PAz * v3_0_2 + WPz * v3_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v1_1_1 = QCx * v1_0_1 + WQx * v1_0_2 + (VT)1.0 * oo2ze * v0_0_2;
+            const VT v2_1_1 = QCx * v2_0_1 + WQx * v2_0_2;
+            const VT v3_1_1 = QCx * v3_0_1 + WQx * v3_0_2;
+            const VT v4_1_0 = QCx * v4_0_0 + WQx * v4_0_1 + (VT)2.0 * oo2ze * v1_0_1;
+            const VT v4_1_1 = QCx * v4_0_1 + WQx * v4_0_2 + (VT)2.0 * oo2ze * v1_0_2;
+            const VT v5_1_0 = QCx * v5_0_0 + WQx * v5_0_1 + (VT)1.0 * oo2ze * v2_0_1;
+            const VT v5_1_1 = QCx * v5_0_1 + WQx * v5_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v6_1_0 = QCx * v6_0_0 + WQx * v6_0_1 + (VT)1.0 * oo2ze * v3_0_1;
+            const VT v6_1_1 = QCx * v6_0_1 + WQx * v6_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v7_1_0 = QCx * v7_0_0 + WQx * v7_0_1;
+            const VT v7_1_1 = QCx * v7_0_1 + WQx * v7_0_2;
+            const VT v8_1_0 = QCx * v8_0_0 + WQx * v8_0_1;
+            const VT v8_1_1 = QCx * v8_0_1 + WQx * v8_0_2;
+            const VT v9_1_0 = QCx * v9_0_0 + WQx * v9_0_1;
+            const VT v9_1_1 = QCx * v9_0_1 + WQx * v9_0_2;
+            const VT v1_2_1 = QCy * v1_0_1 + WQy * v1_0_2;
+            const VT v2_2_1 = QCy * v2_0_1 + WQy * v2_0_2 + (VT)1.0 * oo2ze * v0_0_2;
+            const VT v3_2_1 = QCy * v3_0_1 + WQy * v3_0_2;
+            const VT v4_2_0 = QCy * v4_0_0 + WQy * v4_0_1;
+            const VT v4_2_1 = QCy * v4_0_1 + WQy * v4_0_2;
+            const VT v5_2_0 = QCy * v5_0_0 + WQy * v5_0_1 + (VT)1.0 * oo2ze * v1_0_1;
+            const VT v5_2_1 = QCy * v5_0_1 + WQy * v5_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v6_2_0 = QCy * v6_0_0 + WQy * v6_0_1;
+            const VT v6_2_1 = QCy * v6_0_1 + WQy * v6_0_2;
+            const VT v7_2_0 = QCy * v7_0_0 + WQy * v7_0_1 + (VT)2.0 * oo2ze * v2_0_1;
+            const VT v7_2_1 = QCy * v7_0_1 + WQy * v7_0_2 + (VT)2.0 * oo2ze * v2_0_2;
+            const VT v8_2_0 = QCy * v8_0_0 + WQy * v8_0_1 + (VT)1.0 * oo2ze * v3_0_1;
+            const VT v8_2_1 = QCy * v8_0_1 + WQy * v8_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v9_2_0 = QCy * v9_0_0 + WQy * v9_0_1;
+            const VT v9_2_1 = QCy * v9_0_1 + WQy * v9_0_2;
+            const VT v1_3_1 = QCz * v1_0_1 + WQz * v1_0_2;
+            const VT v2_3_1 = QCz * v2_0_1 + WQz * v2_0_2;
+            const VT v3_3_1 = QCz * v3_0_1 + WQz * v3_0_2 + (VT)1.0 * oo2ze * v0_0_2;
+            const VT v4_3_0 = QCz * v4_0_0 + WQz * v4_0_1;
+            const VT v4_3_1 = QCz * v4_0_1 + WQz * v4_0_2;
+            const VT v5_3_0 = QCz * v5_0_0 + WQz * v5_0_1;
+            const VT v5_3_1 = QCz * v5_0_1 + WQz * v5_0_2;
+            const VT v6_3_0 = QCz * v6_0_0 + WQz * v6_0_1 + (VT)1.0 * oo2ze * v1_0_1;
+            const VT v6_3_1 = QCz * v6_0_1 + WQz * v6_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v7_3_0 = QCz * v7_0_0 + WQz * v7_0_1;
+            const VT v7_3_1 = QCz * v7_0_1 + WQz * v7_0_2;
+            const VT v8_3_0 = QCz * v8_0_0 + WQz * v8_0_1 + (VT)1.0 * oo2ze * v2_0_1;
+            const VT v8_3_1 = QCz * v8_0_1 + WQz * v8_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v9_3_0 = QCz * v9_0_0 + WQz * v9_0_1 + (VT)2.0 * oo2ze * v3_0_1;
+            const VT v9_3_1 = QCz * v9_0_1 + WQz * v9_0_2 + (VT)2.0 * oo2ze * v3_0_2;
+            const VT v4_4_0 = QCx * v4_1_0 + WQx * v4_1_1 + (VT)2.0 * oo2ze * v1_1_1 + (VT)1.0 * oo2e * (v4_0_0 - rho_e * v4_0_1);
+            const VT v5_4_0 = QCx * v5_1_0 + WQx * v5_1_1 + (VT)1.0 * oo2ze * v2_1_1 + (VT)1.0 * oo2e * (v5_0_0 - rho_e * v5_0_1);
+            const VT v6_4_0 = QCx * v6_1_0 + WQx * v6_1_1 + (VT)1.0 * oo2ze * v3_1_1 + (VT)1.0 * oo2e * (v6_0_0 - rho_e * v6_0_1);
+            const VT v7_4_0 = QCx * v7_1_0 + WQx * v7_1_1 + (VT)1.0 * oo2e * (v7_0_0 - rho_e * v7_0_1);
+            const VT v8_4_0 = QCx * v8_1_0 + WQx * v8_1_1 + (VT)1.0 * oo2e * (v8_0_0 - rho_e * v8_0_1);
+            const VT v9_4_0 = QCx * v9_1_0 + WQx * v9_1_1 + (VT)1.0 * oo2e * (v9_0_0 - rho_e * v9_0_1);
+            const VT v4_5_0 = QCx * v4_2_0 + WQx * v4_2_1 + (VT)2.0 * oo2ze * v1_2_1;
+            const VT v5_5_0 = QCx * v5_2_0 + WQx * v5_2_1 + (VT)1.0 * oo2ze * v2_2_1;
+            const VT v6_5_0 = QCx * v6_2_0 + WQx * v6_2_1 + (VT)1.0 * oo2ze * v3_2_1;
+            const VT v7_5_0 = QCx * v7_2_0 + WQx * v7_2_1;
+            const VT v8_5_0 = QCx * v8_2_0 + WQx * v8_2_1;
+            const VT v9_5_0 = QCx * v9_2_0 + WQx * v9_2_1;
+            const VT v4_6_0 = QCx * v4_3_0 + WQx * v4_3_1 + (VT)2.0 * oo2ze * v1_3_1;
+            const VT v5_6_0 = QCx * v5_3_0 + WQx * v5_3_1 + (VT)1.0 * oo2ze * v2_3_1;
+            const VT v6_6_0 = QCx * v6_3_0 + WQx * v6_3_1 + (VT)1.0 * oo2ze * v3_3_1;
+            const VT v7_6_0 = QCx * v7_3_0 + WQx * v7_3_1;
+            const VT v8_6_0 = QCx * v8_3_0 + WQx * v8_3_1;
+            const VT v9_6_0 = QCx * v9_3_0 + WQx * v9_3_1;
+            const VT v4_7_0 = QCy * v4_2_0 + WQy * v4_2_1 + (VT)1.0 * oo2e * (v4_0_0 - rho_e * v4_0_1);
+            const VT v5_7_0 = QCy * v5_2_0 + WQy * v5_2_1 + (VT)1.0 * oo2ze * v1_2_1 + (VT)1.0 * oo2e * (v5_0_0 - rho_e * v5_0_1);
+            const VT v6_7_0 = QCy * v6_2_0 + WQy * v6_2_1 + (VT)1.0 * oo2e * (v6_0_0 - rho_e * v6_0_1);
+            const VT v7_7_0 = QCy * v7_2_0 + WQy * v7_2_1 + (VT)2.0 * oo2ze * v2_2_1 + (VT)1.0 * oo2e * (v7_0_0 - rho_e * v7_0_1);
+            const VT v8_7_0 = QCy * v8_2_0 + WQy * v8_2_1 + (VT)1.0 * oo2ze * v3_2_1 + (VT)1.0 * oo2e * (v8_0_0 - rho_e * v8_0_1);
+            const VT v9_7_0 = QCy * v9_2_0 + WQy * v9_2_1 + (VT)1.0 * oo2e * (v9_0_0 - rho_e * v9_0_1);
+            const VT v4_8_0 = QCy * v4_3_0 + WQy * v4_3_1;
+            const VT v5_8_0 = QCy * v5_3_0 + WQy * v5_3_1 + (VT)1.0 * oo2ze * v1_3_1;
+            const VT v6_8_0 = QCy * v6_3_0 + WQy * v6_3_1;
+            const VT v7_8_0 = QCy * v7_3_0 + WQy * v7_3_1 + (VT)2.0 * oo2ze * v2_3_1;
+            const VT v8_8_0 = QCy * v8_3_0 + WQy * v8_3_1 + (VT)1.0 * oo2ze * v3_3_1;
+            const VT v9_8_0 = QCy * v9_3_0 + WQy * v9_3_1;
+            const VT v4_9_0 = QCz * v4_3_0 + WQz * v4_3_1 + (VT)1.0 * oo2e * (v4_0_0 - rho_e * v4_0_1);
+            const VT v5_9_0 = QCz * v5_3_0 + WQz * v5_3_1 + (VT)1.0 * oo2e * (v5_0_0 - rho_e * v5_0_1);
+            const VT v6_9_0 = QCz * v6_3_0 + WQz * v6_3_1 + (VT)1.0 * oo2ze * v1_3_1 + (VT)1.0 * oo2e * (v6_0_0 - rho_e * v6_0_1);
+            const VT v7_9_0 = QCz * v7_3_0 + WQz * v7_3_1 + (VT)1.0 * oo2e * (v7_0_0 - rho_e * v7_0_1);
+            const VT v8_9_0 = QCz * v8_3_0 + WQz * v8_3_1 + (VT)1.0 * oo2ze * v2_3_1 + (VT)1.0 * oo2e * (v8_0_0 - rho_e * v8_0_1);
+            const VT v9_9_0 = QCz * v9_3_0 + WQz * v9_3_1 + (VT)2.0 * oo2ze * v3_3_1 + (VT)1.0 * oo2e * (v9_0_0 - rho_e * v9_0_1);
+            acc[0] += (double)v4_1_0;
+            acc[1] += (double)v4_2_0;
+            acc[2] += (double)v4_3_0;
+            acc[3] += (double)v4_4_0;
+            acc[4] += (double)v4_5_0;
+            acc[5] += (double)v4_6_0;
+            acc[6] += (double)v4_7_0;
+            acc[7] += (double)v4_8_0;
+            acc[8] += (double)v4_9_0;
+            acc[9] += (double)v5_1_0;
+            acc[10] += (double)v5_2_0;
+            acc[11] += (double)v5_3_0;
+            acc[12] += (double)v5_4_0;
+            acc[13] += (double)v5_5_0;
+            acc[14] += (double)v5_6_0;
+            acc[15] += (double)v5_7_0;
+            acc[16] += (double)v5_8_0;
+            acc[17] += (double)v5_9_0;
+            acc[18] += (double)v6_1_0;
+            acc[19] += (double)v6_2_0;
+            acc[20] += (double)v6_3_0;
+            acc[21] += (double)v6_4_0;
+            acc[22] += (double)v6_5_0;
+            acc[23] += (double)v6_6_0;
+            acc[24] += (double)v6_7_0;
+            acc[25] += (double)v6_8_0;
+            acc[26] += (double)v6_9_0;
+            acc[27] += (double)v7_1_0;
+            acc[28] += (double)v7_2_0;
+            acc[29] += (double)v7_3_0;
+            acc[30] += (double)v7_4_0;
+            acc[31] += (double)v7_5_0;
+            acc[32] += (double)v7_6_0;
+            acc[33] += (double)v7_7_0;
+            acc[34] += (double)v7_8_0;
+            acc[35] += (double)v7_9_0;
+            acc[36] += (double)v8_1_0;
+            acc[37] += (double)v8_2_0;
+            acc[38] += (double)v8_3_0;
+            acc[39] += (double)v8_4_0;
+            acc[40] += (double)v8_5_0;
+            acc[41] += (double)v8_6_0;
+            acc[42] += (double)v8_7_0;
+            acc[43] += (double)v8_8_0;
+            acc[44] += (double)v8_9_0;
+            acc[45] += (double)v9_1_0;
+            acc[46] += (double)v9_2_0;
+            acc[47] += (double)v9_3_0;
+            acc[48] += (double)v9_4_0;
+            acc[49] += (double)v9_5_0;
+            acc[50] += (double)v9_6_0;
+            acc[51] += (double)v9_7_0;
+            acc[52] += (double)v9_8_0;
+            acc[53] += (double)v9_9_0;
+        }
+    }
+    const double4 gb = ldg4(&P.geo[p]);
+    const double4 gk = ldg4(&P.geo[q]);
+    const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
+    const double CDx = gk.x, CDy = gk.y, CDz = gk.z;
+    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
+    const double k4_0_1_1 = acc[3] + CDx * acc[0];
+    const double k4_0_1_2 = acc[4] + CDy * acc[0];
+    const double k4_0_1_3 = acc[5] + CDz * acc[0];
+    const double k4_0_2_1 = acc[4] + CDx * acc[1];
+    const double k4_0_2_2 = acc[6] + CDy * acc[1];
+    const double k4_0_2_3 = acc[7] + CDz * acc[1];
+    const double k4_0_3_1 = acc[5] + CDx * acc[2];
+    const double k4_0_3_2 = acc[7] + CDy * acc[2];
+    const double k4_0_3_3 = acc[8] + CDz * acc[2];
+    const double k5_0_1_1 = acc[12] + CDx * acc[9];
+    const double k5_0_1_2 = acc[13] + CDy * acc[9];
+    const double k5_0_1_3 = acc[14] + CDz * acc[9];
+    const double k5_0_2_1 = acc[13] + CDx * acc[10];
+    const double k5_0_2_2 = acc[15] + CDy * acc[10];
+    const double k5_0_2_3 = acc[16] + CDz * acc[10];
+    const double k5_0_3_1 = acc[14] + CDx * acc[11];
+    const double k5_0_3_2 = acc[16] + CDy * acc[11];
+    const double k5_0_3_3 = acc[17] + CDz * acc[11];
+    const double k6_0_1_1 = acc[21] + CDx * acc[18];
+    const double k6_0_1_2 = acc[22] + CDy * acc[18];
+    const double k6_0_1_3 = acc[23] + CDz * acc[18];
+    const double k6_0_2_1 = acc[22] + CDx * acc[19];
+    const double k6_0_2_2 = acc[24] + CDy * acc[19];
+    const double k6_0_2_3 = acc[25] + CDz * acc[19];
+    const double k6_0_3_1 = acc[23] + CDx * acc[20];
+    const double k6_0_3_2 = acc[25] + CDy * acc[20];
+    const double k6_0_3_3 = acc[26] + CDz * acc[20];
+    const double k7_0_1_1 = acc[30] + CDx * acc[27];
+    const double k7_0_1_2 = acc[31] + CDy * acc[27];
+    const double k7_0_1_3 = acc[32] + CDz * acc[27];
+    const double k7_0_2_1 = acc[31] + CDx * acc[28];
+    const double k7_0_2_2 = acc[33] + CDy * acc[28];
+    const double k7_0_2_3 = acc[34] + CDz * acc[28];
+    const double k7_0_3_1 = acc[32] + CDx * acc[29];
+    const double k7_0_3_2 = acc[34] + CDy * acc[29];
+    const double k7_0_3_3 = acc[35] + CDz * acc[29];
+    const double k8_0_1_1 = acc[39] + CDx * acc[36];
+    const double k8_0_1_2 = acc[40] + CDy * acc[36];
+    const double k8_0_1_3 = acc[41] + CDz * acc[36];
+    const double k8_0_2_1 = acc[40] + CDx * acc[37];
+    const double k8_0_2_2 = acc[42] + CDy * acc[37];
+    const double k8_0_2_3 = acc[43] + CDz * acc[37];
+    const double k8_0_3_1 = acc[41] + CDx * acc[38];
+    const double k8_0_3_2 = acc[43] + CDy * acc[38];
+    const double k8_0_3_3 = acc[44] + CDz * acc[38];
+    const double k9_0_1_1 = acc[48] + CDx * acc[45];
+    const double k9_0_1_2 = acc[49] + CDy * acc[45];
+    const double k9_0_1_3 = acc[50] + CDz * acc[45];
+    const double k9_0_2_1 = acc[49] + CDx * acc[46];
+    const double k9_0_2_2 = acc[51] + CDy * acc[46];
+    const double k9_0_2_3 = acc[52] + CDz * acc[46];
+    const double k9_0_3_1 = acc[50] + CDx * acc[47];
+    const double k9_0_3_2 = acc[52] + CDy * acc[47];
+    const double k9_0_3_3 = acc[53] + CDz * acc[47];
+    res[0] = k4_0_1_1 * 0.5773502691896258;
+    res[1] = k4_0_1_2 * 0.5773502691896258;
+    res[2] = k4_0_1_3 * 0.5773502691896258;
+    res[3] = k4_0_2_1 * 0.5773502691896258;
+    res[4] = k4_0_2_2 * 0.5773502691896258;
+    res[5] = k4_0_2_3 * 0.5773502691896258;
+    res[6] = k4_0_3_1 * 0.5773502691896258;
+    res[7] = k4_0_3_2 * 0.5773502691896258;
+    res[8] = k4_0_3_3 * 0.5773502691896258;
+    res[9] = k5_0_1_1;
+    res[10] = k5_0_1_2;
+    res[11] = k5_0_1_3;
+    res[12] = k5_0_2_1;
+    res[13] = k5_0_2_2;
+    res[14] = k5_0_2_3;
+    res[15] = k5_0_3_1;
+    res[16] = k5_0_3_2;
+    res[17] = k5_0_3_3;
+    res[18] = k6_0_1_1;
+    res[19] = k6_0_1_2;
+    res[20] = k6_0_1_3;
+    res[21] = k6_0_2_1;
+    res[22] = k6_0_2_2;
+    res[23] = k6_0_2_3;
+    res[24] = k6_0_3_1;
+    res[25] = k6_0_3_2;
+    res[26] = k6_0_3_3;
+    res[27] = k7_0_1_1 * 0.5773502691896258;
+    res[28] = k7_0_1_2 * 0.5773502691896258;
+    res[29] = k7_0_1_3 * 0.5773502691896258;
+    res[30] = k7_0_2_1 * 0.5773502691896258;
+    res[31] = k7_0_2_2 * 0.5773502691896258;
+    res[32] = k7_0_2_3 * 0.5773502691896258;
+    res[33] = k7_0_3_1 * 0.5773502691896258;
+    res[34] = k7_0_3_2 * 0.5773502691896258;
+    res[35] = k7_0_3_3 * 0.5773502691896258;
+    res[36] = k8_0_1_1;
+    res[37] = k8_0_1_2;
+    res[38] = k8_0_1_3;
+    res[39] = k8_0_2_1;
+    res[40] = k8_0_2_2;
+    res[41] = k8_0_2_3;
+    res[42] = k8_0_3_1;
+    res[43] = k8_0_3_2;
+    res[44] = k8_0_3_3;
+    res[45] = k9_0_1_1 * 0.5773502691896258;
+    res[46] = k9_0_1_2 * 0.5773502691896258;
+    res[47] = k9_0_1_3 * 0.5773502691896258;
+    res[48] = k9_0_2_1 * 0.5773502691896258;
+    res[49] = k9_0_2_2 * 0.5773502691896258;
+    res[50] = k9_0_2_3 * 0.5773502691896258;
+    res[51] = k9_0_3_1 * 0.5773502691896258;
+    res[52] = k9_0_3_2 * 0.5773502691896258;
+    res[53] = k9_0_3_3 * 0.5773502691896258;
+}
+
+__device__ __forceinline__ void store_dspp(double *__restrict__ out, const int4 ib_, const int4 ik_,
+                                            bool same, const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    (void)dab; (void)dcd;
+    const long long ij_0_0 = pair_index(ib_.z + 0, ib_.w + 0);
+    const long long ij_1_0 = pair_index(ib_.z + 1, ib_.w + 0);
+    const long long ij_2_0 = pair_index(ib_.z + 2, ib_.w + 0);
+    const long long ij_3_0 = pair_index(ib_.z + 3, ib_.w + 0);
+    const long long ij_4_0 = pair_index(ib_.z + 4, ib_.w + 0);
+    const long long ij_5_0 = pair_index(ib_.z + 5, ib_.w + 0);
+    const long long kl_0_0 = pair_index(ik_.z + 0, ik_.w + 0);
+    const long long kl_0_1 = pair_index(ik_.z + 0, ik_.w + 1);
+    const long long kl_0_2 = pair_index(ik_.z + 0, ik_.w + 2);
+    const long long kl_1_0 = pair_index(ik_.z + 1, ik_.w + 0);
+    const long long kl_1_1 = pair_index(ik_.z + 1, ik_.w + 1);
+    const long long kl_1_2 = pair_index(ik_.z + 1, ik_.w + 2);
+    const long long kl_2_0 = pair_index(ik_.z + 2, ik_.w + 0);
+    const long long kl_2_1 = pair_index(ik_.z + 2, ik_.w + 1);
+    const long long kl_2_2 = pair_index(ik_.z + 2, ik_.w + 2);
+    { const long long ij = ij_0_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[0]; }
+    { const long long ij = ij_0_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[1]; }
+    { const long long ij = ij_0_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[2]; }
+    { const long long ij = ij_0_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[3]; }
+    { const long long ij = ij_0_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[4]; }
+    { const long long ij = ij_0_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[5]; }
+    { const long long ij = ij_0_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[6]; }
+    { const long long ij = ij_0_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[7]; }
+    { const long long ij = ij_0_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[8]; }
+    { const long long ij = ij_1_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[9]; }
+    { const long long ij = ij_1_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[10]; }
+    { const long long ij = ij_1_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[11]; }
+    { const long long ij = ij_1_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[12]; }
+    { const long long ij = ij_1_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[13]; }
+    { const long long ij = ij_1_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[14]; }
+    { const long long ij = ij_1_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[15]; }
+    { const long long ij = ij_1_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[16]; }
+    { const long long ij = ij_1_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[17]; }
+    { const long long ij = ij_2_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[18]; }
+    { const long long ij = ij_2_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[19]; }
+    { const long long ij = ij_2_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[20]; }
+    { const long long ij = ij_2_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[21]; }
+    { const long long ij = ij_2_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[22]; }
+    { const long long ij = ij_2_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[23]; }
+    { const long long ij = ij_2_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[24]; }
+    { const long long ij = ij_2_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[25]; }
+    { const long long ij = ij_2_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[26]; }
+    { const long long ij = ij_3_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[27]; }
+    { const long long ij = ij_3_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[28]; }
+    { const long long ij = ij_3_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[29]; }
+    { const long long ij = ij_3_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[30]; }
+    { const long long ij = ij_3_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[31]; }
+    { const long long ij = ij_3_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[32]; }
+    { const long long ij = ij_3_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[33]; }
+    { const long long ij = ij_3_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[34]; }
+    { const long long ij = ij_3_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[35]; }
+    { const long long ij = ij_4_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[36]; }
+    { const long long ij = ij_4_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[37]; }
+    { const long long ij = ij_4_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[38]; }
+    { const long long ij = ij_4_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[39]; }
+    { const long long ij = ij_4_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[40]; }
+    { const long long ij = ij_4_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[41]; }
+    { const long long ij = ij_4_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[42]; }
+    { const long long ij = ij_4_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[43]; }
+    { const long long ij = ij_4_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[44]; }
+    { const long long ij = ij_5_0, kl = kl_0_0;
+      if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[45]; }
+    { const long long ij = ij_5_0, kl = kl_0_1;
+      if ((!dcd || 0 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[46]; }
+    { const long long ij = ij_5_0, kl = kl_0_2;
+      if ((!dcd || 0 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[47]; }
+    { const long long ij = ij_5_0, kl = kl_1_0;
+      if ((!dcd || 1 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[48]; }
+    { const long long ij = ij_5_0, kl = kl_1_1;
+      if ((!dcd || 1 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[49]; }
+    { const long long ij = ij_5_0, kl = kl_1_2;
+      if ((!dcd || 1 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[50]; }
+    { const long long ij = ij_5_0, kl = kl_2_0;
+      if ((!dcd || 2 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[51]; }
+    { const long long ij = ij_5_0, kl = kl_2_1;
+      if ((!dcd || 2 >= 1) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[52]; }
+    { const long long ij = ij_5_0, kl = kl_2_2;
+      if ((!dcd || 2 >= 2) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[53]; }
+}
+
+template <int MIXED>
+__global__ void __launch_bounds__(128) eri_kernel_dspp(const EriLaunch L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.nquart) return;
+    int p, q;
+    decode_quartet(L, t, p, q);
+    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    double res[54];
+    if (bound < L.screen_cut) {
+#pragma unroll
+        for (int x = 0; x < 54; ++x) res[x] = 0.0;
+    } else if (MIXED && bound < L.fp32_cut) {
+        quartet_dspp<float>(L.pairs, L.boys, p, q, res);
+    } else {
+        quartet_dspp<double>(L.pairs, L.boys, p, q, res);
+    }
+    store_dspp(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
+}
+
+void launch_eri_dspp(const EriLaunch &L, int mixed, cudaStream_t s) {
+    if (L.nquart <= 0) return;
+    const long long blocks = (L.nquart + 127) / 128;
+    if (mixed) eri_kernel_dspp<1><<<(unsigned)blocks, 128, 0, s>>>(L);
+    else eri_kernel_dspp<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+}
+
+}  // namespace molints

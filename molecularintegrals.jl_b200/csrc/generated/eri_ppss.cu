@@ -1,0 +1,149 @@
+// Generated by gen_eri.py -- class (pp|ss).  Do not edit.
+// VRR entries: 15, contracted block: 9, HRR lines: 9, outputs: 9.
+#include "../eri_common.cuh"
+
+namespace molints {
+
+// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[9]
+// (ma, mb, mc, md row-major).  VT is the VRR arithmetic type (double, or float for MIXED).
+template <typename VT>
+__device__ __forceinline__ void quartet_ppss(const PairTab &P, const BoysTab &B, int p, int q,
+                                              double *__restrict__ res) {
+    const int4 ib_ = __ldg(&P.info[p]);
+    const int4 ik_ = __ldg(&P.info[q]);
+    double acc[9];
+#pragma unroll
+    for (int x = 0; x < 9; ++x) acc[x] = 0.0;
+    for (int i = 0; i < ib_.y; ++i) {
+        const PrimPair bra = load_pp(P.pp, ib_.x + i);
+        for (int j = 0; j < ik_.y; ++j) {
+            const PrimPair ket = load_pp(P.pp, ik_.x + j);
+            const double r = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = r * r;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double T = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = bra.kab * ket.kab * r;
+            double F[3];
+            boys_fm<2>(T, B, F);
+            const VT PAx = (VT)bra.pax, PAy = (VT)bra.pay, PAz = (VT)bra.paz;
+            const VT QCx = (VT)ket.pax, QCy = (VT)ket.pay, QCz = (VT)ket.paz;
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const VT WPx = (VT)(-ez * PQx), WPy = (VT)(-ez * PQy), WPz = (VT)(-ez * PQz);
+            const VT WQx = (VT)(zz * PQx), WQy = (VT)(zz * PQy), WQz = (VT)(zz * PQz);
+            const VT oo2z = (VT)bra.oo2z, oo2e = (VT)ket.oo2z, oo2ze = (VT)(0.5 * r2);
+            const VT rho_z = (VT)ez, rho_e = (VT)zz;
+            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz;
+            (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;
+            (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;
+            const VT v0_0_0 = (VT)(pref * F[0]);
+            const VT v0_0_1 = (VT)(pref * F[1]);
+            const VT v0_0_2 = (VT)(pref * F[2]);
+            const VT v1_0_0 = PAx * v0_0_0 + WPx * v0_0_1;
+            const VT v1_0_1 = PAx * v0_0_1 + WPx * v0_0_2;
+            const VT v2_0_0 = PAy * v0_0_0 + WPy * v0_0_1;
+            const VT v2_0_1 = PAy * v0_0_1 + WPy * v0_0_2;
+            const VT v3_0_0 = PAz * v0_0_0 + WPz * v0_0_1;
+            const VT v3_0_1 = PAz * v0_0_1 + WPz * v0_0_2;
+            const VT v4_0_0 = PAx * v1_0_0 + WPx * v1_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v5_0_0 = PAx * v2_0_0 + WPx * v2_0_1;
+            const VT v6_0_0 = PAx * v3_0_0 + WPx * v3_0_1;
+            const VT v7_0_0 = PAy * v2_0_0 + WPy * v2_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v8_0_0 = PAy * v3_0_0 + WPy * v3_0_1;
+            const VT v9_0_0 = PAz * v3_0_0 + WPz * v3_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            acc[0] += (double)v1_0_0;
+            acc[1] += (double)v2_0_0;
+            acc[2] += (double)v3_0_0;
+            acc[3] += (double)v4_0_0;
+            acc[4] += (double)v5_0_0;
+            acc[5] += (double)v6_0_0;
+            acc[6] += (double)v7_0_0;
+            acc[7] += (double)v8_0_0;
+            acc[8] += (double)v9_0_0;
+        }
+    }
+    const double4 gb = ldg4(&P.geo[p]);
+    const double4 gk = ldg4(&P.geo[q]);
+    const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
+    const double CDx = gk.x, CDy = gk.y, CDz = gk.z;
+    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
+    const double h1_1_0 = acc[3] + ABx * acc[0];
+    const double h1_2_0 = acc[4] + ABy * acc[0];
+    const double h1_3_0 = acc[5] + ABz * acc[0];
+    const double h2_1_0 = acc[4] + ABx * acc[1];
+    const double h2_2_0 = acc[6] + ABy * acc[1];
+    const double h2_3_0 = acc[7] + ABz * acc[1];
+    const double h3_1_0 = acc[5] + ABx * acc[2];
+    const double h3_2_0 = acc[7] + ABy * acc[2];
+    const double h3_3_0 = acc[8] + ABz * acc[2];
+    res[0] = h1_1_0;
+    res[1] = h1_2_0;
+    res[2] = h1_3_0;
+    res[3] = h2_1_0;
+    res[4] = h2_2_0;
+    res[5] = h2_3_0;
+    res[6] = h3_1_0;
+    res[7] = h3_2_0;
+    res[8] = h3_3_0;
+}
+
+__device__ __forceinline__ void store_ppss(double *__restrict__ out, const int4 ib_, const int4 ik_,
+                                            bool same, const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    (void)dab; (void)dcd;
+    const long long ij_0_0 = pair_index(ib_.z + 0, ib_.w + 0);
+    const long long ij_0_1 = pair_index(ib_.z + 0, ib_.w + 1);
+    const long long ij_0_2 = pair_index(ib_.z + 0, ib_.w + 2);
+    const long long ij_1_0 = pair_index(ib_.z + 1, ib_.w + 0);
+    const long long ij_1_1 = pair_index(ib_.z + 1, ib_.w + 1);
+    const long long ij_1_2 = pair_index(ib_.z + 1, ib_.w + 2);
+    const long long ij_2_0 = pair_index(ib_.z + 2, ib_.w + 0);
+    const long long ij_2_1 = pair_index(ib_.z + 2, ib_.w + 1);
+    const long long ij_2_2 = pair_index(ib_.z + 2, ib_.w + 2);
+    const long long kl_0_0 = pair_index(ik_.z + 0, ik_.w + 0);
+    { const long long ij = ij_0_0, kl = kl_0_0;
+      if ((!dab || 0 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[0]; }
+    { const long long ij = ij_0_1, kl = kl_0_0;
+      if ((!dab || 0 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[1]; }
+    { const long long ij = ij_0_2, kl = kl_0_0;
+      if ((!dab || 0 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[2]; }
+    { const long long ij = ij_1_0, kl = kl_0_0;
+      if ((!dab || 1 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[3]; }
+    { const long long ij = ij_1_1, kl = kl_0_0;
+      if ((!dab || 1 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[4]; }
+    { const long long ij = ij_1_2, kl = kl_0_0;
+      if ((!dab || 1 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[5]; }
+    { const long long ij = ij_2_0, kl = kl_0_0;
+      if ((!dab || 2 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[6]; }
+    { const long long ij = ij_2_1, kl = kl_0_0;
+      if ((!dab || 2 >= 1) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[7]; }
+    { const long long ij = ij_2_2, kl = kl_0_0;
+      if ((!dab || 2 >= 2) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[8]; }
+}
+
+template <int MIXED>
+__global__ void __launch_bounds__(128) eri_kernel_ppss(const EriLaunch L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.nquart) return;
+    int p, q;
+    decode_quartet(L, t, p, q);
+    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    double res[9];
+    if (bound < L.screen_cut) {
+#pragma unroll
+        for (int x = 0; x < 9; ++x) res[x] = 0.0;
+    } else if (MIXED && bound < L.fp32_cut) {
+        quartet_ppss<float>(L.pairs, L.boys, p, q, res);
+    } else {
+        quartet_ppss<double>(L.pairs, L.boys, p, q, res);
+    }
+    store_ppss(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
+}
+
+void launch_eri_ppss(const EriLaunch &L, int mixed, cudaStream_t s) {
+    if (L.nquart <= 0) return;
+    const long long blocks = (L.nquart + 127) / 128;
+    if (mixed) eri_kernel_ppss<1><<<(unsigned)blocks, 128, 0, s>>>(L);
+    else eri_kernel_ppss<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+}
+
+}  // namespace molints

@@ -1,0 +1,630 @@
+// molints.cu -- host side of libmolints_cuda.so: contexts, plans and the C ABI of
+// include/molints.h, plus the device pair builder and the Boys-table kernels.
+//
+// Execution of a plan (all on the context's stream, no host synchronisation):
+//   1. build_pairs_kernel: one thread per canonical shell pair writes its primitive-pair
+//      records (zeta, P, P-A, exp(-ab/zeta |A-B|^2) prefactor) and A-B;
+//   2. schwarz kernels, one per pair class: Q_p = sqrt(max |(ab|ab)|);
+//   3. one generated kernel per class pair (bra class >= ket class) over all its unique
+//      shell quartets, writing the packed iindex vector.
+// The drivers this replaces are all_twoe_ints_chrr (src/HGP.jl:22-34) and all_twoe_ints
+// (src/ERI.jl:104-112) of MolecularIntegrals.jl.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/molints.h"
+#include "eri_common.cuh"
+#include "eri_dispatch.h"
+
+using namespace molints;
+
+struct molints_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int64_t budget = 0;        // bytes, 0 = unbounded
+    int64_t held = 0;          // bytes currently allocated by this context and its plans
+    double *boys_tab = nullptr;
+    double *out_cache = nullptr;  // device buffer for host-output calls
+    int64_t out_cache_len = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+};
+
+struct molints_plan {
+    molints_ctx *ctx = nullptr;
+    molints_options opts{};
+    int nshell = 0;
+    int64_t nbf = 0, npacked = 0;
+    int npair = 0, nprim_pair = 0;
+    int class_start[kNumPairClasses + 1] = {0};
+    // host copies
+    std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
+    std::vector<int4> info_h;
+    std::vector<int> npp_h;
+    // device buffers
+    double *sh_xyz = nullptr, *expn = nullptr, *ncoef = nullptr;
+    int *sh_poff = nullptr, *sh_nprim = nullptr;
+    int2 *pair_ab = nullptr;
+    int4 *info = nullptr;
+    double4 *geo = nullptr;
+    PrimPair *pp = nullptr;
+    int64_t bytes = 0;
+    int n_launches = 0;
+    // per-launch profiling (molints_plan_set_profiling)
+    int profiling = 0;
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<const char *> prof_name;
+};
+
+// ------------------------------------------------------------------ helpers
+namespace {
+
+int fail(molints_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(molints_ctx *ctx, cudaError_t e, const char *what) {
+    return fail(ctx, MOLINTS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define MI_CUDA(ctx, call)                                            \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);    \
+    } while (0)
+
+int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+double dfact2(int n) {
+    double r = 1;
+    for (int k = n; k > 1; k -= 2) r *= k;
+    return r;
+}
+
+// Exact F_m(T) by the series e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)), long double.
+double boys_series(int m, double T) {
+    if (T == 0.0) return 1.0 / (2 * m + 1);
+    long double t = T, sum = 0.0L, term = 1.0L / (2 * m + 1);
+    for (int k = 0; k < 100000; ++k) {
+        sum += term;
+        if (k > T && term < sum * 1e-22L) break;
+        term *= 2.0L * t / (2 * m + 2 * k + 3);
+    }
+    return (double)(expl(-t) * sum);
+}
+
+int pair_class_of(int la, int lb) {
+    for (int c = 0; c < kNumPairClasses; ++c)
+        if (kPairClassLa[c] == la && kPairClassLb[c] == lb) return c;
+    return -1;
+}
+
+template <typename T>
+int dev_alloc(molints_ctx *ctx, T **p, size_t count, int64_t *tally) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (ctx->budget > 0 && ctx->held + (int64_t)bytes > ctx->budget)
+        return fail(ctx, MOLINTS_ERR_BUDGET, "HBM budget exceeded");
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    ctx->held += (int64_t)bytes;
+    if (tally) *tally += (int64_t)bytes;
+    return MOLINTS_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ device kernels
+namespace molints {
+
+__global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
+                                   const int4 *__restrict__ info, const double *__restrict__ xyz,
+                                   const int *__restrict__ poff, const int *__restrict__ nprim,
+                                   const double *__restrict__ expn,
+                                   const double *__restrict__ ncoef, PrimPair *__restrict__ pp,
+                                   double4 *__restrict__ geo) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npair) return;
+    const int2 ab = pair_ab[p];
+    const int4 in = info[p];
+    const double Ax = xyz[3 * ab.x], Ay = xyz[3 * ab.x + 1], Az = xyz[3 * ab.x + 2];
+    const double Bx = xyz[3 * ab.y], By = xyz[3 * ab.y + 1], Bz = xyz[3 * ab.y + 2];
+    const double ABx = Ax - Bx, ABy = Ay - By, ABz = Az - Bz;
+    const double rab2 = ABx * ABx + ABy * ABy + ABz * ABz;
+    const int ka = nprim[ab.x], kb = nprim[ab.y];
+    const int pa0 = poff[ab.x], pb0 = poff[ab.y];
+    const double c0 = 3.5546813524369302;  // sqrt(2) pi^(5/4)
+    int k = in.x;
+    for (int ia = 0; ia < ka; ++ia) {
+        const double a = expn[pa0 + ia], ca = ncoef[pa0 + ia];
+        for (int ib = 0; ib < kb; ++ib, ++k) {
+            const double b = expn[pb0 + ib], cb = ncoef[pb0 + ib];
+            const double zeta = a + b, ooz = 1.0 / zeta;
+            PrimPair r;
+            r.zeta = zeta;
+            r.kab = c0 * ca * cb * exp(-a * b * ooz * rab2) * ooz;
+            r.oo2z = 0.5 * ooz;
+            r.px = (a * Ax + b * Bx) * ooz;
+            r.py = (a * Ay + b * By) * ooz;
+            r.pz = (a * Az + b * Bz) * ooz;
+            r.pax = r.px - Ax;
+            r.pay = r.py - Ay;
+            r.paz = r.pz - Az;
+            r.pad = 0.0;
+            pp[k] = r;
+        }
+    }
+    geo[p] = make_double4(ABx, ABy, ABz, 0.0);
+}
+
+__global__ void boys_eval_kernel(BoysTab bt, int mmax, const double *__restrict__ T, long long n,
+                                 double *__restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double F[23];
+    const double t = T[i];
+    switch (mmax - 1) {
+#define MI_CASE(M) case M: boys_fm<M>(t, bt, F); break;
+        MI_CASE(0) MI_CASE(1) MI_CASE(2) MI_CASE(3) MI_CASE(4) MI_CASE(5) MI_CASE(6)
+        MI_CASE(7) MI_CASE(8) MI_CASE(9) MI_CASE(10) MI_CASE(11) MI_CASE(12)
+        MI_CASE(13) MI_CASE(14) MI_CASE(15)
+#undef MI_CASE
+        default: return;
+    }
+    for (int m = 0; m < mmax; ++m) out[i * mmax + m] = F[m];
+}
+
+}  // namespace molints
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int molints_abi_version(void) { return MOLINTS_ABI_VERSION; }
+
+void molints_default_options(molints_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->method = MOLINTS_METHOD_AUTO;
+    o->precision = MOLINTS_FP64;
+    o->boys = MOLINTS_BOYS_REFERENCE;
+    o->fp32_cutoff = 0.0;
+    o->screen_cutoff = 0.0;
+}
+
+int64_t molints_npacked(int64_t n) { return n < 0 ? -1 : n * (n + 1) * (n * n + n + 2) / 8; }
+
+int64_t molints_nbf(const molints_basis *b) {
+    if (!b || b->nshell < 0 || (b->nshell > 0 && (!b->L || !b->xyz || !b->nprim || !b->prim_off)))
+        return MOLINTS_ERR_INVALID;
+    int64_t n = 0;
+    for (int s = 0; s < b->nshell; ++s) {
+        if (b->L[s] < 0) return MOLINTS_ERR_INVALID;
+        n += ncart(b->L[s]);
+    }
+    return n;
+}
+
+int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags) {
+    if (!out) return MOLINTS_ERR_INVALID;
+    *out = nullptr;
+    if (flags != 0) return MOLINTS_ERR_INVALID;
+    molints_ctx *ctx = new (std::nothrow) molints_ctx();
+    if (!ctx) return MOLINTS_ERR_NOMEM;
+    ctx->device = device;
+    ctx->budget = budget;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { delete ctx; return MOLINTS_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+        molints_destroy(ctx);
+        return MOLINTS_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    // Boys table: F_0..F_22 and e^-T at T_n = n/16, n = 0..640.
+    std::vector<double> tab((size_t)kBoysRows * kBoysCols);
+    for (int n = 0; n < kBoysRows; ++n) {
+        const double T = n * kBoysStep;
+        for (int m = 0; m < kBoysCols - 1; ++m) tab[(size_t)n * kBoysCols + m] = boys_series(m, T);
+        tab[(size_t)n * kBoysCols + kBoysCols - 1] = std::exp(-T);
+    }
+    int rc = dev_alloc(ctx, &ctx->boys_tab, tab.size(), nullptr);
+    if (rc) { molints_destroy(ctx); return rc; }
+    if (cudaMemcpy(ctx->boys_tab, tab.data(), tab.size() * sizeof(double),
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+        molints_destroy(ctx);
+        return MOLINTS_ERR_CUDA;
+    }
+    *out = ctx;
+    return MOLINTS_OK;
+}
+
+int molints_destroy(molints_ctx *ctx) {
+    if (!ctx) return MOLINTS_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+    if (ctx->boys_tab) cudaFree(ctx->boys_tab);
+    if (ctx->out_cache) cudaFree(ctx->out_cache);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return MOLINTS_OK;
+}
+
+const char *molints_last_error(const molints_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int molints_set_stream(molints_ctx *ctx, void *stream) {
+    if (!ctx) return MOLINTS_ERR_INVALID;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return MOLINTS_OK;
+}
+
+static BoysTab boys_of(const molints_ctx *ctx, int mode) {
+    BoysTab bt;
+    bt.tab = ctx->boys_tab;
+    bt.t_switch = (mode == MOLINTS_BOYS_EXACT) ? kBoysTableMax : kBoysReferenceSwitch;
+    return bt;
+}
+
+int molints_boys_eval(molints_ctx *ctx, int32_t mode, int32_t mmax, const double *T, int64_t n,
+                      double *out) {
+    if (!ctx || !T || !out || n < 0 || mmax < 1 || mmax > 16 ||
+        (mode != MOLINTS_BOYS_REFERENCE && mode != MOLINTS_BOYS_EXACT))
+        return fail(ctx, MOLINTS_ERR_INVALID, "molints_boys_eval: bad argument");
+    for (int64_t i = 0; i < n; ++i)
+        if (!(T[i] >= 0.0) || !std::isfinite(T[i]))
+            return fail(ctx, MOLINTS_ERR_INVALID, "molints_boys_eval: T must be finite and >= 0");
+    if (n == 0) return MOLINTS_OK;
+    MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    double *dT = nullptr, *dout = nullptr;
+    int rc = dev_alloc(ctx, &dT, (size_t)n, nullptr);
+    if (rc) return rc;
+    rc = dev_alloc(ctx, &dout, (size_t)n * mmax, nullptr);
+    if (rc) { cudaFree(dT); ctx->held -= n * 8; return rc; }
+    cudaError_t e = cudaMemcpyAsync(dT, T, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        boys_eval_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(boys_of(ctx, mode), mmax,
+                                                                               dT, n, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dout, n * mmax * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(dT);
+    cudaFree(dout);
+    ctx->held -= (int64_t)(n + n * mmax) * 8;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "molints_boys_eval");
+    return MOLINTS_OK;
+}
+
+static void plan_free(molints_plan *p) {
+    if (!p) return;
+    for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
+    void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->sh_nprim, p->pair_ab,
+                    p->info, p->geo, p->pp};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (p->ctx) p->ctx->held -= p->bytes;
+    delete p;
+}
+
+int molints_plan_destroy(molints_plan *p) {
+    if (!p) return MOLINTS_OK;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    plan_free(p);
+    return MOLINTS_OK;
+}
+
+int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_options *opts_in,
+                        molints_plan **out) {
+    if (!ctx || !b || !out) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null argument");
+    *out = nullptr;
+    molints_options opts;
+    if (opts_in) opts = *opts_in; else molints_default_options(&opts);
+    if (opts.precision != MOLINTS_FP64 && opts.precision != MOLINTS_MIXED)
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown precision");
+    if (opts.boys != MOLINTS_BOYS_REFERENCE && opts.boys != MOLINTS_BOYS_EXACT)
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown Boys mode");
+    if (opts.method != MOLINTS_METHOD_AUTO && opts.method != MOLINTS_METHOD_HGP)
+        return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: method not available");
+    if (!(opts.fp32_cutoff >= 0.0) || !(opts.screen_cutoff >= 0.0))
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: cutoffs must be >= 0");
+    const int64_t nbf = molints_nbf(b);
+    if (nbf < 0) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: malformed basis");
+    const int ns = b->nshell;
+    if (ns > 0 && (!b->expn || !b->coef)) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null primitives");
+    int nprim_tot = 0;
+    for (int s = 0; s < ns; ++s) {
+        if (b->L[s] > MOLINTS_LMAX)
+            return fail(ctx, MOLINTS_ERR_UNSUPPORTED,
+                        "plan_create: shell angular momentum above " + std::to_string(MOLINTS_LMAX));
+        if (b->nprim[s] < 1 || b->prim_off[s] < 0)
+            return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: shell without primitives");
+        nprim_tot = std::max(nprim_tot, b->prim_off[s] + b->nprim[s]);
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(b->xyz[3 * s + k])) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: non-finite centre");
+    }
+    // n(n+1)(n^2+n+2)/8 stays well inside int64 and the int pair indices for n <= 46000
+    if (nbf > 46000) return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: basis too large");
+    for (int k = 0; k < nprim_tot; ++k)
+        if (!(b->expn[k] > 0.0) || !std::isfinite(b->expn[k]) || !std::isfinite(b->coef[k]))
+            return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: exponents must be finite and > 0");
+
+    molints_plan *p = new (std::nothrow) molints_plan();
+    if (!p) return MOLINTS_ERR_NOMEM;
+    p->ctx = ctx;
+    p->opts = opts;
+    p->nshell = ns;
+    p->nbf = nbf;
+    p->npacked = molints_npacked(nbf);
+
+    // Normalised coefficients: raw coef x (2a/pi)^(3/4) (4a)^(L/2) x CGBF norm; the component
+    // factor 1/sqrt((2I-1)!!(2J-1)!!(2K-1)!!) is applied by the generated kernels
+    // (PGBF/CGBF normalize!, src/Basis.jl:42-83).
+    std::vector<double> ncoef(std::max(nprim_tot, 1), 0.0);
+    std::vector<int> fn_off(ns + 1, 0);
+    for (int s = 0; s < ns; ++s) {
+        const int L = b->L[s], p0 = b->prim_off[s], K = b->nprim[s];
+        double S = 0;
+        for (int i = 0; i < K; ++i)
+            for (int j = 0; j < K; ++j) {
+                const double x = b->expn[p0 + i], y = b->expn[p0 + j];
+                S += b->coef[p0 + i] * b->coef[p0 + j] * std::pow(2 * std::sqrt(x * y) / (x + y), L + 1.5);
+            }
+        if (!(S > 0.0)) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: zero contracted function"); }
+        const double cn = 1.0 / std::sqrt(S);
+        for (int i = 0; i < K; ++i) {
+            const double a = b->expn[p0 + i];
+            ncoef[p0 + i] = b->coef[p0 + i] * cn * std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * L);
+        }
+        fn_off[s + 1] = fn_off[s] + ncart(L);
+    }
+
+    // Canonical shell pairs (L_A >= L_B), ordered by class, then by descending K_A K_B.
+    struct PairRec { int cls, npp, a, b, ref; };
+    std::vector<PairRec> pr;
+    pr.reserve((size_t)ns * (ns + 1) / 2);
+    for (int i = 0; i < ns; ++i)
+        for (int j = 0; j <= i; ++j) {
+            int a = i, bb = j;
+            if (b->L[a] < b->L[bb]) std::swap(a, bb);
+            pr.push_back({pair_class_of(b->L[a], b->L[bb]), b->nprim[a] * b->nprim[bb], a, bb,
+                          i * (i + 1) / 2 + j});
+        }
+    std::stable_sort(pr.begin(), pr.end(), [](const PairRec &x, const PairRec &y) {
+        return x.cls != y.cls ? x.cls < y.cls : x.npp > y.npp;
+    });
+    p->npair = (int)pr.size();
+    std::vector<int2> ab_h(p->npair);
+    p->info_h.resize(p->npair);
+    p->npp_h.resize(p->npair);
+    p->pair_ref.resize(p->npair);
+    int ppo = 0;
+    for (int k = 0; k < p->npair; ++k) {
+        ab_h[k] = make_int2(pr[k].a, pr[k].b);
+        p->info_h[k] = make_int4(ppo, pr[k].npp, fn_off[pr[k].a], fn_off[pr[k].b]);
+        p->npp_h[k] = pr[k].npp;
+        p->pair_ref[k] = pr[k].ref;
+        ppo += pr[k].npp;
+        p->class_start[pr[k].cls + 1] = k + 1;
+    }
+    for (int c = 1; c <= kNumPairClasses; ++c)
+        p->class_start[c] = std::max(p->class_start[c], p->class_start[c - 1]);
+    p->nprim_pair = ppo;
+
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) { plan_free(p); return cuda_fail(ctx, e, "cudaSetDevice"); }
+    int rc = 0;
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_xyz, (size_t)3 * ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->expn, (size_t)nprim_tot, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->ncoef, (size_t)nprim_tot, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_poff, (size_t)ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_nprim, (size_t)ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->pair_ab, (size_t)p->npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->info, (size_t)p->npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->geo, (size_t)p->npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)ppo, &p->bytes);
+    if (rc) { plan_free(p); return rc; }
+    cudaStream_t s = ctx->stream;
+    const size_t np = (size_t)std::max(nprim_tot, 0);
+    if ((e = cudaMemcpyAsync(p->sh_xyz, b->xyz, 3 * ns * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->expn, b->expn, np * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->ncoef, ncoef.data(), np * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->sh_poff, b->prim_off, ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->sh_nprim, b->nprim, ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), p->npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->info, p->info_h.data(), p->npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaStreamSynchronize(s))) {
+        plan_free(p);
+        return cuda_fail(ctx, e, "plan_create upload");
+    }
+    *out = p;
+    return MOLINTS_OK;
+}
+
+int molints_plan_execute(molints_plan *p, double *out_device) {
+    if (!p || !out_device) return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_execute: null argument");
+    molints_ctx *ctx = p->ctx;
+    MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    int launches = 0;
+    // event pair around each launch when profiling (launch k uses events 2k, 2k+1)
+    auto mark = [&](int k, const char *name, int end) -> int {
+        if (!p->profiling) return 0;
+        while ((int)p->prof_ev.size() < 2 * k + 2) {
+            cudaEvent_t e;
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return cuda_fail(ctx, err, "cudaEventCreate");
+            p->prof_ev.push_back(e);
+        }
+        if ((int)p->prof_name.size() < k + 1) p->prof_name.resize(k + 1);
+        p->prof_name[k] = name;
+        cudaError_t err = cudaEventRecord(p->prof_ev[2 * k + end], s);
+        return err == cudaSuccess ? 0 : cuda_fail(ctx, err, "cudaEventRecord");
+    };
+    MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
+    if (p->npair > 0) {
+        if (int rc = mark(launches, "build_pairs", 0)) return rc;
+        build_pairs_kernel<<<(p->npair + 127) / 128, 128, 0, s>>>(
+            p->npair, p->pair_ab, p->info, p->sh_xyz, p->sh_poff, p->sh_nprim, p->expn, p->ncoef,
+            p->pp, p->geo);
+        if (int rc = mark(launches, "build_pairs", 1)) return rc;
+        ++launches;
+    }
+    PairTab P{p->info, p->geo, p->pp};
+    BoysTab B = boys_of(ctx, p->opts.boys);
+    for (int c = 0; c < kNumPairClasses; ++c) {
+        const int n = p->class_start[c + 1] - p->class_start[c];
+        if (n > 0) {
+            if (int rc = mark(launches, kSchwarzNames[c], 0)) return rc;
+            kSchwarzLaunchers[c](P, B, p->class_start[c], n, p->geo, s);
+            if (int rc = mark(launches, kSchwarzNames[c], 1)) return rc;
+            ++launches;
+        }
+    }
+    const int mixed = p->opts.precision == MOLINTS_MIXED ? 1 : 0;
+    for (int x = 0; x < kNumPairClasses; ++x) {
+        const int nx = p->class_start[x + 1] - p->class_start[x];
+        if (nx == 0) continue;
+        for (int y = 0; y <= x; ++y) {
+            const int ny = p->class_start[y + 1] - p->class_start[y];
+            if (ny == 0) continue;
+            EriLaunch L{};
+            L.pairs = P;
+            L.boys = B;
+            L.out = out_device;
+            L.bra0 = p->class_start[x];
+            L.nbra = nx;
+            L.ket0 = p->class_start[y];
+            L.nket = ny;
+            L.tri = (x == y);
+            L.nquart = L.tri ? (long long)nx * (nx + 1) / 2 : (long long)nx * ny;
+            L.screen_cut = p->opts.screen_cutoff;
+            L.fp32_cut = p->opts.fp32_cutoff;
+            if (int rc = mark(launches, kEriNames[x][y], 0)) return rc;
+            kEriLaunchers[x][y](L, mixed, s);
+            if (int rc = mark(launches, kEriNames[x][y], 1)) return rc;
+            ++launches;
+        }
+    }
+    MI_CUDA(ctx, cudaGetLastError());
+    MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
+    p->n_launches = launches;
+    return MOLINTS_OK;
+}
+
+int molints_plan_stats(const molints_plan *p, molints_stats *st) {
+    if (!p || !st) return MOLINTS_ERR_INVALID;
+    molints_ctx *ctx = p->ctx;
+    std::memset(st, 0, sizeof(*st));
+    st->n_eri = p->npacked;
+    const int64_t np = p->npair;
+    st->n_shell_quartets = np * (np + 1) / 2;
+    int64_t sum = 0, sum2 = 0;
+    for (int k = 0; k < p->npair; ++k) { sum += p->npp_h[k]; sum2 += (int64_t)p->npp_h[k] * p->npp_h[k]; }
+    st->n_prim_quartets = (sum * sum + sum2) / 2;
+    st->n_kernel_launches = p->n_launches;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return MOLINTS_ERR_CUDA;
+    if (cudaEventSynchronize(ctx->ev1) == cudaSuccess) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) st->device_ms = ms;
+    }
+    if (p->opts.precision == MOLINTS_MIXED || p->opts.screen_cutoff > 0.0) {
+        std::vector<double4> g(p->npair);
+        if (cudaMemcpy(g.data(), p->geo, p->npair * sizeof(double4), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return MOLINTS_ERR_CUDA;
+        for (int a = 0; a < p->npair; ++a)
+            for (int c = 0; c <= a; ++c) {
+                const double bnd = g[a].w * g[c].w;
+                if (bnd < p->opts.screen_cutoff) ++st->n_screened;
+                else if (p->opts.precision == MOLINTS_MIXED && bnd < p->opts.fp32_cutoff) ++st->n_fp32_quartets;
+            }
+    }
+    return MOLINTS_OK;
+}
+
+int molints_plan_set_profiling(molints_plan *p, int enable) {
+    if (!p) return MOLINTS_ERR_INVALID;
+    p->profiling = enable ? 1 : 0;
+    return MOLINTS_OK;
+}
+
+int molints_plan_launch_times(molints_plan *p, const char **names, float *ms, int cap) {
+    if (!p || cap < 0 || (cap > 0 && (!names || !ms))) return MOLINTS_ERR_INVALID;
+    molints_ctx *ctx = p->ctx;
+    if (!p->profiling) return fail(ctx, MOLINTS_ERR_INVALID, "launch_times: profiling is off");
+    MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    MI_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+    const int n = p->n_launches;
+    for (int k = 0; k < n && k < cap; ++k) {
+        names[k] = p->prof_name[k];
+        MI_CUDA(ctx, cudaEventElapsedTime(&ms[k], p->prof_ev[2 * k], p->prof_ev[2 * k + 1]));
+    }
+    return n;
+}
+
+int molints_plan_schwarz(molints_plan *p, double *out) {
+    if (!p || !out) return MOLINTS_ERR_INVALID;
+    molints_ctx *ctx = p->ctx;
+    MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    std::vector<double4> g(p->npair);
+    MI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    MI_CUDA(ctx, cudaMemcpy(g.data(), p->geo, p->npair * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < p->npair; ++k) out[p->pair_ref[k]] = g[k].w;
+    return MOLINTS_OK;
+}
+
+int molints_eri_packed(molints_ctx *ctx, const molints_basis *b, const molints_options *opts,
+                       double *out, int out_is_device, molints_stats *stats) {
+    if (!ctx || !b) return fail(ctx, MOLINTS_ERR_INVALID, "eri_packed: null argument");
+    const int64_t nbf = molints_nbf(b);
+    if (nbf < 0) return fail(ctx, MOLINTS_ERR_INVALID, "eri_packed: malformed basis");
+    if (!out && molints_npacked(nbf) > 0) return fail(ctx, MOLINTS_ERR_INVALID, "eri_packed: null output");
+    molints_plan *p = nullptr;
+    int rc = molints_plan_create(ctx, b, opts, &p);
+    if (rc) return rc;
+    if (p->npacked == 0) {
+        if (stats) rc = molints_plan_stats(p, stats);
+        molints_plan_destroy(p);
+        return rc;
+    }
+    double *dout = out;
+    if (!out_is_device) {
+        if (ctx->out_cache_len < p->npacked) {
+            if (ctx->out_cache) {
+                cudaFree(ctx->out_cache);
+                ctx->held -= ctx->out_cache_len * 8;
+                ctx->out_cache = nullptr;
+                ctx->out_cache_len = 0;
+            }
+            rc = dev_alloc(ctx, &ctx->out_cache, (size_t)p->npacked, nullptr);
+            if (rc) { molints_plan_destroy(p); return rc; }
+            ctx->out_cache_len = p->npacked;
+        }
+        dout = ctx->out_cache;
+    }
+    rc = molints_plan_execute(p, dout);
+    if (!rc && !out_is_device && p->npacked > 0) {
+        cudaError_t e = cudaMemcpyAsync(out, dout, p->npacked * sizeof(double), cudaMemcpyDeviceToHost,
+                                        ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "eri_packed D2H");
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "eri_packed sync");
+    }
+    if (!rc && stats) rc = molints_plan_stats(p, stats);
+    molints_plan_destroy(p);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,273 @@
+"""Python host side of libmolints_cuda.so (ctypes over the C ABI of include/molints.h).
+
+The public calls mirror the reference's drivers (MolecularIntegrals.jl):
+
+    all_twoe_ints(shells)        ~ all_twoe_ints(bfs, ERI=coulomb)   src/ERI.jl:104-112
+    all_twoe_ints_chrr(shells)   ~ all_twoe_ints_chrr(bfs)           src/HGP.jl:22-34
+
+Both return the packed vector of unique normalised integrals in iindex order
+(src/Utils.jl:14-19), 0-based.  ``Engine`` exposes the context/plan API for callers that
+keep inputs and outputs on the device.  There is no CPU fallback: if the library is
+missing or no CUDA device is present, these calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libmolints_cuda.so"
+
+FP64, MIXED = 0, 1
+BOYS_REFERENCE, BOYS_EXACT = 0, 1
+METHOD_AUTO, METHOD_HGP = 0, 1
+LMAX = 2
+
+_STATUS = {0: "OK", -1: "invalid argument", -2: "unsupported", -3: "HBM budget exceeded",
+           -4: "CUDA error", -5: "timeout", -6: "out of host memory"}
+
+EXPORTED_SYMBOLS = [
+    "molints_abi_version", "molints_default_options", "molints_nbf", "molints_npacked",
+    "molints_create", "molints_destroy", "molints_last_error", "molints_set_stream",
+    "molints_eri_packed", "molints_plan_create", "molints_plan_execute", "molints_plan_stats",
+    "molints_plan_destroy", "molints_plan_schwarz", "molints_boys_eval",
+    "molints_plan_set_profiling", "molints_plan_launch_times",
+]
+
+
+class MolintsError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Basis(ctypes.Structure):
+    _fields_ = [("nshell", ctypes.c_int32), ("xyz", ctypes.c_void_p), ("L", ctypes.c_void_p),
+                ("nprim", ctypes.c_void_p), ("prim_off", ctypes.c_void_p),
+                ("expn", ctypes.c_void_p), ("coef", ctypes.c_void_p)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("boys", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("fp32_cutoff", ctypes.c_double), ("screen_cutoff", ctypes.c_double)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("n_eri", ctypes.c_int64), ("n_shell_quartets", ctypes.c_int64),
+                ("n_prim_quartets", ctypes.c_int64), ("n_fp32_quartets", ctypes.c_int64),
+                ("n_screened", ctypes.c_int64), ("n_kernel_launches", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("device_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_lib = None
+
+
+def load_library(path: Path | str | None = None):
+    """Load libmolints_cuda.so (built in-tree by build.py); raise if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: run molecularintegrals.jl_b200/build.py")
+    L = ctypes.CDLL(str(p))
+    P, I32, I64, D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    sig = {
+        "molints_abi_version": (ctypes.c_int, []),
+        "molints_default_options": (None, [P]),
+        "molints_nbf": (I64, [P]),
+        "molints_npacked": (I64, [I64]),
+        "molints_create": (ctypes.c_int, [P, ctypes.c_int, I64, ctypes.c_uint32]),
+        "molints_destroy": (ctypes.c_int, [P]),
+        "molints_last_error": (ctypes.c_char_p, [P]),
+        "molints_set_stream": (ctypes.c_int, [P, P]),
+        "molints_eri_packed": (ctypes.c_int, [P, P, P, P, ctypes.c_int, P]),
+        "molints_plan_create": (ctypes.c_int, [P, P, P, P]),
+        "molints_plan_execute": (ctypes.c_int, [P, P]),
+        "molints_plan_stats": (ctypes.c_int, [P, P]),
+        "molints_plan_destroy": (ctypes.c_int, [P]),
+        "molints_plan_schwarz": (ctypes.c_int, [P, P]),
+        "molints_boys_eval": (ctypes.c_int, [P, I32, I32, P, I64, P]),
+        "molints_plan_set_profiling": (ctypes.c_int, [P, ctypes.c_int]),
+        "molints_plan_launch_times": (ctypes.c_int, [P, P, P, ctypes.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class _BasisArrays:
+    """Keeps the contiguous arrays a molints_basis points into alive."""
+
+    def __init__(self, shells):
+        self.xyz = np.ascontiguousarray(shells.xyz, dtype=np.float64).reshape(-1)
+        self.L = np.ascontiguousarray(shells.L, dtype=np.int32)
+        self.nprim = np.ascontiguousarray(shells.nprim, dtype=np.int32)
+        self.prim_off = np.ascontiguousarray(shells.prim_off, dtype=np.int32)
+        self.expn = np.ascontiguousarray(shells.expn, dtype=np.float64)
+        self.coef = np.ascontiguousarray(shells.coef, dtype=np.float64)
+        self.c = Basis(len(self.L), _ptr(self.xyz), _ptr(self.L), _ptr(self.nprim),
+                       _ptr(self.prim_off), _ptr(self.expn), _ptr(self.coef))
+
+
+def make_options(precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0, screen_cutoff=0.0,
+                 method=METHOD_AUTO) -> Options:
+    return Options(method, precision, boys, 0, float(fp32_cutoff), float(screen_cutoff))
+
+
+class Plan:
+    """A basis resident on the device; ``execute`` runs the whole device path."""
+
+    def __init__(self, engine: "Engine", shells, opts: Options):
+        self.engine = engine
+        self._arrs = _BasisArrays(shells)
+        self.nbf = shells.nbf
+        self.npacked = shells.npacked
+        self.nshell = shells.nshell
+        h = ctypes.c_void_p()
+        engine._check(engine.lib.molints_plan_create(engine.ctx, ctypes.byref(self._arrs.c),
+                                                     ctypes.byref(opts), ctypes.byref(h)))
+        self.h = h
+
+    def execute(self, out_device_ptr: int) -> None:
+        """Queue the device path on the engine's stream, writing npacked doubles."""
+        self.engine._check(self.engine.lib.molints_plan_execute(self.h, ctypes.c_void_p(out_device_ptr)))
+
+    def stats(self) -> dict:
+        st = Stats()
+        self.engine._check(self.engine.lib.molints_plan_stats(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def set_profiling(self, enable: bool = True) -> None:
+        self.engine._check(self.engine.lib.molints_plan_set_profiling(self.h, int(enable)))
+
+    def launch_times(self, cap: int = 256):
+        """[(kernel name, ms)] of the last execute (profiling must be on)."""
+        names = (ctypes.c_char_p * cap)()
+        ms = (ctypes.c_float * cap)()
+        n = self.engine.lib.molints_plan_launch_times(self.h, names, ms, cap)
+        if n < 0:
+            self.engine._check(n)
+        return [(names[k].decode(), float(ms[k])) for k in range(min(n, cap))]
+
+    def schwarz(self) -> np.ndarray:
+        out = np.zeros(self.nshell * (self.nshell + 1) // 2)
+        self.engine._check(self.engine.lib.molints_plan_schwarz(self.h, _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.engine.lib.molints_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine:
+    """One molints context on one CUDA device."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.molints_create(ctypes.byref(h), device, int(hbm_budget_bytes), 0)
+        if rc != 0:
+            raise MolintsError(rc, f"molints_create on device {device}")
+        self.ctx = h
+        self.device = device
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self.lib.molints_last_error(self.ctx)
+            raise MolintsError(rc, msg.decode() if msg else "")
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self.lib.molints_set_stream(self.ctx, ctypes.c_void_p(stream_handle or 0)))
+
+    def eri_packed(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
+                   screen_cutoff=0.0, out: np.ndarray | None = None, with_stats=False):
+        """The packed iindex vector of all unique integrals, into a host array."""
+        arrs = _BasisArrays(shells)
+        if out is None:
+            out = np.empty(shells.npacked, dtype=np.float64)
+        if shells.npacked == 0:
+            st = Stats()
+            self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), None, None, 0,
+                                                    ctypes.byref(st)))
+            return (out, st.as_dict()) if with_stats else out
+        if out.dtype != np.float64 or out.size != shells.npacked or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of npacked elements")
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff)
+        st = Stats()
+        self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
+                                                _ptr(out), 0, ctypes.byref(st)))
+        return (out, st.as_dict()) if with_stats else out
+
+    def eri_packed_device(self, shells, out_device_ptr: int, precision=FP64, boys=BOYS_REFERENCE,
+                          fp32_cutoff=0.0, screen_cutoff=0.0):
+        arrs = _BasisArrays(shells)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff)
+        st = Stats()
+        self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
+                                                ctypes.c_void_p(out_device_ptr), 1, ctypes.byref(st)))
+        return st.as_dict()
+
+    def plan(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
+             screen_cutoff=0.0) -> Plan:
+        return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff))
+
+    def boys(self, mmax: int, T, mode=BOYS_REFERENCE) -> np.ndarray:
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        out = np.empty((T.size, mmax))
+        self._check(self.lib.molints_boys_eval(self.ctx, mode, mmax, _ptr(T), T.size, _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.molints_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_engine: Engine | None = None
+
+
+def default_engine() -> Engine:
+    global _default_engine
+    if _default_engine is None:
+        _default_engine = Engine(0)
+    return _default_engine
+
+
+def all_twoe_ints(shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
+                  screen_cutoff=0.0) -> np.ndarray:
+    """Drop-in for all_twoe_ints(bfs) (src/ERI.jl:104-112): packed normalised ERIs."""
+    return default_engine().eri_packed(shells, precision, boys, fp32_cutoff, screen_cutoff)
+
+
+def all_twoe_ints_chrr(shells) -> np.ndarray:
+    """Drop-in for all_twoe_ints_chrr(bfs) (src/HGP.jl:22-34), with its layout and
+    normalisation defects fixed: the same vector as all_twoe_ints."""
+    return default_engine().eri_packed(shells)

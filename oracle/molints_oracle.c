@@ -401,24 +401,46 @@ static void shell_quartet(const oracle_basis *b, int sa, int sb, int sc, int sd,
  * quartet (I>=J, K>=L, pair(IJ)>=pair(KL)) is computed once and scattered to the 0-based
  * iindex positions.  nthreads > 1 uses OpenMP with a dynamic schedule, the analogue of
  * the reference's Threads.@threads over shell quartets. */
+static int64_t eri_packed_hgp_impl(int nshell, const double *xyz, const int *L, const int *nprim,
+                                   const int *prim_off, const double *expn, const double *coef,
+                                   double *out, int nthreads, int64_t stride);
+
 int oracle_eri_packed_hgp(int nshell, const double *xyz, const int *L, const int *nprim,
                           const int *prim_off, const double *expn, const double *coef,
                           double *out, int nthreads) {
+    int64_t r = eri_packed_hgp_impl(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads, 1);
+    return r < 0 ? (int)r : 0;
+}
+
+/* The same driver over every stride-th shell quartet only (a bounded CPU-baseline sample);
+ * returns the number of integrals written, or -1. */
+int64_t oracle_eri_packed_hgp_sample(int nshell, const double *xyz, const int *L,
+                                     const int *nprim, const int *prim_off, const double *expn,
+                                     const double *coef, double *out, int nthreads,
+                                     int64_t stride) {
+    return eri_packed_hgp_impl(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads,
+                               stride < 1 ? 1 : stride);
+}
+
+static int64_t eri_packed_hgp_impl(int nshell, const double *xyz, const int *L, const int *nprim,
+                                   const int *prim_off, const double *expn, const double *coef,
+                                   double *out, int nthreads, int64_t stride) {
     oracle_init();
     oracle_basis b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0};
     for (int s = 0; s < nshell; ++s)
-        if (L[s] < 0 || L[s] > 4 || nprim[s] < 1) return -1;
+        if (L[s] < 0 || L[s] > 3 || nprim[s] < 1) return -1;
     basis_prepare(&b);
     int64_t npair = (int64_t)nshell * (nshell + 1) / 2;
     int64_t nquart = npair * (npair + 1) / 2;
     int *pi = (int *)malloc(sizeof(int) * npair), *pj = (int *)malloc(sizeof(int) * npair);
     for (int i = 0, p = 0; i < nshell; ++i)
         for (int j = 0; j <= i; ++j, ++p) { pi[p] = i; pj[p] = j; }
-#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+    int64_t written = 0;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : written)
     {
     double *buf = (double *)malloc(sizeof(double) * 15 * 15 * 15 * 15);
 #pragma omp for schedule(dynamic, 64)
-    for (int64_t q = 0; q < nquart; ++q) {
+    for (int64_t q = 0; q < nquart; q += stride) {
         int64_t p1 = (int64_t)((sqrt(8.0 * (double)q + 1.0) - 1.0) / 2.0);
         while (tri64(p1) > q) --p1;
         while (tri64(p1 + 1) <= q) ++p1;
@@ -438,13 +460,14 @@ int oracle_eri_packed_hgp(int nshell, const double *xyz, const int *L, const int
                         int64_t ij = tri64(i) + j, kl = tri64(k) + l;
                         if (p1 == p2 && ij < kl) continue;
                         out[oracle_iindex(i, j, k, l)] = buf[x];
+                        ++written;
                     }
     }
     free(buf);
     }
     free(pi); free(pj);
     basis_release(&b);
-    return 0;
+    return written;
 }
 
 /* One contracted, normalised shell quartet (ab|cd), out[ma][mb][mc][md]. */

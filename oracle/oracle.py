@@ -76,6 +76,8 @@ def lib():
         L.oracle_shell_quartet.argtypes = [_I, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]
         L.oracle_coulomb_prim.restype = _D
         L.oracle_coulomb_prim.argtypes = ([_D, _D, _D, _D, _I, _I, _I] * 4)
+        L.oracle_eri_packed_hgp_sample.restype = ctypes.c_int64
+        L.oracle_eri_packed_hgp_sample.argtypes = drv + [ctypes.c_int64]
         L.oracle_set_boys_tmax.argtypes = [_D]
         L.oracle_get_boys_tmax.restype = _D
         L.oracle_init()
@@ -189,6 +191,18 @@ def eri_packed_hgp(shells, nthreads: int = 1) -> np.ndarray:
     if rc != 0:
         raise ValueError("oracle_eri_packed_hgp: unsupported shell")
     return out
+
+
+def eri_packed_hgp_sample(shells, nthreads: int, stride: int, out: np.ndarray | None = None) -> int:
+    """The HGP driver over every stride-th shell quartet; returns the integrals written."""
+    arrs = _shell_arrays(shells)
+    if out is None:
+        out = np.zeros(shells.npacked)
+    n = lib().oracle_eri_packed_hgp_sample(len(arrs[1]), *[_ptr(a) for a in arrs], _ptr(out),
+                                           nthreads, stride)
+    if n < 0:
+        raise ValueError("oracle_eri_packed_hgp_sample: unsupported shell")
+    return int(n)
 
 
 def eri_packed_huzinaga(shells, nthreads: int = 1) -> np.ndarray:

@@ -1,0 +1,215 @@
+"""GPU parity: libmolints_cuda.so (through its C ABI) against the CPU oracle.
+
+Tolerances (max abs, Eh): FP64 path 1e-12 against the restated reference HGP with the same
+Boys branch; mixed precision 1e-9 against the FP64 oracle."""
+import numpy as np
+import pytest
+
+import molints_b200 as mi
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+TOL_MIXED = 1e-9
+
+
+@pytest.fixture(scope="module")
+def eng():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from molints_b200 import engine
+    e = engine.Engine(0)
+    yield e
+    e.close()
+
+
+def _rand_basis(seed, lmax, natom=3, kmax=3, lo=0.15, hi=20.0):
+    rng = np.random.default_rng(seed)
+    lst = []
+    for _ in range(natom):
+        xyz = rng.uniform(-2.0, 2.0, 3)
+        for l in range(lmax + 1):
+            for _ in range(int(rng.integers(1, 3))):
+                lst.append((xyz, l, mi.basis._random_shell(rng, l, int(rng.integers(1, kmax + 1)), lo, hi)))
+    return mi.Shells.from_list(lst, f"rand{seed}")
+
+
+def test_boys_table_against_oracle(eng, oracle):
+    from molints_b200 import engine
+    T = np.concatenate([np.linspace(0, 45, 1441), [1e-20, 1e-12, 29.999999, 30.0, 39.9999, 40.0, 60, 200]])
+    for mmax in (1, 3, 9, 13):
+        got = eng.boys(mmax, T, engine.BOYS_EXACT)
+        for t, row in zip(T[::7], got[::7]):
+            for m in range(mmax):
+                ex = oracle.boys_mpmath(m, t) if t < 40 else oracle.boys(m, t)
+                assert abs(row[m] - ex) <= 4e-15 * max(ex, 1e-300) + 1e-300, (mmax, m, t)
+        ref = eng.boys(mmax, T, engine.BOYS_REFERENCE)
+        for t, row in zip(T, ref):
+            np.testing.assert_allclose(row, oracle.farray(mmax, t), rtol=5e-15, atol=0)
+
+
+def test_h2_sto3g_golden(eng, golden, oracle):
+    ints = eng.eri_packed(mi.build_basis(mi.h2()))
+    idx = {"llll": (0, 0, 0, 0), "rrrr": (1, 1, 1, 1), "llrr": (0, 0, 1, 1),
+           "lllr": (0, 0, 0, 1), "lrlr": (0, 1, 0, 1)}
+    for key, case in golden["h2_sto3g_coulomb"].items():
+        assert ints[oracle.iindex(*idx[key])] == pytest.approx(case["value"], rel=1.5e-8)
+
+
+def test_ethane_sto3g_matches_reference_hgp(eng, oracle):
+    sh = mi.config0()
+    got = eng.eri_packed(sh)
+    ref = oracle.eri_packed_hgp(sh, nthreads=8)
+    huz = oracle.eri_packed_huzinaga(sh, nthreads=8)
+    assert got.shape == (9316,)
+    assert np.max(np.abs(got - ref)) < TOL_FP64
+    assert np.max(np.abs(got - huz)) < TOL_FP64
+
+
+def test_ethane_polarised_all_classes(eng, oracle):
+    """Config 2 (l<=2, 22 class pairs up to (dd|dd)), both Boys modes."""
+    from molints_b200 import engine
+    sh = mi.config2()
+    got = eng.eri_packed(sh)
+    ref = oracle.eri_packed_hgp(sh, nthreads=8)
+    assert np.max(np.abs(got - ref)) < TOL_FP64
+    got_x = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
+    with oracle.exact_boys():
+        ref_x = oracle.eri_packed_hgp(sh, nthreads=8)
+    assert np.max(np.abs(got_x - ref_x)) < TOL_FP64
+
+
+@pytest.mark.parametrize("seed,lmax", [(101, 0), (102, 1), (103, 2), (104, 2)])
+def test_random_bases_against_huzinaga(eng, oracle, seed, lmax):
+    from molints_b200 import engine
+    sh = _rand_basis(seed, lmax)
+    got = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
+    huz = oracle.eri_packed_huzinaga(sh, nthreads=8)
+    assert np.max(np.abs(got - huz)) < TOL_FP64 * max(1.0, np.max(np.abs(huz)))
+
+
+def test_every_slot_written(eng):
+    """A NaN-filled device output has no NaN left after one execute."""
+    import torch
+    sh = mi.config2()
+    out = torch.full((sh.npacked,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    eng.eri_packed_device(sh, out.data_ptr())
+    assert not torch.isnan(out).any().item()
+
+
+def _sample_quartets(sh, nsample, seed):
+    """Random function quartets of a basis -> (packed index, shell quartet, components)."""
+    rng = np.random.default_rng(seed)
+    off = sh.fn_offsets()
+    fsh = np.searchsorted(off, np.arange(sh.nbf), side="right") - 1
+    out = []
+    for _ in range(nsample):
+        f = rng.integers(0, sh.nbf, 4)
+        i, j, k, l = (int(x) for x in f)
+        if i < j:
+            i, j = j, i
+        if k < l:
+            k, l = l, k
+        ij, kl = i * (i + 1) // 2 + j, k * (k + 1) // 2 + l
+        if ij < kl:
+            i, j, k, l = k, l, i, j
+            ij, kl = kl, ij
+        out.append((ij * (ij + 1) // 2 + kl, [(int(fsh[x]), int(x - off[fsh[x]])) for x in (i, j, k, l)]))
+    return out
+
+
+def test_split_valence_24_sampled(eng, oracle):
+    """Config 1 at full size (14.9 M integrals): 400 sampled function quartets against the
+    oracle's per-quartet HGP, plus the Schwarz inequality over the whole vector."""
+    sh = mi.config1()
+    got = eng.eri_packed(sh)
+    assert got.shape == (14908530,)
+    for idx, fq in _sample_quartets(sh, 400, 7):
+        shells = [s for s, _ in fq]
+        q = oracle.shell_quartet(sh, *shells)
+        ref = q[tuple(m for _, m in fq)]
+        assert abs(got[idx] - ref) < TOL_FP64, (idx, fq)
+    n = sh.nbf
+    npair = n * (n + 1) // 2
+    diag = got[np.arange(npair) * (np.arange(npair) + 1) // 2 + np.arange(npair)]
+    assert np.all(diag >= -1e-14)
+    ij = np.repeat(np.arange(npair), np.arange(1, npair + 1))
+    kl = np.arange(len(got)) - ij * (ij + 1) // 2
+    bound = np.sqrt(np.abs(diag[ij] * diag[kl]))
+    assert np.all(np.abs(got) <= bound * (1 + 1e-10) + 1e-14)
+
+
+@pytest.mark.parametrize("cutoff", [1e-4, 1e-3])
+def test_mixed_precision_error_bound(eng, oracle, cutoff):
+    from molints_b200 import engine
+    sh = mi.config2()
+    ref = eng.eri_packed(sh)
+    got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cutoff, with_stats=True)
+    assert st["n_fp32_quartets"] > 0
+    assert np.max(np.abs(got - ref)) < TOL_MIXED
+
+
+def test_screening_writes_zeros(eng):
+    sh = mi.config2()
+    full = eng.eri_packed(sh)
+    scr, st = eng.eri_packed(sh, screen_cutoff=1e-8, with_stats=True)
+    assert st["n_screened"] > 0
+    assert np.max(np.abs(scr - full)) < 1e-8
+
+
+def test_deterministic(eng):
+    sh = mi.config2()
+    a = eng.eri_packed(sh)
+    b = eng.eri_packed(sh)
+    assert np.array_equal(a, b)
+
+
+def test_plan_execute_twice_on_torch_stream(eng, oracle):
+    import torch
+    sh = mi.config0()
+    eng.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        plan = eng.plan(sh)
+        out = torch.empty(sh.npacked, dtype=torch.float64, device="cuda")
+        plan.execute(out.data_ptr())
+        first = out.cpu().numpy().copy()
+        out.zero_()
+        plan.execute(out.data_ptr())
+        second = out.cpu().numpy()
+        assert np.array_equal(first, second)
+        q = plan.schwarz()
+        assert q.shape == (sh.nshell * (sh.nshell + 1) // 2,) and np.all(q > 0)
+        plan.close()
+    finally:
+        eng.set_stream(None)
+    assert np.max(np.abs(first - oracle.eri_packed_hgp(sh))) < TOL_FP64
+
+
+def test_edge_cases(eng):
+    from molints_b200 import engine
+    one = mi.Shells.from_list([((0.0, 0.0, 0.0), 0, [(1.0, 1.0)])])
+    v = eng.eri_packed(one)
+    assert v.shape == (1,) and v[0] == pytest.approx(2 / np.sqrt(np.pi) * np.sqrt(2.0 / 2), rel=1e-14)
+    empty = mi.Shells.from_list([])
+    assert eng.eri_packed(empty).shape == (0,)
+    f_shell = mi.Shells.from_list([((0.0, 0.0, 0.0), 3, [(1.0, 1.0)])])
+    with pytest.raises(engine.MolintsError) as e:
+        eng.eri_packed(f_shell)
+    assert e.value.status == -2
+    bad = mi.Shells.from_list([((0.0, 0.0, 0.0), 0, [(-1.0, 1.0)])])
+    with pytest.raises(engine.MolintsError) as e:
+        eng.eri_packed(bad)
+    assert e.value.status == -1
+
+
+def test_budget_refusal():
+    from molints_b200 import engine
+    e = engine.Engine(0, hbm_budget_bytes=1 << 20)
+    try:
+        with pytest.raises(engine.MolintsError) as err:
+            e.eri_packed(mi.config1())
+        assert err.value.status == -3
+    finally:
+        e.close()
