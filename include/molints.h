@@ -106,7 +106,8 @@ int molints_destroy(molints_ctx *ctx);
 const char *molints_last_error(const molints_ctx *ctx);
 
 /* Set the CUDA stream (a cudaStream_t passed as void*) the context launches on.
- * NULL selects the context's own stream. */
+ * NULL selects the context's own (non-blocking) stream; to launch on the legacy default
+ * stream pass cudaStreamLegacy ((void*)0x1). */
 int molints_set_stream(molints_ctx *ctx, void *stream);
 
 /* One call, the drop-in for all_twoe_ints / all_twoe_ints_chrr: computes every unique

@@ -129,8 +129,8 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
                                    const int4 *__restrict__ info, const double *__restrict__ xyz,
                                    const int *__restrict__ poff, const int *__restrict__ nprim,
                                    const double *__restrict__ expn,
-                                   const double *__restrict__ ncoef, PrimPair *__restrict__ pp,
-                                   double4 *__restrict__ geo) {
+                                   const double *__restrict__ ncoef, double c0,
+                                   PrimPair *__restrict__ pp, double4 *__restrict__ geo) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npair) return;
     const int2 ab = pair_ab[p];
@@ -141,7 +141,6 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
     const double rab2 = ABx * ABx + ABy * ABy + ABz * ABz;
     const int ka = nprim[ab.x], kb = nprim[ab.y];
     const int pa0 = poff[ab.x], pb0 = poff[ab.y];
-    const double c0 = 3.5546813524369302;  // sqrt(2) pi^(5/4)
     int k = in.x;
     for (int ia = 0; ia < ka; ++ia) {
         const double a = expn[pa0 + ia], ca = ncoef[pa0 + ia];
@@ -263,6 +262,7 @@ const char *molints_last_error(const molints_ctx *ctx) { return ctx ? ctx->err.c
 
 int molints_set_stream(molints_ctx *ctx, void *stream) {
     if (!ctx) return MOLINTS_ERR_INVALID;
+    // NULL selects the context's own stream; the legacy default stream is cudaStreamLegacy.
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
     return MOLINTS_OK;
 }
@@ -476,7 +476,7 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         if (int rc = mark(launches, "build_pairs", 0)) return rc;
         build_pairs_kernel<<<(p->npair + 127) / 128, 128, 0, s>>>(
             p->npair, p->pair_ab, p->info, p->sh_xyz, p->sh_poff, p->sh_nprim, p->expn, p->ncoef,
-            p->pp, p->geo);
+            std::sqrt(2.0) * std::pow(M_PI, 1.25), p->pp, p->geo);
         if (int rc = mark(launches, "build_pairs", 1)) return rc;
         ++launches;
     }

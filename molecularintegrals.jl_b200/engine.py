@@ -199,7 +199,15 @@ class Engine:
             raise MolintsError(rc, msg.decode() if msg else "")
 
     def set_stream(self, stream_handle: int | None):
-        self._check(self.lib.molints_set_stream(self.ctx, ctypes.c_void_p(stream_handle or 0)))
+        """Launch on a cudaStream_t handle (e.g. torch's ``Stream.cuda_stream``); handle 0, the
+        legacy default stream, is passed as cudaStreamLegacy; None selects the own stream."""
+        if stream_handle is None:
+            h = None
+        elif stream_handle == 0:
+            h = ctypes.c_void_p(1)  # cudaStreamLegacy
+        else:
+            h = ctypes.c_void_p(stream_handle)
+        self._check(self.lib.molints_set_stream(self.ctx, h))
 
     def eri_packed(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
                    screen_cutoff=0.0, out: np.ndarray | None = None, with_stats=False):
