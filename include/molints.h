@@ -69,9 +69,12 @@ typedef struct molints_options {
     int32_t precision;       /* enum molints_precision */
     int32_t boys;            /* enum molints_boys */
     int32_t reserved;
-    double fp32_cutoff;      /* MIXED: quartets whose Schwarz bound Q_ab*Q_cd is below this
-                                run the VRR in FP32 (FP64 Boys, prefactors, accumulation) */
-    double screen_cutoff;    /* quartets with Q_ab*Q_cd below this are written as 0 */
+    /* Both cutoffs compare against B = Qabs_ab * Qabs_cd, where Qabs_ab is the sum over the
+     * pair's primitive pairs i of sqrt(max |(a_i b_i|a_i b_i)|).  B bounds the sum of the
+     * magnitudes of all primitive contributions to (ab|cd), not only |(ab|cd)|. */
+    double fp32_cutoff;      /* MIXED: quartets with B below this run the VRR in FP32
+                                (FP64 Boys, prefactors, contraction and HRR) */
+    double screen_cutoff;    /* quartets with B below this are written as 0 */
 } molints_options;
 
 typedef struct molints_stats {
@@ -129,8 +132,9 @@ int molints_plan_execute(molints_plan *plan, double *out_device);
 int molints_plan_stats(const molints_plan *plan, molints_stats *stats);
 int molints_plan_destroy(molints_plan *plan);
 
-/* Schwarz bounds Q_ab = sqrt(max |(ab|ab)|) of the plan's shell pairs after an execute,
- * in the reference's pair order (shell i >= shell j, row-major): out[nshell*(nshell+1)/2]. */
+/* Contracted Schwarz bounds Q_ab = sqrt(max |(ab|ab)|) of the plan's shell pairs (computed
+ * on demand on the context's stream; the plan must have been executed once), in the
+ * reference's pair order (shell i >= shell j, row-major): out[nshell*(nshell+1)/2]. */
 int molints_plan_schwarz(molints_plan *plan, double *out_host);
 
 /* Per-launch device times.  After molints_plan_set_profiling(plan, 1), every execute records

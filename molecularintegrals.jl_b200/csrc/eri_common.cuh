@@ -5,7 +5,7 @@
 //     contraction length; structure of arrays:
 //       info[p] = {first primitive pair, number of primitive pairs, first function of A,
 //                  first function of B}                      (int4, 16 B)
-//       geo[p]  = {A-B (x,y,z), Schwarz bound Q_p}          (double4, 32 B)
+//       geo[p]  = {A-B (x,y,z), primitive Schwarz sum Qabs_p} (double4, 32 B)
 //   * primitive pairs, 80 B each (5 x 16 B vector loads): PrimPair below;
 //   * the Boys table (T = 0..40 step 1/16, F_0..F_22 and e^-T per row);
 //   * the packed output vector, 0-based iindex order (src/Utils.jl:14-19).
@@ -39,7 +39,7 @@ static_assert(sizeof(PrimPair) == 80, "PrimPair is 5 x 16 bytes");
 
 struct PairTab {
     const int4 *info;
-    const double4 *geo;
+    const double4 *geo;   // w: primitive Schwarz sum Qabs (0 when the plan needs no bound)
     const PrimPair *pp;
 };
 
@@ -59,8 +59,8 @@ struct EriLaunch {
     int tri;                  // 1: same class on both sides, only q <= p
     int pad;
     long long nquart;         // nbra * nket or nbra * (nbra + 1) / 2
-    double screen_cut;        // Q_p Q_q below this: written as 0
-    double fp32_cut;          // Q_p Q_q below this (MIXED kernels): FP32 VRR
+    double screen_cut;        // Qabs_p Qabs_q below this: written as 0
+    double fp32_cut;          // Qabs_p Qabs_q below this (MIXED kernels): FP32 VRR
 };
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {
@@ -85,9 +85,20 @@ __device__ __forceinline__ void boys_fm(double T, const BoysTab &bt, double *F) 
         const int n = __double2int_rn(T * kBoysStepInv);
         const double d = n * kBoysStep - T;
         const double *__restrict__ row = bt.tab + n * kBoysCols;
-        double f = __ldg(row + M + kBoysTaylor - 1);
+        // F_M..F_M+7 by 16-byte loads from the even column at or below M (rows are 192 B)
+        constexpr int M0 = M & ~1;
+        constexpr int NV = (M - M0 + kBoysTaylor + 1) / 2;
+        double v[2 * NV];
+        const double2 *__restrict__ r2 = reinterpret_cast<const double2 *>(row + M0);
 #pragma unroll
-        for (int k = kBoysTaylor - 1; k >= 1; --k) f = fma(f, d * (1.0 / k), __ldg(row + M + k - 1));
+        for (int k = 0; k < NV; ++k) {
+            const double2 x = __ldg(r2 + k);
+            v[2 * k] = x.x;
+            v[2 * k + 1] = x.y;
+        }
+        double f = v[M - M0 + kBoysTaylor - 1];
+#pragma unroll
+        for (int k = kBoysTaylor - 1; k >= 1; --k) f = fma(f, d * (1.0 / k), v[M - M0 + k - 1]);
         F[M] = f;
         if (M > 0) {
             double ed = 1.0;

@@ -5,19 +5,23 @@
 namespace molints {
 
 // Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[108]
-// (ma, mb, mc, md row-major).  VT is the VRR arithmetic type (double, or float for MIXED).
+// (ma, mb, mc, md row-major), summed over the bra primitive pairs [i0, i1) and the ket
+// primitive pairs [j0, j1) of the two shell pairs.  VT is the VRR arithmetic type (double,
+// or float for MIXED).  The ket loop is outside: a warp shares its bra pair, so the inner
+// bra loads are warp-uniform broadcasts and each lane's ket record is loaded once.
 template <typename VT>
 __device__ __forceinline__ void quartet_dpds(const PairTab &P, const BoysTab &B, int p, int q,
+                                              int i0, int i1, int j0, int j1,
                                               double *__restrict__ res) {
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
     double acc[96];
 #pragma unroll
     for (int x = 0; x < 96; ++x) acc[x] = 0.0;
-    for (int i = 0; i < ib_.y; ++i) {
-        const PrimPair bra = load_pp(P.pp, ib_.x + i);
-        for (int j = 0; j < ik_.y; ++j) {
-            const PrimPair ket = load_pp(P.pp, ik_.x + j);
+    for (int j = j0; j < j1; ++j) {
+        const PrimPair ket = load_pp(P.pp, ik_.x + j);
+        for (int i = i0; i < i1; ++i) {
+            const PrimPair bra = load_pp(P.pp, ib_.x + i);
             const double r = rsqrt(bra.zeta + ket.zeta);
             const double r2 = r * r;
             const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
@@ -889,10 +893,10 @@ __global__ void __launch_bounds__(128) eri_kernel_dpds(const EriLaunch L) {
     if (bound < L.screen_cut) {
 #pragma unroll
         for (int x = 0; x < 108; ++x) res[x] = 0.0;
-    } else if (MIXED && bound < L.fp32_cut) {
-        quartet_dpds<float>(L.pairs, L.boys, p, q, res);
     } else {
-        quartet_dpds<double>(L.pairs, L.boys, p, q, res);
+        const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
+        if (MIXED && bound < L.fp32_cut) quartet_dpds<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+        else quartet_dpds<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
     }
     store_dpds(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
 }

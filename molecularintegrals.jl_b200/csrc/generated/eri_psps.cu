@@ -5,19 +5,23 @@
 namespace molints {
 
 // Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[9]
-// (ma, mb, mc, md row-major).  VT is the VRR arithmetic type (double, or float for MIXED).
+// (ma, mb, mc, md row-major), summed over the bra primitive pairs [i0, i1) and the ket
+// primitive pairs [j0, j1) of the two shell pairs.  VT is the VRR arithmetic type (double,
+// or float for MIXED).  The ket loop is outside: a warp shares its bra pair, so the inner
+// bra loads are warp-uniform broadcasts and each lane's ket record is loaded once.
 template <typename VT>
 __device__ __forceinline__ void quartet_psps(const PairTab &P, const BoysTab &B, int p, int q,
+                                              int i0, int i1, int j0, int j1,
                                               double *__restrict__ res) {
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
     double acc[9];
 #pragma unroll
     for (int x = 0; x < 9; ++x) acc[x] = 0.0;
-    for (int i = 0; i < ib_.y; ++i) {
-        const PrimPair bra = load_pp(P.pp, ib_.x + i);
-        for (int j = 0; j < ik_.y; ++j) {
-            const PrimPair ket = load_pp(P.pp, ik_.x + j);
+    for (int j = j0; j < j1; ++j) {
+        const PrimPair ket = load_pp(P.pp, ik_.x + j);
+        for (int i = i0; i < i1; ++i) {
+            const PrimPair bra = load_pp(P.pp, ib_.x + i);
             const double r = rsqrt(bra.zeta + ket.zeta);
             const double r2 = r * r;
             const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
@@ -122,10 +126,10 @@ __global__ void __launch_bounds__(128) eri_kernel_psps(const EriLaunch L) {
     if (bound < L.screen_cut) {
 #pragma unroll
         for (int x = 0; x < 9; ++x) res[x] = 0.0;
-    } else if (MIXED && bound < L.fp32_cut) {
-        quartet_psps<float>(L.pairs, L.boys, p, q, res);
     } else {
-        quartet_psps<double>(L.pairs, L.boys, p, q, res);
+        const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
+        if (MIXED && bound < L.fp32_cut) quartet_psps<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+        else quartet_psps<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
     }
     store_psps(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
 }
@@ -137,25 +141,44 @@ void launch_eri_psps(const EriLaunch &L, int mixed, cudaStream_t s) {
     else eri_kernel_psps<0><<<(unsigned)blocks, 128, 0, s>>>(L);
 }
 
-// Schwarz bound Q_p = sqrt(max over components of |(ab|ab)|) for the pairs of one class.
+// Primitive Schwarz sum of the pairs of one class:
+//   Qabs_p = sum_i sqrt(max over components |(a_i b_i | a_i b_i)|)
+// over the pair's primitive pairs i.  By the Schwarz inequality on every primitive quartet,
+// Qabs_p Qabs_q bounds sum over primitive quartets of |(a_i b_i | c_k d_k)|, hence both
+// |(ab|cd)| and the magnitude the VRR works at before the contraction cancels.
+// With full != 0 it writes the contracted bound Q_p = sqrt(max |(ab|ab)|) to qout instead.
 __global__ void __launch_bounds__(128) schwarz_kernel_psps(PairTab P, BoysTab B, int p0, int np,
-                                                          double4 *geo_rw) {
+                                                          double4 *geo_rw, double *qout, int full) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= np) return;
     const int p = p0 + t;
+    const int npp = __ldg(&P.info[p]).y;
     double res[9];
-    quartet_psps<double>(P, B, p, p, res);
-    double m = 0.0;
+    if (full) {
+        quartet_psps<double>(P, B, p, p, 0, npp, 0, npp, res);
+        double m = 0.0;
     m = fmax(m, fabs(res[0]));
     m = fmax(m, fabs(res[4]));
     m = fmax(m, fabs(res[8]));
-    geo_rw[p].w = sqrt(m);
+        qout[p] = sqrt(m);
+        return;
+    }
+    double qa = 0.0;
+    for (int i = 0; i < npp; ++i) {
+        quartet_psps<double>(P, B, p, p, i, i + 1, i, i + 1, res);
+        double m = 0.0;
+    m = fmax(m, fabs(res[0]));
+    m = fmax(m, fabs(res[4]));
+    m = fmax(m, fabs(res[8]));
+        qa += sqrt(m);
+    }
+    geo_rw[p].w = qa;
 }
 
 void launch_schwarz_psps(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw,
-                          cudaStream_t s) {
+                          double *qout, int full, cudaStream_t s) {
     if (np <= 0) return;
-    schwarz_kernel_psps<<<(np + 127) / 128, 128, 0, s>>>(P, B, p0, np, geo_rw);
+    schwarz_kernel_psps<<<(np + 127) / 128, 128, 0, s>>>(P, B, p0, np, geo_rw, qout, full);
 }
 
 }  // namespace molints

@@ -56,6 +56,7 @@ struct molints_plan {
     int4 *info = nullptr;
     double4 *geo = nullptr;
     PrimPair *pp = nullptr;
+    double *qcon = nullptr;  // contracted Schwarz bounds, filled on demand by plan_schwarz
     int64_t bytes = 0;
     int n_launches = 0;
     // per-launch profiling (molints_plan_set_profiling)
@@ -309,7 +310,7 @@ static void plan_free(molints_plan *p) {
     if (!p) return;
     for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->sh_nprim, p->pair_ab,
-                    p->info, p->geo, p->pp};
+                    p->info, p->geo, p->pp, p->qcon};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (p->ctx) p->ctx->held -= p->bytes;
@@ -482,11 +483,14 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
     }
     PairTab P{p->info, p->geo, p->pp};
     BoysTab B = boys_of(ctx, p->opts.boys);
-    for (int c = 0; c < kNumPairClasses; ++c) {
+    // The primitive Schwarz sums decide screening and FP32 quartets; a plain FP64 plan
+    // without screening uses neither and skips the pass.
+    const bool need_bounds = p->opts.precision == MOLINTS_MIXED || p->opts.screen_cutoff > 0.0;
+    for (int c = 0; need_bounds && c < kNumPairClasses; ++c) {
         const int n = p->class_start[c + 1] - p->class_start[c];
         if (n > 0) {
             if (int rc = mark(launches, kSchwarzNames[c], 0)) return rc;
-            kSchwarzLaunchers[c](P, B, p->class_start[c], n, p->geo, s);
+            kSchwarzLaunchers[c](P, B, p->class_start[c], n, p->geo, nullptr, 0, s);
             if (int rc = mark(launches, kSchwarzNames[c], 1)) return rc;
             ++launches;
         }
@@ -576,10 +580,23 @@ int molints_plan_schwarz(molints_plan *p, double *out) {
     if (!p || !out) return MOLINTS_ERR_INVALID;
     molints_ctx *ctx = p->ctx;
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
-    std::vector<double4> g(p->npair);
+    if (p->npair == 0) return MOLINTS_OK;
+    if (!p->qcon) {
+        int rc = dev_alloc(ctx, &p->qcon, (size_t)p->npair, &p->bytes);
+        if (rc) return rc;
+    }
+    PairTab P{p->info, p->geo, p->pp};
+    BoysTab B = boys_of(ctx, p->opts.boys);
+    for (int c = 0; c < kNumPairClasses; ++c) {
+        const int n = p->class_start[c + 1] - p->class_start[c];
+        if (n > 0) kSchwarzLaunchers[c](P, B, p->class_start[c], n, nullptr, p->qcon, 1, ctx->stream);
+    }
+    MI_CUDA(ctx, cudaGetLastError());
+    std::vector<double> q(p->npair);
+    MI_CUDA(ctx, cudaMemcpyAsync(q.data(), p->qcon, p->npair * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
     MI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    MI_CUDA(ctx, cudaMemcpy(g.data(), p->geo, p->npair * sizeof(double4), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < p->npair; ++k) out[p->pair_ref[k]] = g[k].w;
+    for (int k = 0; k < p->npair; ++k) out[p->pair_ref[k]] = q[k];
     return MOLINTS_OK;
 }
 

@@ -118,9 +118,38 @@ static double dfact2(int n) { /* factorial2, src/Utils.jl:5; (-1)!! = 1 */
     return r;
 }
 
+/* Gamma(a, x) e^x x^-a for x > a + 1 by the Legendre continued fraction (DLMF 8.9.2),
+ * evaluated with the modified Lentz method. */
+static long double upper_gamma_cf(long double a, long double x) {
+    const long double tiny = 1e-4000L;
+    long double b = x + 1.0L - a, c = 1.0L / tiny, d = 1.0L / b, h = d;
+    for (int i = 1; i < 10000; ++i) {
+        long double an = -i * (i - a);
+        b += 2.0L;
+        d = an * d + b;
+        if (fabsl(d) < tiny) d = tiny;
+        c = b + an / c;
+        if (fabsl(c) < tiny) c = tiny;
+        d = 1.0L / d;
+        long double del = d * c;
+        h *= del;
+        if (fabsl(del - 1.0L) < 1e-21L) break;
+    }
+    return h;
+}
+
 /* Fm(m,T), src/Boys.jl:29-34 (T < 1e-18 returns 1/(2m+1)). */
 double oracle_boys(int m, double T) {
     if (T < 1e-18) return 1.0 / (2 * m + 1);
+    if (T > 50.0 && T > m + 1.5) {
+        /* F_m = (Gamma(m+1/2) - Gamma(m+1/2, T)) / (2 T^(m+1/2)) */
+        long double a = m + 0.5L, t = T;
+        long double g = sqrtl(3.14159265358979323846264338327950288L);
+        for (int k = 1; k <= m; ++k) g *= (k - 0.5L);
+        long double ta = powl(t, a);
+        long double upper = expl(-t) * ta * upper_gamma_cf(a, t);
+        return (double)((g - upper) / (2.0L * ta));
+    }
     long double t = T, sum = 0.0L, term = 1.0L / (2 * m + 1);
     for (int k = 0; k < 100000; ++k) {
         sum += term;
@@ -397,6 +426,16 @@ static void shell_quartet(const oracle_basis *b, int sa, int sb, int sc, int sd,
     free(vrrs); free(cvrrs); free(hrrs);
 }
 
+/* Orientation of each shell quartet handed to chrr.  0 (default): the reference's, chrr(I,J,K,L)
+ * with I >= J, K >= L, pair(IJ) >= pair(KL) by shell index (src/HGP.jl:27-28).  1: the
+ * engine's: in each pair the shell with the larger L is 'a' (ties keep the higher index
+ * first), and the pair of higher class (la+lb, then la) is the bra.  The two are the same
+ * mathematics; their rounding differs, and HRR accuracy depends strongly on which shell
+ * receives the transferred angular momentum. */
+static int g_orient = 0;
+void oracle_set_orientation(int mode) { g_orient = mode; }
+int oracle_get_orientation(void) { return g_orient; }
+
 /* all_twoe_ints_chrr, src/HGP.jl:22-34, with D1-D3 and D5 fixed: every unique shell
  * quartet (I>=J, K>=L, pair(IJ)>=pair(KL)) is computed once and scattered to the 0-based
  * iindex positions.  nthreads > 1 uses OpenMP with a dynamic schedule, the analogue of
@@ -446,6 +485,15 @@ static int64_t eri_packed_hgp_impl(int nshell, const double *xyz, const int *L, 
         while (tri64(p1 + 1) <= q) ++p1;
         int64_t p2 = q - tri64(p1);
         int I = pi[p1], J = pj[p1], K = pi[p2], Lsh = pj[p2];
+        if (g_orient == 1) {
+            int t;
+            if (L[I] < L[J]) { t = I; I = J; J = t; }
+            if (L[K] < L[Lsh]) { t = K; K = Lsh; Lsh = t; }
+            int sb = L[I] + L[J], sk = L[K] + L[Lsh];
+            if (sk > sb || (sk == sb && L[K] > L[I])) {
+                t = I; I = K; K = t; t = J; J = Lsh; Lsh = t;
+            }
+        }
         int na = g_ncart[L[I]], nb = g_ncart[L[J]], nc = g_ncart[L[K]], nd = g_ncart[L[Lsh]];
         shell_quartet(&b, I, J, K, Lsh, buf);
         int x = 0;
@@ -457,7 +505,8 @@ static int64_t eri_packed_hgp_impl(int nshell, const double *xyz, const int *L, 
                         int64_t k = b.fn_off[K] + mc, l = b.fn_off[Lsh] + md;
                         if (I == J && i < j) continue;
                         if (K == Lsh && k < l) continue;
-                        int64_t ij = tri64(i) + j, kl = tri64(k) + l;
+                        int64_t ij = i >= j ? tri64(i) + j : tri64(j) + i;
+                        int64_t kl = k >= l ? tri64(k) + l : tri64(l) + k;
                         if (p1 == p2 && ij < kl) continue;
                         out[oracle_iindex(i, j, k, l)] = buf[x];
                         ++written;

@@ -78,6 +78,8 @@ def lib():
         L.oracle_coulomb_prim.argtypes = ([_D, _D, _D, _D, _I, _I, _I] * 4)
         L.oracle_eri_packed_hgp_sample.restype = ctypes.c_int64
         L.oracle_eri_packed_hgp_sample.argtypes = drv + [ctypes.c_int64]
+        L.oracle_set_orientation.argtypes = [_I]
+        L.oracle_get_orientation.restype = _I
         L.oracle_set_boys_tmax.argtypes = [_D]
         L.oracle_get_boys_tmax.restype = _D
         L.oracle_init()
@@ -116,6 +118,18 @@ class exact_boys:
 
     def __exit__(self, *exc):
         set_boys_tmax(self._old)
+
+
+class engine_orientation:
+    """Context manager: the HGP driver orients each quartet as the engine does (larger L
+    first in each pair, higher class as bra) instead of by shell index as the reference."""
+
+    def __enter__(self):
+        self._old = lib().oracle_get_orientation()
+        lib().oracle_set_orientation(1)
+
+    def __exit__(self, *exc):
+        lib().oracle_set_orientation(self._old)
 
 
 def boys_mpmath(m: int, T: float, dps: int = 40) -> float:
@@ -229,3 +243,102 @@ def shell_quartet(shells, sa, sb, sc, sd) -> np.ndarray:
 def iindex(i, j, k, l) -> int:
     """0-based iindex (src/Utils.jl:19 minus one)."""
     return lib().oracle_iindex(i, j, k, l)
+
+
+# ------------------------------------------------------------------ mpmath Huzinaga
+def coulomb_mpmath(a, b, c, d, dps: int = 40):
+    """Primitive Huzinaga coulomb (src/ERI.jl:15-94) in mpmath at `dps` digits; each argument
+    is (expn, (x,y,z), (I,J,K)).  Returns an mpf."""
+    import mpmath
+    with mpmath.workdps(dps):
+        mpf = mpmath.mpf
+        F = mpmath.factorial
+
+        def boys(m, T):
+            if T == 0:
+                return mpf(1) / (2 * m + 1)
+            am = mpf(m) + mpf(1) / 2
+            return mpmath.gammainc(am, 0, T) / (2 * T ** am)
+
+        def binom(n, k):
+            return mpmath.binomial(n, k) if 0 <= k <= n else mpf(0)
+
+        def bp(s_, ia, ib, xpa, xpb):
+            return sum((binom(ia, s_ - t) * xpa ** (ia - s_ + t) * binom(ib, t) * xpb ** (ib - t)
+                        for t in range(s_ + 1) if s_ - ia <= t <= ib), mpf(0))
+
+        def fr2(x, y):
+            return F(x) / F(y) / F(x - 2 * y)
+
+        def fB(i, l1, l2, pp, aa, bb, r, g):
+            return bp(i, l1, l2, pp - aa, pp - bb) * fr2(i, r) * (4 * g) ** (r - i)
+
+        def barray(l1, l2, l3, l4, pp, aa, bb, qq, cc, dd, g1, g2, delta):
+            B = [mpf(0)] * (l1 + l2 + l3 + l4 + 1)
+            for i1 in range(l1 + l2 + 1):
+                for i2 in range(l3 + l4 + 1):
+                    for r1 in range(i1 // 2 + 1):
+                        for r2 in range(i2 // 2 + 1):
+                            for u in range((i1 + i2) // 2 - r1 - r2 + 1):
+                                e = i1 + i2 - 2 * (r1 + r2)
+                                B[e - u] += (fB(i1, l1, l2, pp, aa, bb, r1, g1) * (-1) ** i2 *
+                                             fB(i2, l3, l4, qq, cc, dd, r2, g2) * (-1) ** u *
+                                             fr2(e, u) * (qq - pp) ** (e - 2 * u) / delta ** (e - u))
+            return B
+
+        (ea, A, ia), (eb, Bc, ib), (ec, C, ic), (ed, D, id_) = a, b, c, d
+        ea, eb, ec, ed = (mpf(float(x)) for x in (ea, eb, ec, ed))
+        A, Bc, C, D = ([mpf(float(t)) for t in v] for v in (A, Bc, C, D))
+        g1, g2 = ea + eb, ec + ed
+        P = [(ea * A[t] + eb * Bc[t]) / g1 for t in range(3)]
+        Q = [(ec * C[t] + ed * D[t]) / g2 for t in range(3)]
+        rab2 = sum((A[t] - Bc[t]) ** 2 for t in range(3))
+        rcd2 = sum((C[t] - D[t]) ** 2 for t in range(3))
+        rpq2 = sum((P[t] - Q[t]) ** 2 for t in range(3))
+        delta = (1 / g1 + 1 / g2) / 4
+        Bs = [barray(ia[t], ib[t], ic[t], id_[t], P[t], A[t], Bc[t], Q[t], C[t], D[t], g1, g2, delta)
+              for t in range(3)]
+        x = rpq2 / (4 * delta)
+        tot = mpf(0)
+        for I in range(len(Bs[0])):
+            for J in range(len(Bs[1])):
+                for K in range(len(Bs[2])):
+                    tot += Bs[0][I] * Bs[1][J] * Bs[2][K] * boys(I + J + K, x)
+        return (2 * mpmath.pi ** mpf(2.5) / (g1 * g2 * mpmath.sqrt(g1 + g2)) *
+                mpmath.exp(-ea * eb * rab2 / g1) * mpmath.exp(-ec * ed * rcd2 / g2) * tot)
+
+
+def contracted_mpmath(shells, funcs, dps: int = 40) -> float:
+    """Normalised contracted integral of four functions given as (shell index, (I,J,K)),
+    in mpmath (contract and normalize!, src/Basis.jl:42-98)."""
+    import mpmath
+    with mpmath.workdps(dps):
+        mpf = mpmath.mpf
+        terms, gfac = [], mpf(1)
+        for s, ijk in funcs:
+            L = int(shells.L[s])
+            p0, K = int(shells.prim_off[s]), int(shells.nprim[s])
+            ex = [mpf(float(x)) for x in shells.expn[p0:p0 + K]]
+            co = [mpf(float(x)) for x in shells.coef[p0:p0 + K]]
+            S = sum(co[i] * co[j] * (2 * mpmath.sqrt(ex[i] * ex[j]) / (ex[i] + ex[j])) ** (L + mpf(3) / 2)
+                    for i in range(K) for j in range(K))
+            cn = 1 / mpmath.sqrt(S)
+            nc = [co[i] * cn * (2 * ex[i] / mpmath.pi) ** (mpf(3) / 4) * (4 * ex[i]) ** (mpf(L) / 2)
+                  for i in range(K)]
+            terms.append((s, ijk, ex, nc))
+            d2 = 1
+            for p in ijk:
+                n = 2 * p - 1
+                while n > 1:
+                    d2 *= n
+                    n -= 2
+            gfac /= mpmath.sqrt(d2)
+        tot = mpf(0)
+        import itertools
+        for idx in itertools.product(*[range(len(t[2])) for t in terms]):
+            args, cf = [], mpf(1)
+            for (s, ijk, ex, nc), k in zip(terms, idx):
+                args.append((ex[k], shells.xyz[s], ijk))
+                cf *= nc[k]
+            tot += cf * coulomb_mpmath(*args, dps=dps)
+        return float(tot * gfac)

@@ -69,15 +69,27 @@ def test_ethane_sto3g_matches_reference_hgp(eng, oracle):
     assert np.max(np.abs(got - huz)) < TOL_FP64
 
 
+# The reference orients each quartet by shell index (chrr(I,J,K,L), I >= J); the engine puts
+# the larger-L shell of each pair first.  Same mathematics, different rounding: with a tight d
+# (exponent ~2e3) and a diffuse p (~0.2) the reference orientation loses ~1e-11 absolute to
+# HRR cancellation while the engine's stays at ~1e-16 (tests/test_oracle_golden.py pins
+# this against 40-digit values).  Exact parity is therefore checked against the oracle in
+# the engine's orientation, and the reference orientation within its own rounding error.
+TOL_REF_ORIENTATION = 2e-11
+
+
 def test_ethane_polarised_all_classes(eng, oracle):
     """Config 2 (l<=2, 22 class pairs up to (dd|dd)), both Boys modes."""
     from molints_b200 import engine
     sh = mi.config2()
     got = eng.eri_packed(sh)
-    ref = oracle.eri_packed_hgp(sh, nthreads=8)
+    with oracle.engine_orientation():
+        ref = oracle.eri_packed_hgp(sh, nthreads=8)
     assert np.max(np.abs(got - ref)) < TOL_FP64
+    ref_o = oracle.eri_packed_hgp(sh, nthreads=8)
+    assert np.max(np.abs(got - ref_o)) < TOL_REF_ORIENTATION
     got_x = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
-    with oracle.exact_boys():
+    with oracle.exact_boys(), oracle.engine_orientation():
         ref_x = oracle.eri_packed_hgp(sh, nthreads=8)
     assert np.max(np.abs(got_x - ref_x)) < TOL_FP64
 
@@ -166,6 +178,25 @@ def test_deterministic(eng):
     a = eng.eri_packed(sh)
     b = eng.eri_packed(sh)
     assert np.array_equal(a, b)
+
+
+def test_contracted_schwarz_bounds(eng, oracle):
+    sh = mi.config0()
+    plan = eng.plan(sh)
+    import torch
+    out = torch.empty(sh.npacked, dtype=torch.float64, device="cuda")
+    plan.execute(out.data_ptr())
+    q = plan.schwarz()
+    ints = out.cpu().numpy()
+    off = sh.fn_offsets()
+    for i in range(sh.nshell):
+        for j in range(i + 1):
+            m = 0.0
+            for a in range(off[i], off[i + 1]):
+                for b in range(off[j], off[j + 1]):
+                    m = max(m, abs(ints[oracle.iindex(a, b, a, b)]))
+            assert q[i * (i + 1) // 2 + j] == pytest.approx(np.sqrt(m), rel=1e-13)
+    plan.close()
 
 
 def test_plan_execute_twice_on_torch_stream(eng, oracle):

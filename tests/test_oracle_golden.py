@@ -150,3 +150,22 @@ def test_reference_boys_branch_error_is_bounded(oracle):
         exact = oracle.eri_packed_hgp(sh, nthreads=8)
     d = np.max(np.abs(ref - exact))
     assert 1e-13 < d < 1e-10
+
+
+
+def test_hrr_orientation_conditioning(oracle):
+    """Config 2's p shell on an H (exponent 0.209) and d shell on a C (exponent 2044): with the
+    diffuse p first -- the reference's index order for this pair -- chrr loses ~1e-11 to HRR
+    cancellation; with the d first -- the engine's order, larger L first -- it is within
+    1e-15 of the 40-digit Huzinaga value."""
+    sh = mi.config2()
+    p, d = 20, 5
+    assert (int(sh.L[p]), int(sh.L[d])) == (1, 2)
+    two = mi.Shells.from_list([(sh.xyz[p], 1, [(sh.expn[sh.prim_off[p]], 1.0)]),
+                               (sh.xyz[d], 2, [(sh.expn[sh.prim_off[d]], 1.0)])])
+    py, dyy = (0, 1, 0), (0, 2, 0)
+    exact = oracle.contracted_mpmath(two, [(0, py), (1, dyy), (0, py), (1, dyy)])
+    ref_order = oracle.shell_quartet(two, 0, 1, 0, 1)[1, 3, 1, 3]
+    eng_order = oracle.shell_quartet(two, 1, 0, 1, 0)[3, 1, 3, 1]
+    assert abs(eng_order - exact) < 1e-15
+    assert abs(ref_order - exact) > 1e-12
