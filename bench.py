@@ -38,7 +38,6 @@ mi = __graft_entry__.load_package()
 METRIC = "ERIs/sec on 1 B200 (mixed vs plain FP64, max err <=1e-9); serve p50/p99 ms"
 UNIT = "ERI/s"
 WORKLOAD = "split_valence_24 (8 heavy s6s3p3s1p1 + 16 H s3s1, seed 1, 104 cart. functions)"
-FP32_CUTOFF = 1e-4
 CPU_SAMPLE_SECONDS = 10.0
 
 
@@ -175,8 +174,11 @@ def run_ours(args):
 
     out = torch.empty(npacked, dtype=torch.float64, device=dev)
     flush = torch.zeros(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    from molints_b200 import autotune
+    fp32_cut, tune_table = autotune.tune_fp32_cutoff(eng, sh)
+    eng.set_stream(stream.cuda_stream)
     plan64 = eng.plan(sh, precision=E.FP64)
-    planmx = eng.plan(sh, precision=E.MIXED, fp32_cutoff=FP32_CUTOFF)
+    planmx = eng.plan(sh, precision=E.MIXED, fp32_cutoff=fp32_cut)
 
     # accuracy of the mixed path against the FP64 path on the same device
     plan64.execute(out.data_ptr())
@@ -243,11 +245,11 @@ def run_ours(args):
     # end to end through the public call: host basis in, pinned host vector out
     host_out = torch.empty(npacked, dtype=torch.float64, pin_memory=True).numpy()
     eng_e2e = E.Engine(local)
-    eng_e2e.eri_packed(sh, precision=E.MIXED, fp32_cutoff=FP32_CUTOFF, out=host_out)
+    eng_e2e.eri_packed(sh, precision=E.MIXED, fp32_cutoff=fp32_cut, out=host_out)
     e2e_t = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        eng_e2e.eri_packed(sh, precision=E.MIXED, fp32_cutoff=FP32_CUTOFF, out=host_out)
+        eng_e2e.eri_packed(sh, precision=E.MIXED, fp32_cutoff=fp32_cut, out=host_out)
         e2e_t.append(time.perf_counter() - t0)
     h2d = int(sh.xyz.nbytes + sh.L.nbytes + sh.nprim.nbytes + sh.prim_off.nbytes +
               sh.expn.nbytes + sh.coef.nbytes)
@@ -269,7 +271,12 @@ def run_ours(args):
             "dtype": "f64 (FP32 VRR below the Schwarz cutoff)", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_eri_per_step": npacked,
                        "shell_quartets": tot["quartets"], "prim_quartets": tot["prim_quartets"],
-                       "fp32_cutoff": FP32_CUTOFF, "fp32_quartets": mx_stats["n_fp32_quartets"],
+                       "fp32_cutoff": fp32_cut, "fp32_quartets": mx_stats["n_fp32_quartets"],
+                       "fp32_cutoff_tuning": tune_table,
+                       "prim_pairs": mx_stats["n_prim_pairs"],
+                       "prim_pairs_kept": mx_stats["n_prim_pairs_kept"],
+                       "prim_quartets_computed": mx_stats["n_prim_quartets"],
+                       "prim_cutoff": E.PRIM_CUTOFF,
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replicas x{world}"},
             "max_abs_err_mixed_vs_fp64": max_err,

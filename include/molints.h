@@ -72,9 +72,14 @@ typedef struct molints_options {
     /* Both cutoffs compare against B = Qabs_ab * Qabs_cd, where Qabs_ab is the sum over the
      * pair's primitive pairs i of sqrt(max |(a_i b_i|a_i b_i)|).  B bounds the sum of the
      * magnitudes of all primitive contributions to (ab|cd), not only |(ab|cd)|. */
-    double fp32_cutoff;      /* MIXED: quartets with B below this run the VRR in FP32
-                                (FP64 Boys, prefactors, contraction and HRR) */
+    double fp32_cutoff;      /* MIXED: quartets with R_ab * R_cd below this run the VRR in
+                                FP32 (FP64 Boys, prefactors, contraction and HRR); R_ab =
+                                (1+|A-B|)^lb sum_i sqrt(max |[e0|e0]_ii|) bounds the VRR
+                                output block the HRR combines */
     double screen_cutoff;    /* quartets with B below this are written as 0 */
+    double prim_cutoff;      /* primitive pairs i with b_i * max_cd Qabs_cd below this are
+                                dropped, b_i = sqrt(max |(a_i b_i|a_i b_i)|); each dropped
+                                contribution is below prim_cutoff.  Default 1e-18. */
 } molints_options;
 
 typedef struct molints_stats {
@@ -86,6 +91,8 @@ typedef struct molints_stats {
     int32_t n_kernel_launches;
     int32_t reserved;
     double device_ms;         /* device time of the last execute (CUDA events) */
+    int64_t n_prim_pairs;     /* primitive pairs of all shell pairs */
+    int64_t n_prim_pairs_kept;/* primitive pairs left after prim_cutoff */
 } molints_stats;
 
 typedef struct molints_ctx molints_ctx;
@@ -94,7 +101,8 @@ typedef struct molints_plan molints_plan;
 /* Library version / ABI check. */
 int molints_abi_version(void);
 
-/* Fill opts with the defaults: AUTO, FP64, reference Boys, fp32_cutoff 0, screen 0. */
+/* Fill opts with the defaults: AUTO, FP64, reference Boys, fp32_cutoff 0, screen_cutoff 0,
+ * prim_cutoff 1e-18. */
 void molints_default_options(molints_options *opts);
 
 /* Number of basis functions of a basis, or a negative status. */
@@ -121,11 +129,13 @@ int molints_eri_packed(molints_ctx *ctx, const molints_basis *basis,
                        const molints_options *opts, double *out, int out_is_device,
                        molints_stats *stats);
 
-/* Plans: the device-resident form of one basis.  plan_create normalises the basis, orders
- * the shell pairs by class and contraction length, uploads them and sizes every buffer;
- * plan_execute then runs the whole device path -- primitive-pair data, Schwarz bounds and
- * all shell quartets -- into a device vector of molints_npacked(nbf) doubles, on the
- * context's stream, without host synchronisation. */
+/* Plans: the device-resident form of one basis.  plan_create normalises the basis, builds
+ * the primitive pairs and their Schwarz bounds on the device, drops negligible primitive
+ * pairs (prim_cutoff), orders the shell pairs by class and kept contraction length and
+ * uploads the pair tables (it synchronises the context's stream once).  plan_execute then
+ * runs the device path -- primitive-pair records and every shell quartet -- into a device
+ * vector of molints_npacked(nbf) doubles, on the context's stream, without host
+ * synchronisation. */
 int molints_plan_create(molints_ctx *ctx, const molints_basis *basis,
                         const molints_options *opts, molints_plan **plan);
 int molints_plan_execute(molints_plan *plan, double *out_device);

@@ -5,7 +5,8 @@
 //     contraction length; structure of arrays:
 //       info[p] = {first primitive pair, number of primitive pairs, first function of A,
 //                  first function of B}                      (int4, 16 B)
-//       geo[p]  = {A-B (x,y,z), primitive Schwarz sum Qabs_p} (double4, 32 B)
+//       geo[p]  = {A-B (x,y,z), unused}                    (double4, 32 B)
+//       bnd[p]  = {Qabs_p, R_p}: bounds for screening and for FP32 quartets (double2)
 //   * primitive pairs, 80 B each (5 x 16 B vector loads): PrimPair below;
 //   * the Boys table (T = 0..40 step 1/16, F_0..F_22 and e^-T per row);
 //   * the packed output vector, 0-based iindex order (src/Utils.jl:14-19).
@@ -39,8 +40,9 @@ static_assert(sizeof(PrimPair) == 80, "PrimPair is 5 x 16 bytes");
 
 struct PairTab {
     const int4 *info;
-    const double4 *geo;   // w: primitive Schwarz sum Qabs (0 when the plan needs no bound)
+    const double4 *geo;   // A - B (w unused)
     const PrimPair *pp;
+    const double2 *bnd;   // x: Qabs_p = sum_k b_k, y: R_p = (1+|AB|)^lb sum_k w_k (kept prims)
 };
 
 struct BoysTab {
@@ -60,7 +62,7 @@ struct EriLaunch {
     int pad;
     long long nquart;         // nbra * nket or nbra * (nbra + 1) / 2
     double screen_cut;        // Qabs_p Qabs_q below this: written as 0
-    double fp32_cut;          // Qabs_p Qabs_q below this (MIXED kernels): FP32 VRR
+    double fp32_cut;          // R_p R_q below this (MIXED kernels): FP32 VRR
 };
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {

@@ -3,34 +3,34 @@
 #include "eri_common.cuh"
 namespace molints {
 void launch_eri_ssss(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_schwarz_ssss(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw, double *qout, int full, cudaStream_t s);
+void launch_schwarz_ssss(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 void launch_eri_psss(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_psps(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_schwarz_psps(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw, double *qout, int full, cudaStream_t s);
+void launch_schwarz_psps(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 void launch_eri_ppss(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_ppps(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_pppp(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_schwarz_pppp(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw, double *qout, int full, cudaStream_t s);
+void launch_schwarz_pppp(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 void launch_eri_dsss(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dsps(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dspp(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dsds(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_schwarz_dsds(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw, double *qout, int full, cudaStream_t s);
+void launch_schwarz_dsds(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 void launch_eri_dpss(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dpps(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dppp(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dpds(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dpdp(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_schwarz_dpdp(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw, double *qout, int full, cudaStream_t s);
+void launch_schwarz_dpdp(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 void launch_eri_ddss(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_ddps(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_ddpp(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_ddds(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dddp(const EriLaunch &L, int mixed, cudaStream_t s);
 void launch_eri_dddd(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_schwarz_dddd(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw, double *qout, int full, cudaStream_t s);
+void launch_schwarz_dddd(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 typedef void (*EriLauncher)(const EriLaunch &, int, cudaStream_t);
-typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, double4 *, double *, int, cudaStream_t);
+typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, double2 *, double *, int, cudaStream_t);
 constexpr int kLmax = 2;
 constexpr int kNumPairClasses = 6;
 // pair class c = (kPairClassLa[c], kPairClassLb[c]), ordered by la+lb then la

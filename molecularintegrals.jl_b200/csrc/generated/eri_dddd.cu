@@ -12,7 +12,8 @@ namespace molints {
 template <typename VT>
 __device__ __forceinline__ void quartet_dddd(const PairTab &P, const BoysTab &B, int p, int q,
                                               int i0, int i1, int j0, int j1,
-                                              double *__restrict__ res) {
+                                              double *__restrict__ res,
+                                              double *__restrict__ acc_out = nullptr) {
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
     double acc[961];
@@ -3331,6 +3332,10 @@ __device__ __forceinline__ void quartet_dddd(const PairTab &P, const BoysTab &B,
             acc[959] += (double)v34_33_0;
             acc[960] += (double)v34_34_0;
         }
+    }
+    if (acc_out) {
+#pragma unroll
+        for (int x = 0; x < 961; ++x) acc_out[x] = acc[x];
     }
     const double4 gb = ldg4(&P.geo[p]);
     const double4 gk = ldg4(&P.geo[q]);
@@ -12604,14 +12609,14 @@ __global__ void __launch_bounds__(128) eri_kernel_dddd(const EriLaunch L) {
     if (t >= L.nquart) return;
     int p, q;
     decode_quartet(L, t, p, q);
-    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    const double2 bp = __ldg(&L.pairs.bnd[p]), bq = __ldg(&L.pairs.bnd[q]);
     double res[1296];
-    if (bound < L.screen_cut) {
+    if (bp.x * bq.x < L.screen_cut) {
 #pragma unroll
         for (int x = 0; x < 1296; ++x) res[x] = 0.0;
     } else {
         const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
-        if (MIXED && bound < L.fp32_cut) quartet_dddd<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+        if (MIXED && bp.y * bq.y < L.fp32_cut) quartet_dddd<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
         else quartet_dddd<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
     }
     store_dddd(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
@@ -12624,21 +12629,23 @@ void launch_eri_dddd(const EriLaunch &L, int mixed, cudaStream_t s) {
     else eri_kernel_dddd<0><<<(unsigned)blocks, 128, 0, s>>>(L);
 }
 
-// Primitive Schwarz sum of the pairs of one class:
-//   Qabs_p = sum_i sqrt(max over components |(a_i b_i | a_i b_i)|)
-// over the pair's primitive pairs i.  By the Schwarz inequality on every primitive quartet,
-// Qabs_p Qabs_q bounds sum over primitive quartets of |(a_i b_i | c_k d_k)|, hence both
-// |(ab|cd)| and the magnitude the VRR works at before the contraction cancels.
-// With full != 0 it writes the contracted bound Q_p = sqrt(max |(ab|ab)|) to qout instead.
+// Bounds of the pairs of one class.
+// full == 0 (plan set-up): for every primitive pair k of pair p, from the diagonal primitive
+//   quartet (a_k b_k | a_k b_k):
+//     pbound[k].x = b_k = sqrt(max over components |(a_k b_k|a_k b_k)|)
+//     pbound[k].y = w_k = sqrt(max over the VRR block |[e0|e0]_kk|), e = la..la+lb
+//   By the Schwarz inequality b_k b_l bounds |(a_k b_k|c_l d_l)| and w_k w_l bounds every
+//   entry of the VRR output block [e0|f0] that the HRR combines.
+// full != 0: the contracted bound Q_p = sqrt(max |(ab|ab)|) into qout[p].
 __global__ void __launch_bounds__(128) schwarz_kernel_dddd(PairTab P, BoysTab B, int p0, int np,
-                                                          double4 *geo_rw, double *qout, int full) {
+                                                          double2 *pbound, double *qout, int full) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= np) return;
     const int p = p0 + t;
-    const int npp = __ldg(&P.info[p]).y;
+    const int4 in = __ldg(&P.info[p]);
     double res[1296];
     if (full) {
-        quartet_dddd<double>(P, B, p, p, 0, npp, 0, npp, res);
+        quartet_dddd<double>(P, B, p, p, 0, in.y, 0, in.y, res);
         double m = 0.0;
     m = fmax(m, fabs(res[0]));
     m = fmax(m, fabs(res[37]));
@@ -12679,10 +12686,10 @@ __global__ void __launch_bounds__(128) schwarz_kernel_dddd(PairTab P, BoysTab B,
         qout[p] = sqrt(m);
         return;
     }
-    double qa = 0.0;
-    for (int i = 0; i < npp; ++i) {
-        quartet_dddd<double>(P, B, p, p, i, i + 1, i, i + 1, res);
-        double m = 0.0;
+    double acc[961];
+    for (int k = 0; k < in.y; ++k) {
+        quartet_dddd<double>(P, B, p, p, k, k + 1, k, k + 1, res, acc);
+        double m = 0.0, w = 0.0;
     m = fmax(m, fabs(res[0]));
     m = fmax(m, fabs(res[37]));
     m = fmax(m, fabs(res[74]));
@@ -12719,15 +12726,45 @@ __global__ void __launch_bounds__(128) schwarz_kernel_dddd(PairTab P, BoysTab B,
     m = fmax(m, fabs(res[1221]));
     m = fmax(m, fabs(res[1258]));
     m = fmax(m, fabs(res[1295]));
-        qa += sqrt(m);
+        w = fmax(w, fabs(acc[0]));
+        w = fmax(w, fabs(acc[32]));
+        w = fmax(w, fabs(acc[64]));
+        w = fmax(w, fabs(acc[96]));
+        w = fmax(w, fabs(acc[128]));
+        w = fmax(w, fabs(acc[160]));
+        w = fmax(w, fabs(acc[192]));
+        w = fmax(w, fabs(acc[224]));
+        w = fmax(w, fabs(acc[256]));
+        w = fmax(w, fabs(acc[288]));
+        w = fmax(w, fabs(acc[320]));
+        w = fmax(w, fabs(acc[352]));
+        w = fmax(w, fabs(acc[384]));
+        w = fmax(w, fabs(acc[416]));
+        w = fmax(w, fabs(acc[448]));
+        w = fmax(w, fabs(acc[480]));
+        w = fmax(w, fabs(acc[512]));
+        w = fmax(w, fabs(acc[544]));
+        w = fmax(w, fabs(acc[576]));
+        w = fmax(w, fabs(acc[608]));
+        w = fmax(w, fabs(acc[640]));
+        w = fmax(w, fabs(acc[672]));
+        w = fmax(w, fabs(acc[704]));
+        w = fmax(w, fabs(acc[736]));
+        w = fmax(w, fabs(acc[768]));
+        w = fmax(w, fabs(acc[800]));
+        w = fmax(w, fabs(acc[832]));
+        w = fmax(w, fabs(acc[864]));
+        w = fmax(w, fabs(acc[896]));
+        w = fmax(w, fabs(acc[928]));
+        w = fmax(w, fabs(acc[960]));
+        pbound[in.x + k] = make_double2(sqrt(m), sqrt(w));
     }
-    geo_rw[p].w = qa;
 }
 
-void launch_schwarz_dddd(const PairTab &P, const BoysTab &B, int p0, int np, double4 *geo_rw,
+void launch_schwarz_dddd(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound,
                           double *qout, int full, cudaStream_t s) {
     if (np <= 0) return;
-    schwarz_kernel_dddd<<<(np + 127) / 128, 128, 0, s>>>(P, B, p0, np, geo_rw, qout, full);
+    schwarz_kernel_dddd<<<(np + 127) / 128, 128, 0, s>>>(P, B, p0, np, pbound, qout, full);
 }
 
 }  // namespace molints

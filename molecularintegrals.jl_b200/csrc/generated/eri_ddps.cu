@@ -12,7 +12,8 @@ namespace molints {
 template <typename VT>
 __device__ __forceinline__ void quartet_ddps(const PairTab &P, const BoysTab &B, int p, int q,
                                               int i0, int i1, int j0, int j1,
-                                              double *__restrict__ res) {
+                                              double *__restrict__ res,
+                                              double *__restrict__ acc_out = nullptr) {
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
     double acc[93];
@@ -331,6 +332,10 @@ __device__ __forceinline__ void quartet_ddps(const PairTab &P, const BoysTab &B,
             acc[91] += (double)v34_2_0;
             acc[92] += (double)v34_3_0;
         }
+    }
+    if (acc_out) {
+#pragma unroll
+        for (int x = 0; x < 93; ++x) acc_out[x] = acc[x];
     }
     const double4 gb = ldg4(&P.geo[p]);
     const double4 gk = ldg4(&P.geo[q]);
@@ -951,14 +956,14 @@ __global__ void __launch_bounds__(128) eri_kernel_ddps(const EriLaunch L) {
     if (t >= L.nquart) return;
     int p, q;
     decode_quartet(L, t, p, q);
-    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    const double2 bp = __ldg(&L.pairs.bnd[p]), bq = __ldg(&L.pairs.bnd[q]);
     double res[108];
-    if (bound < L.screen_cut) {
+    if (bp.x * bq.x < L.screen_cut) {
 #pragma unroll
         for (int x = 0; x < 108; ++x) res[x] = 0.0;
     } else {
         const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
-        if (MIXED && bound < L.fp32_cut) quartet_ddps<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+        if (MIXED && bp.y * bq.y < L.fp32_cut) quartet_ddps<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
         else quartet_ddps<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
     }
     store_ddps(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);

@@ -12,7 +12,8 @@ namespace molints {
 template <typename VT>
 __device__ __forceinline__ void quartet_ppps(const PairTab &P, const BoysTab &B, int p, int q,
                                               int i0, int i1, int j0, int j1,
-                                              double *__restrict__ res) {
+                                              double *__restrict__ res,
+                                              double *__restrict__ acc_out = nullptr) {
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
     double acc[27];
@@ -119,6 +120,10 @@ __device__ __forceinline__ void quartet_ppps(const PairTab &P, const BoysTab &B,
             acc[25] += (double)v9_2_0;
             acc[26] += (double)v9_3_0;
         }
+    }
+    if (acc_out) {
+#pragma unroll
+        for (int x = 0; x < 27; ++x) acc_out[x] = acc[x];
     }
     const double4 gb = ldg4(&P.geo[p]);
     const double4 gk = ldg4(&P.geo[q]);
@@ -259,14 +264,14 @@ __global__ void __launch_bounds__(128) eri_kernel_ppps(const EriLaunch L) {
     if (t >= L.nquart) return;
     int p, q;
     decode_quartet(L, t, p, q);
-    const double bound = ldg4(&L.pairs.geo[p]).w * ldg4(&L.pairs.geo[q]).w;
+    const double2 bp = __ldg(&L.pairs.bnd[p]), bq = __ldg(&L.pairs.bnd[q]);
     double res[27];
-    if (bound < L.screen_cut) {
+    if (bp.x * bq.x < L.screen_cut) {
 #pragma unroll
         for (int x = 0; x < 27; ++x) res[x] = 0.0;
     } else {
         const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
-        if (MIXED && bound < L.fp32_cut) quartet_ppps<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+        if (MIXED && bp.y * bq.y < L.fp32_cut) quartet_ppps<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
         else quartet_ppps<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
     }
     store_ppps(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);

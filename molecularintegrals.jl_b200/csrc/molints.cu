@@ -43,19 +43,22 @@ struct molints_plan {
     molints_options opts{};
     int nshell = 0;
     int64_t nbf = 0, npacked = 0;
-    int npair = 0, nprim_pair = 0;
+    int npair = 0;
+    int64_t nprim_pair_all = 0, nprim_pair_kept = 0;
     int class_start[kNumPairClasses + 1] = {0};
-    // host copies
+    // host copies (final, screened order)
     std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
-    std::vector<int4> info_h;
-    std::vector<int> npp_h;
+    std::vector<int> npp_h;            // kept primitive pairs per shell pair
+    std::vector<double2> bnd_h;        // (Qabs, R) per shell pair
     // device buffers
     double *sh_xyz = nullptr, *expn = nullptr, *ncoef = nullptr;
     int *sh_poff = nullptr, *sh_nprim = nullptr;
     int2 *pair_ab = nullptr;
     int4 *info = nullptr;
+    int *pp_src = nullptr;             // primitive pair k -> (ia << 8) | ib within its shells
     double4 *geo = nullptr;
     PrimPair *pp = nullptr;
+    double2 *bnd = nullptr;
     double *qcon = nullptr;  // contracted Schwarz bounds, filled on demand by plan_schwarz
     int64_t bytes = 0;
     int n_launches = 0;
@@ -127,8 +130,8 @@ int dev_alloc(molints_ctx *ctx, T **p, size_t count, int64_t *tally) {
 namespace molints {
 
 __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
-                                   const int4 *__restrict__ info, const double *__restrict__ xyz,
-                                   const int *__restrict__ poff, const int *__restrict__ nprim,
+                                   const int4 *__restrict__ info, const int *__restrict__ pp_src,
+                                   const double *__restrict__ xyz, const int *__restrict__ poff,
                                    const double *__restrict__ expn,
                                    const double *__restrict__ ncoef, double c0,
                                    PrimPair *__restrict__ pp, double4 *__restrict__ geo) {
@@ -140,27 +143,24 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
     const double Bx = xyz[3 * ab.y], By = xyz[3 * ab.y + 1], Bz = xyz[3 * ab.y + 2];
     const double ABx = Ax - Bx, ABy = Ay - By, ABz = Az - Bz;
     const double rab2 = ABx * ABx + ABy * ABy + ABz * ABz;
-    const int ka = nprim[ab.x], kb = nprim[ab.y];
     const int pa0 = poff[ab.x], pb0 = poff[ab.y];
-    int k = in.x;
-    for (int ia = 0; ia < ka; ++ia) {
-        const double a = expn[pa0 + ia], ca = ncoef[pa0 + ia];
-        for (int ib = 0; ib < kb; ++ib, ++k) {
-            const double b = expn[pb0 + ib], cb = ncoef[pb0 + ib];
-            const double zeta = a + b, ooz = 1.0 / zeta;
-            PrimPair r;
-            r.zeta = zeta;
-            r.kab = c0 * ca * cb * exp(-a * b * ooz * rab2) * ooz;
-            r.oo2z = 0.5 * ooz;
-            r.px = (a * Ax + b * Bx) * ooz;
-            r.py = (a * Ay + b * By) * ooz;
-            r.pz = (a * Az + b * Bz) * ooz;
-            r.pax = r.px - Ax;
-            r.pay = r.py - Ay;
-            r.paz = r.pz - Az;
-            r.pad = 0.0;
-            pp[k] = r;
-        }
+    for (int k = in.x; k < in.x + in.y; ++k) {
+        const int src = pp_src[k];
+        const double a = expn[pa0 + (src >> 8)], ca = ncoef[pa0 + (src >> 8)];
+        const double b = expn[pb0 + (src & 255)], cb = ncoef[pb0 + (src & 255)];
+        const double zeta = a + b, ooz = 1.0 / zeta;
+        PrimPair r;
+        r.zeta = zeta;
+        r.kab = c0 * ca * cb * exp(-a * b * ooz * rab2) * ooz;
+        r.oo2z = 0.5 * ooz;
+        r.px = (a * Ax + b * Bx) * ooz;
+        r.py = (a * Ay + b * By) * ooz;
+        r.pz = (a * Az + b * Bz) * ooz;
+        r.pax = r.px - Ax;
+        r.pay = r.py - Ay;
+        r.paz = r.pz - Az;
+        r.pad = 0.0;
+        pp[k] = r;
     }
     geo[p] = make_double4(ABx, ABy, ABz, 0.0);
 }
@@ -197,6 +197,7 @@ void molints_default_options(molints_options *o) {
     o->boys = MOLINTS_BOYS_REFERENCE;
     o->fp32_cutoff = 0.0;
     o->screen_cutoff = 0.0;
+    o->prim_cutoff = 1e-18;
 }
 
 int64_t molints_npacked(int64_t n) { return n < 0 ? -1 : n * (n + 1) * (n * n + n + 2) / 8; }
@@ -310,7 +311,7 @@ static void plan_free(molints_plan *p) {
     if (!p) return;
     for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->sh_nprim, p->pair_ab,
-                    p->info, p->geo, p->pp, p->qcon};
+                    p->info, p->pp_src, p->geo, p->pp, p->bnd, p->qcon};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (p->ctx) p->ctx->held -= p->bytes;
@@ -337,7 +338,7 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown Boys mode");
     if (opts.method != MOLINTS_METHOD_AUTO && opts.method != MOLINTS_METHOD_HGP)
         return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: method not available");
-    if (!(opts.fp32_cutoff >= 0.0) || !(opts.screen_cutoff >= 0.0))
+    if (!(opts.fp32_cutoff >= 0.0) || !(opts.screen_cutoff >= 0.0) || !(opts.prim_cutoff >= 0.0))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: cutoffs must be >= 0");
     const int64_t nbf = molints_nbf(b);
     if (nbf < 0) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: malformed basis");
@@ -398,52 +399,149 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
         for (int j = 0; j <= i; ++j) {
             int a = i, bb = j;
             if (b->L[a] < b->L[bb]) std::swap(a, bb);
+            if (b->nprim[a] > 255 || b->nprim[bb] > 255) {
+                plan_free(p);
+                return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: more than 255 primitives in a shell");
+            }
             pr.push_back({pair_class_of(b->L[a], b->L[bb]), b->nprim[a] * b->nprim[bb], a, bb,
                           i * (i + 1) / 2 + j});
         }
-    std::stable_sort(pr.begin(), pr.end(), [](const PairRec &x, const PairRec &y) {
+    auto by_class_then_k = [](const PairRec &x, const PairRec &y) {
         return x.cls != y.cls ? x.cls < y.cls : x.npp > y.npp;
-    });
-    p->npair = (int)pr.size();
-    std::vector<int2> ab_h(p->npair);
-    p->info_h.resize(p->npair);
-    p->npp_h.resize(p->npair);
-    p->pair_ref.resize(p->npair);
-    int ppo = 0;
-    for (int k = 0; k < p->npair; ++k) {
-        ab_h[k] = make_int2(pr[k].a, pr[k].b);
-        p->info_h[k] = make_int4(ppo, pr[k].npp, fn_off[pr[k].a], fn_off[pr[k].b]);
-        p->npp_h[k] = pr[k].npp;
-        p->pair_ref[k] = pr[k].ref;
-        ppo += pr[k].npp;
-        p->class_start[pr[k].cls + 1] = k + 1;
-    }
-    for (int c = 1; c <= kNumPairClasses; ++c)
-        p->class_start[c] = std::max(p->class_start[c], p->class_start[c - 1]);
-    p->nprim_pair = ppo;
+    };
+    std::stable_sort(pr.begin(), pr.end(), by_class_then_k);
+    const int npair = (int)pr.size();
+    p->npair = npair;
+
+    // Stage 1: every primitive pair, for the bound pass.
+    std::vector<int2> ab_h(npair);
+    std::vector<int4> info_h(npair);
+    std::vector<int> src_h;
+    std::vector<int> cls_start(kNumPairClasses + 1, 0);
+    auto fill_tables = [&](const std::vector<std::vector<int>> *kept) {
+        src_h.clear();
+        std::fill(cls_start.begin(), cls_start.end(), 0);
+        for (int k = 0; k < npair; ++k) {
+            ab_h[k] = make_int2(pr[k].a, pr[k].b);
+            const int off = (int)src_h.size();
+            const int kb = b->nprim[pr[k].b];
+            if (kept) {
+                for (int x : (*kept)[pr[k].ref]) src_h.push_back(x);
+            } else {
+                for (int ia = 0; ia < b->nprim[pr[k].a]; ++ia)
+                    for (int ib = 0; ib < kb; ++ib) src_h.push_back((ia << 8) | ib);
+            }
+            info_h[k] = make_int4(off, (int)src_h.size() - off, fn_off[pr[k].a], fn_off[pr[k].b]);
+            cls_start[pr[k].cls + 1] = k + 1;
+        }
+        for (int c = 1; c <= kNumPairClasses; ++c) cls_start[c] = std::max(cls_start[c], cls_start[c - 1]);
+    };
+    fill_tables(nullptr);
+    const int64_t nall = (int64_t)src_h.size();
+    p->nprim_pair_all = nall;
 
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) { plan_free(p); return cuda_fail(ctx, e, "cudaSetDevice"); }
+    double2 *pbound = nullptr;
+    int64_t scratch = 0;
     int rc = 0;
     rc = rc ? rc : dev_alloc(ctx, &p->sh_xyz, (size_t)3 * ns, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->expn, (size_t)nprim_tot, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->ncoef, (size_t)nprim_tot, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->sh_poff, (size_t)ns, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->sh_nprim, (size_t)ns, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->pair_ab, (size_t)p->npair, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->info, (size_t)p->npair, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->geo, (size_t)p->npair, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)ppo, &p->bytes);
-    if (rc) { plan_free(p); return rc; }
+    rc = rc ? rc : dev_alloc(ctx, &p->pair_ab, (size_t)npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->info, (size_t)npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->geo, (size_t)npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->bnd, (size_t)npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->pp_src, (size_t)nall, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)nall, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &pbound, (size_t)nall, &scratch);
+    if (rc) {
+        if (pbound) { cudaFree(pbound); ctx->held -= scratch; }
+        plan_free(p);
+        return rc;
+    }
     cudaStream_t s = ctx->stream;
     const size_t np = (size_t)std::max(nprim_tot, 0);
+    const double c0 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
+    std::vector<double2> pb_h(nall);
+    PairTab P{p->info, p->geo, p->pp, p->bnd};
+    BoysTab Bt = boys_of(ctx, opts.boys);
     if ((e = cudaMemcpyAsync(p->sh_xyz, b->xyz, 3 * ns * sizeof(double), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->expn, b->expn, np * sizeof(double), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->ncoef, ncoef.data(), np * sizeof(double), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->sh_poff, b->prim_off, ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->sh_nprim, b->nprim, ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), p->npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->info, p->info_h.data(), p->npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nall * sizeof(int), cudaMemcpyHostToDevice, s))) {
+        cudaFree(pbound); ctx->held -= scratch; plan_free(p);
+        return cuda_fail(ctx, e, "plan_create upload");
+    }
+    if (npair > 0) {
+        build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, p->pair_ab, p->info, p->pp_src,
+                                                               p->sh_xyz, p->sh_poff, p->expn,
+                                                               p->ncoef, c0, p->pp, p->geo);
+        for (int c = 0; c < kNumPairClasses; ++c)
+            kSchwarzLaunchers[c](P, Bt, cls_start[c], cls_start[c + 1] - cls_start[c], pbound, nullptr,
+                                 0, s);
+    }
+    if ((e = cudaGetLastError()) ||
+        (nall > 0 && (e = cudaMemcpyAsync(pb_h.data(), pbound, nall * sizeof(double2),
+                                          cudaMemcpyDeviceToHost, s))) ||
+        (e = cudaStreamSynchronize(s))) {
+        cudaFree(pbound); ctx->held -= scratch; plan_free(p);
+        return cuda_fail(ctx, e, "plan_create bound pass");
+    }
+    cudaFree(pbound);
+    ctx->held -= scratch;
+
+    // Stage 2: drop primitive pairs i with b_i * max Qabs < prim_cutoff (each dropped term of
+    // any integral is below prim_cutoff by the Schwarz inequality), keep pairs' bounds.
+    double qmax = 0.0;
+    std::vector<double> qabs_all(npair, 0.0);
+    for (int k = 0; k < npair; ++k) {
+        for (int x = 0; x < info_h[k].y; ++x) qabs_all[k] += pb_h[info_h[k].x + x].x;
+        qmax = std::max(qmax, qabs_all[k]);
+    }
+    std::vector<std::vector<int>> kept(npair);
+    std::vector<double2> bnd_ref(npair);
+    int64_t nkept = 0;
+    for (int k = 0; k < npair; ++k) {
+        const int ref = pr[k].ref;
+        double qa = 0.0, wa = 0.0;
+        for (int x = 0; x < info_h[k].y; ++x) {
+            const double2 bb = pb_h[info_h[k].x + x];
+            if (opts.prim_cutoff > 0.0 && bb.x * qmax < opts.prim_cutoff) continue;
+            kept[ref].push_back(src_h[info_h[k].x + x]);
+            qa += bb.x;
+            wa += bb.y;
+        }
+        const double *A = b->xyz + 3 * pr[k].a, *Bc = b->xyz + 3 * pr[k].b;
+        const double dab = std::sqrt((A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
+                                     (A[2] - Bc[2]) * (A[2] - Bc[2]));
+        bnd_ref[ref] = make_double2(qa, wa * std::pow(1.0 + dab, b->L[pr[k].b]));
+        pr[k].npp = (int)kept[ref].size();
+        nkept += pr[k].npp;
+    }
+    p->nprim_pair_kept = nkept;
+    std::stable_sort(pr.begin(), pr.end(), by_class_then_k);
+    fill_tables(&kept);
+    for (int c = 0; c <= kNumPairClasses; ++c) p->class_start[c] = cls_start[c];
+    p->pair_ref.resize(npair);
+    p->npp_h.resize(npair);
+    p->bnd_h.resize(npair);
+    for (int k = 0; k < npair; ++k) {
+        p->pair_ref[k] = pr[k].ref;
+        p->npp_h[k] = pr[k].npp;
+        p->bnd_h[k] = bnd_ref[pr[k].ref];
+    }
+    if ((e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->bnd, p->bnd_h.data(), npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
+        (nkept > 0 && (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nkept * sizeof(int),
+                                           cudaMemcpyHostToDevice, s))) ||
         (e = cudaStreamSynchronize(s))) {
         plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
@@ -476,25 +574,13 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
     if (p->npair > 0) {
         if (int rc = mark(launches, "build_pairs", 0)) return rc;
         build_pairs_kernel<<<(p->npair + 127) / 128, 128, 0, s>>>(
-            p->npair, p->pair_ab, p->info, p->sh_xyz, p->sh_poff, p->sh_nprim, p->expn, p->ncoef,
+            p->npair, p->pair_ab, p->info, p->pp_src, p->sh_xyz, p->sh_poff, p->expn, p->ncoef,
             std::sqrt(2.0) * std::pow(M_PI, 1.25), p->pp, p->geo);
         if (int rc = mark(launches, "build_pairs", 1)) return rc;
         ++launches;
     }
-    PairTab P{p->info, p->geo, p->pp};
+    PairTab P{p->info, p->geo, p->pp, p->bnd};
     BoysTab B = boys_of(ctx, p->opts.boys);
-    // The primitive Schwarz sums decide screening and FP32 quartets; a plain FP64 plan
-    // without screening uses neither and skips the pass.
-    const bool need_bounds = p->opts.precision == MOLINTS_MIXED || p->opts.screen_cutoff > 0.0;
-    for (int c = 0; need_bounds && c < kNumPairClasses; ++c) {
-        const int n = p->class_start[c + 1] - p->class_start[c];
-        if (n > 0) {
-            if (int rc = mark(launches, kSchwarzNames[c], 0)) return rc;
-            kSchwarzLaunchers[c](P, B, p->class_start[c], n, p->geo, nullptr, 0, s);
-            if (int rc = mark(launches, kSchwarzNames[c], 1)) return rc;
-            ++launches;
-        }
-    }
     const int mixed = p->opts.precision == MOLINTS_MIXED ? 1 : 0;
     for (int x = 0; x < kNumPairClasses; ++x) {
         const int nx = p->class_start[x + 1] - p->class_start[x];
@@ -537,22 +623,19 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
     for (int k = 0; k < p->npair; ++k) { sum += p->npp_h[k]; sum2 += (int64_t)p->npp_h[k] * p->npp_h[k]; }
     st->n_prim_quartets = (sum * sum + sum2) / 2;
     st->n_kernel_launches = p->n_launches;
+    st->n_prim_pairs = p->nprim_pair_all;
+    st->n_prim_pairs_kept = p->nprim_pair_kept;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return MOLINTS_ERR_CUDA;
-    if (cudaEventSynchronize(ctx->ev1) == cudaSuccess) {
+    if (p->n_launches > 0 && cudaEventSynchronize(ctx->ev1) == cudaSuccess) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) st->device_ms = ms;
     }
-    if (p->opts.precision == MOLINTS_MIXED || p->opts.screen_cutoff > 0.0) {
-        std::vector<double4> g(p->npair);
-        if (cudaMemcpy(g.data(), p->geo, p->npair * sizeof(double4), cudaMemcpyDeviceToHost) != cudaSuccess)
-            return MOLINTS_ERR_CUDA;
-        for (int a = 0; a < p->npair; ++a)
-            for (int c = 0; c <= a; ++c) {
-                const double bnd = g[a].w * g[c].w;
-                if (bnd < p->opts.screen_cutoff) ++st->n_screened;
-                else if (p->opts.precision == MOLINTS_MIXED && bnd < p->opts.fp32_cutoff) ++st->n_fp32_quartets;
-            }
-    }
+    for (int a = 0; a < p->npair; ++a)
+        for (int c = 0; c <= a; ++c) {
+            if (p->bnd_h[a].x * p->bnd_h[c].x < p->opts.screen_cutoff) ++st->n_screened;
+            else if (p->opts.precision == MOLINTS_MIXED && p->bnd_h[a].y * p->bnd_h[c].y < p->opts.fp32_cutoff)
+                ++st->n_fp32_quartets;
+        }
     return MOLINTS_OK;
 }
 
@@ -585,7 +668,7 @@ int molints_plan_schwarz(molints_plan *p, double *out) {
         int rc = dev_alloc(ctx, &p->qcon, (size_t)p->npair, &p->bytes);
         if (rc) return rc;
     }
-    PairTab P{p->info, p->geo, p->pp};
+    PairTab P{p->info, p->geo, p->pp, p->bnd};
     BoysTab B = boys_of(ctx, p->opts.boys);
     for (int c = 0; c < kNumPairClasses; ++c) {
         const int n = p->class_start[c + 1] - p->class_start[c];

@@ -52,14 +52,19 @@ class Basis(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("boys", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("fp32_cutoff", ctypes.c_double), ("screen_cutoff", ctypes.c_double)]
+                ("fp32_cutoff", ctypes.c_double), ("screen_cutoff", ctypes.c_double),
+                ("prim_cutoff", ctypes.c_double)]
+
+
+PRIM_CUTOFF = 1e-18
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("n_eri", ctypes.c_int64), ("n_shell_quartets", ctypes.c_int64),
                 ("n_prim_quartets", ctypes.c_int64), ("n_fp32_quartets", ctypes.c_int64),
                 ("n_screened", ctypes.c_int64), ("n_kernel_launches", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("device_ms", ctypes.c_double)]
+                ("reserved", ctypes.c_int32), ("device_ms", ctypes.c_double),
+                ("n_prim_pairs", ctypes.c_int64), ("n_prim_pairs_kept", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -125,8 +130,9 @@ class _BasisArrays:
 
 
 def make_options(precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0, screen_cutoff=0.0,
-                 method=METHOD_AUTO) -> Options:
-    return Options(method, precision, boys, 0, float(fp32_cutoff), float(screen_cutoff))
+                 method=METHOD_AUTO, prim_cutoff=PRIM_CUTOFF) -> Options:
+    return Options(method, precision, boys, 0, float(fp32_cutoff), float(screen_cutoff),
+                   float(prim_cutoff))
 
 
 class Plan:
@@ -210,7 +216,8 @@ class Engine:
         self._check(self.lib.molints_set_stream(self.ctx, h))
 
     def eri_packed(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
-                   screen_cutoff=0.0, out: np.ndarray | None = None, with_stats=False):
+                   screen_cutoff=0.0, out: np.ndarray | None = None, with_stats=False,
+                   prim_cutoff=PRIM_CUTOFF):
         """The packed iindex vector of all unique integrals, into a host array."""
         arrs = _BasisArrays(shells)
         if out is None:
@@ -222,24 +229,25 @@ class Engine:
             return (out, st.as_dict()) if with_stats else out
         if out.dtype != np.float64 or out.size != shells.npacked or not out.flags.c_contiguous:
             raise ValueError("out must be a contiguous float64 array of npacked elements")
-        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, prim_cutoff=prim_cutoff)
         st = Stats()
         self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
                                                 _ptr(out), 0, ctypes.byref(st)))
         return (out, st.as_dict()) if with_stats else out
 
     def eri_packed_device(self, shells, out_device_ptr: int, precision=FP64, boys=BOYS_REFERENCE,
-                          fp32_cutoff=0.0, screen_cutoff=0.0):
+                          fp32_cutoff=0.0, screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF):
         arrs = _BasisArrays(shells)
-        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, prim_cutoff=prim_cutoff)
         st = Stats()
         self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
                                                 ctypes.c_void_p(out_device_ptr), 1, ctypes.byref(st)))
         return st.as_dict()
 
     def plan(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
-             screen_cutoff=0.0) -> Plan:
-        return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff))
+             screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF) -> Plan:
+        return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff,
+                                               prim_cutoff=prim_cutoff))
 
     def boys(self, mmax: int, T, mode=BOYS_REFERENCE) -> np.ndarray:
         T = np.ascontiguousarray(T, dtype=np.float64)

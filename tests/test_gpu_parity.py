@@ -155,14 +155,28 @@ def test_split_valence_24_sampled(eng, oracle):
     assert np.all(np.abs(got) <= bound * (1 + 1e-10) + 1e-14)
 
 
-@pytest.mark.parametrize("cutoff", [1e-4, 1e-3])
-def test_mixed_precision_error_bound(eng, oracle, cutoff):
-    from molints_b200 import engine
-    sh = mi.config2()
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+def test_mixed_precision_error_bound(eng, cfg):
+    """The tuned FP32 cutoff keeps max |MIXED - FP64| below 1e-9 Eh and uses FP32."""
+    from molints_b200 import autotune, engine
+    sh = getattr(mi, cfg)()
+    cut, table = autotune.tune_fp32_cutoff(eng, sh)
+    assert cut > 0, table
     ref = eng.eri_packed(sh)
-    got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cutoff, with_stats=True)
+    got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cut, with_stats=True)
     assert st["n_fp32_quartets"] > 0
     assert np.max(np.abs(got - ref)) < TOL_MIXED
+
+
+def test_primitive_screening_bound(eng, oracle):
+    """Dropping primitive pairs with b_i * max Qabs < 1e-18 changes no integral by more than
+    1e-15, and removes a large share of config 1's primitive pairs."""
+    sh = mi.config1()
+    full, st0 = eng.eri_packed(sh, prim_cutoff=0.0, with_stats=True)
+    scr, st1 = eng.eri_packed(sh, with_stats=True)
+    assert st0["n_prim_pairs_kept"] == st0["n_prim_pairs"]
+    assert st1["n_prim_pairs_kept"] < 0.7 * st1["n_prim_pairs"]
+    assert np.max(np.abs(full - scr)) < 1e-15
 
 
 def test_screening_writes_zeros(eng):
