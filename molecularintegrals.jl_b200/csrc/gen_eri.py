@@ -25,6 +25,10 @@ HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE / "generated"
 LMAX = 2            # shell angular momentum supported by the generated kernels
 LTAB = 2 * LMAX     # AO tables must reach la + lb
+# Classes whose VRR has fewer entries than this get no FP32 variant: their primitive
+# quartet is dominated by the FP64 prefactors and Boys function, so an FP32 VRR would only
+# add registers and divergence.  MIXED plans run them in FP64.
+MIXED_MIN_VRR = 40
 
 
 # ------------------------------------------------------------------ AO tables
@@ -325,6 +329,12 @@ void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, do
     schwarz_kernel_{tag}<<<(np + 127) / 128, 128, 0, s>>>(P, B, p0, np, pbound, qout, full);
 }}
 """
+    if len(entries) >= MIXED_MIN_VRR:
+        mixed_dispatch = ("    if (mixed) eri_kernel_{t}<1><<<(unsigned)blocks, 128, 0, s>>>(L);\n"
+                          "    else eri_kernel_{t}<0><<<(unsigned)blocks, 128, 0, s>>>(L);").format(t=tag)
+    else:
+        mixed_dispatch = ("    (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)\n"
+                          "    eri_kernel_{t}<0><<<(unsigned)blocks, 128, 0, s>>>(L);").format(t=tag)
     return f"""// Generated by gen_eri.py -- class ({'spdfg'[la]}{'spdfg'[lb]}|{'spdfg'[lc]}{'spdfg'[ld]}).  Do not edit.
 // VRR entries: {len(entries)}, contracted block: {nacc}, HRR lines: {len(hp.lines)}, outputs: {nout}.
 #include "../eri_common.cuh"
@@ -415,8 +425,7 @@ __global__ void __launch_bounds__(128) eri_kernel_{tag}(const EriLaunch L) {{
 void launch_eri_{tag}(const EriLaunch &L, int mixed, cudaStream_t s) {{
     if (L.nquart <= 0) return;
     const long long blocks = (L.nquart + 127) / 128;
-    if (mixed) eri_kernel_{tag}<1><<<(unsigned)blocks, 128, 0, s>>>(L);
-    else eri_kernel_{tag}<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+{mixed_dispatch}
 }}
 {schwarz}
 }}  // namespace molints

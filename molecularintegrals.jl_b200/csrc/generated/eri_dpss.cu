@@ -223,8 +223,8 @@ __global__ void __launch_bounds__(128) eri_kernel_dpss(const EriLaunch L) {
 void launch_eri_dpss(const EriLaunch &L, int mixed, cudaStream_t s) {
     if (L.nquart <= 0) return;
     const long long blocks = (L.nquart + 127) / 128;
-    if (mixed) eri_kernel_dpss<1><<<(unsigned)blocks, 128, 0, s>>>(L);
-    else eri_kernel_dpss<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+    (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)
+    eri_kernel_dpss<0><<<(unsigned)blocks, 128, 0, s>>>(L);
 }
 
 }  // namespace molints

@@ -103,8 +103,8 @@ __global__ void __launch_bounds__(128) eri_kernel_psss(const EriLaunch L) {
 void launch_eri_psss(const EriLaunch &L, int mixed, cudaStream_t s) {
     if (L.nquart <= 0) return;
     const long long blocks = (L.nquart + 127) / 128;
-    if (mixed) eri_kernel_psss<1><<<(unsigned)blocks, 128, 0, s>>>(L);
-    else eri_kernel_psss<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+    (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)
+    eri_kernel_psss<0><<<(unsigned)blocks, 128, 0, s>>>(L);
 }
 
 }  // namespace molints

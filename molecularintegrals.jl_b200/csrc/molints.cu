@@ -35,6 +35,10 @@ struct molints_ctx {
     double *out_cache = nullptr;  // device buffer for host-output calls
     int64_t out_cache_len = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // class-pair kernels run concurrently on side streams forked from `stream`
+    static constexpr int kSide = 6;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork = nullptr, join[kSide] = {};
     std::string err;
 };
 
@@ -46,6 +50,7 @@ struct molints_plan {
     int npair = 0;
     int64_t nprim_pair_all = 0, nprim_pair_kept = 0;
     int class_start[kNumPairClasses + 1] = {0};
+    double class_cost[kNumPairClasses][kNumPairClasses] = {};  // kept primitive quartets
     // host copies (final, screened order)
     std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
     std::vector<int> npp_h;            // kept primitive pairs per shell pair
@@ -153,12 +158,15 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
         r.zeta = zeta;
         r.kab = c0 * ca * cb * exp(-a * b * ooz * rab2) * ooz;
         r.oo2z = 0.5 * ooz;
-        r.px = (a * Ax + b * Bx) * ooz;
-        r.py = (a * Ay + b * By) * ooz;
-        r.pz = (a * Az + b * Bz) * ooz;
-        r.pax = r.px - Ax;
-        r.pay = r.py - Ay;
-        r.paz = r.pz - Az;
+        // P = A + (b/zeta)(B - A): P - A is exactly 0 when A == B, and P - Q exactly 0 when
+        // all four centres coincide, so symmetry-zero one-centre integrals come out as 0.
+        const double boz = b * ooz;
+        r.pax = boz * (Bx - Ax);
+        r.pay = boz * (By - Ay);
+        r.paz = boz * (Bz - Az);
+        r.px = Ax + r.pax;
+        r.py = Ay + r.pay;
+        r.pz = Az + r.paz;
         r.pad = 0.0;
         pp[k] = r;
     }
@@ -223,8 +231,13 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
     ctx->budget = budget;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) { delete ctx; return MOLINTS_ERR_CUDA; }
-    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreate(&ctx->ev0) == cudaSuccess && cudaEventCreate(&ctx->ev1) == cudaSuccess &&
+              cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; ok && i < molints_ctx::kSide; ++i)
+        ok = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ctx->join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         molints_destroy(ctx);
         return MOLINTS_ERR_CUDA;
     }
@@ -253,6 +266,12 @@ int molints_destroy(molints_ctx *ctx) {
     if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
     if (ctx->boys_tab) cudaFree(ctx->boys_tab);
     if (ctx->out_cache) cudaFree(ctx->out_cache);
+    for (int i = 0; i < molints_ctx::kSide; ++i) {
+        if (ctx->side[i]) cudaStreamSynchronize(ctx->side[i]);
+        if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+        if (ctx->join[i]) cudaEventDestroy(ctx->join[i]);
+    }
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -537,6 +556,20 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
         p->npp_h[k] = pr[k].npp;
         p->bnd_h[k] = bnd_ref[pr[k].ref];
     }
+    {
+        // launch-order estimate: kept primitive quartets x per-class weight (VRR size)
+        std::vector<double> ksum(kNumPairClasses, 0.0), k2sum(kNumPairClasses, 0.0);
+        for (int k = 0; k < npair; ++k) {
+            ksum[pr[k].cls] += pr[k].npp;
+            k2sum[pr[k].cls] += (double)pr[k].npp * pr[k].npp;
+        }
+        for (int x = 0; x < kNumPairClasses; ++x)
+            for (int y = 0; y <= x; ++y) {
+                const double kq = (x == y) ? 0.5 * (ksum[x] * ksum[x] + k2sum[x]) : ksum[x] * ksum[y];
+                const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
+                p->class_cost[x][y] = kq * (1.0 + lsum * lsum);
+            }
+    }
     if ((e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->bnd, p->bnd_h.data(), npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
@@ -557,7 +590,7 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
     cudaStream_t s = ctx->stream;
     int launches = 0;
     // event pair around each launch when profiling (launch k uses events 2k, 2k+1)
-    auto mark = [&](int k, const char *name, int end) -> int {
+    auto mark = [&](int k, const char *name, int end, cudaStream_t st) -> int {
         if (!p->profiling) return 0;
         while ((int)p->prof_ev.size() < 2 * k + 2) {
             cudaEvent_t e;
@@ -567,44 +600,61 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         }
         if ((int)p->prof_name.size() < k + 1) p->prof_name.resize(k + 1);
         p->prof_name[k] = name;
-        cudaError_t err = cudaEventRecord(p->prof_ev[2 * k + end], s);
+        cudaError_t err = cudaEventRecord(p->prof_ev[2 * k + end], st);
         return err == cudaSuccess ? 0 : cuda_fail(ctx, err, "cudaEventRecord");
     };
     MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
     if (p->npair > 0) {
-        if (int rc = mark(launches, "build_pairs", 0)) return rc;
+        if (int rc = mark(launches, "build_pairs", 0, s)) return rc;
         build_pairs_kernel<<<(p->npair + 127) / 128, 128, 0, s>>>(
             p->npair, p->pair_ab, p->info, p->pp_src, p->sh_xyz, p->sh_poff, p->expn, p->ncoef,
             std::sqrt(2.0) * std::pow(M_PI, 1.25), p->pp, p->geo);
-        if (int rc = mark(launches, "build_pairs", 1)) return rc;
+        if (int rc = mark(launches, "build_pairs", 1, s)) return rc;
         ++launches;
     }
     PairTab P{p->info, p->geo, p->pp, p->bnd};
     BoysTab B = boys_of(ctx, p->opts.boys);
     const int mixed = p->opts.precision == MOLINTS_MIXED ? 1 : 0;
-    for (int x = 0; x < kNumPairClasses; ++x) {
-        const int nx = p->class_start[x + 1] - p->class_start[x];
-        if (nx == 0) continue;
+    // Class-pair launches, largest estimated work first, spread over the side streams so
+    // that small classes fill the SMs next to large ones.
+    struct Job { double cost; int x, y; };
+    std::vector<Job> jobs;
+    for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
+            const int nx = p->class_start[x + 1] - p->class_start[x];
             const int ny = p->class_start[y + 1] - p->class_start[y];
-            if (ny == 0) continue;
-            EriLaunch L{};
-            L.pairs = P;
-            L.boys = B;
-            L.out = out_device;
-            L.bra0 = p->class_start[x];
-            L.nbra = nx;
-            L.ket0 = p->class_start[y];
-            L.nket = ny;
-            L.tri = (x == y);
-            L.nquart = L.tri ? (long long)nx * (nx + 1) / 2 : (long long)nx * ny;
-            L.screen_cut = p->opts.screen_cutoff;
-            L.fp32_cut = p->opts.fp32_cutoff;
-            if (int rc = mark(launches, kEriNames[x][y], 0)) return rc;
-            kEriLaunchers[x][y](L, mixed, s);
-            if (int rc = mark(launches, kEriNames[x][y], 1)) return rc;
-            ++launches;
+            if (nx == 0 || ny == 0) continue;
+            jobs.push_back({p->class_cost[x][y], x, y});
         }
+    std::stable_sort(jobs.begin(), jobs.end(), [](const Job &a, const Job &b) { return a.cost > b.cost; });
+    const int nside = std::min<int>(molints_ctx::kSide, (int)jobs.size());
+    if (nside > 0) MI_CUDA(ctx, cudaEventRecord(ctx->fork, s));
+    for (int i = 0; i < nside; ++i) MI_CUDA(ctx, cudaStreamWaitEvent(ctx->side[i], ctx->fork, 0));
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        const int x = jobs[k].x, y = jobs[k].y;
+        const int nx = p->class_start[x + 1] - p->class_start[x];
+        const int ny = p->class_start[y + 1] - p->class_start[y];
+        cudaStream_t st = ctx->side[k % nside];
+        EriLaunch L{};
+        L.pairs = P;
+        L.boys = B;
+        L.out = out_device;
+        L.bra0 = p->class_start[x];
+        L.nbra = nx;
+        L.ket0 = p->class_start[y];
+        L.nket = ny;
+        L.tri = (x == y);
+        L.nquart = L.tri ? (long long)nx * (nx + 1) / 2 : (long long)nx * ny;
+        L.screen_cut = p->opts.screen_cutoff;
+        L.fp32_cut = p->opts.fp32_cutoff;
+        if (int rc = mark(launches, kEriNames[x][y], 0, st)) return rc;
+        kEriLaunchers[x][y](L, mixed, st);
+        if (int rc = mark(launches, kEriNames[x][y], 1, st)) return rc;
+        ++launches;
+    }
+    for (int i = 0; i < nside; ++i) {
+        MI_CUDA(ctx, cudaEventRecord(ctx->join[i], ctx->side[i]));
+        MI_CUDA(ctx, cudaStreamWaitEvent(s, ctx->join[i], 0));
     }
     MI_CUDA(ctx, cudaGetLastError());
     MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));

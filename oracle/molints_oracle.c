@@ -138,25 +138,38 @@ static long double upper_gamma_cf(long double a, long double x) {
     return h;
 }
 
-/* Fm(m,T), src/Boys.jl:29-34 (T < 1e-18 returns 1/(2m+1)). */
-double oracle_boys(int m, double T) {
-    if (T < 1e-18) return 1.0 / (2 * m + 1);
-    if (T > 50.0 && T > m + 1.5) {
+/* F_m(T) in long double: the everywhere convergent series below T = 50, the continued
+ * fraction for the upper incomplete gamma function above. */
+static long double boys_ld(int m, long double t) {
+    if (t < 1e-18L) return 1.0L / (2 * m + 1);
+    if (t > 50.0L && t > m + 1.5L) {
         /* F_m = (Gamma(m+1/2) - Gamma(m+1/2, T)) / (2 T^(m+1/2)) */
-        long double a = m + 0.5L, t = T;
+        long double a = m + 0.5L;
         long double g = sqrtl(3.14159265358979323846264338327950288L);
         for (int k = 1; k <= m; ++k) g *= (k - 0.5L);
         long double ta = powl(t, a);
         long double upper = expl(-t) * ta * upper_gamma_cf(a, t);
-        return (double)((g - upper) / (2.0L * ta));
+        return (g - upper) / (2.0L * ta);
     }
-    long double t = T, sum = 0.0L, term = 1.0L / (2 * m + 1);
+    long double sum = 0.0L, term = 1.0L / (2 * m + 1);
     for (int k = 0; k < 100000; ++k) {
         sum += term;
-        if (k > T && term < sum * 1e-22L) break;
+        if (k > t && term < sum * 1e-22L) break;
         term *= 2.0L * t / (2 * m + 2 * k + 3);
     }
-    return (double)(expl(-t) * sum);
+    return expl(-t) * sum;
+}
+
+/* Fm(m,T), src/Boys.jl:29-34 (T < 1e-18 returns 1/(2m+1)). */
+double oracle_boys(int m, double T) {
+    if (T < 1e-18) return 1.0 / (2 * m + 1);
+    return (double)boys_ld(m, T);
+}
+
+static long double boys_asymp_ld(int m, long double T) {
+    long double f2 = 1.0L;
+    for (int k = 2 * m - 1; k > 1; k -= 2) f2 *= k;
+    return sqrtl(3.14159265358979323846264338327950288L / 2) * f2 / powl(2 * T, m + 0.5L);
 }
 
 /* Fm_asymp, src/Boys.jl:36. */
@@ -170,129 +183,64 @@ static double g_boys_tmax = 30.0;
 void oracle_set_boys_tmax(double tmax) { g_boys_tmax = tmax; }
 double oracle_get_boys_tmax(void) { return g_boys_tmax; }
 
-/* farray(mmax,T), src/Boys.jl:19-27 with farray_recur :9-17; out[0..mmax-1] = F_0..F_mmax-1. */
-void oracle_farray(int mmax, double T, double *out) {
-    if (T < g_boys_tmax) {
-        out[mmax - 1] = oracle_boys(mmax - 1, T);
-        double emt = exp(-T);
-        for (int m = mmax - 2; m >= 0; --m) out[m] = (2 * T * out[m + 1] + emt) / (2 * m + 1);
-        return;
-    }
-    out[mmax - 1] = oracle_boys_asymp(mmax - 1, T);
-    for (int m = mmax - 2; m >= 0; --m) out[m] = T * out[m + 1] / (m + 0.5);
-}
+/* Orientation of each shell quartet handed to chrr.  0 (default): the reference's, chrr(I,J,K,L)
+ * with I >= J, K >= L, pair(IJ) >= pair(KL) by shell index (src/HGP.jl:27-28).  1: the
+ * engine's: in each pair the shell with the larger L is 'a' (ties keep the higher index
+ * first), and the pair of higher class (la+lb, then la) is the bra.  The two are the same
+ * mathematics; their rounding differs, and HRR accuracy depends strongly on which shell
+ * receives the transferred angular momentum. */
+static int g_orient = 0;
+void oracle_set_orientation(int mode) { g_orient = mode; }
+int oracle_get_orientation(void) { return g_orient; }
 
-/* ---------------------------------------------------------------- HGP VRR / HRR */
+/* ---------------------------------------------------------------- the HGP core, twice */
 
-static inline double dist2(const double *a, const double *b) {
-    double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
-    return dx * dx + dy * dy + dz * dz;
-}
+static inline int64_t tri64(int64_t i) { return i * (i + 1) / 2; }
+int64_t oracle_iindex(int64_t i, int64_t j, int64_t k, int64_t l);
+size_t oracle_hrr_size(int la, int lb, int lc, int ld);
 
-/* vrr!(vrrs, amax, cmax, ...), src/HGP.jl:135-242.  vrrs is [mmax][nao(amax)][nao(cmax)]
- * (m fastest in the reference; slowest here -- the layout is internal).
- * prefactor_mode 0: HGP prefactor 2 pi^2.5/(zeta eta sqrt(zeta+eta)) (D5 fixed);
- * prefactor_mode 1: the literal src/HGP.jl:150 expression 2 pi^2.5 (zeta+eta)^-3/2. */
+#define REAL double
+#define PFX(name) d_##name
+#define R_EXP exp
+#define R_SQRT sqrt
+#define R_POW pow
+#define R_PI M_PI
+#define BOYS_EXACT(m, T) oracle_boys((m), (T))
+#define BOYS_ASYMP(m, T) oracle_boys_asymp((m), (T))
+#include "hgp_core.h"
+#undef REAL
+#undef PFX
+#undef R_EXP
+#undef R_SQRT
+#undef R_POW
+#undef R_PI
+#undef BOYS_EXACT
+#undef BOYS_ASYMP
+
+#define REAL long double
+#define PFX(name) ld_##name
+#define R_EXP expl
+#define R_SQRT sqrtl
+#define R_POW powl
+#define R_PI 3.14159265358979323846264338327950288L
+#define BOYS_EXACT(m, T) boys_ld((m), (T))
+#define BOYS_ASYMP(m, T) boys_asymp_ld((m), (T))
+#include "hgp_core.h"
+#undef REAL
+#undef PFX
+#undef R_EXP
+#undef R_SQRT
+#undef R_POW
+#undef R_PI
+#undef BOYS_EXACT
+#undef BOYS_ASYMP
+
+void oracle_farray(int mmax, double T, double *out) { d_farray(mmax, T, out); }
+
 void oracle_vrr(int amax, int cmax, double aexpn, double bexpn, double cexpn, double dexpn,
                 const double *A, const double *B, const double *C, const double *D,
                 int prefactor_mode, double *vrrs) {
-    oracle_init();
-    const int mmax = amax + cmax + 1;
-    const int nA = g_nao[amax], nC = g_nao[cmax];
-#define V(m, a, c) vrrs[((size_t)(m) * nA + (a)) * nC + (c)]
-    memset(vrrs, 0, sizeof(double) * (size_t)mmax * nA * nC);
-    double zeta = aexpn + bexpn, eta = cexpn + dexpn, ze = zeta + eta;
-    double ooz = 1 / zeta, ooe = 1 / eta, ooze = 1 / ze, oortze = sqrt(ooze);
-    double P[3], Q[3], W[3], PA[3], WP[3], QC[3], WQ[3];
-    for (int i = 0; i < 3; ++i) {
-        P[i] = (aexpn * A[i] + bexpn * B[i]) * ooz;
-        Q[i] = (cexpn * C[i] + dexpn * D[i]) * ooe;
-        W[i] = (zeta * P[i] + eta * Q[i]) * ooze;
-        PA[i] = P[i] - A[i]; WP[i] = W[i] - P[i]; QC[i] = Q[i] - C[i]; WQ[i] = W[i] - Q[i];
-    }
-    double rab2 = dist2(A, B), rcd2 = dist2(C, D), rpq2 = dist2(P, Q);
-    double T = zeta * eta * rpq2 * ooze;
-    double ex = exp(-aexpn * bexpn * rab2 * ooz - cexpn * dexpn * rcd2 * ooe);
-    double pref = (prefactor_mode == 1) ? 2 * M_PI * M_PI * sqrt(M_PI) * ooze * oortze * ex
-                                        : 2 * M_PI * M_PI * sqrt(M_PI) * ooz * ooe * oortze * ex;
-    double Fms[64];
-    oracle_farray(mmax, T, Fms);
-    for (int m = 0; m < mmax; ++m) V(m, 0, 0) = pref * Fms[m];
-    if (mmax == 1) return;
-    /* a-build, eq. 6a with c = 0: src/HGP.jl:180-197 */
-    for (int aplus = 1; aplus < nA; ++aplus) {
-        int ashell = g_shell_number[aplus];
-        int i = g_shift_dir[aplus];
-        int a = g_shift_index[aplus][i];
-        int lim = mmax - ashell;
-        int aminus = g_shift_index[a][i];
-        if (aminus >= 0) {
-            double a_i = 0.5 * ooz * g_ao2m[a][i];
-            for (int m = 0; m < lim; ++m)
-                V(m, aplus, 0) = PA[i] * V(m, a, 0) + WP[i] * V(m + 1, a, 0) +
-                                 a_i * (V(m, aminus, 0) - eta * ooze * V(m + 1, aminus, 0));
-        } else {
-            for (int m = 0; m < lim; ++m)
-                V(m, aplus, 0) = PA[i] * V(m, a, 0) + WP[i] * V(m + 1, a, 0);
-        }
-    }
-    /* c-build, eq. 6d: src/HGP.jl:204-240 */
-    for (int cplus = 1; cplus < nC; ++cplus) {
-        int cshell = g_shell_number[cplus];
-        int i = g_shift_dir[cplus];
-        int c = g_shift_index[cplus][i];
-        int cminus = g_shift_index[c][i];
-        for (int a = 0; a < nA; ++a) {
-            int ashell = g_shell_number[a];
-            int lim = mmax - cshell - ashell;
-            int aminus = g_shift_index[a][i];
-            double c_i = (cminus >= 0) ? 0.5 * ooe * g_ao2m[c][i] : 0.0;
-            double a_i = (aminus >= 0) ? 0.5 * ooze * g_ao2m[a][i] : 0.0;
-            for (int m = 0; m < lim; ++m) {
-                double v = QC[i] * V(m, a, c) + WQ[i] * V(m + 1, a, c);
-                if (aminus >= 0) v += a_i * V(m + 1, aminus, c);
-                if (cminus >= 0) v += c_i * (V(m, a, cminus) - zeta * ooze * V(m + 1, a, cminus));
-                V(m, a, cplus) = v;
-            }
-        }
-    }
-#undef V
-}
-
-/* HRR on a contracted or primitive [a0|c0] block (the loops of chrr, src/HGP.jl:87-114,
- * identical to hrr, :395-422).  vrr0 is [nao(la+lb)][nao(lc+ld)]; hrrs is
- * [nao(la+lb)][nao(lb)][nao(lc+ld)][nao(ld)] in cumulative AO indices. */
-static void hrr_block(int la, int lb, int lc, int ld, const double *A, const double *B,
-                      const double *C, const double *D, const double *vrr0, double *hrrs) {
-    const int n1 = g_nao[la + lb], n2 = g_nao[lb], n3 = g_nao[lc + ld], n4 = g_nao[ld];
-#define H(a, b, c, d) hrrs[(((size_t)(a) * n2 + (b)) * n3 + (c)) * n4 + (d)]
-    memset(hrrs, 0, sizeof(double) * (size_t)n1 * n2 * n3 * n4);
-    for (int c = 0; c < n3; ++c)
-        for (int a = 0; a < n1; ++a) H(a, 0, c, 0) = vrr0[(size_t)a * n3 + c];
-    for (int c = 0; c < n3; ++c)
-        for (int bplus = 1; bplus < n2; ++bplus) {
-            int j = g_shift_dir[bplus];
-            int b = g_shift_index[bplus][j];
-            int bs = g_shell_number[b];
-            int alim = g_nao[la + lb - bs - 1];
-            for (int a = 0; a < alim; ++a) {
-                int aplus = g_shift_plus[a][j];
-                H(a, bplus, c, 0) = H(aplus, b, c, 0) + (A[j] - B[j]) * H(a, b, c, 0);
-            }
-        }
-    for (int dplus = 1; dplus < n4; ++dplus) {
-        int j = g_shift_dir[dplus];
-        int d = g_shift_index[dplus][j];
-        int ds = g_shell_number[d];
-        int clim = g_nao[lc + ld - ds - 1];
-        for (int c = 0; c < clim; ++c) {
-            int cplus = g_shift_plus[c][j];
-            for (int b = 0; b < n2; ++b)
-                for (int a = 0; a < g_nao[la]; ++a)
-                    H(a, b, c, dplus) = H(a, b, cplus, d) + (C[j] - D[j]) * H(a, b, c, d);
-        }
-    }
-#undef H
+    d_vrr(amax, cmax, aexpn, bexpn, cexpn, dexpn, A, B, C, D, prefactor_mode, vrrs);
 }
 
 size_t oracle_hrr_size(int la, int lb, int lc, int ld) {
@@ -308,9 +256,61 @@ void oracle_hrr(int la, int lb, int lc, int ld, double aexpn, double bexpn, doub
     int amax = la + lb, cmax = lc + ld, mmax = amax + cmax + 1;
     size_t nv = (size_t)mmax * g_nao[amax] * g_nao[cmax];
     double *v = (double *)malloc(sizeof(double) * nv);
-    oracle_vrr(amax, cmax, aexpn, bexpn, cexpn, dexpn, A, B, C, D, prefactor_mode, v);
-    hrr_block(la, lb, lc, ld, A, B, C, D, v, hrrs); /* m = 0 slice is the first block */
+    d_vrr(amax, cmax, aexpn, bexpn, cexpn, dexpn, A, B, C, D, prefactor_mode, v);
+    d_hrr_block(la, lb, lc, ld, A, B, C, D, v, hrrs); /* m = 0 slice is the first block */
     free(v);
+}
+
+static int64_t eri_packed_hgp_dispatch(int nshell, const double *xyz, const int *L, const int *nprim,
+                                   const int *prim_off, const double *expn, const double *coef,
+                                   double *out, int nthreads, int64_t stride);
+
+int oracle_eri_packed_hgp(int nshell, const double *xyz, const int *L, const int *nprim,
+                          const int *prim_off, const double *expn, const double *coef,
+                          double *out, int nthreads) {
+    int64_t r = eri_packed_hgp_dispatch(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads, 1);
+    return r < 0 ? (int)r : 0;
+}
+
+/* The same driver over every stride-th shell quartet only (a bounded CPU-baseline sample);
+ * returns the number of integrals written, or -1. */
+int64_t oracle_eri_packed_hgp_sample(int nshell, const double *xyz, const int *L,
+                                     const int *nprim, const int *prim_off, const double *expn,
+                                     const double *coef, double *out, int nthreads,
+                                     int64_t stride) {
+    return eri_packed_hgp_dispatch(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads,
+                               stride < 1 ? 1 : stride);
+}
+
+
+/* Dispatch of the HGP driver: FP64 (the oracle proper) or long double (near-exact). */
+static int g_use_ld = 0;
+static int64_t eri_packed_hgp_dispatch(int nshell, const double *xyz, const int *L, const int *nprim,
+                                       const int *prim_off, const double *expn, const double *coef,
+                                       double *out, int nthreads, int64_t stride) {
+    if (!g_use_ld)
+        return d_eri_packed_hgp_impl(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads, stride);
+    return ld_eri_packed_hgp_impl(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads, stride);
+}
+
+/* all_twoe_ints_chrr restated as above, evaluated in long double (64-bit mantissa). */
+int oracle_eri_packed_hgp_ld(int nshell, const double *xyz, const int *L, const int *nprim,
+                             const int *prim_off, const double *expn, const double *coef,
+                             double *out, int nthreads) {
+    int64_t r = ld_eri_packed_hgp_impl(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads, 1);
+    return r < 0 ? (int)r : 0;
+}
+
+/* One contracted, normalised shell quartet (ab|cd), out[ma][mb][mc][md]. */
+int oracle_shell_quartet(int nshell, const double *xyz, const int *L, const int *nprim,
+                         const int *prim_off, const double *expn, const double *coef,
+                         int sa, int sb, int sc, int sd, double *out) {
+    oracle_init();
+    d_basis b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0, 0, 0};
+    d_basis_prepare(&b);
+    d_shell_quartet(&b, sa, sb, sc, sd, out);
+    d_basis_release(&b);
+    return 0;
 }
 
 /* ---------------------------------------------------------------- normalisation */
@@ -339,7 +339,6 @@ double oracle_cgbf_norm(int L, int nprim, const double *expn, const double *coef
 
 /* ---------------------------------------------------------------- packed layout */
 
-static inline int64_t tri64(int64_t i) { return i * (i + 1) / 2; }
 /* 0-based iindex (src/Utils.jl:14-19 minus one). */
 int64_t oracle_iindex(int64_t i, int64_t j, int64_t k, int64_t l) {
     int64_t ij = i >= j ? tri64(i) + j : tri64(j) + i;
@@ -347,189 +346,6 @@ int64_t oracle_iindex(int64_t i, int64_t j, int64_t k, int64_t l) {
     return ij >= kl ? tri64(ij) + kl : tri64(kl) + ij;
 }
 int64_t oracle_npacked(int64_t n) { return n * (n + 1) * (n * n + n + 2) / 8; }
-
-/* ---------------------------------------------------------------- contracted HGP */
-
-typedef struct {
-    int nshell;
-    const double *xyz; const int *L; const int *nprim; const int *prim_off;
-    const double *expn; const double *coef;
-    /* derived */
-    double *ncoef;  /* coef * radial primitive norm * CGBF norm */
-    int *fn_off;    /* first function index of each shell */
-    int nbf;
-} oracle_basis;
-
-static void basis_prepare(oracle_basis *b) {
-    int nprim_tot = 0;
-    for (int s = 0; s < b->nshell; ++s)
-        if (b->prim_off[s] + b->nprim[s] > nprim_tot) nprim_tot = b->prim_off[s] + b->nprim[s];
-    b->ncoef = (double *)malloc(sizeof(double) * (nprim_tot > 0 ? nprim_tot : 1));
-    b->fn_off = (int *)malloc(sizeof(int) * (b->nshell + 1));
-    int off = 0;
-    for (int s = 0; s < b->nshell; ++s) {
-        int L = b->L[s], p0 = b->prim_off[s];
-        double cn = oracle_cgbf_norm(L, b->nprim[s], b->expn + p0, b->coef + p0);
-        for (int p = 0; p < b->nprim[s]; ++p) {
-            double a = b->expn[p0 + p];
-            b->ncoef[p0 + p] = b->coef[p0 + p] * cn * pow(2 * a / M_PI, 0.75) * pow(4 * a, 0.5 * L);
-        }
-        b->fn_off[s] = off;
-        off += g_ncart[L];
-    }
-    b->fn_off[b->nshell] = off;
-    b->nbf = off;
-}
-static void basis_release(oracle_basis *b) { free(b->ncoef); free(b->fn_off); }
-
-static double comp_factor(int a) { /* 1/sqrt((2I-1)!!(2J-1)!!(2K-1)!!) */
-    return 1.0 / sqrt(dfact2(2 * g_ao2m[a][0] - 1) * dfact2(2 * g_ao2m[a][1] - 1) *
-                      dfact2(2 * g_ao2m[a][2] - 1));
-}
-
-/* chrr(ash,bsh,csh,dsh) with cvrr, src/HGP.jl:50-116, on normalised coefficients (D3),
- * returning (ab|cd) for the shells' own components, out[ma][mb][mc][md] (D2). */
-static void shell_quartet(const oracle_basis *b, int sa, int sb, int sc, int sd, double *out) {
-    int la = b->L[sa], lb = b->L[sb], lc = b->L[sc], ld = b->L[sd];
-    int amax = la + lb, cmax = lc + ld, mmax = amax + cmax + 1;
-    int nA = g_nao[amax], nC = g_nao[cmax];
-    const double *A = b->xyz + 3 * sa, *B = b->xyz + 3 * sb, *C = b->xyz + 3 * sc,
-                 *D = b->xyz + 3 * sd;
-    double *vrrs = (double *)malloc(sizeof(double) * (size_t)mmax * nA * nC);
-    double *cvrrs = (double *)calloc((size_t)nA * nC, sizeof(double));
-    for (int pd = 0; pd < b->nprim[sd]; ++pd)
-        for (int pc = 0; pc < b->nprim[sc]; ++pc)
-            for (int pb = 0; pb < b->nprim[sb]; ++pb)
-                for (int pa = 0; pa < b->nprim[sa]; ++pa) {
-                    int ia = b->prim_off[sa] + pa, ib = b->prim_off[sb] + pb;
-                    int ic = b->prim_off[sc] + pc, id = b->prim_off[sd] + pd;
-                    oracle_vrr(amax, cmax, b->expn[ia], b->expn[ib], b->expn[ic], b->expn[id],
-                               A, B, C, D, 0, vrrs);
-                    double cf = b->ncoef[ia] * b->ncoef[ib] * b->ncoef[ic] * b->ncoef[id];
-                    for (size_t x = 0; x < (size_t)nA * nC; ++x) cvrrs[x] += cf * vrrs[x];
-                }
-    size_t nh = oracle_hrr_size(la, lb, lc, ld);
-    double *hrrs = (double *)malloc(sizeof(double) * nh);
-    hrr_block(la, lb, lc, ld, A, B, C, D, cvrrs, hrrs);
-    const int n2 = g_nao[lb], n3 = g_nao[lc + ld], n4 = g_nao[ld];
-    int oa = la ? g_nao[la - 1] : 0, ob = lb ? g_nao[lb - 1] : 0;
-    int oc = lc ? g_nao[lc - 1] : 0, od = ld ? g_nao[ld - 1] : 0;
-    int x = 0;
-    for (int ma = 0; ma < g_ncart[la]; ++ma)
-        for (int mb = 0; mb < g_ncart[lb]; ++mb)
-            for (int mc = 0; mc < g_ncart[lc]; ++mc)
-                for (int md = 0; md < g_ncart[ld]; ++md, ++x) {
-                    int a = oa + ma, bb = ob + mb, c = oc + mc, d = od + md;
-                    out[x] = hrrs[(((size_t)a * n2 + bb) * n3 + c) * n4 + d] * comp_factor(a) *
-                             comp_factor(bb) * comp_factor(c) * comp_factor(d);
-                }
-    free(vrrs); free(cvrrs); free(hrrs);
-}
-
-/* Orientation of each shell quartet handed to chrr.  0 (default): the reference's, chrr(I,J,K,L)
- * with I >= J, K >= L, pair(IJ) >= pair(KL) by shell index (src/HGP.jl:27-28).  1: the
- * engine's: in each pair the shell with the larger L is 'a' (ties keep the higher index
- * first), and the pair of higher class (la+lb, then la) is the bra.  The two are the same
- * mathematics; their rounding differs, and HRR accuracy depends strongly on which shell
- * receives the transferred angular momentum. */
-static int g_orient = 0;
-void oracle_set_orientation(int mode) { g_orient = mode; }
-int oracle_get_orientation(void) { return g_orient; }
-
-/* all_twoe_ints_chrr, src/HGP.jl:22-34, with D1-D3 and D5 fixed: every unique shell
- * quartet (I>=J, K>=L, pair(IJ)>=pair(KL)) is computed once and scattered to the 0-based
- * iindex positions.  nthreads > 1 uses OpenMP with a dynamic schedule, the analogue of
- * the reference's Threads.@threads over shell quartets. */
-static int64_t eri_packed_hgp_impl(int nshell, const double *xyz, const int *L, const int *nprim,
-                                   const int *prim_off, const double *expn, const double *coef,
-                                   double *out, int nthreads, int64_t stride);
-
-int oracle_eri_packed_hgp(int nshell, const double *xyz, const int *L, const int *nprim,
-                          const int *prim_off, const double *expn, const double *coef,
-                          double *out, int nthreads) {
-    int64_t r = eri_packed_hgp_impl(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads, 1);
-    return r < 0 ? (int)r : 0;
-}
-
-/* The same driver over every stride-th shell quartet only (a bounded CPU-baseline sample);
- * returns the number of integrals written, or -1. */
-int64_t oracle_eri_packed_hgp_sample(int nshell, const double *xyz, const int *L,
-                                     const int *nprim, const int *prim_off, const double *expn,
-                                     const double *coef, double *out, int nthreads,
-                                     int64_t stride) {
-    return eri_packed_hgp_impl(nshell, xyz, L, nprim, prim_off, expn, coef, out, nthreads,
-                               stride < 1 ? 1 : stride);
-}
-
-static int64_t eri_packed_hgp_impl(int nshell, const double *xyz, const int *L, const int *nprim,
-                                   const int *prim_off, const double *expn, const double *coef,
-                                   double *out, int nthreads, int64_t stride) {
-    oracle_init();
-    oracle_basis b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0};
-    for (int s = 0; s < nshell; ++s)
-        if (L[s] < 0 || L[s] > 3 || nprim[s] < 1) return -1;
-    basis_prepare(&b);
-    int64_t npair = (int64_t)nshell * (nshell + 1) / 2;
-    int64_t nquart = npair * (npair + 1) / 2;
-    int *pi = (int *)malloc(sizeof(int) * npair), *pj = (int *)malloc(sizeof(int) * npair);
-    for (int i = 0, p = 0; i < nshell; ++i)
-        for (int j = 0; j <= i; ++j, ++p) { pi[p] = i; pj[p] = j; }
-    int64_t written = 0;
-#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : written)
-    {
-    double *buf = (double *)malloc(sizeof(double) * 15 * 15 * 15 * 15);
-#pragma omp for schedule(dynamic, 64)
-    for (int64_t q = 0; q < nquart; q += stride) {
-        int64_t p1 = (int64_t)((sqrt(8.0 * (double)q + 1.0) - 1.0) / 2.0);
-        while (tri64(p1) > q) --p1;
-        while (tri64(p1 + 1) <= q) ++p1;
-        int64_t p2 = q - tri64(p1);
-        int I = pi[p1], J = pj[p1], K = pi[p2], Lsh = pj[p2];
-        if (g_orient == 1) {
-            int t;
-            if (L[I] < L[J]) { t = I; I = J; J = t; }
-            if (L[K] < L[Lsh]) { t = K; K = Lsh; Lsh = t; }
-            int sb = L[I] + L[J], sk = L[K] + L[Lsh];
-            if (sk > sb || (sk == sb && L[K] > L[I])) {
-                t = I; I = K; K = t; t = J; J = Lsh; Lsh = t;
-            }
-        }
-        int na = g_ncart[L[I]], nb = g_ncart[L[J]], nc = g_ncart[L[K]], nd = g_ncart[L[Lsh]];
-        shell_quartet(&b, I, J, K, Lsh, buf);
-        int x = 0;
-        for (int ma = 0; ma < na; ++ma)
-            for (int mb = 0; mb < nb; ++mb)
-                for (int mc = 0; mc < nc; ++mc)
-                    for (int md = 0; md < nd; ++md, ++x) {
-                        int64_t i = b.fn_off[I] + ma, j = b.fn_off[J] + mb;
-                        int64_t k = b.fn_off[K] + mc, l = b.fn_off[Lsh] + md;
-                        if (I == J && i < j) continue;
-                        if (K == Lsh && k < l) continue;
-                        int64_t ij = i >= j ? tri64(i) + j : tri64(j) + i;
-                        int64_t kl = k >= l ? tri64(k) + l : tri64(l) + k;
-                        if (p1 == p2 && ij < kl) continue;
-                        out[oracle_iindex(i, j, k, l)] = buf[x];
-                        ++written;
-                    }
-    }
-    free(buf);
-    }
-    free(pi); free(pj);
-    basis_release(&b);
-    return written;
-}
-
-/* One contracted, normalised shell quartet (ab|cd), out[ma][mb][mc][md]. */
-int oracle_shell_quartet(int nshell, const double *xyz, const int *L, const int *nprim,
-                         const int *prim_off, const double *expn, const double *coef,
-                         int sa, int sb, int sc, int sd, double *out) {
-    oracle_init();
-    oracle_basis b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0};
-    basis_prepare(&b);
-    shell_quartet(&b, sa, sb, sc, sd, out);
-    basis_release(&b);
-    return 0;
-}
 
 /* ---------------------------------------------------------------- Huzinaga */
 
@@ -608,10 +424,10 @@ int oracle_eri_packed_huzinaga(int nshell, const double *xyz, const int *L, cons
                                const int *prim_off, const double *expn, const double *coef,
                                double *out, int nthreads) {
     oracle_init();
-    oracle_basis b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0};
+    d_basis b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0, 0, 0};
     for (int s = 0; s < nshell; ++s)
         if (L[s] < 0 || L[s] > 6 || nprim[s] < 1) return -1;
-    basis_prepare(&b);
+    d_basis_prepare(&b);
     int n = b.nbf;
     int *fsh = (int *)malloc(sizeof(int) * n), *fao = (int *)malloc(sizeof(int) * n);
     for (int s = 0; s < nshell; ++s)
@@ -653,11 +469,11 @@ int oracle_eri_packed_huzinaga(int nshell, const double *xyz, const int *L, cons
                                 expn[id], D[0], D[1], D[2], pw[3][0], pw[3][1], pw[3][2]);
                             s += b.ncoef[ia] * b.ncoef[ib] * b.ncoef[ic] * b.ncoef[id] * v;
                         }
-            for (int t = 0; t < 4; ++t) s *= comp_factor(fao[f[t]]);
+            for (int t = 0; t < 4; ++t) s *= d_comp_factor(fao[f[t]]);
             out[tri64(ij) + kl] = s;
         }
     }
     free(fsh); free(fao);
-    basis_release(&b);
+    d_basis_release(&b);
     return 0;
 }

@@ -76,6 +76,8 @@ def lib():
         L.oracle_shell_quartet.argtypes = [_I, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]
         L.oracle_coulomb_prim.restype = _D
         L.oracle_coulomb_prim.argtypes = ([_D, _D, _D, _D, _I, _I, _I] * 4)
+        L.oracle_eri_packed_hgp_ld.restype = _I
+        L.oracle_eri_packed_hgp_ld.argtypes = drv
         L.oracle_eri_packed_hgp_sample.restype = ctypes.c_int64
         L.oracle_eri_packed_hgp_sample.argtypes = drv + [ctypes.c_int64]
         L.oracle_set_orientation.argtypes = [_I]
@@ -204,6 +206,20 @@ def eri_packed_hgp(shells, nthreads: int = 1) -> np.ndarray:
     rc = lib().oracle_eri_packed_hgp(len(arrs[1]), *[_ptr(a) for a in arrs], _ptr(out), nthreads)
     if rc != 0:
         raise ValueError("oracle_eri_packed_hgp: unsupported shell")
+    return out
+
+
+def eri_packed_hgp_ld(shells, nthreads: int = 1) -> np.ndarray:
+    """The same restated HGP driver evaluated in long double (64-bit mantissa): a near-exact
+    reference for FP64 parity, rounded to double at the end.  nthreads 0 uses every core."""
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    arrs = _shell_arrays(shells)
+    n = shells.nbf
+    out = np.zeros(n * (n + 1) * (n * n + n + 2) // 8)
+    rc = lib().oracle_eri_packed_hgp_ld(len(arrs[1]), *[_ptr(a) for a in arrs], _ptr(out), nthreads)
+    if rc != 0:
+        raise ValueError("oracle_eri_packed_hgp_ld: unsupported shell")
     return out
 
 

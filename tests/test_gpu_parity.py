@@ -69,29 +69,51 @@ def test_ethane_sto3g_matches_reference_hgp(eng, oracle):
     assert np.max(np.abs(got - huz)) < TOL_FP64
 
 
-# The reference orients each quartet by shell index (chrr(I,J,K,L), I >= J); the engine puts
-# the larger-L shell of each pair first.  Same mathematics, different rounding: with a tight d
-# (exponent ~2e3) and a diffuse p (~0.2) the reference orientation loses ~1e-11 absolute to
-# HRR cancellation while the engine's stays at ~1e-16 (tests/test_oracle_golden.py pins
-# this against 40-digit values).  Exact parity is therefore checked against the oracle in
-# the engine's orientation, and the reference orientation within its own rounding error.
-TOL_REF_ORIENTATION = 2e-11
+# FP64 parity.  The reference algorithm (HGP, restated by the oracle) is evaluated in long
+# double as the near-exact value; the FP64 GPU path must be within 1e-12 Eh of it.  The same
+# algorithm in FP64 -- the reference's own arithmetic -- is itself up to ~2.4e-12 (config 1)
+# and ~1.1e-11 (config 2, in the reference's quartet orientation) from that value: tight
+# primitives (exponents to 1e4) with random-sign contractions cancel, and the reference
+# orients (p d| pairs with the diffuse shell first, which the HRR amplifies.  Against the
+# FP64 oracle the GPU is therefore checked within that oracle's own measured error.
+
+
+def _fp64_oracle_bound(oracle, sh, ld):
+    ref = oracle.eri_packed_hgp(sh, nthreads=8)
+    return ref, float(np.max(np.abs(ref - ld)))
 
 
 def test_ethane_polarised_all_classes(eng, oracle):
-    """Config 2 (l<=2, 22 class pairs up to (dd|dd)), both Boys modes."""
+    """Config 2 (l<=2, every class pair up to (dd|dd)), both Boys modes."""
     from molints_b200 import engine
     sh = mi.config2()
     got = eng.eri_packed(sh)
-    with oracle.engine_orientation():
-        ref = oracle.eri_packed_hgp(sh, nthreads=8)
-    assert np.max(np.abs(got - ref)) < TOL_FP64
-    ref_o = oracle.eri_packed_hgp(sh, nthreads=8)
-    assert np.max(np.abs(got - ref_o)) < TOL_REF_ORIENTATION
+    ld = oracle.eri_packed_hgp_ld(sh, nthreads=8)
+    assert np.max(np.abs(got - ld)) < TOL_FP64
+    ref, own = _fp64_oracle_bound(oracle, sh, ld)
+    assert np.max(np.abs(got - ref)) < own + TOL_FP64
     got_x = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
-    with oracle.exact_boys(), oracle.engine_orientation():
-        ref_x = oracle.eri_packed_hgp(sh, nthreads=8)
-    assert np.max(np.abs(got_x - ref_x)) < TOL_FP64
+    with oracle.exact_boys():
+        ld_x = oracle.eri_packed_hgp_ld(sh, nthreads=8)
+    assert np.max(np.abs(got_x - ld_x)) < TOL_FP64
+
+
+def test_split_valence_24_full(eng, oracle):
+    """Config 1 at full size: all 14,908,530 integrals against the long-double oracle, and
+    the Schwarz inequality over the whole vector."""
+    sh = mi.config1()
+    got = eng.eri_packed(sh)
+    assert got.shape == (14908530,)
+    ld = oracle.eri_packed_hgp_ld(sh, nthreads=0)
+    assert np.max(np.abs(got - ld)) < TOL_FP64
+    n = sh.nbf
+    npair = n * (n + 1) // 2
+    diag = got[np.arange(npair) * (np.arange(npair) + 1) // 2 + np.arange(npair)]
+    assert np.all(diag >= -1e-14)
+    ij = np.repeat(np.arange(npair), np.arange(1, npair + 1))
+    kl = np.arange(len(got)) - ij * (ij + 1) // 2
+    bound = np.sqrt(np.abs(diag[ij] * diag[kl]))
+    assert np.all(np.abs(got) <= bound * (1 + 1e-10) + 1e-14)
 
 
 @pytest.mark.parametrize("seed,lmax", [(101, 0), (102, 1), (103, 2), (104, 2)])
@@ -111,48 +133,6 @@ def test_every_slot_written(eng):
     torch.cuda.synchronize()
     eng.eri_packed_device(sh, out.data_ptr())
     assert not torch.isnan(out).any().item()
-
-
-def _sample_quartets(sh, nsample, seed):
-    """Random function quartets of a basis -> (packed index, shell quartet, components)."""
-    rng = np.random.default_rng(seed)
-    off = sh.fn_offsets()
-    fsh = np.searchsorted(off, np.arange(sh.nbf), side="right") - 1
-    out = []
-    for _ in range(nsample):
-        f = rng.integers(0, sh.nbf, 4)
-        i, j, k, l = (int(x) for x in f)
-        if i < j:
-            i, j = j, i
-        if k < l:
-            k, l = l, k
-        ij, kl = i * (i + 1) // 2 + j, k * (k + 1) // 2 + l
-        if ij < kl:
-            i, j, k, l = k, l, i, j
-            ij, kl = kl, ij
-        out.append((ij * (ij + 1) // 2 + kl, [(int(fsh[x]), int(x - off[fsh[x]])) for x in (i, j, k, l)]))
-    return out
-
-
-def test_split_valence_24_sampled(eng, oracle):
-    """Config 1 at full size (14.9 M integrals): 400 sampled function quartets against the
-    oracle's per-quartet HGP, plus the Schwarz inequality over the whole vector."""
-    sh = mi.config1()
-    got = eng.eri_packed(sh)
-    assert got.shape == (14908530,)
-    for idx, fq in _sample_quartets(sh, 400, 7):
-        shells = [s for s, _ in fq]
-        q = oracle.shell_quartet(sh, *shells)
-        ref = q[tuple(m for _, m in fq)]
-        assert abs(got[idx] - ref) < TOL_FP64, (idx, fq)
-    n = sh.nbf
-    npair = n * (n + 1) // 2
-    diag = got[np.arange(npair) * (np.arange(npair) + 1) // 2 + np.arange(npair)]
-    assert np.all(diag >= -1e-14)
-    ij = np.repeat(np.arange(npair), np.arange(1, npair + 1))
-    kl = np.arange(len(got)) - ij * (ij + 1) // 2
-    bound = np.sqrt(np.abs(diag[ij] * diag[kl]))
-    assert np.all(np.abs(got) <= bound * (1 + 1e-10) + 1e-14)
 
 
 @pytest.mark.parametrize("cfg", ["config1", "config2"])
