@@ -228,9 +228,9 @@ def run_ours(args):
     top_flop = per_class[top_name[4:]]["flop"]
     peak_fp64 = measure_fp64_peak(dev)
     traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
+    tfile = ROOT / "profiles" / "dram_traffic_split_valence_24.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(top_name)
+        traffic = json.loads(tfile.read_text()).get("bytes_per_launch", {}).get(top_name)
     roofline = {
         "bound": "fp64", "kernel": top_name, "achieved": top_flop / (top_ms * 1e-3) / 1e12,
         "peak": peak_fp64, "unit": "TFLOP/s",

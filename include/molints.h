@@ -147,8 +147,9 @@ int molints_plan_destroy(molints_plan *plan);
  * reference's pair order (shell i >= shell j, row-major): out[nshell*(nshell+1)/2]. */
 int molints_plan_schwarz(molints_plan *plan, double *out_host);
 
-/* Per-launch device times.  After molints_plan_set_profiling(plan, 1), every execute records
- * a CUDA event pair around each kernel launch; molints_plan_launch_times then waits for the
+/* Per-launch device times.  After molints_plan_set_profiling(plan, 1), every execute runs
+ * its kernels one after another on the context's stream (no side streams) and records a CUDA
+ * event pair around each launch; molints_plan_launch_times then waits for the
  * last execute and returns up to cap entries: names[k] (static strings such as
  * "eri_ssss", "schwarz_pp", "build_pairs") and ms[k].  Returns the number of launches of the
  * last execute, or a negative status. */

@@ -627,14 +627,15 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
             jobs.push_back({p->class_cost[x][y], x, y});
         }
     std::stable_sort(jobs.begin(), jobs.end(), [](const Job &a, const Job &b) { return a.cost > b.cost; });
-    const int nside = std::min<int>(molints_ctx::kSide, (int)jobs.size());
+    // Profiling runs every launch on the caller's stream, so each event pair times one kernel.
+    const int nside = p->profiling ? 0 : std::min<int>(molints_ctx::kSide, (int)jobs.size());
     if (nside > 0) MI_CUDA(ctx, cudaEventRecord(ctx->fork, s));
     for (int i = 0; i < nside; ++i) MI_CUDA(ctx, cudaStreamWaitEvent(ctx->side[i], ctx->fork, 0));
     for (size_t k = 0; k < jobs.size(); ++k) {
         const int x = jobs[k].x, y = jobs[k].y;
         const int nx = p->class_start[x + 1] - p->class_start[x];
         const int ny = p->class_start[y + 1] - p->class_start[y];
-        cudaStream_t st = ctx->side[k % nside];
+        cudaStream_t st = nside ? ctx->side[k % nside] : s;
         EriLaunch L{};
         L.pairs = P;
         L.boys = B;
