@@ -161,6 +161,22 @@ int molints_plan_launch_times(molints_plan *plan, const char **names, float *ms,
 int molints_boys_eval(molints_ctx *ctx, int32_t boys_mode, int32_t mmax, const double *T,
                       int64_t n, double *out);
 
+/* The ERI path for callers that cannot allocate device memory where they need the
+ * integrals: code running inside CUDA stream capture, where cudaMalloc is not allowed, and
+ * frameworks whose allocator owns the whole GPU.  There is no counterpart in the reference.
+ * It needs no context and allocates nothing: the caller passes the basis (host arrays, as for
+ * molints_eri_packed) and its own device vector out_device of molints_npacked(nbf) doubles;
+ * the Boys table and the pair tables live in one static device array of 8 MiB that every GPU
+ * which loads the library holds until exit.  Bases whose tables do not fit are rejected with
+ * MOLINTS_ERR_UNSUPPORTED and a message in err (err may be NULL).  FP64 without screening
+ * only (opts NULL = defaults; prim_cutoff is ignored: every primitive pair is kept).  The
+ * first call on a device looks the array up with cudaGetSymbolAddress and copies the Boys
+ * table into it synchronously, so make that first call before any stream capture.  The call
+ * enqueues its work on `stream` (a cudaStream_t; NULL is the legacy default stream) and
+ * returns; all calls share the array, so calls whose GPU work overlaps race on it. */
+int molints_eri_packed_noalloc(const molints_basis *basis, const molints_options *opts,
+                               double *out_device, void *stream, char *err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,7 +42,7 @@ def sources():
     finally:
         sys.path.pop(0)
     gen = gen_eri.generate()
-    return [CSRC / "molints.cu"] + sorted(gen)
+    return [CSRC / "molints.cu", CSRC / "noalloc.cu"] + sorted(gen)
 
 
 def _deps(src: Path):

@@ -192,6 +192,30 @@ __global__ void boys_eval_kernel(BoysTab bt, int mmax, const double *__restrict_
 
 }  // namespace molints
 
+// ------------------------------------------------------------------ helpers for noalloc.cu
+namespace molints {
+
+// Launch the primitive-pair builder (used by the allocation-free entry point).
+void launch_build_pairs(int npair, const int2 *pair_ab, const int4 *info, const int *pp_src,
+                        const double *xyz, const int *poff, const double *expn,
+                        const double *ncoef, PrimPair *pp, double4 *geo, cudaStream_t s) {
+    if (npair <= 0) return;
+    build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, pair_ab, info, pp_src, xyz, poff,
+                                                          expn, ncoef, std::sqrt(2.0) * std::pow(M_PI, 1.25),
+                                                          pp, geo);
+}
+
+// The Boys table the contexts upload: F_0..F_22 and e^-T at T_n = n/16, n = 0..640.
+void fill_boys_table(double *tab) {
+    for (int n = 0; n < kBoysRows; ++n) {
+        const double T = n * kBoysStep;
+        for (int m = 0; m < kBoysCols - 1; ++m) tab[(size_t)n * kBoysCols + m] = boys_series(m, T);
+        tab[(size_t)n * kBoysCols + kBoysCols - 1] = std::exp(-T);
+    }
+}
+
+}  // namespace molints
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 

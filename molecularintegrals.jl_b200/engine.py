@@ -33,7 +33,7 @@ EXPORTED_SYMBOLS = [
     "molints_create", "molints_destroy", "molints_last_error", "molints_set_stream",
     "molints_eri_packed", "molints_plan_create", "molints_plan_execute", "molints_plan_stats",
     "molints_plan_destroy", "molints_plan_schwarz", "molints_boys_eval",
-    "molints_plan_set_profiling", "molints_plan_launch_times",
+    "molints_plan_set_profiling", "molints_plan_launch_times", "molints_eri_packed_noalloc",
 ]
 
 
@@ -101,6 +101,7 @@ def load_library(path: Path | str | None = None):
         "molints_boys_eval": (ctypes.c_int, [P, I32, I32, P, I64, P]),
         "molints_plan_set_profiling": (ctypes.c_int, [P, ctypes.c_int]),
         "molints_plan_launch_times": (ctypes.c_int, [P, P, P, ctypes.c_int]),
+        "molints_eri_packed_noalloc": (ctypes.c_int, [P, P, P, P, ctypes.c_char_p, ctypes.c_size_t]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
