@@ -22,6 +22,8 @@ constexpr int kBoysTaylor = 8;            // Taylor terms about T_n; |T - T_n| <
 constexpr double kBoysStepInv = 16.0;
 constexpr double kBoysStep = 0.0625;
 constexpr double kBoysTableMax = 40.0;    // exact-mode switch to the asymptotic form
+constexpr int kBoysMaxM1 = 16;            // scaled tables exist for M = 0..15
+constexpr int kBoysScaledCols = 10;       // F_{M+k}(T_n)/k! for k < 8, e^-T_n, pad (80 B)
 constexpr double kBoysReferenceSwitch = 30.0;  // farray's Tmax, src/Boys.jl:19
 
 // Record of one primitive pair (a, b) of a canonical shell pair (A, B):
@@ -46,8 +48,9 @@ struct PairTab {
 };
 
 struct BoysTab {
-    const double *tab;  // [kBoysRows][kBoysCols]
-    double t_switch;    // asymptotic form at T >= t_switch
+    const double *tab;     // [kBoysRows][kBoysCols]: F_0..F_22, e^-T_n
+    const double *scaled;  // [kBoysMaxM1][kBoysRows][kBoysScaledCols]
+    double t_switch;       // asymptotic form at T >= t_switch
 };
 
 // One launch of a class-pair kernel: a rectangle (bra pairs x ket pairs) or, when both
@@ -76,37 +79,44 @@ __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, i
 }
 
 // F_0..F_M at T: the farray structure of src/Boys.jl:19-27.
-//   T <  t_switch: F_M by an 8-term Taylor expansion about the nearest table point
-//                  (F_m(T_n - d) = sum_k F_{m+k}(T_n) d^k / k!), e^-T = e^-T_n e^d, then
-//                  the downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1).
+//   T <  t_switch: F_M by an 8-term Taylor expansion about the nearest table point,
+//                  F_M(T_n - d) = sum_k [F_{M+k}(T_n)/k!] d^k (the table row of M holds the
+//                  bracketed coefficients, so this is 7 FMAs), e^-T = e^-T_n e^d, then the
+//                  downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1).
 //   T >= t_switch: the asymptotic family F_m = (2m-1)!! / (2T)^m * sqrt(pi/T)/2, the values
 //                  farray's Fm_asymp top order and e^-T-free recursion produce.
+// The table index is rounded with the 1.5*2^52 trick: T*16 + 1.5*2^52 holds round(T*16) in
+// its low mantissa bits, and subtracting the constant back gives T_n*16 exactly.
 template <int M>
 __device__ __forceinline__ void boys_fm(double T, const BoysTab &bt, double *F) {
+    static_assert(M < kBoysMaxM1, "Boys order beyond the scaled tables");
     if (T < bt.t_switch) {
-        const int n = __double2int_rn(T * kBoysStepInv);
-        const double d = n * kBoysStep - T;
-        const double *__restrict__ row = bt.tab + n * kBoysCols;
-        // F_M..F_M+7 by 16-byte loads from the even column at or below M (rows are 192 B)
-        constexpr int M0 = M & ~1;
-        constexpr int NV = (M - M0 + kBoysTaylor + 1) / 2;
-        double v[2 * NV];
-        const double2 *__restrict__ r2 = reinterpret_cast<const double2 *>(row + M0);
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            const double2 x = __ldg(r2 + k);
-            v[2 * k] = x.x;
-            v[2 * k + 1] = x.y;
-        }
-        double f = v[M - M0 + kBoysTaylor - 1];
-#pragma unroll
-        for (int k = kBoysTaylor - 1; k >= 1; --k) f = fma(f, d * (1.0 / k), v[M - M0 + k - 1]);
+        constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+        const double t16 = fma(T, kBoysStepInv, kMagic);
+        const int n = __double2loint(t16);
+        const double d = fma(t16 - kMagic, kBoysStep, -T);
+        const double2 *__restrict__ r2 = reinterpret_cast<const double2 *>(
+            bt.scaled + ((size_t)M * kBoysRows + n) * kBoysScaledCols);
+        const double2 c01 = __ldg(r2), c23 = __ldg(r2 + 1), c45 = __ldg(r2 + 2), c67 = __ldg(r2 + 3);
+        double f = fma(c67.y, d, c67.x);
+        f = fma(f, d, c45.y);
+        f = fma(f, d, c45.x);
+        f = fma(f, d, c23.y);
+        f = fma(f, d, c23.x);
+        f = fma(f, d, c01.y);
+        f = fma(f, d, c01.x);
         F[M] = f;
         if (M > 0) {
-            double ed = 1.0;
-#pragma unroll
-            for (int k = kBoysTaylor - 1; k >= 1; --k) ed = fma(ed, d * (1.0 / k), 1.0);
-            const double emt = __ldg(row + kBoysCols - 1) * ed;
+            const double emtn = __ldg(r2 + 4).x;
+            // e^d for |d| <= 1/32 by its Taylor polynomial to d^7
+            double ed = fma(d, 1.0 / 5040, 1.0 / 720);
+            ed = fma(ed, d, 1.0 / 120);
+            ed = fma(ed, d, 1.0 / 24);
+            ed = fma(ed, d, 1.0 / 6);
+            ed = fma(ed, d, 0.5);
+            ed = fma(ed, d, 1.0);
+            ed = fma(ed, d, 1.0);
+            const double emt = emtn * ed;
             const double t2 = 2.0 * T;
 #pragma unroll
             for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], emt) * (1.0 / (2 * m + 1));

@@ -31,7 +31,12 @@ struct molints_ctx {
     cudaStream_t stream = nullptr;
     int64_t budget = 0;        // bytes, 0 = unbounded
     int64_t held = 0;          // bytes currently allocated by this context and its plans
+    // Stream-ordered pool for every device buffer of the context and its plans: freed blocks
+    // stay cached (release threshold = max), so plan creation and destruction neither call
+    // cudaMalloc/cudaFree nor synchronise the device.
+    cudaMemPool_t pool = nullptr;
     double *boys_tab = nullptr;
+    double *boys_scaled = nullptr;  // per-M tables F_{M+k}(T_n)/k!, k < 8, and e^-T_n
     double *out_cache = nullptr;  // device buffer for host-output calls
     int64_t out_cache_len = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -122,11 +127,15 @@ int dev_alloc(molints_ctx *ctx, T **p, size_t count, int64_t *tally) {
     size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
     if (ctx->budget > 0 && ctx->held + (int64_t)bytes > ctx->budget)
         return fail(ctx, MOLINTS_ERR_BUDGET, "HBM budget exceeded");
-    cudaError_t e = cudaMalloc((void **)p, bytes);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    cudaError_t e = cudaMallocFromPoolAsync((void **)p, bytes, ctx->pool, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync");
     ctx->held += (int64_t)bytes;
     if (tally) *tally += (int64_t)bytes;
     return MOLINTS_OK;
+}
+
+void dev_free(molints_ctx *ctx, void *p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
 }
 
 }  // namespace
@@ -205,13 +214,21 @@ void launch_build_pairs(int npair, const int2 *pair_ab, const int4 *info, const 
                                                           pp, geo);
 }
 
-// The Boys table the contexts upload: F_0..F_22 and e^-T at T_n = n/16, n = 0..640.
-void fill_boys_table(double *tab) {
-    for (int n = 0; n < kBoysRows; ++n) {
-        const double T = n * kBoysStep;
-        for (int m = 0; m < kBoysCols - 1; ++m) tab[(size_t)n * kBoysCols + m] = boys_series(m, T);
-        tab[(size_t)n * kBoysCols + kBoysCols - 1] = std::exp(-T);
-    }
+// The scaled Boys tables of the kernels for M = 0..nM-1: row n of table M holds
+// F_{M+k}(T_n)/k! (k < 8), e^-T_n and a pad, T_n = n/16, n = 0..640.
+void fill_boys_scaled(double *sc, int nM) {
+    for (int M = 0; M < nM; ++M)
+        for (int n = 0; n < kBoysRows; ++n) {
+            const double T = n * kBoysStep;
+            double *row = sc + ((size_t)M * kBoysRows + n) * kBoysScaledCols;
+            double fact = 1.0;
+            for (int k = 0; k < kBoysTaylor; ++k) {
+                if (k > 0) fact *= k;
+                row[k] = boys_series(M + k, T) / fact;
+            }
+            row[kBoysTaylor] = std::exp(-T);
+            row[kBoysTaylor + 1] = 0.0;
+        }
 }
 
 }  // namespace molints
@@ -266,6 +283,17 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
         return MOLINTS_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&ctx->pool, &props) != cudaSuccess) {
+        ctx->pool = nullptr;
+        molints_destroy(ctx);
+        return MOLINTS_ERR_CUDA;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     // Boys table: F_0..F_22 and e^-T at T_n = n/16, n = 0..640.
     std::vector<double> tab((size_t)kBoysRows * kBoysCols);
     for (int n = 0; n < kBoysRows; ++n) {
@@ -273,10 +301,18 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
         for (int m = 0; m < kBoysCols - 1; ++m) tab[(size_t)n * kBoysCols + m] = boys_series(m, T);
         tab[(size_t)n * kBoysCols + kBoysCols - 1] = std::exp(-T);
     }
+    // Per-M tables for the kernels: row n of table M holds F_{M+k}(T_n)/k! (k = 0..7) and
+    // e^-T_n, padded to 10 doubles, so the Taylor sum is a Horner chain of 7 FMAs.
+    std::vector<double> sc((size_t)kBoysMaxM1 * kBoysRows * kBoysScaledCols, 0.0);
+    fill_boys_scaled(sc.data(), kBoysMaxM1);
     int rc = dev_alloc(ctx, &ctx->boys_tab, tab.size(), nullptr);
+    if (!rc) rc = dev_alloc(ctx, &ctx->boys_scaled, sc.size(), nullptr);
     if (rc) { molints_destroy(ctx); return rc; }
-    if (cudaMemcpy(ctx->boys_tab, tab.data(), tab.size() * sizeof(double),
-                   cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (cudaMemcpyAsync(ctx->boys_tab, tab.data(), tab.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->boys_scaled, sc.data(), sc.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         molints_destroy(ctx);
         return MOLINTS_ERR_CUDA;
     }
@@ -288,8 +324,15 @@ int molints_destroy(molints_ctx *ctx) {
     if (!ctx) return MOLINTS_OK;
     cudaSetDevice(ctx->device);
     if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
-    if (ctx->boys_tab) cudaFree(ctx->boys_tab);
-    if (ctx->out_cache) cudaFree(ctx->out_cache);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->stream = ctx->own_stream;
+    if (ctx->own_stream) {
+        dev_free(ctx, ctx->boys_tab);
+        dev_free(ctx, ctx->boys_scaled);
+        dev_free(ctx, ctx->out_cache);
+        cudaStreamSynchronize(ctx->own_stream);
+    }
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     for (int i = 0; i < molints_ctx::kSide; ++i) {
         if (ctx->side[i]) cudaStreamSynchronize(ctx->side[i]);
         if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
@@ -315,6 +358,7 @@ int molints_set_stream(molints_ctx *ctx, void *stream) {
 static BoysTab boys_of(const molints_ctx *ctx, int mode) {
     BoysTab bt;
     bt.tab = ctx->boys_tab;
+    bt.scaled = ctx->boys_scaled;
     bt.t_switch = (mode == MOLINTS_BOYS_EXACT) ? kBoysTableMax : kBoysReferenceSwitch;
     return bt;
 }
@@ -333,7 +377,7 @@ int molints_boys_eval(molints_ctx *ctx, int32_t mode, int32_t mmax, const double
     int rc = dev_alloc(ctx, &dT, (size_t)n, nullptr);
     if (rc) return rc;
     rc = dev_alloc(ctx, &dout, (size_t)n * mmax, nullptr);
-    if (rc) { cudaFree(dT); ctx->held -= n * 8; return rc; }
+    if (rc) { dev_free(ctx, dT); ctx->held -= n * 8; return rc; }
     cudaError_t e = cudaMemcpyAsync(dT, T, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
         boys_eval_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(boys_of(ctx, mode), mmax,
@@ -343,8 +387,8 @@ int molints_boys_eval(molints_ctx *ctx, int32_t mode, int32_t mmax, const double
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(out, dout, n * mmax * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    cudaFree(dT);
-    cudaFree(dout);
+    dev_free(ctx, dT);
+    dev_free(ctx, dout);
     ctx->held -= (int64_t)(n + n * mmax) * 8;
     if (e != cudaSuccess) return cuda_fail(ctx, e, "molints_boys_eval");
     return MOLINTS_OK;
@@ -355,8 +399,7 @@ static void plan_free(molints_plan *p) {
     for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->sh_nprim, p->pair_ab,
                     p->info, p->pp_src, p->geo, p->pp, p->bnd, p->qcon};
-    for (void *b : bufs)
-        if (b) cudaFree(b);
+    for (void *b : bufs) dev_free(p->ctx, b);
     if (p->ctx) p->ctx->held -= p->bytes;
     delete p;
 }
@@ -364,8 +407,7 @@ static void plan_free(molints_plan *p) {
 int molints_plan_destroy(molints_plan *p) {
     if (!p) return MOLINTS_OK;
     cudaSetDevice(p->ctx->device);
-    cudaStreamSynchronize(p->ctx->stream);
-    plan_free(p);
+    plan_free(p);  // stream-ordered frees after the plan's queued work
     return MOLINTS_OK;
 }
 
@@ -501,7 +543,7 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
     rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)nall, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &pbound, (size_t)nall, &scratch);
     if (rc) {
-        if (pbound) { cudaFree(pbound); ctx->held -= scratch; }
+        if (pbound) { dev_free(ctx, pbound); ctx->held -= scratch; }
         plan_free(p);
         return rc;
     }
@@ -519,7 +561,7 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
         (e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nall * sizeof(int), cudaMemcpyHostToDevice, s))) {
-        cudaFree(pbound); ctx->held -= scratch; plan_free(p);
+        dev_free(ctx, pbound); ctx->held -= scratch; plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
     }
     if (npair > 0) {
@@ -534,10 +576,10 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
         (nall > 0 && (e = cudaMemcpyAsync(pb_h.data(), pbound, nall * sizeof(double2),
                                           cudaMemcpyDeviceToHost, s))) ||
         (e = cudaStreamSynchronize(s))) {
-        cudaFree(pbound); ctx->held -= scratch; plan_free(p);
+        dev_free(ctx, pbound); ctx->held -= scratch; plan_free(p);
         return cuda_fail(ctx, e, "plan_create bound pass");
     }
-    cudaFree(pbound);
+    dev_free(ctx, pbound);
     ctx->held -= scratch;
 
     // Stage 2: drop primitive pairs i with b_i * max Qabs < prim_cutoff (each dropped term of
@@ -776,7 +818,7 @@ int molints_eri_packed(molints_ctx *ctx, const molints_basis *b, const molints_o
     if (!out_is_device) {
         if (ctx->out_cache_len < p->npacked) {
             if (ctx->out_cache) {
-                cudaFree(ctx->out_cache);
+                dev_free(ctx, ctx->out_cache);
                 ctx->held -= ctx->out_cache_len * 8;
                 ctx->out_cache = nullptr;
                 ctx->out_cache_len = 0;

@@ -31,7 +31,7 @@ namespace molints {
 void launch_build_pairs(int npair, const int2 *pair_ab, const int4 *info, const int *pp_src,
                         const double *xyz, const int *poff, const double *expn,
                         const double *ncoef, PrimPair *pp, double4 *geo, cudaStream_t s);
-void fill_boys_table(double *tab);
+void fill_boys_scaled(double *sc, int nM);
 }  // namespace molints
 
 using namespace molints;
@@ -40,7 +40,9 @@ namespace {
 
 constexpr size_t kScratchBytes = (size_t)8 << 20;  // the stated maximum: 8 MiB
 constexpr size_t kAlign = 256;
-constexpr size_t kTableBytes = ((size_t)kBoysRows * kBoysCols * sizeof(double) + kAlign - 1) / kAlign * kAlign;
+constexpr int kTableM = 4 * MOLINTS_LMAX + 1;  // Boys orders the class kernels use
+constexpr size_t kTableBytes =
+    ((size_t)kTableM * kBoysRows * kBoysScaledCols * sizeof(double) + kAlign - 1) / kAlign * kAlign;
 constexpr int kMaxDevices = 64;
 
 // Device scratch.  In host code this name is only a stand-in for the symbol, never an
@@ -142,8 +144,9 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_scratch);
         if (e != cudaSuccess || !ptr) return noalloc_fail(err, err_len, MOLINTS_ERR_CUDA, "cudaGetSymbolAddress failed");
-        fill_boys_table(reinterpret_cast<double *>(g_host));
-        e = cudaMemcpy(ptr, g_host, (size_t)kBoysRows * kBoysCols * sizeof(double), cudaMemcpyHostToDevice);
+        fill_boys_scaled(reinterpret_cast<double *>(g_host), kTableM);
+        e = cudaMemcpy(ptr, g_host, (size_t)kTableM * kBoysRows * kBoysScaledCols * sizeof(double),
+                       cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return noalloc_fail(err, err_len, MOLINTS_ERR_CUDA, "Boys table copy failed");
         g_dev_ptr[dev] = ptr;
         g_dev_ready[dev] = true;
@@ -237,7 +240,8 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
                        d_pp, d_geo, s);
     PairTab P{d_info, d_geo, d_pp, reinterpret_cast<const double2 *>(data + o_bnd)};
     BoysTab B;
-    B.tab = reinterpret_cast<const double *>(base);
+    B.tab = nullptr;  // the class kernels read only the scaled tables
+    B.scaled = reinterpret_cast<const double *>(base);
     B.t_switch = boys_mode == MOLINTS_BOYS_EXACT ? kBoysTableMax : kBoysReferenceSwitch;
     for (int x = 0; x < kNumPairClasses; ++x) {
         const int nx = class_start[x + 1] - class_start[x];
