@@ -138,13 +138,22 @@ int molints_eri_packed(molints_ctx *ctx, const molints_basis *basis,
  * synchronisation. */
 int molints_plan_create(molints_ctx *ctx, const molints_basis *basis,
                         const molints_options *opts, molints_plan **plan);
+/* A plan over nmol molecules at once (no reference counterpart; the batched form of
+ * all_twoe_ints).  One execute computes every molecule; molecule m's packed vector starts at
+ * out_device + sum over m' < m of molints_npacked(nbf(m')).  All shell quartets of all
+ * molecules go through one work queue per class pair. */
+int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
+                              const molints_options *opts, molints_plan **plan);
+/* Doubles the plan writes per execute (all molecules), or a negative status. */
+int64_t molints_plan_npacked(const molints_plan *plan);
 int molints_plan_execute(molints_plan *plan, double *out_device);
 int molints_plan_stats(const molints_plan *plan, molints_stats *stats);
 int molints_plan_destroy(molints_plan *plan);
 
 /* Contracted Schwarz bounds Q_ab = sqrt(max |(ab|ab)|) of the plan's shell pairs (computed
  * on demand on the context's stream; the plan must have been executed once), in the
- * reference's pair order (shell i >= shell j, row-major): out[nshell*(nshell+1)/2]. */
+ * reference's pair order (shell i >= shell j, row-major): out[nshell*(nshell+1)/2], one such
+ * block per molecule of a batch plan, in molecule order. */
 int molints_plan_schwarz(molints_plan *plan, double *out_host);
 
 /* Per-launch device times.  After molints_plan_set_profiling(plan, 1), every execute runs

@@ -53,19 +53,19 @@ struct BoysTab {
     double t_switch;       // asymptotic form at T >= t_switch
 };
 
-// One launch of a class-pair kernel: a rectangle (bra pairs x ket pairs) or, when both
-// come from the same pair class, the triangle q <= p of it.
-struct EriLaunch {
+// The chunk queue of one class pair: chunk c = {bra pair, first ket pair, ket count,
+// molecule}; lane l of the warp that takes it computes (bra | first + l + 32 i).  Chunks never
+// cross a bra pair, a molecule or, when bra and ket class coincide, the triangle q <= p.
+struct EriQueue {
     PairTab pairs;
     BoysTab boys;
-    double *out;              // packed output (device)
-    int bra0, nbra;           // bra shell pairs [bra0, bra0 + nbra)
-    int ket0, nket;           // ket shell pairs [ket0, ket0 + nket)
-    int tri;                  // 1: same class on both sides, only q <= p
-    int pad;
-    long long nquart;         // nbra * nket or nbra * (nbra + 1) / 2
-    double screen_cut;        // Qabs_p Qabs_q below this: written as 0
-    double fp32_cut;          // R_p R_q below this (MIXED kernels): FP32 VRR
+    double *out;                  // packed outputs of all molecules (device)
+    const long long *mol_out;     // offset of each molecule's packed vector in out
+    const int4 *chunks;
+    int nchunks;
+    int *counter;                 // next chunk; zero at launch
+    double screen_cut;            // Qabs_p Qabs_q below this: written as 0
+    double fp32_cut;              // R_p R_q below this (MIXED kernels): FP32 VRR
 };
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {
@@ -144,22 +144,6 @@ __device__ __forceinline__ long long packed_index(long long ij, long long kl) {
 }
 __device__ __forceinline__ long long pair_index(int i, int j) {
     return i >= j ? tri_ll(i) + j : tri_ll(j) + i;
-}
-
-// Decode a quartet's linear index in a launch into (bra pair, ket pair).
-__device__ __forceinline__ void decode_quartet(const EriLaunch &L, long long t, int &p, int &q) {
-    if (L.tri) {
-        long long pp = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-        while (tri_ll(pp) > t) --pp;
-        while (tri_ll(pp + 1) <= t) ++pp;
-        p = (int)pp;
-        q = (int)(t - tri_ll(pp));
-    } else {
-        p = (int)(t / L.nket);
-        q = (int)(t - (long long)p * L.nket);
-    }
-    p += L.bra0;
-    q += L.ket0;
 }
 
 }  // namespace molints

@@ -2,34 +2,56 @@
 #pragma once
 #include "eri_common.cuh"
 namespace molints {
-void launch_eri_ssss(const EriLaunch &L, int mixed, cudaStream_t s);
+void launch_eri_ssss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ssss(int mixed);
 void launch_schwarz_ssss(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_eri_psss(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_psps(const EriLaunch &L, int mixed, cudaStream_t s);
+void launch_eri_psss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_psss(int mixed);
+void launch_eri_psps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_psps(int mixed);
 void launch_schwarz_psps(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_eri_ppss(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_ppps(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_pppp(const EriLaunch &L, int mixed, cudaStream_t s);
+void launch_eri_ppss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ppss(int mixed);
+void launch_eri_ppps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ppps(int mixed);
+void launch_eri_pppp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_pppp(int mixed);
 void launch_schwarz_pppp(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_eri_dsss(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dsps(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dspp(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dsds(const EriLaunch &L, int mixed, cudaStream_t s);
+void launch_eri_dsss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dsss(int mixed);
+void launch_eri_dsps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dsps(int mixed);
+void launch_eri_dspp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dspp(int mixed);
+void launch_eri_dsds(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dsds(int mixed);
 void launch_schwarz_dsds(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_eri_dpss(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dpps(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dppp(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dpds(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dpdp(const EriLaunch &L, int mixed, cudaStream_t s);
+void launch_eri_dpss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dpss(int mixed);
+void launch_eri_dpps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dpps(int mixed);
+void launch_eri_dppp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dppp(int mixed);
+void launch_eri_dpds(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dpds(int mixed);
+void launch_eri_dpdp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dpdp(int mixed);
 void launch_schwarz_dpdp(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_eri_ddss(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_ddps(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_ddpp(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_ddds(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dddp(const EriLaunch &L, int mixed, cudaStream_t s);
-void launch_eri_dddd(const EriLaunch &L, int mixed, cudaStream_t s);
+void launch_eri_ddss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ddss(int mixed);
+void launch_eri_ddps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ddps(int mixed);
+void launch_eri_ddpp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ddpp(int mixed);
+void launch_eri_ddds(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ddds(int mixed);
+void launch_eri_dddp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dddp(int mixed);
+void launch_eri_dddd(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_dddd(int mixed);
 void launch_schwarz_dddd(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-typedef void (*EriLauncher)(const EriLaunch &, int, cudaStream_t);
+typedef void (*EriLauncher)(const EriQueue &, int, int, cudaStream_t);
+typedef int (*EriOccupancy)(int);
 typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, double2 *, double *, int, cudaStream_t);
 constexpr int kLmax = 2;
 constexpr int kNumPairClasses = 6;
@@ -44,6 +66,14 @@ static const EriLauncher kEriLaunchers[6][6] = {
     {launch_eri_dsss, launch_eri_dsps, launch_eri_dspp, launch_eri_dsds, nullptr, nullptr},
     {launch_eri_dpss, launch_eri_dpps, launch_eri_dppp, launch_eri_dpds, launch_eri_dpdp, nullptr},
     {launch_eri_ddss, launch_eri_ddps, launch_eri_ddpp, launch_eri_ddds, launch_eri_dddp, launch_eri_dddd},
+};
+static const EriOccupancy kEriOccupancy[6][6] = {
+    {occupancy_eri_ssss, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {occupancy_eri_psss, occupancy_eri_psps, nullptr, nullptr, nullptr, nullptr},
+    {occupancy_eri_ppss, occupancy_eri_ppps, occupancy_eri_pppp, nullptr, nullptr, nullptr},
+    {occupancy_eri_dsss, occupancy_eri_dsps, occupancy_eri_dspp, occupancy_eri_dsds, nullptr, nullptr},
+    {occupancy_eri_dpss, occupancy_eri_dpps, occupancy_eri_dppp, occupancy_eri_dpds, occupancy_eri_dpdp, nullptr},
+    {occupancy_eri_ddss, occupancy_eri_ddps, occupancy_eri_ddpp, occupancy_eri_ddds, occupancy_eri_dddp, occupancy_eri_dddd},
 };
 static const char *const kEriNames[6][6] = {
     {"eri_ssss", nullptr, nullptr, nullptr, nullptr, nullptr},

@@ -330,11 +330,15 @@ void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, do
 }}
 """
     if len(entries) >= MIXED_MIN_VRR:
-        mixed_dispatch = ("    if (mixed) eri_kernel_{t}<1><<<(unsigned)blocks, 128, 0, s>>>(L);\n"
-                          "    else eri_kernel_{t}<0><<<(unsigned)blocks, 128, 0, s>>>(L);").format(t=tag)
+        mixed_dispatch = ("    if (mixed) eri_queue_{t}<1><<<grid, 128, 0, s>>>(Q);\n"
+                          "    else eri_queue_{t}<0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
+        occ_dispatch = ("    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<1>, 128, 0);\n"
+                        "    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0>, 128, 0);").format(t=tag)
     else:
         mixed_dispatch = ("    (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)\n"
-                          "    eri_kernel_{t}<0><<<(unsigned)blocks, 128, 0, s>>>(L);").format(t=tag)
+                          "    eri_queue_{t}<0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
+        occ_dispatch = ("    (void)mixed;\n"
+                        "    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0>, 128, 0);").format(t=tag)
     return f"""// Generated by gen_eri.py -- class ({'spdfg'[la]}{'spdfg'[lb]}|{'spdfg'[lc]}{'spdfg'[ld]}).  Do not edit.
 // VRR entries: {len(entries)}, contracted block: {nacc}, HRR lines: {len(hp.lines)}, outputs: {nout}.
 #include "../eri_common.cuh"
@@ -403,29 +407,46 @@ __device__ __forceinline__ void store_{tag}(double *__restrict__ out, const int4
 {store_code}
 }}
 
+// Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
+// ket pairs of one molecule) from a shared counter until the chunk list, ordered by
+// decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
 template <int MIXED>
-__global__ void __launch_bounds__(128) eri_kernel_{tag}(const EriLaunch L) {{
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= L.nquart) return;
-    int p, q;
-    decode_quartet(L, t, p, q);
-    const double2 bp = __ldg(&L.pairs.bnd[p]), bq = __ldg(&L.pairs.bnd[q]);
-    double res[{nout}];
-    if (bp.x * bq.x < L.screen_cut) {{
+__global__ void __launch_bounds__(128) eri_queue_{tag}(const EriQueue Q) {{
+    const int lane = threadIdx.x & 31;
+    for (;;) {{
+        int c = 0;
+        if (lane == 0) c = atomicAdd(Q.counter, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= Q.nchunks) return;
+        const int4 ch = __ldg(&Q.chunks[c]);
+        for (int q = ch.y + lane; q < ch.y + ch.z; q += 32) {{
+        const int p = ch.x;
+        const double2 bp = __ldg(&Q.pairs.bnd[p]), bq = __ldg(&Q.pairs.bnd[q]);
+        double res[{nout}];
+        if (bp.x * bq.x < Q.screen_cut) {{
 #pragma unroll
-        for (int x = 0; x < {nout}; ++x) res[x] = 0.0;
-    }} else {{
-        const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
-        if (MIXED && bp.y * bq.y < L.fp32_cut) quartet_{tag}<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
-        else quartet_{tag}<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+            for (int x = 0; x < {nout}; ++x) res[x] = 0.0;
+        }} else {{
+            const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
+            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_{tag}<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+            else quartet_{tag}<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+        }}
+        store_{tag}(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                    p == q, res);
+        }}
     }}
-    store_{tag}(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
 }}
 
-void launch_eri_{tag}(const EriLaunch &L, int mixed, cudaStream_t s) {{
-    if (L.nquart <= 0) return;
-    const long long blocks = (L.nquart + 127) / 128;
+void launch_eri_{tag}(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {{
+    if (Q.nchunks <= 0 || grid <= 0) return;
 {mixed_dispatch}
+}}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_eri_{tag}(int mixed) {{
+    int n = 0;
+{occ_dispatch}
+    return n;
 }}
 {schwarz}
 }}  // namespace molints
@@ -438,11 +459,13 @@ def emit_dispatch(pairs):
              '#include "eri_common.cuh"', "namespace molints {"]
     for X, Y in pairs:
         t = tag_of(X, Y)
-        lines.append(f"void launch_eri_{t}(const EriLaunch &L, int mixed, cudaStream_t s);")
+        lines.append(f"void launch_eri_{t}(const EriQueue &Q, int mixed, int grid, cudaStream_t s);")
+        lines.append(f"int occupancy_eri_{t}(int mixed);")
         if X == Y:
             lines.append(f"void launch_schwarz_{t}(const PairTab &P, const BoysTab &B, int p0, "
                          f"int np, double2 *pbound, double *qout, int full, cudaStream_t s);")
-    lines.append("typedef void (*EriLauncher)(const EriLaunch &, int, cudaStream_t);")
+    lines.append("typedef void (*EriLauncher)(const EriQueue &, int, int, cudaStream_t);")
+    lines.append("typedef int (*EriOccupancy)(int);")
     lines.append("typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, "
                  "double2 *, double *, int, cudaStream_t);")
     lines.append(f"constexpr int kLmax = {LMAX};")
@@ -456,6 +479,11 @@ def emit_dispatch(pairs):
         row = []
         for j, Y in enumerate(cls):
             row.append(f"launch_eri_{tag_of(X, Y)}" if j <= i else "nullptr")
+        lines.append("    {" + ", ".join(row) + "},")
+    lines.append("};")
+    lines.append(f"static const EriOccupancy kEriOccupancy[{len(cls)}][{len(cls)}] = {{")
+    for i, X in enumerate(cls):
+        row = [f"occupancy_eri_{tag_of(X, Y)}" if j <= i else "nullptr" for j, Y in enumerate(cls)]
         lines.append("    {" + ", ".join(row) + "},")
     lines.append("};")
     lines.append(f"static const char *const kEriNames[{len(cls)}][{len(cls)}] = {{")

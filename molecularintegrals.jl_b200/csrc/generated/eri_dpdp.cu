@@ -2565,30 +2565,48 @@ __device__ __forceinline__ void store_dpdp(double *__restrict__ out, const int4 
       if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[323]; }
 }
 
+// Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
+// ket pairs of one molecule) from a shared counter until the chunk list, ordered by
+// decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
 template <int MIXED>
-__global__ void __launch_bounds__(128) eri_kernel_dpdp(const EriLaunch L) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= L.nquart) return;
-    int p, q;
-    decode_quartet(L, t, p, q);
-    const double2 bp = __ldg(&L.pairs.bnd[p]), bq = __ldg(&L.pairs.bnd[q]);
-    double res[324];
-    if (bp.x * bq.x < L.screen_cut) {
+__global__ void __launch_bounds__(128) eri_queue_dpdp(const EriQueue Q) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(Q.counter, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= Q.nchunks) return;
+        const int4 ch = __ldg(&Q.chunks[c]);
+        for (int q = ch.y + lane; q < ch.y + ch.z; q += 32) {
+        const int p = ch.x;
+        const double2 bp = __ldg(&Q.pairs.bnd[p]), bq = __ldg(&Q.pairs.bnd[q]);
+        double res[324];
+        if (bp.x * bq.x < Q.screen_cut) {
 #pragma unroll
-        for (int x = 0; x < 324; ++x) res[x] = 0.0;
-    } else {
-        const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
-        if (MIXED && bp.y * bq.y < L.fp32_cut) quartet_dpdp<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
-        else quartet_dpdp<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+            for (int x = 0; x < 324; ++x) res[x] = 0.0;
+        } else {
+            const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
+            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_dpdp<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+            else quartet_dpdp<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+        }
+        store_dpdp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                    p == q, res);
+        }
     }
-    store_dpdp(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
 }
 
-void launch_eri_dpdp(const EriLaunch &L, int mixed, cudaStream_t s) {
-    if (L.nquart <= 0) return;
-    const long long blocks = (L.nquart + 127) / 128;
-    if (mixed) eri_kernel_dpdp<1><<<(unsigned)blocks, 128, 0, s>>>(L);
-    else eri_kernel_dpdp<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+void launch_eri_dpdp(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    if (mixed) eri_queue_dpdp<1><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_dpdp<0><<<grid, 128, 0, s>>>(Q);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_eri_dpdp(int mixed) {
+    int n = 0;
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpdp<1>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpdp<0>, 128, 0);
+    return n;
 }
 
 // Bounds of the pairs of one class.

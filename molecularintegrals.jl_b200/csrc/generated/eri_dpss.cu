@@ -201,30 +201,48 @@ __device__ __forceinline__ void store_dpss(double *__restrict__ out, const int4 
       if ((!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[17]; }
 }
 
+// Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
+// ket pairs of one molecule) from a shared counter until the chunk list, ordered by
+// decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
 template <int MIXED>
-__global__ void __launch_bounds__(128) eri_kernel_dpss(const EriLaunch L) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= L.nquart) return;
-    int p, q;
-    decode_quartet(L, t, p, q);
-    const double2 bp = __ldg(&L.pairs.bnd[p]), bq = __ldg(&L.pairs.bnd[q]);
-    double res[18];
-    if (bp.x * bq.x < L.screen_cut) {
+__global__ void __launch_bounds__(128) eri_queue_dpss(const EriQueue Q) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(Q.counter, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= Q.nchunks) return;
+        const int4 ch = __ldg(&Q.chunks[c]);
+        for (int q = ch.y + lane; q < ch.y + ch.z; q += 32) {
+        const int p = ch.x;
+        const double2 bp = __ldg(&Q.pairs.bnd[p]), bq = __ldg(&Q.pairs.bnd[q]);
+        double res[18];
+        if (bp.x * bq.x < Q.screen_cut) {
 #pragma unroll
-        for (int x = 0; x < 18; ++x) res[x] = 0.0;
-    } else {
-        const int nb = __ldg(&L.pairs.info[p]).y, nk = __ldg(&L.pairs.info[q]).y;
-        if (MIXED && bp.y * bq.y < L.fp32_cut) quartet_dpss<float>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
-        else quartet_dpss<double>(L.pairs, L.boys, p, q, 0, nb, 0, nk, res);
+            for (int x = 0; x < 18; ++x) res[x] = 0.0;
+        } else {
+            const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
+            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_dpss<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+            else quartet_dpss<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+        }
+        store_dpss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                    p == q, res);
+        }
     }
-    store_dpss(L.out, __ldg(&L.pairs.info[p]), __ldg(&L.pairs.info[q]), p == q, res);
 }
 
-void launch_eri_dpss(const EriLaunch &L, int mixed, cudaStream_t s) {
-    if (L.nquart <= 0) return;
-    const long long blocks = (L.nquart + 127) / 128;
+void launch_eri_dpss(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
     (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)
-    eri_kernel_dpss<0><<<(unsigned)blocks, 128, 0, s>>>(L);
+    eri_queue_dpss<0><<<grid, 128, 0, s>>>(Q);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_eri_dpss(int mixed) {
+    int n = 0;
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpss<0>, 128, 0);
+    return n;
 }
 
 }  // namespace molints

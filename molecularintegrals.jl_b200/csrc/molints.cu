@@ -44,31 +44,43 @@ struct molints_ctx {
     static constexpr int kSide = 6;
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork = nullptr, join[kSide] = {};
+    int num_sms = 0;
+    int occupancy[kNumPairClasses][kNumPairClasses][2] = {};  // blocks/SM, 0 = not queried
     std::string err;
 };
 
 struct molints_plan {
     molints_ctx *ctx = nullptr;
     molints_options opts{};
+    int nmol = 0;
     int nshell = 0;
-    int64_t nbf = 0, npacked = 0;
+    int64_t npacked = 0;               // all molecules
+    std::vector<int64_t> mol_out_h;    // offset of each molecule's packed vector
+    std::vector<int> mol_nshell;
     int npair = 0;
     int64_t nprim_pair_all = 0, nprim_pair_kept = 0;
     int class_start[kNumPairClasses + 1] = {0};
+    // work queues: chunks of class pair (x, y) are chunk[q_off[x][y] .. + q_len[x][y])
+    int q_off[kNumPairClasses][kNumPairClasses] = {};
+    int q_len[kNumPairClasses][kNumPairClasses] = {};
     double class_cost[kNumPairClasses][kNumPairClasses] = {};  // kept primitive quartets
     // host copies (final, screened order)
     std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
+    std::vector<int> pair_mol;         // canonical pair -> molecule
     std::vector<int> npp_h;            // kept primitive pairs per shell pair
     std::vector<double2> bnd_h;        // (Qabs, R) per shell pair
     // device buffers
     double *sh_xyz = nullptr, *expn = nullptr, *ncoef = nullptr;
-    int *sh_poff = nullptr, *sh_nprim = nullptr;
+    int *sh_poff = nullptr;
     int2 *pair_ab = nullptr;
     int4 *info = nullptr;
     int *pp_src = nullptr;             // primitive pair k -> (ia << 8) | ib within its shells
     double4 *geo = nullptr;
     PrimPair *pp = nullptr;
     double2 *bnd = nullptr;
+    int4 *chunks = nullptr;
+    int *counters = nullptr;           // one per class pair, zeroed by every execute
+    long long *mol_out = nullptr;
     double *qcon = nullptr;  // contracted Schwarz bounds, filled on demand by plan_schwarz
     int64_t bytes = 0;
     int n_launches = 0;
@@ -283,6 +295,8 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
         return MOLINTS_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
+    if (cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        ctx->num_sms = 1;
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -397,8 +411,8 @@ int molints_boys_eval(molints_ctx *ctx, int32_t mode, int32_t mmax, const double
 static void plan_free(molints_plan *p) {
     if (!p) return;
     for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
-    void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->sh_nprim, p->pair_ab,
-                    p->info, p->pp_src, p->geo, p->pp, p->bnd, p->qcon};
+    void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src,
+                    p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon};
     for (void *b : bufs) dev_free(p->ctx, b);
     if (p->ctx) p->ctx->held -= p->bytes;
     delete p;
@@ -411,9 +425,37 @@ int molints_plan_destroy(molints_plan *p) {
     return MOLINTS_OK;
 }
 
-int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_options *opts_in,
-                        molints_plan **out) {
-    if (!ctx || !b || !out) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null argument");
+// Validate one basis; returns its nprim_tot (>= 0) or a negative status with ctx->err set.
+static int check_basis(molints_ctx *ctx, const molints_basis *b, int64_t *nbf_out) {
+    const int64_t nbf = molints_nbf(b);
+    if (nbf < 0) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: malformed basis");
+    if (nbf > 46000) return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: basis too large");
+    const int ns = b->nshell;
+    if (ns > 0 && (!b->expn || !b->coef)) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null primitives");
+    int nprim_tot = 0;
+    for (int s = 0; s < ns; ++s) {
+        if (b->L[s] > MOLINTS_LMAX)
+            return fail(ctx, MOLINTS_ERR_UNSUPPORTED,
+                        "plan_create: shell angular momentum above " + std::to_string(MOLINTS_LMAX));
+        if (b->nprim[s] < 1 || b->prim_off[s] < 0)
+            return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: shell without primitives");
+        if (b->nprim[s] > 255)
+            return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: more than 255 primitives in a shell");
+        nprim_tot = std::max(nprim_tot, b->prim_off[s] + b->nprim[s]);
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(b->xyz[3 * s + k])) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: non-finite centre");
+    }
+    for (int k = 0; k < nprim_tot; ++k)
+        if (!(b->expn[k] > 0.0) || !std::isfinite(b->expn[k]) || !std::isfinite(b->coef[k]))
+            return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: exponents must be finite and > 0");
+    *nbf_out = nbf;
+    return nprim_tot;
+}
+
+int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
+                              const molints_options *opts_in, molints_plan **out) {
+    if (!ctx || !out || nmol < 0 || (nmol > 0 && !bases))
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null argument");
     *out = nullptr;
     molints_options opts;
     if (opts_in) opts = *opts_in; else molints_default_options(&opts);
@@ -425,96 +467,98 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
         return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: method not available");
     if (!(opts.fp32_cutoff >= 0.0) || !(opts.screen_cutoff >= 0.0) || !(opts.prim_cutoff >= 0.0))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: cutoffs must be >= 0");
-    const int64_t nbf = molints_nbf(b);
-    if (nbf < 0) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: malformed basis");
-    const int ns = b->nshell;
-    if (ns > 0 && (!b->expn || !b->coef)) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null primitives");
-    int nprim_tot = 0;
-    for (int s = 0; s < ns; ++s) {
-        if (b->L[s] > MOLINTS_LMAX)
-            return fail(ctx, MOLINTS_ERR_UNSUPPORTED,
-                        "plan_create: shell angular momentum above " + std::to_string(MOLINTS_LMAX));
-        if (b->nprim[s] < 1 || b->prim_off[s] < 0)
-            return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: shell without primitives");
-        nprim_tot = std::max(nprim_tot, b->prim_off[s] + b->nprim[s]);
-        for (int k = 0; k < 3; ++k)
-            if (!std::isfinite(b->xyz[3 * s + k])) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: non-finite centre");
-    }
-    // n(n+1)(n^2+n+2)/8 stays well inside int64 and the int pair indices for n <= 46000
-    if (nbf > 46000) return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: basis too large");
-    for (int k = 0; k < nprim_tot; ++k)
-        if (!(b->expn[k] > 0.0) || !std::isfinite(b->expn[k]) || !std::isfinite(b->coef[k]))
-            return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: exponents must be finite and > 0");
 
+    // ---- molecules: validation, output offsets, global shell and primitive arrays
+    std::vector<int> shell_off(nmol + 1, 0), prim_base(nmol + 1, 0);
+    std::vector<int64_t> mol_nbf(nmol), mol_out(nmol + 1, 0);
+    for (int m = 0; m < nmol; ++m) {
+        int64_t nbf = 0;
+        const int np = check_basis(ctx, &bases[m], &nbf);
+        if (np < 0) return np;
+        mol_nbf[m] = nbf;
+        shell_off[m + 1] = shell_off[m] + bases[m].nshell;
+        prim_base[m + 1] = prim_base[m] + np;
+        mol_out[m + 1] = mol_out[m] + molints_npacked(nbf);
+    }
+    const int ns = shell_off[nmol], nprim = prim_base[nmol];
     molints_plan *p = new (std::nothrow) molints_plan();
     if (!p) return MOLINTS_ERR_NOMEM;
     p->ctx = ctx;
     p->opts = opts;
+    p->nmol = nmol;
     p->nshell = ns;
-    p->nbf = nbf;
-    p->npacked = molints_npacked(nbf);
+    p->npacked = mol_out[nmol];
+    p->mol_out_h.assign(mol_out.begin(), mol_out.end() - (nmol > 0 ? 1 : 0));
+    p->mol_nshell.resize(nmol);
 
     // Normalised coefficients: raw coef x (2a/pi)^(3/4) (4a)^(L/2) x CGBF norm; the component
     // factor 1/sqrt((2I-1)!!(2J-1)!!(2K-1)!!) is applied by the generated kernels
     // (PGBF/CGBF normalize!, src/Basis.jl:42-83).
-    std::vector<double> ncoef(std::max(nprim_tot, 1), 0.0);
-    std::vector<int> fn_off(ns + 1, 0);
-    for (int s = 0; s < ns; ++s) {
-        const int L = b->L[s], p0 = b->prim_off[s], K = b->nprim[s];
-        double S = 0;
-        for (int i = 0; i < K; ++i)
-            for (int j = 0; j < K; ++j) {
-                const double x = b->expn[p0 + i], y = b->expn[p0 + j];
-                S += b->coef[p0 + i] * b->coef[p0 + j] * std::pow(2 * std::sqrt(x * y) / (x + y), L + 1.5);
+    std::vector<double> xyz(3 * (size_t)std::max(ns, 1)), expn(std::max(nprim, 1)), ncoef(std::max(nprim, 1));
+    std::vector<int> L(std::max(ns, 1)), K(std::max(ns, 1)), poff(std::max(ns, 1)), fn_off(std::max(ns, 1));
+    for (int m = 0; m < nmol; ++m) {
+        const molints_basis *b = &bases[m];
+        p->mol_nshell[m] = b->nshell;
+        int f = 0;
+        for (int s = 0; s < b->nshell; ++s) {
+            const int g = shell_off[m] + s, p0 = b->prim_off[s], Ks = b->nprim[s], Ls = b->L[s];
+            for (int k = 0; k < 3; ++k) xyz[3 * g + k] = b->xyz[3 * s + k];
+            L[g] = Ls; K[g] = Ks; poff[g] = prim_base[m] + p0; fn_off[g] = f;
+            f += ncart(Ls);
+            double S = 0;
+            for (int i = 0; i < Ks; ++i)
+                for (int j = 0; j < Ks; ++j) {
+                    const double x = b->expn[p0 + i], y = b->expn[p0 + j];
+                    S += b->coef[p0 + i] * b->coef[p0 + j] * std::pow(2 * std::sqrt(x * y) / (x + y), Ls + 1.5);
+                }
+            if (!(S > 0.0)) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: zero contracted function"); }
+            const double cn = 1.0 / std::sqrt(S);
+            for (int i = 0; i < Ks; ++i) {
+                const double a = b->expn[p0 + i];
+                expn[poff[g] + i] = a;
+                ncoef[poff[g] + i] = b->coef[p0 + i] * cn * std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * Ls);
             }
-        if (!(S > 0.0)) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: zero contracted function"); }
-        const double cn = 1.0 / std::sqrt(S);
-        for (int i = 0; i < K; ++i) {
-            const double a = b->expn[p0 + i];
-            ncoef[p0 + i] = b->coef[p0 + i] * cn * std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * L);
         }
-        fn_off[s + 1] = fn_off[s] + ncart(L);
     }
 
-    // Canonical shell pairs (L_A >= L_B), ordered by class, then by descending K_A K_B.
-    struct PairRec { int cls, npp, a, b, ref; };
+    // ---- canonical shell pairs (L_A >= L_B) of every molecule, ordered by class, molecule,
+    // then descending primitive-pair count
+    struct PairRec { int cls, mol, npp, a, b, ref; };
     std::vector<PairRec> pr;
-    pr.reserve((size_t)ns * (ns + 1) / 2);
-    for (int i = 0; i < ns; ++i)
-        for (int j = 0; j <= i; ++j) {
-            int a = i, bb = j;
-            if (b->L[a] < b->L[bb]) std::swap(a, bb);
-            if (b->nprim[a] > 255 || b->nprim[bb] > 255) {
-                plan_free(p);
-                return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: more than 255 primitives in a shell");
+    for (int m = 0; m < nmol; ++m) {
+        const int n = bases[m].nshell;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j <= i; ++j) {
+                int a = shell_off[m] + i, bb = shell_off[m] + j;
+                if (L[a] < L[bb]) std::swap(a, bb);
+                pr.push_back({pair_class_of(L[a], L[bb]), m, K[a] * K[bb], a, bb, i * (i + 1) / 2 + j});
             }
-            pr.push_back({pair_class_of(b->L[a], b->L[bb]), b->nprim[a] * b->nprim[bb], a, bb,
-                          i * (i + 1) / 2 + j});
-        }
-    auto by_class_then_k = [](const PairRec &x, const PairRec &y) {
-        return x.cls != y.cls ? x.cls < y.cls : x.npp > y.npp;
+    }
+    auto order = [](const PairRec &x, const PairRec &y) {
+        if (x.cls != y.cls) return x.cls < y.cls;
+        if (x.mol != y.mol) return x.mol < y.mol;
+        return x.npp > y.npp;
     };
-    std::stable_sort(pr.begin(), pr.end(), by_class_then_k);
+    std::stable_sort(pr.begin(), pr.end(), order);
     const int npair = (int)pr.size();
     p->npair = npair;
 
-    // Stage 1: every primitive pair, for the bound pass.
     std::vector<int2> ab_h(npair);
     std::vector<int4> info_h(npair);
     std::vector<int> src_h;
     std::vector<int> cls_start(kNumPairClasses + 1, 0);
-    auto fill_tables = [&](const std::vector<std::vector<int>> *kept) {
+    std::vector<std::vector<int>> kept;  // indexed by position in the stage-1 order
+    auto fill_tables = [&](const std::vector<int> *stage1_pos) {
         src_h.clear();
         std::fill(cls_start.begin(), cls_start.end(), 0);
         for (int k = 0; k < npair; ++k) {
             ab_h[k] = make_int2(pr[k].a, pr[k].b);
             const int off = (int)src_h.size();
-            const int kb = b->nprim[pr[k].b];
-            if (kept) {
-                for (int x : (*kept)[pr[k].ref]) src_h.push_back(x);
+            if (stage1_pos) {
+                for (int x : kept[(*stage1_pos)[k]]) src_h.push_back(x);
             } else {
-                for (int ia = 0; ia < b->nprim[pr[k].a]; ++ia)
-                    for (int ib = 0; ib < kb; ++ib) src_h.push_back((ia << 8) | ib);
+                for (int ia = 0; ia < K[pr[k].a]; ++ia)
+                    for (int ib = 0; ib < K[pr[k].b]; ++ib) src_h.push_back((ia << 8) | ib);
             }
             info_h[k] = make_int4(off, (int)src_h.size() - off, fn_off[pr[k].a], fn_off[pr[k].b]);
             cls_start[pr[k].cls + 1] = k + 1;
@@ -530,17 +574,19 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
     double2 *pbound = nullptr;
     int64_t scratch = 0;
     int rc = 0;
+    const int nc2 = kNumPairClasses * kNumPairClasses;
     rc = rc ? rc : dev_alloc(ctx, &p->sh_xyz, (size_t)3 * ns, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->expn, (size_t)nprim_tot, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->ncoef, (size_t)nprim_tot, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->expn, (size_t)nprim, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->ncoef, (size_t)nprim, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->sh_poff, (size_t)ns, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->sh_nprim, (size_t)ns, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->pair_ab, (size_t)npair, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->info, (size_t)npair, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->geo, (size_t)npair, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->bnd, (size_t)npair, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->pp_src, (size_t)nall, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)nall, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->counters, (size_t)nc2, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->mol_out, (size_t)std::max(nmol, 1), &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &pbound, (size_t)nall, &scratch);
     if (rc) {
         if (pbound) { dev_free(ctx, pbound); ctx->held -= scratch; }
@@ -548,16 +594,14 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
         return rc;
     }
     cudaStream_t s = ctx->stream;
-    const size_t np = (size_t)std::max(nprim_tot, 0);
     const double c0 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
     std::vector<double2> pb_h(nall);
     PairTab P{p->info, p->geo, p->pp, p->bnd};
     BoysTab Bt = boys_of(ctx, opts.boys);
-    if ((e = cudaMemcpyAsync(p->sh_xyz, b->xyz, 3 * ns * sizeof(double), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->expn, b->expn, np * sizeof(double), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->ncoef, ncoef.data(), np * sizeof(double), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->sh_poff, b->prim_off, ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->sh_nprim, b->nprim, ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+    if ((e = cudaMemcpyAsync(p->sh_xyz, xyz.data(), 3 * (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->expn, expn.data(), (size_t)nprim * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->ncoef, ncoef.data(), (size_t)nprim * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->sh_poff, poff.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nall * sizeof(int), cudaMemcpyHostToDevice, s))) {
@@ -582,75 +626,148 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
     dev_free(ctx, pbound);
     ctx->held -= scratch;
 
-    // Stage 2: drop primitive pairs i with b_i * max Qabs < prim_cutoff (each dropped term of
-    // any integral is below prim_cutoff by the Schwarz inequality), keep pairs' bounds.
-    double qmax = 0.0;
-    std::vector<double> qabs_all(npair, 0.0);
+    // ---- stage 2: drop primitive pairs i with b_i * max Qabs (of the same molecule) below
+    // prim_cutoff -- each dropped term of any integral is below prim_cutoff by the Schwarz
+    // inequality -- and record each pair's bounds.
+    std::vector<double> qmax(std::max(nmol, 1), 0.0);
     for (int k = 0; k < npair; ++k) {
-        for (int x = 0; x < info_h[k].y; ++x) qabs_all[k] += pb_h[info_h[k].x + x].x;
-        qmax = std::max(qmax, qabs_all[k]);
+        double q = 0;
+        for (int x = 0; x < info_h[k].y; ++x) q += pb_h[info_h[k].x + x].x;
+        qmax[pr[k].mol] = std::max(qmax[pr[k].mol], q);
     }
-    std::vector<std::vector<int>> kept(npair);
-    std::vector<double2> bnd_ref(npair);
+    kept.assign(npair, {});
+    std::vector<double2> bnd1(npair);
     int64_t nkept = 0;
     for (int k = 0; k < npair; ++k) {
-        const int ref = pr[k].ref;
         double qa = 0.0, wa = 0.0;
         for (int x = 0; x < info_h[k].y; ++x) {
             const double2 bb = pb_h[info_h[k].x + x];
-            if (opts.prim_cutoff > 0.0 && bb.x * qmax < opts.prim_cutoff) continue;
-            kept[ref].push_back(src_h[info_h[k].x + x]);
+            if (opts.prim_cutoff > 0.0 && bb.x * qmax[pr[k].mol] < opts.prim_cutoff) continue;
+            kept[k].push_back(src_h[info_h[k].x + x]);
             qa += bb.x;
             wa += bb.y;
         }
-        const double *A = b->xyz + 3 * pr[k].a, *Bc = b->xyz + 3 * pr[k].b;
+        const double *A = &xyz[3 * pr[k].a], *Bc = &xyz[3 * pr[k].b];
         const double dab = std::sqrt((A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
                                      (A[2] - Bc[2]) * (A[2] - Bc[2]));
-        bnd_ref[ref] = make_double2(qa, wa * std::pow(1.0 + dab, b->L[pr[k].b]));
-        pr[k].npp = (int)kept[ref].size();
-        nkept += pr[k].npp;
+        bnd1[k] = make_double2(qa, wa * std::pow(1.0 + dab, L[pr[k].b]));
+        nkept += (int64_t)kept[k].size();
     }
     p->nprim_pair_kept = nkept;
-    std::stable_sort(pr.begin(), pr.end(), by_class_then_k);
-    fill_tables(&kept);
+    // re-sort by kept count, remembering each pair's stage-1 position
+    std::vector<int> pos1(npair);
+    for (int k = 0; k < npair; ++k) { pos1[k] = k; pr[k].npp = (int)kept[k].size(); }
+    std::vector<int> perm(npair);
+    for (int k = 0; k < npair; ++k) perm[k] = k;
+    std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return order(pr[x], pr[y]); });
+    {
+        std::vector<PairRec> pr2(npair);
+        for (int k = 0; k < npair; ++k) { pr2[k] = pr[perm[k]]; pos1[k] = perm[k]; }
+        pr.swap(pr2);
+    }
+    fill_tables(&pos1);
     for (int c = 0; c <= kNumPairClasses; ++c) p->class_start[c] = cls_start[c];
     p->pair_ref.resize(npair);
+    p->pair_mol.resize(npair);
     p->npp_h.resize(npair);
     p->bnd_h.resize(npair);
     for (int k = 0; k < npair; ++k) {
         p->pair_ref[k] = pr[k].ref;
+        p->pair_mol[k] = pr[k].mol;
         p->npp_h[k] = pr[k].npp;
-        p->bnd_h[k] = bnd_ref[pr[k].ref];
+        p->bnd_h[k] = bnd1[pos1[k]];
     }
-    {
-        // launch-order estimate: kept primitive quartets x per-class weight (VRR size)
-        std::vector<double> ksum(kNumPairClasses, 0.0), k2sum(kNumPairClasses, 0.0);
-        for (int k = 0; k < npair; ++k) {
-            ksum[pr[k].cls] += pr[k].npp;
-            k2sum[pr[k].cls] += (double)pr[k].npp * pr[k].npp;
-        }
-        for (int x = 0; x < kNumPairClasses; ++x)
-            for (int y = 0; y <= x; ++y) {
-                const double kq = (x == y) ? 0.5 * (ksum[x] * ksum[x] + k2sum[x]) : ksum[x] * ksum[y];
-                const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
-                p->class_cost[x][y] = kq * (1.0 + lsum * lsum);
+
+    // ---- work queues: per class pair, chunks of one bra pair and <= 32 ket pairs of the same
+    // molecule, ordered by decreasing estimated cost (kept primitive quartets x class weight)
+    std::vector<int> mol_cls_start((size_t)(nmol + 1) * kNumPairClasses, 0);  // [cls][mol] ranges
+    auto range_of = [&](int cls, int m, int &b0, int &b1) {
+        b0 = b1 = cls_start[cls];
+        // pairs of class cls are sorted by molecule: binary search the molecule's run
+        b0 = (int)(std::lower_bound(p->pair_mol.begin() + cls_start[cls], p->pair_mol.begin() + cls_start[cls + 1], m) -
+                   p->pair_mol.begin());
+        b1 = (int)(std::upper_bound(p->pair_mol.begin() + cls_start[cls], p->pair_mol.begin() + cls_start[cls + 1], m) -
+                   p->pair_mol.begin());
+    };
+    std::vector<int4> chunks;
+    struct CostedChunk { double cost; int4 c; };
+    std::vector<CostedChunk> tmp;
+    // chunk width: 32 ket pairs (one per lane), widened in steps of 32 for large batches so
+    // that the queues stay near kMaxChunks entries
+    constexpr double kMaxChunks = 4.0e6;
+    double nchunk32 = 0.0;
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y)
+            for (int m = 0; m < nmol; ++m) {
+                int b0, b1, k0, k1;
+                range_of(x, m, b0, b1);
+                range_of(y, m, k0, k1);
+                const double nb = b1 - b0, nk = k1 - k0;
+                nchunk32 += (x == y) ? nb * (nb + 1) / 64.0 + nb : nb * (nk / 32.0 + 1.0);
             }
-    }
+    const int width = 32 * std::max(1, (int)std::ceil(nchunk32 / kMaxChunks));
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            tmp.clear();
+            const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
+            const double w = 1.0 + lsum * lsum;
+            double total = 0.0;
+            for (int m = 0; m < nmol; ++m) {
+                int b0, b1, k0, k1;
+                range_of(x, m, b0, b1);
+                range_of(y, m, k0, k1);
+                for (int pb = b0; pb < b1; ++pb) {
+                    const int kend = (x == y) ? pb + 1 : k1;
+                    for (int q0 = k0; q0 < kend; q0 += width) {
+                        const int n = std::min(width, kend - q0);
+                        double kq = 0;
+                        for (int t = 0; t < n; ++t) kq += p->npp_h[q0 + t];
+                        const double cost = w * p->npp_h[pb] * kq;
+                        total += cost;
+                        tmp.push_back({cost, make_int4(pb, q0, n, m)});
+                    }
+                }
+            }
+            std::stable_sort(tmp.begin(), tmp.end(),
+                             [](const CostedChunk &a, const CostedChunk &b) { return a.cost > b.cost; });
+            p->q_off[x][y] = (int)chunks.size();
+            p->q_len[x][y] = (int)tmp.size();
+            p->class_cost[x][y] = total;
+            for (const CostedChunk &cc : tmp) chunks.push_back(cc.c);
+        }
+    std::vector<long long> mol_out_ll(std::max(nmol, 1), 0);
+    for (int m = 0; m < nmol; ++m) mol_out_ll[m] = (long long)p->mol_out_h[m];
+    rc = dev_alloc(ctx, &p->chunks, chunks.size(), &p->bytes);
+    if (rc) { plan_free(p); return rc; }
     if ((e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->bnd, p->bnd_h.data(), npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
         (nkept > 0 && (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nkept * sizeof(int),
                                            cudaMemcpyHostToDevice, s))) ||
+        (chunks.size() > 0 && (e = cudaMemcpyAsync(p->chunks, chunks.data(), chunks.size() * sizeof(int4),
+                                                   cudaMemcpyHostToDevice, s))) ||
+        (e = cudaMemcpyAsync(p->mol_out, mol_out_ll.data(), mol_out_ll.size() * sizeof(long long),
+                             cudaMemcpyHostToDevice, s)) ||
         (e = cudaStreamSynchronize(s))) {
         plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
     }
+    (void)mol_cls_start;
     *out = p;
     return MOLINTS_OK;
 }
 
+int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_options *opts,
+                        molints_plan **out) {
+    if (!b) return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null argument");
+    return molints_plan_create_batch(ctx, 1, b, opts, out);
+}
+
+int64_t molints_plan_npacked(const molints_plan *p) { return p ? p->npacked : MOLINTS_ERR_INVALID; }
+
 int molints_plan_execute(molints_plan *p, double *out_device) {
-    if (!p || !out_device) return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_execute: null argument");
+    if (!p || (!out_device && p->npacked > 0))
+        return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_execute: null argument");
     molints_ctx *ctx = p->ctx;
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
@@ -670,6 +787,7 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         return err == cudaSuccess ? 0 : cuda_fail(ctx, err, "cudaEventRecord");
     };
     MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
+    MI_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(int) * kNumPairClasses * kNumPairClasses, s));
     if (p->npair > 0) {
         if (int rc = mark(launches, "build_pairs", 0, s)) return rc;
         build_pairs_kernel<<<(p->npair + 127) / 128, 128, 0, s>>>(
@@ -681,17 +799,13 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
     PairTab P{p->info, p->geo, p->pp, p->bnd};
     BoysTab B = boys_of(ctx, p->opts.boys);
     const int mixed = p->opts.precision == MOLINTS_MIXED ? 1 : 0;
-    // Class-pair launches, largest estimated work first, spread over the side streams so
-    // that small classes fill the SMs next to large ones.
+    // Class-pair queues, largest estimated work first, spread over the side streams so that
+    // small classes fill the SMs next to large ones.
     struct Job { double cost; int x, y; };
     std::vector<Job> jobs;
     for (int x = 0; x < kNumPairClasses; ++x)
-        for (int y = 0; y <= x; ++y) {
-            const int nx = p->class_start[x + 1] - p->class_start[x];
-            const int ny = p->class_start[y + 1] - p->class_start[y];
-            if (nx == 0 || ny == 0) continue;
-            jobs.push_back({p->class_cost[x][y], x, y});
-        }
+        for (int y = 0; y <= x; ++y)
+            if (p->q_len[x][y] > 0) jobs.push_back({p->class_cost[x][y], x, y});
     std::stable_sort(jobs.begin(), jobs.end(), [](const Job &a, const Job &b) { return a.cost > b.cost; });
     // Profiling runs every launch on the caller's stream, so each event pair times one kernel.
     const int nside = p->profiling ? 0 : std::min<int>(molints_ctx::kSide, (int)jobs.size());
@@ -699,23 +813,22 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
     for (int i = 0; i < nside; ++i) MI_CUDA(ctx, cudaStreamWaitEvent(ctx->side[i], ctx->fork, 0));
     for (size_t k = 0; k < jobs.size(); ++k) {
         const int x = jobs[k].x, y = jobs[k].y;
-        const int nx = p->class_start[x + 1] - p->class_start[x];
-        const int ny = p->class_start[y + 1] - p->class_start[y];
         cudaStream_t st = nside ? ctx->side[k % nside] : s;
-        EriLaunch L{};
-        L.pairs = P;
-        L.boys = B;
-        L.out = out_device;
-        L.bra0 = p->class_start[x];
-        L.nbra = nx;
-        L.ket0 = p->class_start[y];
-        L.nket = ny;
-        L.tri = (x == y);
-        L.nquart = L.tri ? (long long)nx * (nx + 1) / 2 : (long long)nx * ny;
-        L.screen_cut = p->opts.screen_cutoff;
-        L.fp32_cut = p->opts.fp32_cutoff;
+        int &occ = ctx->occupancy[x][y][mixed];
+        if (occ == 0) occ = std::max(1, kEriOccupancy[x][y](mixed));
+        EriQueue Q{};
+        Q.pairs = P;
+        Q.boys = B;
+        Q.out = out_device;
+        Q.mol_out = p->mol_out;
+        Q.chunks = p->chunks + p->q_off[x][y];
+        Q.nchunks = p->q_len[x][y];
+        Q.counter = p->counters + x * kNumPairClasses + y;
+        Q.screen_cut = p->opts.screen_cutoff;
+        Q.fp32_cut = p->opts.fp32_cutoff;
+        const int grid = (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);
         if (int rc = mark(launches, kEriNames[x][y], 0, st)) return rc;
-        kEriLaunchers[x][y](L, mixed, st);
+        kEriLaunchers[x][y](Q, mixed, grid, st);
         if (int rc = mark(launches, kEriNames[x][y], 1, st)) return rc;
         ++launches;
     }
@@ -734,25 +847,32 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
     molints_ctx *ctx = p->ctx;
     std::memset(st, 0, sizeof(*st));
     st->n_eri = p->npacked;
-    const int64_t np = p->npair;
-    st->n_shell_quartets = np * (np + 1) / 2;
-    int64_t sum = 0, sum2 = 0;
-    for (int k = 0; k < p->npair; ++k) { sum += p->npp_h[k]; sum2 += (int64_t)p->npp_h[k] * p->npp_h[k]; }
-    st->n_prim_quartets = (sum * sum + sum2) / 2;
     st->n_kernel_launches = p->n_launches;
     st->n_prim_pairs = p->nprim_pair_all;
     st->n_prim_pairs_kept = p->nprim_pair_kept;
+    // per molecule: its pairs are interleaved by class, so gather them first
+    std::vector<std::vector<int>> by_mol(std::max(p->nmol, 1));
+    for (int k = 0; k < p->npair; ++k) by_mol[p->pair_mol[k]].push_back(k);
+    for (int m = 0; m < p->nmol; ++m) {
+        const std::vector<int> &v = by_mol[m];
+        const int64_t np = (int64_t)v.size();
+        st->n_shell_quartets += np * (np + 1) / 2;
+        int64_t sum = 0, sum2 = 0;
+        for (int k : v) { sum += p->npp_h[k]; sum2 += (int64_t)p->npp_h[k] * p->npp_h[k]; }
+        st->n_prim_quartets += (sum * sum + sum2) / 2;
+        for (size_t a = 0; a < v.size(); ++a)
+            for (size_t c = 0; c <= a; ++c) {
+                const double2 ba = p->bnd_h[v[a]], bc = p->bnd_h[v[c]];
+                if (ba.x * bc.x < p->opts.screen_cutoff) ++st->n_screened;
+                else if (p->opts.precision == MOLINTS_MIXED && ba.y * bc.y < p->opts.fp32_cutoff)
+                    ++st->n_fp32_quartets;
+            }
+    }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return MOLINTS_ERR_CUDA;
     if (p->n_launches > 0 && cudaEventSynchronize(ctx->ev1) == cudaSuccess) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) st->device_ms = ms;
     }
-    for (int a = 0; a < p->npair; ++a)
-        for (int c = 0; c <= a; ++c) {
-            if (p->bnd_h[a].x * p->bnd_h[c].x < p->opts.screen_cutoff) ++st->n_screened;
-            else if (p->opts.precision == MOLINTS_MIXED && p->bnd_h[a].y * p->bnd_h[c].y < p->opts.fp32_cutoff)
-                ++st->n_fp32_quartets;
-        }
     return MOLINTS_OK;
 }
 
@@ -796,7 +916,10 @@ int molints_plan_schwarz(molints_plan *p, double *out) {
     MI_CUDA(ctx, cudaMemcpyAsync(q.data(), p->qcon, p->npair * sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->stream));
     MI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    for (int k = 0; k < p->npair; ++k) out[p->pair_ref[k]] = q[k];
+    std::vector<int64_t> base(std::max(p->nmol, 1), 0);
+    for (int m = 1; m < p->nmol; ++m)
+        base[m] = base[m - 1] + (int64_t)p->mol_nshell[m - 1] * (p->mol_nshell[m - 1] + 1) / 2;
+    for (int k = 0; k < p->npair; ++k) out[base[p->pair_mol[k]] + p->pair_ref[k]] = q[k];
     return MOLINTS_OK;
 }
 

@@ -112,8 +112,22 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
     // Sizes of the per-call tables; reject what does not fit the static scratch.
     const int64_t npair = (int64_t)ns * (ns + 1) / 2;
     int64_t nall = 0;
+    int64_t ncls[kNumPairClasses] = {0};
     for (int i = 0; i < ns; ++i)
-        for (int j = 0; j <= i; ++j) nall += (int64_t)b->nprim[i] * b->nprim[j];
+        for (int j = 0; j <= i; ++j) {
+            nall += (int64_t)b->nprim[i] * b->nprim[j];
+            ncls[pair_class(std::max(b->L[i], b->L[j]), std::min(b->L[i], b->L[j]))] += 1;
+        }
+    // work-queue chunks: one bra pair and up to 32 ket pairs each
+    int64_t nchunk = 0;
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            if (x == y)
+                for (int64_t i = 0; i < ncls[x]; ++i) nchunk += (i + 1 + 31) / 32;
+            else
+                nchunk += ncls[x] * ((ncls[y] + 31) / 32);
+        }
+    const int nc2 = kNumPairClasses * kNumPairClasses;
     size_t off = 0;
     const size_t o_xyz = off;   off = align_up(off + 3 * (size_t)ns * sizeof(double));
     const size_t o_expn = off;  off = align_up(off + (size_t)nprim_tot * sizeof(double));
@@ -123,6 +137,9 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
     const size_t o_info = off;  off = align_up(off + (size_t)npair * sizeof(int4));
     const size_t o_src = off;   off = align_up(off + (size_t)nall * sizeof(int));
     const size_t o_bnd = off;   off = align_up(off + (size_t)npair * sizeof(double2));
+    const size_t o_chunk = off; off = align_up(off + (size_t)nchunk * sizeof(int4));
+    const size_t o_cnt = off;   off = align_up(off + (size_t)nc2 * sizeof(int));
+    const size_t o_mol = off;   off = align_up(off + sizeof(long long));
     const size_t upload = off;  // everything above is copied from the host mirror
     const size_t o_geo = off;   off = align_up(off + (size_t)npair * sizeof(double4));
     const size_t o_pp = off;    off = align_up(off + (size_t)nall * sizeof(PrimPair));
@@ -224,6 +241,24 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
         class_start[cls + 1] = k + 1;
     }
     for (int c = 1; c <= kNumPairClasses; ++c) class_start[c] = std::max(class_start[c], class_start[c - 1]);
+    // chunk queues in natural order; the counters and the molecule offset start at zero
+    int4 *chunk = reinterpret_cast<int4 *>(g_host + o_chunk);
+    int q_off[kNumPairClasses][kNumPairClasses] = {}, q_len[kNumPairClasses][kNumPairClasses] = {};
+    int nq = 0;
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            q_off[x][y] = nq;
+            for (int pb = class_start[x]; pb < class_start[x + 1]; ++pb) {
+                const int kend = (x == y) ? pb + 1 : class_start[y + 1];
+                for (int q0 = class_start[y]; q0 < kend; q0 += 32)
+                    chunk[nq++] = make_int4(pb, q0, std::min(32, kend - q0), 0);
+            }
+            q_len[x][y] = nq - q_off[x][y];
+        }
+    std::memset(g_host + o_cnt, 0, (size_t)nc2 * sizeof(int));
+    std::memset(g_host + o_mol, 0, sizeof(long long));
+    int nsm = 1;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) nsm = 1;
 
     // One copy of the prepared tables into the scratch, then the device path on `stream`.
     // g_host is pageable: cudaMemcpyAsync returns once it has been staged, so the next call
@@ -243,26 +278,23 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
     B.tab = nullptr;  // the class kernels read only the scaled tables
     B.scaled = reinterpret_cast<const double *>(base);
     B.t_switch = boys_mode == MOLINTS_BOYS_EXACT ? kBoysTableMax : kBoysReferenceSwitch;
-    for (int x = 0; x < kNumPairClasses; ++x) {
-        const int nx = class_start[x + 1] - class_start[x];
-        for (int y = 0; y <= x && nx > 0; ++y) {
-            const int ny = class_start[y + 1] - class_start[y];
-            if (ny == 0) continue;
-            EriLaunch L{};
-            L.pairs = P;
-            L.boys = B;
-            L.out = out_device;
-            L.bra0 = class_start[x];
-            L.nbra = nx;
-            L.ket0 = class_start[y];
-            L.nket = ny;
-            L.tri = (x == y);
-            L.nquart = L.tri ? (long long)nx * (nx + 1) / 2 : (long long)nx * ny;
-            L.screen_cut = 0.0;
-            L.fp32_cut = 0.0;
-            kEriLaunchers[x][y](L, 0, s);
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            if (q_len[x][y] == 0) continue;
+            EriQueue Q{};
+            Q.pairs = P;
+            Q.boys = B;
+            Q.out = out_device;
+            Q.mol_out = reinterpret_cast<const long long *>(data + o_mol);
+            Q.chunks = reinterpret_cast<const int4 *>(data + o_chunk) + q_off[x][y];
+            Q.nchunks = q_len[x][y];
+            Q.counter = reinterpret_cast<int *>(data + o_cnt) + x * kNumPairClasses + y;
+            Q.screen_cut = 0.0;
+            Q.fp32_cut = 0.0;
+            const int occ = std::max(1, kEriOccupancy[x][y](0));
+            const int grid = (int)std::min<long long>((long long)occ * nsm, (Q.nchunks + 3) / 4);
+            kEriLaunchers[x][y](Q, 0, grid, s);
         }
-    }
     e = cudaGetLastError();
     if (e != cudaSuccess) return noalloc_fail(err, err_len, MOLINTS_ERR_CUDA, cudaGetErrorString(e));
     return MOLINTS_OK;

@@ -34,6 +34,7 @@ EXPORTED_SYMBOLS = [
     "molints_eri_packed", "molints_plan_create", "molints_plan_execute", "molints_plan_stats",
     "molints_plan_destroy", "molints_plan_schwarz", "molints_boys_eval",
     "molints_plan_set_profiling", "molints_plan_launch_times", "molints_eri_packed_noalloc",
+    "molints_plan_create_batch", "molints_plan_npacked",
 ]
 
 
@@ -102,6 +103,8 @@ def load_library(path: Path | str | None = None):
         "molints_plan_set_profiling": (ctypes.c_int, [P, ctypes.c_int]),
         "molints_plan_launch_times": (ctypes.c_int, [P, P, P, ctypes.c_int]),
         "molints_eri_packed_noalloc": (ctypes.c_int, [P, P, P, P, ctypes.c_char_p, ctypes.c_size_t]),
+        "molints_plan_create_batch": (ctypes.c_int, [P, I32, P, P, P]),
+        "molints_plan_npacked": (I64, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -137,18 +140,30 @@ def make_options(precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0, screen_cu
 
 
 class Plan:
-    """A basis resident on the device; ``execute`` runs the whole device path."""
+    """One basis (or a batch of them) resident on the device; ``execute`` runs the whole
+    device path.  For a batch, molecule m's packed vector starts at ``offsets[m]``."""
 
     def __init__(self, engine: "Engine", shells, opts: Options):
         self.engine = engine
-        self._arrs = _BasisArrays(shells)
-        self.nbf = shells.nbf
-        self.npacked = shells.npacked
-        self.nshell = shells.nshell
+        batch = isinstance(shells, (list, tuple))
+        mols = list(shells) if batch else [shells]
+        self._arrs = [_BasisArrays(sh) for sh in mols]
+        self.nbf = [sh.nbf for sh in mols] if batch else shells.nbf
+        self.offsets = np.concatenate([[0], np.cumsum([sh.npacked for sh in mols])]).astype(np.int64)
+        self.npacked = int(self.offsets[-1])
+        self.nshell = sum(sh.nshell for sh in mols)
+        self._nshells = [sh.nshell for sh in mols]
         h = ctypes.c_void_p()
-        engine._check(engine.lib.molints_plan_create(engine.ctx, ctypes.byref(self._arrs.c),
-                                                     ctypes.byref(opts), ctypes.byref(h)))
+        if batch:
+            arr = (Basis * len(mols))(*[a.c for a in self._arrs])
+            self._carr = arr
+            engine._check(engine.lib.molints_plan_create_batch(engine.ctx, len(mols), arr,
+                                                               ctypes.byref(opts), ctypes.byref(h)))
+        else:
+            engine._check(engine.lib.molints_plan_create(engine.ctx, ctypes.byref(self._arrs[0].c),
+                                                         ctypes.byref(opts), ctypes.byref(h)))
         self.h = h
+        assert engine.lib.molints_plan_npacked(h) == self.npacked
 
     def execute(self, out_device_ptr: int) -> None:
         """Queue the device path on the engine's stream, writing npacked doubles."""
@@ -172,7 +187,7 @@ class Plan:
         return [(names[k].decode(), float(ms[k])) for k in range(min(n, cap))]
 
     def schwarz(self) -> np.ndarray:
-        out = np.zeros(self.nshell * (self.nshell + 1) // 2)
+        out = np.zeros(sum(n * (n + 1) // 2 for n in self._nshells))
         self.engine._check(self.engine.lib.molints_plan_schwarz(self.h, _ptr(out)))
         return out
 
@@ -249,6 +264,12 @@ class Engine:
              screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF) -> Plan:
         return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff,
                                                prim_cutoff=prim_cutoff))
+
+    def plan_batch(self, shells_list, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
+                   screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF) -> Plan:
+        """One plan over several molecules: a single execute computes all of them."""
+        return Plan(self, list(shells_list), make_options(precision, boys, fp32_cutoff,
+                                                          screen_cutoff, prim_cutoff=prim_cutoff))
 
     def boys(self, mmax: int, T, mode=BOYS_REFERENCE) -> np.ndarray:
         T = np.ascontiguousarray(T, dtype=np.float64)

@@ -214,6 +214,30 @@ def test_plan_execute_twice_on_torch_stream(eng, oracle):
     assert np.max(np.abs(first - oracle.eri_packed_hgp(sh))) < TOL_FP64
 
 
+def test_batch_plan_equals_single_plans(eng):
+    """Three molecules in one batch plan (one work queue per class pair across molecules)
+    give each molecule's single-plan vector exactly, at its offset."""
+    import torch
+    mols = [mi.config2(), mi.config0(), _rand_basis(105, 2)]
+    plan = eng.plan_batch(mols)
+    out = torch.full((plan.npacked,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    eng.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        plan.execute(out.data_ptr())
+    finally:
+        eng.set_stream(None)
+    got = out.cpu().numpy()
+    assert not np.isnan(got).any()
+    for m, sh in enumerate(mols):
+        single = eng.eri_packed(sh)
+        part = got[plan.offsets[m]:plan.offsets[m + 1]]
+        assert np.array_equal(part, single), m
+    st = plan.stats()
+    assert st["n_eri"] == plan.npacked
+    plan.close()
+
+
 def test_edge_cases(eng):
     from molints_b200 import engine
     one = mi.Shells.from_list([((0.0, 0.0, 0.0), 0, [(1.0, 1.0)])])
