@@ -257,6 +257,8 @@ def run_ours(args):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": npacked * 8,
            "timing": "host wall clock around molints_eri_packed (synchronous call)"}
 
+    batch = measure_batch(eng, stream, dev, fp32_cut, rank, world)
+
     cpu = None
     if rank == 0 and world == 1:
         r, dt, passes = cpu_reference_rate(sh, os.cpu_count() or 1, CPU_SAMPLE_SECONDS)
@@ -284,6 +286,7 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batch_config3": batch,
             "gpu_launches": args.steps * 2 * plan64.stats()["n_kernel_launches"],
             "clocks": clocks,
         }
@@ -295,6 +298,60 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def measure_batch(eng, stream, dev, fp32_cut, rank, world, cap=1.5e9):
+    """The 256-molecule batch (4-40 atoms, l <= 2, 4.9e10 integrals): molecules sharded over
+    ranks round-robin by size, grouped into batch plans of at most `cap` doubles of output
+    each (HBM holds one group's output at a time), every shell quartet of a group in one work
+    queue per class pair.  Device-timed executes of all groups, FP64 and MIXED; plan creation
+    (host tables, device bound pass) is timed separately."""
+    import torch
+    from molints_b200 import engine as E
+    mols = mi.config3(256)
+    order = sorted(range(len(mols)), key=lambda i: -mols[i].npacked)
+    mine = order[rank::world]
+    groups, cur, tot = [], [], 0
+    for i in mine:
+        if cur and tot + mols[i].npacked > cap:
+            groups.append(cur)
+            cur, tot = [], 0
+        cur.append(i)
+        tot += mols[i].npacked
+    if cur:
+        groups.append(cur)
+    n_eri = sum(mols[i].npacked for i in mine)
+    out = torch.empty(int(max(sum(mols[i].npacked for i in g) for g in groups)), dtype=torch.float64,
+                      device=dev)
+    eng.set_stream(stream.cuda_stream)
+    res = {"workload": "256 molecules, seeds 3000+m, l<=2, K in {1,3,6,7}", "n_eri_this_rank": n_eri,
+           "groups": len(groups), "output_cap_doubles": cap}
+    for name, prec, cut in (("fp64", E.FP64, 0.0), ("mixed", E.MIXED, fp32_cut)):
+        t_plan = t_exec = 0.0
+        for g in groups:
+            t0 = time.perf_counter()
+            plan = eng.plan_batch([mols[i] for i in g], precision=prec, fp32_cutoff=cut)
+            t_plan += time.perf_counter() - t0
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            plan.execute(out.data_ptr())
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            t_exec += a.elapsed_time(b) * 1e-3
+            plan.close()
+        tot_eri, t_max = float(n_eri), t_exec
+        if world > 1:
+            import torch.distributed as dist
+            v = torch.tensor([float(n_eri), t_exec], dtype=torch.float64, device=dev)
+            n_t = v[:1].clone()
+            dist.all_reduce(n_t, op=dist.ReduceOp.SUM)
+            t_t = v[1:].clone()
+            dist.all_reduce(t_t, op=dist.ReduceOp.MAX)
+            tot_eri, t_max = n_t.item(), t_t.item()
+        res[name] = {"value": tot_eri / t_max, "unit": UNIT, "exec_s_max_over_ranks": t_max,
+                     "plan_s": t_plan}
+    res["fp32_cutoff"] = fp32_cut
+    return res
 
 
 def measure_fp64_peak(dev) -> float:

@@ -692,6 +692,7 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
     std::vector<int4> chunks;
     struct CostedChunk { double cost; int4 c; };
     std::vector<CostedChunk> tmp;
+    chunks.reserve(1 << 16);
     // chunk width: 32 ket pairs (one per lane), widened in steps of 32 for large batches so
     // that the queues stay near kMaxChunks entries
     constexpr double kMaxChunks = 4.0e6;
@@ -728,12 +729,23 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
                     }
                 }
             }
-            std::stable_sort(tmp.begin(), tmp.end(),
-                             [](const CostedChunk &a, const CostedChunk &b) { return a.cost > b.cost; });
+            // heaviest first, bucketed by log2(cost): an O(n) order that is all the load
+            // balance needs (a full sort of millions of chunks dominated large batches)
+            constexpr int kBuckets = 64;
+            int cnt[kBuckets + 1] = {0};
+            auto bucket = [](double c) {
+                int e2 = 0;
+                std::frexp(c > 0 ? c : 1.0, &e2);
+                return std::max(0, std::min(kBuckets - 1, kBuckets - 1 - (e2 + 8)));
+            };
+            for (const CostedChunk &cc : tmp) ++cnt[bucket(cc.cost) + 1];
+            for (int k = 1; k <= kBuckets; ++k) cnt[k] += cnt[k - 1];
             p->q_off[x][y] = (int)chunks.size();
             p->q_len[x][y] = (int)tmp.size();
             p->class_cost[x][y] = total;
-            for (const CostedChunk &cc : tmp) chunks.push_back(cc.c);
+            chunks.resize(chunks.size() + tmp.size());
+            int4 *dst = chunks.data() + p->q_off[x][y];
+            for (const CostedChunk &cc : tmp) dst[cnt[bucket(cc.cost)]++] = cc.c;
         }
     std::vector<long long> mol_out_ll(std::max(nmol, 1), 0);
     for (int m = 0; m < nmol; ++m) mol_out_ll[m] = (long long)p->mol_out_h[m];
