@@ -477,3 +477,218 @@ int oracle_eri_packed_huzinaga(int nshell, const double *xyz, const int *L, cons
     d_basis_release(&b);
     return 0;
 }
+
+/* ---------------------------------------------------------------- Rys quadrature */
+
+/* Rys roots and weights in long double, independently of the reference's fitted polynomials
+ * (Root1..Root5, src/Rys.jl:176-1478): the measure exp(-X t^2) dt on t in [0,1] is
+ * discretised by Gauss-Legendre on [0, t_max] (t_max = min(1, sqrt(80/X)), beyond which the
+ * measure is below e^-80), the Stieltjes procedure gives the recurrence of the polynomials
+ * orthogonal in x = t^2 (discretised Stieltjes, Gautschi), the nodes are the zeros of the
+ * degree-n polynomial found by Sturm bisection of the Jacobi matrix, and the weights are the
+ * Christoffel numbers 1 / sum_k p_k(x_i)^2 of the orthonormal polynomials. */
+#define RYS_NGL 240
+static long double g_gl_t[RYS_NGL], g_gl_w[RYS_NGL];
+static int g_gl_ready = 0;
+
+static void gauss_legendre_ld(void) {
+    if (g_gl_ready) return;
+    const int n = RYS_NGL;
+    const long double pi = 3.14159265358979323846264338327950288L;
+    for (int i = 0; i < (n + 1) / 2; ++i) {
+        long double z = cosl(pi * (i + 0.75L) / (n + 0.5L)), pp = 0;
+        for (int it = 0; it < 100; ++it) {
+            long double p1 = 1, p2 = 0;
+            for (int j = 1; j <= n; ++j) {
+                long double p3 = p2;
+                p2 = p1;
+                p1 = ((2 * j - 1) * z * p2 - (j - 1) * p3) / j;
+            }
+            pp = n * (z * p1 - p2) / (z * z - 1);
+            long double dz = p1 / pp;
+            z -= dz;
+            if (fabsl(dz) < 1e-21L) break;
+        }
+        /* nodes on [-1,1] -> [0,1] */
+        g_gl_t[i] = (1 - z) / 2;
+        g_gl_t[n - 1 - i] = (1 + z) / 2;
+        g_gl_w[i] = g_gl_w[n - 1 - i] = 1.0L / ((1 - z * z) * pp * pp);
+    }
+    g_gl_ready = 1;
+}
+
+/* number of eigenvalues of the symmetric tridiagonal (a, sqrt(b)) below x (Sturm count) */
+static int sturm_count(int n, const long double *a, const long double *b, long double x) {
+    int c = 0;
+    long double q = a[0] - x;
+    if (q < 0) ++c;
+    for (int k = 1; k < n; ++k) {
+        if (q == 0) q = 1e-4000L;
+        q = (a[k] - x) - b[k] / q;
+        if (q < 0) ++c;
+    }
+    return c;
+}
+
+int oracle_rys_roots(int n, double X, double *roots, double *weights) {
+    if (n < 1 || n > 12 || !(X >= 0)) return -1;
+    gauss_legendre_ld();
+    long double tmax = X > 80.0 ? sqrtl(80.0L / X) : 1.0L;
+    long double x[RYS_NGL], lam[RYS_NGL], p0[RYS_NGL], p1[RYS_NGL];
+    for (int k = 0; k < RYS_NGL; ++k) {
+        long double t = tmax * g_gl_t[k];
+        x[k] = t * t;
+        lam[k] = tmax * g_gl_w[k] * expl(-(long double)X * t * t);
+        p0[k] = 0;
+        p1[k] = 1;
+    }
+    long double a[16], b[16], norm_prev = 0;
+    for (int j = 0; j < n; ++j) {
+        long double nrm = 0, xn = 0;
+        for (int k = 0; k < RYS_NGL; ++k) {
+            nrm += lam[k] * p1[k] * p1[k];
+            xn += lam[k] * x[k] * p1[k] * p1[k];
+        }
+        a[j] = xn / nrm;
+        b[j] = j == 0 ? nrm : nrm / norm_prev;
+        norm_prev = nrm;
+        for (int k = 0; k < RYS_NGL; ++k) {
+            long double pn = (x[k] - a[j]) * p1[k] - (j ? b[j] : 0) * p0[k];
+            p0[k] = p1[k];
+            p1[k] = pn;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        long double lo = 0, hi = 1;
+        for (int it = 0; it < 200; ++it) {
+            long double mid = (lo + hi) / 2;
+            if (sturm_count(n, a, b, mid) > i) hi = mid; else lo = mid;
+            if (hi - lo < 1e-22L * hi) break;
+        }
+        long double xi = (lo + hi) / 2;
+        /* orthonormal polynomials at xi: p_{k+1} = ((x - a_k) p_k - sqrt(b_k) p_{k-1}) / sqrt(b_{k+1}) */
+        long double s = 0, q0 = 0, q1 = 1 / sqrtl(b[0]);
+        s += q1 * q1;
+        for (int k = 0; k + 1 < n; ++k) {
+            long double q2 = ((xi - a[k]) * q1 - (k ? sqrtl(b[k]) : 0) * q0) / sqrtl(b[k + 1]);
+            q0 = q1;
+            q1 = q2;
+            s += q1 * q1;
+        }
+        roots[i] = (double)xi;
+        weights[i] = (double)(1 / s);
+    }
+    return 0;
+}
+
+/* RecurFactors, Recur, Shift and Int1d of src/Rys.jl:86-156, with the root in x = t^2
+ * (the reference passes u = t^2/(1-t^2): 1/(1+u) = 1-x, u/(1+u) = x). */
+static double rys_int1d(double x, int i, int j, int k, int l, double xi, double xj, double xk,
+                        double xl, double ai, double aj, double ak, double al, double G[8][8]) {
+    const int n = i + j, m = k + l;
+    const double A = ai + aj, B = ak + al;
+    const double Px = (ai * xi + aj * xj) / A, Qx = (ak * xk + al * xl) / B;
+    const double ooopt = 1 - x, fact = x / (A + B);
+    const double B0 = 0.5 * fact, B1 = 0.5 * ooopt / A + 0.5 * fact, B1p = 0.5 * ooopt / B + 0.5 * fact;
+    const double C = (Px - xi) * ooopt + (B * (Qx - xi) + A * (Px - xi)) * fact;
+    const double Cp = (Qx - xk) * ooopt + (B * (Qx - xk) + A * (Px - xk)) * fact;
+    G[0][0] = M_PI * exp(-ai * aj * (xi - xj) * (xi - xj) / (ai + aj) -
+                         ak * al * (xk - xl) * (xk - xl) / (ak + al)) / sqrt(A * B);
+    if (n > 0) G[1][0] = C * G[0][0];
+    if (m > 0) G[0][1] = Cp * G[0][0];
+    for (int a = 2; a <= n; ++a) G[a][0] = B1 * (a - 1) * G[a - 2][0] + C * G[a - 1][0];
+    for (int bb = 2; bb <= m; ++bb) G[0][bb] = B1p * (bb - 1) * G[0][bb - 2] + Cp * G[0][bb - 1];
+    if (m > 0 && n > 0)
+        for (int a = 1; a <= n; ++a) {
+            G[a][1] = a * B0 * G[a - 1][0] + Cp * G[a][0];
+            for (int bb = 2; bb <= m; ++bb)
+                G[a][bb] = B1p * (bb - 1) * G[a][bb - 2] + a * B0 * G[a - 1][bb - 1] + Cp * G[a][bb - 1];
+        }
+    /* Shift: I(i,j,k,l) from G(n,m) = I(n,0,m,0) */
+    double ijkl = 0;
+    for (int mm = 0; mm <= l; ++mm) {
+        double ijm0 = 0;
+        for (int nn = 0; nn <= j; ++nn) ijm0 += binom(j, nn) * ipow(xi - xj, j - nn) * G[nn + i][mm + k];
+        ijkl += binom(l, mm) * ipow(xk - xl, l - mm) * ijm0;
+    }
+    return ijkl;
+}
+
+/* coulomb_rys(PGBF...) without norms, src/Rys.jl:59-83. */
+double oracle_coulomb_rys_prim(double aexpn, const double *A, const int *ia, double bexpn,
+                               const double *B, const int *ib, double cexpn, const double *C,
+                               const int *ic, double dexpn, const double *D, const int *id) {
+    int norder = (ia[0] + ia[1] + ia[2] + ib[0] + ib[1] + ib[2] + ic[0] + ic[1] + ic[2] + id[0] +
+                  id[1] + id[2]) / 2 + 1;
+    double zeta = aexpn + bexpn, eta = cexpn + dexpn, rho = zeta * eta / (zeta + eta);
+    double P[3], Q[3], rpq2 = 0;
+    for (int t = 0; t < 3; ++t) {
+        P[t] = (aexpn * A[t] + bexpn * B[t]) / zeta;
+        Q[t] = (cexpn * C[t] + dexpn * D[t]) / eta;
+        rpq2 += (P[t] - Q[t]) * (P[t] - Q[t]);
+    }
+    double roots[16], weights[16], G[8][8], s = 0;
+    if (oracle_rys_roots(norder, rpq2 * rho, roots, weights) != 0) return NAN;
+    for (int r = 0; r < norder; ++r) {
+        double v = weights[r];
+        for (int t = 0; t < 3; ++t)
+            v *= rys_int1d(roots[r], ia[t], ib[t], ic[t], id[t], A[t], B[t], C[t], D[t], aexpn, bexpn,
+                           cexpn, dexpn, G);
+        s += v;
+    }
+    return 2 * sqrt(rho / M_PI) * s;
+}
+
+/* all_twoe_ints_rys, src/Rys.jl:16-43, with the contracted-function norms applied (D4): one
+ * normalised contracted Rys integral per unique function quartet, at iindex. */
+int oracle_eri_packed_rys(int nshell, const double *xyz, const int *L, const int *nprim,
+                          const int *prim_off, const double *expn, const double *coef,
+                          double *out, int nthreads) {
+    oracle_init();
+    d_basis b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0, 0, 0};
+    for (int s = 0; s < nshell; ++s)
+        if (L[s] < 0 || L[s] > 4 || nprim[s] < 1) return -1;
+    d_basis_prepare(&b);
+    int n = b.nbf;
+    int *fsh = (int *)malloc(sizeof(int) * n), *fao = (int *)malloc(sizeof(int) * n);
+    for (int s = 0; s < nshell; ++s)
+        for (int m = 0; m < g_ncart[L[s]]; ++m) {
+            fsh[b.fn_off[s] + m] = s;
+            fao[b.fn_off[s] + m] = (L[s] ? g_nao[L[s] - 1] : 0) + m;
+        }
+    int64_t npair = (int64_t)n * (n + 1) / 2;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1)
+    for (int64_t ij = 0; ij < npair; ++ij) {
+        int64_t i = (int64_t)((sqrt(8.0 * (double)ij + 1.0) - 1.0) / 2.0);
+        while (tri64(i) > ij) --i;
+        while (tri64(i + 1) <= ij) ++i;
+        int f[4] = {(int)i, (int)(ij - tri64(i)), 0, 0};
+        for (int64_t kl = 0; kl <= ij; ++kl) {
+            int64_t k = (int64_t)((sqrt(8.0 * (double)kl + 1.0) - 1.0) / 2.0);
+            while (tri64(k) > kl) --k;
+            while (tri64(k + 1) <= kl) ++k;
+            f[2] = (int)k;
+            f[3] = (int)(kl - tri64(k));
+            int sh[4];
+            for (int t = 0; t < 4; ++t) sh[t] = fsh[f[t]];
+            double s = 0;
+            for (int pa = 0; pa < nprim[sh[0]]; ++pa)
+                for (int pb = 0; pb < nprim[sh[1]]; ++pb)
+                    for (int pc = 0; pc < nprim[sh[2]]; ++pc)
+                        for (int pd = 0; pd < nprim[sh[3]]; ++pd) {
+                            int ii[4] = {prim_off[sh[0]] + pa, prim_off[sh[1]] + pb,
+                                         prim_off[sh[2]] + pc, prim_off[sh[3]] + pd};
+                            double v = oracle_coulomb_rys_prim(
+                                expn[ii[0]], xyz + 3 * sh[0], g_ao2m[fao[f[0]]], expn[ii[1]],
+                                xyz + 3 * sh[1], g_ao2m[fao[f[1]]], expn[ii[2]], xyz + 3 * sh[2],
+                                g_ao2m[fao[f[2]]], expn[ii[3]], xyz + 3 * sh[3], g_ao2m[fao[f[3]]]);
+                            s += b.ncoef[ii[0]] * b.ncoef[ii[1]] * b.ncoef[ii[2]] * b.ncoef[ii[3]] * v;
+                        }
+            for (int t = 0; t < 4; ++t) s *= d_comp_factor(fao[f[t]]);
+            out[tri64(ij) + kl] = s;
+        }
+    }
+    free(fsh); free(fao);
+    d_basis_release(&b);
+    return 0;
+}

@@ -80,6 +80,12 @@ def lib():
         L.oracle_eri_packed_hgp_ld.argtypes = drv
         L.oracle_eri_packed_hgp_sample.restype = ctypes.c_int64
         L.oracle_eri_packed_hgp_sample.argtypes = drv + [ctypes.c_int64]
+        L.oracle_rys_roots.restype = _I
+        L.oracle_rys_roots.argtypes = [_I, _D, _P, _P]
+        L.oracle_eri_packed_rys.restype = _I
+        L.oracle_eri_packed_rys.argtypes = drv
+        L.oracle_coulomb_rys_prim.restype = _D
+        L.oracle_coulomb_rys_prim.argtypes = [_D, _P, _P, _D, _P, _P, _D, _P, _P, _D, _P, _P]
         L.oracle_set_orientation.argtypes = [_I]
         L.oracle_get_orientation.restype = _I
         L.oracle_set_boys_tmax.argtypes = [_D]
@@ -358,3 +364,70 @@ def contracted_mpmath(shells, funcs, dps: int = 40) -> float:
                 cf *= nc[k]
             tot += cf * coulomb_mpmath(*args, dps=dps)
         return float(tot * gfac)
+
+
+# ------------------------------------------------------------------ Rys
+def rys_roots(n: int, X: float):
+    """Nodes x_i = t_i^2 and weights of the n-point Rys rule (long-double discretised
+    Stieltjes; the reference's Roots for n <= 5, src/Rys.jl:161-174)."""
+    r = np.zeros(n)
+    w = np.zeros(n)
+    if lib().oracle_rys_roots(n, X, _ptr(r), _ptr(w)) != 0:
+        raise ValueError("oracle_rys_roots: bad n or X")
+    return r, w
+
+
+def rys_roots_mpmath(n: int, X: float, dps: int = 50):
+    """The same rule from the moments F_k(X) at `dps` digits (modified Chebyshev algorithm +
+    Golub-Welsch), for pinning."""
+    import mpmath
+    with mpmath.workdps(dps):
+        Xm = mpmath.mpf(X)
+
+        def boys(k):
+            if Xm == 0:
+                return mpmath.mpf(1) / (2 * k + 1)
+            a = mpmath.mpf(k) + mpmath.mpf(1) / 2
+            return mpmath.gammainc(a, 0, Xm) / (2 * Xm ** a)
+        mu = [boys(k) for k in range(2 * n)]
+        s2, s1 = [mpmath.mpf(0)] * (2 * n), mu[:]
+        al, be = [mu[1] / mu[0]], [mu[0]]
+        for k in range(1, n):
+            sg = [mpmath.mpf(0)] * (2 * n)
+            for l in range(k, 2 * n - k):
+                sg[l] = s1[l + 1] - al[k - 1] * s1[l] - be[k - 1] * s2[l]
+            al.append(sg[k + 1] / sg[k] - s1[k] / s1[k - 1])
+            be.append(sg[k] / s1[k - 1])
+            s2, s1 = s1, sg
+        J = mpmath.zeros(n, n)
+        for i in range(n):
+            J[i, i] = al[i]
+            if i + 1 < n:
+                J[i, i + 1] = J[i + 1, i] = mpmath.sqrt(be[i + 1])
+        E, Q = mpmath.eigsy(J)
+        idx = sorted(range(n), key=lambda i: E[i])
+        return (np.array([float(E[i]) for i in idx]),
+                np.array([float(be[0] * Q[0, i] ** 2) for i in idx]))
+
+
+def coulomb_rys_prim(a, b, c, d) -> float:
+    """coulomb_rys on raw primitives (src/Rys.jl:59-83); args (expn, xyz, ijk)."""
+    args = []
+    keep = []
+    for expn, xyz, ijk in (a, b, c, d):
+        X = np.ascontiguousarray(xyz, dtype=np.float64)
+        I = np.ascontiguousarray(ijk, dtype=np.int32)
+        keep += [X, I]
+        args += [float(expn), _ptr(X), _ptr(I)]
+    return lib().oracle_coulomb_rys_prim(*args)
+
+
+def eri_packed_rys(shells, nthreads: int = 1) -> np.ndarray:
+    """all_twoe_ints_rys (src/Rys.jl:16-43) with the CGBF norms applied (D4)."""
+    arrs = _shell_arrays(shells)
+    n = shells.nbf
+    out = np.zeros(n * (n + 1) * (n * n + n + 2) // 8)
+    rc = lib().oracle_eri_packed_rys(len(arrs[1]), *[_ptr(a) for a in arrs], _ptr(out), nthreads)
+    if rc != 0:
+        raise ValueError("oracle_eri_packed_rys: unsupported shell")
+    return out

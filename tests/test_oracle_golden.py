@@ -169,3 +169,48 @@ def test_hrr_orientation_conditioning(oracle):
     eng_order = oracle.shell_quartet(two, 1, 0, 1, 0)[3, 1, 3, 1]
     assert abs(eng_order - exact) < 1e-15
     assert abs(ref_order - exact) > 1e-12
+
+
+# ------------------------------------------------------------------ Rys (src/Rys.jl)
+def test_rys_golden_pins(golden, oracle):
+    """The coulomb_rys known answers of test/runtests.jl:130-149 (same values as coulomb)."""
+    o = (0.0, 0.0, 0.0)
+    s = (1.0, o, (0, 0, 0))
+    px = (1.0, o, (1, 0, 0))
+    ns, npx = oracle.pgbf_norm(1.0, 0, 0, 0), oracle.pgbf_norm(1.0, 1, 0, 0)
+    g = golden["coulomb"]
+    assert ns ** 4 * oracle.coulomb_rys_prim(s, s, s, s) == pytest.approx(g["c,c,c,c"]["value"], rel=RTOL_REF)
+    assert ns ** 2 * npx ** 2 * oracle.coulomb_rys_prim(s, s, px, px) == pytest.approx(
+        g["s,s,px,px"]["value"], rel=RTOL_REF)
+    assert abs(oracle.coulomb_rys_prim(s, s, s, px)) < 1e-17
+    for case in golden["ss_distance_sweep"]:
+        s3 = (1.0, (0.0, 0.0, case["r"]), (0, 0, 0))
+        assert ns ** 4 * oracle.coulomb_rys_prim(s, s, s3, s3) == pytest.approx(case["value"], rel=RTOL_REF)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7])
+def test_rys_roots_against_mpmath(oracle, n):
+    for X in [0.0, 1e-9, 0.4, 3.3, 17.0, 49.5, 99.9, 100.0, 640.0, 1e5]:
+        r, w = oracle.rys_roots(n, X)
+        R, W = oracle.rys_roots_mpmath(n, X)
+        assert np.max(np.abs(r - R) / R) < 4e-15, (n, X)
+        assert np.max(np.abs(w - W) / W) < 4e-15, (n, X)
+        # sum W_i x_i^k = F_k(X)
+        for k in range(2 * n):
+            assert np.sum(w * r ** k) == pytest.approx(oracle.boys_mpmath(k, X), rel=1e-13)
+
+
+def test_rys_h2_whole_basis(oracle):
+    """test/runtests.jl:60 compares all_twoe_ints_rys with all_twoe_ints at rtol 1e-7."""
+    sh = mi.build_basis(mi.h2())
+    assert np.max(np.abs(oracle.eri_packed_rys(sh) - oracle.eri_packed_huzinaga(sh))) < 1e-15
+
+
+@pytest.mark.parametrize("lmax,seed", [(1, 11), (2, 12), (3, 13)])
+def test_rys_equals_hgp_random_classes(oracle, lmax, seed):
+    """Rys with the CGBF norms applied (D4 fixed) equals the long-double HGP up to f shells."""
+    sh = _small_random_basis(seed, lmax)
+    r = oracle.eri_packed_rys(sh, nthreads=8)
+    with oracle.exact_boys():
+        h = oracle.eri_packed_hgp_ld(sh, nthreads=8)
+    assert np.max(np.abs(r - h)) < 1e-13 * max(1.0, np.max(np.abs(h)))
