@@ -258,6 +258,7 @@ def run_ours(args):
            "timing": "host wall clock around molints_eri_packed (synchronous call)"}
 
     batch = measure_batch(eng, stream, dev, fp32_cut, rank, world)
+    serving = measure_serving(local, fp32_cut, args.serve_window, rank)
 
     cpu = None
     if rank == 0 and world == 1:
@@ -287,6 +288,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "batch_config3": batch,
+            "serving_config4": serving,
             "gpu_launches": args.steps * 2 * plan64.stats()["n_kernel_launches"],
             "clocks": clocks,
         }
@@ -354,6 +356,76 @@ def measure_batch(eng, stream, dev, fp32_cut, rank, world, cap=1.5e9):
     return res
 
 
+def measure_serving(device, fp32_cut, window_s, rank, rate=200.0, nslots=8,
+                    budget=150 * 10**9):
+    """The serving stream: Poisson arrivals (mean `rate` per s over `window_s` s) of
+    synthetic molecules with 20-285 cartesian functions, l <= 3 (f shells on heavy atoms
+    half the time), submitted to the engine's server as they arrive.  The server admits them
+    against a 150 GB HBM ledger (result vectors kept resident until released plus the pair
+    tables of running plans) into `nslots` concurrent slots.  The client releases each result
+    as soon as it is ready.  Latency = completion - submission (host steady clock inside the
+    library); throughput = integrals / (last completion - first arrival).  FP64 and MIXED."""
+    from molints_b200 import engine as E
+    arrivals = mi.config4_arrivals(rate=rate, window_s=window_s)
+    mols = [mi.config4_request(r) for r in range(len(arrivals))]
+    out = {"workload": f"Poisson {rate:g}/s for {window_s:g} s, {len(mols)} molecules "
+                       f"({min(m.nbf for m in mols)}-{max(m.nbf for m in mols)} functions, l<=3)",
+           "slots": nslots, "hbm_budget_bytes": budget,
+           "n_eri": int(sum(m.npacked for m in mols))}
+    srv = E.Engine(device)
+    try:
+        srv.serve_start(nslots=nslots, hbm_budget_bytes=budget)
+        for sh in mols[:nslots]:  # warm-up: kernel attributes, pools
+            r = srv.submit(sh)
+            r.poll(-1)
+            r.release()
+        for name, prec, cut in (("fp64", E.FP64, 0.0), ("mixed", E.MIXED, fp32_cut)):
+            pending, lat = [], []
+            t0 = time.perf_counter()
+            first = last = None
+            k = 0
+            while k < len(mols) or pending:
+                now = time.perf_counter() - t0
+                while k < len(mols) and arrivals[k] <= now:
+                    pending.append(srv.submit(mols[k], precision=prec, fp32_cutoff=cut))
+                    k += 1
+                still = []
+                for r in pending:
+                    if r.poll(0):
+                        inf = r.info()
+                        lat.append(inf["t_done"] - inf["t_submit"])
+                        first = inf["t_submit"] if first is None else min(first, inf["t_submit"])
+                        last = inf["t_done"] if last is None else max(last, inf["t_done"])
+                        r.release()
+                    else:
+                        still.append(r)
+                pending = still
+                if k < len(mols):
+                    time.sleep(max(0.0, min(0.002, arrivals[k] - (time.perf_counter() - t0))))
+                else:
+                    time.sleep(0.001)
+            lat = np.array(lat) * 1e3
+            out[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+                         "throughput_eri_per_s": out["n_eri"] / (last - first),
+                         "requests_per_s": len(mols) / (last - first), "span_s": last - first}
+        # accuracy of the mixed path on a sample of the stream
+        errs = []
+        for sh in mols[:6]:
+            a = srv.submit(sh)
+            b = srv.submit(sh, precision=E.MIXED, fp32_cutoff=fp32_cut)
+            a.poll(-1)
+            b.poll(-1)
+            errs.append(float(np.max(np.abs(a.result() - b.result()))))
+            a.release()
+            b.release()
+        out["max_abs_err_mixed_vs_fp64_sample"] = max(errs)
+        out["fp32_cutoff"] = fp32_cut
+    finally:
+        srv.close()
+    return out
+
+
 def measure_fp64_peak(dev) -> float:
     import torch
     a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
@@ -377,6 +449,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--serve-window", type=float, default=5.0,
+                    help="seconds of Poisson arrivals in the serving measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

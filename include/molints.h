@@ -37,7 +37,11 @@ enum molints_status {
     MOLINTS_ERR_NOMEM = -6         /* host allocation failed */
 };
 
-enum molints_method { MOLINTS_METHOD_AUTO = 0, MOLINTS_METHOD_HGP = 1 };
+/* AUTO: per class pair, the context's method table (molints_set_class_methods), else HGP where
+ * an HGP kernel exists (shells up to d) and Rys otherwise.  HGP: all_twoe_ints_chrr's
+ * algorithm (src/HGP.jl:22-242) wherever it exists, Rys for classes with an f shell.  RYS:
+ * all_twoe_ints_rys's algorithm (src/Rys.jl:16-156) for every class pair. */
+enum molints_method { MOLINTS_METHOD_AUTO = 0, MOLINTS_METHOD_HGP = 1, MOLINTS_METHOD_RYS = 2 };
 enum molints_precision { MOLINTS_FP64 = 0, MOLINTS_MIXED = 1 };
 enum molints_boys {
     /* farray of src/Boys.jl:19-27: exact F_m below T = 30, the asymptotic form (without the
@@ -47,8 +51,13 @@ enum molints_boys {
     MOLINTS_BOYS_EXACT = 1
 };
 
-/* Largest shell angular momentum the engine accepts (d = 2). */
-#define MOLINTS_LMAX 2
+/* Largest shell angular momentum the engine accepts (f = 3).  Class pairs with an f shell run
+ * the Rys kernels (n <= 7 roots). */
+#define MOLINTS_LMAX 3
+/* Number of shell-pair classes, ordered by la+lb then la: ss ps pp ds dp fs dd fp df fd ff.
+ * A pair is oriented with the larger L first, except that equal-L pairs and f-d pairs put the
+ * tighter shell first (hence the class df). */
+#define MOLINTS_NUM_PAIR_CLASSES 11
 
 /* A basis set as flat shell arrays: what the reference's Basis/Shell hold
  * (src/Basis.jl:147-177).  Functions are numbered shell by shell, components in the
@@ -67,7 +76,8 @@ typedef struct molints_basis {
 typedef struct molints_options {
     int32_t method;          /* enum molints_method */
     int32_t precision;       /* enum molints_precision */
-    int32_t boys;            /* enum molints_boys */
+    int32_t boys;            /* enum molints_boys; the Rys kernels always evaluate the exact
+                                quadrature (there is no T >= 30 branch to follow) */
     int32_t reserved;
     /* Both cutoffs compare against B = Qabs_ab * Qabs_cd, where Qabs_ab is the sum over the
      * pair's primitive pairs i of sqrt(max |(a_i b_i|a_i b_i)|).  B bounds the sum of the
@@ -115,6 +125,14 @@ int64_t molints_npacked(int64_t nbf);
 int molints_create(molints_ctx **ctx, int device, int64_t hbm_budget_bytes, uint32_t flags);
 int molints_destroy(molints_ctx *ctx);
 const char *molints_last_error(const molints_ctx *ctx);
+
+/* Per class pair method for MOLINTS_METHOD_AUTO plans created afterwards (the autotuner's
+ * choice).  methods[x * MOLINTS_NUM_PAIR_CLASSES + y] for bra class x >= ket class y is
+ * MOLINTS_METHOD_HGP, MOLINTS_METHOD_RYS or MOLINTS_METHOD_AUTO (default: HGP where it
+ * exists); entries with y > x are ignored.  methods == NULL resets the table.  n must be
+ * MOLINTS_NUM_PAIR_CLASSES^2.  No reference counterpart (the reference picks its driver by
+ * function name). */
+int molints_set_class_methods(molints_ctx *ctx, const int32_t *methods, int32_t n);
 
 /* Set the CUDA stream (a cudaStream_t passed as void*) the context launches on.
  * NULL selects the context's own (non-blocking) stream; to launch on the legacy default
@@ -185,6 +203,47 @@ int molints_boys_eval(molints_ctx *ctx, int32_t boys_mode, int32_t mmax, const d
  * returns; all calls share the array, so calls whose GPU work overlaps race on it. */
 int molints_eri_packed_noalloc(const molints_basis *basis, const molints_options *opts,
                                double *out_device, void *stream, char *err, size_t err_len);
+
+/* ------------------------------------------------------------------------------------------
+ * Serving: molecules submitted as they arrive, computed concurrently, results kept on the
+ * device until released.  No reference counterpart (the reference computes one basis per
+ * blocking call); each request's vector is what molints_eri_packed would write for it.
+ *
+ * molints_serve_start gives the context a server of nslots slot workers (host threads, each
+ * with its own engine context and stream on the context's device).  Requests queue in arrival
+ * order; a free slot admits the head request once the server's HBM ledger -- resident result
+ * vectors plus the pair tables of running plans -- has room for it under hbm_budget_bytes
+ * (0 = no bound), so new requests join the ones already running and their kernels overlap on
+ * the device.  A request larger than the whole budget fails with MOLINTS_ERR_BUDGET.
+ * submit, poll, result, release and request_info may be called from any host thread. */
+typedef struct molints_request molints_request;
+
+int molints_serve_start(molints_ctx *ctx, int32_t nslots, int64_t hbm_budget_bytes);
+/* Stop the server: queued requests fail, running ones finish; results stay valid until
+ * released.  molints_destroy stops the context's server. */
+int molints_serve_stop(molints_ctx *ctx);
+/* Queue one basis (copied; the caller's arrays may be reused at once). */
+int molints_submit(molints_ctx *ctx, const molints_basis *basis, const molints_options *opts,
+                   molints_request **req);
+/* Wait up to timeout_ms (0: do not wait, < 0: no limit) for the request: MOLINTS_OK when its
+ * result is ready, MOLINTS_ERR_TIMEOUT if not yet, or the request's own error status. */
+int molints_poll(molints_request *req, int32_t timeout_ms);
+/* The finished request's packed vector: a device pointer of *len doubles on the server's
+ * device, valid until molints_release. */
+int molints_result(molints_request *req, double **out_device, int64_t *len);
+/* Copy the finished request's vector (len == its length) into host memory. */
+int molints_result_copy(molints_request *req, double *out_host, int64_t len);
+/* Host steady-clock seconds of submission, admission and completion, and the slot that ran
+ * the request (MOLINTS_ERR_TIMEOUT while it is not finished). */
+int molints_request_info(molints_request *req, double *t_submit, double *t_admit, double *t_done,
+                         int32_t *slot);
+const char *molints_request_error(const molints_request *req);
+/* Give the request back: frees its result (or withdraws it from the queue; a running request
+ * is freed when it finishes).  The handle is invalid afterwards. */
+int molints_release(molints_request *req);
+/* Ledger bytes in use, queued, finished and failed request counts of the context's server. */
+int molints_serve_stats(molints_ctx *ctx, int64_t *ledger_bytes, int64_t *queued, int64_t *done,
+                        int64_t *failed);
 
 #ifdef __cplusplus
 }

@@ -42,11 +42,14 @@ def sources():
     finally:
         sys.path.pop(0)
     gen = gen_eri.generate()
-    return [CSRC / "molints.cu", CSRC / "noalloc.cu"] + sorted(gen)
+    return ([CSRC / "molints.cu", CSRC / "noalloc.cu", CSRC / "serve.cu",
+             CSRC / "generated" / "rys_tables.cu"] +
+            sorted(gen))
 
 
 def _deps(src: Path):
-    return [src, CSRC / "eri_common.cuh", CSRC / "eri_dispatch.h", INCLUDE / "molints.h"]
+    return [src, CSRC / "eri_common.cuh", CSRC / "rys_common.cuh", CSRC / "eri_dispatch.h",
+            INCLUDE / "molints.h"]
 
 
 def _compile(src: Path, force: bool):

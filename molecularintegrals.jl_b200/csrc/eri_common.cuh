@@ -53,6 +53,16 @@ struct BoysTab {
     double t_switch;       // asymptotic form at T >= t_switch
 };
 
+// Rys quadrature tables (generated/rys_tables.cu): for n = 1..7 roots, Chebyshev series of
+// the nodes u_i = t_i^2 and weights W_i on unit intervals of X < 100, and the Gauss-Hermite
+// limits x_i = h_i^2 / X, W_i = g_i / sqrt(X) above.
+struct RysTab {
+    const double *cheb;     // [n][interval j < 100][2n functions][16 coefficients]
+    const double *herm_x2;  // h_i^2 of the 2n-point Gauss-Hermite rule, n at n(n-1)/2
+    const double *herm_w;   // g_i, same layout
+};
+int rys_tables(RysTab *t);  // device addresses on the current device; 0 on success
+
 // The chunk queue of one class pair: chunk c = {bra pair, first ket pair, ket count,
 // molecule}; lane l of the warp that takes it computes (bra | first + l + 32 i).  Chunks never
 // cross a bra pair, a molecule or, when bra and ket class coincide, the triangle q <= p.

@@ -23,6 +23,20 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE / "generated"
+
+
+def _load_gen_rys():
+    import importlib.util
+    if "gen_rys" in sys.modules:
+        return sys.modules["gen_rys"]
+    spec = importlib.util.spec_from_file_location("gen_rys", HERE / "gen_rys.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["gen_rys"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+gen_rys = _load_gen_rys()
 LMAX = 2            # shell angular momentum supported by the generated kernels
 LTAB = 2 * LMAX     # AO tables must reach la + lb
 # Classes whose VRR has fewer entries than this get no FP32 variant: their primitive
@@ -454,7 +468,10 @@ int occupancy_eri_{tag}(int mixed) {{
 
 
 def emit_dispatch(pairs):
-    cls = pair_classes()
+    """eri_dispatch.h: launch tables over all pair classes up to f (gen_rys.LMAX).  HGP kernels
+    exist for the class pairs of shells up to d; Rys kernels for every class pair."""
+    cls = gen_rys.pair_classes()
+    hgp = set(pairs)
     lines = ["// Generated by gen_eri.py.  Do not edit.", "#pragma once",
              '#include "eri_common.cuh"', "namespace molints {"]
     for X, Y in pairs:
@@ -464,38 +481,52 @@ def emit_dispatch(pairs):
         if X == Y:
             lines.append(f"void launch_schwarz_{t}(const PairTab &P, const BoysTab &B, int p0, "
                          f"int np, double2 *pbound, double *qout, int full, cudaStream_t s);")
+    for X, Y in gen_rys.class_pairs():
+        t = tag_of(X, Y)
+        lines.append(f"void launch_rys_{t}(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);")
+        lines.append(f"int occupancy_rys_{t}();")
+        if X == Y:
+            lines.append(f"void launch_rys_bound_{t}(const PairTab &P, const RysTab &R, int p0, int np, "
+                         f"double2 *pbound, double *qout, int full, cudaStream_t s);")
     lines.append("typedef void (*EriLauncher)(const EriQueue &, int, int, cudaStream_t);")
     lines.append("typedef int (*EriOccupancy)(int);")
     lines.append("typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, "
                  "double2 *, double *, int, cudaStream_t);")
-    lines.append(f"constexpr int kLmax = {LMAX};")
+    lines.append("typedef void (*RysLauncher)(const EriQueue &, const RysTab &, int, cudaStream_t);")
+    lines.append("typedef int (*RysOccupancy)();")
+    lines.append("typedef void (*RysBoundLauncher)(const PairTab &, const RysTab &, int, int, "
+                 "double2 *, double *, int, cudaStream_t);")
+    lines.append(f"constexpr int kLmax = {gen_rys.LMAX};      // shells up to f (Rys)")
+    lines.append(f"constexpr int kLmaxHgp = {LMAX};   // HGP kernels: shells up to d")
     lines.append(f"constexpr int kNumPairClasses = {len(cls)};")
     lines.append("// pair class c = (kPairClassLa[c], kPairClassLb[c]), ordered by la+lb then la")
     lines.append("constexpr int kPairClassLa[] = {" + ", ".join(str(c[0]) for c in cls) + "};")
     lines.append("constexpr int kPairClassLb[] = {" + ", ".join(str(c[1]) for c in cls) + "};")
-    lines.append("// kEriLaunchers[x][y], x >= y (bra class x, ket class y)")
-    lines.append(f"static const EriLauncher kEriLaunchers[{len(cls)}][{len(cls)}] = {{")
-    for i, X in enumerate(cls):
-        row = []
-        for j, Y in enumerate(cls):
-            row.append(f"launch_eri_{tag_of(X, Y)}" if j <= i else "nullptr")
-        lines.append("    {" + ", ".join(row) + "},")
-    lines.append("};")
-    lines.append(f"static const EriOccupancy kEriOccupancy[{len(cls)}][{len(cls)}] = {{")
-    for i, X in enumerate(cls):
-        row = [f"occupancy_eri_{tag_of(X, Y)}" if j <= i else "nullptr" for j, Y in enumerate(cls)]
-        lines.append("    {" + ", ".join(row) + "},")
-    lines.append("};")
-    lines.append(f"static const char *const kEriNames[{len(cls)}][{len(cls)}] = {{")
-    for i, X in enumerate(cls):
-        row = [f'"eri_{tag_of(X, Y)}"' if j <= i else "nullptr" for j, Y in enumerate(cls)]
-        lines.append("    {" + ", ".join(row) + "},")
-    lines.append("};")
-    lines.append(f"static const char *const kSchwarzNames[{len(cls)}] = {{")
+    n = len(cls)
+
+    def table(ctype, name, fmt, cond=lambda X, Y: True):
+        lines.append(f"static const {ctype} {name}[{n}][{n}] = {{")
+        for i, X in enumerate(cls):
+            row = [fmt(X, Y) if (j <= i and cond(X, Y)) else "nullptr" for j, Y in enumerate(cls)]
+            lines.append("    {" + ", ".join(row) + "},")
+        lines.append("};")
+
+    lines.append("// [x][y], x >= y (bra class x, ket class y); nullptr where no HGP kernel exists")
+    table("EriLauncher", "kEriLaunchers", lambda X, Y: f"launch_eri_{tag_of(X, Y)}", lambda X, Y: (X, Y) in hgp)
+    table("EriOccupancy", "kEriOccupancy", lambda X, Y: f"occupancy_eri_{tag_of(X, Y)}", lambda X, Y: (X, Y) in hgp)
+    table("char *const", "kEriNames", lambda X, Y: f'"eri_{tag_of(X, Y)}"', lambda X, Y: (X, Y) in hgp)
+    table("RysLauncher", "kRysLaunchers", lambda X, Y: f"launch_rys_{tag_of(X, Y)}")
+    table("RysOccupancy", "kRysOccupancy", lambda X, Y: f"occupancy_rys_{tag_of(X, Y)}")
+    table("char *const", "kRysNames", lambda X, Y: f'"rys_{tag_of(X, Y)}"')
+    lines.append(f"static const char *const kSchwarzNames[{n}] = {{")
     lines.append("    " + ", ".join(f'"schwarz_{tag_of(X, X)[:2]}"' for X in cls))
     lines.append("};")
-    lines.append(f"static const SchwarzLauncher kSchwarzLaunchers[{len(cls)}] = {{")
-    lines.append("    " + ", ".join(f"launch_schwarz_{tag_of(X, X)}" for X in cls))
+    lines.append(f"static const SchwarzLauncher kSchwarzLaunchers[{n}] = {{")
+    lines.append("    " + ", ".join(f"launch_schwarz_{tag_of(X, X)}" if (X, X) in hgp else "nullptr"
+                                   for X in cls))
+    lines.append("};")
+    lines.append(f"static const RysBoundLauncher kRysBoundLaunchers[{n}] = {{")
+    lines.append("    " + ", ".join(f"launch_rys_bound_{tag_of(X, X)}" for X in cls))
     lines.append("};")
     lines.append("}  // namespace molints")
     return "\n".join(lines) + "\n"
@@ -511,6 +542,7 @@ def generate(out_dir: Path = OUT_DIR):
         if not p.exists() or p.read_text() != src:
             p.write_text(src)
         written.append(p)
+    written += gen_rys.generate(out_dir)
     d = HERE / "eri_dispatch.h"
     src = emit_dispatch(pairs)
     if not d.exists() or d.read_text() != src:

@@ -188,7 +188,7 @@ def main():
 
 namespace molints {{
 
-__device__ const double kRysCheb[{len(flat)}] = {{
+__device__ __align__(16) const double kRysCheb[{len(flat)}] = {{
 {arr(flat)}
 }};
 __device__ const double kRysHermX2[{len(hx)}] = {{

@@ -1,0 +1,92 @@
+// Generated by gen_rys.py -- Rys class (dp|ds).  Do not edit.
+// roots 3, block 16 x 6, outputs 18 x 6, group 32 threads,
+// 3 primitive quartets per batch, 3 accumulators per thread, 11648 B shared per block.
+#include "../rys_common.cuh"
+
+namespace molints {
+
+struct C_dpds {
+    static constexpr int LA = 2, LB = 1, LC = 2, LD = 0;
+    static constexpr int E = 3, F = 2, NR = 3;
+    static constexpr int NA = 16, NC = 6, NBLK = 96;
+    static constexpr int NB = 3, ND = 1;
+    static constexpr int NAB = 18, NCD = 6;
+    static constexpr int G = 32, NPB = 3, ACC = 3;
+    static constexpr int S = 12;
+    static constexpr int SMEM_GROUP = 364;
+};
+
+// block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
+__device__ const uint32_t kBlk_dpds[96] = {
+    8, 263, 65543, 518, 65798, 131078, 773, 1028, 66308, 1283, 66563, 131843,
+    196613, 196868, 262148, 197123, 262403, 327683, 1538, 1793, 67073, 2048, 67328, 132608,
+    197378, 197633, 262913, 197888, 263168, 328448, 393218, 393473, 458753, 393728, 459008, 524288,
+    11, 266, 65546, 521, 65801, 131081, 776, 1031, 66311, 1286, 66566, 131846,
+    196616, 196871, 262151, 197126, 262406, 327686, 1541, 1796, 67076, 2051, 67331, 132611,
+    393221, 393476, 458756, 393731, 459011, 524291, 197381, 197636, 262916, 197891, 263171, 328451,
+    2306, 2561, 67841, 2816, 68096, 133376, 198146, 198401, 263681, 198656, 263936, 329216,
+    393986, 394241, 459521, 394496, 459776, 525056, 589826, 590081, 655361, 590336, 655616, 720896,
+};
+// HRR terms: block index | monomial << 8 | binomial << 16, per output pair
+__device__ const uint16_t kBraOff_dpds[19] = {
+    0, 2, 4, 6, 8, 10, 12, 14, 16, 18, 20, 22,
+    24, 26, 28, 30, 32, 34, 36,
+};
+__device__ const uint32_t kBraTerm_dpds[36] = {
+    65792, 65542, 66048, 65543, 66304, 65544, 65793, 65543, 66049, 65545, 66305, 65547,
+    65794, 65544, 66050, 65547, 66306, 65546, 65795, 65545, 66051, 65548, 66307, 65549,
+    65796, 65547, 66052, 65549, 66308, 65550, 65797, 65546, 66053, 65550, 66309, 65551,
+};
+__device__ const uint16_t kKetOff_dpds[7] = {
+    0, 1, 2, 3, 4, 5, 6,
+};
+__device__ const uint32_t kKetTerm_dpds[6] = {
+    65536, 65537, 65538, 65539, 65540, 65541,
+};
+__device__ const double kNormAB_dpds[18] = {
+    0.5773502691896258, 0.5773502691896258, 0.5773502691896258, 1.0,
+    1.0, 1.0, 1.0, 1.0,
+    1.0, 0.5773502691896258, 0.5773502691896258, 0.5773502691896258,
+    1.0, 1.0, 1.0, 0.5773502691896258,
+    0.5773502691896258, 0.5773502691896258,
+};
+__device__ const double kNormCD_dpds[6] = {
+    0.5773502691896258, 1.0, 1.0, 0.5773502691896258,
+    1.0, 0.5773502691896258,
+};
+
+__device__ __forceinline__ RysClassTabs tabs_dpds() {
+    return RysClassTabs{kBlk_dpds, kBraOff_dpds, kBraTerm_dpds, kKetOff_dpds, kKetTerm_dpds,
+                        kNormAB_dpds, kNormCD_dpds};
+}
+
+__global__ void __launch_bounds__(128) rys_queue_dpds(const EriQueue Q, const RysTab R) {
+    rys_queue_body<C_dpds>(Q, R, tabs_dpds());
+}
+
+static void rys_prepare_dpds() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(rys_queue_dpds, cudaFuncAttributeMaxDynamicSharedMemorySize, 11648);
+
+        done[dev] = true;
+    }
+}
+
+void launch_rys_dpds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    rys_prepare_dpds();
+    rys_queue_dpds<<<grid, 128, 11648, s>>>(Q, R);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_rys_dpds() {
+    rys_prepare_dpds();
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpds, 128, 11648);
+    return n;
+}
+
+}  // namespace molints

@@ -1,0 +1,98 @@
+// Generated by gen_rys.py -- Rys class (dp|pp).  Do not edit.
+// roots 3, block 16 x 9, outputs 18 x 9, group 64 threads,
+// 7 primitive quartets per batch, 3 accumulators per thread, 12736 B shared per block.
+#include "../rys_common.cuh"
+
+namespace molints {
+
+struct C_dppp {
+    static constexpr int LA = 2, LB = 1, LC = 1, LD = 1;
+    static constexpr int E = 3, F = 2, NR = 3;
+    static constexpr int NA = 16, NC = 9, NBLK = 144;
+    static constexpr int NB = 3, ND = 3;
+    static constexpr int NAB = 18, NCD = 9;
+    static constexpr int G = 64, NPB = 7, ACC = 3;
+    static constexpr int S = 12;
+    static constexpr int SMEM_GROUP = 796;
+};
+
+// block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
+__device__ const uint32_t kBlk_dppp[144] = {
+    7, 262, 65542, 8, 263, 65543, 518, 65798, 131078, 772, 1027, 66307,
+    773, 1028, 66308, 1283, 66563, 131843, 196612, 196867, 262147, 196613, 196868, 262148,
+    197123, 262403, 327683, 1537, 1792, 67072, 1538, 1793, 67073, 2048, 67328, 132608,
+    197377, 197632, 262912, 197378, 197633, 262913, 197888, 263168, 328448, 393217, 393472, 458752,
+    393218, 393473, 458753, 393728, 459008, 524288, 10, 265, 65545, 11, 266, 65546,
+    521, 65801, 131081, 775, 1030, 66310, 776, 1031, 66311, 1286, 66566, 131846,
+    196615, 196870, 262150, 196616, 196871, 262151, 197126, 262406, 327686, 1540, 1795, 67075,
+    1541, 1796, 67076, 2051, 67331, 132611, 393220, 393475, 458755, 393221, 393476, 458756,
+    393731, 459011, 524291, 197380, 197635, 262915, 197381, 197636, 262916, 197891, 263171, 328451,
+    2305, 2560, 67840, 2306, 2561, 67841, 2816, 68096, 133376, 198145, 198400, 263680,
+    198146, 198401, 263681, 198656, 263936, 329216, 393985, 394240, 459520, 393986, 394241, 459521,
+    394496, 459776, 525056, 589825, 590080, 655360, 589826, 590081, 655361, 590336, 655616, 720896,
+};
+// HRR terms: block index | monomial << 8 | binomial << 16, per output pair
+__device__ const uint16_t kBraOff_dppp[19] = {
+    0, 2, 4, 6, 8, 10, 12, 14, 16, 18, 20, 22,
+    24, 26, 28, 30, 32, 34, 36,
+};
+__device__ const uint32_t kBraTerm_dppp[36] = {
+    65792, 65542, 66048, 65543, 66304, 65544, 65793, 65543, 66049, 65545, 66305, 65547,
+    65794, 65544, 66050, 65547, 66306, 65546, 65795, 65545, 66051, 65548, 66307, 65549,
+    65796, 65547, 66052, 65549, 66308, 65550, 65797, 65546, 66053, 65550, 66309, 65551,
+};
+__device__ const uint16_t kKetOff_dppp[10] = {
+    0, 2, 4, 6, 8, 10, 12, 14, 16, 18,
+};
+__device__ const uint32_t kKetTerm_dppp[18] = {
+    65792, 65539, 66048, 65540, 66304, 65541, 65793, 65540, 66049, 65542, 66305, 65543,
+    65794, 65541, 66050, 65543, 66306, 65544,
+};
+__device__ const double kNormAB_dppp[18] = {
+    0.5773502691896258, 0.5773502691896258, 0.5773502691896258, 1.0,
+    1.0, 1.0, 1.0, 1.0,
+    1.0, 0.5773502691896258, 0.5773502691896258, 0.5773502691896258,
+    1.0, 1.0, 1.0, 0.5773502691896258,
+    0.5773502691896258, 0.5773502691896258,
+};
+__device__ const double kNormCD_dppp[9] = {
+    1.0, 1.0, 1.0, 1.0,
+    1.0, 1.0, 1.0, 1.0,
+    1.0,
+};
+
+__device__ __forceinline__ RysClassTabs tabs_dppp() {
+    return RysClassTabs{kBlk_dppp, kBraOff_dppp, kBraTerm_dppp, kKetOff_dppp, kKetTerm_dppp,
+                        kNormAB_dppp, kNormCD_dppp};
+}
+
+__global__ void __launch_bounds__(128) rys_queue_dppp(const EriQueue Q, const RysTab R) {
+    rys_queue_body<C_dppp>(Q, R, tabs_dppp());
+}
+
+static void rys_prepare_dppp() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(rys_queue_dppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 12736);
+
+        done[dev] = true;
+    }
+}
+
+void launch_rys_dppp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    rys_prepare_dppp();
+    rys_queue_dppp<<<grid, 128, 12736, s>>>(Q, R);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_rys_dppp() {
+    rys_prepare_dppp();
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dppp, 128, 12736);
+    return n;
+}
+
+}  // namespace molints

@@ -1,0 +1,85 @@
+// Generated by gen_rys.py -- Rys class (ds|pp).  Do not edit.
+// roots 3, block 6 x 9, outputs 6 x 9, group 32 threads,
+// 3 primitive quartets per batch, 2 accumulators per thread, 9056 B shared per block.
+#include "../rys_common.cuh"
+
+namespace molints {
+
+struct C_dspp {
+    static constexpr int LA = 2, LB = 0, LC = 1, LD = 1;
+    static constexpr int E = 2, F = 2, NR = 3;
+    static constexpr int NA = 6, NC = 9, NBLK = 54;
+    static constexpr int NB = 1, ND = 3;
+    static constexpr int NAB = 6, NCD = 9;
+    static constexpr int G = 32, NPB = 3, ACC = 2;
+    static constexpr int S = 9;
+    static constexpr int SMEM_GROUP = 283;
+};
+
+// block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
+__device__ const uint32_t kBlk_dspp[54] = {
+    7, 262, 65542, 8, 263, 65543, 518, 65798, 131078, 772, 1027, 66307,
+    773, 1028, 66308, 1283, 66563, 131843, 196612, 196867, 262147, 196613, 196868, 262148,
+    197123, 262403, 327683, 1537, 1792, 67072, 1538, 1793, 67073, 2048, 67328, 132608,
+    197377, 197632, 262912, 197378, 197633, 262913, 197888, 263168, 328448, 393217, 393472, 458752,
+    393218, 393473, 458753, 393728, 459008, 524288,
+};
+// HRR terms: block index | monomial << 8 | binomial << 16, per output pair
+__device__ const uint16_t kBraOff_dspp[7] = {
+    0, 1, 2, 3, 4, 5, 6,
+};
+__device__ const uint32_t kBraTerm_dspp[6] = {
+    65536, 65537, 65538, 65539, 65540, 65541,
+};
+__device__ const uint16_t kKetOff_dspp[10] = {
+    0, 2, 4, 6, 8, 10, 12, 14, 16, 18,
+};
+__device__ const uint32_t kKetTerm_dspp[18] = {
+    65792, 65539, 66048, 65540, 66304, 65541, 65793, 65540, 66049, 65542, 66305, 65543,
+    65794, 65541, 66050, 65543, 66306, 65544,
+};
+__device__ const double kNormAB_dspp[6] = {
+    0.5773502691896258, 1.0, 1.0, 0.5773502691896258,
+    1.0, 0.5773502691896258,
+};
+__device__ const double kNormCD_dspp[9] = {
+    1.0, 1.0, 1.0, 1.0,
+    1.0, 1.0, 1.0, 1.0,
+    1.0,
+};
+
+__device__ __forceinline__ RysClassTabs tabs_dspp() {
+    return RysClassTabs{kBlk_dspp, kBraOff_dspp, kBraTerm_dspp, kKetOff_dspp, kKetTerm_dspp,
+                        kNormAB_dspp, kNormCD_dspp};
+}
+
+__global__ void __launch_bounds__(128) rys_queue_dspp(const EriQueue Q, const RysTab R) {
+    rys_queue_body<C_dspp>(Q, R, tabs_dspp());
+}
+
+static void rys_prepare_dspp() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(rys_queue_dspp, cudaFuncAttributeMaxDynamicSharedMemorySize, 9056);
+
+        done[dev] = true;
+    }
+}
+
+void launch_rys_dspp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    rys_prepare_dspp();
+    rys_queue_dspp<<<grid, 128, 9056, s>>>(Q, R);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_rys_dspp() {
+    rys_prepare_dspp();
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp, 128, 9056);
+    return n;
+}
+
+}  // namespace molints

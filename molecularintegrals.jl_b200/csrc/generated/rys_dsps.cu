@@ -1,0 +1,79 @@
+// Generated by gen_rys.py -- Rys class (ds|ps).  Do not edit.
+// roots 2, block 6 x 3, outputs 6 x 3, group 32 threads,
+// 5 primitive quartets per batch, 1 accumulators per thread, 7040 B shared per block.
+#include "../rys_common.cuh"
+
+namespace molints {
+
+struct C_dsps {
+    static constexpr int LA = 2, LB = 0, LC = 1, LD = 0;
+    static constexpr int E = 2, F = 1, NR = 2;
+    static constexpr int NA = 6, NC = 3, NBLK = 18;
+    static constexpr int NB = 1, ND = 1;
+    static constexpr int NAB = 6, NCD = 3;
+    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int S = 6;
+    static constexpr int SMEM_GROUP = 220;
+};
+
+// block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
+__device__ const uint32_t kBlk_dsps[18] = {
+    5, 260, 65540, 515, 770, 66050, 131075, 131330, 196610, 1025, 1280, 66560,
+    131585, 131840, 197120, 262145, 262400, 327680,
+};
+// HRR terms: block index | monomial << 8 | binomial << 16, per output pair
+__device__ const uint16_t kBraOff_dsps[7] = {
+    0, 1, 2, 3, 4, 5, 6,
+};
+__device__ const uint32_t kBraTerm_dsps[6] = {
+    65536, 65537, 65538, 65539, 65540, 65541,
+};
+__device__ const uint16_t kKetOff_dsps[4] = {
+    0, 1, 2, 3,
+};
+__device__ const uint32_t kKetTerm_dsps[3] = {
+    65536, 65537, 65538,
+};
+__device__ const double kNormAB_dsps[6] = {
+    0.5773502691896258, 1.0, 1.0, 0.5773502691896258,
+    1.0, 0.5773502691896258,
+};
+__device__ const double kNormCD_dsps[3] = {
+    1.0, 1.0, 1.0,
+};
+
+__device__ __forceinline__ RysClassTabs tabs_dsps() {
+    return RysClassTabs{kBlk_dsps, kBraOff_dsps, kBraTerm_dsps, kKetOff_dsps, kKetTerm_dsps,
+                        kNormAB_dsps, kNormCD_dsps};
+}
+
+__global__ void __launch_bounds__(128) rys_queue_dsps(const EriQueue Q, const RysTab R) {
+    rys_queue_body<C_dsps>(Q, R, tabs_dsps());
+}
+
+static void rys_prepare_dsps() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(rys_queue_dsps, cudaFuncAttributeMaxDynamicSharedMemorySize, 7040);
+
+        done[dev] = true;
+    }
+}
+
+void launch_rys_dsps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    rys_prepare_dsps();
+    rys_queue_dsps<<<grid, 128, 7040, s>>>(Q, R);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_rys_dsps() {
+    rys_prepare_dsps();
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsps, 128, 7040);
+    return n;
+}
+
+}  // namespace molints

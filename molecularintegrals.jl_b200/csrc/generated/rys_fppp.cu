@@ -1,0 +1,111 @@
+// Generated by gen_rys.py -- Rys class (fp|pp).  Do not edit.
+// roots 4, block 25 x 9, outputs 30 x 9, group 64 threads,
+// 5 primitive quartets per batch, 4 accumulators per thread, 15040 B shared per block.
+#include "../rys_common.cuh"
+
+namespace molints {
+
+struct C_fppp {
+    static constexpr int LA = 3, LB = 1, LC = 1, LD = 1;
+    static constexpr int E = 4, F = 2, NR = 4;
+    static constexpr int NA = 25, NC = 9, NBLK = 225;
+    static constexpr int NB = 3, ND = 3;
+    static constexpr int NAB = 30, NCD = 9;
+    static constexpr int G = 64, NPB = 5, ACC = 4;
+    static constexpr int S = 15;
+    static constexpr int SMEM_GROUP = 940;
+};
+
+// block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
+__device__ const uint32_t kBlk_fppp[225] = {
+    10, 265, 65545, 11, 266, 65546, 521, 65801, 131081, 775, 1030, 66310,
+    776, 1031, 66311, 1286, 66566, 131846, 196615, 196870, 262150, 196616, 196871, 262151,
+    197126, 262406, 327686, 1540, 1795, 67075, 1541, 1796, 67076, 2051, 67331, 132611,
+    393220, 393475, 458755, 393221, 393476, 458756, 393731, 459011, 524291, 197380, 197635, 262915,
+    197381, 197636, 262916, 197891, 263171, 328451, 2305, 2560, 67840, 2306, 2561, 67841,
+    2816, 68096, 133376, 198145, 198400, 263680, 198146, 198401, 263681, 198656, 263936, 329216,
+    393985, 394240, 459520, 393986, 394241, 459521, 394496, 459776, 525056, 589825, 590080, 655360,
+    589826, 590081, 655361, 590336, 655616, 720896, 13, 268, 65548, 14, 269, 65549,
+    524, 65804, 131084, 778, 1033, 66313, 779, 1034, 66314, 1289, 66569, 131849,
+    196618, 196873, 262153, 196619, 196874, 262154, 197129, 262409, 327689, 1543, 1798, 67078,
+    1544, 1799, 67079, 2054, 67334, 132614, 197383, 197638, 262918, 197384, 197639, 262919,
+    197894, 263174, 328454, 393223, 393478, 458758, 393224, 393479, 458759, 393734, 459014, 524294,
+    2308, 2563, 67843, 2309, 2564, 67844, 2819, 68099, 133379, 198148, 198403, 263683,
+    198149, 198404, 263684, 198659, 263939, 329219, 393988, 394243, 459523, 393989, 394244, 459524,
+    394499, 459779, 525059, 589828, 590083, 655363, 589829, 590084, 655364, 590339, 655619, 720899,
+    3073, 3328, 68608, 3074, 3329, 68609, 3584, 68864, 134144, 198913, 199168, 264448,
+    198914, 199169, 264449, 199424, 264704, 329984, 394753, 395008, 460288, 394754, 395009, 460289,
+    395264, 460544, 525824, 590593, 590848, 656128, 590594, 590849, 656129, 591104, 656384, 721664,
+    786433, 786688, 851968, 786434, 786689, 851969, 786944, 852224, 917504,
+};
+// HRR terms: block index | monomial << 8 | binomial << 16, per output pair
+__device__ const uint16_t kBraOff_fppp[31] = {
+    0, 2, 4, 6, 8, 10, 12, 14, 16, 18, 20, 22,
+    24, 26, 28, 30, 32, 34, 36, 38, 40, 42, 44, 46,
+    48, 50, 52, 54, 56, 58, 60,
+};
+__device__ const uint32_t kBraTerm_fppp[60] = {
+    65792, 65546, 66048, 65547, 66304, 65548, 65793, 65547, 66049, 65549, 66305, 65550,
+    65794, 65548, 66050, 65550, 66306, 65551, 65795, 65549, 66051, 65552, 66307, 65553,
+    65796, 65551, 66052, 65554, 66308, 65555, 65797, 65550, 66053, 65553, 66309, 65554,
+    65798, 65552, 66054, 65556, 66310, 65557, 65799, 65553, 66055, 65557, 66311, 65558,
+    65800, 65554, 66056, 65558, 66312, 65559, 65801, 65555, 66057, 65559, 66313, 65560,
+};
+__device__ const uint16_t kKetOff_fppp[10] = {
+    0, 2, 4, 6, 8, 10, 12, 14, 16, 18,
+};
+__device__ const uint32_t kKetTerm_fppp[18] = {
+    65792, 65539, 66048, 65540, 66304, 65541, 65793, 65540, 66049, 65542, 66305, 65543,
+    65794, 65541, 66050, 65543, 66306, 65544,
+};
+__device__ const double kNormAB_fppp[30] = {
+    0.2581988897471611, 0.2581988897471611, 0.2581988897471611, 0.5773502691896258,
+    0.5773502691896258, 0.5773502691896258, 0.5773502691896258, 0.5773502691896258,
+    0.5773502691896258, 0.5773502691896258, 0.5773502691896258, 0.5773502691896258,
+    0.5773502691896258, 0.5773502691896258, 0.5773502691896258, 1.0,
+    1.0, 1.0, 0.2581988897471611, 0.2581988897471611,
+    0.2581988897471611, 0.5773502691896258, 0.5773502691896258, 0.5773502691896258,
+    0.5773502691896258, 0.5773502691896258, 0.5773502691896258, 0.2581988897471611,
+    0.2581988897471611, 0.2581988897471611,
+};
+__device__ const double kNormCD_fppp[9] = {
+    1.0, 1.0, 1.0, 1.0,
+    1.0, 1.0, 1.0, 1.0,
+    1.0,
+};
+
+__device__ __forceinline__ RysClassTabs tabs_fppp() {
+    return RysClassTabs{kBlk_fppp, kBraOff_fppp, kBraTerm_fppp, kKetOff_fppp, kKetTerm_fppp,
+                        kNormAB_fppp, kNormCD_fppp};
+}
+
+__global__ void __launch_bounds__(128) rys_queue_fppp(const EriQueue Q, const RysTab R) {
+    rys_queue_body<C_fppp>(Q, R, tabs_fppp());
+}
+
+static void rys_prepare_fppp() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(rys_queue_fppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 15040);
+
+        done[dev] = true;
+    }
+}
+
+void launch_rys_fppp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    rys_prepare_fppp();
+    rys_queue_fppp<<<grid, 128, 15040, s>>>(Q, R);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_rys_fppp() {
+    rys_prepare_fppp();
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fppp, 128, 15040);
+    return n;
+}
+
+}  // namespace molints

@@ -1,0 +1,99 @@
+// Generated by gen_rys.py -- Rys class (fs|dp).  Do not edit.
+// roots 4, block 10 x 16, outputs 10 x 18, group 64 threads,
+// 5 primitive quartets per batch, 3 accumulators per thread, 16000 B shared per block.
+#include "../rys_common.cuh"
+
+namespace molints {
+
+struct C_fsdp {
+    static constexpr int LA = 3, LB = 0, LC = 2, LD = 1;
+    static constexpr int E = 3, F = 3, NR = 4;
+    static constexpr int NA = 10, NC = 16, NBLK = 160;
+    static constexpr int NB = 1, ND = 3;
+    static constexpr int NAB = 10, NCD = 18;
+    static constexpr int G = 64, NPB = 5, ACC = 3;
+    static constexpr int S = 16;
+    static constexpr int SMEM_GROUP = 1000;
+};
+
+// block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
+__device__ const uint32_t kBlk_fsdp[160] = {
+    14, 269, 65549, 524, 65804, 131084, 15, 270, 65550, 525, 131085, 65805,
+    780, 66060, 131340, 196620, 1034, 1289, 66569, 1544, 66824, 132104, 1035, 1290,
+    66570, 1545, 132105, 66825, 1800, 67080, 132360, 197640, 262154, 262409, 327689, 262664,
+    327944, 393224, 262155, 262410, 327690, 262665, 393225, 327945, 262920, 328200, 393480, 458760,
+    2054, 2309, 67589, 2564, 67844, 133124, 2055, 2310, 67590, 2565, 133125, 67845,
+    2820, 68100, 133380, 198660, 524294, 524549, 589829, 524804, 590084, 655364, 524295, 524550,
+    589830, 524805, 655365, 590085, 525060, 590340, 655620, 720900, 263174, 263429, 328709, 263684,
+    328964, 394244, 263175, 263430, 328710, 263685, 394245, 328965, 263940, 329220, 394500, 459780,
+    3074, 3329, 68609, 3584, 68864, 134144, 3075, 3330, 68610, 3585, 134145, 68865,
+    3840, 69120, 134400, 199680, 264194, 264449, 329729, 264704, 329984, 395264, 264195, 264450,
+    329730, 264705, 395265, 329985, 264960, 330240, 395520, 460800, 525314, 525569, 590849, 525824,
+    591104, 656384, 525315, 525570, 590850, 525825, 656385, 591105, 526080, 591360, 656640, 721920,
+    786434, 786689, 851969, 786944, 852224, 917504, 786435, 786690, 851970, 786945, 917505, 852225,
+    787200, 852480, 917760, 983040,
+};
+// HRR terms: block index | monomial << 8 | binomial << 16, per output pair
+__device__ const uint16_t kBraOff_fsdp[11] = {
+    0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10,
+};
+__device__ const uint32_t kBraTerm_fsdp[10] = {
+    65536, 65537, 65538, 65539, 65540, 65541, 65542, 65543, 65544, 65545,
+};
+__device__ const uint16_t kKetOff_fsdp[19] = {
+    0, 2, 4, 6, 8, 10, 12, 14, 16, 18, 20, 22,
+    24, 26, 28, 30, 32, 34, 36,
+};
+__device__ const uint32_t kKetTerm_fsdp[36] = {
+    65792, 65542, 66048, 65543, 66304, 65544, 65793, 65543, 66049, 65545, 66305, 65547,
+    65794, 65544, 66050, 65547, 66306, 65546, 65795, 65545, 66051, 65548, 66307, 65549,
+    65796, 65547, 66052, 65549, 66308, 65550, 65797, 65546, 66053, 65550, 66309, 65551,
+};
+__device__ const double kNormAB_fsdp[10] = {
+    0.2581988897471611, 0.5773502691896258, 0.5773502691896258, 0.5773502691896258,
+    0.5773502691896258, 1.0, 0.2581988897471611, 0.5773502691896258,
+    0.5773502691896258, 0.2581988897471611,
+};
+__device__ const double kNormCD_fsdp[18] = {
+    0.5773502691896258, 0.5773502691896258, 0.5773502691896258, 1.0,
+    1.0, 1.0, 1.0, 1.0,
+    1.0, 0.5773502691896258, 0.5773502691896258, 0.5773502691896258,
+    1.0, 1.0, 1.0, 0.5773502691896258,
+    0.5773502691896258, 0.5773502691896258,
+};
+
+__device__ __forceinline__ RysClassTabs tabs_fsdp() {
+    return RysClassTabs{kBlk_fsdp, kBraOff_fsdp, kBraTerm_fsdp, kKetOff_fsdp, kKetTerm_fsdp,
+                        kNormAB_fsdp, kNormCD_fsdp};
+}
+
+__global__ void __launch_bounds__(128) rys_queue_fsdp(const EriQueue Q, const RysTab R) {
+    rys_queue_body<C_fsdp>(Q, R, tabs_fsdp());
+}
+
+static void rys_prepare_fsdp() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(rys_queue_fsdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 16000);
+
+        done[dev] = true;
+    }
+}
+
+void launch_rys_fsdp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    rys_prepare_fsdp();
+    rys_queue_fsdp<<<grid, 128, 16000, s>>>(Q, R);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_rys_fsdp() {
+    rys_prepare_fsdp();
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsdp, 128, 16000);
+    return n;
+}
+
+}  // namespace molints

@@ -45,7 +45,10 @@ struct molints_ctx {
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork = nullptr, join[kSide] = {};
     int num_sms = 0;
-    int occupancy[kNumPairClasses][kNumPairClasses][2] = {};  // blocks/SM, 0 = not queried
+    // blocks/SM of the queue kernels, 0 = not queried: [x][y][HGP FP64, HGP MIXED, Rys]
+    int occupancy[kNumPairClasses][kNumPairClasses][3] = {};
+    RysTab rys{};  // device addresses of the Rys root/weight tables on this device
+    int32_t class_method[kNumPairClasses][kNumPairClasses] = {};  // AUTO choices (0 = default)
     std::string err;
 };
 
@@ -64,6 +67,7 @@ struct molints_plan {
     int q_off[kNumPairClasses][kNumPairClasses] = {};
     int q_len[kNumPairClasses][kNumPairClasses] = {};
     double class_cost[kNumPairClasses][kNumPairClasses] = {};  // kept primitive quartets
+    int method[kNumPairClasses][kNumPairClasses] = {};  // MOLINTS_METHOD_HGP or _RYS
     // host copies (final, screened order)
     std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
     std::vector<int> pair_mol;         // canonical pair -> molecule
@@ -245,6 +249,10 @@ void fill_boys_scaled(double *sc, int nM) {
 
 }  // namespace molints
 
+namespace molints {
+int ctx_device_of(const molints_ctx *ctx) { return ctx->device; }
+}  // namespace molints
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -295,6 +303,10 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
         return MOLINTS_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
+    if (rys_tables(&ctx->rys) != 0) {
+        molints_destroy(ctx);
+        return MOLINTS_ERR_CUDA;
+    }
     if (cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         ctx->num_sms = 1;
     cudaMemPoolProps props = {};
@@ -336,6 +348,7 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
 
 int molints_destroy(molints_ctx *ctx) {
     if (!ctx) return MOLINTS_OK;
+    molints_serve_stop(ctx);
     cudaSetDevice(ctx->device);
     if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
@@ -361,6 +374,25 @@ int molints_destroy(molints_ctx *ctx) {
 }
 
 const char *molints_last_error(const molints_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int molints_set_class_methods(molints_ctx *ctx, const int32_t *methods, int32_t n) {
+    if (!ctx) return MOLINTS_ERR_INVALID;
+    if (!methods) {
+        std::memset(ctx->class_method, 0, sizeof(ctx->class_method));
+        return MOLINTS_OK;
+    }
+    if (n != kNumPairClasses * kNumPairClasses)
+        return fail(ctx, MOLINTS_ERR_INVALID, "set_class_methods: n must be MOLINTS_NUM_PAIR_CLASSES^2");
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            const int32_t m = methods[x * kNumPairClasses + y];
+            if (m != MOLINTS_METHOD_AUTO && m != MOLINTS_METHOD_HGP && m != MOLINTS_METHOD_RYS)
+                return fail(ctx, MOLINTS_ERR_INVALID, "set_class_methods: unknown method");
+        }
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) ctx->class_method[x][y] = methods[x * kNumPairClasses + y];
+    return MOLINTS_OK;
+}
 
 int molints_set_stream(molints_ctx *ctx, void *stream) {
     if (!ctx) return MOLINTS_ERR_INVALID;
@@ -463,8 +495,9 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown precision");
     if (opts.boys != MOLINTS_BOYS_REFERENCE && opts.boys != MOLINTS_BOYS_EXACT)
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown Boys mode");
-    if (opts.method != MOLINTS_METHOD_AUTO && opts.method != MOLINTS_METHOD_HGP)
-        return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create: method not available");
+    if (opts.method != MOLINTS_METHOD_AUTO && opts.method != MOLINTS_METHOD_HGP &&
+        opts.method != MOLINTS_METHOD_RYS)
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown method");
     if (!(opts.fp32_cutoff >= 0.0) || !(opts.screen_cutoff >= 0.0) || !(opts.prim_cutoff >= 0.0))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: cutoffs must be >= 0");
 
@@ -490,6 +523,15 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
     p->npacked = mol_out[nmol];
     p->mol_out_h.assign(mol_out.begin(), mol_out.end() - (nmol > 0 ? 1 : 0));
     p->mol_nshell.resize(nmol);
+    // method per class pair: Rys where no HGP kernel exists (an f shell), else the request
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            int m = opts.method;
+            if (m == MOLINTS_METHOD_AUTO) m = ctx->class_method[x][y];
+            if (m == MOLINTS_METHOD_AUTO) m = MOLINTS_METHOD_HGP;
+            if (!kEriLaunchers[x][y]) m = MOLINTS_METHOD_RYS;
+            p->method[x][y] = m;
+        }
 
     // Normalised coefficients: raw coef x (2a/pi)^(3/4) (4a)^(L/2) x CGBF norm; the component
     // factor 1/sqrt((2I-1)!!(2J-1)!!(2K-1)!!) is applied by the generated kernels
@@ -521,8 +563,25 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
         }
     }
 
-    // ---- canonical shell pairs (L_A >= L_B) of every molecule, ordered by class, molecule,
-    // then descending primitive-pair count
+    // ---- canonical shell pairs of every molecule, ordered by class, molecule, then
+    // descending primitive-pair count.  Orientation (A first): the larger L; for equal L, and
+    // for an f-d pair, the tighter shell (larger sqrt(min * max exponent)), so that the HRR
+    // moves angular momentum away from the tight shell: with a diffuse A and a tight B the
+    // pair centre P sits near B and the HRR cancels large terms (up to 1e-6 Eh lost for
+    // (ff|ff) with random contractions, measured against the long-double oracle).
+    std::vector<double> tight(std::max(ns, 1));
+    for (int g = 0; g < ns; ++g) {
+        double lo = expn[poff[g]], hi = lo;
+        for (int i = 1; i < K[g]; ++i) {
+            lo = std::min(lo, expn[poff[g] + i]);
+            hi = std::max(hi, expn[poff[g] + i]);
+        }
+        tight[g] = std::sqrt(lo * hi);
+    }
+    auto a_first = [&](int x, int y) {  // x should be A of the pair (x, y)
+        if (L[x] == L[y] || (L[x] >= 2 && L[y] >= 2 && L[x] + L[y] == 5)) return tight[x] >= tight[y];
+        return L[x] > L[y];
+    };
     struct PairRec { int cls, mol, npp, a, b, ref; };
     std::vector<PairRec> pr;
     for (int m = 0; m < nmol; ++m) {
@@ -530,7 +589,7 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
         for (int i = 0; i < n; ++i)
             for (int j = 0; j <= i; ++j) {
                 int a = shell_off[m] + i, bb = shell_off[m] + j;
-                if (L[a] < L[bb]) std::swap(a, bb);
+                if (!a_first(a, bb)) std::swap(a, bb);
                 pr.push_back({pair_class_of(L[a], L[bb]), m, K[a] * K[bb], a, bb, i * (i + 1) / 2 + j});
             }
     }
@@ -612,9 +671,11 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
         build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, p->pair_ab, p->info, p->pp_src,
                                                                p->sh_xyz, p->sh_poff, p->expn,
                                                                p->ncoef, c0, p->pp, p->geo);
-        for (int c = 0; c < kNumPairClasses; ++c)
-            kSchwarzLaunchers[c](P, Bt, cls_start[c], cls_start[c + 1] - cls_start[c], pbound, nullptr,
-                                 0, s);
+        for (int c = 0; c < kNumPairClasses; ++c) {
+            const int n = cls_start[c + 1] - cls_start[c];
+            if (kSchwarzLaunchers[c]) kSchwarzLaunchers[c](P, Bt, cls_start[c], n, pbound, nullptr, 0, s);
+            else kRysBoundLaunchers[c](P, ctx->rys, cls_start[c], n, pbound, nullptr, 0, s);
+        }
     }
     if ((e = cudaGetLastError()) ||
         (nall > 0 && (e = cudaMemcpyAsync(pb_h.data(), pbound, nall * sizeof(double2),
@@ -826,8 +887,9 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
     for (size_t k = 0; k < jobs.size(); ++k) {
         const int x = jobs[k].x, y = jobs[k].y;
         cudaStream_t st = nside ? ctx->side[k % nside] : s;
-        int &occ = ctx->occupancy[x][y][mixed];
-        if (occ == 0) occ = std::max(1, kEriOccupancy[x][y](mixed));
+        const bool rys = p->method[x][y] == MOLINTS_METHOD_RYS;
+        int &occ = ctx->occupancy[x][y][rys ? 2 : mixed];
+        if (occ == 0) occ = std::max(1, rys ? kRysOccupancy[x][y]() : kEriOccupancy[x][y](mixed));
         EriQueue Q{};
         Q.pairs = P;
         Q.boys = B;
@@ -839,9 +901,11 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         Q.screen_cut = p->opts.screen_cutoff;
         Q.fp32_cut = p->opts.fp32_cutoff;
         const int grid = (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);
-        if (int rc = mark(launches, kEriNames[x][y], 0, st)) return rc;
-        kEriLaunchers[x][y](Q, mixed, grid, st);
-        if (int rc = mark(launches, kEriNames[x][y], 1, st)) return rc;
+        const char *name = rys ? kRysNames[x][y] : kEriNames[x][y];
+        if (int rc = mark(launches, name, 0, st)) return rc;
+        if (rys) kRysLaunchers[x][y](Q, ctx->rys, grid, st);
+        else kEriLaunchers[x][y](Q, mixed, grid, st);
+        if (int rc = mark(launches, name, 1, st)) return rc;
         ++launches;
     }
     for (int i = 0; i < nside; ++i) {
@@ -921,7 +985,9 @@ int molints_plan_schwarz(molints_plan *p, double *out) {
     BoysTab B = boys_of(ctx, p->opts.boys);
     for (int c = 0; c < kNumPairClasses; ++c) {
         const int n = p->class_start[c + 1] - p->class_start[c];
-        if (n > 0) kSchwarzLaunchers[c](P, B, p->class_start[c], n, nullptr, p->qcon, 1, ctx->stream);
+        if (n <= 0) continue;
+        if (kSchwarzLaunchers[c]) kSchwarzLaunchers[c](P, B, p->class_start[c], n, nullptr, p->qcon, 1, ctx->stream);
+        else kRysBoundLaunchers[c](P, ctx->rys, p->class_start[c], n, nullptr, p->qcon, 1, ctx->stream);
     }
     MI_CUDA(ctx, cudaGetLastError());
     std::vector<double> q(p->npair);

@@ -40,7 +40,7 @@ namespace {
 
 constexpr size_t kScratchBytes = (size_t)8 << 20;  // the stated maximum: 8 MiB
 constexpr size_t kAlign = 256;
-constexpr int kTableM = 4 * MOLINTS_LMAX + 1;  // Boys orders the class kernels use
+constexpr int kTableM = 4 * kLmaxHgp + 1;  // Boys orders the HGP class kernels use
 constexpr size_t kTableBytes =
     ((size_t)kTableM * kBoysRows * kBoysScaledCols * sizeof(double) + kAlign - 1) / kAlign * kAlign;
 constexpr int kMaxDevices = 64;
@@ -97,7 +97,7 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
     if (ns > 0 && (!b->expn || !b->coef)) return noalloc_fail(err, err_len, MOLINTS_ERR_INVALID, "null primitives");
     int nprim_tot = 0;
     for (int s = 0; s < ns; ++s) {
-        if (b->L[s] > MOLINTS_LMAX) return noalloc_fail(err, err_len, MOLINTS_ERR_UNSUPPORTED, "shell above d");
+        if (b->L[s] > kLmaxHgp) return noalloc_fail(err, err_len, MOLINTS_ERR_UNSUPPORTED, "shell above d");
         if (b->nprim[s] < 1 || b->nprim[s] > 255 || b->prim_off[s] < 0)
             return noalloc_fail(err, err_len, MOLINTS_ERR_INVALID, "shell primitive count out of range");
         nprim_tot = std::max(nprim_tot, b->prim_off[s] + b->nprim[s]);
@@ -201,6 +201,15 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
             ncoef[p0 + i] = b->coef[p0 + i] * cn * std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * L);
         }
     }
+    auto tightness = [&](int sh) {
+        const int p0 = b->prim_off[sh];
+        double lo = b->expn[p0], hi = lo;
+        for (int i = 1; i < b->nprim[sh]; ++i) {
+            lo = std::min(lo, b->expn[p0 + i]);
+            hi = std::max(hi, b->expn[p0 + i]);
+        }
+        return std::sqrt(lo * hi);
+    };
     // pair k (reference order i >= j) -> canonical (a, b), class, K; sort keys in g_order
     auto canon = [&](int k, int &a, int &bb, int &cls, int &npp) {
         int i = (int)((std::sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
@@ -209,7 +218,9 @@ extern "C" int molints_eri_packed_noalloc(const molints_basis *b, const molints_
         const int j = k - i * (i + 1) / 2;
         a = i;
         bb = j;
-        if (b->L[a] < b->L[bb]) std::swap(a, bb);
+        // larger L first; for equal L the tighter shell (larger sqrt(min * max exponent)), so
+        // that the HRR moves angular momentum away from it
+        if (b->L[a] < b->L[bb] || (b->L[a] == b->L[bb] && tightness(a) < tightness(bb))) std::swap(a, bb);
         cls = pair_class(b->L[a], b->L[bb]);
         npp = b->nprim[a] * b->nprim[bb];
     };

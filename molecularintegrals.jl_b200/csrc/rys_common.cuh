@@ -1,0 +1,330 @@
+// rys_common.cuh -- device templates of the Rys class kernels (generated/rys_*.cu).
+//
+// One group of C::G threads owns one contracted shell quartet (ab|cd) at a time:
+//   1. rys_contract: the primitive quartets in batches of C::NPB.  Stage 1, one thread per
+//      (primitive quartet, root, axis): the Rys node u and weight W of that root, then the
+//      2-D table I(a, c), a <= E, c <= F, of that axis (the x table carries the prefactor
+//      and W) into shared memory.  Stage 2, every thread: its own entries of the [e0|f0]
+//      block, sum over the batch and the roots of I_x I_y I_z, accumulated in registers in
+//      FP64.  The contracted block ends in shared memory.
+//   2. rys_hrr: bra HRR into a (ab|f0) buffer, then ket HRR, both in the closed binomial form,
+//      times the component norms; a sink stores (or reduces) each (ab|cd).
+// Recurrences: Rys, Dupuis and King's 2-D integrals in the Head-Gordon/Pople variables, with
+// u = t^2 the root (see gen_rys.py); MolecularIntegrals.jl states the same method in
+// src/Rys.jl:59-156.
+#pragma once
+#include "eri_common.cuh"
+
+namespace molints {
+
+constexpr int kRysXmax = 100;   // Chebyshev fits on [0, 100); Gauss-Hermite limit above
+constexpr int kRysNcheb = 16;
+constexpr int kRysNmono = 20;   // AB^(px,py,pz), px+py+pz <= 3
+
+// Class tables emitted by gen_rys.py.
+struct RysClassTabs {
+    const uint32_t *blk;       // [NBLK] block entry -> table offsets x | y << 8 | z << 16
+    const uint16_t *bra_off;   // [NAB+1] term ranges of the bra outputs
+    const uint32_t *bra_term;  // block row | monomial << 8 | binomial << 16
+    const uint16_t *ket_off;   // [NCD+1]
+    const uint32_t *ket_term;  // block column | monomial << 8 | binomial << 16
+    const double *norm_ab;     // [NAB] component norms of a and b
+    const double *norm_cd;     // [NCD]
+};
+
+// (px, py, pz) of monomial m, packed px | py << 2 | pz << 4, in gen_rys.MONOS order.
+static __device__ const unsigned char kRysMonoPow[kRysNmono] = {
+    0x00, 0x01, 0x04, 0x10, 0x02, 0x05, 0x11, 0x08, 0x14, 0x20,
+    0x03, 0x06, 0x12, 0x09, 0x15, 0x21, 0x0c, 0x18, 0x24, 0x30};
+
+__device__ __forceinline__ double rys_monomial(int m, double x, double y, double z) {
+    const unsigned p = kRysMonoPow[m];
+    double v = 1.0;
+    for (unsigned i = 0; i < (p & 3u); ++i) v *= x;
+    for (unsigned i = 0; i < ((p >> 2) & 3u); ++i) v *= y;
+    for (unsigned i = 0; i < ((p >> 4) & 3u); ++i) v *= z;
+    return v;
+}
+
+// sum_k c_k T_k(s) for 16 coefficients by Clenshaw's recurrence.
+__device__ __forceinline__ double clenshaw16(const double *__restrict__ c, double s) {
+    const double2 *v = reinterpret_cast<const double2 *>(c);
+    double2 q[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) q[k] = __ldg(v + k);
+    const double s2 = 2.0 * s;
+    double b1 = 0.0, b2 = 0.0;
+#pragma unroll
+    for (int k = 15; k >= 1; --k) {
+        const double ck = (k & 1) ? q[k >> 1].y : q[k >> 1].x;
+        const double t = fma(s2, b1, ck - b2);
+        b2 = b1;
+        b1 = t;
+    }
+    return fma(s, b1, q[0].x - b2);
+}
+
+// Node u_r = t_r^2 and weight W_r of the NR-point Rys rule at X >= 0:
+// sum_r W_r u_r^m = F_m(X) for m < 2 NR.
+template <int NR>
+__device__ __forceinline__ void rys_root(const RysTab &R, double X, int r, double &u, double &w) {
+    if (X < (double)kRysXmax) {
+        const int j = (int)X;
+        const double s = 2.0 * (X - (double)j) - 1.0;
+        const double *c = R.cheb + (size_t)kRysXmax * kRysNcheb * NR * (NR - 1) +
+                          ((size_t)j * 2 * NR + r) * kRysNcheb;
+        u = clenshaw16(c, s);
+        w = clenshaw16(c + NR * kRysNcheb, s);
+    } else {
+        const int o = NR * (NR - 1) / 2 + r;
+        const double ox = 1.0 / X;
+        u = __ldg(R.herm_x2 + o) * ox;
+        w = __ldg(R.herm_w + o) * sqrt(ox);
+    }
+}
+
+// Barrier over the G threads of group gid (named barrier gid+1 for 64-thread groups).
+template <int G>
+__device__ __forceinline__ void group_sync(int gid) {
+    if constexpr (G == 32) {
+        __syncwarp();
+    } else if constexpr (G >= 128) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(gid + 1), "r"(G) : "memory");
+    }
+}
+
+template <int G>
+__device__ __forceinline__ double group_max(double v, double *red, int gid) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if constexpr (G == 32) {
+        return v;
+    } else {
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+        group_sync<G>(gid);
+        double r = 0.0;
+#pragma unroll
+        for (int w = 0; w < G / 32; ++w) r = fmax(r, red[gid * (G / 32) + w]);
+        group_sync<G>(gid);
+        return r;
+    }
+}
+
+// The contracted [e0|f0] block of bra pair ib (primitive pairs [i0, i1)) and ket pair ik
+// ([j0, j1)) into work[0 .. NBLK).  All G threads of the group call it; it ends with a barrier.
+template <class C>
+__device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, const RysClassTabs &T,
+                                             const int4 ib, const int4 ik, int i0, int i1, int j0,
+                                             int j1, double *__restrict__ work, int lane, int gid) {
+    constexpr int S = C::S, F1 = C::F + 1, NR = C::NR, E = C::E, F = C::F;
+    double acc[C::ACC];
+    uint32_t off[C::ACC];
+#pragma unroll
+    for (int k = 0; k < C::ACC; ++k) {
+        acc[k] = 0.0;
+        const int e = lane + k * C::G;
+        off[k] = (e < C::NBLK) ? __ldg(&T.blk[e]) : 0u;
+    }
+    const int nbp = i1 - i0, nq = nbp * (j1 - j0);
+    const int tb = lane / (3 * NR), tr = (lane / 3) % NR, tax = lane % 3;
+    for (int g0 = 0; g0 < nq; g0 += C::NPB) {
+        const int nb = min(C::NPB, nq - g0);
+        if (tb < nb) {
+            const int g = g0 + tb;
+            const int gj = g / nbp;
+            const PrimPair bra = load_pp(P.pp, ib.x + i0 + (g - gj * nbp));
+            const PrimPair ket = load_pp(P.pp, ik.x + j0 + gj);
+            const double rz = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = rz * rz;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double X = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            double u, w;
+            rys_root<NR>(R, X, tr, u, w);
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const double PQ = tax == 0 ? PQx : (tax == 1 ? PQy : PQz);
+            const double PA = tax == 0 ? bra.pax : (tax == 1 ? bra.pay : bra.paz);
+            const double QC = tax == 0 ? ket.pax : (tax == 1 ? ket.pay : ket.paz);
+            const double c00 = fma(-ez * PQ, u, PA);
+            const double d00 = fma(zz * PQ, u, QC);
+            const double b10 = bra.oo2z * fma(-ez, u, 1.0);
+            const double b01 = ket.oo2z * fma(-zz, u, 1.0);
+            const double b00 = 0.5 * r2 * u;
+            double *tab = work + ((tb * NR + tr) * 3 + tax) * S;
+            // column c = 0 by the a-recurrence, then column c+1 from columns c and c-1
+            double cur[E + 1], prev[E + 1];
+            cur[0] = tax == 0 ? bra.kab * ket.kab * rz * w : 1.0;
+            if (E > 0) cur[1] = c00 * cur[0];
+#pragma unroll
+            for (int a = 1; a < E; ++a) cur[a + 1] = fma(c00, cur[a], (double)a * b10 * cur[a - 1]);
+#pragma unroll
+            for (int a = 0; a <= E; ++a) {
+                tab[a * F1] = cur[a];
+                prev[a] = 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < F; ++c) {
+                double nxt[E + 1];
+#pragma unroll
+                for (int a = 0; a <= E; ++a) {
+                    double v = d00 * cur[a];
+                    if (c > 0) v = fma((double)c * b01, prev[a], v);
+                    if (a > 0) v = fma((double)a * b00, cur[a - 1], v);
+                    nxt[a] = v;
+                }
+#pragma unroll
+                for (int a = 0; a <= E; ++a) {
+                    prev[a] = cur[a];
+                    cur[a] = nxt[a];
+                    tab[a * F1 + c + 1] = nxt[a];
+                }
+            }
+        }
+        group_sync<C::G>(gid);
+        for (int b = 0; b < nb; ++b) {
+#pragma unroll 1
+            for (int r = 0; r < NR; ++r) {
+                const double *__restrict__ tx = work + (b * NR + r) * 3 * S;
+#pragma unroll
+                for (int k = 0; k < C::ACC; ++k) {
+                    const uint32_t o = off[k];
+                    acc[k] = fma(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], acc[k]);
+                }
+            }
+        }
+        group_sync<C::G>(gid);
+    }
+#pragma unroll
+    for (int k = 0; k < C::ACC; ++k) {
+        const int e = lane + k * C::G;
+        if (e < C::NBLK) work[e] = acc[k];
+    }
+    group_sync<C::G>(gid);
+}
+
+// HRR of the contracted block blk[NA][NC] (shared) into the normalised (ab|cd): bra pass into
+// mid[NAB][NC], barrier, ket pass; sink(r, s, value) gets output (r = ia*NB + ib,
+// s = ic*ND + id).  DIAG: only the outputs s == r (the bound kernels, bra pair == ket pair).
+template <class C, bool DIAG, class Sink>
+__device__ __forceinline__ void rys_hrr(const RysClassTabs &T, const double *__restrict__ blk,
+                                        double *__restrict__ mid, const double *__restrict__ mono,
+                                        int lane, int gid, Sink &&sink) {
+    for (int w = lane; w < C::NAB * C::NC; w += C::G) {
+        const int r = w / C::NC, c = w - r * C::NC;
+        const int t1 = __ldg(&T.bra_off[r + 1]);
+        double v = 0.0;
+        for (int t = __ldg(&T.bra_off[r]); t < t1; ++t) {
+            const uint32_t x = __ldg(&T.bra_term[t]);
+            v = fma((double)(x >> 16) * mono[(x >> 8) & 255u], blk[(x & 255u) * C::NC + c], v);
+        }
+        mid[w] = v;
+    }
+    group_sync<C::G>(gid);
+    const double *__restrict__ mcd = mono + kRysNmono;
+    if constexpr (DIAG) {
+        for (int r = lane; r < C::NAB; r += C::G) {
+            const int t1 = __ldg(&T.ket_off[r + 1]);
+            double v = 0.0;
+            for (int t = __ldg(&T.ket_off[r]); t < t1; ++t) {
+                const uint32_t x = __ldg(&T.ket_term[t]);
+                v = fma((double)(x >> 16) * mcd[(x >> 8) & 255u], mid[r * C::NC + (x & 255u)], v);
+            }
+            sink(r, r, v * __ldg(&T.norm_ab[r]) * __ldg(&T.norm_cd[r]));
+        }
+    } else {
+        for (int w = lane; w < C::NAB * C::NCD; w += C::G) {
+            const int s = w / C::NAB, r = w - s * C::NAB;
+            const int t1 = __ldg(&T.ket_off[s + 1]);
+            double v = 0.0;
+            for (int t = __ldg(&T.ket_off[s]); t < t1; ++t) {
+                const uint32_t x = __ldg(&T.ket_term[t]);
+                v = fma((double)(x >> 16) * mcd[(x >> 8) & 255u], mid[r * C::NC + (x & 255u)], v);
+            }
+            sink(r, s, v * __ldg(&T.norm_ab[r]) * __ldg(&T.norm_cd[s]));
+        }
+    }
+}
+
+// Persistent work-queue kernel body: each group takes chunks (one bra pair, a run of ket pairs
+// of one molecule) from the class pair's counter and computes their quartets one by one.
+template <class C>
+__device__ __forceinline__ void rys_queue_body(const EriQueue &Q, const RysTab &R, const RysClassTabs &T) {
+    extern __shared__ __align__(16) double rys_smem[];
+    __shared__ int s_chunk[128 / C::G];
+    const int gid = threadIdx.x / C::G, lane = threadIdx.x - gid * C::G;
+    double *mono = rys_smem + gid * C::SMEM_GROUP;
+    double *work = mono + 2 * kRysNmono;
+    for (;;) {
+        if (lane == 0) s_chunk[gid] = atomicAdd(Q.counter, 1);
+        group_sync<C::G>(gid);
+        const int c = s_chunk[gid];
+        group_sync<C::G>(gid);
+        if (c >= Q.nchunks) return;
+        const int4 ch = __ldg(&Q.chunks[c]);
+        double *__restrict__ out = Q.out + __ldg(&Q.mol_out[ch.w]);
+        const int p = ch.x;
+        const int4 ib = __ldg(&Q.pairs.info[p]);
+        const double2 bp = __ldg(&Q.pairs.bnd[p]);
+        const double4 gb = ldg4(&Q.pairs.geo[p]);
+        for (int q = ch.y; q < ch.y + ch.z; ++q) {
+            const int4 ik = __ldg(&Q.pairs.info[q]);
+            const double2 bq = __ldg(&Q.pairs.bnd[q]);
+            const int nbp = (bp.x * bq.x < Q.screen_cut) ? 0 : ib.y;  // screened: written as 0
+            rys_contract<C>(Q.pairs, R, T, ib, ik, 0, nbp, 0, ik.y, work, lane, gid);
+            const double4 gk = ldg4(&Q.pairs.geo[q]);
+            for (int m = lane; m < 2 * kRysNmono; m += C::G)
+                mono[m] = m < kRysNmono ? rys_monomial(m, gb.x, gb.y, gb.z)
+                                        : rys_monomial(m - kRysNmono, gk.x, gk.y, gk.z);
+            group_sync<C::G>(gid);
+            const bool dab = ib.z == ib.w, dcd = ik.z == ik.w, same = p == q;
+            rys_hrr<C, false>(T, work, work + C::NBLK, mono, lane, gid, [&](int r, int s, double v) {
+                const int ia = r / C::NB, jb = r - ia * C::NB, ic = s / C::ND, jd = s - ic * C::ND;
+                if ((dab && ia < jb) || (dcd && ic < jd)) return;
+                const long long ij = pair_index(ib.z + ia, ib.w + jb), kl = pair_index(ik.z + ic, ik.w + jd);
+                if (same && ij < kl) return;
+                out[packed_index(ij, kl)] = v;
+            });
+            group_sync<C::G>(gid);
+        }
+    }
+}
+
+// Bounds of the pairs [p0, p0+np) of a pair class (bra class == ket class), one group per pair:
+// full == 0: for every primitive pair k, from the diagonal primitive quartet,
+//   pbound[k] = {sqrt(max |(a_k b_k|a_k b_k)|), sqrt(max |[e0|e0]_kk|)};
+// full != 0: the contracted Q_p = sqrt(max |(ab|ab)|) into qout[p].
+template <class C>
+__device__ __forceinline__ void rys_bound_body(const PairTab &P, const RysTab &R, const RysClassTabs &T,
+                                               int p0, int np, double2 *pbound, double *qout, int full) {
+    extern __shared__ __align__(16) double rys_smem[];
+    __shared__ double s_red[4];
+    constexpr int NG = 128 / C::G;
+    const int gid = threadIdx.x / C::G, lane = threadIdx.x - gid * C::G;
+    const int t = blockIdx.x * NG + gid;
+    if (t >= np) return;
+    double *mono = rys_smem + gid * C::SMEM_GROUP;
+    double *work = mono + 2 * kRysNmono;
+    const int p = p0 + t;
+    const int4 in = __ldg(&P.info[p]);
+    const double4 g = ldg4(&P.geo[p]);
+    for (int m = lane; m < 2 * kRysNmono; m += C::G) mono[m] = rys_monomial(m % kRysNmono, g.x, g.y, g.z);
+    const int nk = full ? 1 : in.y;
+    for (int k = 0; k < nk; ++k) {
+        const int i0 = full ? 0 : k, i1 = full ? in.y : k + 1;
+        rys_contract<C>(P, R, T, in, in, i0, i1, i0, i1, work, lane, gid);
+        double wmax = 0.0, m = 0.0;
+        for (int a = lane; a < C::NA; a += C::G) wmax = fmax(wmax, fabs(work[a * C::NC + a]));
+        rys_hrr<C, true>(T, work, work + C::NBLK, mono, lane, gid,
+                         [&](int, int, double v) { m = fmax(m, fabs(v)); });
+        m = group_max<C::G>(m, s_red, gid);
+        wmax = group_max<C::G>(wmax, s_red, gid);
+        if (lane == 0) {
+            if (full) qout[p] = sqrt(m);
+            else pbound[in.x + k] = make_double2(sqrt(m), sqrt(wmax));
+        }
+        group_sync<C::G>(gid);
+    }
+}
+
+}  // namespace molints

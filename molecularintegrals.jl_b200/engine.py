@@ -4,6 +4,7 @@ The public calls mirror the reference's drivers (MolecularIntegrals.jl):
 
     all_twoe_ints(shells)        ~ all_twoe_ints(bfs, ERI=coulomb)   src/ERI.jl:104-112
     all_twoe_ints_chrr(shells)   ~ all_twoe_ints_chrr(bfs)           src/HGP.jl:22-34
+    all_twoe_ints_rys(shells)    ~ all_twoe_ints_rys(bfs)            src/Rys.jl:16-24
 
 Both return the packed vector of unique normalised integrals in iindex order
 (src/Utils.jl:14-19), 0-based.  ``Engine`` exposes the context/plan API for callers that
@@ -22,8 +23,11 @@ LIB_PATH = HERE / "libmolints_cuda.so"
 
 FP64, MIXED = 0, 1
 BOYS_REFERENCE, BOYS_EXACT = 0, 1
-METHOD_AUTO, METHOD_HGP = 0, 1
-LMAX = 2
+METHOD_AUTO, METHOD_HGP, METHOD_RYS = 0, 1, 2
+LMAX = 3
+# shell-pair classes in the engine's order (la+lb, then la): index -> (la, lb)
+PAIR_CLASSES = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (3, 0), (2, 2), (3, 1), (2, 3), (3, 2), (3, 3)]
+NUM_PAIR_CLASSES = len(PAIR_CLASSES)
 
 _STATUS = {0: "OK", -1: "invalid argument", -2: "unsupported", -3: "HBM budget exceeded",
            -4: "CUDA error", -5: "timeout", -6: "out of host memory"}
@@ -34,7 +38,10 @@ EXPORTED_SYMBOLS = [
     "molints_eri_packed", "molints_plan_create", "molints_plan_execute", "molints_plan_stats",
     "molints_plan_destroy", "molints_plan_schwarz", "molints_boys_eval",
     "molints_plan_set_profiling", "molints_plan_launch_times", "molints_eri_packed_noalloc",
-    "molints_plan_create_batch", "molints_plan_npacked",
+    "molints_plan_create_batch", "molints_plan_npacked", "molints_set_class_methods",
+    "molints_serve_start", "molints_serve_stop", "molints_submit", "molints_poll",
+    "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
+    "molints_release", "molints_serve_stats",
 ]
 
 
@@ -105,6 +112,17 @@ def load_library(path: Path | str | None = None):
         "molints_eri_packed_noalloc": (ctypes.c_int, [P, P, P, P, ctypes.c_char_p, ctypes.c_size_t]),
         "molints_plan_create_batch": (ctypes.c_int, [P, I32, P, P, P]),
         "molints_plan_npacked": (I64, [P]),
+        "molints_set_class_methods": (ctypes.c_int, [P, P, I32]),
+        "molints_serve_start": (ctypes.c_int, [P, I32, I64]),
+        "molints_serve_stop": (ctypes.c_int, [P]),
+        "molints_submit": (ctypes.c_int, [P, P, P, P]),
+        "molints_poll": (ctypes.c_int, [P, I32]),
+        "molints_result": (ctypes.c_int, [P, P, P]),
+        "molints_result_copy": (ctypes.c_int, [P, P, I64]),
+        "molints_request_info": (ctypes.c_int, [P, P, P, P, P]),
+        "molints_request_error": (ctypes.c_char_p, [P]),
+        "molints_release": (ctypes.c_int, [P]),
+        "molints_serve_stats": (ctypes.c_int, [P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -203,6 +221,46 @@ class Plan:
             pass
 
 
+class Request:
+    """One submitted molecule of the serving API (molints_submit)."""
+
+    def __init__(self, engine: "Engine", handle: ctypes.c_void_p, npacked: int):
+        self.engine = engine
+        self.h = handle
+        self.npacked = npacked
+
+    def poll(self, timeout_ms: int = 0) -> bool:
+        """True once the result is ready, False on timeout; raises the request's error."""
+        rc = self.engine.lib.molints_poll(self.h, int(timeout_ms))
+        if rc == -5:
+            return False
+        if rc != 0:
+            msg = self.engine.lib.molints_request_error(self.h)
+            raise MolintsError(rc, msg.decode() if msg else "")
+        return True
+
+    def device_ptr(self) -> int:
+        ptr, n = ctypes.c_void_p(), ctypes.c_int64()
+        self.engine._check_req(self.engine.lib.molints_result(self.h, ctypes.byref(ptr), ctypes.byref(n)), self)
+        return ptr.value or 0
+
+    def result(self) -> np.ndarray:
+        out = np.empty(self.npacked, dtype=np.float64)
+        self.engine._check_req(self.engine.lib.molints_result_copy(self.h, _ptr(out), out.size), self)
+        return out
+
+    def info(self) -> dict:
+        t = [ctypes.c_double() for _ in range(3)]
+        slot = ctypes.c_int32()
+        self.engine.lib.molints_request_info(self.h, *[ctypes.byref(x) for x in t], ctypes.byref(slot))
+        return {"t_submit": t[0].value, "t_admit": t[1].value, "t_done": t[2].value, "slot": slot.value}
+
+    def release(self):
+        if self.h is not None:
+            self.engine.lib.molints_release(self.h)
+            self.h = None
+
+
 class Engine:
     """One molints context on one CUDA device."""
 
@@ -233,7 +291,7 @@ class Engine:
 
     def eri_packed(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
                    screen_cutoff=0.0, out: np.ndarray | None = None, with_stats=False,
-                   prim_cutoff=PRIM_CUTOFF):
+                   prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO):
         """The packed iindex vector of all unique integrals, into a host array."""
         arrs = _BasisArrays(shells)
         if out is None:
@@ -245,31 +303,70 @@ class Engine:
             return (out, st.as_dict()) if with_stats else out
         if out.dtype != np.float64 or out.size != shells.npacked or not out.flags.c_contiguous:
             raise ValueError("out must be a contiguous float64 array of npacked elements")
-        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, prim_cutoff=prim_cutoff)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff)
         st = Stats()
         self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
                                                 _ptr(out), 0, ctypes.byref(st)))
         return (out, st.as_dict()) if with_stats else out
 
     def eri_packed_device(self, shells, out_device_ptr: int, precision=FP64, boys=BOYS_REFERENCE,
-                          fp32_cutoff=0.0, screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF):
+                          fp32_cutoff=0.0, screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF,
+                          method=METHOD_AUTO):
         arrs = _BasisArrays(shells)
-        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, prim_cutoff=prim_cutoff)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff)
         st = Stats()
         self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
                                                 ctypes.c_void_p(out_device_ptr), 1, ctypes.byref(st)))
         return st.as_dict()
 
     def plan(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
-             screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF) -> Plan:
+             screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO) -> Plan:
         return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff,
-                                               prim_cutoff=prim_cutoff))
+                                               method, prim_cutoff))
 
     def plan_batch(self, shells_list, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
-                   screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF) -> Plan:
+                   screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO) -> Plan:
         """One plan over several molecules: a single execute computes all of them."""
         return Plan(self, list(shells_list), make_options(precision, boys, fp32_cutoff,
-                                                          screen_cutoff, prim_cutoff=prim_cutoff))
+                                                          screen_cutoff, method, prim_cutoff))
+
+    def set_class_methods(self, table=None):
+        """Per class pair method for METHOD_AUTO plans: ``table[(x, y)] = METHOD_HGP or
+        METHOD_RYS`` for pair-class indices x >= y (PAIR_CLASSES order); None resets."""
+        if table is None:
+            self._check(self.lib.molints_set_class_methods(self.ctx, None, 0))
+            return
+        arr = np.zeros(NUM_PAIR_CLASSES * NUM_PAIR_CLASSES, dtype=np.int32)
+        for (x, y), m in dict(table).items():
+            arr[x * NUM_PAIR_CLASSES + y] = m
+        self._check(self.lib.molints_set_class_methods(self.ctx, _ptr(arr), arr.size))
+
+    # ---- serving
+    def serve_start(self, nslots: int = 4, hbm_budget_bytes: int = 0):
+        """Start this context's server: nslots concurrent slots, admission by HBM budget."""
+        self._check(self.lib.molints_serve_start(self.ctx, int(nslots), int(hbm_budget_bytes)))
+
+    def serve_stop(self):
+        self._check(self.lib.molints_serve_stop(self.ctx))
+
+    def submit(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
+               screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO) -> Request:
+        arrs = _BasisArrays(shells)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff)
+        h = ctypes.c_void_p()
+        self._check(self.lib.molints_submit(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
+                                            ctypes.byref(h)))
+        return Request(self, h, shells.npacked)
+
+    def serve_stats(self) -> dict:
+        v = [ctypes.c_int64() for _ in range(4)]
+        self._check(self.lib.molints_serve_stats(self.ctx, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("ledger_bytes", "queued", "done", "failed"), [x.value for x in v]))
+
+    def _check_req(self, rc: int, req: Request):
+        if rc != 0:
+            msg = self.lib.molints_request_error(req.h)
+            raise MolintsError(rc, msg.decode() if msg else "")
 
     def boys(self, mmax: int, T, mode=BOYS_REFERENCE) -> np.ndarray:
         T = np.ascontiguousarray(T, dtype=np.float64)
@@ -308,4 +405,10 @@ def all_twoe_ints(shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
 def all_twoe_ints_chrr(shells) -> np.ndarray:
     """Drop-in for all_twoe_ints_chrr(bfs) (src/HGP.jl:22-34), with its layout and
     normalisation defects fixed: the same vector as all_twoe_ints."""
-    return default_engine().eri_packed(shells)
+    return default_engine().eri_packed(shells, method=METHOD_HGP)
+
+
+def all_twoe_ints_rys(shells) -> np.ndarray:
+    """Drop-in for all_twoe_ints_rys(bfs) (src/Rys.jl:16-24): Rys quadrature for every class
+    pair, with the contracted-function norms the reference driver leaves out applied."""
+    return default_engine().eri_packed(shells, method=METHOD_RYS, boys=BOYS_EXACT)

@@ -218,7 +218,7 @@ def test_batch_plan_equals_single_plans(eng):
     """Three molecules in one batch plan (one work queue per class pair across molecules)
     give each molecule's single-plan vector exactly, at its offset."""
     import torch
-    mols = [mi.config2(), mi.config0(), _rand_basis(105, 2)]
+    mols = [mi.config2(), mi.config0(), _rand_basis(105, 2), _f_molecule(7)]
     plan = eng.plan_batch(mols)
     out = torch.full((plan.npacked,), float("nan"), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
@@ -245,10 +245,16 @@ def test_edge_cases(eng):
     assert v.shape == (1,) and v[0] == pytest.approx(2 / np.sqrt(np.pi) * np.sqrt(2.0 / 2), rel=1e-14)
     empty = mi.Shells.from_list([])
     assert eng.eri_packed(empty).shape == (0,)
-    f_shell = mi.Shells.from_list([((0.0, 0.0, 0.0), 3, [(1.0, 1.0)])])
+    g_shell = mi.Shells.from_list([((0.0, 0.0, 0.0), 4, [(1.0, 1.0)])])
     with pytest.raises(engine.MolintsError) as e:
-        eng.eri_packed(f_shell)
+        eng.eri_packed(g_shell)
     assert e.value.status == -2
+    # one f shell: (ff|ff) on one centre, against the oracle
+    f_shell = mi.Shells.from_list([((0.1, -0.2, 0.3), 3, [(1.3, 1.0)])])
+    from oracle import oracle as O
+    with O.exact_boys():
+        ref = O.eri_packed_hgp_ld(f_shell, nthreads=4)
+    assert np.max(np.abs(eng.eri_packed(f_shell) - ref)) < TOL_FP64
     bad = mi.Shells.from_list([((0.0, 0.0, 0.0), 0, [(-1.0, 1.0)])])
     with pytest.raises(engine.MolintsError) as e:
         eng.eri_packed(bad)
@@ -264,3 +270,98 @@ def test_budget_refusal():
         assert err.value.status == -3
     finally:
         e.close()
+
+
+# ------------------------------------------------------------------ f shells and Rys
+def _f_molecule(seed, nheavy=2, nh=2):
+    """A small molecule of the serving workload's shape: polarised heavy atoms that carry an
+    f(K=1) shell, and hydrogens."""
+    return mi.basis.synthetic_molecule(seed, nheavy, nh, mi.basis.POLARISED_C, mi.basis.POLARISED_H,
+                                       0.1, 1e4, f"fmol{seed}", heavy_extra=[(3, 1)])
+
+
+def _exact_ld(oracle, sh):
+    with oracle.exact_boys():
+        return oracle.eri_packed_hgp_ld(sh, nthreads=0)
+
+
+@pytest.mark.parametrize("seed", [201, 202, 203])
+def test_f_shells_random_bases(eng, oracle, seed):
+    """Random l <= 3 bases (every class pair up to (ff|ff); the f classes run the Rys
+    kernels): within 1e-12 Eh of the long-double HGP oracle, and of Huzinaga."""
+    from molints_b200 import engine
+    sh = _rand_basis(seed, 3, natom=2, kmax=2)
+    got = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
+    ld = _exact_ld(oracle, sh)
+    assert np.max(np.abs(got - ld)) < TOL_FP64
+    huz = oracle.eri_packed_huzinaga(sh, nthreads=0)
+    assert np.max(np.abs(got - huz)) < TOL_FP64
+
+
+def test_f_molecule_serving_shape(eng, oracle):
+    """A molecule of the serving workload's recipe (l <= 3, exponents to 1e4, K up to 7)."""
+    from molints_b200 import engine
+    sh = _f_molecule(11)
+    assert 3 in set(sh.L.tolist())
+    got = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
+    ld = _exact_ld(oracle, sh)
+    assert np.max(np.abs(got - ld)) < TOL_FP64
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2"])
+def test_rys_method_every_class(eng, oracle, cfg):
+    """METHOD_RYS (all_twoe_ints_rys's algorithm) for every class pair of configs 1 and 2."""
+    from molints_b200 import engine
+    sh = getattr(mi, cfg)()
+    got = eng.eri_packed(sh, method=engine.METHOD_RYS, boys=engine.BOYS_EXACT)
+    ld = _exact_ld(oracle, sh)
+    assert np.max(np.abs(got - ld)) < TOL_FP64
+
+
+def test_class_method_table(eng):
+    """AUTO follows the context's per-class table; HGP and Rys agree class by class."""
+    from molints_b200 import engine
+    sh = mi.config2()
+    hgp = eng.eri_packed(sh, boys=engine.BOYS_EXACT, method=engine.METHOD_HGP)
+    table = {(x, y): engine.METHOD_RYS for x in range(engine.NUM_PAIR_CLASSES) for y in range(x + 1)
+             if (x + y) % 2 == 0}
+    eng.set_class_methods(table)
+    try:
+        mix = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
+        plan = eng.plan(sh, boys=engine.BOYS_EXACT)
+        import torch
+        out = torch.empty(sh.npacked, dtype=torch.float64, device="cuda")
+        plan.set_profiling(True)
+        plan.execute(out.data_ptr())
+        names = [n for n, _ in plan.launch_times()]
+        plan.close()
+    finally:
+        eng.set_class_methods(None)
+    assert any(n.startswith("rys_") for n in names) and any(n.startswith("eri_") for n in names)
+    assert np.max(np.abs(mix - hgp)) < TOL_FP64
+    with pytest.raises(engine.MolintsError):
+        eng.set_class_methods({(0, 0): 7})
+
+
+def test_f_shell_schwarz_bounds(eng, oracle):
+    """Contracted Schwarz bounds of pairs with f shells (the Rys bound kernels)."""
+    import torch
+    sh = _f_molecule(13, nheavy=1, nh=1)
+    plan = eng.plan(sh)
+    out = torch.empty(sh.npacked, dtype=torch.float64, device="cuda")
+    plan.execute(out.data_ptr())
+    q = plan.schwarz()
+    ints = out.cpu().numpy()
+    plan.close()
+    off = sh.fn_offsets()
+    n = sh.nbf
+    npair = n * (n + 1) // 2
+    diag = ints[np.arange(npair) * (np.arange(npair) + 1) // 2 + np.arange(npair)]
+    for i in range(sh.nshell):
+        for j in range(i + 1):
+            m = 0.0
+            for a in range(off[i], off[i + 1]):
+                for b in range(off[j], off[j + 1]):
+                    ab = a * (a + 1) // 2 + b if a >= b else b * (b + 1) // 2 + a
+                    m = max(m, abs(diag[ab]))
+            assert q[i * (i + 1) // 2 + j] == pytest.approx(np.sqrt(m), rel=1e-12)

@@ -1,0 +1,181 @@
+"""CPU tests of the Rys path's generated data: the root/weight tables the kernels read, and the
+per-class tables (block offsets, closed-form HRR terms, norms) driven through a numpy
+emulation of the kernel's algorithm (rys_common.cuh) against the oracle."""
+import math
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import molints_b200 as mi
+
+ROOT = Path(__file__).resolve().parent.parent
+CSRC = ROOT / "molecularintegrals.jl_b200" / "csrc"
+sys.path.insert(0, str(CSRC))
+import gen_eri  # noqa: E402
+import gen_rys  # noqa: E402
+
+sys.path.pop(0)
+
+XMAX, NCHEB = 100, 16
+
+
+@pytest.fixture(scope="module")
+def rys_tables():
+    """The generated tables, read back from generated/rys_tables.cu as the kernels see them."""
+    text = (CSRC / "generated" / "rys_tables.cu").read_text()
+    out = {}
+    for name in ("kRysCheb", "kRysHermX2", "kRysHermW"):
+        body = re.search(name + r"\[\d+\] = \{(.*?)\};", text, re.S).group(1)
+        out[name] = np.array([float.fromhex(v) for v in re.findall(r"-?0x[0-9a-fp.+-]+", body)])
+    return out
+
+
+def _clenshaw(cf, s):
+    b1 = b2 = 0.0
+    for c in cf[:0:-1]:
+        b1, b2 = 2 * s * b1 - b2 + c, b1
+    return s * b1 - b2 + cf[0]
+
+
+def table_roots(tabs, n, X):
+    """Nodes and weights exactly as rys_root<n> evaluates them on the device."""
+    u, w = np.zeros(n), np.zeros(n)
+    if X < XMAX:
+        j = int(X)
+        s = 2.0 * (X - j) - 1.0
+        base = XMAX * NCHEB * n * (n - 1) + j * 2 * n * NCHEB
+        for r in range(n):
+            u[r] = _clenshaw(tabs["kRysCheb"][base + r * NCHEB: base + (r + 1) * NCHEB], s)
+            w[r] = _clenshaw(tabs["kRysCheb"][base + (n + r) * NCHEB: base + (n + r + 1) * NCHEB], s)
+    else:
+        o = n * (n - 1) // 2
+        u[:] = tabs["kRysHermX2"][o:o + n] / X
+        w[:] = tabs["kRysHermW"][o:o + n] / math.sqrt(X)
+    return u, w
+
+
+@pytest.mark.parametrize("n", range(1, 8))
+def test_root_tables_against_long_double_solver(oracle, rys_tables, n):
+    assert rys_tables["kRysCheb"].size == XMAX * NCHEB * 7 * 8
+    rng = np.random.default_rng(n)
+    Xs = np.concatenate([[0.0, 1e-12, 0.5, 0.999999, 1.0, 29.99, 30.0, 99.999, 100.0, 150.0, 1e4],
+                         rng.uniform(0, 100, 60), np.exp(rng.uniform(np.log(100), np.log(1e6), 10))])
+    for X in Xs:
+        u, w = table_roots(rys_tables, n, X)
+        ru, rw = oracle.rys_roots(n, X)
+        np.testing.assert_allclose(u, ru, rtol=2e-14, atol=0, err_msg=f"nodes n={n} X={X}")
+        np.testing.assert_allclose(w, rw, rtol=2e-14, atol=1e-300, err_msg=f"weights n={n} X={X}")
+        # the rule integrates the Boys moments: sum W u^k = F_k(X)
+        for k in range(2 * n):
+            Fk = oracle.boys(k, X)
+            assert abs(np.sum(w * u ** k) - Fk) <= 1e-14 * Fk + 1e-300, (n, X, k)
+
+
+def test_monomial_table_matches_generator():
+    text = (CSRC / "rys_common.cuh").read_text()
+    body = re.search(r"kRysMonoPow\[kRysNmono\] = \{(.*?)\};", text, re.S).group(1)
+    vals = [int(v, 16) for v in re.findall(r"0x[0-9a-f]+", body)]
+    assert vals == [px | (py << 2) | (pz << 4) for px, py, pz in gen_rys.MONOS]
+
+
+def _emulate_rys(X, Y, bra_prims, ket_prims, A, B, C, D, roots):
+    """rys_contract + rys_hrr of rys_common.cuh in numpy (FP64), with the class tables."""
+    t = gen_rys.class_tables(X, Y)
+    E, F, NR, S = t["e"], t["f"], t["nr"], t["S"]
+    blk = np.zeros(t["nblk"])
+    offs = np.array(t["blk"])
+    c0 = math.sqrt(2.0) * math.pi ** 1.25
+    for (a, ca), (b, cb) in bra_prims:
+        z = a + b
+        P = A + b / z * (B - A)
+        kab = c0 * ca * cb * math.exp(-a * b / z * np.sum((A - B) ** 2)) / z
+        for (c, cc), (d, cd) in ket_prims:
+            et = c + d
+            Q = C + d / et * (D - C)
+            kcd = c0 * cc * cd * math.exp(-c * d / et * np.sum((C - D) ** 2)) / et
+            r2 = 1.0 / (z + et)
+            rz = math.sqrt(r2)
+            PQ = P - Q
+            Xv = z * et * r2 * float(PQ @ PQ)
+            u, w = roots(NR, Xv)
+            ez, zz = et * r2, z * r2
+            for r in range(NR):
+                tabs = np.zeros((3, E + 1, F + 1))
+                for ax in range(3):
+                    c00 = (P - A)[ax] - ez * PQ[ax] * u[r]
+                    d00 = (Q - C)[ax] + zz * PQ[ax] * u[r]
+                    b10 = 0.5 / z * (1 - ez * u[r])
+                    b01 = 0.5 / et * (1 - zz * u[r])
+                    b00 = 0.5 * r2 * u[r]
+                    I = tabs[ax]
+                    I[0, 0] = kab * kcd * rz * w[r] if ax == 0 else 1.0
+                    for ia in range(E):
+                        I[ia + 1, 0] = c00 * I[ia, 0] + (ia * b10 * I[ia - 1, 0] if ia else 0.0)
+                    for ic in range(F):
+                        for ia in range(E + 1):
+                            v = d00 * I[ia, ic]
+                            if ic:
+                                v += ic * b01 * I[ia, ic - 1]
+                            if ia:
+                                v += ia * b00 * I[ia - 1, ic]
+                            I[ia, ic + 1] = v
+                fl = tabs.reshape(3, S)
+                blk += fl[0][offs[:, 0]] * fl[1][offs[:, 1]] * fl[2][offs[:, 2]]
+    AB, CD = A - B, C - D
+    mab = np.array([AB[0] ** m[0] * AB[1] ** m[1] * AB[2] ** m[2] for m in gen_rys.MONOS])
+    mcd = np.array([CD[0] ** m[0] * CD[1] ** m[1] * CD[2] ** m[2] for m in gen_rys.MONOS])
+    blk = blk.reshape(t["na"], t["nc"])
+    mid = np.array([sum(bn * mab[m] * blk[src] for src, m, bn in terms) for terms in t["bra"]])
+    out = np.zeros((t["nab"], t["ncd"]))
+    for s, terms in enumerate(t["ket"]):
+        out[:, s] = sum(bn * mcd[m] * mid[:, src] for src, m, bn in terms)
+    out *= np.outer(t["norm_ab"], t["norm_cd"])
+    return out.reshape(-1)
+
+
+def _norm_prims(l, prims):
+    ex = np.array([p[0] for p in prims])
+    co = np.array([p[1] for p in prims])
+    s = sum(co[i] * co[j] * (2 * np.sqrt(ex[i] * ex[j]) / (ex[i] + ex[j])) ** (l + 1.5)
+            for i in range(len(ex)) for j in range(len(ex)))
+    cn = 1 / np.sqrt(s)
+    return [(e, c * cn * (2 * e / np.pi) ** 0.75 * (4 * e) ** (l / 2)) for e, c in zip(ex, co)]
+
+
+@pytest.mark.parametrize("X,Y", gen_rys.class_pairs())
+def test_rys_class_emulation_matches_oracle(oracle, rys_tables, X, Y):
+    rng = np.random.default_rng(hash((X, Y, "rys")) % 2**32)
+    centres = [rng.uniform(-1.2, 1.2, 3) for _ in range(4)]
+    ls = [X[0], X[1], Y[0], Y[1]]
+    shells = []
+    for l, xyz in zip(ls, centres):
+        k = int(rng.integers(1, 3))
+        shells.append((xyz, l, mi.basis._random_shell(rng, l, k, 0.3, 6.0)))
+    sh = mi.Shells.from_list(shells)
+    with oracle.exact_boys():
+        ref = oracle.shell_quartet(sh, 0, 1, 2, 3).reshape(-1)
+    bra = [(p, q) for p in _norm_prims(ls[0], shells[0][2]) for q in _norm_prims(ls[1], shells[1][2])]
+    ket = [(p, q) for p in _norm_prims(ls[2], shells[2][2]) for q in _norm_prims(ls[3], shells[3][2])]
+    got = _emulate_rys(X, Y, bra, ket, *[np.asarray(c) for c in centres],
+                       roots=lambda n, x: table_roots(rys_tables, n, x))
+    assert np.max(np.abs(got - ref)) < 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_class_kernel_limits():
+    """Every class fits one block's shared memory and the 2-D tables fit one batch."""
+    for X, Y in gen_rys.class_pairs():
+        t = gen_rys.class_tables(X, Y)
+        assert (128 // t["G"]) * t["smem_group"] * 8 <= 227 * 1024
+        assert t["npb"] * 3 * t["nr"] <= t["G"]
+        assert max(max(o) for o in t["blk"]) < t["S"] < 256
+        assert t["na"] < 256 and t["nc"] < 256
+
+
+def test_rys_sources_are_current():
+    for X, Y in gen_rys.class_pairs():
+        p = gen_rys.OUT_DIR / f"rys_{gen_rys.tag_of(X, Y)}.cu"
+        assert p.read_text() == gen_rys.emit_class_pair(X, Y), p.name
+    assert (gen_eri.HERE / "eri_dispatch.h").read_text() == gen_eri.emit_dispatch(gen_eri.class_pairs())
