@@ -11,4 +11,4 @@ repository's ``__graft_entry__.py``.
 """
 from . import basis  # noqa: F401
 from .basis import (Shells, atom, build_basis, config0, config1, config2, config3,  # noqa: F401
-                    config3_molecule, config4_request, h2, ethane_staggered)
+                    config3_molecule, config4_arrivals, config4_request, h2, ethane_staggered)

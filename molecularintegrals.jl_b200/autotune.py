@@ -44,3 +44,50 @@ def tune_fp32_cutoff(engine, shells, target: float = 1e-9, safety: float = 0.25,
         return best, table
     finally:
         engine.set_stream(None)
+
+
+def _class_index(tag: str):
+    """'ddps' -> (bra pair-class index, ket pair-class index) in the engine's order."""
+    from . import engine as E
+    lv = {"s": 0, "p": 1, "d": 2, "f": 3}
+    bra = (lv[tag[0]], lv[tag[1]])
+    ket = (lv[tag[2]], lv[tag[3]])
+    return E.PAIR_CLASSES.index(bra), E.PAIR_CLASSES.index(ket)
+
+
+def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95):
+    """Per class pair, HGP or Rys, whichever kernel is faster on `molecules` (one batch plan
+    per method; each launch timed alone with CUDA events in profiling mode, best of
+    `repeats`).  Rys is taken only where it is faster by `margin`.  Returns (table, timings):
+    table[(x, y)] = METHOD_HGP or METHOD_RYS for engine.set_class_methods; timings maps the
+    class tag to (HGP ms, Rys ms).  Classes with an f shell have only Rys and are not listed."""
+    import torch
+    from . import engine as E
+    mols = list(molecules)
+    dev = torch.device("cuda", engine.device)
+    n = sum(m.npacked for m in mols)
+    out = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    engine.set_stream(stream.cuda_stream)
+    best = {}
+    try:
+        for meth, prefix in ((E.METHOD_HGP, "eri_"), (E.METHOD_RYS, "rys_")):
+            plan = engine.plan_batch(mols, method=meth, boys=E.BOYS_EXACT)
+            plan.set_profiling(True)
+            for _ in range(repeats):
+                plan.execute(out.data_ptr())
+                for name, ms in plan.launch_times():
+                    if name.startswith(prefix):
+                        key = (name[4:], meth)
+                        best[key] = min(best.get(key, float("inf")), ms)
+            plan.close()
+    finally:
+        engine.set_stream(None)
+    table, timings = {}, {}
+    for (tag, meth), ms in best.items():
+        if meth != E.METHOD_HGP or (tag, E.METHOD_RYS) not in best:
+            continue
+        rys = best[(tag, E.METHOD_RYS)]
+        timings[tag] = (ms, rys)
+        table[_class_index(tag)] = E.METHOD_RYS if rys < margin * ms else E.METHOD_HGP
+    return table, timings

@@ -259,9 +259,12 @@ static void rys_prepare_{tag}() {{
     }}
 }}
 
-void launch_rys_{tag}(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {{
-    if (Q.nchunks <= 0 || grid <= 0) return;
+// grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
+void launch_rys_{tag}(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {{
+    if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_{tag}();
+    constexpr int ng = 128 / C_{tag}::G;
+    const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
     rys_queue_{tag}<<<grid, 128, {smem_block}, s>>>(Q, R);
 }}
 

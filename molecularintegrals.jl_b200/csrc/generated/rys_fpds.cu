@@ -86,9 +86,12 @@ static void rys_prepare_fpds() {
     }
 }
 
-void launch_rys_fpds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
-    if (Q.nchunks <= 0 || grid <= 0) return;
+// grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
+void launch_rys_fpds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fpds();
+    constexpr int ng = 128 / C_fpds::G;
+    const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
     rys_queue_fpds<<<grid, 128, 15040, s>>>(Q, R);
 }
 

@@ -63,9 +63,12 @@ static void rys_prepare_ppss() {
     }
 }
 
-void launch_rys_ppss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s) {
-    if (Q.nchunks <= 0 || grid <= 0) return;
+// grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
+void launch_rys_ppss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_ppss();
+    constexpr int ng = 128 / C_ppss::G;
+    const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
     rys_queue_ppss<<<grid, 128, 4160, s>>>(Q, R);
 }
 

@@ -767,10 +767,14 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
                 const double nb = b1 - b0, nk = k1 - k0;
                 nchunk32 += (x == y) ? nb * (nb + 1) / 64.0 + nb : nb * (nk / 32.0 + 1.0);
             }
-    const int width = 32 * std::max(1, (int)std::ceil(nchunk32 / kMaxChunks));
+    const int widen = std::max(1, (int)std::ceil(nchunk32 / kMaxChunks));
+    // A Rys group computes a chunk's quartets one after another, so its chunks are short
+    // (kRysChunk ket pairs) to spread small classes over many groups.
+    constexpr int kRysChunk = 4;
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
             tmp.clear();
+            const int width = (p->method[x][y] == MOLINTS_METHOD_RYS ? kRysChunk : 32) * widen;
             const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
             const double w = 1.0 + lsum * lsum;
             double total = 0.0;
@@ -900,7 +904,9 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         Q.counter = p->counters + x * kNumPairClasses + y;
         Q.screen_cut = p->opts.screen_cutoff;
         Q.fp32_cut = p->opts.fp32_cutoff;
-        const int grid = (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);
+        // HGP: one warp per chunk, four per block; Rys: the launcher divides by its groups/block
+        const int grid = rys ? occ * ctx->num_sms
+                             : (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);
         const char *name = rys ? kRysNames[x][y] : kEriNames[x][y];
         if (int rc = mark(launches, name, 0, st)) return rc;
         if (rys) kRysLaunchers[x][y](Q, ctx->rys, grid, st);

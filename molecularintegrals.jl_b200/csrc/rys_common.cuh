@@ -13,6 +13,8 @@
 // u = t^2 the root (see gen_rys.py); MolecularIntegrals.jl states the same method in
 // src/Rys.jl:59-156.
 #pragma once
+#include <algorithm>
+
 #include "eri_common.cuh"
 
 namespace molints {
