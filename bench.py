@@ -257,8 +257,18 @@ def run_ours(args):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": npacked * 8,
            "timing": "host wall clock around molints_eri_packed (synchronous call)"}
 
+    # per-class HGP/Rys choice for the batch and serving workloads (l <= 3 molecules)
+    from molints_b200 import autotune as AT
+    t_tune = time.perf_counter()
+    class_table, class_timings = AT.tune_class_methods(
+        eng, [mi.config3_molecule(m) for m in range(1, 16, 2)] + [mi.config4_request(r) for r in range(4)])
+    t_tune = time.perf_counter() - t_tune
+    eng.set_class_methods(class_table)
+    eng.set_stream(stream.cuda_stream)
     batch = measure_batch(eng, stream, dev, fp32_cut, rank, world)
-    serving = measure_serving(local, fp32_cut, args.serve_window, rank)
+    serving = measure_serving(local, fp32_cut, args.serve_window, rank, class_table=class_table)
+    tuned = {"seconds": t_tune, "rys_classes": sorted(
+        t for t, (h, r) in class_timings.items() if class_table[AT._class_index(t)] == E.METHOD_RYS)}
 
     cpu = None
     if rank == 0 and world == 1:
@@ -289,6 +299,7 @@ def run_ours(args):
             "e2e": e2e,
             "batch_config3": batch,
             "serving_config4": serving,
+            "class_method_tuning": tuned,
             "gpu_launches": args.steps * 2 * plan64.stats()["n_kernel_launches"],
             "clocks": clocks,
         }
@@ -357,7 +368,7 @@ def measure_batch(eng, stream, dev, fp32_cut, rank, world, cap=1.5e9):
 
 
 def measure_serving(device, fp32_cut, window_s, rank, rate=200.0, nslots=8,
-                    budget=150 * 10**9):
+                    budget=150 * 10**9, class_table=None):
     """The serving stream: Poisson arrivals (mean `rate` per s over `window_s` s) of
     synthetic molecules with 20-285 cartesian functions, l <= 3 (f shells on heavy atoms
     half the time), submitted to the engine's server as they arrive.  The server admits them
@@ -374,9 +385,12 @@ def measure_serving(device, fp32_cut, window_s, rank, rate=200.0, nslots=8,
            "n_eri": int(sum(m.npacked for m in mols))}
     srv = E.Engine(device)
     try:
+        if class_table:
+            srv.set_class_methods(class_table)
         srv.serve_start(nslots=nslots, hbm_budget_bytes=budget)
-        for sh in mols[:nslots]:  # warm-up: kernel attributes, pools
-            r = srv.submit(sh)
+        # warm-up: kernel attributes and the result pool, grown by the largest requests
+        big = sorted(mols, key=lambda m: -m.npacked)[:4 * nslots]
+        for r in [srv.submit(sh) for sh in big]:
             r.poll(-1)
             r.release()
         for name, prec, cut in (("fp64", E.FP64, 0.0), ("mixed", E.MIXED, fp32_cut)):

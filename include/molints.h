@@ -162,7 +162,19 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *basis,
  * molecules go through one work queue per class pair. */
 int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                               const molints_options *opts, molints_plan **plan);
-/* Doubles the plan writes per execute (all molecules), or a negative status. */
+/* Sharding one basis over nshards devices (no reference counterpart).  Shard r owns the shell
+ * quartets whose highest shell index lies in a contiguous shell range (split by estimated
+ * cost), which are exactly the integrals of one contiguous slice [lo, hi) of the packed
+ * vector.  molints_shard_range gives the slice (host only, no device needed);
+ * molints_plan_create_shard makes a plan whose execute writes that slice into
+ * out_device[0 .. hi-lo).  The slices of shards 0..nshards-1 tile the vector in order. */
+int molints_shard_range(const molints_basis *basis, int32_t shard, int32_t nshards, int64_t *lo,
+                        int64_t *hi);
+int molints_plan_create_shard(molints_ctx *ctx, const molints_basis *basis,
+                              const molints_options *opts, int32_t shard, int32_t nshards,
+                              molints_plan **plan);
+/* Doubles the plan writes per execute (all molecules; a shard plan: its slice), or a negative
+ * status. */
 int64_t molints_plan_npacked(const molints_plan *plan);
 int molints_plan_execute(molints_plan *plan, double *out_device);
 int molints_plan_stats(const molints_plan *plan, molints_stats *stats);
@@ -218,6 +230,8 @@ int molints_eri_packed_noalloc(const molints_basis *basis, const molints_options
  * submit, poll, result, release and request_info may be called from any host thread. */
 typedef struct molints_request molints_request;
 
+/* The slots take the context's per-class method table (molints_set_class_methods) as it is at
+ * this call. */
 int molints_serve_start(molints_ctx *ctx, int32_t nslots, int64_t hbm_budget_bytes);
 /* Stop the server: queued requests fail, running ones finish; results stay valid until
  * released.  molints_destroy stops the context's server. */

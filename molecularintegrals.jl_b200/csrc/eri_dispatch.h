@@ -37,6 +37,19 @@ int occupancy_eri_dpds(int mixed);
 void launch_eri_dpdp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
 int occupancy_eri_dpdp(int mixed);
 void launch_schwarz_dpdp(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
+void launch_eri_fsss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fsss(int mixed);
+void launch_eri_fsps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fsps(int mixed);
+void launch_eri_fspp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fspp(int mixed);
+void launch_eri_fsds(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fsds(int mixed);
+void launch_eri_fsdp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fsdp(int mixed);
+void launch_eri_fsfs(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fsfs(int mixed);
+void launch_schwarz_fsfs(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 void launch_eri_ddss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
 int occupancy_eri_ddss(int mixed);
 void launch_eri_ddps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
@@ -50,6 +63,20 @@ int occupancy_eri_dddp(int mixed);
 void launch_eri_dddd(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
 int occupancy_eri_dddd(int mixed);
 void launch_schwarz_dddd(const PairTab &P, const BoysTab &B, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
+void launch_eri_fpss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fpss(int mixed);
+void launch_eri_fpps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fpps(int mixed);
+void launch_eri_fppp(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fppp(int mixed);
+void launch_eri_fpds(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fpds(int mixed);
+void launch_eri_fdss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fdss(int mixed);
+void launch_eri_fdps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_fdps(int mixed);
+void launch_eri_ffss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
+int occupancy_eri_ffss(int mixed);
 void launch_rys_ssss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
 int occupancy_rys_ssss();
 void launch_rys_bound_ssss(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
@@ -200,7 +227,7 @@ typedef void (*RysLauncher)(const EriQueue &, const RysTab &, int, cudaStream_t)
 typedef int (*RysOccupancy)();
 typedef void (*RysBoundLauncher)(const PairTab &, const RysTab &, int, int, double2 *, double *, int, cudaStream_t);
 constexpr int kLmax = 3;      // shells up to f (Rys)
-constexpr int kLmaxHgp = 2;   // HGP kernels: shells up to d
+constexpr int kLmaxHgp = 2;   // every class pair up to d has an HGP kernel
 constexpr int kNumPairClasses = 11;
 // pair class c = (kPairClassLa[c], kPairClassLb[c]), ordered by la+lb then la
 constexpr int kPairClassLa[] = {0, 1, 1, 2, 2, 3, 2, 3, 2, 3, 3};
@@ -212,12 +239,12 @@ static const EriLauncher kEriLaunchers[11][11] = {
     {launch_eri_ppss, launch_eri_ppps, launch_eri_pppp, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {launch_eri_dsss, launch_eri_dsps, launch_eri_dspp, launch_eri_dsds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {launch_eri_dpss, launch_eri_dpps, launch_eri_dppp, launch_eri_dpds, launch_eri_dpdp, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {launch_eri_fsss, launch_eri_fsps, launch_eri_fspp, launch_eri_fsds, launch_eri_fsdp, launch_eri_fsfs, nullptr, nullptr, nullptr, nullptr, nullptr},
     {launch_eri_ddss, launch_eri_ddps, launch_eri_ddpp, launch_eri_ddds, launch_eri_dddp, nullptr, launch_eri_dddd, nullptr, nullptr, nullptr, nullptr},
+    {launch_eri_fpss, launch_eri_fpps, launch_eri_fppp, launch_eri_fpds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {launch_eri_fdss, launch_eri_fdps, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {launch_eri_ffss, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
 };
 static const EriOccupancy kEriOccupancy[11][11] = {
     {occupancy_eri_ssss, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
@@ -225,12 +252,12 @@ static const EriOccupancy kEriOccupancy[11][11] = {
     {occupancy_eri_ppss, occupancy_eri_ppps, occupancy_eri_pppp, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {occupancy_eri_dsss, occupancy_eri_dsps, occupancy_eri_dspp, occupancy_eri_dsds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {occupancy_eri_dpss, occupancy_eri_dpps, occupancy_eri_dppp, occupancy_eri_dpds, occupancy_eri_dpdp, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {occupancy_eri_fsss, occupancy_eri_fsps, occupancy_eri_fspp, occupancy_eri_fsds, occupancy_eri_fsdp, occupancy_eri_fsfs, nullptr, nullptr, nullptr, nullptr, nullptr},
     {occupancy_eri_ddss, occupancy_eri_ddps, occupancy_eri_ddpp, occupancy_eri_ddds, occupancy_eri_dddp, nullptr, occupancy_eri_dddd, nullptr, nullptr, nullptr, nullptr},
+    {occupancy_eri_fpss, occupancy_eri_fpps, occupancy_eri_fppp, occupancy_eri_fpds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {occupancy_eri_fdss, occupancy_eri_fdps, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {occupancy_eri_ffss, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
 };
 static const char *const kEriNames[11][11] = {
     {"eri_ssss", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
@@ -238,12 +265,12 @@ static const char *const kEriNames[11][11] = {
     {"eri_ppss", "eri_ppps", "eri_pppp", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {"eri_dsss", "eri_dsps", "eri_dspp", "eri_dsds", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {"eri_dpss", "eri_dpps", "eri_dppp", "eri_dpds", "eri_dpdp", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {"eri_fsss", "eri_fsps", "eri_fspp", "eri_fsds", "eri_fsdp", "eri_fsfs", nullptr, nullptr, nullptr, nullptr, nullptr},
     {"eri_ddss", "eri_ddps", "eri_ddpp", "eri_ddds", "eri_dddp", nullptr, "eri_dddd", nullptr, nullptr, nullptr, nullptr},
+    {"eri_fpss", "eri_fpps", "eri_fppp", "eri_fpds", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
-    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {"eri_fdss", "eri_fdps", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
+    {"eri_ffss", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
 };
 static const RysLauncher kRysLaunchers[11][11] = {
     {launch_rys_ssss, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
@@ -288,7 +315,7 @@ static const char *const kSchwarzNames[11] = {
     "schwarz_ss", "schwarz_ps", "schwarz_pp", "schwarz_ds", "schwarz_dp", "schwarz_fs", "schwarz_dd", "schwarz_fp", "schwarz_df", "schwarz_fd", "schwarz_ff"
 };
 static const SchwarzLauncher kSchwarzLaunchers[11] = {
-    launch_schwarz_ssss, launch_schwarz_psps, launch_schwarz_pppp, launch_schwarz_dsds, launch_schwarz_dpdp, nullptr, launch_schwarz_dddd, nullptr, nullptr, nullptr, nullptr
+    launch_schwarz_ssss, launch_schwarz_psps, launch_schwarz_pppp, launch_schwarz_dsds, launch_schwarz_dpdp, launch_schwarz_fsfs, launch_schwarz_dddd, nullptr, nullptr, nullptr, nullptr
 };
 static const RysBoundLauncher kRysBoundLaunchers[11] = {
     launch_rys_bound_ssss, launch_rys_bound_psps, launch_rys_bound_pppp, launch_rys_bound_dsds, launch_rys_bound_dpdp, launch_rys_bound_fsfs, launch_rys_bound_dddd, launch_rys_bound_fpfp, launch_rys_bound_dfdf, launch_rys_bound_fdfd, launch_rys_bound_ffff

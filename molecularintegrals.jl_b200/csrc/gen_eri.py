@@ -37,8 +37,12 @@ def _load_gen_rys():
 
 
 gen_rys = _load_gen_rys()
-LMAX = 2            # shell angular momentum supported by the generated kernels
+LMAX = 3            # shell angular momentum of the classes considered
+LMAX_ALL_HGP = 2    # every class pair of shells up to d has an HGP kernel
 LTAB = 2 * LMAX     # AO tables must reach la + lb
+# Class pairs with an f shell get an HGP kernel when their VRR has at most this many entries
+# (the low-L partners of f, e.g. (fs|ss), (fp|ps)); the rest run only the Rys kernels.
+HGP_MAX_VRR = 500
 # Classes whose VRR has fewer entries than this get no FP32 variant: their primitive
 # quartet is dominated by the FP64 prefactors and Boys function, so an FP32 VRR would only
 # add registers and divergence.  MIXED plans run them in FP64.
@@ -114,11 +118,16 @@ def pair_classes(lmax=LMAX):
 
 
 def class_pairs(lmax=LMAX):
+    """Class pairs (X|Y), X at or above Y, that get an HGP kernel."""
     cls = pair_classes(lmax)
     out = []
     for i, X in enumerate(cls):
         for j in range(i + 1):
-            out.append((X, cls[j]))
+            Y = cls[j]
+            if max(X + Y) > LMAX_ALL_HGP and \
+                    len(vrr_entries(X[0], X[0] + X[1], Y[0], Y[0] + Y[1])) > HGP_MAX_VRR:
+                continue
+            out.append((X, Y))
     return out
 
 
@@ -497,7 +506,7 @@ def emit_dispatch(pairs):
     lines.append("typedef void (*RysBoundLauncher)(const PairTab &, const RysTab &, int, int, "
                  "double2 *, double *, int, cudaStream_t);")
     lines.append(f"constexpr int kLmax = {gen_rys.LMAX};      // shells up to f (Rys)")
-    lines.append(f"constexpr int kLmaxHgp = {LMAX};   // HGP kernels: shells up to d")
+    lines.append(f"constexpr int kLmaxHgp = {LMAX_ALL_HGP};   // every class pair up to d has an HGP kernel")
     lines.append(f"constexpr int kNumPairClasses = {len(cls)};")
     lines.append("// pair class c = (kPairClassLa[c], kPairClassLb[c]), ordered by la+lb then la")
     lines.append("constexpr int kPairClassLa[] = {" + ", ".join(str(c[0]) for c in cls) + "};")

@@ -21,9 +21,10 @@ src/Rys.jl:27-156), reorganised for the GPU as Rys VRR + HGP HRR:
 
 A group of G threads (32, 64 or 128; a block of 128 threads holds 128/G groups) owns one
 contracted shell quartet at a time.  Stage 1 of a primitive batch: one thread per
-(primitive quartet, root, axis) builds one 2-D table into shared memory; stage 2: every
-thread accumulates its own entries of the [e0|f0] block in registers.  After the primitive
-loop the block goes to shared memory for the two HRR passes.
+(primitive quartet, root) evaluates the root and builds the three 2-D tables into shared
+memory; stage 2: every thread accumulates its own entries of the [e0|f0] block in registers
+(small blocks: NSLOT threads per entry, each over every NSLOT-th quartet of the batch).
+After the primitive loop the block goes to shared memory for the two HRR passes.
 
 The class-specific data (block entry -> table offsets, HRR term lists, norms) are emitted as
 device arrays; the kernel body is the template in rys_common.cuh.
@@ -146,11 +147,18 @@ def class_tables(X, Y):
         G = 64
     else:
         G = 128
-    npb = max(1, G // (3 * nr))
-    smem_group = 2 * NMONO + max(npb * nr * 3 * S, nblk + nab * nc)
+    # primitive quartets per batch: one stage-1 thread per (quartet, root); the batch's 2-D
+    # tables may use the HRR buffers' room (at least 6144 doubles)
+    hrr_room = max(nblk + nab * nc, 6144)
+    npb = max(1, min(G // nr, hrr_room // (3 * nr * S)))
+    # stage-2 slots: a small block is accumulated by NSLOT threads per entry, each taking every
+    # NSLOT-th quartet of a batch, and the slots are summed after the primitive loop
+    nslot = max(1, min(npb, G // nblk)) if 2 * nblk <= G else 1
+    acc = 1 if nslot > 1 else (nblk + G - 1) // G
+    smem_group = 2 * NMONO + max(npb * nr * 3 * S, nblk + nab * nc, nslot * nblk)
     return dict(la=la, lb=lb, lc=lc, ld=ld, e=e, f=f, nr=nr, rows=rows, cols=cols, S=S,
                 blk=blk, bra=bra, ket=ket, norm_ab=norm_ab, norm_cd=norm_cd, na=na, nc=nc,
-                nblk=nblk, nab=nab, ncd=ncd, G=G, npb=npb, acc=(nblk + G - 1) // G,
+                nblk=nblk, nab=nab, ncd=ncd, G=G, npb=npb, nslot=nslot, acc=acc,
                 smem_group=smem_group)
 
 
@@ -199,7 +207,7 @@ void launch_rys_bound_{tag}(const PairTab &P, const RysTab &R, int p0, int np, d
 """
     return f"""// Generated by gen_rys.py -- Rys class ({tag[0]}{tag[1]}|{tag[2]}{tag[3]}).  Do not edit.
 // roots {t['nr']}, block {t['na']} x {t['nc']}, outputs {t['nab']} x {t['ncd']}, group {t['G']} threads,
-// {t['npb']} primitive quartets per batch, {t['acc']} accumulators per thread, {smem_block} B shared per block.
+// {t['npb']} primitive quartets per batch, {t['nslot']} slot(s), {t['acc']} accumulators per thread, {smem_block} B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {{
@@ -210,7 +218,7 @@ struct C_{tag} {{
     static constexpr int NA = {t['na']}, NC = {t['nc']}, NBLK = {t['nblk']};
     static constexpr int NB = {ncart(t['lb'])}, ND = {ncart(t['ld'])};
     static constexpr int NAB = {t['nab']}, NCD = {t['ncd']};
-    static constexpr int G = {t['G']}, NPB = {t['npb']}, ACC = {t['acc']};
+    static constexpr int G = {t['G']}, NPB = {t['npb']}, NSLOT = {t['nslot']}, ACC = {t['acc']};
     static constexpr int S = {t['S']};
     static constexpr int SMEM_GROUP = {t['smem_group']};
 }};

@@ -1,0 +1,1470 @@
+// Generated by gen_eri.py -- class (fp|ds).  Do not edit.
+// VRR entries: 458, contracted block: 150, HRR lines: 180, outputs: 180.
+#include "../eri_common.cuh"
+
+namespace molints {
+
+// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[180]
+// (ma, mb, mc, md row-major), summed over the bra primitive pairs [i0, i1) and the ket
+// primitive pairs [j0, j1) of the two shell pairs.  VT is the VRR arithmetic type (double,
+// or float for MIXED).  The ket loop is outside: a warp shares its bra pair, so the inner
+// bra loads are warp-uniform broadcasts and each lane's ket record is loaded once.
+template <typename VT>
+__device__ __forceinline__ void quartet_fpds(const PairTab &P, const BoysTab &B, int p, int q,
+                                              int i0, int i1, int j0, int j1,
+                                              double *__restrict__ res,
+                                              double *__restrict__ acc_out = nullptr) {
+    const int4 ib_ = __ldg(&P.info[p]);
+    const int4 ik_ = __ldg(&P.info[q]);
+    double acc[150];
+#pragma unroll
+    for (int x = 0; x < 150; ++x) acc[x] = 0.0;
+    for (int j = j0; j < j1; ++j) {
+        const PrimPair ket = load_pp(P.pp, ik_.x + j);
+        for (int i = i0; i < i1; ++i) {
+            const PrimPair bra = load_pp(P.pp, ib_.x + i);
+            const double r = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = r * r;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double T = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = bra.kab * ket.kab * r;
+            double F[7];
+            boys_fm<6>(T, B, F);
+            const VT PAx = (VT)bra.pax, PAy = (VT)bra.pay, PAz = (VT)bra.paz;
+            const VT QCx = (VT)ket.pax, QCy = (VT)ket.pay, QCz = (VT)ket.paz;
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const VT WPx = (VT)(-ez * PQx), WPy = (VT)(-ez * PQy), WPz = (VT)(-ez * PQz);
+            const VT WQx = (VT)(zz * PQx), WQy = (VT)(zz * PQy), WQz = (VT)(zz * PQz);
+            const VT oo2z = (VT)bra.oo2z, oo2e = (VT)ket.oo2z, oo2ze = (VT)(0.5 * r2);
+            const VT rho_z = (VT)ez, rho_e = (VT)zz;
+            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz;
+            (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;
+            (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;
+            const VT v0_0_0 = (VT)(pref * F[0]);
+            const VT v0_0_1 = (VT)(pref * F[1]);
+            const VT v0_0_2 = (VT)(pref * F[2]);
+            const VT v0_0_3 = (VT)(pref * F[3]);
+            const VT v0_0_4 = (VT)(pref * F[4]);
+            const VT v0_0_5 = (VT)(pref * F[5]);
+            const VT v0_0_6 = (VT)(pref * F[6]);
+            const VT v1_0_0 = PAx * v0_0_0 + WPx * v0_0_1;
+            const VT v1_0_1 = PAx * v0_0_1 + WPx * v0_0_2;
+            const VT v1_0_2 = PAx * v0_0_2 + WPx * v0_0_3;
+            const VT v1_0_3 = PAx * v0_0_3 + WPx * v0_0_4;
+            const VT v1_0_4 = PAx * v0_0_4 + WPx * v0_0_5;
+            const VT v1_0_5 = PAx * v0_0_5 + WPx * v0_0_6;
+            const VT v2_0_0 = PAy * v0_0_0 + WPy * v0_0_1;
+            const VT v2_0_1 = PAy * v0_0_1 + WPy * v0_0_2;
+            const VT v2_0_2 = PAy * v0_0_2 + WPy * v0_0_3;
+            const VT v2_0_3 = PAy * v0_0_3 + WPy * v0_0_4;
+            const VT v2_0_4 = PAy * v0_0_4 + WPy * v0_0_5;
+            const VT v2_0_5 = PAy * v0_0_5 + WPy * v0_0_6;
+            const VT v3_0_0 = PAz * v0_0_0 + WPz * v0_0_1;
+            const VT v3_0_1 = PAz * v0_0_1 + WPz * v0_0_2;
+            const VT v3_0_2 = PAz * v0_0_2 + WPz * v0_0_3;
+            const VT v3_0_3 = PAz * v0_0_3 + WPz * v0_0_4;
+            const VT v3_0_4 = PAz * v0_0_4 + WPz * v0_0_5;
+            const VT v3_0_5 = PAz * v0_0_5 + WPz * v0_0_6;
+            const VT v4_0_0 = PAx * v1_0_0 + WPx * v1_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v4_0_1 = PAx * v1_0_1 + WPx * v1_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v4_0_2 = PAx * v1_0_2 + WPx * v1_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v4_0_3 = PAx * v1_0_3 + WPx * v1_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v4_0_4 = PAx * v1_0_4 + WPx * v1_0_5 + (VT)1.0 * oo2z * (v0_0_4 - rho_z * v0_0_5);
+            const VT v5_0_0 = PAx * v2_0_0 + WPx * v2_0_1;
+            const VT v5_0_1 = PAx * v2_0_1 + WPx * v2_0_2;
+            const VT v5_0_2 = PAx * v2_0_2 + WPx * v2_0_3;
+            const VT v5_0_3 = PAx * v2_0_3 + WPx * v2_0_4;
+            const VT v5_0_4 = PAx * v2_0_4 + WPx * v2_0_5;
+            const VT v6_0_0 = PAx * v3_0_0 + WPx * v3_0_1;
+            const VT v6_0_1 = PAx * v3_0_1 + WPx * v3_0_2;
+            const VT v6_0_2 = PAx * v3_0_2 + WPx * v3_0_3;
+            const VT v6_0_3 = PAx * v3_0_3 + WPx * v3_0_4;
+            const VT v6_0_4 = PAx * v3_0_4 + WPx * v3_0_5;
+            const VT v7_0_0 = PAy * v2_0_0 + WPy * v2_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v7_0_1 = PAy * v2_0_1 + WPy * v2_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v7_0_2 = PAy * v2_0_2 + WPy * v2_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v7_0_3 = PAy * v2_0_3 + WPy * v2_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v7_0_4 = PAy * v2_0_4 + WPy * v2_0_5 + (VT)1.0 * oo2z * (v0_0_4 - rho_z * v0_0_5);
+            const VT v8_0_0 = PAy * v3_0_0 + WPy * v3_0_1;
+            const VT v8_0_1 = PAy * v3_0_1 + WPy * v3_0_2;
+            const VT v8_0_2 = PAy * v3_0_2 + WPy * v3_0_3;
+            const VT v8_0_3 = PAy * v3_0_3 + WPy * v3_0_4;
+            const VT v8_0_4 = PAy * v3_0_4 + WPy * v3_0_5;
+            const VT v9_0_0 = PAz * v3_0_0 + WPz * v3_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v9_0_1 = PAz * v3_0_1 + WPz * v3_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v9_0_2 = PAz * v3_0_2 + WPz * v3_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v9_0_3 = PAz * v3_0_3 + WPz * v3_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v9_0_4 = PAz * v3_0_4 + WPz * v3_0_5 + (VT)1.0 * oo2z * (v0_0_4 - rho_z * v0_0_5);
+            const VT v10_0_0 = PAx * v4_0_0 + WPx * v4_0_1 + (VT)2.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v10_0_1 = PAx * v4_0_1 + WPx * v4_0_2 + (VT)2.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v10_0_2 = PAx * v4_0_2 + WPx * v4_0_3 + (VT)2.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v10_0_3 = PAx * v4_0_3 + WPx * v4_0_4 + (VT)2.0 * oo2z * (v1_0_3 - rho_z * v1_0_4);
+            const VT v11_0_0 = PAx * v5_0_0 + WPx * v5_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v11_0_1 = PAx * v5_0_1 + WPx * v5_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v11_0_2 = PAx * v5_0_2 + WPx * v5_0_3 + (VT)1.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v11_0_3 = PAx * v5_0_3 + WPx * v5_0_4 + (VT)1.0 * oo2z * (v2_0_3 - rho_z * v2_0_4);
+            const VT v12_0_0 = PAx * v6_0_0 + WPx * v6_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v12_0_1 = PAx * v6_0_1 + WPx * v6_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v12_0_2 = PAx * v6_0_2 + WPx * v6_0_3 + (VT)1.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v12_0_3 = PAx * v6_0_3 + WPx * v6_0_4 + (VT)1.0 * oo2z * (v3_0_3 - rho_z * v3_0_4);
+            const VT v13_0_0 = PAy * v5_0_0 + WPy * v5_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v13_0_1 = PAy * v5_0_1 + WPy * v5_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v13_0_2 = PAy * v5_0_2 + WPy * v5_0_3 + (VT)1.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v13_0_3 = PAy * v5_0_3 + WPy * v5_0_4 + (VT)1.0 * oo2z * (v1_0_3 - rho_z * v1_0_4);
+            const VT v14_0_0 = PAz * v6_0_0 + WPz * v6_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v14_0_1 = PAz * v6_0_1 + WPz * v6_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v14_0_2 = PAz * v6_0_2 + WPz * v6_0_3 + (VT)1.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v14_0_3 = PAz * v6_0_3 + WPz * v6_0_4 + (VT)1.0 * oo2z * (v1_0_3 - rho_z * v1_0_4);
+            const VT v15_0_0 = PAx * v8_0_0 + WPx * v8_0_1;
+            const VT v15_0_1 = PAx * v8_0_1 + WPx * v8_0_2;
+            const VT v15_0_2 = PAx * v8_0_2 + WPx * v8_0_3;
+            const VT v15_0_3 = PAx * v8_0_3 + WPx * v8_0_4;
+            const VT v16_0_0 = PAy * v7_0_0 + WPy * v7_0_1 + (VT)2.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v16_0_1 = PAy * v7_0_1 + WPy * v7_0_2 + (VT)2.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v16_0_2 = PAy * v7_0_2 + WPy * v7_0_3 + (VT)2.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v16_0_3 = PAy * v7_0_3 + WPy * v7_0_4 + (VT)2.0 * oo2z * (v2_0_3 - rho_z * v2_0_4);
+            const VT v17_0_0 = PAy * v8_0_0 + WPy * v8_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v17_0_1 = PAy * v8_0_1 + WPy * v8_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v17_0_2 = PAy * v8_0_2 + WPy * v8_0_3 + (VT)1.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v17_0_3 = PAy * v8_0_3 + WPy * v8_0_4 + (VT)1.0 * oo2z * (v3_0_3 - rho_z * v3_0_4);
+            const VT v18_0_0 = PAz * v8_0_0 + WPz * v8_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v18_0_1 = PAz * v8_0_1 + WPz * v8_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v18_0_2 = PAz * v8_0_2 + WPz * v8_0_3 + (VT)1.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v18_0_3 = PAz * v8_0_3 + WPz * v8_0_4 + (VT)1.0 * oo2z * (v2_0_3 - rho_z * v2_0_4);
+            const VT v19_0_0 = PAz * v9_0_0 + WPz * v9_0_1 + (VT)2.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v19_0_1 = PAz * v9_0_1 + WPz * v9_0_2 + (VT)2.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v19_0_2 = PAz * v9_0_2 + WPz * v9_0_3 + (VT)2.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v19_0_3 = PAz * v9_0_3 + WPz * v9_0_4 + (VT)2.0 * oo2z * (v3_0_3 - rho_z * v3_0_4);
+            const VT v20_0_0 = PAx * v10_0_0 + WPx * v10_0_1 + (VT)3.0 * oo2z * (v4_0_0 - rho_z * v4_0_1);
+            const VT v20_0_1 = PAx * v10_0_1 + WPx * v10_0_2 + (VT)3.0 * oo2z * (v4_0_1 - rho_z * v4_0_2);
+            const VT v20_0_2 = PAx * v10_0_2 + WPx * v10_0_3 + (VT)3.0 * oo2z * (v4_0_2 - rho_z * v4_0_3);
+            const VT v21_0_0 = PAx * v11_0_0 + WPx * v11_0_1 + (VT)2.0 * oo2z * (v5_0_0 - rho_z * v5_0_1);
+            const VT v21_0_1 = PAx * v11_0_1 + WPx * v11_0_2 + (VT)2.0 * oo2z * (v5_0_1 - rho_z * v5_0_2);
+            const VT v21_0_2 = PAx * v11_0_2 + WPx * v11_0_3 + (VT)2.0 * oo2z * (v5_0_2 - rho_z * v5_0_3);
+            const VT v22_0_0 = PAx * v12_0_0 + WPx * v12_0_1 + (VT)2.0 * oo2z * (v6_0_0 - rho_z * v6_0_1);
+            const VT v22_0_1 = PAx * v12_0_1 + WPx * v12_0_2 + (VT)2.0 * oo2z * (v6_0_1 - rho_z * v6_0_2);
+            const VT v22_0_2 = PAx * v12_0_2 + WPx * v12_0_3 + (VT)2.0 * oo2z * (v6_0_2 - rho_z * v6_0_3);
+            const VT v23_0_0 = PAx * v13_0_0 + WPx * v13_0_1 + (VT)1.0 * oo2z * (v7_0_0 - rho_z * v7_0_1);
+            const VT v23_0_1 = PAx * v13_0_1 + WPx * v13_0_2 + (VT)1.0 * oo2z * (v7_0_1 - rho_z * v7_0_2);
+            const VT v23_0_2 = PAx * v13_0_2 + WPx * v13_0_3 + (VT)1.0 * oo2z * (v7_0_2 - rho_z * v7_0_3);
+            const VT v24_0_0 = PAx * v15_0_0 + WPx * v15_0_1 + (VT)1.0 * oo2z * (v8_0_0 - rho_z * v8_0_1);
+            const VT v24_0_1 = PAx * v15_0_1 + WPx * v15_0_2 + (VT)1.0 * oo2z * (v8_0_1 - rho_z * v8_0_2);
+            const VT v24_0_2 = PAx * v15_0_2 + WPx * v15_0_3 + (VT)1.0 * oo2z * (v8_0_2 - rho_z * v8_0_3);
+            const VT v25_0_0 = PAx * v14_0_0 + WPx * v14_0_1 + (VT)1.0 * oo2z * (v9_0_0 - rho_z * v9_0_1);
+            const VT v25_0_1 = PAx * v14_0_1 + WPx * v14_0_2 + (VT)1.0 * oo2z * (v9_0_1 - rho_z * v9_0_2);
+            const VT v25_0_2 = PAx * v14_0_2 + WPx * v14_0_3 + (VT)1.0 * oo2z * (v9_0_2 - rho_z * v9_0_3);
+            const VT v26_0_0 = PAy * v13_0_0 + WPy * v13_0_1 + (VT)2.0 * oo2z * (v5_0_0 - rho_z * v5_0_1);
+            const VT v26_0_1 = PAy * v13_0_1 + WPy * v13_0_2 + (VT)2.0 * oo2z * (v5_0_1 - rho_z * v5_0_2);
+            const VT v26_0_2 = PAy * v13_0_2 + WPy * v13_0_3 + (VT)2.0 * oo2z * (v5_0_2 - rho_z * v5_0_3);
+            const VT v27_0_0 = PAy * v15_0_0 + WPy * v15_0_1 + (VT)1.0 * oo2z * (v6_0_0 - rho_z * v6_0_1);
+            const VT v27_0_1 = PAy * v15_0_1 + WPy * v15_0_2 + (VT)1.0 * oo2z * (v6_0_1 - rho_z * v6_0_2);
+            const VT v27_0_2 = PAy * v15_0_2 + WPy * v15_0_3 + (VT)1.0 * oo2z * (v6_0_2 - rho_z * v6_0_3);
+            const VT v28_0_0 = PAz * v15_0_0 + WPz * v15_0_1 + (VT)1.0 * oo2z * (v5_0_0 - rho_z * v5_0_1);
+            const VT v28_0_1 = PAz * v15_0_1 + WPz * v15_0_2 + (VT)1.0 * oo2z * (v5_0_1 - rho_z * v5_0_2);
+            const VT v28_0_2 = PAz * v15_0_2 + WPz * v15_0_3 + (VT)1.0 * oo2z * (v5_0_2 - rho_z * v5_0_3);
+            const VT v29_0_0 = PAz * v14_0_0 + WPz * v14_0_1 + (VT)2.0 * oo2z * (v6_0_0 - rho_z * v6_0_1);
+            const VT v29_0_1 = PAz * v14_0_1 + WPz * v14_0_2 + (VT)2.0 * oo2z * (v6_0_1 - rho_z * v6_0_2);
+            const VT v29_0_2 = PAz * v14_0_2 + WPz * v14_0_3 + (VT)2.0 * oo2z * (v6_0_2 - rho_z * v6_0_3);
+            const VT v30_0_0 = PAy * v16_0_0 + WPy * v16_0_1 + (VT)3.0 * oo2z * (v7_0_0 - rho_z * v7_0_1);
+            const VT v30_0_1 = PAy * v16_0_1 + WPy * v16_0_2 + (VT)3.0 * oo2z * (v7_0_1 - rho_z * v7_0_2);
+            const VT v30_0_2 = PAy * v16_0_2 + WPy * v16_0_3 + (VT)3.0 * oo2z * (v7_0_2 - rho_z * v7_0_3);
+            const VT v31_0_0 = PAy * v17_0_0 + WPy * v17_0_1 + (VT)2.0 * oo2z * (v8_0_0 - rho_z * v8_0_1);
+            const VT v31_0_1 = PAy * v17_0_1 + WPy * v17_0_2 + (VT)2.0 * oo2z * (v8_0_1 - rho_z * v8_0_2);
+            const VT v31_0_2 = PAy * v17_0_2 + WPy * v17_0_3 + (VT)2.0 * oo2z * (v8_0_2 - rho_z * v8_0_3);
+            const VT v32_0_0 = PAy * v18_0_0 + WPy * v18_0_1 + (VT)1.0 * oo2z * (v9_0_0 - rho_z * v9_0_1);
+            const VT v32_0_1 = PAy * v18_0_1 + WPy * v18_0_2 + (VT)1.0 * oo2z * (v9_0_1 - rho_z * v9_0_2);
+            const VT v32_0_2 = PAy * v18_0_2 + WPy * v18_0_3 + (VT)1.0 * oo2z * (v9_0_2 - rho_z * v9_0_3);
+            const VT v33_0_0 = PAz * v18_0_0 + WPz * v18_0_1 + (VT)2.0 * oo2z * (v8_0_0 - rho_z * v8_0_1);
+            const VT v33_0_1 = PAz * v18_0_1 + WPz * v18_0_2 + (VT)2.0 * oo2z * (v8_0_1 - rho_z * v8_0_2);
+            const VT v33_0_2 = PAz * v18_0_2 + WPz * v18_0_3 + (VT)2.0 * oo2z * (v8_0_2 - rho_z * v8_0_3);
+            const VT v34_0_0 = PAz * v19_0_0 + WPz * v19_0_1 + (VT)3.0 * oo2z * (v9_0_0 - rho_z * v9_0_1);
+            const VT v34_0_1 = PAz * v19_0_1 + WPz * v19_0_2 + (VT)3.0 * oo2z * (v9_0_1 - rho_z * v9_0_2);
+            const VT v34_0_2 = PAz * v19_0_2 + WPz * v19_0_3 + (VT)3.0 * oo2z * (v9_0_2 - rho_z * v9_0_3);
+            const VT v4_1_1 = QCx * v4_0_1 + WQx * v4_0_2 + (VT)2.0 * oo2ze * v1_0_2;
+            const VT v5_1_1 = QCx * v5_0_1 + WQx * v5_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v6_1_1 = QCx * v6_0_1 + WQx * v6_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v7_1_1 = QCx * v7_0_1 + WQx * v7_0_2;
+            const VT v8_1_1 = QCx * v8_0_1 + WQx * v8_0_2;
+            const VT v9_1_1 = QCx * v9_0_1 + WQx * v9_0_2;
+            const VT v10_1_0 = QCx * v10_0_0 + WQx * v10_0_1 + (VT)3.0 * oo2ze * v4_0_1;
+            const VT v10_1_1 = QCx * v10_0_1 + WQx * v10_0_2 + (VT)3.0 * oo2ze * v4_0_2;
+            const VT v11_1_0 = QCx * v11_0_0 + WQx * v11_0_1 + (VT)2.0 * oo2ze * v5_0_1;
+            const VT v11_1_1 = QCx * v11_0_1 + WQx * v11_0_2 + (VT)2.0 * oo2ze * v5_0_2;
+            const VT v12_1_0 = QCx * v12_0_0 + WQx * v12_0_1 + (VT)2.0 * oo2ze * v6_0_1;
+            const VT v12_1_1 = QCx * v12_0_1 + WQx * v12_0_2 + (VT)2.0 * oo2ze * v6_0_2;
+            const VT v13_1_0 = QCx * v13_0_0 + WQx * v13_0_1 + (VT)1.0 * oo2ze * v7_0_1;
+            const VT v13_1_1 = QCx * v13_0_1 + WQx * v13_0_2 + (VT)1.0 * oo2ze * v7_0_2;
+            const VT v14_1_0 = QCx * v14_0_0 + WQx * v14_0_1 + (VT)1.0 * oo2ze * v9_0_1;
+            const VT v14_1_1 = QCx * v14_0_1 + WQx * v14_0_2 + (VT)1.0 * oo2ze * v9_0_2;
+            const VT v15_1_0 = QCx * v15_0_0 + WQx * v15_0_1 + (VT)1.0 * oo2ze * v8_0_1;
+            const VT v15_1_1 = QCx * v15_0_1 + WQx * v15_0_2 + (VT)1.0 * oo2ze * v8_0_2;
+            const VT v16_1_0 = QCx * v16_0_0 + WQx * v16_0_1;
+            const VT v16_1_1 = QCx * v16_0_1 + WQx * v16_0_2;
+            const VT v17_1_0 = QCx * v17_0_0 + WQx * v17_0_1;
+            const VT v17_1_1 = QCx * v17_0_1 + WQx * v17_0_2;
+            const VT v18_1_0 = QCx * v18_0_0 + WQx * v18_0_1;
+            const VT v18_1_1 = QCx * v18_0_1 + WQx * v18_0_2;
+            const VT v19_1_0 = QCx * v19_0_0 + WQx * v19_0_1;
+            const VT v19_1_1 = QCx * v19_0_1 + WQx * v19_0_2;
+            const VT v20_1_0 = QCx * v20_0_0 + WQx * v20_0_1 + (VT)4.0 * oo2ze * v10_0_1;
+            const VT v20_1_1 = QCx * v20_0_1 + WQx * v20_0_2 + (VT)4.0 * oo2ze * v10_0_2;
+            const VT v21_1_0 = QCx * v21_0_0 + WQx * v21_0_1 + (VT)3.0 * oo2ze * v11_0_1;
+            const VT v21_1_1 = QCx * v21_0_1 + WQx * v21_0_2 + (VT)3.0 * oo2ze * v11_0_2;
+            const VT v22_1_0 = QCx * v22_0_0 + WQx * v22_0_1 + (VT)3.0 * oo2ze * v12_0_1;
+            const VT v22_1_1 = QCx * v22_0_1 + WQx * v22_0_2 + (VT)3.0 * oo2ze * v12_0_2;
+            const VT v23_1_0 = QCx * v23_0_0 + WQx * v23_0_1 + (VT)2.0 * oo2ze * v13_0_1;
+            const VT v23_1_1 = QCx * v23_0_1 + WQx * v23_0_2 + (VT)2.0 * oo2ze * v13_0_2;
+            const VT v24_1_0 = QCx * v24_0_0 + WQx * v24_0_1 + (VT)2.0 * oo2ze * v15_0_1;
+            const VT v24_1_1 = QCx * v24_0_1 + WQx * v24_0_2 + (VT)2.0 * oo2ze * v15_0_2;
+            const VT v25_1_0 = QCx * v25_0_0 + WQx * v25_0_1 + (VT)2.0 * oo2ze * v14_0_1;
+            const VT v25_1_1 = QCx * v25_0_1 + WQx * v25_0_2 + (VT)2.0 * oo2ze * v14_0_2;
+            const VT v26_1_0 = QCx * v26_0_0 + WQx * v26_0_1 + (VT)1.0 * oo2ze * v16_0_1;
+            const VT v26_1_1 = QCx * v26_0_1 + WQx * v26_0_2 + (VT)1.0 * oo2ze * v16_0_2;
+            const VT v27_1_0 = QCx * v27_0_0 + WQx * v27_0_1 + (VT)1.0 * oo2ze * v17_0_1;
+            const VT v27_1_1 = QCx * v27_0_1 + WQx * v27_0_2 + (VT)1.0 * oo2ze * v17_0_2;
+            const VT v28_1_0 = QCx * v28_0_0 + WQx * v28_0_1 + (VT)1.0 * oo2ze * v18_0_1;
+            const VT v28_1_1 = QCx * v28_0_1 + WQx * v28_0_2 + (VT)1.0 * oo2ze * v18_0_2;
+            const VT v29_1_0 = QCx * v29_0_0 + WQx * v29_0_1 + (VT)1.0 * oo2ze * v19_0_1;
+            const VT v29_1_1 = QCx * v29_0_1 + WQx * v29_0_2 + (VT)1.0 * oo2ze * v19_0_2;
+            const VT v30_1_0 = QCx * v30_0_0 + WQx * v30_0_1;
+            const VT v30_1_1 = QCx * v30_0_1 + WQx * v30_0_2;
+            const VT v31_1_0 = QCx * v31_0_0 + WQx * v31_0_1;
+            const VT v31_1_1 = QCx * v31_0_1 + WQx * v31_0_2;
+            const VT v32_1_0 = QCx * v32_0_0 + WQx * v32_0_1;
+            const VT v32_1_1 = QCx * v32_0_1 + WQx * v32_0_2;
+            const VT v33_1_0 = QCx * v33_0_0 + WQx * v33_0_1;
+            const VT v33_1_1 = QCx * v33_0_1 + WQx * v33_0_2;
+            const VT v34_1_0 = QCx * v34_0_0 + WQx * v34_0_1;
+            const VT v34_1_1 = QCx * v34_0_1 + WQx * v34_0_2;
+            const VT v4_2_1 = QCy * v4_0_1 + WQy * v4_0_2;
+            const VT v5_2_1 = QCy * v5_0_1 + WQy * v5_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v6_2_1 = QCy * v6_0_1 + WQy * v6_0_2;
+            const VT v7_2_1 = QCy * v7_0_1 + WQy * v7_0_2 + (VT)2.0 * oo2ze * v2_0_2;
+            const VT v8_2_1 = QCy * v8_0_1 + WQy * v8_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v9_2_1 = QCy * v9_0_1 + WQy * v9_0_2;
+            const VT v10_2_0 = QCy * v10_0_0 + WQy * v10_0_1;
+            const VT v10_2_1 = QCy * v10_0_1 + WQy * v10_0_2;
+            const VT v11_2_0 = QCy * v11_0_0 + WQy * v11_0_1 + (VT)1.0 * oo2ze * v4_0_1;
+            const VT v11_2_1 = QCy * v11_0_1 + WQy * v11_0_2 + (VT)1.0 * oo2ze * v4_0_2;
+            const VT v12_2_0 = QCy * v12_0_0 + WQy * v12_0_1;
+            const VT v12_2_1 = QCy * v12_0_1 + WQy * v12_0_2;
+            const VT v13_2_0 = QCy * v13_0_0 + WQy * v13_0_1 + (VT)2.0 * oo2ze * v5_0_1;
+            const VT v13_2_1 = QCy * v13_0_1 + WQy * v13_0_2 + (VT)2.0 * oo2ze * v5_0_2;
+            const VT v14_2_0 = QCy * v14_0_0 + WQy * v14_0_1;
+            const VT v14_2_1 = QCy * v14_0_1 + WQy * v14_0_2;
+            const VT v15_2_0 = QCy * v15_0_0 + WQy * v15_0_1 + (VT)1.0 * oo2ze * v6_0_1;
+            const VT v15_2_1 = QCy * v15_0_1 + WQy * v15_0_2 + (VT)1.0 * oo2ze * v6_0_2;
+            const VT v16_2_0 = QCy * v16_0_0 + WQy * v16_0_1 + (VT)3.0 * oo2ze * v7_0_1;
+            const VT v16_2_1 = QCy * v16_0_1 + WQy * v16_0_2 + (VT)3.0 * oo2ze * v7_0_2;
+            const VT v17_2_0 = QCy * v17_0_0 + WQy * v17_0_1 + (VT)2.0 * oo2ze * v8_0_1;
+            const VT v17_2_1 = QCy * v17_0_1 + WQy * v17_0_2 + (VT)2.0 * oo2ze * v8_0_2;
+            const VT v18_2_0 = QCy * v18_0_0 + WQy * v18_0_1 + (VT)1.0 * oo2ze * v9_0_1;
+            const VT v18_2_1 = QCy * v18_0_1 + WQy * v18_0_2 + (VT)1.0 * oo2ze * v9_0_2;
+            const VT v19_2_0 = QCy * v19_0_0 + WQy * v19_0_1;
+            const VT v19_2_1 = QCy * v19_0_1 + WQy * v19_0_2;
+            const VT v20_2_0 = QCy * v20_0_0 + WQy * v20_0_1;
+            const VT v20_2_1 = QCy * v20_0_1 + WQy * v20_0_2;
+            const VT v21_2_0 = QCy * v21_0_0 + WQy * v21_0_1 + (VT)1.0 * oo2ze * v10_0_1;
+            const VT v21_2_1 = QCy * v21_0_1 + WQy * v21_0_2 + (VT)1.0 * oo2ze * v10_0_2;
+            const VT v22_2_0 = QCy * v22_0_0 + WQy * v22_0_1;
+            const VT v22_2_1 = QCy * v22_0_1 + WQy * v22_0_2;
+            const VT v23_2_0 = QCy * v23_0_0 + WQy * v23_0_1 + (VT)2.0 * oo2ze * v11_0_1;
+            const VT v23_2_1 = QCy * v23_0_1 + WQy * v23_0_2 + (VT)2.0 * oo2ze * v11_0_2;
+            const VT v24_2_0 = QCy * v24_0_0 + WQy * v24_0_1 + (VT)1.0 * oo2ze * v12_0_1;
+            const VT v24_2_1 = QCy * v24_0_1 + WQy * v24_0_2 + (VT)1.0 * oo2ze * v12_0_2;
+            const VT v25_2_0 = QCy * v25_0_0 + WQy * v25_0_1;
+            const VT v25_2_1 = QCy * v25_0_1 + WQy * v25_0_2;
+            const VT v26_2_0 = QCy * v26_0_0 + WQy * v26_0_1 + (VT)3.0 * oo2ze * v13_0_1;
+            const VT v26_2_1 = QCy * v26_0_1 + WQy * v26_0_2 + (VT)3.0 * oo2ze * v13_0_2;
+            const VT v27_2_0 = QCy * v27_0_0 + WQy * v27_0_1 + (VT)2.0 * oo2ze * v15_0_1;
+            const VT v27_2_1 = QCy * v27_0_1 + WQy * v27_0_2 + (VT)2.0 * oo2ze * v15_0_2;
+            const VT v28_2_0 = QCy * v28_0_0 + WQy * v28_0_1 + (VT)1.0 * oo2ze * v14_0_1;
+            const VT v28_2_1 = QCy * v28_0_1 + WQy * v28_0_2 + (VT)1.0 * oo2ze * v14_0_2;
+            const VT v29_2_0 = QCy * v29_0_0 + WQy * v29_0_1;
+            const VT v29_2_1 = QCy * v29_0_1 + WQy * v29_0_2;
+            const VT v30_2_0 = QCy * v30_0_0 + WQy * v30_0_1 + (VT)4.0 * oo2ze * v16_0_1;
+            const VT v30_2_1 = QCy * v30_0_1 + WQy * v30_0_2 + (VT)4.0 * oo2ze * v16_0_2;
+            const VT v31_2_0 = QCy * v31_0_0 + WQy * v31_0_1 + (VT)3.0 * oo2ze * v17_0_1;
+            const VT v31_2_1 = QCy * v31_0_1 + WQy * v31_0_2 + (VT)3.0 * oo2ze * v17_0_2;
+            const VT v32_2_0 = QCy * v32_0_0 + WQy * v32_0_1 + (VT)2.0 * oo2ze * v18_0_1;
+            const VT v32_2_1 = QCy * v32_0_1 + WQy * v32_0_2 + (VT)2.0 * oo2ze * v18_0_2;
+            const VT v33_2_0 = QCy * v33_0_0 + WQy * v33_0_1 + (VT)1.0 * oo2ze * v19_0_1;
+            const VT v33_2_1 = QCy * v33_0_1 + WQy * v33_0_2 + (VT)1.0 * oo2ze * v19_0_2;
+            const VT v34_2_0 = QCy * v34_0_0 + WQy * v34_0_1;
+            const VT v34_2_1 = QCy * v34_0_1 + WQy * v34_0_2;
+            const VT v4_3_1 = QCz * v4_0_1 + WQz * v4_0_2;
+            const VT v5_3_1 = QCz * v5_0_1 + WQz * v5_0_2;
+            const VT v6_3_1 = QCz * v6_0_1 + WQz * v6_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v7_3_1 = QCz * v7_0_1 + WQz * v7_0_2;
+            const VT v8_3_1 = QCz * v8_0_1 + WQz * v8_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v9_3_1 = QCz * v9_0_1 + WQz * v9_0_2 + (VT)2.0 * oo2ze * v3_0_2;
+            const VT v10_3_0 = QCz * v10_0_0 + WQz * v10_0_1;
+            const VT v10_3_1 = QCz * v10_0_1 + WQz * v10_0_2;
+            const VT v11_3_0 = QCz * v11_0_0 + WQz * v11_0_1;
+            const VT v11_3_1 = QCz * v11_0_1 + WQz * v11_0_2;
+            const VT v12_3_0 = QCz * v12_0_0 + WQz * v12_0_1 + (VT)1.0 * oo2ze * v4_0_1;
+            const VT v12_3_1 = QCz * v12_0_1 + WQz * v12_0_2 + (VT)1.0 * oo2ze * v4_0_2;
+            const VT v13_3_0 = QCz * v13_0_0 + WQz * v13_0_1;
+            const VT v13_3_1 = QCz * v13_0_1 + WQz * v13_0_2;
+            const VT v14_3_0 = QCz * v14_0_0 + WQz * v14_0_1 + (VT)2.0 * oo2ze * v6_0_1;
+            const VT v14_3_1 = QCz * v14_0_1 + WQz * v14_0_2 + (VT)2.0 * oo2ze * v6_0_2;
+            const VT v15_3_0 = QCz * v15_0_0 + WQz * v15_0_1 + (VT)1.0 * oo2ze * v5_0_1;
+            const VT v15_3_1 = QCz * v15_0_1 + WQz * v15_0_2 + (VT)1.0 * oo2ze * v5_0_2;
+            const VT v16_3_0 = QCz * v16_0_0 + WQz * v16_0_1;
+            const VT v16_3_1 = QCz * v16_0_1 + WQz * v16_0_2;
+            const VT v17_3_0 = QCz * v17_0_0 + WQz * v17_0_1 + (VT)1.0 * oo2ze * v7_0_1;
+            const VT v17_3_1 = QCz * v17_0_1 + WQz * v17_0_2 + (VT)1.0 * oo2ze * v7_0_2;
+            const VT v18_3_0 = QCz * v18_0_0 + WQz * v18_0_1 + (VT)2.0 * oo2ze * v8_0_1;
+            const VT v18_3_1 = QCz * v18_0_1 + WQz * v18_0_2 + (VT)2.0 * oo2ze * v8_0_2;
+            const VT v19_3_0 = QCz * v19_0_0 + WQz * v19_0_1 + (VT)3.0 * oo2ze * v9_0_1;
+            const VT v19_3_1 = QCz * v19_0_1 + WQz * v19_0_2 + (VT)3.0 * oo2ze * v9_0_2;
+            const VT v20_3_0 = QCz * v20_0_0 + WQz * v20_0_1;
+            const VT v20_3_1 = QCz * v20_0_1 + WQz * v20_0_2;
+            const VT v21_3_0 = QCz * v21_0_0 + WQz * v21_0_1;
+            const VT v21_3_1 = QCz * v21_0_1 + WQz * v21_0_2;
+            const VT v22_3_0 = QCz * v22_0_0 + WQz * v22_0_1 + (VT)1.0 * oo2ze * v10_0_1;
+            const VT v22_3_1 = QCz * v22_0_1 + WQz * v22_0_2 + (VT)1.0 * oo2ze * v10_0_2;
+            const VT v23_3_0 = QCz * v23_0_0 + WQz * v23_0_1;
+            const VT v23_3_1 = QCz * v23_0_1 + WQz * v23_0_2;
+            const VT v24_3_0 = QCz * v24_0_0 + WQz * v24_0_1 + (VT)1.0 * oo2ze * v11_0_1;
+            const VT v24_3_1 = QCz * v24_0_1 + WQz * v24_0_2 + (VT)1.0 * oo2ze * v11_0_2;
+            const VT v25_3_0 = QCz * v25_0_0 + WQz * v25_0_1 + (VT)2.0 * oo2ze * v12_0_1;
+            const VT v25_3_1 = QCz * v25_0_1 + WQz * v25_0_2 + (VT)2.0 * oo2ze * v12_0_2;
+            const VT v26_3_0 = QCz * v26_0_0 + WQz * v26_0_1;
+            const VT v26_3_1 = QCz * v26_0_1 + WQz * v26_0_2;
+            const VT v27_3_0 = QCz * v27_0_0 + WQz * v27_0_1 + (VT)1.0 * oo2ze * v13_0_1;
+            const VT v27_3_1 = QCz * v27_0_1 + WQz * v27_0_2 + (VT)1.0 * oo2ze * v13_0_2;
+            const VT v28_3_0 = QCz * v28_0_0 + WQz * v28_0_1 + (VT)2.0 * oo2ze * v15_0_1;
+            const VT v28_3_1 = QCz * v28_0_1 + WQz * v28_0_2 + (VT)2.0 * oo2ze * v15_0_2;
+            const VT v29_3_0 = QCz * v29_0_0 + WQz * v29_0_1 + (VT)3.0 * oo2ze * v14_0_1;
+            const VT v29_3_1 = QCz * v29_0_1 + WQz * v29_0_2 + (VT)3.0 * oo2ze * v14_0_2;
+            const VT v30_3_0 = QCz * v30_0_0 + WQz * v30_0_1;
+            const VT v30_3_1 = QCz * v30_0_1 + WQz * v30_0_2;
+            const VT v31_3_0 = QCz * v31_0_0 + WQz * v31_0_1 + (VT)1.0 * oo2ze * v16_0_1;
+            const VT v31_3_1 = QCz * v31_0_1 + WQz * v31_0_2 + (VT)1.0 * oo2ze * v16_0_2;
+            const VT v32_3_0 = QCz * v32_0_0 + WQz * v32_0_1 + (VT)2.0 * oo2ze * v17_0_1;
+            const VT v32_3_1 = QCz * v32_0_1 + WQz * v32_0_2 + (VT)2.0 * oo2ze * v17_0_2;
+            const VT v33_3_0 = QCz * v33_0_0 + WQz * v33_0_1 + (VT)3.0 * oo2ze * v18_0_1;
+            const VT v33_3_1 = QCz * v33_0_1 + WQz * v33_0_2 + (VT)3.0 * oo2ze * v18_0_2;
+            const VT v34_3_0 = QCz * v34_0_0 + WQz * v34_0_1 + (VT)4.0 * oo2ze * v19_0_1;
+            const VT v34_3_1 = QCz * v34_0_1 + WQz * v34_0_2 + (VT)4.0 * oo2ze * v19_0_2;
+            const VT v10_4_0 = QCx * v10_1_0 + WQx * v10_1_1 + (VT)3.0 * oo2ze * v4_1_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v11_4_0 = QCx * v11_1_0 + WQx * v11_1_1 + (VT)2.0 * oo2ze * v5_1_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v12_4_0 = QCx * v12_1_0 + WQx * v12_1_1 + (VT)2.0 * oo2ze * v6_1_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v13_4_0 = QCx * v13_1_0 + WQx * v13_1_1 + (VT)1.0 * oo2ze * v7_1_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v14_4_0 = QCx * v14_1_0 + WQx * v14_1_1 + (VT)1.0 * oo2ze * v9_1_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v15_4_0 = QCx * v15_1_0 + WQx * v15_1_1 + (VT)1.0 * oo2ze * v8_1_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v16_4_0 = QCx * v16_1_0 + WQx * v16_1_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v17_4_0 = QCx * v17_1_0 + WQx * v17_1_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v18_4_0 = QCx * v18_1_0 + WQx * v18_1_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v19_4_0 = QCx * v19_1_0 + WQx * v19_1_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v20_4_0 = QCx * v20_1_0 + WQx * v20_1_1 + (VT)4.0 * oo2ze * v10_1_1 + (VT)1.0 * oo2e * (v20_0_0 - rho_e * v20_0_1);
+            const VT v21_4_0 = QCx * v21_1_0 + WQx * v21_1_1 + (VT)3.0 * oo2ze * v11_1_1 + (VT)1.0 * oo2e * (v21_0_0 - rho_e * v21_0_1);
+            const VT v22_4_0 = QCx * v22_1_0 + WQx * v22_1_1 + (VT)3.0 * oo2ze * v12_1_1 + (VT)1.0 * oo2e * (v22_0_0 - rho_e * v22_0_1);
+            const VT v23_4_0 = QCx * v23_1_0 + WQx * v23_1_1 + (VT)2.0 * oo2ze * v13_1_1 + (VT)1.0 * oo2e * (v23_0_0 - rho_e * v23_0_1);
+            const VT v24_4_0 = QCx * v24_1_0 + WQx * v24_1_1 + (VT)2.0 * oo2ze * v15_1_1 + (VT)1.0 * oo2e * (v24_0_0 - rho_e * v24_0_1);
+            const VT v25_4_0 = QCx * v25_1_0 + WQx * v25_1_1 + (VT)2.0 * oo2ze * v14_1_1 + (VT)1.0 * oo2e * (v25_0_0 - rho_e * v25_0_1);
+            const VT v26_4_0 = QCx * v26_1_0 + WQx * v26_1_1 + (VT)1.0 * oo2ze * v16_1_1 + (VT)1.0 * oo2e * (v26_0_0 - rho_e * v26_0_1);
+            const VT v27_4_0 = QCx * v27_1_0 + WQx * v27_1_1 + (VT)1.0 * oo2ze * v17_1_1 + (VT)1.0 * oo2e * (v27_0_0 - rho_e * v27_0_1);
+            const VT v28_4_0 = QCx * v28_1_0 + WQx * v28_1_1 + (VT)1.0 * oo2ze * v18_1_1 + (VT)1.0 * oo2e * (v28_0_0 - rho_e * v28_0_1);
+            const VT v29_4_0 = QCx * v29_1_0 + WQx * v29_1_1 + (VT)1.0 * oo2ze * v19_1_1 + (VT)1.0 * oo2e * (v29_0_0 - rho_e * v29_0_1);
+            const VT v30_4_0 = QCx * v30_1_0 + WQx * v30_1_1 + (VT)1.0 * oo2e * (v30_0_0 - rho_e * v30_0_1);
+            const VT v31_4_0 = QCx * v31_1_0 + WQx * v31_1_1 + (VT)1.0 * oo2e * (v31_0_0 - rho_e * v31_0_1);
+            const VT v32_4_0 = QCx * v32_1_0 + WQx * v32_1_1 + (VT)1.0 * oo2e * (v32_0_0 - rho_e * v32_0_1);
+            const VT v33_4_0 = QCx * v33_1_0 + WQx * v33_1_1 + (VT)1.0 * oo2e * (v33_0_0 - rho_e * v33_0_1);
+            const VT v34_4_0 = QCx * v34_1_0 + WQx * v34_1_1 + (VT)1.0 * oo2e * (v34_0_0 - rho_e * v34_0_1);
+            const VT v10_5_0 = QCx * v10_2_0 + WQx * v10_2_1 + (VT)3.0 * oo2ze * v4_2_1;
+            const VT v11_5_0 = QCx * v11_2_0 + WQx * v11_2_1 + (VT)2.0 * oo2ze * v5_2_1;
+            const VT v12_5_0 = QCx * v12_2_0 + WQx * v12_2_1 + (VT)2.0 * oo2ze * v6_2_1;
+            const VT v13_5_0 = QCx * v13_2_0 + WQx * v13_2_1 + (VT)1.0 * oo2ze * v7_2_1;
+            const VT v14_5_0 = QCx * v14_2_0 + WQx * v14_2_1 + (VT)1.0 * oo2ze * v9_2_1;
+            const VT v15_5_0 = QCx * v15_2_0 + WQx * v15_2_1 + (VT)1.0 * oo2ze * v8_2_1;
+            const VT v16_5_0 = QCx * v16_2_0 + WQx * v16_2_1;
+            const VT v17_5_0 = QCx * v17_2_0 + WQx * v17_2_1;
+            const VT v18_5_0 = QCx * v18_2_0 + WQx * v18_2_1;
+            const VT v19_5_0 = QCx * v19_2_0 + WQx * v19_2_1;
+            const VT v20_5_0 = QCx * v20_2_0 + WQx * v20_2_1 + (VT)4.0 * oo2ze * v10_2_1;
+            const VT v21_5_0 = QCx * v21_2_0 + WQx * v21_2_1 + (VT)3.0 * oo2ze * v11_2_1;
+            const VT v22_5_0 = QCx * v22_2_0 + WQx * v22_2_1 + (VT)3.0 * oo2ze * v12_2_1;
+            const VT v23_5_0 = QCx * v23_2_0 + WQx * v23_2_1 + (VT)2.0 * oo2ze * v13_2_1;
+            const VT v24_5_0 = QCx * v24_2_0 + WQx * v24_2_1 + (VT)2.0 * oo2ze * v15_2_1;
+            const VT v25_5_0 = QCx * v25_2_0 + WQx * v25_2_1 + (VT)2.0 * oo2ze * v14_2_1;
+            const VT v26_5_0 = QCx * v26_2_0 + WQx * v26_2_1 + (VT)1.0 * oo2ze * v16_2_1;
+            const VT v27_5_0 = QCx * v27_2_0 + WQx * v27_2_1 + (VT)1.0 * oo2ze * v17_2_1;
+            const VT v28_5_0 = QCx * v28_2_0 + WQx * v28_2_1 + (VT)1.0 * oo2ze * v18_2_1;
+            const VT v29_5_0 = QCx * v29_2_0 + WQx * v29_2_1 + (VT)1.0 * oo2ze * v19_2_1;
+            const VT v30_5_0 = QCx * v30_2_0 + WQx * v30_2_1;
+            const VT v31_5_0 = QCx * v31_2_0 + WQx * v31_2_1;
+            const VT v32_5_0 = QCx * v32_2_0 + WQx * v32_2_1;
+            const VT v33_5_0 = QCx * v33_2_0 + WQx * v33_2_1;
+            const VT v34_5_0 = QCx * v34_2_0 + WQx * v34_2_1;
+            const VT v10_6_0 = QCx * v10_3_0 + WQx * v10_3_1 + (VT)3.0 * oo2ze * v4_3_1;
+            const VT v11_6_0 = QCx * v11_3_0 + WQx * v11_3_1 + (VT)2.0 * oo2ze * v5_3_1;
+            const VT v12_6_0 = QCx * v12_3_0 + WQx * v12_3_1 + (VT)2.0 * oo2ze * v6_3_1;
+            const VT v13_6_0 = QCx * v13_3_0 + WQx * v13_3_1 + (VT)1.0 * oo2ze * v7_3_1;
+            const VT v14_6_0 = QCx * v14_3_0 + WQx * v14_3_1 + (VT)1.0 * oo2ze * v9_3_1;
+            const VT v15_6_0 = QCx * v15_3_0 + WQx * v15_3_1 + (VT)1.0 * oo2ze * v8_3_1;
+            const VT v16_6_0 = QCx * v16_3_0 + WQx * v16_3_1;
+            const VT v17_6_0 = QCx * v17_3_0 + WQx * v17_3_1;
+            const VT v18_6_0 = QCx * v18_3_0 + WQx * v18_3_1;
+            const VT v19_6_0 = QCx * v19_3_0 + WQx * v19_3_1;
+            const VT v20_6_0 = QCx * v20_3_0 + WQx * v20_3_1 + (VT)4.0 * oo2ze * v10_3_1;
+            const VT v21_6_0 = QCx * v21_3_0 + WQx * v21_3_1 + (VT)3.0 * oo2ze * v11_3_1;
+            const VT v22_6_0 = QCx * v22_3_0 + WQx * v22_3_1 + (VT)3.0 * oo2ze * v12_3_1;
+            const VT v23_6_0 = QCx * v23_3_0 + WQx * v23_3_1 + (VT)2.0 * oo2ze * v13_3_1;
+            const VT v24_6_0 = QCx * v24_3_0 + WQx * v24_3_1 + (VT)2.0 * oo2ze * v15_3_1;
+            const VT v25_6_0 = QCx * v25_3_0 + WQx * v25_3_1 + (VT)2.0 * oo2ze * v14_3_1;
+            const VT v26_6_0 = QCx * v26_3_0 + WQx * v26_3_1 + (VT)1.0 * oo2ze * v16_3_1;
+            const VT v27_6_0 = QCx * v27_3_0 + WQx * v27_3_1 + (VT)1.0 * oo2ze * v17_3_1;
+            const VT v28_6_0 = QCx * v28_3_0 + WQx * v28_3_1 + (VT)1.0 * oo2ze * v18_3_1;
+            const VT v29_6_0 = QCx * v29_3_0 + WQx * v29_3_1 + (VT)1.0 * oo2ze * v19_3_1;
+            const VT v30_6_0 = QCx * v30_3_0 + WQx * v30_3_1;
+            const VT v31_6_0 = QCx * v31_3_0 + WQx * v31_3_1;
+            const VT v32_6_0 = QCx * v32_3_0 + WQx * v32_3_1;
+            const VT v33_6_0 = QCx * v33_3_0 + WQx * v33_3_1;
+            const VT v34_6_0 = QCx * v34_3_0 + WQx * v34_3_1;
+            const VT v10_7_0 = QCy * v10_2_0 + WQy * v10_2_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v11_7_0 = QCy * v11_2_0 + WQy * v11_2_1 + (VT)1.0 * oo2ze * v4_2_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v12_7_0 = QCy * v12_2_0 + WQy * v12_2_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v13_7_0 = QCy * v13_2_0 + WQy * v13_2_1 + (VT)2.0 * oo2ze * v5_2_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v14_7_0 = QCy * v14_2_0 + WQy * v14_2_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v15_7_0 = QCy * v15_2_0 + WQy * v15_2_1 + (VT)1.0 * oo2ze * v6_2_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v16_7_0 = QCy * v16_2_0 + WQy * v16_2_1 + (VT)3.0 * oo2ze * v7_2_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v17_7_0 = QCy * v17_2_0 + WQy * v17_2_1 + (VT)2.0 * oo2ze * v8_2_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v18_7_0 = QCy * v18_2_0 + WQy * v18_2_1 + (VT)1.0 * oo2ze * v9_2_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v19_7_0 = QCy * v19_2_0 + WQy * v19_2_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v20_7_0 = QCy * v20_2_0 + WQy * v20_2_1 + (VT)1.0 * oo2e * (v20_0_0 - rho_e * v20_0_1);
+            const VT v21_7_0 = QCy * v21_2_0 + WQy * v21_2_1 + (VT)1.0 * oo2ze * v10_2_1 + (VT)1.0 * oo2e * (v21_0_0 - rho_e * v21_0_1);
+            const VT v22_7_0 = QCy * v22_2_0 + WQy * v22_2_1 + (VT)1.0 * oo2e * (v22_0_0 - rho_e * v22_0_1);
+            const VT v23_7_0 = QCy * v23_2_0 + WQy * v23_2_1 + (VT)2.0 * oo2ze * v11_2_1 + (VT)1.0 * oo2e * (v23_0_0 - rho_e * v23_0_1);
+            const VT v24_7_0 = QCy * v24_2_0 + WQy * v24_2_1 + (VT)1.0 * oo2ze * v12_2_1 + (VT)1.0 * oo2e * (v24_0_0 - rho_e * v24_0_1);
+            const VT v25_7_0 = QCy * v25_2_0 + WQy * v25_2_1 + (VT)1.0 * oo2e * (v25_0_0 - rho_e * v25_0_1);
+            const VT v26_7_0 = QCy * v26_2_0 + WQy * v26_2_1 + (VT)3.0 * oo2ze * v13_2_1 + (VT)1.0 * oo2e * (v26_0_0 - rho_e * v26_0_1);
+            const VT v27_7_0 = QCy * v27_2_0 + WQy * v27_2_1 + (VT)2.0 * oo2ze * v15_2_1 + (VT)1.0 * oo2e * (v27_0_0 - rho_e * v27_0_1);
+            const VT v28_7_0 = QCy * v28_2_0 + WQy * v28_2_1 + (VT)1.0 * oo2ze * v14_2_1 + (VT)1.0 * oo2e * (v28_0_0 - rho_e * v28_0_1);
+            const VT v29_7_0 = QCy * v29_2_0 + WQy * v29_2_1 + (VT)1.0 * oo2e * (v29_0_0 - rho_e * v29_0_1);
+            const VT v30_7_0 = QCy * v30_2_0 + WQy * v30_2_1 + (VT)4.0 * oo2ze * v16_2_1 + (VT)1.0 * oo2e * (v30_0_0 - rho_e * v30_0_1);
+            const VT v31_7_0 = QCy * v31_2_0 + WQy * v31_2_1 + (VT)3.0 * oo2ze * v17_2_1 + (VT)1.0 * oo2e * (v31_0_0 - rho_e * v31_0_1);
+            const VT v32_7_0 = QCy * v32_2_0 + WQy * v32_2_1 + (VT)2.0 * oo2ze * v18_2_1 + (VT)1.0 * oo2e * (v32_0_0 - rho_e * v32_0_1);
+            const VT v33_7_0 = QCy * v33_2_0 + WQy * v33_2_1 + (VT)1.0 * oo2ze * v19_2_1 + (VT)1.0 * oo2e * (v33_0_0 - rho_e * v33_0_1);
+            const VT v34_7_0 = QCy * v34_2_0 + WQy * v34_2_1 + (VT)1.0 * oo2e * (v34_0_0 - rho_e * v34_0_1);
+            const VT v10_8_0 = QCy * v10_3_0 + WQy * v10_3_1;
+            const VT v11_8_0 = QCy * v11_3_0 + WQy * v11_3_1 + (VT)1.0 * oo2ze * v4_3_1;
+            const VT v12_8_0 = QCy * v12_3_0 + WQy * v12_3_1;
+            const VT v13_8_0 = QCy * v13_3_0 + WQy * v13_3_1 + (VT)2.0 * oo2ze * v5_3_1;
+            const VT v14_8_0 = QCy * v14_3_0 + WQy * v14_3_1;
+            const VT v15_8_0 = QCy * v15_3_0 + WQy * v15_3_1 + (VT)1.0 * oo2ze * v6_3_1;
+            const VT v16_8_0 = QCy * v16_3_0 + WQy * v16_3_1 + (VT)3.0 * oo2ze * v7_3_1;
+            const VT v17_8_0 = QCy * v17_3_0 + WQy * v17_3_1 + (VT)2.0 * oo2ze * v8_3_1;
+            const VT v18_8_0 = QCy * v18_3_0 + WQy * v18_3_1 + (VT)1.0 * oo2ze * v9_3_1;
+            const VT v19_8_0 = QCy * v19_3_0 + WQy * v19_3_1;
+            const VT v20_8_0 = QCy * v20_3_0 + WQy * v20_3_1;
+            const VT v21_8_0 = QCy * v21_3_0 + WQy * v21_3_1 + (VT)1.0 * oo2ze * v10_3_1;
+            const VT v22_8_0 = QCy * v22_3_0 + WQy * v22_3_1;
+            const VT v23_8_0 = QCy * v23_3_0 + WQy * v23_3_1 + (VT)2.0 * oo2ze * v11_3_1;
+            const VT v24_8_0 = QCy * v24_3_0 + WQy * v24_3_1 + (VT)1.0 * oo2ze * v12_3_1;
+            const VT v25_8_0 = QCy * v25_3_0 + WQy * v25_3_1;
+            const VT v26_8_0 = QCy * v26_3_0 + WQy * v26_3_1 + (VT)3.0 * oo2ze * v13_3_1;
+            const VT v27_8_0 = QCy * v27_3_0 + WQy * v27_3_1 + (VT)2.0 * oo2ze * v15_3_1;
+            const VT v28_8_0 = QCy * v28_3_0 + WQy * v28_3_1 + (VT)1.0 * oo2ze * v14_3_1;
+            const VT v29_8_0 = QCy * v29_3_0 + WQy * v29_3_1;
+            const VT v30_8_0 = QCy * v30_3_0 + WQy * v30_3_1 + (VT)4.0 * oo2ze * v16_3_1;
+            const VT v31_8_0 = QCy * v31_3_0 + WQy * v31_3_1 + (VT)3.0 * oo2ze * v17_3_1;
+            const VT v32_8_0 = QCy * v32_3_0 + WQy * v32_3_1 + (VT)2.0 * oo2ze * v18_3_1;
+            const VT v33_8_0 = QCy * v33_3_0 + WQy * v33_3_1 + (VT)1.0 * oo2ze * v19_3_1;
+            const VT v34_8_0 = QCy * v34_3_0 + WQy * v34_3_1;
+            const VT v10_9_0 = QCz * v10_3_0 + WQz * v10_3_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v11_9_0 = QCz * v11_3_0 + WQz * v11_3_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v12_9_0 = QCz * v12_3_0 + WQz * v12_3_1 + (VT)1.0 * oo2ze * v4_3_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v13_9_0 = QCz * v13_3_0 + WQz * v13_3_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v14_9_0 = QCz * v14_3_0 + WQz * v14_3_1 + (VT)2.0 * oo2ze * v6_3_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v15_9_0 = QCz * v15_3_0 + WQz * v15_3_1 + (VT)1.0 * oo2ze * v5_3_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v16_9_0 = QCz * v16_3_0 + WQz * v16_3_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v17_9_0 = QCz * v17_3_0 + WQz * v17_3_1 + (VT)1.0 * oo2ze * v7_3_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v18_9_0 = QCz * v18_3_0 + WQz * v18_3_1 + (VT)2.0 * oo2ze * v8_3_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v19_9_0 = QCz * v19_3_0 + WQz * v19_3_1 + (VT)3.0 * oo2ze * v9_3_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v20_9_0 = QCz * v20_3_0 + WQz * v20_3_1 + (VT)1.0 * oo2e * (v20_0_0 - rho_e * v20_0_1);
+            const VT v21_9_0 = QCz * v21_3_0 + WQz * v21_3_1 + (VT)1.0 * oo2e * (v21_0_0 - rho_e * v21_0_1);
+            const VT v22_9_0 = QCz * v22_3_0 + WQz * v22_3_1 + (VT)1.0 * oo2ze * v10_3_1 + (VT)1.0 * oo2e * (v22_0_0 - rho_e * v22_0_1);
+            const VT v23_9_0 = QCz * v23_3_0 + WQz * v23_3_1 + (VT)1.0 * oo2e * (v23_0_0 - rho_e * v23_0_1);
+            const VT v24_9_0 = QCz * v24_3_0 + WQz * v24_3_1 + (VT)1.0 * oo2ze * v11_3_1 + (VT)1.0 * oo2e * (v24_0_0 - rho_e * v24_0_1);
+            const VT v25_9_0 = QCz * v25_3_0 + WQz * v25_3_1 + (VT)2.0 * oo2ze * v12_3_1 + (VT)1.0 * oo2e * (v25_0_0 - rho_e * v25_0_1);
+            const VT v26_9_0 = QCz * v26_3_0 + WQz * v26_3_1 + (VT)1.0 * oo2e * (v26_0_0 - rho_e * v26_0_1);
+            const VT v27_9_0 = QCz * v27_3_0 + WQz * v27_3_1 + (VT)1.0 * oo2ze * v13_3_1 + (VT)1.0 * oo2e * (v27_0_0 - rho_e * v27_0_1);
+            const VT v28_9_0 = QCz * v28_3_0 + WQz * v28_3_1 + (VT)2.0 * oo2ze * v15_3_1 + (VT)1.0 * oo2e * (v28_0_0 - rho_e * v28_0_1);
+            const VT v29_9_0 = QCz * v29_3_0 + WQz * v29_3_1 + (VT)3.0 * oo2ze * v14_3_1 + (VT)1.0 * oo2e * (v29_0_0 - rho_e * v29_0_1);
+            const VT v30_9_0 = QCz * v30_3_0 + WQz * v30_3_1 + (VT)1.0 * oo2e * (v30_0_0 - rho_e * v30_0_1);
+            const VT v31_9_0 = QCz * v31_3_0 + WQz * v31_3_1 + (VT)1.0 * oo2ze * v16_3_1 + (VT)1.0 * oo2e * (v31_0_0 - rho_e * v31_0_1);
+            const VT v32_9_0 = QCz * v32_3_0 + WQz * v32_3_1 + (VT)2.0 * oo2ze * v17_3_1 + (VT)1.0 * oo2e * (v32_0_0 - rho_e * v32_0_1);
+            const VT v33_9_0 = QCz * v33_3_0 + WQz * v33_3_1 + (VT)3.0 * oo2ze * v18_3_1 + (VT)1.0 * oo2e * (v33_0_0 - rho_e * v33_0_1);
+            const VT v34_9_0 = QCz * v34_3_0 + WQz * v34_3_1 + (VT)4.0 * oo2ze * v19_3_1 + (VT)1.0 * oo2e * (v34_0_0 - rho_e * v34_0_1);
+            acc[0] += (double)v10_4_0;
+            acc[1] += (double)v10_5_0;
+            acc[2] += (double)v10_6_0;
+            acc[3] += (double)v10_7_0;
+            acc[4] += (double)v10_8_0;
+            acc[5] += (double)v10_9_0;
+            acc[6] += (double)v11_4_0;
+            acc[7] += (double)v11_5_0;
+            acc[8] += (double)v11_6_0;
+            acc[9] += (double)v11_7_0;
+            acc[10] += (double)v11_8_0;
+            acc[11] += (double)v11_9_0;
+            acc[12] += (double)v12_4_0;
+            acc[13] += (double)v12_5_0;
+            acc[14] += (double)v12_6_0;
+            acc[15] += (double)v12_7_0;
+            acc[16] += (double)v12_8_0;
+            acc[17] += (double)v12_9_0;
+            acc[18] += (double)v13_4_0;
+            acc[19] += (double)v13_5_0;
+            acc[20] += (double)v13_6_0;
+            acc[21] += (double)v13_7_0;
+            acc[22] += (double)v13_8_0;
+            acc[23] += (double)v13_9_0;
+            acc[24] += (double)v14_4_0;
+            acc[25] += (double)v14_5_0;
+            acc[26] += (double)v14_6_0;
+            acc[27] += (double)v14_7_0;
+            acc[28] += (double)v14_8_0;
+            acc[29] += (double)v14_9_0;
+            acc[30] += (double)v15_4_0;
+            acc[31] += (double)v15_5_0;
+            acc[32] += (double)v15_6_0;
+            acc[33] += (double)v15_7_0;
+            acc[34] += (double)v15_8_0;
+            acc[35] += (double)v15_9_0;
+            acc[36] += (double)v16_4_0;
+            acc[37] += (double)v16_5_0;
+            acc[38] += (double)v16_6_0;
+            acc[39] += (double)v16_7_0;
+            acc[40] += (double)v16_8_0;
+            acc[41] += (double)v16_9_0;
+            acc[42] += (double)v17_4_0;
+            acc[43] += (double)v17_5_0;
+            acc[44] += (double)v17_6_0;
+            acc[45] += (double)v17_7_0;
+            acc[46] += (double)v17_8_0;
+            acc[47] += (double)v17_9_0;
+            acc[48] += (double)v18_4_0;
+            acc[49] += (double)v18_5_0;
+            acc[50] += (double)v18_6_0;
+            acc[51] += (double)v18_7_0;
+            acc[52] += (double)v18_8_0;
+            acc[53] += (double)v18_9_0;
+            acc[54] += (double)v19_4_0;
+            acc[55] += (double)v19_5_0;
+            acc[56] += (double)v19_6_0;
+            acc[57] += (double)v19_7_0;
+            acc[58] += (double)v19_8_0;
+            acc[59] += (double)v19_9_0;
+            acc[60] += (double)v20_4_0;
+            acc[61] += (double)v20_5_0;
+            acc[62] += (double)v20_6_0;
+            acc[63] += (double)v20_7_0;
+            acc[64] += (double)v20_8_0;
+            acc[65] += (double)v20_9_0;
+            acc[66] += (double)v21_4_0;
+            acc[67] += (double)v21_5_0;
+            acc[68] += (double)v21_6_0;
+            acc[69] += (double)v21_7_0;
+            acc[70] += (double)v21_8_0;
+            acc[71] += (double)v21_9_0;
+            acc[72] += (double)v22_4_0;
+            acc[73] += (double)v22_5_0;
+            acc[74] += (double)v22_6_0;
+            acc[75] += (double)v22_7_0;
+            acc[76] += (double)v22_8_0;
+            acc[77] += (double)v22_9_0;
+            acc[78] += (double)v23_4_0;
+            acc[79] += (double)v23_5_0;
+            acc[80] += (double)v23_6_0;
+            acc[81] += (double)v23_7_0;
+            acc[82] += (double)v23_8_0;
+            acc[83] += (double)v23_9_0;
+            acc[84] += (double)v24_4_0;
+            acc[85] += (double)v24_5_0;
+            acc[86] += (double)v24_6_0;
+            acc[87] += (double)v24_7_0;
+            acc[88] += (double)v24_8_0;
+            acc[89] += (double)v24_9_0;
+            acc[90] += (double)v25_4_0;
+            acc[91] += (double)v25_5_0;
+            acc[92] += (double)v25_6_0;
+            acc[93] += (double)v25_7_0;
+            acc[94] += (double)v25_8_0;
+            acc[95] += (double)v25_9_0;
+            acc[96] += (double)v26_4_0;
+            acc[97] += (double)v26_5_0;
+            acc[98] += (double)v26_6_0;
+            acc[99] += (double)v26_7_0;
+            acc[100] += (double)v26_8_0;
+            acc[101] += (double)v26_9_0;
+            acc[102] += (double)v27_4_0;
+            acc[103] += (double)v27_5_0;
+            acc[104] += (double)v27_6_0;
+            acc[105] += (double)v27_7_0;
+            acc[106] += (double)v27_8_0;
+            acc[107] += (double)v27_9_0;
+            acc[108] += (double)v28_4_0;
+            acc[109] += (double)v28_5_0;
+            acc[110] += (double)v28_6_0;
+            acc[111] += (double)v28_7_0;
+            acc[112] += (double)v28_8_0;
+            acc[113] += (double)v28_9_0;
+            acc[114] += (double)v29_4_0;
+            acc[115] += (double)v29_5_0;
+            acc[116] += (double)v29_6_0;
+            acc[117] += (double)v29_7_0;
+            acc[118] += (double)v29_8_0;
+            acc[119] += (double)v29_9_0;
+            acc[120] += (double)v30_4_0;
+            acc[121] += (double)v30_5_0;
+            acc[122] += (double)v30_6_0;
+            acc[123] += (double)v30_7_0;
+            acc[124] += (double)v30_8_0;
+            acc[125] += (double)v30_9_0;
+            acc[126] += (double)v31_4_0;
+            acc[127] += (double)v31_5_0;
+            acc[128] += (double)v31_6_0;
+            acc[129] += (double)v31_7_0;
+            acc[130] += (double)v31_8_0;
+            acc[131] += (double)v31_9_0;
+            acc[132] += (double)v32_4_0;
+            acc[133] += (double)v32_5_0;
+            acc[134] += (double)v32_6_0;
+            acc[135] += (double)v32_7_0;
+            acc[136] += (double)v32_8_0;
+            acc[137] += (double)v32_9_0;
+            acc[138] += (double)v33_4_0;
+            acc[139] += (double)v33_5_0;
+            acc[140] += (double)v33_6_0;
+            acc[141] += (double)v33_7_0;
+            acc[142] += (double)v33_8_0;
+            acc[143] += (double)v33_9_0;
+            acc[144] += (double)v34_4_0;
+            acc[145] += (double)v34_5_0;
+            acc[146] += (double)v34_6_0;
+            acc[147] += (double)v34_7_0;
+            acc[148] += (double)v34_8_0;
+            acc[149] += (double)v34_9_0;
+        }
+    }
+    if (acc_out) {
+#pragma unroll
+        for (int x = 0; x < 150; ++x) acc_out[x] = acc[x];
+    }
+    const double4 gb = ldg4(&P.geo[p]);
+    const double4 gk = ldg4(&P.geo[q]);
+    const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
+    const double CDx = gk.x, CDy = gk.y, CDz = gk.z;
+    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
+    const double h10_1_4 = acc[60] + ABx * acc[0];
+    const double h10_1_5 = acc[61] + ABx * acc[1];
+    const double h10_1_6 = acc[62] + ABx * acc[2];
+    const double h10_1_7 = acc[63] + ABx * acc[3];
+    const double h10_1_8 = acc[64] + ABx * acc[4];
+    const double h10_1_9 = acc[65] + ABx * acc[5];
+    const double h10_2_4 = acc[66] + ABy * acc[0];
+    const double h10_2_5 = acc[67] + ABy * acc[1];
+    const double h10_2_6 = acc[68] + ABy * acc[2];
+    const double h10_2_7 = acc[69] + ABy * acc[3];
+    const double h10_2_8 = acc[70] + ABy * acc[4];
+    const double h10_2_9 = acc[71] + ABy * acc[5];
+    const double h10_3_4 = acc[72] + ABz * acc[0];
+    const double h10_3_5 = acc[73] + ABz * acc[1];
+    const double h10_3_6 = acc[74] + ABz * acc[2];
+    const double h10_3_7 = acc[75] + ABz * acc[3];
+    const double h10_3_8 = acc[76] + ABz * acc[4];
+    const double h10_3_9 = acc[77] + ABz * acc[5];
+    const double h11_1_4 = acc[66] + ABx * acc[6];
+    const double h11_1_5 = acc[67] + ABx * acc[7];
+    const double h11_1_6 = acc[68] + ABx * acc[8];
+    const double h11_1_7 = acc[69] + ABx * acc[9];
+    const double h11_1_8 = acc[70] + ABx * acc[10];
+    const double h11_1_9 = acc[71] + ABx * acc[11];
+    const double h11_2_4 = acc[78] + ABy * acc[6];
+    const double h11_2_5 = acc[79] + ABy * acc[7];
+    const double h11_2_6 = acc[80] + ABy * acc[8];
+    const double h11_2_7 = acc[81] + ABy * acc[9];
+    const double h11_2_8 = acc[82] + ABy * acc[10];
+    const double h11_2_9 = acc[83] + ABy * acc[11];
+    const double h11_3_4 = acc[84] + ABz * acc[6];
+    const double h11_3_5 = acc[85] + ABz * acc[7];
+    const double h11_3_6 = acc[86] + ABz * acc[8];
+    const double h11_3_7 = acc[87] + ABz * acc[9];
+    const double h11_3_8 = acc[88] + ABz * acc[10];
+    const double h11_3_9 = acc[89] + ABz * acc[11];
+    const double h12_1_4 = acc[72] + ABx * acc[12];
+    const double h12_1_5 = acc[73] + ABx * acc[13];
+    const double h12_1_6 = acc[74] + ABx * acc[14];
+    const double h12_1_7 = acc[75] + ABx * acc[15];
+    const double h12_1_8 = acc[76] + ABx * acc[16];
+    const double h12_1_9 = acc[77] + ABx * acc[17];
+    const double h12_2_4 = acc[84] + ABy * acc[12];
+    const double h12_2_5 = acc[85] + ABy * acc[13];
+    const double h12_2_6 = acc[86] + ABy * acc[14];
+    const double h12_2_7 = acc[87] + ABy * acc[15];
+    const double h12_2_8 = acc[88] + ABy * acc[16];
+    const double h12_2_9 = acc[89] + ABy * acc[17];
+    const double h12_3_4 = acc[90] + ABz * acc[12];
+    const double h12_3_5 = acc[91] + ABz * acc[13];
+    const double h12_3_6 = acc[92] + ABz * acc[14];
+    const double h12_3_7 = acc[93] + ABz * acc[15];
+    const double h12_3_8 = acc[94] + ABz * acc[16];
+    const double h12_3_9 = acc[95] + ABz * acc[17];
+    const double h13_1_4 = acc[78] + ABx * acc[18];
+    const double h13_1_5 = acc[79] + ABx * acc[19];
+    const double h13_1_6 = acc[80] + ABx * acc[20];
+    const double h13_1_7 = acc[81] + ABx * acc[21];
+    const double h13_1_8 = acc[82] + ABx * acc[22];
+    const double h13_1_9 = acc[83] + ABx * acc[23];
+    const double h13_2_4 = acc[96] + ABy * acc[18];
+    const double h13_2_5 = acc[97] + ABy * acc[19];
+    const double h13_2_6 = acc[98] + ABy * acc[20];
+    const double h13_2_7 = acc[99] + ABy * acc[21];
+    const double h13_2_8 = acc[100] + ABy * acc[22];
+    const double h13_2_9 = acc[101] + ABy * acc[23];
+    const double h13_3_4 = acc[102] + ABz * acc[18];
+    const double h13_3_5 = acc[103] + ABz * acc[19];
+    const double h13_3_6 = acc[104] + ABz * acc[20];
+    const double h13_3_7 = acc[105] + ABz * acc[21];
+    const double h13_3_8 = acc[106] + ABz * acc[22];
+    const double h13_3_9 = acc[107] + ABz * acc[23];
+    const double h14_1_4 = acc[90] + ABx * acc[24];
+    const double h14_1_5 = acc[91] + ABx * acc[25];
+    const double h14_1_6 = acc[92] + ABx * acc[26];
+    const double h14_1_7 = acc[93] + ABx * acc[27];
+    const double h14_1_8 = acc[94] + ABx * acc[28];
+    const double h14_1_9 = acc[95] + ABx * acc[29];
+    const double h14_2_4 = acc[108] + ABy * acc[24];
+    const double h14_2_5 = acc[109] + ABy * acc[25];
+    const double h14_2_6 = acc[110] + ABy * acc[26];
+    const double h14_2_7 = acc[111] + ABy * acc[27];
+    const double h14_2_8 = acc[112] + ABy * acc[28];
+    const double h14_2_9 = acc[113] + ABy * acc[29];
+    const double h14_3_4 = acc[114] + ABz * acc[24];
+    const double h14_3_5 = acc[115] + ABz * acc[25];
+    const double h14_3_6 = acc[116] + ABz * acc[26];
+    const double h14_3_7 = acc[117] + ABz * acc[27];
+    const double h14_3_8 = acc[118] + ABz * acc[28];
+    const double h14_3_9 = acc[119] + ABz * acc[29];
+    const double h15_1_4 = acc[84] + ABx * acc[30];
+    const double h15_1_5 = acc[85] + ABx * acc[31];
+    const double h15_1_6 = acc[86] + ABx * acc[32];
+    const double h15_1_7 = acc[87] + ABx * acc[33];
+    const double h15_1_8 = acc[88] + ABx * acc[34];
+    const double h15_1_9 = acc[89] + ABx * acc[35];
+    const double h15_2_4 = acc[102] + ABy * acc[30];
+    const double h15_2_5 = acc[103] + ABy * acc[31];
+    const double h15_2_6 = acc[104] + ABy * acc[32];
+    const double h15_2_7 = acc[105] + ABy * acc[33];
+    const double h15_2_8 = acc[106] + ABy * acc[34];
+    const double h15_2_9 = acc[107] + ABy * acc[35];
+    const double h15_3_4 = acc[108] + ABz * acc[30];
+    const double h15_3_5 = acc[109] + ABz * acc[31];
+    const double h15_3_6 = acc[110] + ABz * acc[32];
+    const double h15_3_7 = acc[111] + ABz * acc[33];
+    const double h15_3_8 = acc[112] + ABz * acc[34];
+    const double h15_3_9 = acc[113] + ABz * acc[35];
+    const double h16_1_4 = acc[96] + ABx * acc[36];
+    const double h16_1_5 = acc[97] + ABx * acc[37];
+    const double h16_1_6 = acc[98] + ABx * acc[38];
+    const double h16_1_7 = acc[99] + ABx * acc[39];
+    const double h16_1_8 = acc[100] + ABx * acc[40];
+    const double h16_1_9 = acc[101] + ABx * acc[41];
+    const double h16_2_4 = acc[120] + ABy * acc[36];
+    const double h16_2_5 = acc[121] + ABy * acc[37];
+    const double h16_2_6 = acc[122] + ABy * acc[38];
+    const double h16_2_7 = acc[123] + ABy * acc[39];
+    const double h16_2_8 = acc[124] + ABy * acc[40];
+    const double h16_2_9 = acc[125] + ABy * acc[41];
+    const double h16_3_4 = acc[126] + ABz * acc[36];
+    const double h16_3_5 = acc[127] + ABz * acc[37];
+    const double h16_3_6 = acc[128] + ABz * acc[38];
+    const double h16_3_7 = acc[129] + ABz * acc[39];
+    const double h16_3_8 = acc[130] + ABz * acc[40];
+    const double h16_3_9 = acc[131] + ABz * acc[41];
+    const double h17_1_4 = acc[102] + ABx * acc[42];
+    const double h17_1_5 = acc[103] + ABx * acc[43];
+    const double h17_1_6 = acc[104] + ABx * acc[44];
+    const double h17_1_7 = acc[105] + ABx * acc[45];
+    const double h17_1_8 = acc[106] + ABx * acc[46];
+    const double h17_1_9 = acc[107] + ABx * acc[47];
+    const double h17_2_4 = acc[126] + ABy * acc[42];
+    const double h17_2_5 = acc[127] + ABy * acc[43];
+    const double h17_2_6 = acc[128] + ABy * acc[44];
+    const double h17_2_7 = acc[129] + ABy * acc[45];
+    const double h17_2_8 = acc[130] + ABy * acc[46];
+    const double h17_2_9 = acc[131] + ABy * acc[47];
+    const double h17_3_4 = acc[132] + ABz * acc[42];
+    const double h17_3_5 = acc[133] + ABz * acc[43];
+    const double h17_3_6 = acc[134] + ABz * acc[44];
+    const double h17_3_7 = acc[135] + ABz * acc[45];
+    const double h17_3_8 = acc[136] + ABz * acc[46];
+    const double h17_3_9 = acc[137] + ABz * acc[47];
+    const double h18_1_4 = acc[108] + ABx * acc[48];
+    const double h18_1_5 = acc[109] + ABx * acc[49];
+    const double h18_1_6 = acc[110] + ABx * acc[50];
+    const double h18_1_7 = acc[111] + ABx * acc[51];
+    const double h18_1_8 = acc[112] + ABx * acc[52];
+    const double h18_1_9 = acc[113] + ABx * acc[53];
+    const double h18_2_4 = acc[132] + ABy * acc[48];
+    const double h18_2_5 = acc[133] + ABy * acc[49];
+    const double h18_2_6 = acc[134] + ABy * acc[50];
+    const double h18_2_7 = acc[135] + ABy * acc[51];
+    const double h18_2_8 = acc[136] + ABy * acc[52];
+    const double h18_2_9 = acc[137] + ABy * acc[53];
+    const double h18_3_4 = acc[138] + ABz * acc[48];
+    const double h18_3_5 = acc[139] + ABz * acc[49];
+    const double h18_3_6 = acc[140] + ABz * acc[50];
+    const double h18_3_7 = acc[141] + ABz * acc[51];
+    const double h18_3_8 = acc[142] + ABz * acc[52];
+    const double h18_3_9 = acc[143] + ABz * acc[53];
+    const double h19_1_4 = acc[114] + ABx * acc[54];
+    const double h19_1_5 = acc[115] + ABx * acc[55];
+    const double h19_1_6 = acc[116] + ABx * acc[56];
+    const double h19_1_7 = acc[117] + ABx * acc[57];
+    const double h19_1_8 = acc[118] + ABx * acc[58];
+    const double h19_1_9 = acc[119] + ABx * acc[59];
+    const double h19_2_4 = acc[138] + ABy * acc[54];
+    const double h19_2_5 = acc[139] + ABy * acc[55];
+    const double h19_2_6 = acc[140] + ABy * acc[56];
+    const double h19_2_7 = acc[141] + ABy * acc[57];
+    const double h19_2_8 = acc[142] + ABy * acc[58];
+    const double h19_2_9 = acc[143] + ABy * acc[59];
+    const double h19_3_4 = acc[144] + ABz * acc[54];
+    const double h19_3_5 = acc[145] + ABz * acc[55];
+    const double h19_3_6 = acc[146] + ABz * acc[56];
+    const double h19_3_7 = acc[147] + ABz * acc[57];
+    const double h19_3_8 = acc[148] + ABz * acc[58];
+    const double h19_3_9 = acc[149] + ABz * acc[59];
+    res[0] = h10_1_4 * 0.14907119849998599;
+    res[1] = h10_1_5 * 0.2581988897471611;
+    res[2] = h10_1_6 * 0.2581988897471611;
+    res[3] = h10_1_7 * 0.14907119849998599;
+    res[4] = h10_1_8 * 0.2581988897471611;
+    res[5] = h10_1_9 * 0.14907119849998599;
+    res[6] = h10_2_4 * 0.14907119849998599;
+    res[7] = h10_2_5 * 0.2581988897471611;
+    res[8] = h10_2_6 * 0.2581988897471611;
+    res[9] = h10_2_7 * 0.14907119849998599;
+    res[10] = h10_2_8 * 0.2581988897471611;
+    res[11] = h10_2_9 * 0.14907119849998599;
+    res[12] = h10_3_4 * 0.14907119849998599;
+    res[13] = h10_3_5 * 0.2581988897471611;
+    res[14] = h10_3_6 * 0.2581988897471611;
+    res[15] = h10_3_7 * 0.14907119849998599;
+    res[16] = h10_3_8 * 0.2581988897471611;
+    res[17] = h10_3_9 * 0.14907119849998599;
+    res[18] = h11_1_4 * 0.3333333333333334;
+    res[19] = h11_1_5 * 0.5773502691896258;
+    res[20] = h11_1_6 * 0.5773502691896258;
+    res[21] = h11_1_7 * 0.3333333333333334;
+    res[22] = h11_1_8 * 0.5773502691896258;
+    res[23] = h11_1_9 * 0.3333333333333334;
+    res[24] = h11_2_4 * 0.3333333333333334;
+    res[25] = h11_2_5 * 0.5773502691896258;
+    res[26] = h11_2_6 * 0.5773502691896258;
+    res[27] = h11_2_7 * 0.3333333333333334;
+    res[28] = h11_2_8 * 0.5773502691896258;
+    res[29] = h11_2_9 * 0.3333333333333334;
+    res[30] = h11_3_4 * 0.3333333333333334;
+    res[31] = h11_3_5 * 0.5773502691896258;
+    res[32] = h11_3_6 * 0.5773502691896258;
+    res[33] = h11_3_7 * 0.3333333333333334;
+    res[34] = h11_3_8 * 0.5773502691896258;
+    res[35] = h11_3_9 * 0.3333333333333334;
+    res[36] = h12_1_4 * 0.3333333333333334;
+    res[37] = h12_1_5 * 0.5773502691896258;
+    res[38] = h12_1_6 * 0.5773502691896258;
+    res[39] = h12_1_7 * 0.3333333333333334;
+    res[40] = h12_1_8 * 0.5773502691896258;
+    res[41] = h12_1_9 * 0.3333333333333334;
+    res[42] = h12_2_4 * 0.3333333333333334;
+    res[43] = h12_2_5 * 0.5773502691896258;
+    res[44] = h12_2_6 * 0.5773502691896258;
+    res[45] = h12_2_7 * 0.3333333333333334;
+    res[46] = h12_2_8 * 0.5773502691896258;
+    res[47] = h12_2_9 * 0.3333333333333334;
+    res[48] = h12_3_4 * 0.3333333333333334;
+    res[49] = h12_3_5 * 0.5773502691896258;
+    res[50] = h12_3_6 * 0.5773502691896258;
+    res[51] = h12_3_7 * 0.3333333333333334;
+    res[52] = h12_3_8 * 0.5773502691896258;
+    res[53] = h12_3_9 * 0.3333333333333334;
+    res[54] = h13_1_4 * 0.3333333333333334;
+    res[55] = h13_1_5 * 0.5773502691896258;
+    res[56] = h13_1_6 * 0.5773502691896258;
+    res[57] = h13_1_7 * 0.3333333333333334;
+    res[58] = h13_1_8 * 0.5773502691896258;
+    res[59] = h13_1_9 * 0.3333333333333334;
+    res[60] = h13_2_4 * 0.3333333333333334;
+    res[61] = h13_2_5 * 0.5773502691896258;
+    res[62] = h13_2_6 * 0.5773502691896258;
+    res[63] = h13_2_7 * 0.3333333333333334;
+    res[64] = h13_2_8 * 0.5773502691896258;
+    res[65] = h13_2_9 * 0.3333333333333334;
+    res[66] = h13_3_4 * 0.3333333333333334;
+    res[67] = h13_3_5 * 0.5773502691896258;
+    res[68] = h13_3_6 * 0.5773502691896258;
+    res[69] = h13_3_7 * 0.3333333333333334;
+    res[70] = h13_3_8 * 0.5773502691896258;
+    res[71] = h13_3_9 * 0.3333333333333334;
+    res[72] = h14_1_4 * 0.3333333333333334;
+    res[73] = h14_1_5 * 0.5773502691896258;
+    res[74] = h14_1_6 * 0.5773502691896258;
+    res[75] = h14_1_7 * 0.3333333333333334;
+    res[76] = h14_1_8 * 0.5773502691896258;
+    res[77] = h14_1_9 * 0.3333333333333334;
+    res[78] = h14_2_4 * 0.3333333333333334;
+    res[79] = h14_2_5 * 0.5773502691896258;
+    res[80] = h14_2_6 * 0.5773502691896258;
+    res[81] = h14_2_7 * 0.3333333333333334;
+    res[82] = h14_2_8 * 0.5773502691896258;
+    res[83] = h14_2_9 * 0.3333333333333334;
+    res[84] = h14_3_4 * 0.3333333333333334;
+    res[85] = h14_3_5 * 0.5773502691896258;
+    res[86] = h14_3_6 * 0.5773502691896258;
+    res[87] = h14_3_7 * 0.3333333333333334;
+    res[88] = h14_3_8 * 0.5773502691896258;
+    res[89] = h14_3_9 * 0.3333333333333334;
+    res[90] = h15_1_4 * 0.5773502691896258;
+    res[91] = h15_1_5;
+    res[92] = h15_1_6;
+    res[93] = h15_1_7 * 0.5773502691896258;
+    res[94] = h15_1_8;
+    res[95] = h15_1_9 * 0.5773502691896258;
+    res[96] = h15_2_4 * 0.5773502691896258;
+    res[97] = h15_2_5;
+    res[98] = h15_2_6;
+    res[99] = h15_2_7 * 0.5773502691896258;
+    res[100] = h15_2_8;
+    res[101] = h15_2_9 * 0.5773502691896258;
+    res[102] = h15_3_4 * 0.5773502691896258;
+    res[103] = h15_3_5;
+    res[104] = h15_3_6;
+    res[105] = h15_3_7 * 0.5773502691896258;
+    res[106] = h15_3_8;
+    res[107] = h15_3_9 * 0.5773502691896258;
+    res[108] = h16_1_4 * 0.14907119849998599;
+    res[109] = h16_1_5 * 0.2581988897471611;
+    res[110] = h16_1_6 * 0.2581988897471611;
+    res[111] = h16_1_7 * 0.14907119849998599;
+    res[112] = h16_1_8 * 0.2581988897471611;
+    res[113] = h16_1_9 * 0.14907119849998599;
+    res[114] = h16_2_4 * 0.14907119849998599;
+    res[115] = h16_2_5 * 0.2581988897471611;
+    res[116] = h16_2_6 * 0.2581988897471611;
+    res[117] = h16_2_7 * 0.14907119849998599;
+    res[118] = h16_2_8 * 0.2581988897471611;
+    res[119] = h16_2_9 * 0.14907119849998599;
+    res[120] = h16_3_4 * 0.14907119849998599;
+    res[121] = h16_3_5 * 0.2581988897471611;
+    res[122] = h16_3_6 * 0.2581988897471611;
+    res[123] = h16_3_7 * 0.14907119849998599;
+    res[124] = h16_3_8 * 0.2581988897471611;
+    res[125] = h16_3_9 * 0.14907119849998599;
+    res[126] = h17_1_4 * 0.3333333333333334;
+    res[127] = h17_1_5 * 0.5773502691896258;
+    res[128] = h17_1_6 * 0.5773502691896258;
+    res[129] = h17_1_7 * 0.3333333333333334;
+    res[130] = h17_1_8 * 0.5773502691896258;
+    res[131] = h17_1_9 * 0.3333333333333334;
+    res[132] = h17_2_4 * 0.3333333333333334;
+    res[133] = h17_2_5 * 0.5773502691896258;
+    res[134] = h17_2_6 * 0.5773502691896258;
+    res[135] = h17_2_7 * 0.3333333333333334;
+    res[136] = h17_2_8 * 0.5773502691896258;
+    res[137] = h17_2_9 * 0.3333333333333334;
+    res[138] = h17_3_4 * 0.3333333333333334;
+    res[139] = h17_3_5 * 0.5773502691896258;
+    res[140] = h17_3_6 * 0.5773502691896258;
+    res[141] = h17_3_7 * 0.3333333333333334;
+    res[142] = h17_3_8 * 0.5773502691896258;
+    res[143] = h17_3_9 * 0.3333333333333334;
+    res[144] = h18_1_4 * 0.3333333333333334;
+    res[145] = h18_1_5 * 0.5773502691896258;
+    res[146] = h18_1_6 * 0.5773502691896258;
+    res[147] = h18_1_7 * 0.3333333333333334;
+    res[148] = h18_1_8 * 0.5773502691896258;
+    res[149] = h18_1_9 * 0.3333333333333334;
+    res[150] = h18_2_4 * 0.3333333333333334;
+    res[151] = h18_2_5 * 0.5773502691896258;
+    res[152] = h18_2_6 * 0.5773502691896258;
+    res[153] = h18_2_7 * 0.3333333333333334;
+    res[154] = h18_2_8 * 0.5773502691896258;
+    res[155] = h18_2_9 * 0.3333333333333334;
+    res[156] = h18_3_4 * 0.3333333333333334;
+    res[157] = h18_3_5 * 0.5773502691896258;
+    res[158] = h18_3_6 * 0.5773502691896258;
+    res[159] = h18_3_7 * 0.3333333333333334;
+    res[160] = h18_3_8 * 0.5773502691896258;
+    res[161] = h18_3_9 * 0.3333333333333334;
+    res[162] = h19_1_4 * 0.14907119849998599;
+    res[163] = h19_1_5 * 0.2581988897471611;
+    res[164] = h19_1_6 * 0.2581988897471611;
+    res[165] = h19_1_7 * 0.14907119849998599;
+    res[166] = h19_1_8 * 0.2581988897471611;
+    res[167] = h19_1_9 * 0.14907119849998599;
+    res[168] = h19_2_4 * 0.14907119849998599;
+    res[169] = h19_2_5 * 0.2581988897471611;
+    res[170] = h19_2_6 * 0.2581988897471611;
+    res[171] = h19_2_7 * 0.14907119849998599;
+    res[172] = h19_2_8 * 0.2581988897471611;
+    res[173] = h19_2_9 * 0.14907119849998599;
+    res[174] = h19_3_4 * 0.14907119849998599;
+    res[175] = h19_3_5 * 0.2581988897471611;
+    res[176] = h19_3_6 * 0.2581988897471611;
+    res[177] = h19_3_7 * 0.14907119849998599;
+    res[178] = h19_3_8 * 0.2581988897471611;
+    res[179] = h19_3_9 * 0.14907119849998599;
+}
+
+__device__ __forceinline__ void store_fpds(double *__restrict__ out, const int4 ib_, const int4 ik_,
+                                            bool same, const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    (void)dab; (void)dcd;
+    const long long ij_0_0 = pair_index(ib_.z + 0, ib_.w + 0);
+    const long long ij_0_1 = pair_index(ib_.z + 0, ib_.w + 1);
+    const long long ij_0_2 = pair_index(ib_.z + 0, ib_.w + 2);
+    const long long ij_1_0 = pair_index(ib_.z + 1, ib_.w + 0);
+    const long long ij_1_1 = pair_index(ib_.z + 1, ib_.w + 1);
+    const long long ij_1_2 = pair_index(ib_.z + 1, ib_.w + 2);
+    const long long ij_2_0 = pair_index(ib_.z + 2, ib_.w + 0);
+    const long long ij_2_1 = pair_index(ib_.z + 2, ib_.w + 1);
+    const long long ij_2_2 = pair_index(ib_.z + 2, ib_.w + 2);
+    const long long ij_3_0 = pair_index(ib_.z + 3, ib_.w + 0);
+    const long long ij_3_1 = pair_index(ib_.z + 3, ib_.w + 1);
+    const long long ij_3_2 = pair_index(ib_.z + 3, ib_.w + 2);
+    const long long ij_4_0 = pair_index(ib_.z + 4, ib_.w + 0);
+    const long long ij_4_1 = pair_index(ib_.z + 4, ib_.w + 1);
+    const long long ij_4_2 = pair_index(ib_.z + 4, ib_.w + 2);
+    const long long ij_5_0 = pair_index(ib_.z + 5, ib_.w + 0);
+    const long long ij_5_1 = pair_index(ib_.z + 5, ib_.w + 1);
+    const long long ij_5_2 = pair_index(ib_.z + 5, ib_.w + 2);
+    const long long ij_6_0 = pair_index(ib_.z + 6, ib_.w + 0);
+    const long long ij_6_1 = pair_index(ib_.z + 6, ib_.w + 1);
+    const long long ij_6_2 = pair_index(ib_.z + 6, ib_.w + 2);
+    const long long ij_7_0 = pair_index(ib_.z + 7, ib_.w + 0);
+    const long long ij_7_1 = pair_index(ib_.z + 7, ib_.w + 1);
+    const long long ij_7_2 = pair_index(ib_.z + 7, ib_.w + 2);
+    const long long ij_8_0 = pair_index(ib_.z + 8, ib_.w + 0);
+    const long long ij_8_1 = pair_index(ib_.z + 8, ib_.w + 1);
+    const long long ij_8_2 = pair_index(ib_.z + 8, ib_.w + 2);
+    const long long ij_9_0 = pair_index(ib_.z + 9, ib_.w + 0);
+    const long long ij_9_1 = pair_index(ib_.z + 9, ib_.w + 1);
+    const long long ij_9_2 = pair_index(ib_.z + 9, ib_.w + 2);
+    const long long kl_0_0 = pair_index(ik_.z + 0, ik_.w + 0);
+    const long long kl_1_0 = pair_index(ik_.z + 1, ik_.w + 0);
+    const long long kl_2_0 = pair_index(ik_.z + 2, ik_.w + 0);
+    const long long kl_3_0 = pair_index(ik_.z + 3, ik_.w + 0);
+    const long long kl_4_0 = pair_index(ik_.z + 4, ik_.w + 0);
+    const long long kl_5_0 = pair_index(ik_.z + 5, ik_.w + 0);
+    { const long long ij = ij_0_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[0]; }
+    { const long long ij = ij_0_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[1]; }
+    { const long long ij = ij_0_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[2]; }
+    { const long long ij = ij_0_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[3]; }
+    { const long long ij = ij_0_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[4]; }
+    { const long long ij = ij_0_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[5]; }
+    { const long long ij = ij_0_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[6]; }
+    { const long long ij = ij_0_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[7]; }
+    { const long long ij = ij_0_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[8]; }
+    { const long long ij = ij_0_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[9]; }
+    { const long long ij = ij_0_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[10]; }
+    { const long long ij = ij_0_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[11]; }
+    { const long long ij = ij_0_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[12]; }
+    { const long long ij = ij_0_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[13]; }
+    { const long long ij = ij_0_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[14]; }
+    { const long long ij = ij_0_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[15]; }
+    { const long long ij = ij_0_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[16]; }
+    { const long long ij = ij_0_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[17]; }
+    { const long long ij = ij_1_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[18]; }
+    { const long long ij = ij_1_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[19]; }
+    { const long long ij = ij_1_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[20]; }
+    { const long long ij = ij_1_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[21]; }
+    { const long long ij = ij_1_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[22]; }
+    { const long long ij = ij_1_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[23]; }
+    { const long long ij = ij_1_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[24]; }
+    { const long long ij = ij_1_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[25]; }
+    { const long long ij = ij_1_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[26]; }
+    { const long long ij = ij_1_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[27]; }
+    { const long long ij = ij_1_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[28]; }
+    { const long long ij = ij_1_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[29]; }
+    { const long long ij = ij_1_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[30]; }
+    { const long long ij = ij_1_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[31]; }
+    { const long long ij = ij_1_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[32]; }
+    { const long long ij = ij_1_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[33]; }
+    { const long long ij = ij_1_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[34]; }
+    { const long long ij = ij_1_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[35]; }
+    { const long long ij = ij_2_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[36]; }
+    { const long long ij = ij_2_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[37]; }
+    { const long long ij = ij_2_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[38]; }
+    { const long long ij = ij_2_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[39]; }
+    { const long long ij = ij_2_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[40]; }
+    { const long long ij = ij_2_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[41]; }
+    { const long long ij = ij_2_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[42]; }
+    { const long long ij = ij_2_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[43]; }
+    { const long long ij = ij_2_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[44]; }
+    { const long long ij = ij_2_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[45]; }
+    { const long long ij = ij_2_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[46]; }
+    { const long long ij = ij_2_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[47]; }
+    { const long long ij = ij_2_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[48]; }
+    { const long long ij = ij_2_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[49]; }
+    { const long long ij = ij_2_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[50]; }
+    { const long long ij = ij_2_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[51]; }
+    { const long long ij = ij_2_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[52]; }
+    { const long long ij = ij_2_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[53]; }
+    { const long long ij = ij_3_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[54]; }
+    { const long long ij = ij_3_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[55]; }
+    { const long long ij = ij_3_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[56]; }
+    { const long long ij = ij_3_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[57]; }
+    { const long long ij = ij_3_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[58]; }
+    { const long long ij = ij_3_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[59]; }
+    { const long long ij = ij_3_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[60]; }
+    { const long long ij = ij_3_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[61]; }
+    { const long long ij = ij_3_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[62]; }
+    { const long long ij = ij_3_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[63]; }
+    { const long long ij = ij_3_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[64]; }
+    { const long long ij = ij_3_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[65]; }
+    { const long long ij = ij_3_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[66]; }
+    { const long long ij = ij_3_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[67]; }
+    { const long long ij = ij_3_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[68]; }
+    { const long long ij = ij_3_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[69]; }
+    { const long long ij = ij_3_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[70]; }
+    { const long long ij = ij_3_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[71]; }
+    { const long long ij = ij_4_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[72]; }
+    { const long long ij = ij_4_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[73]; }
+    { const long long ij = ij_4_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[74]; }
+    { const long long ij = ij_4_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[75]; }
+    { const long long ij = ij_4_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[76]; }
+    { const long long ij = ij_4_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[77]; }
+    { const long long ij = ij_4_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[78]; }
+    { const long long ij = ij_4_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[79]; }
+    { const long long ij = ij_4_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[80]; }
+    { const long long ij = ij_4_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[81]; }
+    { const long long ij = ij_4_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[82]; }
+    { const long long ij = ij_4_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[83]; }
+    { const long long ij = ij_4_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[84]; }
+    { const long long ij = ij_4_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[85]; }
+    { const long long ij = ij_4_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[86]; }
+    { const long long ij = ij_4_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[87]; }
+    { const long long ij = ij_4_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[88]; }
+    { const long long ij = ij_4_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[89]; }
+    { const long long ij = ij_5_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[90]; }
+    { const long long ij = ij_5_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[91]; }
+    { const long long ij = ij_5_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[92]; }
+    { const long long ij = ij_5_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[93]; }
+    { const long long ij = ij_5_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[94]; }
+    { const long long ij = ij_5_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[95]; }
+    { const long long ij = ij_5_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[96]; }
+    { const long long ij = ij_5_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[97]; }
+    { const long long ij = ij_5_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[98]; }
+    { const long long ij = ij_5_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[99]; }
+    { const long long ij = ij_5_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[100]; }
+    { const long long ij = ij_5_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[101]; }
+    { const long long ij = ij_5_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[102]; }
+    { const long long ij = ij_5_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[103]; }
+    { const long long ij = ij_5_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[104]; }
+    { const long long ij = ij_5_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[105]; }
+    { const long long ij = ij_5_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[106]; }
+    { const long long ij = ij_5_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[107]; }
+    { const long long ij = ij_6_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[108]; }
+    { const long long ij = ij_6_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[109]; }
+    { const long long ij = ij_6_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[110]; }
+    { const long long ij = ij_6_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[111]; }
+    { const long long ij = ij_6_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[112]; }
+    { const long long ij = ij_6_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[113]; }
+    { const long long ij = ij_6_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[114]; }
+    { const long long ij = ij_6_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[115]; }
+    { const long long ij = ij_6_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[116]; }
+    { const long long ij = ij_6_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[117]; }
+    { const long long ij = ij_6_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[118]; }
+    { const long long ij = ij_6_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[119]; }
+    { const long long ij = ij_6_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[120]; }
+    { const long long ij = ij_6_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[121]; }
+    { const long long ij = ij_6_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[122]; }
+    { const long long ij = ij_6_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[123]; }
+    { const long long ij = ij_6_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[124]; }
+    { const long long ij = ij_6_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[125]; }
+    { const long long ij = ij_7_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[126]; }
+    { const long long ij = ij_7_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[127]; }
+    { const long long ij = ij_7_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[128]; }
+    { const long long ij = ij_7_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[129]; }
+    { const long long ij = ij_7_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[130]; }
+    { const long long ij = ij_7_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[131]; }
+    { const long long ij = ij_7_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[132]; }
+    { const long long ij = ij_7_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[133]; }
+    { const long long ij = ij_7_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[134]; }
+    { const long long ij = ij_7_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[135]; }
+    { const long long ij = ij_7_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[136]; }
+    { const long long ij = ij_7_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[137]; }
+    { const long long ij = ij_7_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[138]; }
+    { const long long ij = ij_7_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[139]; }
+    { const long long ij = ij_7_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[140]; }
+    { const long long ij = ij_7_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[141]; }
+    { const long long ij = ij_7_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[142]; }
+    { const long long ij = ij_7_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[143]; }
+    { const long long ij = ij_8_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[144]; }
+    { const long long ij = ij_8_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[145]; }
+    { const long long ij = ij_8_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[146]; }
+    { const long long ij = ij_8_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[147]; }
+    { const long long ij = ij_8_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[148]; }
+    { const long long ij = ij_8_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[149]; }
+    { const long long ij = ij_8_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[150]; }
+    { const long long ij = ij_8_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[151]; }
+    { const long long ij = ij_8_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[152]; }
+    { const long long ij = ij_8_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[153]; }
+    { const long long ij = ij_8_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[154]; }
+    { const long long ij = ij_8_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[155]; }
+    { const long long ij = ij_8_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[156]; }
+    { const long long ij = ij_8_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[157]; }
+    { const long long ij = ij_8_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[158]; }
+    { const long long ij = ij_8_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[159]; }
+    { const long long ij = ij_8_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[160]; }
+    { const long long ij = ij_8_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[161]; }
+    { const long long ij = ij_9_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[162]; }
+    { const long long ij = ij_9_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[163]; }
+    { const long long ij = ij_9_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[164]; }
+    { const long long ij = ij_9_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[165]; }
+    { const long long ij = ij_9_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[166]; }
+    { const long long ij = ij_9_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[167]; }
+    { const long long ij = ij_9_1, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[168]; }
+    { const long long ij = ij_9_1, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[169]; }
+    { const long long ij = ij_9_1, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[170]; }
+    { const long long ij = ij_9_1, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[171]; }
+    { const long long ij = ij_9_1, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[172]; }
+    { const long long ij = ij_9_1, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[173]; }
+    { const long long ij = ij_9_2, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[174]; }
+    { const long long ij = ij_9_2, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[175]; }
+    { const long long ij = ij_9_2, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[176]; }
+    { const long long ij = ij_9_2, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[177]; }
+    { const long long ij = ij_9_2, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[178]; }
+    { const long long ij = ij_9_2, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[179]; }
+}
+
+// Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
+// ket pairs of one molecule) from a shared counter until the chunk list, ordered by
+// decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
+template <int MIXED>
+__global__ void __launch_bounds__(128) eri_queue_fpds(const EriQueue Q) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(Q.counter, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= Q.nchunks) return;
+        const int4 ch = __ldg(&Q.chunks[c]);
+        for (int q = ch.y + lane; q < ch.y + ch.z; q += 32) {
+        const int p = ch.x;
+        const double2 bp = __ldg(&Q.pairs.bnd[p]), bq = __ldg(&Q.pairs.bnd[q]);
+        double res[180];
+        if (bp.x * bq.x < Q.screen_cut) {
+#pragma unroll
+            for (int x = 0; x < 180; ++x) res[x] = 0.0;
+        } else {
+            const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
+            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_fpds<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+            else quartet_fpds<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+        }
+        store_fpds(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                    p == q, res);
+        }
+    }
+}
+
+void launch_eri_fpds(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    if (mixed) eri_queue_fpds<1><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_fpds<0><<<grid, 128, 0, s>>>(Q);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_eri_fpds(int mixed) {
+    int n = 0;
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fpds<1>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fpds<0>, 128, 0);
+    return n;
+}
+
+}  // namespace molints

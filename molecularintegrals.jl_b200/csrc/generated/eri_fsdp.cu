@@ -1,0 +1,1500 @@
+// Generated by gen_eri.py -- class (fs|dp).  Do not edit.
+// VRR entries: 486, contracted block: 160, HRR lines: 180, outputs: 180.
+#include "../eri_common.cuh"
+
+namespace molints {
+
+// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[180]
+// (ma, mb, mc, md row-major), summed over the bra primitive pairs [i0, i1) and the ket
+// primitive pairs [j0, j1) of the two shell pairs.  VT is the VRR arithmetic type (double,
+// or float for MIXED).  The ket loop is outside: a warp shares its bra pair, so the inner
+// bra loads are warp-uniform broadcasts and each lane's ket record is loaded once.
+template <typename VT>
+__device__ __forceinline__ void quartet_fsdp(const PairTab &P, const BoysTab &B, int p, int q,
+                                              int i0, int i1, int j0, int j1,
+                                              double *__restrict__ res,
+                                              double *__restrict__ acc_out = nullptr) {
+    const int4 ib_ = __ldg(&P.info[p]);
+    const int4 ik_ = __ldg(&P.info[q]);
+    double acc[160];
+#pragma unroll
+    for (int x = 0; x < 160; ++x) acc[x] = 0.0;
+    for (int j = j0; j < j1; ++j) {
+        const PrimPair ket = load_pp(P.pp, ik_.x + j);
+        for (int i = i0; i < i1; ++i) {
+            const PrimPair bra = load_pp(P.pp, ib_.x + i);
+            const double r = rsqrt(bra.zeta + ket.zeta);
+            const double r2 = r * r;
+            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
+            const double T = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = bra.kab * ket.kab * r;
+            double F[7];
+            boys_fm<6>(T, B, F);
+            const VT PAx = (VT)bra.pax, PAy = (VT)bra.pay, PAz = (VT)bra.paz;
+            const VT QCx = (VT)ket.pax, QCy = (VT)ket.pay, QCz = (VT)ket.paz;
+            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+            const VT WPx = (VT)(-ez * PQx), WPy = (VT)(-ez * PQy), WPz = (VT)(-ez * PQz);
+            const VT WQx = (VT)(zz * PQx), WQy = (VT)(zz * PQy), WQz = (VT)(zz * PQz);
+            const VT oo2z = (VT)bra.oo2z, oo2e = (VT)ket.oo2z, oo2ze = (VT)(0.5 * r2);
+            const VT rho_z = (VT)ez, rho_e = (VT)zz;
+            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz;
+            (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;
+            (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;
+            const VT v0_0_0 = (VT)(pref * F[0]);
+            const VT v0_0_1 = (VT)(pref * F[1]);
+            const VT v0_0_2 = (VT)(pref * F[2]);
+            const VT v0_0_3 = (VT)(pref * F[3]);
+            const VT v0_0_4 = (VT)(pref * F[4]);
+            const VT v0_0_5 = (VT)(pref * F[5]);
+            const VT v0_0_6 = (VT)(pref * F[6]);
+            const VT v1_0_0 = PAx * v0_0_0 + WPx * v0_0_1;
+            const VT v1_0_1 = PAx * v0_0_1 + WPx * v0_0_2;
+            const VT v1_0_2 = PAx * v0_0_2 + WPx * v0_0_3;
+            const VT v1_0_3 = PAx * v0_0_3 + WPx * v0_0_4;
+            const VT v1_0_4 = PAx * v0_0_4 + WPx * v0_0_5;
+            const VT v1_0_5 = PAx * v0_0_5 + WPx * v0_0_6;
+            const VT v2_0_0 = PAy * v0_0_0 + WPy * v0_0_1;
+            const VT v2_0_1 = PAy * v0_0_1 + WPy * v0_0_2;
+            const VT v2_0_2 = PAy * v0_0_2 + WPy * v0_0_3;
+            const VT v2_0_3 = PAy * v0_0_3 + WPy * v0_0_4;
+            const VT v2_0_4 = PAy * v0_0_4 + WPy * v0_0_5;
+            const VT v2_0_5 = PAy * v0_0_5 + WPy * v0_0_6;
+            const VT v3_0_0 = PAz * v0_0_0 + WPz * v0_0_1;
+            const VT v3_0_1 = PAz * v0_0_1 + WPz * v0_0_2;
+            const VT v3_0_2 = PAz * v0_0_2 + WPz * v0_0_3;
+            const VT v3_0_3 = PAz * v0_0_3 + WPz * v0_0_4;
+            const VT v3_0_4 = PAz * v0_0_4 + WPz * v0_0_5;
+            const VT v3_0_5 = PAz * v0_0_5 + WPz * v0_0_6;
+            const VT v4_0_0 = PAx * v1_0_0 + WPx * v1_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v4_0_1 = PAx * v1_0_1 + WPx * v1_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v4_0_2 = PAx * v1_0_2 + WPx * v1_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v4_0_3 = PAx * v1_0_3 + WPx * v1_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v4_0_4 = PAx * v1_0_4 + WPx * v1_0_5 + (VT)1.0 * oo2z * (v0_0_4 - rho_z * v0_0_5);
+            const VT v5_0_0 = PAx * v2_0_0 + WPx * v2_0_1;
+            const VT v5_0_1 = PAx * v2_0_1 + WPx * v2_0_2;
+            const VT v5_0_2 = PAx * v2_0_2 + WPx * v2_0_3;
+            const VT v5_0_3 = PAx * v2_0_3 + WPx * v2_0_4;
+            const VT v5_0_4 = PAx * v2_0_4 + WPx * v2_0_5;
+            const VT v6_0_0 = PAx * v3_0_0 + WPx * v3_0_1;
+            const VT v6_0_1 = PAx * v3_0_1 + WPx * v3_0_2;
+            const VT v6_0_2 = PAx * v3_0_2 + WPx * v3_0_3;
+            const VT v6_0_3 = PAx * v3_0_3 + WPx * v3_0_4;
+            const VT v6_0_4 = PAx * v3_0_4 + WPx * v3_0_5;
+            const VT v7_0_0 = PAy * v2_0_0 + WPy * v2_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v7_0_1 = PAy * v2_0_1 + WPy * v2_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v7_0_2 = PAy * v2_0_2 + WPy * v2_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v7_0_3 = PAy * v2_0_3 + WPy * v2_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v7_0_4 = PAy * v2_0_4 + WPy * v2_0_5 + (VT)1.0 * oo2z * (v0_0_4 - rho_z * v0_0_5);
+            const VT v8_0_0 = PAy * v3_0_0 + WPy * v3_0_1;
+            const VT v8_0_1 = PAy * v3_0_1 + WPy * v3_0_2;
+            const VT v8_0_2 = PAy * v3_0_2 + WPy * v3_0_3;
+            const VT v8_0_3 = PAy * v3_0_3 + WPy * v3_0_4;
+            const VT v8_0_4 = PAy * v3_0_4 + WPy * v3_0_5;
+            const VT v9_0_0 = PAz * v3_0_0 + WPz * v3_0_1 + (VT)1.0 * oo2z * (v0_0_0 - rho_z * v0_0_1);
+            const VT v9_0_1 = PAz * v3_0_1 + WPz * v3_0_2 + (VT)1.0 * oo2z * (v0_0_1 - rho_z * v0_0_2);
+            const VT v9_0_2 = PAz * v3_0_2 + WPz * v3_0_3 + (VT)1.0 * oo2z * (v0_0_2 - rho_z * v0_0_3);
+            const VT v9_0_3 = PAz * v3_0_3 + WPz * v3_0_4 + (VT)1.0 * oo2z * (v0_0_3 - rho_z * v0_0_4);
+            const VT v9_0_4 = PAz * v3_0_4 + WPz * v3_0_5 + (VT)1.0 * oo2z * (v0_0_4 - rho_z * v0_0_5);
+            const VT v10_0_0 = PAx * v4_0_0 + WPx * v4_0_1 + (VT)2.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v10_0_1 = PAx * v4_0_1 + WPx * v4_0_2 + (VT)2.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v10_0_2 = PAx * v4_0_2 + WPx * v4_0_3 + (VT)2.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v10_0_3 = PAx * v4_0_3 + WPx * v4_0_4 + (VT)2.0 * oo2z * (v1_0_3 - rho_z * v1_0_4);
+            const VT v11_0_0 = PAx * v5_0_0 + WPx * v5_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v11_0_1 = PAx * v5_0_1 + WPx * v5_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v11_0_2 = PAx * v5_0_2 + WPx * v5_0_3 + (VT)1.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v11_0_3 = PAx * v5_0_3 + WPx * v5_0_4 + (VT)1.0 * oo2z * (v2_0_3 - rho_z * v2_0_4);
+            const VT v12_0_0 = PAx * v6_0_0 + WPx * v6_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v12_0_1 = PAx * v6_0_1 + WPx * v6_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v12_0_2 = PAx * v6_0_2 + WPx * v6_0_3 + (VT)1.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v12_0_3 = PAx * v6_0_3 + WPx * v6_0_4 + (VT)1.0 * oo2z * (v3_0_3 - rho_z * v3_0_4);
+            const VT v13_0_0 = PAy * v5_0_0 + WPy * v5_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v13_0_1 = PAy * v5_0_1 + WPy * v5_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v13_0_2 = PAy * v5_0_2 + WPy * v5_0_3 + (VT)1.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v13_0_3 = PAy * v5_0_3 + WPy * v5_0_4 + (VT)1.0 * oo2z * (v1_0_3 - rho_z * v1_0_4);
+            const VT v14_0_0 = PAz * v6_0_0 + WPz * v6_0_1 + (VT)1.0 * oo2z * (v1_0_0 - rho_z * v1_0_1);
+            const VT v14_0_1 = PAz * v6_0_1 + WPz * v6_0_2 + (VT)1.0 * oo2z * (v1_0_1 - rho_z * v1_0_2);
+            const VT v14_0_2 = PAz * v6_0_2 + WPz * v6_0_3 + (VT)1.0 * oo2z * (v1_0_2 - rho_z * v1_0_3);
+            const VT v14_0_3 = PAz * v6_0_3 + WPz * v6_0_4 + (VT)1.0 * oo2z * (v1_0_3 - rho_z * v1_0_4);
+            const VT v15_0_0 = PAx * v8_0_0 + WPx * v8_0_1;
+            const VT v15_0_1 = PAx * v8_0_1 + WPx * v8_0_2;
+            const VT v15_0_2 = PAx * v8_0_2 + WPx * v8_0_3;
+            const VT v15_0_3 = PAx * v8_0_3 + WPx * v8_0_4;
+            const VT v16_0_0 = PAy * v7_0_0 + WPy * v7_0_1 + (VT)2.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v16_0_1 = PAy * v7_0_1 + WPy * v7_0_2 + (VT)2.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v16_0_2 = PAy * v7_0_2 + WPy * v7_0_3 + (VT)2.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v16_0_3 = PAy * v7_0_3 + WPy * v7_0_4 + (VT)2.0 * oo2z * (v2_0_3 - rho_z * v2_0_4);
+            const VT v17_0_0 = PAy * v8_0_0 + WPy * v8_0_1 + (VT)1.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v17_0_1 = PAy * v8_0_1 + WPy * v8_0_2 + (VT)1.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v17_0_2 = PAy * v8_0_2 + WPy * v8_0_3 + (VT)1.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v17_0_3 = PAy * v8_0_3 + WPy * v8_0_4 + (VT)1.0 * oo2z * (v3_0_3 - rho_z * v3_0_4);
+            const VT v18_0_0 = PAz * v8_0_0 + WPz * v8_0_1 + (VT)1.0 * oo2z * (v2_0_0 - rho_z * v2_0_1);
+            const VT v18_0_1 = PAz * v8_0_1 + WPz * v8_0_2 + (VT)1.0 * oo2z * (v2_0_1 - rho_z * v2_0_2);
+            const VT v18_0_2 = PAz * v8_0_2 + WPz * v8_0_3 + (VT)1.0 * oo2z * (v2_0_2 - rho_z * v2_0_3);
+            const VT v18_0_3 = PAz * v8_0_3 + WPz * v8_0_4 + (VT)1.0 * oo2z * (v2_0_3 - rho_z * v2_0_4);
+            const VT v19_0_0 = PAz * v9_0_0 + WPz * v9_0_1 + (VT)2.0 * oo2z * (v3_0_0 - rho_z * v3_0_1);
+            const VT v19_0_1 = PAz * v9_0_1 + WPz * v9_0_2 + (VT)2.0 * oo2z * (v3_0_1 - rho_z * v3_0_2);
+            const VT v19_0_2 = PAz * v9_0_2 + WPz * v9_0_3 + (VT)2.0 * oo2z * (v3_0_2 - rho_z * v3_0_3);
+            const VT v19_0_3 = PAz * v9_0_3 + WPz * v9_0_4 + (VT)2.0 * oo2z * (v3_0_3 - rho_z * v3_0_4);
+            const VT v1_1_2 = QCx * v1_0_2 + WQx * v1_0_3 + (VT)1.0 * oo2ze * v0_0_3;
+            const VT v2_1_2 = QCx * v2_0_2 + WQx * v2_0_3;
+            const VT v3_1_2 = QCx * v3_0_2 + WQx * v3_0_3;
+            const VT v4_1_1 = QCx * v4_0_1 + WQx * v4_0_2 + (VT)2.0 * oo2ze * v1_0_2;
+            const VT v4_1_2 = QCx * v4_0_2 + WQx * v4_0_3 + (VT)2.0 * oo2ze * v1_0_3;
+            const VT v5_1_1 = QCx * v5_0_1 + WQx * v5_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v5_1_2 = QCx * v5_0_2 + WQx * v5_0_3 + (VT)1.0 * oo2ze * v2_0_3;
+            const VT v6_1_1 = QCx * v6_0_1 + WQx * v6_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v6_1_2 = QCx * v6_0_2 + WQx * v6_0_3 + (VT)1.0 * oo2ze * v3_0_3;
+            const VT v7_1_1 = QCx * v7_0_1 + WQx * v7_0_2;
+            const VT v7_1_2 = QCx * v7_0_2 + WQx * v7_0_3;
+            const VT v8_1_1 = QCx * v8_0_1 + WQx * v8_0_2;
+            const VT v8_1_2 = QCx * v8_0_2 + WQx * v8_0_3;
+            const VT v9_1_1 = QCx * v9_0_1 + WQx * v9_0_2;
+            const VT v9_1_2 = QCx * v9_0_2 + WQx * v9_0_3;
+            const VT v10_1_0 = QCx * v10_0_0 + WQx * v10_0_1 + (VT)3.0 * oo2ze * v4_0_1;
+            const VT v10_1_1 = QCx * v10_0_1 + WQx * v10_0_2 + (VT)3.0 * oo2ze * v4_0_2;
+            const VT v10_1_2 = QCx * v10_0_2 + WQx * v10_0_3 + (VT)3.0 * oo2ze * v4_0_3;
+            const VT v11_1_0 = QCx * v11_0_0 + WQx * v11_0_1 + (VT)2.0 * oo2ze * v5_0_1;
+            const VT v11_1_1 = QCx * v11_0_1 + WQx * v11_0_2 + (VT)2.0 * oo2ze * v5_0_2;
+            const VT v11_1_2 = QCx * v11_0_2 + WQx * v11_0_3 + (VT)2.0 * oo2ze * v5_0_3;
+            const VT v12_1_0 = QCx * v12_0_0 + WQx * v12_0_1 + (VT)2.0 * oo2ze * v6_0_1;
+            const VT v12_1_1 = QCx * v12_0_1 + WQx * v12_0_2 + (VT)2.0 * oo2ze * v6_0_2;
+            const VT v12_1_2 = QCx * v12_0_2 + WQx * v12_0_3 + (VT)2.0 * oo2ze * v6_0_3;
+            const VT v13_1_0 = QCx * v13_0_0 + WQx * v13_0_1 + (VT)1.0 * oo2ze * v7_0_1;
+            const VT v13_1_1 = QCx * v13_0_1 + WQx * v13_0_2 + (VT)1.0 * oo2ze * v7_0_2;
+            const VT v13_1_2 = QCx * v13_0_2 + WQx * v13_0_3 + (VT)1.0 * oo2ze * v7_0_3;
+            const VT v14_1_0 = QCx * v14_0_0 + WQx * v14_0_1 + (VT)1.0 * oo2ze * v9_0_1;
+            const VT v14_1_1 = QCx * v14_0_1 + WQx * v14_0_2 + (VT)1.0 * oo2ze * v9_0_2;
+            const VT v14_1_2 = QCx * v14_0_2 + WQx * v14_0_3 + (VT)1.0 * oo2ze * v9_0_3;
+            const VT v15_1_0 = QCx * v15_0_0 + WQx * v15_0_1 + (VT)1.0 * oo2ze * v8_0_1;
+            const VT v15_1_1 = QCx * v15_0_1 + WQx * v15_0_2 + (VT)1.0 * oo2ze * v8_0_2;
+            const VT v15_1_2 = QCx * v15_0_2 + WQx * v15_0_3 + (VT)1.0 * oo2ze * v8_0_3;
+            const VT v16_1_0 = QCx * v16_0_0 + WQx * v16_0_1;
+            const VT v16_1_1 = QCx * v16_0_1 + WQx * v16_0_2;
+            const VT v16_1_2 = QCx * v16_0_2 + WQx * v16_0_3;
+            const VT v17_1_0 = QCx * v17_0_0 + WQx * v17_0_1;
+            const VT v17_1_1 = QCx * v17_0_1 + WQx * v17_0_2;
+            const VT v17_1_2 = QCx * v17_0_2 + WQx * v17_0_3;
+            const VT v18_1_0 = QCx * v18_0_0 + WQx * v18_0_1;
+            const VT v18_1_1 = QCx * v18_0_1 + WQx * v18_0_2;
+            const VT v18_1_2 = QCx * v18_0_2 + WQx * v18_0_3;
+            const VT v19_1_0 = QCx * v19_0_0 + WQx * v19_0_1;
+            const VT v19_1_1 = QCx * v19_0_1 + WQx * v19_0_2;
+            const VT v19_1_2 = QCx * v19_0_2 + WQx * v19_0_3;
+            const VT v1_2_2 = QCy * v1_0_2 + WQy * v1_0_3;
+            const VT v2_2_2 = QCy * v2_0_2 + WQy * v2_0_3 + (VT)1.0 * oo2ze * v0_0_3;
+            const VT v3_2_2 = QCy * v3_0_2 + WQy * v3_0_3;
+            const VT v4_2_1 = QCy * v4_0_1 + WQy * v4_0_2;
+            const VT v4_2_2 = QCy * v4_0_2 + WQy * v4_0_3;
+            const VT v5_2_1 = QCy * v5_0_1 + WQy * v5_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v5_2_2 = QCy * v5_0_2 + WQy * v5_0_3 + (VT)1.0 * oo2ze * v1_0_3;
+            const VT v6_2_1 = QCy * v6_0_1 + WQy * v6_0_2;
+            const VT v6_2_2 = QCy * v6_0_2 + WQy * v6_0_3;
+            const VT v7_2_1 = QCy * v7_0_1 + WQy * v7_0_2 + (VT)2.0 * oo2ze * v2_0_2;
+            const VT v7_2_2 = QCy * v7_0_2 + WQy * v7_0_3 + (VT)2.0 * oo2ze * v2_0_3;
+            const VT v8_2_1 = QCy * v8_0_1 + WQy * v8_0_2 + (VT)1.0 * oo2ze * v3_0_2;
+            const VT v8_2_2 = QCy * v8_0_2 + WQy * v8_0_3 + (VT)1.0 * oo2ze * v3_0_3;
+            const VT v9_2_1 = QCy * v9_0_1 + WQy * v9_0_2;
+            const VT v9_2_2 = QCy * v9_0_2 + WQy * v9_0_3;
+            const VT v10_2_0 = QCy * v10_0_0 + WQy * v10_0_1;
+            const VT v10_2_1 = QCy * v10_0_1 + WQy * v10_0_2;
+            const VT v10_2_2 = QCy * v10_0_2 + WQy * v10_0_3;
+            const VT v11_2_0 = QCy * v11_0_0 + WQy * v11_0_1 + (VT)1.0 * oo2ze * v4_0_1;
+            const VT v11_2_1 = QCy * v11_0_1 + WQy * v11_0_2 + (VT)1.0 * oo2ze * v4_0_2;
+            const VT v11_2_2 = QCy * v11_0_2 + WQy * v11_0_3 + (VT)1.0 * oo2ze * v4_0_3;
+            const VT v12_2_0 = QCy * v12_0_0 + WQy * v12_0_1;
+            const VT v12_2_1 = QCy * v12_0_1 + WQy * v12_0_2;
+            const VT v12_2_2 = QCy * v12_0_2 + WQy * v12_0_3;
+            const VT v13_2_0 = QCy * v13_0_0 + WQy * v13_0_1 + (VT)2.0 * oo2ze * v5_0_1;
+            const VT v13_2_1 = QCy * v13_0_1 + WQy * v13_0_2 + (VT)2.0 * oo2ze * v5_0_2;
+            const VT v13_2_2 = QCy * v13_0_2 + WQy * v13_0_3 + (VT)2.0 * oo2ze * v5_0_3;
+            const VT v14_2_0 = QCy * v14_0_0 + WQy * v14_0_1;
+            const VT v14_2_1 = QCy * v14_0_1 + WQy * v14_0_2;
+            const VT v14_2_2 = QCy * v14_0_2 + WQy * v14_0_3;
+            const VT v15_2_0 = QCy * v15_0_0 + WQy * v15_0_1 + (VT)1.0 * oo2ze * v6_0_1;
+            const VT v15_2_1 = QCy * v15_0_1 + WQy * v15_0_2 + (VT)1.0 * oo2ze * v6_0_2;
+            const VT v15_2_2 = QCy * v15_0_2 + WQy * v15_0_3 + (VT)1.0 * oo2ze * v6_0_3;
+            const VT v16_2_0 = QCy * v16_0_0 + WQy * v16_0_1 + (VT)3.0 * oo2ze * v7_0_1;
+            const VT v16_2_1 = QCy * v16_0_1 + WQy * v16_0_2 + (VT)3.0 * oo2ze * v7_0_2;
+            const VT v16_2_2 = QCy * v16_0_2 + WQy * v16_0_3 + (VT)3.0 * oo2ze * v7_0_3;
+            const VT v17_2_0 = QCy * v17_0_0 + WQy * v17_0_1 + (VT)2.0 * oo2ze * v8_0_1;
+            const VT v17_2_1 = QCy * v17_0_1 + WQy * v17_0_2 + (VT)2.0 * oo2ze * v8_0_2;
+            const VT v17_2_2 = QCy * v17_0_2 + WQy * v17_0_3 + (VT)2.0 * oo2ze * v8_0_3;
+            const VT v18_2_0 = QCy * v18_0_0 + WQy * v18_0_1 + (VT)1.0 * oo2ze * v9_0_1;
+            const VT v18_2_1 = QCy * v18_0_1 + WQy * v18_0_2 + (VT)1.0 * oo2ze * v9_0_2;
+            const VT v18_2_2 = QCy * v18_0_2 + WQy * v18_0_3 + (VT)1.0 * oo2ze * v9_0_3;
+            const VT v19_2_0 = QCy * v19_0_0 + WQy * v19_0_1;
+            const VT v19_2_1 = QCy * v19_0_1 + WQy * v19_0_2;
+            const VT v19_2_2 = QCy * v19_0_2 + WQy * v19_0_3;
+            const VT v1_3_2 = QCz * v1_0_2 + WQz * v1_0_3;
+            const VT v2_3_2 = QCz * v2_0_2 + WQz * v2_0_3;
+            const VT v3_3_2 = QCz * v3_0_2 + WQz * v3_0_3 + (VT)1.0 * oo2ze * v0_0_3;
+            const VT v4_3_1 = QCz * v4_0_1 + WQz * v4_0_2;
+            const VT v4_3_2 = QCz * v4_0_2 + WQz * v4_0_3;
+            const VT v5_3_1 = QCz * v5_0_1 + WQz * v5_0_2;
+            const VT v5_3_2 = QCz * v5_0_2 + WQz * v5_0_3;
+            const VT v6_3_1 = QCz * v6_0_1 + WQz * v6_0_2 + (VT)1.0 * oo2ze * v1_0_2;
+            const VT v6_3_2 = QCz * v6_0_2 + WQz * v6_0_3 + (VT)1.0 * oo2ze * v1_0_3;
+            const VT v7_3_1 = QCz * v7_0_1 + WQz * v7_0_2;
+            const VT v7_3_2 = QCz * v7_0_2 + WQz * v7_0_3;
+            const VT v8_3_1 = QCz * v8_0_1 + WQz * v8_0_2 + (VT)1.0 * oo2ze * v2_0_2;
+            const VT v8_3_2 = QCz * v8_0_2 + WQz * v8_0_3 + (VT)1.0 * oo2ze * v2_0_3;
+            const VT v9_3_1 = QCz * v9_0_1 + WQz * v9_0_2 + (VT)2.0 * oo2ze * v3_0_2;
+            const VT v9_3_2 = QCz * v9_0_2 + WQz * v9_0_3 + (VT)2.0 * oo2ze * v3_0_3;
+            const VT v10_3_0 = QCz * v10_0_0 + WQz * v10_0_1;
+            const VT v10_3_1 = QCz * v10_0_1 + WQz * v10_0_2;
+            const VT v10_3_2 = QCz * v10_0_2 + WQz * v10_0_3;
+            const VT v11_3_0 = QCz * v11_0_0 + WQz * v11_0_1;
+            const VT v11_3_1 = QCz * v11_0_1 + WQz * v11_0_2;
+            const VT v11_3_2 = QCz * v11_0_2 + WQz * v11_0_3;
+            const VT v12_3_0 = QCz * v12_0_0 + WQz * v12_0_1 + (VT)1.0 * oo2ze * v4_0_1;
+            const VT v12_3_1 = QCz * v12_0_1 + WQz * v12_0_2 + (VT)1.0 * oo2ze * v4_0_2;
+            const VT v12_3_2 = QCz * v12_0_2 + WQz * v12_0_3 + (VT)1.0 * oo2ze * v4_0_3;
+            const VT v13_3_0 = QCz * v13_0_0 + WQz * v13_0_1;
+            const VT v13_3_1 = QCz * v13_0_1 + WQz * v13_0_2;
+            const VT v13_3_2 = QCz * v13_0_2 + WQz * v13_0_3;
+            const VT v14_3_0 = QCz * v14_0_0 + WQz * v14_0_1 + (VT)2.0 * oo2ze * v6_0_1;
+            const VT v14_3_1 = QCz * v14_0_1 + WQz * v14_0_2 + (VT)2.0 * oo2ze * v6_0_2;
+            const VT v14_3_2 = QCz * v14_0_2 + WQz * v14_0_3 + (VT)2.0 * oo2ze * v6_0_3;
+            const VT v15_3_0 = QCz * v15_0_0 + WQz * v15_0_1 + (VT)1.0 * oo2ze * v5_0_1;
+            const VT v15_3_1 = QCz * v15_0_1 + WQz * v15_0_2 + (VT)1.0 * oo2ze * v5_0_2;
+            const VT v15_3_2 = QCz * v15_0_2 + WQz * v15_0_3 + (VT)1.0 * oo2ze * v5_0_3;
+            const VT v16_3_0 = QCz * v16_0_0 + WQz * v16_0_1;
+            const VT v16_3_1 = QCz * v16_0_1 + WQz * v16_0_2;
+            const VT v16_3_2 = QCz * v16_0_2 + WQz * v16_0_3;
+            const VT v17_3_0 = QCz * v17_0_0 + WQz * v17_0_1 + (VT)1.0 * oo2ze * v7_0_1;
+            const VT v17_3_1 = QCz * v17_0_1 + WQz * v17_0_2 + (VT)1.0 * oo2ze * v7_0_2;
+            const VT v17_3_2 = QCz * v17_0_2 + WQz * v17_0_3 + (VT)1.0 * oo2ze * v7_0_3;
+            const VT v18_3_0 = QCz * v18_0_0 + WQz * v18_0_1 + (VT)2.0 * oo2ze * v8_0_1;
+            const VT v18_3_1 = QCz * v18_0_1 + WQz * v18_0_2 + (VT)2.0 * oo2ze * v8_0_2;
+            const VT v18_3_2 = QCz * v18_0_2 + WQz * v18_0_3 + (VT)2.0 * oo2ze * v8_0_3;
+            const VT v19_3_0 = QCz * v19_0_0 + WQz * v19_0_1 + (VT)3.0 * oo2ze * v9_0_1;
+            const VT v19_3_1 = QCz * v19_0_1 + WQz * v19_0_2 + (VT)3.0 * oo2ze * v9_0_2;
+            const VT v19_3_2 = QCz * v19_0_2 + WQz * v19_0_3 + (VT)3.0 * oo2ze * v9_0_3;
+            const VT v4_4_1 = QCx * v4_1_1 + WQx * v4_1_2 + (VT)2.0 * oo2ze * v1_1_2 + (VT)1.0 * oo2e * (v4_0_1 - rho_e * v4_0_2);
+            const VT v5_4_1 = QCx * v5_1_1 + WQx * v5_1_2 + (VT)1.0 * oo2ze * v2_1_2 + (VT)1.0 * oo2e * (v5_0_1 - rho_e * v5_0_2);
+            const VT v6_4_1 = QCx * v6_1_1 + WQx * v6_1_2 + (VT)1.0 * oo2ze * v3_1_2 + (VT)1.0 * oo2e * (v6_0_1 - rho_e * v6_0_2);
+            const VT v7_4_1 = QCx * v7_1_1 + WQx * v7_1_2 + (VT)1.0 * oo2e * (v7_0_1 - rho_e * v7_0_2);
+            const VT v8_4_1 = QCx * v8_1_1 + WQx * v8_1_2 + (VT)1.0 * oo2e * (v8_0_1 - rho_e * v8_0_2);
+            const VT v9_4_1 = QCx * v9_1_1 + WQx * v9_1_2 + (VT)1.0 * oo2e * (v9_0_1 - rho_e * v9_0_2);
+            const VT v10_4_0 = QCx * v10_1_0 + WQx * v10_1_1 + (VT)3.0 * oo2ze * v4_1_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v10_4_1 = QCx * v10_1_1 + WQx * v10_1_2 + (VT)3.0 * oo2ze * v4_1_2 + (VT)1.0 * oo2e * (v10_0_1 - rho_e * v10_0_2);
+            const VT v11_4_0 = QCx * v11_1_0 + WQx * v11_1_1 + (VT)2.0 * oo2ze * v5_1_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v11_4_1 = QCx * v11_1_1 + WQx * v11_1_2 + (VT)2.0 * oo2ze * v5_1_2 + (VT)1.0 * oo2e * (v11_0_1 - rho_e * v11_0_2);
+            const VT v12_4_0 = QCx * v12_1_0 + WQx * v12_1_1 + (VT)2.0 * oo2ze * v6_1_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v12_4_1 = QCx * v12_1_1 + WQx * v12_1_2 + (VT)2.0 * oo2ze * v6_1_2 + (VT)1.0 * oo2e * (v12_0_1 - rho_e * v12_0_2);
+            const VT v13_4_0 = QCx * v13_1_0 + WQx * v13_1_1 + (VT)1.0 * oo2ze * v7_1_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v13_4_1 = QCx * v13_1_1 + WQx * v13_1_2 + (VT)1.0 * oo2ze * v7_1_2 + (VT)1.0 * oo2e * (v13_0_1 - rho_e * v13_0_2);
+            const VT v14_4_0 = QCx * v14_1_0 + WQx * v14_1_1 + (VT)1.0 * oo2ze * v9_1_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v14_4_1 = QCx * v14_1_1 + WQx * v14_1_2 + (VT)1.0 * oo2ze * v9_1_2 + (VT)1.0 * oo2e * (v14_0_1 - rho_e * v14_0_2);
+            const VT v15_4_0 = QCx * v15_1_0 + WQx * v15_1_1 + (VT)1.0 * oo2ze * v8_1_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v15_4_1 = QCx * v15_1_1 + WQx * v15_1_2 + (VT)1.0 * oo2ze * v8_1_2 + (VT)1.0 * oo2e * (v15_0_1 - rho_e * v15_0_2);
+            const VT v16_4_0 = QCx * v16_1_0 + WQx * v16_1_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v16_4_1 = QCx * v16_1_1 + WQx * v16_1_2 + (VT)1.0 * oo2e * (v16_0_1 - rho_e * v16_0_2);
+            const VT v17_4_0 = QCx * v17_1_0 + WQx * v17_1_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v17_4_1 = QCx * v17_1_1 + WQx * v17_1_2 + (VT)1.0 * oo2e * (v17_0_1 - rho_e * v17_0_2);
+            const VT v18_4_0 = QCx * v18_1_0 + WQx * v18_1_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v18_4_1 = QCx * v18_1_1 + WQx * v18_1_2 + (VT)1.0 * oo2e * (v18_0_1 - rho_e * v18_0_2);
+            const VT v19_4_0 = QCx * v19_1_0 + WQx * v19_1_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v19_4_1 = QCx * v19_1_1 + WQx * v19_1_2 + (VT)1.0 * oo2e * (v19_0_1 - rho_e * v19_0_2);
+            const VT v4_5_1 = QCx * v4_2_1 + WQx * v4_2_2 + (VT)2.0 * oo2ze * v1_2_2;
+            const VT v5_5_1 = QCx * v5_2_1 + WQx * v5_2_2 + (VT)1.0 * oo2ze * v2_2_2;
+            const VT v6_5_1 = QCx * v6_2_1 + WQx * v6_2_2 + (VT)1.0 * oo2ze * v3_2_2;
+            const VT v7_5_1 = QCx * v7_2_1 + WQx * v7_2_2;
+            const VT v8_5_1 = QCx * v8_2_1 + WQx * v8_2_2;
+            const VT v9_5_1 = QCx * v9_2_1 + WQx * v9_2_2;
+            const VT v10_5_0 = QCx * v10_2_0 + WQx * v10_2_1 + (VT)3.0 * oo2ze * v4_2_1;
+            const VT v10_5_1 = QCx * v10_2_1 + WQx * v10_2_2 + (VT)3.0 * oo2ze * v4_2_2;
+            const VT v11_5_0 = QCx * v11_2_0 + WQx * v11_2_1 + (VT)2.0 * oo2ze * v5_2_1;
+            const VT v11_5_1 = QCx * v11_2_1 + WQx * v11_2_2 + (VT)2.0 * oo2ze * v5_2_2;
+            const VT v12_5_0 = QCx * v12_2_0 + WQx * v12_2_1 + (VT)2.0 * oo2ze * v6_2_1;
+            const VT v12_5_1 = QCx * v12_2_1 + WQx * v12_2_2 + (VT)2.0 * oo2ze * v6_2_2;
+            const VT v13_5_0 = QCx * v13_2_0 + WQx * v13_2_1 + (VT)1.0 * oo2ze * v7_2_1;
+            const VT v13_5_1 = QCx * v13_2_1 + WQx * v13_2_2 + (VT)1.0 * oo2ze * v7_2_2;
+            const VT v14_5_0 = QCx * v14_2_0 + WQx * v14_2_1 + (VT)1.0 * oo2ze * v9_2_1;
+            const VT v14_5_1 = QCx * v14_2_1 + WQx * v14_2_2 + (VT)1.0 * oo2ze * v9_2_2;
+            const VT v15_5_0 = QCx * v15_2_0 + WQx * v15_2_1 + (VT)1.0 * oo2ze * v8_2_1;
+            const VT v15_5_1 = QCx * v15_2_1 + WQx * v15_2_2 + (VT)1.0 * oo2ze * v8_2_2;
+            const VT v16_5_0 = QCx * v16_2_0 + WQx * v16_2_1;
+            const VT v16_5_1 = QCx * v16_2_1 + WQx * v16_2_2;
+            const VT v17_5_0 = QCx * v17_2_0 + WQx * v17_2_1;
+            const VT v17_5_1 = QCx * v17_2_1 + WQx * v17_2_2;
+            const VT v18_5_0 = QCx * v18_2_0 + WQx * v18_2_1;
+            const VT v18_5_1 = QCx * v18_2_1 + WQx * v18_2_2;
+            const VT v19_5_0 = QCx * v19_2_0 + WQx * v19_2_1;
+            const VT v19_5_1 = QCx * v19_2_1 + WQx * v19_2_2;
+            const VT v4_6_1 = QCx * v4_3_1 + WQx * v4_3_2 + (VT)2.0 * oo2ze * v1_3_2;
+            const VT v5_6_1 = QCx * v5_3_1 + WQx * v5_3_2 + (VT)1.0 * oo2ze * v2_3_2;
+            const VT v6_6_1 = QCx * v6_3_1 + WQx * v6_3_2 + (VT)1.0 * oo2ze * v3_3_2;
+            const VT v7_6_1 = QCx * v7_3_1 + WQx * v7_3_2;
+            const VT v8_6_1 = QCx * v8_3_1 + WQx * v8_3_2;
+            const VT v9_6_1 = QCx * v9_3_1 + WQx * v9_3_2;
+            const VT v10_6_0 = QCx * v10_3_0 + WQx * v10_3_1 + (VT)3.0 * oo2ze * v4_3_1;
+            const VT v10_6_1 = QCx * v10_3_1 + WQx * v10_3_2 + (VT)3.0 * oo2ze * v4_3_2;
+            const VT v11_6_0 = QCx * v11_3_0 + WQx * v11_3_1 + (VT)2.0 * oo2ze * v5_3_1;
+            const VT v11_6_1 = QCx * v11_3_1 + WQx * v11_3_2 + (VT)2.0 * oo2ze * v5_3_2;
+            const VT v12_6_0 = QCx * v12_3_0 + WQx * v12_3_1 + (VT)2.0 * oo2ze * v6_3_1;
+            const VT v12_6_1 = QCx * v12_3_1 + WQx * v12_3_2 + (VT)2.0 * oo2ze * v6_3_2;
+            const VT v13_6_0 = QCx * v13_3_0 + WQx * v13_3_1 + (VT)1.0 * oo2ze * v7_3_1;
+            const VT v13_6_1 = QCx * v13_3_1 + WQx * v13_3_2 + (VT)1.0 * oo2ze * v7_3_2;
+            const VT v14_6_0 = QCx * v14_3_0 + WQx * v14_3_1 + (VT)1.0 * oo2ze * v9_3_1;
+            const VT v14_6_1 = QCx * v14_3_1 + WQx * v14_3_2 + (VT)1.0 * oo2ze * v9_3_2;
+            const VT v15_6_0 = QCx * v15_3_0 + WQx * v15_3_1 + (VT)1.0 * oo2ze * v8_3_1;
+            const VT v15_6_1 = QCx * v15_3_1 + WQx * v15_3_2 + (VT)1.0 * oo2ze * v8_3_2;
+            const VT v16_6_0 = QCx * v16_3_0 + WQx * v16_3_1;
+            const VT v16_6_1 = QCx * v16_3_1 + WQx * v16_3_2;
+            const VT v17_6_0 = QCx * v17_3_0 + WQx * v17_3_1;
+            const VT v17_6_1 = QCx * v17_3_1 + WQx * v17_3_2;
+            const VT v18_6_0 = QCx * v18_3_0 + WQx * v18_3_1;
+            const VT v18_6_1 = QCx * v18_3_1 + WQx * v18_3_2;
+            const VT v19_6_0 = QCx * v19_3_0 + WQx * v19_3_1;
+            const VT v19_6_1 = QCx * v19_3_1 + WQx * v19_3_2;
+            const VT v4_7_1 = QCy * v4_2_1 + WQy * v4_2_2 + (VT)1.0 * oo2e * (v4_0_1 - rho_e * v4_0_2);
+            const VT v5_7_1 = QCy * v5_2_1 + WQy * v5_2_2 + (VT)1.0 * oo2ze * v1_2_2 + (VT)1.0 * oo2e * (v5_0_1 - rho_e * v5_0_2);
+            const VT v6_7_1 = QCy * v6_2_1 + WQy * v6_2_2 + (VT)1.0 * oo2e * (v6_0_1 - rho_e * v6_0_2);
+            const VT v7_7_1 = QCy * v7_2_1 + WQy * v7_2_2 + (VT)2.0 * oo2ze * v2_2_2 + (VT)1.0 * oo2e * (v7_0_1 - rho_e * v7_0_2);
+            const VT v8_7_1 = QCy * v8_2_1 + WQy * v8_2_2 + (VT)1.0 * oo2ze * v3_2_2 + (VT)1.0 * oo2e * (v8_0_1 - rho_e * v8_0_2);
+            const VT v9_7_1 = QCy * v9_2_1 + WQy * v9_2_2 + (VT)1.0 * oo2e * (v9_0_1 - rho_e * v9_0_2);
+            const VT v10_7_0 = QCy * v10_2_0 + WQy * v10_2_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v10_7_1 = QCy * v10_2_1 + WQy * v10_2_2 + (VT)1.0 * oo2e * (v10_0_1 - rho_e * v10_0_2);
+            const VT v11_7_0 = QCy * v11_2_0 + WQy * v11_2_1 + (VT)1.0 * oo2ze * v4_2_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v11_7_1 = QCy * v11_2_1 + WQy * v11_2_2 + (VT)1.0 * oo2ze * v4_2_2 + (VT)1.0 * oo2e * (v11_0_1 - rho_e * v11_0_2);
+            const VT v12_7_0 = QCy * v12_2_0 + WQy * v12_2_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v12_7_1 = QCy * v12_2_1 + WQy * v12_2_2 + (VT)1.0 * oo2e * (v12_0_1 - rho_e * v12_0_2);
+            const VT v13_7_0 = QCy * v13_2_0 + WQy * v13_2_1 + (VT)2.0 * oo2ze * v5_2_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v13_7_1 = QCy * v13_2_1 + WQy * v13_2_2 + (VT)2.0 * oo2ze * v5_2_2 + (VT)1.0 * oo2e * (v13_0_1 - rho_e * v13_0_2);
+            const VT v14_7_0 = QCy * v14_2_0 + WQy * v14_2_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v14_7_1 = QCy * v14_2_1 + WQy * v14_2_2 + (VT)1.0 * oo2e * (v14_0_1 - rho_e * v14_0_2);
+            const VT v15_7_0 = QCy * v15_2_0 + WQy * v15_2_1 + (VT)1.0 * oo2ze * v6_2_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v15_7_1 = QCy * v15_2_1 + WQy * v15_2_2 + (VT)1.0 * oo2ze * v6_2_2 + (VT)1.0 * oo2e * (v15_0_1 - rho_e * v15_0_2);
+            const VT v16_7_0 = QCy * v16_2_0 + WQy * v16_2_1 + (VT)3.0 * oo2ze * v7_2_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v16_7_1 = QCy * v16_2_1 + WQy * v16_2_2 + (VT)3.0 * oo2ze * v7_2_2 + (VT)1.0 * oo2e * (v16_0_1 - rho_e * v16_0_2);
+            const VT v17_7_0 = QCy * v17_2_0 + WQy * v17_2_1 + (VT)2.0 * oo2ze * v8_2_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v17_7_1 = QCy * v17_2_1 + WQy * v17_2_2 + (VT)2.0 * oo2ze * v8_2_2 + (VT)1.0 * oo2e * (v17_0_1 - rho_e * v17_0_2);
+            const VT v18_7_0 = QCy * v18_2_0 + WQy * v18_2_1 + (VT)1.0 * oo2ze * v9_2_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v18_7_1 = QCy * v18_2_1 + WQy * v18_2_2 + (VT)1.0 * oo2ze * v9_2_2 + (VT)1.0 * oo2e * (v18_0_1 - rho_e * v18_0_2);
+            const VT v19_7_0 = QCy * v19_2_0 + WQy * v19_2_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v19_7_1 = QCy * v19_2_1 + WQy * v19_2_2 + (VT)1.0 * oo2e * (v19_0_1 - rho_e * v19_0_2);
+            const VT v4_8_1 = QCy * v4_3_1 + WQy * v4_3_2;
+            const VT v5_8_1 = QCy * v5_3_1 + WQy * v5_3_2 + (VT)1.0 * oo2ze * v1_3_2;
+            const VT v6_8_1 = QCy * v6_3_1 + WQy * v6_3_2;
+            const VT v7_8_1 = QCy * v7_3_1 + WQy * v7_3_2 + (VT)2.0 * oo2ze * v2_3_2;
+            const VT v8_8_1 = QCy * v8_3_1 + WQy * v8_3_2 + (VT)1.0 * oo2ze * v3_3_2;
+            const VT v9_8_1 = QCy * v9_3_1 + WQy * v9_3_2;
+            const VT v10_8_0 = QCy * v10_3_0 + WQy * v10_3_1;
+            const VT v10_8_1 = QCy * v10_3_1 + WQy * v10_3_2;
+            const VT v11_8_0 = QCy * v11_3_0 + WQy * v11_3_1 + (VT)1.0 * oo2ze * v4_3_1;
+            const VT v11_8_1 = QCy * v11_3_1 + WQy * v11_3_2 + (VT)1.0 * oo2ze * v4_3_2;
+            const VT v12_8_0 = QCy * v12_3_0 + WQy * v12_3_1;
+            const VT v12_8_1 = QCy * v12_3_1 + WQy * v12_3_2;
+            const VT v13_8_0 = QCy * v13_3_0 + WQy * v13_3_1 + (VT)2.0 * oo2ze * v5_3_1;
+            const VT v13_8_1 = QCy * v13_3_1 + WQy * v13_3_2 + (VT)2.0 * oo2ze * v5_3_2;
+            const VT v14_8_0 = QCy * v14_3_0 + WQy * v14_3_1;
+            const VT v14_8_1 = QCy * v14_3_1 + WQy * v14_3_2;
+            const VT v15_8_0 = QCy * v15_3_0 + WQy * v15_3_1 + (VT)1.0 * oo2ze * v6_3_1;
+            const VT v15_8_1 = QCy * v15_3_1 + WQy * v15_3_2 + (VT)1.0 * oo2ze * v6_3_2;
+            const VT v16_8_0 = QCy * v16_3_0 + WQy * v16_3_1 + (VT)3.0 * oo2ze * v7_3_1;
+            const VT v16_8_1 = QCy * v16_3_1 + WQy * v16_3_2 + (VT)3.0 * oo2ze * v7_3_2;
+            const VT v17_8_0 = QCy * v17_3_0 + WQy * v17_3_1 + (VT)2.0 * oo2ze * v8_3_1;
+            const VT v17_8_1 = QCy * v17_3_1 + WQy * v17_3_2 + (VT)2.0 * oo2ze * v8_3_2;
+            const VT v18_8_0 = QCy * v18_3_0 + WQy * v18_3_1 + (VT)1.0 * oo2ze * v9_3_1;
+            const VT v18_8_1 = QCy * v18_3_1 + WQy * v18_3_2 + (VT)1.0 * oo2ze * v9_3_2;
+            const VT v19_8_0 = QCy * v19_3_0 + WQy * v19_3_1;
+            const VT v19_8_1 = QCy * v19_3_1 + WQy * v19_3_2;
+            const VT v4_9_1 = QCz * v4_3_1 + WQz * v4_3_2 + (VT)1.0 * oo2e * (v4_0_1 - rho_e * v4_0_2);
+            const VT v5_9_1 = QCz * v5_3_1 + WQz * v5_3_2 + (VT)1.0 * oo2e * (v5_0_1 - rho_e * v5_0_2);
+            const VT v6_9_1 = QCz * v6_3_1 + WQz * v6_3_2 + (VT)1.0 * oo2ze * v1_3_2 + (VT)1.0 * oo2e * (v6_0_1 - rho_e * v6_0_2);
+            const VT v7_9_1 = QCz * v7_3_1 + WQz * v7_3_2 + (VT)1.0 * oo2e * (v7_0_1 - rho_e * v7_0_2);
+            const VT v8_9_1 = QCz * v8_3_1 + WQz * v8_3_2 + (VT)1.0 * oo2ze * v2_3_2 + (VT)1.0 * oo2e * (v8_0_1 - rho_e * v8_0_2);
+            const VT v9_9_1 = QCz * v9_3_1 + WQz * v9_3_2 + (VT)2.0 * oo2ze * v3_3_2 + (VT)1.0 * oo2e * (v9_0_1 - rho_e * v9_0_2);
+            const VT v10_9_0 = QCz * v10_3_0 + WQz * v10_3_1 + (VT)1.0 * oo2e * (v10_0_0 - rho_e * v10_0_1);
+            const VT v10_9_1 = QCz * v10_3_1 + WQz * v10_3_2 + (VT)1.0 * oo2e * (v10_0_1 - rho_e * v10_0_2);
+            const VT v11_9_0 = QCz * v11_3_0 + WQz * v11_3_1 + (VT)1.0 * oo2e * (v11_0_0 - rho_e * v11_0_1);
+            const VT v11_9_1 = QCz * v11_3_1 + WQz * v11_3_2 + (VT)1.0 * oo2e * (v11_0_1 - rho_e * v11_0_2);
+            const VT v12_9_0 = QCz * v12_3_0 + WQz * v12_3_1 + (VT)1.0 * oo2ze * v4_3_1 + (VT)1.0 * oo2e * (v12_0_0 - rho_e * v12_0_1);
+            const VT v12_9_1 = QCz * v12_3_1 + WQz * v12_3_2 + (VT)1.0 * oo2ze * v4_3_2 + (VT)1.0 * oo2e * (v12_0_1 - rho_e * v12_0_2);
+            const VT v13_9_0 = QCz * v13_3_0 + WQz * v13_3_1 + (VT)1.0 * oo2e * (v13_0_0 - rho_e * v13_0_1);
+            const VT v13_9_1 = QCz * v13_3_1 + WQz * v13_3_2 + (VT)1.0 * oo2e * (v13_0_1 - rho_e * v13_0_2);
+            const VT v14_9_0 = QCz * v14_3_0 + WQz * v14_3_1 + (VT)2.0 * oo2ze * v6_3_1 + (VT)1.0 * oo2e * (v14_0_0 - rho_e * v14_0_1);
+            const VT v14_9_1 = QCz * v14_3_1 + WQz * v14_3_2 + (VT)2.0 * oo2ze * v6_3_2 + (VT)1.0 * oo2e * (v14_0_1 - rho_e * v14_0_2);
+            const VT v15_9_0 = QCz * v15_3_0 + WQz * v15_3_1 + (VT)1.0 * oo2ze * v5_3_1 + (VT)1.0 * oo2e * (v15_0_0 - rho_e * v15_0_1);
+            const VT v15_9_1 = QCz * v15_3_1 + WQz * v15_3_2 + (VT)1.0 * oo2ze * v5_3_2 + (VT)1.0 * oo2e * (v15_0_1 - rho_e * v15_0_2);
+            const VT v16_9_0 = QCz * v16_3_0 + WQz * v16_3_1 + (VT)1.0 * oo2e * (v16_0_0 - rho_e * v16_0_1);
+            const VT v16_9_1 = QCz * v16_3_1 + WQz * v16_3_2 + (VT)1.0 * oo2e * (v16_0_1 - rho_e * v16_0_2);
+            const VT v17_9_0 = QCz * v17_3_0 + WQz * v17_3_1 + (VT)1.0 * oo2ze * v7_3_1 + (VT)1.0 * oo2e * (v17_0_0 - rho_e * v17_0_1);
+            const VT v17_9_1 = QCz * v17_3_1 + WQz * v17_3_2 + (VT)1.0 * oo2ze * v7_3_2 + (VT)1.0 * oo2e * (v17_0_1 - rho_e * v17_0_2);
+            const VT v18_9_0 = QCz * v18_3_0 + WQz * v18_3_1 + (VT)2.0 * oo2ze * v8_3_1 + (VT)1.0 * oo2e * (v18_0_0 - rho_e * v18_0_1);
+            const VT v18_9_1 = QCz * v18_3_1 + WQz * v18_3_2 + (VT)2.0 * oo2ze * v8_3_2 + (VT)1.0 * oo2e * (v18_0_1 - rho_e * v18_0_2);
+            const VT v19_9_0 = QCz * v19_3_0 + WQz * v19_3_1 + (VT)3.0 * oo2ze * v9_3_1 + (VT)1.0 * oo2e * (v19_0_0 - rho_e * v19_0_1);
+            const VT v19_9_1 = QCz * v19_3_1 + WQz * v19_3_2 + (VT)3.0 * oo2ze * v9_3_2 + (VT)1.0 * oo2e * (v19_0_1 - rho_e * v19_0_2);
+            const VT v10_10_0 = QCx * v10_4_0 + WQx * v10_4_1 + (VT)3.0 * oo2ze * v4_4_1 + (VT)2.0 * oo2e * (v10_1_0 - rho_e * v10_1_1);
+            const VT v11_10_0 = QCx * v11_4_0 + WQx * v11_4_1 + (VT)2.0 * oo2ze * v5_4_1 + (VT)2.0 * oo2e * (v11_1_0 - rho_e * v11_1_1);
+            const VT v12_10_0 = QCx * v12_4_0 + WQx * v12_4_1 + (VT)2.0 * oo2ze * v6_4_1 + (VT)2.0 * oo2e * (v12_1_0 - rho_e * v12_1_1);
+            const VT v13_10_0 = QCx * v13_4_0 + WQx * v13_4_1 + (VT)1.0 * oo2ze * v7_4_1 + (VT)2.0 * oo2e * (v13_1_0 - rho_e * v13_1_1);
+            const VT v14_10_0 = QCx * v14_4_0 + WQx * v14_4_1 + (VT)1.0 * oo2ze * v9_4_1 + (VT)2.0 * oo2e * (v14_1_0 - rho_e * v14_1_1);
+            const VT v15_10_0 = QCx * v15_4_0 + WQx * v15_4_1 + (VT)1.0 * oo2ze * v8_4_1 + (VT)2.0 * oo2e * (v15_1_0 - rho_e * v15_1_1);
+            const VT v16_10_0 = QCx * v16_4_0 + WQx * v16_4_1 + (VT)2.0 * oo2e * (v16_1_0 - rho_e * v16_1_1);
+            const VT v17_10_0 = QCx * v17_4_0 + WQx * v17_4_1 + (VT)2.0 * oo2e * (v17_1_0 - rho_e * v17_1_1);
+            const VT v18_10_0 = QCx * v18_4_0 + WQx * v18_4_1 + (VT)2.0 * oo2e * (v18_1_0 - rho_e * v18_1_1);
+            const VT v19_10_0 = QCx * v19_4_0 + WQx * v19_4_1 + (VT)2.0 * oo2e * (v19_1_0 - rho_e * v19_1_1);
+            const VT v10_11_0 = QCx * v10_5_0 + WQx * v10_5_1 + (VT)3.0 * oo2ze * v4_5_1 + (VT)1.0 * oo2e * (v10_2_0 - rho_e * v10_2_1);
+            const VT v11_11_0 = QCx * v11_5_0 + WQx * v11_5_1 + (VT)2.0 * oo2ze * v5_5_1 + (VT)1.0 * oo2e * (v11_2_0 - rho_e * v11_2_1);
+            const VT v12_11_0 = QCx * v12_5_0 + WQx * v12_5_1 + (VT)2.0 * oo2ze * v6_5_1 + (VT)1.0 * oo2e * (v12_2_0 - rho_e * v12_2_1);
+            const VT v13_11_0 = QCx * v13_5_0 + WQx * v13_5_1 + (VT)1.0 * oo2ze * v7_5_1 + (VT)1.0 * oo2e * (v13_2_0 - rho_e * v13_2_1);
+            const VT v14_11_0 = QCx * v14_5_0 + WQx * v14_5_1 + (VT)1.0 * oo2ze * v9_5_1 + (VT)1.0 * oo2e * (v14_2_0 - rho_e * v14_2_1);
+            const VT v15_11_0 = QCx * v15_5_0 + WQx * v15_5_1 + (VT)1.0 * oo2ze * v8_5_1 + (VT)1.0 * oo2e * (v15_2_0 - rho_e * v15_2_1);
+            const VT v16_11_0 = QCx * v16_5_0 + WQx * v16_5_1 + (VT)1.0 * oo2e * (v16_2_0 - rho_e * v16_2_1);
+            const VT v17_11_0 = QCx * v17_5_0 + WQx * v17_5_1 + (VT)1.0 * oo2e * (v17_2_0 - rho_e * v17_2_1);
+            const VT v18_11_0 = QCx * v18_5_0 + WQx * v18_5_1 + (VT)1.0 * oo2e * (v18_2_0 - rho_e * v18_2_1);
+            const VT v19_11_0 = QCx * v19_5_0 + WQx * v19_5_1 + (VT)1.0 * oo2e * (v19_2_0 - rho_e * v19_2_1);
+            const VT v10_12_0 = QCx * v10_6_0 + WQx * v10_6_1 + (VT)3.0 * oo2ze * v4_6_1 + (VT)1.0 * oo2e * (v10_3_0 - rho_e * v10_3_1);
+            const VT v11_12_0 = QCx * v11_6_0 + WQx * v11_6_1 + (VT)2.0 * oo2ze * v5_6_1 + (VT)1.0 * oo2e * (v11_3_0 - rho_e * v11_3_1);
+            const VT v12_12_0 = QCx * v12_6_0 + WQx * v12_6_1 + (VT)2.0 * oo2ze * v6_6_1 + (VT)1.0 * oo2e * (v12_3_0 - rho_e * v12_3_1);
+            const VT v13_12_0 = QCx * v13_6_0 + WQx * v13_6_1 + (VT)1.0 * oo2ze * v7_6_1 + (VT)1.0 * oo2e * (v13_3_0 - rho_e * v13_3_1);
+            const VT v14_12_0 = QCx * v14_6_0 + WQx * v14_6_1 + (VT)1.0 * oo2ze * v9_6_1 + (VT)1.0 * oo2e * (v14_3_0 - rho_e * v14_3_1);
+            const VT v15_12_0 = QCx * v15_6_0 + WQx * v15_6_1 + (VT)1.0 * oo2ze * v8_6_1 + (VT)1.0 * oo2e * (v15_3_0 - rho_e * v15_3_1);
+            const VT v16_12_0 = QCx * v16_6_0 + WQx * v16_6_1 + (VT)1.0 * oo2e * (v16_3_0 - rho_e * v16_3_1);
+            const VT v17_12_0 = QCx * v17_6_0 + WQx * v17_6_1 + (VT)1.0 * oo2e * (v17_3_0 - rho_e * v17_3_1);
+            const VT v18_12_0 = QCx * v18_6_0 + WQx * v18_6_1 + (VT)1.0 * oo2e * (v18_3_0 - rho_e * v18_3_1);
+            const VT v19_12_0 = QCx * v19_6_0 + WQx * v19_6_1 + (VT)1.0 * oo2e * (v19_3_0 - rho_e * v19_3_1);
+            const VT v10_13_0 = QCy * v10_5_0 + WQy * v10_5_1 + (VT)1.0 * oo2e * (v10_1_0 - rho_e * v10_1_1);
+            const VT v11_13_0 = QCy * v11_5_0 + WQy * v11_5_1 + (VT)1.0 * oo2ze * v4_5_1 + (VT)1.0 * oo2e * (v11_1_0 - rho_e * v11_1_1);
+            const VT v12_13_0 = QCy * v12_5_0 + WQy * v12_5_1 + (VT)1.0 * oo2e * (v12_1_0 - rho_e * v12_1_1);
+            const VT v13_13_0 = QCy * v13_5_0 + WQy * v13_5_1 + (VT)2.0 * oo2ze * v5_5_1 + (VT)1.0 * oo2e * (v13_1_0 - rho_e * v13_1_1);
+            const VT v14_13_0 = QCy * v14_5_0 + WQy * v14_5_1 + (VT)1.0 * oo2e * (v14_1_0 - rho_e * v14_1_1);
+            const VT v15_13_0 = QCy * v15_5_0 + WQy * v15_5_1 + (VT)1.0 * oo2ze * v6_5_1 + (VT)1.0 * oo2e * (v15_1_0 - rho_e * v15_1_1);
+            const VT v16_13_0 = QCy * v16_5_0 + WQy * v16_5_1 + (VT)3.0 * oo2ze * v7_5_1 + (VT)1.0 * oo2e * (v16_1_0 - rho_e * v16_1_1);
+            const VT v17_13_0 = QCy * v17_5_0 + WQy * v17_5_1 + (VT)2.0 * oo2ze * v8_5_1 + (VT)1.0 * oo2e * (v17_1_0 - rho_e * v17_1_1);
+            const VT v18_13_0 = QCy * v18_5_0 + WQy * v18_5_1 + (VT)1.0 * oo2ze * v9_5_1 + (VT)1.0 * oo2e * (v18_1_0 - rho_e * v18_1_1);
+            const VT v19_13_0 = QCy * v19_5_0 + WQy * v19_5_1 + (VT)1.0 * oo2e * (v19_1_0 - rho_e * v19_1_1);
+            const VT v10_14_0 = QCz * v10_6_0 + WQz * v10_6_1 + (VT)1.0 * oo2e * (v10_1_0 - rho_e * v10_1_1);
+            const VT v11_14_0 = QCz * v11_6_0 + WQz * v11_6_1 + (VT)1.0 * oo2e * (v11_1_0 - rho_e * v11_1_1);
+            const VT v12_14_0 = QCz * v12_6_0 + WQz * v12_6_1 + (VT)1.0 * oo2ze * v4_6_1 + (VT)1.0 * oo2e * (v12_1_0 - rho_e * v12_1_1);
+            const VT v13_14_0 = QCz * v13_6_0 + WQz * v13_6_1 + (VT)1.0 * oo2e * (v13_1_0 - rho_e * v13_1_1);
+            const VT v14_14_0 = QCz * v14_6_0 + WQz * v14_6_1 + (VT)2.0 * oo2ze * v6_6_1 + (VT)1.0 * oo2e * (v14_1_0 - rho_e * v14_1_1);
+            const VT v15_14_0 = QCz * v15_6_0 + WQz * v15_6_1 + (VT)1.0 * oo2ze * v5_6_1 + (VT)1.0 * oo2e * (v15_1_0 - rho_e * v15_1_1);
+            const VT v16_14_0 = QCz * v16_6_0 + WQz * v16_6_1 + (VT)1.0 * oo2e * (v16_1_0 - rho_e * v16_1_1);
+            const VT v17_14_0 = QCz * v17_6_0 + WQz * v17_6_1 + (VT)1.0 * oo2ze * v7_6_1 + (VT)1.0 * oo2e * (v17_1_0 - rho_e * v17_1_1);
+            const VT v18_14_0 = QCz * v18_6_0 + WQz * v18_6_1 + (VT)2.0 * oo2ze * v8_6_1 + (VT)1.0 * oo2e * (v18_1_0 - rho_e * v18_1_1);
+            const VT v19_14_0 = QCz * v19_6_0 + WQz * v19_6_1 + (VT)3.0 * oo2ze * v9_6_1 + (VT)1.0 * oo2e * (v19_1_0 - rho_e * v19_1_1);
+            const VT v10_15_0 = QCx * v10_8_0 + WQx * v10_8_1 + (VT)3.0 * oo2ze * v4_8_1;
+            const VT v11_15_0 = QCx * v11_8_0 + WQx * v11_8_1 + (VT)2.0 * oo2ze * v5_8_1;
+            const VT v12_15_0 = QCx * v12_8_0 + WQx * v12_8_1 + (VT)2.0 * oo2ze * v6_8_1;
+            const VT v13_15_0 = QCx * v13_8_0 + WQx * v13_8_1 + (VT)1.0 * oo2ze * v7_8_1;
+            const VT v14_15_0 = QCx * v14_8_0 + WQx * v14_8_1 + (VT)1.0 * oo2ze * v9_8_1;
+            const VT v15_15_0 = QCx * v15_8_0 + WQx * v15_8_1 + (VT)1.0 * oo2ze * v8_8_1;
+            const VT v16_15_0 = QCx * v16_8_0 + WQx * v16_8_1;
+            const VT v17_15_0 = QCx * v17_8_0 + WQx * v17_8_1;
+            const VT v18_15_0 = QCx * v18_8_0 + WQx * v18_8_1;
+            const VT v19_15_0 = QCx * v19_8_0 + WQx * v19_8_1;
+            const VT v10_16_0 = QCy * v10_7_0 + WQy * v10_7_1 + (VT)2.0 * oo2e * (v10_2_0 - rho_e * v10_2_1);
+            const VT v11_16_0 = QCy * v11_7_0 + WQy * v11_7_1 + (VT)1.0 * oo2ze * v4_7_1 + (VT)2.0 * oo2e * (v11_2_0 - rho_e * v11_2_1);
+            const VT v12_16_0 = QCy * v12_7_0 + WQy * v12_7_1 + (VT)2.0 * oo2e * (v12_2_0 - rho_e * v12_2_1);
+            const VT v13_16_0 = QCy * v13_7_0 + WQy * v13_7_1 + (VT)2.0 * oo2ze * v5_7_1 + (VT)2.0 * oo2e * (v13_2_0 - rho_e * v13_2_1);
+            const VT v14_16_0 = QCy * v14_7_0 + WQy * v14_7_1 + (VT)2.0 * oo2e * (v14_2_0 - rho_e * v14_2_1);
+            const VT v15_16_0 = QCy * v15_7_0 + WQy * v15_7_1 + (VT)1.0 * oo2ze * v6_7_1 + (VT)2.0 * oo2e * (v15_2_0 - rho_e * v15_2_1);
+            const VT v16_16_0 = QCy * v16_7_0 + WQy * v16_7_1 + (VT)3.0 * oo2ze * v7_7_1 + (VT)2.0 * oo2e * (v16_2_0 - rho_e * v16_2_1);
+            const VT v17_16_0 = QCy * v17_7_0 + WQy * v17_7_1 + (VT)2.0 * oo2ze * v8_7_1 + (VT)2.0 * oo2e * (v17_2_0 - rho_e * v17_2_1);
+            const VT v18_16_0 = QCy * v18_7_0 + WQy * v18_7_1 + (VT)1.0 * oo2ze * v9_7_1 + (VT)2.0 * oo2e * (v18_2_0 - rho_e * v18_2_1);
+            const VT v19_16_0 = QCy * v19_7_0 + WQy * v19_7_1 + (VT)2.0 * oo2e * (v19_2_0 - rho_e * v19_2_1);
+            const VT v10_17_0 = QCy * v10_8_0 + WQy * v10_8_1 + (VT)1.0 * oo2e * (v10_3_0 - rho_e * v10_3_1);
+            const VT v11_17_0 = QCy * v11_8_0 + WQy * v11_8_1 + (VT)1.0 * oo2ze * v4_8_1 + (VT)1.0 * oo2e * (v11_3_0 - rho_e * v11_3_1);
+            const VT v12_17_0 = QCy * v12_8_0 + WQy * v12_8_1 + (VT)1.0 * oo2e * (v12_3_0 - rho_e * v12_3_1);
+            const VT v13_17_0 = QCy * v13_8_0 + WQy * v13_8_1 + (VT)2.0 * oo2ze * v5_8_1 + (VT)1.0 * oo2e * (v13_3_0 - rho_e * v13_3_1);
+            const VT v14_17_0 = QCy * v14_8_0 + WQy * v14_8_1 + (VT)1.0 * oo2e * (v14_3_0 - rho_e * v14_3_1);
+            const VT v15_17_0 = QCy * v15_8_0 + WQy * v15_8_1 + (VT)1.0 * oo2ze * v6_8_1 + (VT)1.0 * oo2e * (v15_3_0 - rho_e * v15_3_1);
+            const VT v16_17_0 = QCy * v16_8_0 + WQy * v16_8_1 + (VT)3.0 * oo2ze * v7_8_1 + (VT)1.0 * oo2e * (v16_3_0 - rho_e * v16_3_1);
+            const VT v17_17_0 = QCy * v17_8_0 + WQy * v17_8_1 + (VT)2.0 * oo2ze * v8_8_1 + (VT)1.0 * oo2e * (v17_3_0 - rho_e * v17_3_1);
+            const VT v18_17_0 = QCy * v18_8_0 + WQy * v18_8_1 + (VT)1.0 * oo2ze * v9_8_1 + (VT)1.0 * oo2e * (v18_3_0 - rho_e * v18_3_1);
+            const VT v19_17_0 = QCy * v19_8_0 + WQy * v19_8_1 + (VT)1.0 * oo2e * (v19_3_0 - rho_e * v19_3_1);
+            const VT v10_18_0 = QCz * v10_8_0 + WQz * v10_8_1 + (VT)1.0 * oo2e * (v10_2_0 - rho_e * v10_2_1);
+            const VT v11_18_0 = QCz * v11_8_0 + WQz * v11_8_1 + (VT)1.0 * oo2e * (v11_2_0 - rho_e * v11_2_1);
+            const VT v12_18_0 = QCz * v12_8_0 + WQz * v12_8_1 + (VT)1.0 * oo2ze * v4_8_1 + (VT)1.0 * oo2e * (v12_2_0 - rho_e * v12_2_1);
+            const VT v13_18_0 = QCz * v13_8_0 + WQz * v13_8_1 + (VT)1.0 * oo2e * (v13_2_0 - rho_e * v13_2_1);
+            const VT v14_18_0 = QCz * v14_8_0 + WQz * v14_8_1 + (VT)2.0 * oo2ze * v6_8_1 + (VT)1.0 * oo2e * (v14_2_0 - rho_e * v14_2_1);
+            const VT v15_18_0 = QCz * v15_8_0 + WQz * v15_8_1 + (VT)1.0 * oo2ze * v5_8_1 + (VT)1.0 * oo2e * (v15_2_0 - rho_e * v15_2_1);
+            const VT v16_18_0 = QCz * v16_8_0 + WQz * v16_8_1 + (VT)1.0 * oo2e * (v16_2_0 - rho_e * v16_2_1);
+            const VT v17_18_0 = QCz * v17_8_0 + WQz * v17_8_1 + (VT)1.0 * oo2ze * v7_8_1 + (VT)1.0 * oo2e * (v17_2_0 - rho_e * v17_2_1);
+            const VT v18_18_0 = QCz * v18_8_0 + WQz * v18_8_1 + (VT)2.0 * oo2ze * v8_8_1 + (VT)1.0 * oo2e * (v18_2_0 - rho_e * v18_2_1);
+            const VT v19_18_0 = QCz * v19_8_0 + WQz * v19_8_1 + (VT)3.0 * oo2ze * v9_8_1 + (VT)1.0 * oo2e * (v19_2_0 - rho_e * v19_2_1);
+            const VT v10_19_0 = QCz * v10_9_0 + WQz * v10_9_1 + (VT)2.0 * oo2e * (v10_3_0 - rho_e * v10_3_1);
+            const VT v11_19_0 = QCz * v11_9_0 + WQz * v11_9_1 + (VT)2.0 * oo2e * (v11_3_0 - rho_e * v11_3_1);
+            const VT v12_19_0 = QCz * v12_9_0 + WQz * v12_9_1 + (VT)1.0 * oo2ze * v4_9_1 + (VT)2.0 * oo2e * (v12_3_0 - rho_e * v12_3_1);
+            const VT v13_19_0 = QCz * v13_9_0 + WQz * v13_9_1 + (VT)2.0 * oo2e * (v13_3_0 - rho_e * v13_3_1);
+            const VT v14_19_0 = QCz * v14_9_0 + WQz * v14_9_1 + (VT)2.0 * oo2ze * v6_9_1 + (VT)2.0 * oo2e * (v14_3_0 - rho_e * v14_3_1);
+            const VT v15_19_0 = QCz * v15_9_0 + WQz * v15_9_1 + (VT)1.0 * oo2ze * v5_9_1 + (VT)2.0 * oo2e * (v15_3_0 - rho_e * v15_3_1);
+            const VT v16_19_0 = QCz * v16_9_0 + WQz * v16_9_1 + (VT)2.0 * oo2e * (v16_3_0 - rho_e * v16_3_1);
+            const VT v17_19_0 = QCz * v17_9_0 + WQz * v17_9_1 + (VT)1.0 * oo2ze * v7_9_1 + (VT)2.0 * oo2e * (v17_3_0 - rho_e * v17_3_1);
+            const VT v18_19_0 = QCz * v18_9_0 + WQz * v18_9_1 + (VT)2.0 * oo2ze * v8_9_1 + (VT)2.0 * oo2e * (v18_3_0 - rho_e * v18_3_1);
+            const VT v19_19_0 = QCz * v19_9_0 + WQz * v19_9_1 + (VT)3.0 * oo2ze * v9_9_1 + (VT)2.0 * oo2e * (v19_3_0 - rho_e * v19_3_1);
+            acc[0] += (double)v10_4_0;
+            acc[1] += (double)v10_5_0;
+            acc[2] += (double)v10_6_0;
+            acc[3] += (double)v10_7_0;
+            acc[4] += (double)v10_8_0;
+            acc[5] += (double)v10_9_0;
+            acc[6] += (double)v10_10_0;
+            acc[7] += (double)v10_11_0;
+            acc[8] += (double)v10_12_0;
+            acc[9] += (double)v10_13_0;
+            acc[10] += (double)v10_14_0;
+            acc[11] += (double)v10_15_0;
+            acc[12] += (double)v10_16_0;
+            acc[13] += (double)v10_17_0;
+            acc[14] += (double)v10_18_0;
+            acc[15] += (double)v10_19_0;
+            acc[16] += (double)v11_4_0;
+            acc[17] += (double)v11_5_0;
+            acc[18] += (double)v11_6_0;
+            acc[19] += (double)v11_7_0;
+            acc[20] += (double)v11_8_0;
+            acc[21] += (double)v11_9_0;
+            acc[22] += (double)v11_10_0;
+            acc[23] += (double)v11_11_0;
+            acc[24] += (double)v11_12_0;
+            acc[25] += (double)v11_13_0;
+            acc[26] += (double)v11_14_0;
+            acc[27] += (double)v11_15_0;
+            acc[28] += (double)v11_16_0;
+            acc[29] += (double)v11_17_0;
+            acc[30] += (double)v11_18_0;
+            acc[31] += (double)v11_19_0;
+            acc[32] += (double)v12_4_0;
+            acc[33] += (double)v12_5_0;
+            acc[34] += (double)v12_6_0;
+            acc[35] += (double)v12_7_0;
+            acc[36] += (double)v12_8_0;
+            acc[37] += (double)v12_9_0;
+            acc[38] += (double)v12_10_0;
+            acc[39] += (double)v12_11_0;
+            acc[40] += (double)v12_12_0;
+            acc[41] += (double)v12_13_0;
+            acc[42] += (double)v12_14_0;
+            acc[43] += (double)v12_15_0;
+            acc[44] += (double)v12_16_0;
+            acc[45] += (double)v12_17_0;
+            acc[46] += (double)v12_18_0;
+            acc[47] += (double)v12_19_0;
+            acc[48] += (double)v13_4_0;
+            acc[49] += (double)v13_5_0;
+            acc[50] += (double)v13_6_0;
+            acc[51] += (double)v13_7_0;
+            acc[52] += (double)v13_8_0;
+            acc[53] += (double)v13_9_0;
+            acc[54] += (double)v13_10_0;
+            acc[55] += (double)v13_11_0;
+            acc[56] += (double)v13_12_0;
+            acc[57] += (double)v13_13_0;
+            acc[58] += (double)v13_14_0;
+            acc[59] += (double)v13_15_0;
+            acc[60] += (double)v13_16_0;
+            acc[61] += (double)v13_17_0;
+            acc[62] += (double)v13_18_0;
+            acc[63] += (double)v13_19_0;
+            acc[64] += (double)v14_4_0;
+            acc[65] += (double)v14_5_0;
+            acc[66] += (double)v14_6_0;
+            acc[67] += (double)v14_7_0;
+            acc[68] += (double)v14_8_0;
+            acc[69] += (double)v14_9_0;
+            acc[70] += (double)v14_10_0;
+            acc[71] += (double)v14_11_0;
+            acc[72] += (double)v14_12_0;
+            acc[73] += (double)v14_13_0;
+            acc[74] += (double)v14_14_0;
+            acc[75] += (double)v14_15_0;
+            acc[76] += (double)v14_16_0;
+            acc[77] += (double)v14_17_0;
+            acc[78] += (double)v14_18_0;
+            acc[79] += (double)v14_19_0;
+            acc[80] += (double)v15_4_0;
+            acc[81] += (double)v15_5_0;
+            acc[82] += (double)v15_6_0;
+            acc[83] += (double)v15_7_0;
+            acc[84] += (double)v15_8_0;
+            acc[85] += (double)v15_9_0;
+            acc[86] += (double)v15_10_0;
+            acc[87] += (double)v15_11_0;
+            acc[88] += (double)v15_12_0;
+            acc[89] += (double)v15_13_0;
+            acc[90] += (double)v15_14_0;
+            acc[91] += (double)v15_15_0;
+            acc[92] += (double)v15_16_0;
+            acc[93] += (double)v15_17_0;
+            acc[94] += (double)v15_18_0;
+            acc[95] += (double)v15_19_0;
+            acc[96] += (double)v16_4_0;
+            acc[97] += (double)v16_5_0;
+            acc[98] += (double)v16_6_0;
+            acc[99] += (double)v16_7_0;
+            acc[100] += (double)v16_8_0;
+            acc[101] += (double)v16_9_0;
+            acc[102] += (double)v16_10_0;
+            acc[103] += (double)v16_11_0;
+            acc[104] += (double)v16_12_0;
+            acc[105] += (double)v16_13_0;
+            acc[106] += (double)v16_14_0;
+            acc[107] += (double)v16_15_0;
+            acc[108] += (double)v16_16_0;
+            acc[109] += (double)v16_17_0;
+            acc[110] += (double)v16_18_0;
+            acc[111] += (double)v16_19_0;
+            acc[112] += (double)v17_4_0;
+            acc[113] += (double)v17_5_0;
+            acc[114] += (double)v17_6_0;
+            acc[115] += (double)v17_7_0;
+            acc[116] += (double)v17_8_0;
+            acc[117] += (double)v17_9_0;
+            acc[118] += (double)v17_10_0;
+            acc[119] += (double)v17_11_0;
+            acc[120] += (double)v17_12_0;
+            acc[121] += (double)v17_13_0;
+            acc[122] += (double)v17_14_0;
+            acc[123] += (double)v17_15_0;
+            acc[124] += (double)v17_16_0;
+            acc[125] += (double)v17_17_0;
+            acc[126] += (double)v17_18_0;
+            acc[127] += (double)v17_19_0;
+            acc[128] += (double)v18_4_0;
+            acc[129] += (double)v18_5_0;
+            acc[130] += (double)v18_6_0;
+            acc[131] += (double)v18_7_0;
+            acc[132] += (double)v18_8_0;
+            acc[133] += (double)v18_9_0;
+            acc[134] += (double)v18_10_0;
+            acc[135] += (double)v18_11_0;
+            acc[136] += (double)v18_12_0;
+            acc[137] += (double)v18_13_0;
+            acc[138] += (double)v18_14_0;
+            acc[139] += (double)v18_15_0;
+            acc[140] += (double)v18_16_0;
+            acc[141] += (double)v18_17_0;
+            acc[142] += (double)v18_18_0;
+            acc[143] += (double)v18_19_0;
+            acc[144] += (double)v19_4_0;
+            acc[145] += (double)v19_5_0;
+            acc[146] += (double)v19_6_0;
+            acc[147] += (double)v19_7_0;
+            acc[148] += (double)v19_8_0;
+            acc[149] += (double)v19_9_0;
+            acc[150] += (double)v19_10_0;
+            acc[151] += (double)v19_11_0;
+            acc[152] += (double)v19_12_0;
+            acc[153] += (double)v19_13_0;
+            acc[154] += (double)v19_14_0;
+            acc[155] += (double)v19_15_0;
+            acc[156] += (double)v19_16_0;
+            acc[157] += (double)v19_17_0;
+            acc[158] += (double)v19_18_0;
+            acc[159] += (double)v19_19_0;
+        }
+    }
+    if (acc_out) {
+#pragma unroll
+        for (int x = 0; x < 160; ++x) acc_out[x] = acc[x];
+    }
+    const double4 gb = ldg4(&P.geo[p]);
+    const double4 gk = ldg4(&P.geo[q]);
+    const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
+    const double CDx = gk.x, CDy = gk.y, CDz = gk.z;
+    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
+    const double k10_0_4_1 = acc[6] + CDx * acc[0];
+    const double k10_0_4_2 = acc[7] + CDy * acc[0];
+    const double k10_0_4_3 = acc[8] + CDz * acc[0];
+    const double k10_0_5_1 = acc[7] + CDx * acc[1];
+    const double k10_0_5_2 = acc[9] + CDy * acc[1];
+    const double k10_0_5_3 = acc[11] + CDz * acc[1];
+    const double k10_0_6_1 = acc[8] + CDx * acc[2];
+    const double k10_0_6_2 = acc[11] + CDy * acc[2];
+    const double k10_0_6_3 = acc[10] + CDz * acc[2];
+    const double k10_0_7_1 = acc[9] + CDx * acc[3];
+    const double k10_0_7_2 = acc[12] + CDy * acc[3];
+    const double k10_0_7_3 = acc[13] + CDz * acc[3];
+    const double k10_0_8_1 = acc[11] + CDx * acc[4];
+    const double k10_0_8_2 = acc[13] + CDy * acc[4];
+    const double k10_0_8_3 = acc[14] + CDz * acc[4];
+    const double k10_0_9_1 = acc[10] + CDx * acc[5];
+    const double k10_0_9_2 = acc[14] + CDy * acc[5];
+    const double k10_0_9_3 = acc[15] + CDz * acc[5];
+    const double k11_0_4_1 = acc[22] + CDx * acc[16];
+    const double k11_0_4_2 = acc[23] + CDy * acc[16];
+    const double k11_0_4_3 = acc[24] + CDz * acc[16];
+    const double k11_0_5_1 = acc[23] + CDx * acc[17];
+    const double k11_0_5_2 = acc[25] + CDy * acc[17];
+    const double k11_0_5_3 = acc[27] + CDz * acc[17];
+    const double k11_0_6_1 = acc[24] + CDx * acc[18];
+    const double k11_0_6_2 = acc[27] + CDy * acc[18];
+    const double k11_0_6_3 = acc[26] + CDz * acc[18];
+    const double k11_0_7_1 = acc[25] + CDx * acc[19];
+    const double k11_0_7_2 = acc[28] + CDy * acc[19];
+    const double k11_0_7_3 = acc[29] + CDz * acc[19];
+    const double k11_0_8_1 = acc[27] + CDx * acc[20];
+    const double k11_0_8_2 = acc[29] + CDy * acc[20];
+    const double k11_0_8_3 = acc[30] + CDz * acc[20];
+    const double k11_0_9_1 = acc[26] + CDx * acc[21];
+    const double k11_0_9_2 = acc[30] + CDy * acc[21];
+    const double k11_0_9_3 = acc[31] + CDz * acc[21];
+    const double k12_0_4_1 = acc[38] + CDx * acc[32];
+    const double k12_0_4_2 = acc[39] + CDy * acc[32];
+    const double k12_0_4_3 = acc[40] + CDz * acc[32];
+    const double k12_0_5_1 = acc[39] + CDx * acc[33];
+    const double k12_0_5_2 = acc[41] + CDy * acc[33];
+    const double k12_0_5_3 = acc[43] + CDz * acc[33];
+    const double k12_0_6_1 = acc[40] + CDx * acc[34];
+    const double k12_0_6_2 = acc[43] + CDy * acc[34];
+    const double k12_0_6_3 = acc[42] + CDz * acc[34];
+    const double k12_0_7_1 = acc[41] + CDx * acc[35];
+    const double k12_0_7_2 = acc[44] + CDy * acc[35];
+    const double k12_0_7_3 = acc[45] + CDz * acc[35];
+    const double k12_0_8_1 = acc[43] + CDx * acc[36];
+    const double k12_0_8_2 = acc[45] + CDy * acc[36];
+    const double k12_0_8_3 = acc[46] + CDz * acc[36];
+    const double k12_0_9_1 = acc[42] + CDx * acc[37];
+    const double k12_0_9_2 = acc[46] + CDy * acc[37];
+    const double k12_0_9_3 = acc[47] + CDz * acc[37];
+    const double k13_0_4_1 = acc[54] + CDx * acc[48];
+    const double k13_0_4_2 = acc[55] + CDy * acc[48];
+    const double k13_0_4_3 = acc[56] + CDz * acc[48];
+    const double k13_0_5_1 = acc[55] + CDx * acc[49];
+    const double k13_0_5_2 = acc[57] + CDy * acc[49];
+    const double k13_0_5_3 = acc[59] + CDz * acc[49];
+    const double k13_0_6_1 = acc[56] + CDx * acc[50];
+    const double k13_0_6_2 = acc[59] + CDy * acc[50];
+    const double k13_0_6_3 = acc[58] + CDz * acc[50];
+    const double k13_0_7_1 = acc[57] + CDx * acc[51];
+    const double k13_0_7_2 = acc[60] + CDy * acc[51];
+    const double k13_0_7_3 = acc[61] + CDz * acc[51];
+    const double k13_0_8_1 = acc[59] + CDx * acc[52];
+    const double k13_0_8_2 = acc[61] + CDy * acc[52];
+    const double k13_0_8_3 = acc[62] + CDz * acc[52];
+    const double k13_0_9_1 = acc[58] + CDx * acc[53];
+    const double k13_0_9_2 = acc[62] + CDy * acc[53];
+    const double k13_0_9_3 = acc[63] + CDz * acc[53];
+    const double k14_0_4_1 = acc[70] + CDx * acc[64];
+    const double k14_0_4_2 = acc[71] + CDy * acc[64];
+    const double k14_0_4_3 = acc[72] + CDz * acc[64];
+    const double k14_0_5_1 = acc[71] + CDx * acc[65];
+    const double k14_0_5_2 = acc[73] + CDy * acc[65];
+    const double k14_0_5_3 = acc[75] + CDz * acc[65];
+    const double k14_0_6_1 = acc[72] + CDx * acc[66];
+    const double k14_0_6_2 = acc[75] + CDy * acc[66];
+    const double k14_0_6_3 = acc[74] + CDz * acc[66];
+    const double k14_0_7_1 = acc[73] + CDx * acc[67];
+    const double k14_0_7_2 = acc[76] + CDy * acc[67];
+    const double k14_0_7_3 = acc[77] + CDz * acc[67];
+    const double k14_0_8_1 = acc[75] + CDx * acc[68];
+    const double k14_0_8_2 = acc[77] + CDy * acc[68];
+    const double k14_0_8_3 = acc[78] + CDz * acc[68];
+    const double k14_0_9_1 = acc[74] + CDx * acc[69];
+    const double k14_0_9_2 = acc[78] + CDy * acc[69];
+    const double k14_0_9_3 = acc[79] + CDz * acc[69];
+    const double k15_0_4_1 = acc[86] + CDx * acc[80];
+    const double k15_0_4_2 = acc[87] + CDy * acc[80];
+    const double k15_0_4_3 = acc[88] + CDz * acc[80];
+    const double k15_0_5_1 = acc[87] + CDx * acc[81];
+    const double k15_0_5_2 = acc[89] + CDy * acc[81];
+    const double k15_0_5_3 = acc[91] + CDz * acc[81];
+    const double k15_0_6_1 = acc[88] + CDx * acc[82];
+    const double k15_0_6_2 = acc[91] + CDy * acc[82];
+    const double k15_0_6_3 = acc[90] + CDz * acc[82];
+    const double k15_0_7_1 = acc[89] + CDx * acc[83];
+    const double k15_0_7_2 = acc[92] + CDy * acc[83];
+    const double k15_0_7_3 = acc[93] + CDz * acc[83];
+    const double k15_0_8_1 = acc[91] + CDx * acc[84];
+    const double k15_0_8_2 = acc[93] + CDy * acc[84];
+    const double k15_0_8_3 = acc[94] + CDz * acc[84];
+    const double k15_0_9_1 = acc[90] + CDx * acc[85];
+    const double k15_0_9_2 = acc[94] + CDy * acc[85];
+    const double k15_0_9_3 = acc[95] + CDz * acc[85];
+    const double k16_0_4_1 = acc[102] + CDx * acc[96];
+    const double k16_0_4_2 = acc[103] + CDy * acc[96];
+    const double k16_0_4_3 = acc[104] + CDz * acc[96];
+    const double k16_0_5_1 = acc[103] + CDx * acc[97];
+    const double k16_0_5_2 = acc[105] + CDy * acc[97];
+    const double k16_0_5_3 = acc[107] + CDz * acc[97];
+    const double k16_0_6_1 = acc[104] + CDx * acc[98];
+    const double k16_0_6_2 = acc[107] + CDy * acc[98];
+    const double k16_0_6_3 = acc[106] + CDz * acc[98];
+    const double k16_0_7_1 = acc[105] + CDx * acc[99];
+    const double k16_0_7_2 = acc[108] + CDy * acc[99];
+    const double k16_0_7_3 = acc[109] + CDz * acc[99];
+    const double k16_0_8_1 = acc[107] + CDx * acc[100];
+    const double k16_0_8_2 = acc[109] + CDy * acc[100];
+    const double k16_0_8_3 = acc[110] + CDz * acc[100];
+    const double k16_0_9_1 = acc[106] + CDx * acc[101];
+    const double k16_0_9_2 = acc[110] + CDy * acc[101];
+    const double k16_0_9_3 = acc[111] + CDz * acc[101];
+    const double k17_0_4_1 = acc[118] + CDx * acc[112];
+    const double k17_0_4_2 = acc[119] + CDy * acc[112];
+    const double k17_0_4_3 = acc[120] + CDz * acc[112];
+    const double k17_0_5_1 = acc[119] + CDx * acc[113];
+    const double k17_0_5_2 = acc[121] + CDy * acc[113];
+    const double k17_0_5_3 = acc[123] + CDz * acc[113];
+    const double k17_0_6_1 = acc[120] + CDx * acc[114];
+    const double k17_0_6_2 = acc[123] + CDy * acc[114];
+    const double k17_0_6_3 = acc[122] + CDz * acc[114];
+    const double k17_0_7_1 = acc[121] + CDx * acc[115];
+    const double k17_0_7_2 = acc[124] + CDy * acc[115];
+    const double k17_0_7_3 = acc[125] + CDz * acc[115];
+    const double k17_0_8_1 = acc[123] + CDx * acc[116];
+    const double k17_0_8_2 = acc[125] + CDy * acc[116];
+    const double k17_0_8_3 = acc[126] + CDz * acc[116];
+    const double k17_0_9_1 = acc[122] + CDx * acc[117];
+    const double k17_0_9_2 = acc[126] + CDy * acc[117];
+    const double k17_0_9_3 = acc[127] + CDz * acc[117];
+    const double k18_0_4_1 = acc[134] + CDx * acc[128];
+    const double k18_0_4_2 = acc[135] + CDy * acc[128];
+    const double k18_0_4_3 = acc[136] + CDz * acc[128];
+    const double k18_0_5_1 = acc[135] + CDx * acc[129];
+    const double k18_0_5_2 = acc[137] + CDy * acc[129];
+    const double k18_0_5_3 = acc[139] + CDz * acc[129];
+    const double k18_0_6_1 = acc[136] + CDx * acc[130];
+    const double k18_0_6_2 = acc[139] + CDy * acc[130];
+    const double k18_0_6_3 = acc[138] + CDz * acc[130];
+    const double k18_0_7_1 = acc[137] + CDx * acc[131];
+    const double k18_0_7_2 = acc[140] + CDy * acc[131];
+    const double k18_0_7_3 = acc[141] + CDz * acc[131];
+    const double k18_0_8_1 = acc[139] + CDx * acc[132];
+    const double k18_0_8_2 = acc[141] + CDy * acc[132];
+    const double k18_0_8_3 = acc[142] + CDz * acc[132];
+    const double k18_0_9_1 = acc[138] + CDx * acc[133];
+    const double k18_0_9_2 = acc[142] + CDy * acc[133];
+    const double k18_0_9_3 = acc[143] + CDz * acc[133];
+    const double k19_0_4_1 = acc[150] + CDx * acc[144];
+    const double k19_0_4_2 = acc[151] + CDy * acc[144];
+    const double k19_0_4_3 = acc[152] + CDz * acc[144];
+    const double k19_0_5_1 = acc[151] + CDx * acc[145];
+    const double k19_0_5_2 = acc[153] + CDy * acc[145];
+    const double k19_0_5_3 = acc[155] + CDz * acc[145];
+    const double k19_0_6_1 = acc[152] + CDx * acc[146];
+    const double k19_0_6_2 = acc[155] + CDy * acc[146];
+    const double k19_0_6_3 = acc[154] + CDz * acc[146];
+    const double k19_0_7_1 = acc[153] + CDx * acc[147];
+    const double k19_0_7_2 = acc[156] + CDy * acc[147];
+    const double k19_0_7_3 = acc[157] + CDz * acc[147];
+    const double k19_0_8_1 = acc[155] + CDx * acc[148];
+    const double k19_0_8_2 = acc[157] + CDy * acc[148];
+    const double k19_0_8_3 = acc[158] + CDz * acc[148];
+    const double k19_0_9_1 = acc[154] + CDx * acc[149];
+    const double k19_0_9_2 = acc[158] + CDy * acc[149];
+    const double k19_0_9_3 = acc[159] + CDz * acc[149];
+    res[0] = k10_0_4_1 * 0.14907119849998599;
+    res[1] = k10_0_4_2 * 0.14907119849998599;
+    res[2] = k10_0_4_3 * 0.14907119849998599;
+    res[3] = k10_0_5_1 * 0.2581988897471611;
+    res[4] = k10_0_5_2 * 0.2581988897471611;
+    res[5] = k10_0_5_3 * 0.2581988897471611;
+    res[6] = k10_0_6_1 * 0.2581988897471611;
+    res[7] = k10_0_6_2 * 0.2581988897471611;
+    res[8] = k10_0_6_3 * 0.2581988897471611;
+    res[9] = k10_0_7_1 * 0.14907119849998599;
+    res[10] = k10_0_7_2 * 0.14907119849998599;
+    res[11] = k10_0_7_3 * 0.14907119849998599;
+    res[12] = k10_0_8_1 * 0.2581988897471611;
+    res[13] = k10_0_8_2 * 0.2581988897471611;
+    res[14] = k10_0_8_3 * 0.2581988897471611;
+    res[15] = k10_0_9_1 * 0.14907119849998599;
+    res[16] = k10_0_9_2 * 0.14907119849998599;
+    res[17] = k10_0_9_3 * 0.14907119849998599;
+    res[18] = k11_0_4_1 * 0.3333333333333334;
+    res[19] = k11_0_4_2 * 0.3333333333333334;
+    res[20] = k11_0_4_3 * 0.3333333333333334;
+    res[21] = k11_0_5_1 * 0.5773502691896258;
+    res[22] = k11_0_5_2 * 0.5773502691896258;
+    res[23] = k11_0_5_3 * 0.5773502691896258;
+    res[24] = k11_0_6_1 * 0.5773502691896258;
+    res[25] = k11_0_6_2 * 0.5773502691896258;
+    res[26] = k11_0_6_3 * 0.5773502691896258;
+    res[27] = k11_0_7_1 * 0.3333333333333334;
+    res[28] = k11_0_7_2 * 0.3333333333333334;
+    res[29] = k11_0_7_3 * 0.3333333333333334;
+    res[30] = k11_0_8_1 * 0.5773502691896258;
+    res[31] = k11_0_8_2 * 0.5773502691896258;
+    res[32] = k11_0_8_3 * 0.5773502691896258;
+    res[33] = k11_0_9_1 * 0.3333333333333334;
+    res[34] = k11_0_9_2 * 0.3333333333333334;
+    res[35] = k11_0_9_3 * 0.3333333333333334;
+    res[36] = k12_0_4_1 * 0.3333333333333334;
+    res[37] = k12_0_4_2 * 0.3333333333333334;
+    res[38] = k12_0_4_3 * 0.3333333333333334;
+    res[39] = k12_0_5_1 * 0.5773502691896258;
+    res[40] = k12_0_5_2 * 0.5773502691896258;
+    res[41] = k12_0_5_3 * 0.5773502691896258;
+    res[42] = k12_0_6_1 * 0.5773502691896258;
+    res[43] = k12_0_6_2 * 0.5773502691896258;
+    res[44] = k12_0_6_3 * 0.5773502691896258;
+    res[45] = k12_0_7_1 * 0.3333333333333334;
+    res[46] = k12_0_7_2 * 0.3333333333333334;
+    res[47] = k12_0_7_3 * 0.3333333333333334;
+    res[48] = k12_0_8_1 * 0.5773502691896258;
+    res[49] = k12_0_8_2 * 0.5773502691896258;
+    res[50] = k12_0_8_3 * 0.5773502691896258;
+    res[51] = k12_0_9_1 * 0.3333333333333334;
+    res[52] = k12_0_9_2 * 0.3333333333333334;
+    res[53] = k12_0_9_3 * 0.3333333333333334;
+    res[54] = k13_0_4_1 * 0.3333333333333334;
+    res[55] = k13_0_4_2 * 0.3333333333333334;
+    res[56] = k13_0_4_3 * 0.3333333333333334;
+    res[57] = k13_0_5_1 * 0.5773502691896258;
+    res[58] = k13_0_5_2 * 0.5773502691896258;
+    res[59] = k13_0_5_3 * 0.5773502691896258;
+    res[60] = k13_0_6_1 * 0.5773502691896258;
+    res[61] = k13_0_6_2 * 0.5773502691896258;
+    res[62] = k13_0_6_3 * 0.5773502691896258;
+    res[63] = k13_0_7_1 * 0.3333333333333334;
+    res[64] = k13_0_7_2 * 0.3333333333333334;
+    res[65] = k13_0_7_3 * 0.3333333333333334;
+    res[66] = k13_0_8_1 * 0.5773502691896258;
+    res[67] = k13_0_8_2 * 0.5773502691896258;
+    res[68] = k13_0_8_3 * 0.5773502691896258;
+    res[69] = k13_0_9_1 * 0.3333333333333334;
+    res[70] = k13_0_9_2 * 0.3333333333333334;
+    res[71] = k13_0_9_3 * 0.3333333333333334;
+    res[72] = k14_0_4_1 * 0.3333333333333334;
+    res[73] = k14_0_4_2 * 0.3333333333333334;
+    res[74] = k14_0_4_3 * 0.3333333333333334;
+    res[75] = k14_0_5_1 * 0.5773502691896258;
+    res[76] = k14_0_5_2 * 0.5773502691896258;
+    res[77] = k14_0_5_3 * 0.5773502691896258;
+    res[78] = k14_0_6_1 * 0.5773502691896258;
+    res[79] = k14_0_6_2 * 0.5773502691896258;
+    res[80] = k14_0_6_3 * 0.5773502691896258;
+    res[81] = k14_0_7_1 * 0.3333333333333334;
+    res[82] = k14_0_7_2 * 0.3333333333333334;
+    res[83] = k14_0_7_3 * 0.3333333333333334;
+    res[84] = k14_0_8_1 * 0.5773502691896258;
+    res[85] = k14_0_8_2 * 0.5773502691896258;
+    res[86] = k14_0_8_3 * 0.5773502691896258;
+    res[87] = k14_0_9_1 * 0.3333333333333334;
+    res[88] = k14_0_9_2 * 0.3333333333333334;
+    res[89] = k14_0_9_3 * 0.3333333333333334;
+    res[90] = k15_0_4_1 * 0.5773502691896258;
+    res[91] = k15_0_4_2 * 0.5773502691896258;
+    res[92] = k15_0_4_3 * 0.5773502691896258;
+    res[93] = k15_0_5_1;
+    res[94] = k15_0_5_2;
+    res[95] = k15_0_5_3;
+    res[96] = k15_0_6_1;
+    res[97] = k15_0_6_2;
+    res[98] = k15_0_6_3;
+    res[99] = k15_0_7_1 * 0.5773502691896258;
+    res[100] = k15_0_7_2 * 0.5773502691896258;
+    res[101] = k15_0_7_3 * 0.5773502691896258;
+    res[102] = k15_0_8_1;
+    res[103] = k15_0_8_2;
+    res[104] = k15_0_8_3;
+    res[105] = k15_0_9_1 * 0.5773502691896258;
+    res[106] = k15_0_9_2 * 0.5773502691896258;
+    res[107] = k15_0_9_3 * 0.5773502691896258;
+    res[108] = k16_0_4_1 * 0.14907119849998599;
+    res[109] = k16_0_4_2 * 0.14907119849998599;
+    res[110] = k16_0_4_3 * 0.14907119849998599;
+    res[111] = k16_0_5_1 * 0.2581988897471611;
+    res[112] = k16_0_5_2 * 0.2581988897471611;
+    res[113] = k16_0_5_3 * 0.2581988897471611;
+    res[114] = k16_0_6_1 * 0.2581988897471611;
+    res[115] = k16_0_6_2 * 0.2581988897471611;
+    res[116] = k16_0_6_3 * 0.2581988897471611;
+    res[117] = k16_0_7_1 * 0.14907119849998599;
+    res[118] = k16_0_7_2 * 0.14907119849998599;
+    res[119] = k16_0_7_3 * 0.14907119849998599;
+    res[120] = k16_0_8_1 * 0.2581988897471611;
+    res[121] = k16_0_8_2 * 0.2581988897471611;
+    res[122] = k16_0_8_3 * 0.2581988897471611;
+    res[123] = k16_0_9_1 * 0.14907119849998599;
+    res[124] = k16_0_9_2 * 0.14907119849998599;
+    res[125] = k16_0_9_3 * 0.14907119849998599;
+    res[126] = k17_0_4_1 * 0.3333333333333334;
+    res[127] = k17_0_4_2 * 0.3333333333333334;
+    res[128] = k17_0_4_3 * 0.3333333333333334;
+    res[129] = k17_0_5_1 * 0.5773502691896258;
+    res[130] = k17_0_5_2 * 0.5773502691896258;
+    res[131] = k17_0_5_3 * 0.5773502691896258;
+    res[132] = k17_0_6_1 * 0.5773502691896258;
+    res[133] = k17_0_6_2 * 0.5773502691896258;
+    res[134] = k17_0_6_3 * 0.5773502691896258;
+    res[135] = k17_0_7_1 * 0.3333333333333334;
+    res[136] = k17_0_7_2 * 0.3333333333333334;
+    res[137] = k17_0_7_3 * 0.3333333333333334;
+    res[138] = k17_0_8_1 * 0.5773502691896258;
+    res[139] = k17_0_8_2 * 0.5773502691896258;
+    res[140] = k17_0_8_3 * 0.5773502691896258;
+    res[141] = k17_0_9_1 * 0.3333333333333334;
+    res[142] = k17_0_9_2 * 0.3333333333333334;
+    res[143] = k17_0_9_3 * 0.3333333333333334;
+    res[144] = k18_0_4_1 * 0.3333333333333334;
+    res[145] = k18_0_4_2 * 0.3333333333333334;
+    res[146] = k18_0_4_3 * 0.3333333333333334;
+    res[147] = k18_0_5_1 * 0.5773502691896258;
+    res[148] = k18_0_5_2 * 0.5773502691896258;
+    res[149] = k18_0_5_3 * 0.5773502691896258;
+    res[150] = k18_0_6_1 * 0.5773502691896258;
+    res[151] = k18_0_6_2 * 0.5773502691896258;
+    res[152] = k18_0_6_3 * 0.5773502691896258;
+    res[153] = k18_0_7_1 * 0.3333333333333334;
+    res[154] = k18_0_7_2 * 0.3333333333333334;
+    res[155] = k18_0_7_3 * 0.3333333333333334;
+    res[156] = k18_0_8_1 * 0.5773502691896258;
+    res[157] = k18_0_8_2 * 0.5773502691896258;
+    res[158] = k18_0_8_3 * 0.5773502691896258;
+    res[159] = k18_0_9_1 * 0.3333333333333334;
+    res[160] = k18_0_9_2 * 0.3333333333333334;
+    res[161] = k18_0_9_3 * 0.3333333333333334;
+    res[162] = k19_0_4_1 * 0.14907119849998599;
+    res[163] = k19_0_4_2 * 0.14907119849998599;
+    res[164] = k19_0_4_3 * 0.14907119849998599;
+    res[165] = k19_0_5_1 * 0.2581988897471611;
+    res[166] = k19_0_5_2 * 0.2581988897471611;
+    res[167] = k19_0_5_3 * 0.2581988897471611;
+    res[168] = k19_0_6_1 * 0.2581988897471611;
+    res[169] = k19_0_6_2 * 0.2581988897471611;
+    res[170] = k19_0_6_3 * 0.2581988897471611;
+    res[171] = k19_0_7_1 * 0.14907119849998599;
+    res[172] = k19_0_7_2 * 0.14907119849998599;
+    res[173] = k19_0_7_3 * 0.14907119849998599;
+    res[174] = k19_0_8_1 * 0.2581988897471611;
+    res[175] = k19_0_8_2 * 0.2581988897471611;
+    res[176] = k19_0_8_3 * 0.2581988897471611;
+    res[177] = k19_0_9_1 * 0.14907119849998599;
+    res[178] = k19_0_9_2 * 0.14907119849998599;
+    res[179] = k19_0_9_3 * 0.14907119849998599;
+}
+
+__device__ __forceinline__ void store_fsdp(double *__restrict__ out, const int4 ib_, const int4 ik_,
+                                            bool same, const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    (void)dab; (void)dcd;
+    const long long ij_0_0 = pair_index(ib_.z + 0, ib_.w + 0);
+    const long long ij_1_0 = pair_index(ib_.z + 1, ib_.w + 0);
+    const long long ij_2_0 = pair_index(ib_.z + 2, ib_.w + 0);
+    const long long ij_3_0 = pair_index(ib_.z + 3, ib_.w + 0);
+    const long long ij_4_0 = pair_index(ib_.z + 4, ib_.w + 0);
+    const long long ij_5_0 = pair_index(ib_.z + 5, ib_.w + 0);
+    const long long ij_6_0 = pair_index(ib_.z + 6, ib_.w + 0);
+    const long long ij_7_0 = pair_index(ib_.z + 7, ib_.w + 0);
+    const long long ij_8_0 = pair_index(ib_.z + 8, ib_.w + 0);
+    const long long ij_9_0 = pair_index(ib_.z + 9, ib_.w + 0);
+    const long long kl_0_0 = pair_index(ik_.z + 0, ik_.w + 0);
+    const long long kl_0_1 = pair_index(ik_.z + 0, ik_.w + 1);
+    const long long kl_0_2 = pair_index(ik_.z + 0, ik_.w + 2);
+    const long long kl_1_0 = pair_index(ik_.z + 1, ik_.w + 0);
+    const long long kl_1_1 = pair_index(ik_.z + 1, ik_.w + 1);
+    const long long kl_1_2 = pair_index(ik_.z + 1, ik_.w + 2);
+    const long long kl_2_0 = pair_index(ik_.z + 2, ik_.w + 0);
+    const long long kl_2_1 = pair_index(ik_.z + 2, ik_.w + 1);
+    const long long kl_2_2 = pair_index(ik_.z + 2, ik_.w + 2);
+    const long long kl_3_0 = pair_index(ik_.z + 3, ik_.w + 0);
+    const long long kl_3_1 = pair_index(ik_.z + 3, ik_.w + 1);
+    const long long kl_3_2 = pair_index(ik_.z + 3, ik_.w + 2);
+    const long long kl_4_0 = pair_index(ik_.z + 4, ik_.w + 0);
+    const long long kl_4_1 = pair_index(ik_.z + 4, ik_.w + 1);
+    const long long kl_4_2 = pair_index(ik_.z + 4, ik_.w + 2);
+    const long long kl_5_0 = pair_index(ik_.z + 5, ik_.w + 0);
+    const long long kl_5_1 = pair_index(ik_.z + 5, ik_.w + 1);
+    const long long kl_5_2 = pair_index(ik_.z + 5, ik_.w + 2);
+    { const long long ij = ij_0_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[0]; }
+    { const long long ij = ij_0_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[1]; }
+    { const long long ij = ij_0_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[2]; }
+    { const long long ij = ij_0_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[3]; }
+    { const long long ij = ij_0_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[4]; }
+    { const long long ij = ij_0_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[5]; }
+    { const long long ij = ij_0_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[6]; }
+    { const long long ij = ij_0_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[7]; }
+    { const long long ij = ij_0_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[8]; }
+    { const long long ij = ij_0_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[9]; }
+    { const long long ij = ij_0_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[10]; }
+    { const long long ij = ij_0_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[11]; }
+    { const long long ij = ij_0_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[12]; }
+    { const long long ij = ij_0_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[13]; }
+    { const long long ij = ij_0_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[14]; }
+    { const long long ij = ij_0_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[15]; }
+    { const long long ij = ij_0_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[16]; }
+    { const long long ij = ij_0_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[17]; }
+    { const long long ij = ij_1_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[18]; }
+    { const long long ij = ij_1_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[19]; }
+    { const long long ij = ij_1_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[20]; }
+    { const long long ij = ij_1_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[21]; }
+    { const long long ij = ij_1_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[22]; }
+    { const long long ij = ij_1_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[23]; }
+    { const long long ij = ij_1_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[24]; }
+    { const long long ij = ij_1_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[25]; }
+    { const long long ij = ij_1_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[26]; }
+    { const long long ij = ij_1_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[27]; }
+    { const long long ij = ij_1_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[28]; }
+    { const long long ij = ij_1_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[29]; }
+    { const long long ij = ij_1_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[30]; }
+    { const long long ij = ij_1_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[31]; }
+    { const long long ij = ij_1_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[32]; }
+    { const long long ij = ij_1_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[33]; }
+    { const long long ij = ij_1_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[34]; }
+    { const long long ij = ij_1_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[35]; }
+    { const long long ij = ij_2_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[36]; }
+    { const long long ij = ij_2_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[37]; }
+    { const long long ij = ij_2_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[38]; }
+    { const long long ij = ij_2_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[39]; }
+    { const long long ij = ij_2_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[40]; }
+    { const long long ij = ij_2_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[41]; }
+    { const long long ij = ij_2_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[42]; }
+    { const long long ij = ij_2_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[43]; }
+    { const long long ij = ij_2_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[44]; }
+    { const long long ij = ij_2_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[45]; }
+    { const long long ij = ij_2_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[46]; }
+    { const long long ij = ij_2_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[47]; }
+    { const long long ij = ij_2_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[48]; }
+    { const long long ij = ij_2_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[49]; }
+    { const long long ij = ij_2_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[50]; }
+    { const long long ij = ij_2_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[51]; }
+    { const long long ij = ij_2_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[52]; }
+    { const long long ij = ij_2_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[53]; }
+    { const long long ij = ij_3_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[54]; }
+    { const long long ij = ij_3_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[55]; }
+    { const long long ij = ij_3_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[56]; }
+    { const long long ij = ij_3_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[57]; }
+    { const long long ij = ij_3_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[58]; }
+    { const long long ij = ij_3_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[59]; }
+    { const long long ij = ij_3_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[60]; }
+    { const long long ij = ij_3_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[61]; }
+    { const long long ij = ij_3_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[62]; }
+    { const long long ij = ij_3_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[63]; }
+    { const long long ij = ij_3_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[64]; }
+    { const long long ij = ij_3_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[65]; }
+    { const long long ij = ij_3_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[66]; }
+    { const long long ij = ij_3_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[67]; }
+    { const long long ij = ij_3_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[68]; }
+    { const long long ij = ij_3_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[69]; }
+    { const long long ij = ij_3_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[70]; }
+    { const long long ij = ij_3_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[71]; }
+    { const long long ij = ij_4_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[72]; }
+    { const long long ij = ij_4_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[73]; }
+    { const long long ij = ij_4_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[74]; }
+    { const long long ij = ij_4_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[75]; }
+    { const long long ij = ij_4_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[76]; }
+    { const long long ij = ij_4_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[77]; }
+    { const long long ij = ij_4_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[78]; }
+    { const long long ij = ij_4_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[79]; }
+    { const long long ij = ij_4_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[80]; }
+    { const long long ij = ij_4_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[81]; }
+    { const long long ij = ij_4_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[82]; }
+    { const long long ij = ij_4_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[83]; }
+    { const long long ij = ij_4_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[84]; }
+    { const long long ij = ij_4_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[85]; }
+    { const long long ij = ij_4_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[86]; }
+    { const long long ij = ij_4_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[87]; }
+    { const long long ij = ij_4_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[88]; }
+    { const long long ij = ij_4_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[89]; }
+    { const long long ij = ij_5_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[90]; }
+    { const long long ij = ij_5_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[91]; }
+    { const long long ij = ij_5_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[92]; }
+    { const long long ij = ij_5_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[93]; }
+    { const long long ij = ij_5_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[94]; }
+    { const long long ij = ij_5_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[95]; }
+    { const long long ij = ij_5_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[96]; }
+    { const long long ij = ij_5_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[97]; }
+    { const long long ij = ij_5_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[98]; }
+    { const long long ij = ij_5_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[99]; }
+    { const long long ij = ij_5_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[100]; }
+    { const long long ij = ij_5_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[101]; }
+    { const long long ij = ij_5_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[102]; }
+    { const long long ij = ij_5_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[103]; }
+    { const long long ij = ij_5_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[104]; }
+    { const long long ij = ij_5_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[105]; }
+    { const long long ij = ij_5_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[106]; }
+    { const long long ij = ij_5_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[107]; }
+    { const long long ij = ij_6_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[108]; }
+    { const long long ij = ij_6_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[109]; }
+    { const long long ij = ij_6_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[110]; }
+    { const long long ij = ij_6_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[111]; }
+    { const long long ij = ij_6_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[112]; }
+    { const long long ij = ij_6_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[113]; }
+    { const long long ij = ij_6_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[114]; }
+    { const long long ij = ij_6_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[115]; }
+    { const long long ij = ij_6_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[116]; }
+    { const long long ij = ij_6_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[117]; }
+    { const long long ij = ij_6_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[118]; }
+    { const long long ij = ij_6_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[119]; }
+    { const long long ij = ij_6_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[120]; }
+    { const long long ij = ij_6_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[121]; }
+    { const long long ij = ij_6_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[122]; }
+    { const long long ij = ij_6_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[123]; }
+    { const long long ij = ij_6_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[124]; }
+    { const long long ij = ij_6_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[125]; }
+    { const long long ij = ij_7_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[126]; }
+    { const long long ij = ij_7_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[127]; }
+    { const long long ij = ij_7_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[128]; }
+    { const long long ij = ij_7_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[129]; }
+    { const long long ij = ij_7_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[130]; }
+    { const long long ij = ij_7_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[131]; }
+    { const long long ij = ij_7_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[132]; }
+    { const long long ij = ij_7_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[133]; }
+    { const long long ij = ij_7_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[134]; }
+    { const long long ij = ij_7_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[135]; }
+    { const long long ij = ij_7_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[136]; }
+    { const long long ij = ij_7_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[137]; }
+    { const long long ij = ij_7_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[138]; }
+    { const long long ij = ij_7_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[139]; }
+    { const long long ij = ij_7_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[140]; }
+    { const long long ij = ij_7_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[141]; }
+    { const long long ij = ij_7_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[142]; }
+    { const long long ij = ij_7_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[143]; }
+    { const long long ij = ij_8_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[144]; }
+    { const long long ij = ij_8_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[145]; }
+    { const long long ij = ij_8_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[146]; }
+    { const long long ij = ij_8_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[147]; }
+    { const long long ij = ij_8_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[148]; }
+    { const long long ij = ij_8_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[149]; }
+    { const long long ij = ij_8_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[150]; }
+    { const long long ij = ij_8_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[151]; }
+    { const long long ij = ij_8_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[152]; }
+    { const long long ij = ij_8_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[153]; }
+    { const long long ij = ij_8_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[154]; }
+    { const long long ij = ij_8_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[155]; }
+    { const long long ij = ij_8_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[156]; }
+    { const long long ij = ij_8_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[157]; }
+    { const long long ij = ij_8_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[158]; }
+    { const long long ij = ij_8_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[159]; }
+    { const long long ij = ij_8_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[160]; }
+    { const long long ij = ij_8_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[161]; }
+    { const long long ij = ij_9_0, kl = kl_0_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[162]; }
+    { const long long ij = ij_9_0, kl = kl_0_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[163]; }
+    { const long long ij = ij_9_0, kl = kl_0_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[164]; }
+    { const long long ij = ij_9_0, kl = kl_1_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[165]; }
+    { const long long ij = ij_9_0, kl = kl_1_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[166]; }
+    { const long long ij = ij_9_0, kl = kl_1_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[167]; }
+    { const long long ij = ij_9_0, kl = kl_2_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[168]; }
+    { const long long ij = ij_9_0, kl = kl_2_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[169]; }
+    { const long long ij = ij_9_0, kl = kl_2_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[170]; }
+    { const long long ij = ij_9_0, kl = kl_3_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[171]; }
+    { const long long ij = ij_9_0, kl = kl_3_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[172]; }
+    { const long long ij = ij_9_0, kl = kl_3_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[173]; }
+    { const long long ij = ij_9_0, kl = kl_4_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[174]; }
+    { const long long ij = ij_9_0, kl = kl_4_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[175]; }
+    { const long long ij = ij_9_0, kl = kl_4_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[176]; }
+    { const long long ij = ij_9_0, kl = kl_5_0;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[177]; }
+    { const long long ij = ij_9_0, kl = kl_5_1;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[178]; }
+    { const long long ij = ij_9_0, kl = kl_5_2;
+      if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[179]; }
+}
+
+// Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
+// ket pairs of one molecule) from a shared counter until the chunk list, ordered by
+// decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
+template <int MIXED>
+__global__ void __launch_bounds__(128) eri_queue_fsdp(const EriQueue Q) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(Q.counter, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= Q.nchunks) return;
+        const int4 ch = __ldg(&Q.chunks[c]);
+        for (int q = ch.y + lane; q < ch.y + ch.z; q += 32) {
+        const int p = ch.x;
+        const double2 bp = __ldg(&Q.pairs.bnd[p]), bq = __ldg(&Q.pairs.bnd[q]);
+        double res[180];
+        if (bp.x * bq.x < Q.screen_cut) {
+#pragma unroll
+            for (int x = 0; x < 180; ++x) res[x] = 0.0;
+        } else {
+            const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
+            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_fsdp<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+            else quartet_fsdp<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+        }
+        store_fsdp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                    p == q, res);
+        }
+    }
+}
+
+void launch_eri_fsdp(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
+    if (Q.nchunks <= 0 || grid <= 0) return;
+    if (mixed) eri_queue_fsdp<1><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_fsdp<0><<<grid, 128, 0, s>>>(Q);
+}
+
+// Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
+int occupancy_eri_fsdp(int mixed) {
+    int n = 0;
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fsdp<1>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fsdp<0>, 128, 0);
+    return n;
+}
+
+}  // namespace molints

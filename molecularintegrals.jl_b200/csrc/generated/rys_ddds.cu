@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (dd|ds).  Do not edit.
 // roots 4, block 31 x 6, outputs 36 x 6, group 64 threads,
-// 5 primitive quartets per batch, 3 accumulators per thread, 15040 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 3 accumulators per thread, 46720 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_ddds {
     static constexpr int NA = 31, NC = 6, NBLK = 186;
     static constexpr int NB = 6, ND = 1;
     static constexpr int NAB = 36, NCD = 6;
-    static constexpr int G = 64, NPB = 5, ACC = 3;
+    static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 3;
     static constexpr int S = 15;
-    static constexpr int SMEM_GROUP = 940;
+    static constexpr int SMEM_GROUP = 2920;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -91,7 +91,7 @@ static void rys_prepare_ddds() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ddds, cudaFuncAttributeMaxDynamicSharedMemorySize, 15040);
+        cudaFuncSetAttribute(rys_queue_ddds, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
 
         done[dev] = true;
     }
@@ -103,14 +103,14 @@ void launch_rys_ddds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_ddds();
     constexpr int ng = 128 / C_ddds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ddds<<<grid, 128, 15040, s>>>(Q, R);
+    rys_queue_ddds<<<grid, 128, 46720, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_ddds() {
     rys_prepare_ddds();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddds, 128, 15040);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddds, 128, 46720);
     return n;
 }
 

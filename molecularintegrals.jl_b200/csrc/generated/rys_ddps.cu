@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (dd|ps).  Do not edit.
 // roots 3, block 31 x 3, outputs 36 x 3, group 32 threads,
-// 3 primitive quartets per batch, 3 accumulators per thread, 9920 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 3 accumulators per thread, 30080 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_ddps {
     static constexpr int NA = 31, NC = 3, NBLK = 93;
     static constexpr int NB = 6, ND = 1;
     static constexpr int NAB = 36, NCD = 3;
-    static constexpr int G = 32, NPB = 3, ACC = 3;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 3;
     static constexpr int S = 10;
-    static constexpr int SMEM_GROUP = 310;
+    static constexpr int SMEM_GROUP = 940;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -82,7 +82,7 @@ static void rys_prepare_ddps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ddps, cudaFuncAttributeMaxDynamicSharedMemorySize, 9920);
+        cudaFuncSetAttribute(rys_queue_ddps, cudaFuncAttributeMaxDynamicSharedMemorySize, 30080);
 
         done[dev] = true;
     }
@@ -94,14 +94,14 @@ void launch_rys_ddps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_ddps();
     constexpr int ng = 128 / C_ddps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ddps<<<grid, 128, 9920, s>>>(Q, R);
+    rys_queue_ddps<<<grid, 128, 30080, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_ddps() {
     rys_prepare_ddps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddps, 128, 9920);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddps, 128, 30080);
     return n;
 }
 

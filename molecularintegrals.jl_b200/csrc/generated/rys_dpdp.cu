@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (dp|dp).  Do not edit.
 // roots 4, block 16 x 16, outputs 18 x 18, group 64 threads,
-// 5 primitive quartets per batch, 4 accumulators per thread, 16000 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 4 accumulators per thread, 49792 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dpdp {
     static constexpr int NA = 16, NC = 16, NBLK = 256;
     static constexpr int NB = 3, ND = 3;
     static constexpr int NAB = 18, NCD = 18;
-    static constexpr int G = 64, NPB = 5, ACC = 4;
+    static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 4;
     static constexpr int S = 16;
-    static constexpr int SMEM_GROUP = 1000;
+    static constexpr int SMEM_GROUP = 3112;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -94,8 +94,8 @@ static void rys_prepare_dpdp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 16000);
-        cudaFuncSetAttribute(rys_bound_kernel_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 16000);
+        cudaFuncSetAttribute(rys_queue_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
+        cudaFuncSetAttribute(rys_bound_kernel_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
         done[dev] = true;
     }
 }
@@ -106,14 +106,14 @@ void launch_rys_dpdp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dpdp();
     constexpr int ng = 128 / C_dpdp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dpdp<<<grid, 128, 16000, s>>>(Q, R);
+    rys_queue_dpdp<<<grid, 128, 49792, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dpdp() {
     rys_prepare_dpdp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp, 128, 16000);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp, 128, 49792);
     return n;
 }
 
@@ -122,7 +122,7 @@ void launch_rys_bound_dpdp(const PairTab &P, const RysTab &R, int p0, int np, do
     if (np <= 0) return;
     rys_prepare_dpdp();
     constexpr int ng = 128 / C_dpdp::G;
-    rys_bound_kernel_dpdp<<<(np + ng - 1) / ng, 128, 16000, s>>>(P, R, p0, np, pbound, qout, full);
+    rys_bound_kernel_dpdp<<<(np + ng - 1) / ng, 128, 49792, s>>>(P, R, p0, np, pbound, qout, full);
 }
 
 }  // namespace molints

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (dp|pp).  Do not edit.
 // roots 3, block 16 x 9, outputs 18 x 9, group 64 threads,
-// 7 primitive quartets per batch, 3 accumulators per thread, 12736 B shared per block.
+// 21 primitive quartets per batch, 1 slot(s), 3 accumulators per thread, 36928 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dppp {
     static constexpr int NA = 16, NC = 9, NBLK = 144;
     static constexpr int NB = 3, ND = 3;
     static constexpr int NAB = 18, NCD = 9;
-    static constexpr int G = 64, NPB = 7, ACC = 3;
+    static constexpr int G = 64, NPB = 21, NSLOT = 1, ACC = 3;
     static constexpr int S = 12;
-    static constexpr int SMEM_GROUP = 796;
+    static constexpr int SMEM_GROUP = 2308;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -75,7 +75,7 @@ static void rys_prepare_dppp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 12736);
+        cudaFuncSetAttribute(rys_queue_dppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 36928);
 
         done[dev] = true;
     }
@@ -87,14 +87,14 @@ void launch_rys_dppp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dppp();
     constexpr int ng = 128 / C_dppp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dppp<<<grid, 128, 12736, s>>>(Q, R);
+    rys_queue_dppp<<<grid, 128, 36928, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dppp() {
     rys_prepare_dppp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dppp, 128, 12736);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dppp, 128, 36928);
     return n;
 }
 

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (dp|ps).  Do not edit.
 // roots 3, block 16 x 3, outputs 18 x 3, group 32 threads,
-// 3 primitive quartets per batch, 2 accumulators per thread, 8192 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 2 accumulators per thread, 24320 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dpps {
     static constexpr int NA = 16, NC = 3, NBLK = 48;
     static constexpr int NB = 3, ND = 1;
     static constexpr int NAB = 18, NCD = 3;
-    static constexpr int G = 32, NPB = 3, ACC = 2;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 8;
-    static constexpr int SMEM_GROUP = 256;
+    static constexpr int SMEM_GROUP = 760;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -64,7 +64,7 @@ static void rys_prepare_dpps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpps, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192);
+        cudaFuncSetAttribute(rys_queue_dpps, cudaFuncAttributeMaxDynamicSharedMemorySize, 24320);
 
         done[dev] = true;
     }
@@ -76,14 +76,14 @@ void launch_rys_dpps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dpps();
     constexpr int ng = 128 / C_dpps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dpps<<<grid, 128, 8192, s>>>(Q, R);
+    rys_queue_dpps<<<grid, 128, 24320, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dpps() {
     rys_prepare_dpps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpps, 128, 8192);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpps, 128, 24320);
     return n;
 }
 

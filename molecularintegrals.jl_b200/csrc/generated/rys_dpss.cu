@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (dp|ss).  Do not edit.
 // roots 2, block 16 x 1, outputs 18 x 1, group 32 threads,
-// 5 primitive quartets per batch, 1 accumulators per thread, 5120 B shared per block.
+// 16 primitive quartets per batch, 2 slot(s), 1 accumulators per thread, 13568 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dpss {
     static constexpr int NA = 16, NC = 1, NBLK = 16;
     static constexpr int NB = 3, ND = 1;
     static constexpr int NAB = 18, NCD = 1;
-    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int G = 32, NPB = 16, NSLOT = 2, ACC = 1;
     static constexpr int S = 4;
-    static constexpr int SMEM_GROUP = 160;
+    static constexpr int SMEM_GROUP = 424;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -62,7 +62,7 @@ static void rys_prepare_dpss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpss, cudaFuncAttributeMaxDynamicSharedMemorySize, 5120);
+        cudaFuncSetAttribute(rys_queue_dpss, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
 
         done[dev] = true;
     }
@@ -74,14 +74,14 @@ void launch_rys_dpss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dpss();
     constexpr int ng = 128 / C_dpss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dpss<<<grid, 128, 5120, s>>>(Q, R);
+    rys_queue_dpss<<<grid, 128, 13568, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dpss() {
     rys_prepare_dpss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpss, 128, 5120);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpss, 128, 13568);
     return n;
 }
 

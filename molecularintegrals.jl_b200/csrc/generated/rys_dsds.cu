@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (ds|ds).  Do not edit.
 // roots 3, block 6 x 6, outputs 6 x 6, group 32 threads,
-// 3 primitive quartets per batch, 2 accumulators per thread, 9056 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 2 accumulators per thread, 27200 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dsds {
     static constexpr int NA = 6, NC = 6, NBLK = 36;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 6, NCD = 6;
-    static constexpr int G = 32, NPB = 3, ACC = 2;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 9;
-    static constexpr int SMEM_GROUP = 283;
+    static constexpr int SMEM_GROUP = 850;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -63,8 +63,8 @@ static void rys_prepare_dsds() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dsds, cudaFuncAttributeMaxDynamicSharedMemorySize, 9056);
-        cudaFuncSetAttribute(rys_bound_kernel_dsds, cudaFuncAttributeMaxDynamicSharedMemorySize, 9056);
+        cudaFuncSetAttribute(rys_queue_dsds, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
+        cudaFuncSetAttribute(rys_bound_kernel_dsds, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
         done[dev] = true;
     }
 }
@@ -75,14 +75,14 @@ void launch_rys_dsds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dsds();
     constexpr int ng = 128 / C_dsds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dsds<<<grid, 128, 9056, s>>>(Q, R);
+    rys_queue_dsds<<<grid, 128, 27200, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dsds() {
     rys_prepare_dsds();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsds, 128, 9056);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsds, 128, 27200);
     return n;
 }
 
@@ -91,7 +91,7 @@ void launch_rys_bound_dsds(const PairTab &P, const RysTab &R, int p0, int np, do
     if (np <= 0) return;
     rys_prepare_dsds();
     constexpr int ng = 128 / C_dsds::G;
-    rys_bound_kernel_dsds<<<(np + ng - 1) / ng, 128, 9056, s>>>(P, R, p0, np, pbound, qout, full);
+    rys_bound_kernel_dsds<<<(np + ng - 1) / ng, 128, 27200, s>>>(P, R, p0, np, pbound, qout, full);
 }
 
 }  // namespace molints

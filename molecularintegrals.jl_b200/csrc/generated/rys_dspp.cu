@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (ds|pp).  Do not edit.
 // roots 3, block 6 x 9, outputs 6 x 9, group 32 threads,
-// 3 primitive quartets per batch, 2 accumulators per thread, 9056 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 2 accumulators per thread, 27200 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dspp {
     static constexpr int NA = 6, NC = 9, NBLK = 54;
     static constexpr int NB = 1, ND = 3;
     static constexpr int NAB = 6, NCD = 9;
-    static constexpr int G = 32, NPB = 3, ACC = 2;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 9;
-    static constexpr int SMEM_GROUP = 283;
+    static constexpr int SMEM_GROUP = 850;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -62,7 +62,7 @@ static void rys_prepare_dspp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dspp, cudaFuncAttributeMaxDynamicSharedMemorySize, 9056);
+        cudaFuncSetAttribute(rys_queue_dspp, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
 
         done[dev] = true;
     }
@@ -74,14 +74,14 @@ void launch_rys_dspp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dspp();
     constexpr int ng = 128 / C_dspp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dspp<<<grid, 128, 9056, s>>>(Q, R);
+    rys_queue_dspp<<<grid, 128, 27200, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dspp() {
     rys_prepare_dspp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp, 128, 9056);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp, 128, 27200);
     return n;
 }
 

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (ds|ps).  Do not edit.
 // roots 2, block 6 x 3, outputs 6 x 3, group 32 threads,
-// 5 primitive quartets per batch, 1 accumulators per thread, 7040 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 1 accumulators per thread, 19712 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dsps {
     static constexpr int NA = 6, NC = 3, NBLK = 18;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 6, NCD = 3;
-    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int G = 32, NPB = 16, NSLOT = 1, ACC = 1;
     static constexpr int S = 6;
-    static constexpr int SMEM_GROUP = 220;
+    static constexpr int SMEM_GROUP = 616;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -56,7 +56,7 @@ static void rys_prepare_dsps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dsps, cudaFuncAttributeMaxDynamicSharedMemorySize, 7040);
+        cudaFuncSetAttribute(rys_queue_dsps, cudaFuncAttributeMaxDynamicSharedMemorySize, 19712);
 
         done[dev] = true;
     }
@@ -68,14 +68,14 @@ void launch_rys_dsps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dsps();
     constexpr int ng = 128 / C_dsps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dsps<<<grid, 128, 7040, s>>>(Q, R);
+    rys_queue_dsps<<<grid, 128, 19712, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dsps() {
     rys_prepare_dsps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsps, 128, 7040);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsps, 128, 19712);
     return n;
 }
 

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (ds|ss).  Do not edit.
 // roots 2, block 6 x 1, outputs 6 x 1, group 32 threads,
-// 5 primitive quartets per batch, 1 accumulators per thread, 4160 B shared per block.
+// 16 primitive quartets per batch, 5 slot(s), 1 accumulators per thread, 10496 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_dsss {
     static constexpr int NA = 6, NC = 1, NBLK = 6;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 6, NCD = 1;
-    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int G = 32, NPB = 16, NSLOT = 5, ACC = 1;
     static constexpr int S = 3;
-    static constexpr int SMEM_GROUP = 130;
+    static constexpr int SMEM_GROUP = 328;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -55,7 +55,7 @@ static void rys_prepare_dsss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dsss, cudaFuncAttributeMaxDynamicSharedMemorySize, 4160);
+        cudaFuncSetAttribute(rys_queue_dsss, cudaFuncAttributeMaxDynamicSharedMemorySize, 10496);
 
         done[dev] = true;
     }
@@ -67,14 +67,14 @@ void launch_rys_dsss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_dsss();
     constexpr int ng = 128 / C_dsss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dsss<<<grid, 128, 4160, s>>>(Q, R);
+    rys_queue_dsss<<<grid, 128, 10496, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dsss() {
     rys_prepare_dsss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsss, 128, 4160);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsss, 128, 10496);
     return n;
 }
 

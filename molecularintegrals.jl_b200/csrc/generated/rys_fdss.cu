@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fd|ss).  Do not edit.
 // roots 3, block 46 x 1, outputs 60 x 1, group 32 threads,
-// 3 primitive quartets per batch, 2 accumulators per thread, 6464 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 2 accumulators per thread, 18560 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fdss {
     static constexpr int NA = 46, NC = 1, NBLK = 46;
     static constexpr int NB = 6, ND = 1;
     static constexpr int NAB = 60, NCD = 1;
-    static constexpr int G = 32, NPB = 3, ACC = 2;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 6;
-    static constexpr int SMEM_GROUP = 202;
+    static constexpr int SMEM_GROUP = 580;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -93,7 +93,7 @@ static void rys_prepare_fdss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fdss, cudaFuncAttributeMaxDynamicSharedMemorySize, 6464);
+        cudaFuncSetAttribute(rys_queue_fdss, cudaFuncAttributeMaxDynamicSharedMemorySize, 18560);
 
         done[dev] = true;
     }
@@ -105,14 +105,14 @@ void launch_rys_fdss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fdss();
     constexpr int ng = 128 / C_fdss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fdss<<<grid, 128, 6464, s>>>(Q, R);
+    rys_queue_fdss<<<grid, 128, 18560, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fdss() {
     rys_prepare_fdss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fdss, 128, 6464);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fdss, 128, 18560);
     return n;
 }
 

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fp|ds).  Do not edit.
 // roots 4, block 25 x 6, outputs 30 x 6, group 64 threads,
-// 5 primitive quartets per batch, 3 accumulators per thread, 15040 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 3 accumulators per thread, 46720 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fpds {
     static constexpr int NA = 25, NC = 6, NBLK = 150;
     static constexpr int NB = 3, ND = 1;
     static constexpr int NAB = 30, NCD = 6;
-    static constexpr int G = 64, NPB = 5, ACC = 3;
+    static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 3;
     static constexpr int S = 15;
-    static constexpr int SMEM_GROUP = 940;
+    static constexpr int SMEM_GROUP = 2920;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -80,7 +80,7 @@ static void rys_prepare_fpds() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fpds, cudaFuncAttributeMaxDynamicSharedMemorySize, 15040);
+        cudaFuncSetAttribute(rys_queue_fpds, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
 
         done[dev] = true;
     }
@@ -92,14 +92,14 @@ void launch_rys_fpds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fpds();
     constexpr int ng = 128 / C_fpds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fpds<<<grid, 128, 15040, s>>>(Q, R);
+    rys_queue_fpds<<<grid, 128, 46720, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fpds() {
     rys_prepare_fpds();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpds, 128, 15040);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpds, 128, 46720);
     return n;
 }
 

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fp|fs).  Do not edit.
 // roots 4, block 25 x 10, outputs 30 x 10, group 64 threads,
-// 5 primitive quartets per batch, 4 accumulators per thread, 19840 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 4 accumulators per thread, 62080 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fpfs {
     static constexpr int NA = 25, NC = 10, NBLK = 250;
     static constexpr int NB = 3, ND = 1;
     static constexpr int NAB = 30, NCD = 10;
-    static constexpr int G = 64, NPB = 5, ACC = 4;
+    static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 4;
     static constexpr int S = 20;
-    static constexpr int SMEM_GROUP = 1240;
+    static constexpr int SMEM_GROUP = 3880;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -89,7 +89,7 @@ static void rys_prepare_fpfs() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fpfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 19840);
+        cudaFuncSetAttribute(rys_queue_fpfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 62080);
 
         done[dev] = true;
     }
@@ -101,14 +101,14 @@ void launch_rys_fpfs(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fpfs();
     constexpr int ng = 128 / C_fpfs::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fpfs<<<grid, 128, 19840, s>>>(Q, R);
+    rys_queue_fpfs<<<grid, 128, 62080, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fpfs() {
     rys_prepare_fpfs();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpfs, 128, 19840);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpfs, 128, 62080);
     return n;
 }
 

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fp|pp).  Do not edit.
 // roots 4, block 25 x 9, outputs 30 x 9, group 64 threads,
-// 5 primitive quartets per batch, 4 accumulators per thread, 15040 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 4 accumulators per thread, 46720 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fppp {
     static constexpr int NA = 25, NC = 9, NBLK = 225;
     static constexpr int NB = 3, ND = 3;
     static constexpr int NAB = 30, NCD = 9;
-    static constexpr int G = 64, NPB = 5, ACC = 4;
+    static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 4;
     static constexpr int S = 15;
-    static constexpr int SMEM_GROUP = 940;
+    static constexpr int SMEM_GROUP = 2920;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -88,7 +88,7 @@ static void rys_prepare_fppp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 15040);
+        cudaFuncSetAttribute(rys_queue_fppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
 
         done[dev] = true;
     }
@@ -100,14 +100,14 @@ void launch_rys_fppp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fppp();
     constexpr int ng = 128 / C_fppp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fppp<<<grid, 128, 15040, s>>>(Q, R);
+    rys_queue_fppp<<<grid, 128, 46720, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fppp() {
     rys_prepare_fppp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fppp, 128, 15040);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fppp, 128, 46720);
     return n;
 }
 

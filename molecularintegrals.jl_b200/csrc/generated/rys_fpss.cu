@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fp|ss).  Do not edit.
 // roots 3, block 25 x 1, outputs 30 x 1, group 32 threads,
-// 3 primitive quartets per batch, 1 accumulators per thread, 5600 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 1 accumulators per thread, 15680 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fpss {
     static constexpr int NA = 25, NC = 1, NBLK = 25;
     static constexpr int NB = 3, ND = 1;
     static constexpr int NAB = 30, NCD = 1;
-    static constexpr int G = 32, NPB = 3, ACC = 1;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 1;
     static constexpr int S = 5;
-    static constexpr int SMEM_GROUP = 175;
+    static constexpr int SMEM_GROUP = 490;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -69,7 +69,7 @@ static void rys_prepare_fpss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fpss, cudaFuncAttributeMaxDynamicSharedMemorySize, 5600);
+        cudaFuncSetAttribute(rys_queue_fpss, cudaFuncAttributeMaxDynamicSharedMemorySize, 15680);
 
         done[dev] = true;
     }
@@ -81,14 +81,14 @@ void launch_rys_fpss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fpss();
     constexpr int ng = 128 / C_fpss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fpss<<<grid, 128, 5600, s>>>(Q, R);
+    rys_queue_fpss<<<grid, 128, 15680, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fpss() {
     rys_prepare_fpss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpss, 128, 5600);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpss, 128, 15680);
     return n;
 }
 

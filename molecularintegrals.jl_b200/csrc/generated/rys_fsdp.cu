@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fs|dp).  Do not edit.
 // roots 4, block 10 x 16, outputs 10 x 18, group 64 threads,
-// 5 primitive quartets per batch, 3 accumulators per thread, 16000 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 3 accumulators per thread, 49792 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fsdp {
     static constexpr int NA = 10, NC = 16, NBLK = 160;
     static constexpr int NB = 1, ND = 3;
     static constexpr int NAB = 10, NCD = 18;
-    static constexpr int G = 64, NPB = 5, ACC = 3;
+    static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 3;
     static constexpr int S = 16;
-    static constexpr int SMEM_GROUP = 1000;
+    static constexpr int SMEM_GROUP = 3112;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -76,7 +76,7 @@ static void rys_prepare_fsdp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 16000);
+        cudaFuncSetAttribute(rys_queue_fsdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
 
         done[dev] = true;
     }
@@ -88,14 +88,14 @@ void launch_rys_fsdp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fsdp();
     constexpr int ng = 128 / C_fsdp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsdp<<<grid, 128, 16000, s>>>(Q, R);
+    rys_queue_fsdp<<<grid, 128, 49792, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fsdp() {
     rys_prepare_fsdp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsdp, 128, 16000);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsdp, 128, 49792);
     return n;
 }
 

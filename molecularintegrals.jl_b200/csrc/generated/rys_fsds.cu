@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fs|ds).  Do not edit.
 // roots 3, block 10 x 6, outputs 10 x 6, group 32 threads,
-// 3 primitive quartets per batch, 2 accumulators per thread, 11648 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 2 accumulators per thread, 35840 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fsds {
     static constexpr int NA = 10, NC = 6, NBLK = 60;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 10, NCD = 6;
-    static constexpr int G = 32, NPB = 3, ACC = 2;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 12;
-    static constexpr int SMEM_GROUP = 364;
+    static constexpr int SMEM_GROUP = 1120;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -61,7 +61,7 @@ static void rys_prepare_fsds() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsds, cudaFuncAttributeMaxDynamicSharedMemorySize, 11648);
+        cudaFuncSetAttribute(rys_queue_fsds, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
 
         done[dev] = true;
     }
@@ -73,14 +73,14 @@ void launch_rys_fsds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fsds();
     constexpr int ng = 128 / C_fsds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsds<<<grid, 128, 11648, s>>>(Q, R);
+    rys_queue_fsds<<<grid, 128, 35840, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fsds() {
     rys_prepare_fsds();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsds, 128, 11648);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsds, 128, 35840);
     return n;
 }
 

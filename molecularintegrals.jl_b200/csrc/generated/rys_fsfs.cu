@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fs|fs).  Do not edit.
 // roots 4, block 10 x 10, outputs 10 x 10, group 32 threads,
-// 2 primitive quartets per batch, 4 accumulators per thread, 13568 B shared per block.
+// 8 primitive quartets per batch, 1 slot(s), 4 accumulators per thread, 50432 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fsfs {
     static constexpr int NA = 10, NC = 10, NBLK = 100;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 10, NCD = 10;
-    static constexpr int G = 32, NPB = 2, ACC = 4;
+    static constexpr int G = 32, NPB = 8, NSLOT = 1, ACC = 4;
     static constexpr int S = 16;
-    static constexpr int SMEM_GROUP = 424;
+    static constexpr int SMEM_GROUP = 1576;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -71,8 +71,8 @@ static void rys_prepare_fsfs() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
-        cudaFuncSetAttribute(rys_bound_kernel_fsfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+        cudaFuncSetAttribute(rys_queue_fsfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
+        cudaFuncSetAttribute(rys_bound_kernel_fsfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
         done[dev] = true;
     }
 }
@@ -83,14 +83,14 @@ void launch_rys_fsfs(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fsfs();
     constexpr int ng = 128 / C_fsfs::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsfs<<<grid, 128, 13568, s>>>(Q, R);
+    rys_queue_fsfs<<<grid, 128, 50432, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fsfs() {
     rys_prepare_fsfs();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsfs, 128, 13568);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsfs, 128, 50432);
     return n;
 }
 
@@ -99,7 +99,7 @@ void launch_rys_bound_fsfs(const PairTab &P, const RysTab &R, int p0, int np, do
     if (np <= 0) return;
     rys_prepare_fsfs();
     constexpr int ng = 128 / C_fsfs::G;
-    rys_bound_kernel_fsfs<<<(np + ng - 1) / ng, 128, 13568, s>>>(P, R, p0, np, pbound, qout, full);
+    rys_bound_kernel_fsfs<<<(np + ng - 1) / ng, 128, 50432, s>>>(P, R, p0, np, pbound, qout, full);
 }
 
 }  // namespace molints

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fs|pp).  Do not edit.
 // roots 3, block 10 x 9, outputs 10 x 9, group 32 threads,
-// 3 primitive quartets per batch, 3 accumulators per thread, 11648 B shared per block.
+// 10 primitive quartets per batch, 1 slot(s), 3 accumulators per thread, 35840 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fspp {
     static constexpr int NA = 10, NC = 9, NBLK = 90;
     static constexpr int NB = 1, ND = 3;
     static constexpr int NAB = 10, NCD = 9;
-    static constexpr int G = 32, NPB = 3, ACC = 3;
+    static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 3;
     static constexpr int S = 12;
-    static constexpr int SMEM_GROUP = 364;
+    static constexpr int SMEM_GROUP = 1120;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -66,7 +66,7 @@ static void rys_prepare_fspp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fspp, cudaFuncAttributeMaxDynamicSharedMemorySize, 11648);
+        cudaFuncSetAttribute(rys_queue_fspp, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
 
         done[dev] = true;
     }
@@ -78,14 +78,14 @@ void launch_rys_fspp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fspp();
     constexpr int ng = 128 / C_fspp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fspp<<<grid, 128, 11648, s>>>(Q, R);
+    rys_queue_fspp<<<grid, 128, 35840, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fspp() {
     rys_prepare_fspp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fspp, 128, 11648);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fspp, 128, 35840);
     return n;
 }
 

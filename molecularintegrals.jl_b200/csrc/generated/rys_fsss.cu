@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (fs|ss).  Do not edit.
 // roots 2, block 10 x 1, outputs 10 x 1, group 32 threads,
-// 5 primitive quartets per batch, 1 accumulators per thread, 5120 B shared per block.
+// 16 primitive quartets per batch, 3 slot(s), 1 accumulators per thread, 13568 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_fsss {
     static constexpr int NA = 10, NC = 1, NBLK = 10;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 10, NCD = 1;
-    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int G = 32, NPB = 16, NSLOT = 3, ACC = 1;
     static constexpr int S = 4;
-    static constexpr int SMEM_GROUP = 160;
+    static constexpr int SMEM_GROUP = 424;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -56,7 +56,7 @@ static void rys_prepare_fsss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsss, cudaFuncAttributeMaxDynamicSharedMemorySize, 5120);
+        cudaFuncSetAttribute(rys_queue_fsss, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
 
         done[dev] = true;
     }
@@ -68,14 +68,14 @@ void launch_rys_fsss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_fsss();
     constexpr int ng = 128 / C_fsss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsss<<<grid, 128, 5120, s>>>(Q, R);
+    rys_queue_fsss<<<grid, 128, 13568, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fsss() {
     rys_prepare_fsss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsss, 128, 5120);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsss, 128, 13568);
     return n;
 }
 

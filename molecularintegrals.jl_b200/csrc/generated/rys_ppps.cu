@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (pp|ps).  Do not edit.
 // roots 2, block 9 x 3, outputs 9 x 3, group 32 threads,
-// 5 primitive quartets per batch, 1 accumulators per thread, 7040 B shared per block.
+// 16 primitive quartets per batch, 1 slot(s), 1 accumulators per thread, 19712 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_ppps {
     static constexpr int NA = 9, NC = 3, NBLK = 27;
     static constexpr int NB = 3, ND = 1;
     static constexpr int NAB = 9, NCD = 3;
-    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int G = 32, NPB = 16, NSLOT = 1, ACC = 1;
     static constexpr int S = 6;
-    static constexpr int SMEM_GROUP = 220;
+    static constexpr int SMEM_GROUP = 616;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -59,7 +59,7 @@ static void rys_prepare_ppps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ppps, cudaFuncAttributeMaxDynamicSharedMemorySize, 7040);
+        cudaFuncSetAttribute(rys_queue_ppps, cudaFuncAttributeMaxDynamicSharedMemorySize, 19712);
 
         done[dev] = true;
     }
@@ -71,14 +71,14 @@ void launch_rys_ppps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_ppps();
     constexpr int ng = 128 / C_ppps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ppps<<<grid, 128, 7040, s>>>(Q, R);
+    rys_queue_ppps<<<grid, 128, 19712, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_ppps() {
     rys_prepare_ppps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppps, 128, 7040);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppps, 128, 19712);
     return n;
 }
 

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (pp|ss).  Do not edit.
 // roots 2, block 9 x 1, outputs 9 x 1, group 32 threads,
-// 5 primitive quartets per batch, 1 accumulators per thread, 4160 B shared per block.
+// 16 primitive quartets per batch, 3 slot(s), 1 accumulators per thread, 10496 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_ppss {
     static constexpr int NA = 9, NC = 1, NBLK = 9;
     static constexpr int NB = 3, ND = 1;
     static constexpr int NAB = 9, NCD = 1;
-    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int G = 32, NPB = 16, NSLOT = 3, ACC = 1;
     static constexpr int S = 3;
-    static constexpr int SMEM_GROUP = 130;
+    static constexpr int SMEM_GROUP = 328;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -57,7 +57,7 @@ static void rys_prepare_ppss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ppss, cudaFuncAttributeMaxDynamicSharedMemorySize, 4160);
+        cudaFuncSetAttribute(rys_queue_ppss, cudaFuncAttributeMaxDynamicSharedMemorySize, 10496);
 
         done[dev] = true;
     }
@@ -69,14 +69,14 @@ void launch_rys_ppss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_ppss();
     constexpr int ng = 128 / C_ppss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ppss<<<grid, 128, 4160, s>>>(Q, R);
+    rys_queue_ppss<<<grid, 128, 10496, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_ppss() {
     rys_prepare_ppss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppss, 128, 4160);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppss, 128, 10496);
     return n;
 }
 

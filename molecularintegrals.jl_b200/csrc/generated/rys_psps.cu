@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (ps|ps).  Do not edit.
 // roots 2, block 3 x 3, outputs 3 x 3, group 32 threads,
-// 5 primitive quartets per batch, 1 accumulators per thread, 5120 B shared per block.
+// 16 primitive quartets per batch, 3 slot(s), 1 accumulators per thread, 13568 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_psps {
     static constexpr int NA = 3, NC = 3, NBLK = 9;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 3, NCD = 3;
-    static constexpr int G = 32, NPB = 5, ACC = 1;
+    static constexpr int G = 32, NPB = 16, NSLOT = 3, ACC = 1;
     static constexpr int S = 4;
-    static constexpr int SMEM_GROUP = 160;
+    static constexpr int SMEM_GROUP = 424;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -59,8 +59,8 @@ static void rys_prepare_psps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_psps, cudaFuncAttributeMaxDynamicSharedMemorySize, 5120);
-        cudaFuncSetAttribute(rys_bound_kernel_psps, cudaFuncAttributeMaxDynamicSharedMemorySize, 5120);
+        cudaFuncSetAttribute(rys_queue_psps, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+        cudaFuncSetAttribute(rys_bound_kernel_psps, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
         done[dev] = true;
     }
 }
@@ -71,14 +71,14 @@ void launch_rys_psps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_psps();
     constexpr int ng = 128 / C_psps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_psps<<<grid, 128, 5120, s>>>(Q, R);
+    rys_queue_psps<<<grid, 128, 13568, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_psps() {
     rys_prepare_psps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psps, 128, 5120);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psps, 128, 13568);
     return n;
 }
 
@@ -87,7 +87,7 @@ void launch_rys_bound_psps(const PairTab &P, const RysTab &R, int p0, int np, do
     if (np <= 0) return;
     rys_prepare_psps();
     constexpr int ng = 128 / C_psps::G;
-    rys_bound_kernel_psps<<<(np + ng - 1) / ng, 128, 5120, s>>>(P, R, p0, np, pbound, qout, full);
+    rys_bound_kernel_psps<<<(np + ng - 1) / ng, 128, 13568, s>>>(P, R, p0, np, pbound, qout, full);
 }
 
 }  // namespace molints

@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (ps|ss).  Do not edit.
 // roots 1, block 3 x 1, outputs 3 x 1, group 32 threads,
-// 10 primitive quartets per batch, 1 accumulators per thread, 3200 B shared per block.
+// 32 primitive quartets per batch, 10 slot(s), 1 accumulators per thread, 7424 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_psss {
     static constexpr int NA = 3, NC = 1, NBLK = 3;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 3, NCD = 1;
-    static constexpr int G = 32, NPB = 10, ACC = 1;
+    static constexpr int G = 32, NPB = 32, NSLOT = 10, ACC = 1;
     static constexpr int S = 2;
-    static constexpr int SMEM_GROUP = 100;
+    static constexpr int SMEM_GROUP = 232;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -54,7 +54,7 @@ static void rys_prepare_psss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_psss, cudaFuncAttributeMaxDynamicSharedMemorySize, 3200);
+        cudaFuncSetAttribute(rys_queue_psss, cudaFuncAttributeMaxDynamicSharedMemorySize, 7424);
 
         done[dev] = true;
     }
@@ -66,14 +66,14 @@ void launch_rys_psss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_psss();
     constexpr int ng = 128 / C_psss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_psss<<<grid, 128, 3200, s>>>(Q, R);
+    rys_queue_psss<<<grid, 128, 7424, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_psss() {
     rys_prepare_psss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psss, 128, 3200);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psss, 128, 7424);
     return n;
 }
 

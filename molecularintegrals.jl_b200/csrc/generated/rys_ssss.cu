@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (ss|ss).  Do not edit.
 // roots 1, block 1 x 1, outputs 1 x 1, group 32 threads,
-// 10 primitive quartets per batch, 1 accumulators per thread, 2240 B shared per block.
+// 32 primitive quartets per batch, 32 slot(s), 1 accumulators per thread, 4352 B shared per block.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,9 @@ struct C_ssss {
     static constexpr int NA = 1, NC = 1, NBLK = 1;
     static constexpr int NB = 1, ND = 1;
     static constexpr int NAB = 1, NCD = 1;
-    static constexpr int G = 32, NPB = 10, ACC = 1;
+    static constexpr int G = 32, NPB = 32, NSLOT = 32, ACC = 1;
     static constexpr int S = 1;
-    static constexpr int SMEM_GROUP = 70;
+    static constexpr int SMEM_GROUP = 136;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -59,8 +59,8 @@ static void rys_prepare_ssss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ssss, cudaFuncAttributeMaxDynamicSharedMemorySize, 2240);
-        cudaFuncSetAttribute(rys_bound_kernel_ssss, cudaFuncAttributeMaxDynamicSharedMemorySize, 2240);
+        cudaFuncSetAttribute(rys_queue_ssss, cudaFuncAttributeMaxDynamicSharedMemorySize, 4352);
+        cudaFuncSetAttribute(rys_bound_kernel_ssss, cudaFuncAttributeMaxDynamicSharedMemorySize, 4352);
         done[dev] = true;
     }
 }
@@ -71,14 +71,14 @@ void launch_rys_ssss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStrea
     rys_prepare_ssss();
     constexpr int ng = 128 / C_ssss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ssss<<<grid, 128, 2240, s>>>(Q, R);
+    rys_queue_ssss<<<grid, 128, 4352, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_ssss() {
     rys_prepare_ssss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ssss, 128, 2240);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ssss, 128, 4352);
     return n;
 }
 
@@ -87,7 +87,7 @@ void launch_rys_bound_ssss(const PairTab &P, const RysTab &R, int p0, int np, do
     if (np <= 0) return;
     rys_prepare_ssss();
     constexpr int ng = 128 / C_ssss::G;
-    rys_bound_kernel_ssss<<<(np + ng - 1) / ng, 128, 2240, s>>>(P, R, p0, np, pbound, qout, full);
+    rys_bound_kernel_ssss<<<(np + ng - 1) / ng, 128, 4352, s>>>(P, R, p0, np, pbound, qout, full);
 }
 
 }  // namespace molints

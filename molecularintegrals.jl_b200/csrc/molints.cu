@@ -251,6 +251,10 @@ void fill_boys_scaled(double *sc, int nM) {
 
 namespace molints {
 int ctx_device_of(const molints_ctx *ctx) { return ctx->device; }
+// The AUTO method table of src, given to dst (the serving slots inherit their owner's table).
+void ctx_copy_methods(molints_ctx *dst, const molints_ctx *src) {
+    std::memcpy(dst->class_method, src->class_method, sizeof(dst->class_method));
+}
 }  // namespace molints
 
 // ------------------------------------------------------------------ C ABI
@@ -484,8 +488,77 @@ static int check_basis(molints_ctx *ctx, const molints_basis *b, int64_t *nbf_ou
     return nprim_tot;
 }
 
+// Shard `shard` of `nshards` of one basis: the shells M in [*s_lo, *s_hi) whose shell quartets
+// (those whose highest shell index is M) it computes, and its packed slice [*lo, *hi).  Every
+// entry of a quartet has its largest function index in the quartet's highest shell, and the
+// entries whose largest function index lies in [f, f') are the contiguous packed range
+// [tri(tri(f)), tri(tri(f'))).  Shells are split by an estimate of the quartet cost
+// (K_p K_q (1 + L_p)^2 (1 + L_q)^2 per pair product, L_p = la + lb).
+static void shard_bounds(const molints_basis *b, int shard, int nshards, int *s_lo, int *s_hi,
+                         int64_t *lo, int64_t *hi) {
+    const int ns = b->nshell;
+    std::vector<double> cost(ns, 0.0);
+    double below = 0.0, total = 0.0;
+    for (int M = 0; M < ns; ++M) {
+        double w = 0.0, w2 = 0.0;
+        for (int j = 0; j <= M; ++j) {
+            const double c = (double)b->nprim[M] * b->nprim[j] * (1 + b->L[M] + b->L[j]) * (1 + b->L[M] + b->L[j]);
+            w += c;
+            w2 += c * c;
+        }
+        cost[M] = w * below + 0.5 * (w * w + w2);
+        below += w;
+        total += cost[M];
+    }
+    std::vector<int> S(nshards + 1, ns);
+    S[0] = 0;
+    double acc = 0.0;
+    int r = 1;
+    for (int M = 0; M < ns && r < nshards; ++M) {
+        acc += cost[M];
+        while (r < nshards && acc >= total * r / nshards) S[r++] = M + 1;
+    }
+    for (int k = 1; k <= nshards; ++k) S[k] = std::max(S[k], S[k - 1]);
+    *s_lo = S[shard];
+    *s_hi = S[shard + 1];
+    auto first_fn = [&](int sh) {
+        int64_t f = 0;
+        for (int t = 0; t < sh; ++t) f += ncart(b->L[t]);
+        return f;
+    };
+    auto tri = [](int64_t n) { return n * (n + 1) / 2; };
+    *lo = tri(tri(first_fn(*s_lo)));
+    *hi = tri(tri(first_fn(*s_hi)));
+}
+
+static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
+                            const molints_options *opts_in, int shard, int nshards,
+                            molints_plan **out);
+
 int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                               const molints_options *opts_in, molints_plan **out) {
+    return plan_create_impl(ctx, nmol, bases, opts_in, 0, 1, out);
+}
+
+int molints_shard_range(const molints_basis *b, int32_t shard, int32_t nshards, int64_t *lo,
+                        int64_t *hi) {
+    if (!b || !lo || !hi || nshards < 1 || shard < 0 || shard >= nshards || molints_nbf(b) < 0)
+        return MOLINTS_ERR_INVALID;
+    int s0, s1;
+    shard_bounds(b, shard, nshards, &s0, &s1, lo, hi);
+    return MOLINTS_OK;
+}
+
+int molints_plan_create_shard(molints_ctx *ctx, const molints_basis *b, const molints_options *opts,
+                              int32_t shard, int32_t nshards, molints_plan **out) {
+    if (!b || nshards < 1 || shard < 0 || shard >= nshards)
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create_shard: bad argument");
+    return plan_create_impl(ctx, 1, b, opts, shard, nshards, out);
+}
+
+static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
+                            const molints_options *opts_in, int shard, int nshards,
+                            molints_plan **out) {
     if (!ctx || !out || nmol < 0 || (nmol > 0 && !bases))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null argument");
     *out = nullptr;
@@ -522,6 +595,14 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
     p->nshell = ns;
     p->npacked = mol_out[nmol];
     p->mol_out_h.assign(mol_out.begin(), mol_out.end() - (nmol > 0 ? 1 : 0));
+    int shard_s0 = 0, shard_s1 = 0;
+    int64_t shard_lo = 0, shard_hi = 0;
+    if (nshards > 1) {
+        if (nmol != 1) { delete p; return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: shards need one molecule"); }
+        shard_bounds(&bases[0], shard, nshards, &shard_s0, &shard_s1, &shard_lo, &shard_hi);
+        p->npacked = shard_hi - shard_lo;
+        p->mol_out_h[0] = -shard_lo;  // kernels write out[iindex - lo]
+    }
     p->mol_nshell.resize(nmol);
     // method per class pair: Rys where no HGP kernel exists (an f shell), else the request
     for (int x = 0; x < kNumPairClasses; ++x)
@@ -582,7 +663,9 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
         if (L[x] == L[y] || (L[x] >= 2 && L[y] >= 2 && L[x] + L[y] == 5)) return tight[x] >= tight[y];
         return L[x] > L[y];
     };
-    struct PairRec { int cls, mol, npp, a, b, ref; };
+    // ms: the pair's higher shell index in its molecule (shard plans order by it so that each
+    // bra pair's owned ket pairs are one contiguous run)
+    struct PairRec { int cls, mol, npp, a, b, ref, ms; };
     std::vector<PairRec> pr;
     for (int m = 0; m < nmol; ++m) {
         const int n = bases[m].nshell;
@@ -590,12 +673,14 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
             for (int j = 0; j <= i; ++j) {
                 int a = shell_off[m] + i, bb = shell_off[m] + j;
                 if (!a_first(a, bb)) std::swap(a, bb);
-                pr.push_back({pair_class_of(L[a], L[bb]), m, K[a] * K[bb], a, bb, i * (i + 1) / 2 + j});
+                pr.push_back({pair_class_of(L[a], L[bb]), m, K[a] * K[bb], a, bb, i * (i + 1) / 2 + j, i});
             }
     }
-    auto order = [](const PairRec &x, const PairRec &y) {
+    const bool sharded = nshards > 1;
+    auto order = [sharded](const PairRec &x, const PairRec &y) {
         if (x.cls != y.cls) return x.cls < y.cls;
         if (x.mol != y.mol) return x.mol < y.mol;
+        if (sharded && x.ms != y.ms) return x.ms < y.ms;
         return x.npp > y.npp;
     };
     std::stable_sort(pr.begin(), pr.end(), order);
@@ -783,8 +868,26 @@ int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basi
                 range_of(x, m, b0, b1);
                 range_of(y, m, k0, k1);
                 for (int pb = b0; pb < b1; ++pb) {
-                    const int kend = (x == y) ? pb + 1 : k1;
-                    for (int q0 = k0; q0 < kend; q0 += width) {
+                    int kbeg = k0, kend = (x == y) ? pb + 1 : k1;
+                    if (sharded) {
+                        // quartet owner: the higher of the two pairs' max shells
+                        const int mp = pr[pb].ms;
+                        auto first_ms_at_least = [&](int v) {
+                            return (int)(std::partition_point(pr.begin() + k0, pr.begin() + k1,
+                                                              [v](const PairRec &r) { return r.ms < v; }) -
+                                         pr.begin());
+                        };
+                        if (mp >= shard_s1) continue;
+                        if (x == y) {
+                            if (mp < shard_s0) continue;  // q <= pb in list order: owner is mp
+                        } else if (mp >= shard_s0) {
+                            kend = first_ms_at_least(shard_s1);
+                        } else {
+                            kbeg = first_ms_at_least(shard_s0);
+                            kend = first_ms_at_least(shard_s1);
+                        }
+                    }
+                    for (int q0 = kbeg; q0 < kend; q0 += width) {
                         const int n = std::min(width, kend - q0);
                         double kq = 0;
                         for (int t = 0; t < n; ++t) kq += p->npp_h[q0 + t];

@@ -2,11 +2,12 @@
 //
 // One group of C::G threads owns one contracted shell quartet (ab|cd) at a time:
 //   1. rys_contract: the primitive quartets in batches of C::NPB.  Stage 1, one thread per
-//      (primitive quartet, root, axis): the Rys node u and weight W of that root, then the
-//      2-D table I(a, c), a <= E, c <= F, of that axis (the x table carries the prefactor
-//      and W) into shared memory.  Stage 2, every thread: its own entries of the [e0|f0]
-//      block, sum over the batch and the roots of I_x I_y I_z, accumulated in registers in
-//      FP64.  The contracted block ends in shared memory.
+//      (primitive quartet, root): the Rys node u and weight W of that root, then the three
+//      2-D tables I(a, c), a <= E, c <= F (the x table carries the prefactor and W) into
+//      shared memory.  Stage 2, every thread: its own entries of the [e0|f0] block, sum over
+//      the batch and the roots of I_x I_y I_z, accumulated in registers in FP64 (blocks of
+//      at most G/2 entries: C::NSLOT threads per entry, summed at the end).  The contracted
+//      block ends in shared memory.
 //   2. rys_hrr: bra HRR into a (ab|f0) buffer, then ket HRR, both in the closed binomial form,
 //      times the component norms; a sink stores (or reduces) each (ab|cd).
 // Recurrences: Rys, Dupuis and King's 2-D integrals in the Head-Gordon/Pople variables, with
@@ -121,16 +122,19 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
                                              const int4 ib, const int4 ik, int i0, int i1, int j0,
                                              int j1, double *__restrict__ work, int lane, int gid) {
     constexpr int S = C::S, F1 = C::F + 1, NR = C::NR, E = C::E, F = C::F;
+    constexpr int NSLOT = C::NSLOT;
     double acc[C::ACC];
     uint32_t off[C::ACC];
+    // slot layout (NSLOT > 1): thread = slot * NBLK + entry, ACC == 1
+    const int slot = NSLOT > 1 ? lane / C::NBLK : 0;
 #pragma unroll
     for (int k = 0; k < C::ACC; ++k) {
         acc[k] = 0.0;
-        const int e = lane + k * C::G;
-        off[k] = (e < C::NBLK) ? __ldg(&T.blk[e]) : 0u;
+        const int e = NSLOT > 1 ? lane - slot * C::NBLK : lane + k * C::G;
+        off[k] = (e < C::NBLK && slot < NSLOT) ? __ldg(&T.blk[e]) : 0u;
     }
     const int nbp = i1 - i0, nq = nbp * (j1 - j0);
-    const int tb = lane / (3 * NR), tr = (lane / 3) % NR, tax = lane % 3;
+    const int tb = lane / NR, tr = lane - tb * NR;
     for (int g0 = 0; g0 < nq; g0 += C::NPB) {
         const int nb = min(C::NPB, nq - g0);
         if (tb < nb) {
@@ -140,67 +144,81 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
             const PrimPair ket = load_pp(P.pp, ik.x + j0 + gj);
             const double rz = rsqrt(bra.zeta + ket.zeta);
             const double r2 = rz * rz;
-            const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
-            const double X = bra.zeta * ket.zeta * r2 * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double PQv[3] = {bra.px - ket.px, bra.py - ket.py, bra.pz - ket.pz};
+            const double X = bra.zeta * ket.zeta * r2 * (PQv[0] * PQv[0] + PQv[1] * PQv[1] + PQv[2] * PQv[2]);
             double u, w;
             rys_root<NR>(R, X, tr, u, w);
             const double ez = ket.zeta * r2, zz = bra.zeta * r2;
-            const double PQ = tax == 0 ? PQx : (tax == 1 ? PQy : PQz);
-            const double PA = tax == 0 ? bra.pax : (tax == 1 ? bra.pay : bra.paz);
-            const double QC = tax == 0 ? ket.pax : (tax == 1 ? ket.pay : ket.paz);
-            const double c00 = fma(-ez * PQ, u, PA);
-            const double d00 = fma(zz * PQ, u, QC);
+            const double PAv[3] = {bra.pax, bra.pay, bra.paz}, QCv[3] = {ket.pax, ket.pay, ket.paz};
             const double b10 = bra.oo2z * fma(-ez, u, 1.0);
             const double b01 = ket.oo2z * fma(-zz, u, 1.0);
             const double b00 = 0.5 * r2 * u;
-            double *tab = work + ((tb * NR + tr) * 3 + tax) * S;
-            // column c = 0 by the a-recurrence, then column c+1 from columns c and c-1
-            double cur[E + 1], prev[E + 1];
-            cur[0] = tax == 0 ? bra.kab * ket.kab * rz * w : 1.0;
-            if (E > 0) cur[1] = c00 * cur[0];
 #pragma unroll
-            for (int a = 1; a < E; ++a) cur[a + 1] = fma(c00, cur[a], (double)a * b10 * cur[a - 1]);
+            for (int ax = 0; ax < 3; ++ax) {
+                const double c00 = fma(-ez * PQv[ax], u, PAv[ax]);
+                const double d00 = fma(zz * PQv[ax], u, QCv[ax]);
+                double *tab = work + ((tb * NR + tr) * 3 + ax) * S;
+                // column c = 0 by the a-recurrence, then column c+1 from columns c and c-1
+                double cur[E + 1], prev[E + 1];
+                cur[0] = ax == 0 ? bra.kab * ket.kab * rz * w : 1.0;
+                if (E > 0) cur[1] = c00 * cur[0];
 #pragma unroll
-            for (int a = 0; a <= E; ++a) {
-                tab[a * F1] = cur[a];
-                prev[a] = 0.0;
-            }
-#pragma unroll
-            for (int c = 0; c < F; ++c) {
-                double nxt[E + 1];
+                for (int a = 1; a < E; ++a) cur[a + 1] = fma(c00, cur[a], (double)a * b10 * cur[a - 1]);
 #pragma unroll
                 for (int a = 0; a <= E; ++a) {
-                    double v = d00 * cur[a];
-                    if (c > 0) v = fma((double)c * b01, prev[a], v);
-                    if (a > 0) v = fma((double)a * b00, cur[a - 1], v);
-                    nxt[a] = v;
+                    tab[a * F1] = cur[a];
+                    prev[a] = 0.0;
                 }
 #pragma unroll
-                for (int a = 0; a <= E; ++a) {
-                    prev[a] = cur[a];
-                    cur[a] = nxt[a];
-                    tab[a * F1 + c + 1] = nxt[a];
+                for (int c = 0; c < F; ++c) {
+                    double nxt[E + 1];
+#pragma unroll
+                    for (int a = 0; a <= E; ++a) {
+                        double v = d00 * cur[a];
+                        if (c > 0) v = fma((double)c * b01, prev[a], v);
+                        if (a > 0) v = fma((double)a * b00, cur[a - 1], v);
+                        nxt[a] = v;
+                    }
+#pragma unroll
+                    for (int a = 0; a <= E; ++a) {
+                        prev[a] = cur[a];
+                        cur[a] = nxt[a];
+                        tab[a * F1 + c + 1] = nxt[a];
+                    }
                 }
             }
         }
         group_sync<C::G>(gid);
-        for (int b = 0; b < nb; ++b) {
+        if (slot < NSLOT) {
+            for (int b = slot; b < nb; b += NSLOT) {
 #pragma unroll 1
-            for (int r = 0; r < NR; ++r) {
-                const double *__restrict__ tx = work + (b * NR + r) * 3 * S;
+                for (int r = 0; r < NR; ++r) {
+                    const double *__restrict__ tx = work + (b * NR + r) * 3 * S;
 #pragma unroll
-                for (int k = 0; k < C::ACC; ++k) {
-                    const uint32_t o = off[k];
-                    acc[k] = fma(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], acc[k]);
+                    for (int k = 0; k < C::ACC; ++k) {
+                        const uint32_t o = off[k];
+                        acc[k] = fma(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], acc[k]);
+                    }
                 }
             }
         }
         group_sync<C::G>(gid);
     }
+    if constexpr (NSLOT > 1) {
+        if (slot < NSLOT) work[lane] = acc[0];  // work[slot * NBLK + entry]
+        group_sync<C::G>(gid);
+        if (lane < C::NBLK) {
+            double v = work[lane];
 #pragma unroll
-    for (int k = 0; k < C::ACC; ++k) {
-        const int e = lane + k * C::G;
-        if (e < C::NBLK) work[e] = acc[k];
+            for (int s2 = 1; s2 < NSLOT; ++s2) v += work[s2 * C::NBLK + lane];
+            work[lane] = v;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < C::ACC; ++k) {
+            const int e = lane + k * C::G;
+            if (e < C::NBLK) work[e] = acc[k];
+        }
     }
     group_sync<C::G>(gid);
 }

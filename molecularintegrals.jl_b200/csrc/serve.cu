@@ -206,6 +206,7 @@ Server *server_start(molints_ctx *ctx, int device, int nslots, int64_t budget, s
             break;
         }
         molints_set_stream(c, st);
+        molints::ctx_copy_methods(c, ctx);  // the slots follow the owner's AUTO method table
         S->ctxs.push_back(c);
         S->streams.push_back(st);
     }
@@ -220,7 +221,6 @@ Server *server_start(molints_ctx *ctx, int device, int nslots, int64_t budget, s
         delete S;
         return nullptr;
     }
-    (void)ctx;
     for (int i = 0; i < nslots; ++i) S->workers.emplace_back(&Server::worker, S, i);
     return S;
 }
@@ -229,7 +229,8 @@ Server *server_start(molints_ctx *ctx, int device, int nslots, int64_t budget, s
 
 // ------------------------------------------------------------------ C ABI
 namespace molints {
-int ctx_device_of(const molints_ctx *ctx);  // molints.cu
+int ctx_device_of(const molints_ctx *ctx);                          // molints.cu
+void ctx_copy_methods(molints_ctx *dst, const molints_ctx *src);    // molints.cu
 }
 
 namespace {

@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = [
     "molints_plan_create_batch", "molints_plan_npacked", "molints_set_class_methods",
     "molints_serve_start", "molints_serve_stop", "molints_submit", "molints_poll",
     "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
-    "molints_release", "molints_serve_stats",
+    "molints_release", "molints_serve_stats", "molints_shard_range", "molints_plan_create_shard",
 ]
 
 
@@ -123,6 +123,8 @@ def load_library(path: Path | str | None = None):
         "molints_request_error": (ctypes.c_char_p, [P]),
         "molints_release": (ctypes.c_int, [P]),
         "molints_serve_stats": (ctypes.c_int, [P, P, P, P, P]),
+        "molints_shard_range": (ctypes.c_int, [P, I32, I32, P, P]),
+        "molints_plan_create_shard": (ctypes.c_int, [P, P, P, I32, I32, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -161,7 +163,7 @@ class Plan:
     """One basis (or a batch of them) resident on the device; ``execute`` runs the whole
     device path.  For a batch, molecule m's packed vector starts at ``offsets[m]``."""
 
-    def __init__(self, engine: "Engine", shells, opts: Options):
+    def __init__(self, engine: "Engine", shells, opts: Options, shard=None):
         self.engine = engine
         batch = isinstance(shells, (list, tuple))
         mols = list(shells) if batch else [shells]
@@ -177,6 +179,13 @@ class Plan:
             self._carr = arr
             engine._check(engine.lib.molints_plan_create_batch(engine.ctx, len(mols), arr,
                                                                ctypes.byref(opts), ctypes.byref(h)))
+        elif shard is not None:
+            r, n = shard
+            engine._check(engine.lib.molints_plan_create_shard(engine.ctx, ctypes.byref(self._arrs[0].c),
+                                                               ctypes.byref(opts), int(r), int(n),
+                                                               ctypes.byref(h)))
+            self.slice = shard_range(shells, r, n)
+            self.npacked = self.slice[1] - self.slice[0]
         else:
             engine._check(engine.lib.molints_plan_create(engine.ctx, ctypes.byref(self._arrs[0].c),
                                                          ctypes.byref(opts), ctypes.byref(h)))
@@ -324,6 +333,14 @@ class Engine:
         return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff,
                                                method, prim_cutoff))
 
+    def plan_shard(self, shells, shard: int, nshards: int, precision=FP64, boys=BOYS_REFERENCE,
+                   fp32_cutoff=0.0, screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF,
+                   method=METHOD_AUTO) -> Plan:
+        """Plan of shard `shard` of `nshards`: its execute writes the packed slice
+        ``shard_range(shells, shard, nshards)`` (offsets relative to the slice start)."""
+        return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff,
+                                               method, prim_cutoff), shard=(shard, nshards))
+
     def plan_batch(self, shells_list, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
                    screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO) -> Plan:
         """One plan over several molecules: a single execute computes all of them."""
@@ -384,6 +401,18 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def shard_range(shells, shard: int, nshards: int):
+    """(lo, hi): the contiguous packed slice shard `shard` of `nshards` owns (host only)."""
+    lib = load_library()
+    arrs = _BasisArrays(shells)
+    lo, hi = ctypes.c_int64(), ctypes.c_int64()
+    rc = lib.molints_shard_range(ctypes.byref(arrs.c), int(shard), int(nshards), ctypes.byref(lo),
+                                 ctypes.byref(hi))
+    if rc != 0:
+        raise MolintsError(rc, "molints_shard_range")
+    return lo.value, hi.value
 
 
 _default_engine: Engine | None = None

@@ -169,7 +169,9 @@ def test_class_kernel_limits():
     for X, Y in gen_rys.class_pairs():
         t = gen_rys.class_tables(X, Y)
         assert (128 // t["G"]) * t["smem_group"] * 8 <= 227 * 1024
-        assert t["npb"] * 3 * t["nr"] <= t["G"]
+        assert t["npb"] * t["nr"] <= t["G"]
+        assert t["nslot"] == 1 or (t["nslot"] <= t["npb"] and t["nslot"] * t["nblk"] <= t["G"])
+        assert (t["acc"] == 1) if t["nslot"] > 1 else (t["acc"] * t["G"] >= t["nblk"])
         assert max(max(o) for o in t["blk"]) < t["S"] < 256
         assert t["na"] < 256 and t["nc"] < 256
 
