@@ -257,21 +257,26 @@ def run_ours(args):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": npacked * 8,
            "timing": "host wall clock around molints_eri_packed (synchronous call)"}
 
-    # per-class HGP/Rys choice for the batch and serving workloads (l <= 3 molecules)
-    from molints_b200 import autotune as AT
-    t_tune = time.perf_counter()
-    class_table, class_timings = AT.tune_class_methods(
-        eng, [mi.config3_molecule(m) for m in range(1, 16, 2)] + [mi.config4_request(r) for r in range(4)])
-    t_tune = time.perf_counter() - t_tune
-    eng.set_class_methods(class_table)
-    eng.set_stream(stream.cuda_stream)
-    batch = measure_batch(eng, stream, dev, fp32_cut, rank, world)
-    serving = measure_serving(local, fp32_cut, args.serve_window, rank, class_table=class_table)
-    tuned = {"seconds": t_tune, "rys_classes": sorted(
-        t for t, (h, r) in class_timings.items() if class_table[AT._class_index(t)] == E.METHOD_RYS)}
+    batch = serving = tuned = None
+    parts = set(args.parts.split(","))
+    if parts & {"batch", "serve"}:
+        # per-class HGP/Rys choice for the batch and serving workloads (l <= 3 molecules)
+        from molints_b200 import autotune as AT
+        t_tune = time.perf_counter()
+        class_table, class_timings = AT.tune_class_methods(
+            eng, [mi.config3_molecule(m) for m in range(1, 16, 2)] + [mi.config4_request(r) for r in range(4)])
+        t_tune = time.perf_counter() - t_tune
+        eng.set_class_methods(class_table)
+        eng.set_stream(stream.cuda_stream)
+        tuned = {"seconds": t_tune, "rys_classes": sorted(
+            t for t, (h, r) in class_timings.items() if class_table[AT._class_index(t)] == E.METHOD_RYS)}
+        if "batch" in parts:
+            batch = measure_batch(eng, stream, dev, fp32_cut, rank, world)
+        if "serve" in parts:
+            serving = measure_serving(local, fp32_cut, args.serve_window, rank, class_table=class_table)
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and "cpu" in parts:
         r, dt, passes = cpu_reference_rate(sh, os.cpu_count() or 1, CPU_SAMPLE_SECONDS)
         cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                "sample": f"{passes} full passes over the workload in {dt:.1f} s (oracle HGP, OpenMP)"}
@@ -465,6 +470,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--serve-window", type=float, default=5.0,
                     help="seconds of Poisson arrivals in the serving measurement")
+    ap.add_argument("--parts", default="batch,serve,cpu",
+                    help="extra measurements beside the headline workload (profiling runs "
+                         "pass an empty string)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
