@@ -835,6 +835,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         b1 = (int)(std::upper_bound(p->pair_mol.begin() + cls_start[cls], p->pair_mol.begin() + cls_start[cls + 1], m) -
                    p->pair_mol.begin());
     };
+    std::vector<int64_t> npp_prefix(npair + 1, 0);  // kept primitive pairs of pairs [0, k)
+    for (int k = 0; k < npair; ++k) npp_prefix[k + 1] = npp_prefix[k] + p->npp_h[k];
     std::vector<int4> chunks;
     struct CostedChunk { double cost; int4 c; };
     std::vector<CostedChunk> tmp;
@@ -889,8 +891,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                     }
                     for (int q0 = kbeg; q0 < kend; q0 += width) {
                         const int n = std::min(width, kend - q0);
-                        double kq = 0;
-                        for (int t = 0; t < n; ++t) kq += p->npp_h[q0 + t];
+                        const double kq = (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
                         const double cost = w * p->npp_h[pb] * kq;
                         total += cost;
                         tmp.push_back({cost, make_int4(pb, q0, n, m)});
@@ -1045,13 +1046,30 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
         int64_t sum = 0, sum2 = 0;
         for (int k : v) { sum += p->npp_h[k]; sum2 += (int64_t)p->npp_h[k] * p->npp_h[k]; }
         st->n_prim_quartets += (sum * sum + sum2) / 2;
-        for (size_t a = 0; a < v.size(); ++a)
-            for (size_t c = 0; c <= a; ++c) {
-                const double2 ba = p->bnd_h[v[a]], bc = p->bnd_h[v[c]];
-                if (ba.x * bc.x < p->opts.screen_cutoff) ++st->n_screened;
-                else if (p->opts.precision == MOLINTS_MIXED && ba.y * bc.y < p->opts.fp32_cutoff)
-                    ++st->n_fp32_quartets;
+        const bool mixed = p->opts.precision == MOLINTS_MIXED && p->opts.fp32_cutoff > 0.0;
+        if (p->opts.screen_cutoff > 0.0) {
+            // both conditions: the direct count over pair pairs
+            for (size_t a = 0; a < v.size(); ++a)
+                for (size_t c = 0; c <= a; ++c) {
+                    const double2 ba = p->bnd_h[v[a]], bc = p->bnd_h[v[c]];
+                    if (ba.x * bc.x < p->opts.screen_cutoff) ++st->n_screened;
+                    else if (mixed && ba.y * bc.y < p->opts.fp32_cutoff) ++st->n_fp32_quartets;
+                }
+        } else if (mixed) {
+            // unordered pairs {a, c} (a == c included) with y_a y_c < cut, from the sorted y:
+            // (sum_a #{c : y_c < cut / y_a} + #{a : y_a^2 < cut}) / 2
+            std::vector<double> y(v.size());
+            for (size_t a = 0; a < v.size(); ++a) y[a] = p->bnd_h[v[a]].y;
+            std::sort(y.begin(), y.end());
+            const double cut = p->opts.fp32_cutoff;
+            int64_t ordered = 0, diag = 0;
+            for (double ya : y) {
+                if (ya <= 0.0) { ordered += (int64_t)y.size(); diag += 1; continue; }
+                ordered += std::lower_bound(y.begin(), y.end(), cut / ya) - y.begin();
+                if (ya * ya < cut) ++diag;
             }
+            st->n_fp32_quartets += (ordered + diag) / 2;
+        }
     }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return MOLINTS_ERR_CUDA;
     if (p->n_launches > 0 && cudaEventSynchronize(ctx->ev1) == cudaSuccess) {

@@ -315,7 +315,7 @@ class Engine:
         opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff)
         st = Stats()
         self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
-                                                _ptr(out), 0, ctypes.byref(st)))
+                                                _ptr(out), 0, ctypes.byref(st) if with_stats else None))
         return (out, st.as_dict()) if with_stats else out
 
     def eri_packed_device(self, shells, out_device_ptr: int, precision=FP64, boys=BOYS_REFERENCE,
