@@ -103,6 +103,9 @@ typedef struct molints_stats {
     double device_ms;         /* device time of the last execute (CUDA events) */
     int64_t n_prim_pairs;     /* primitive pairs of all shell pairs */
     int64_t n_prim_pairs_kept;/* primitive pairs left after prim_cutoff */
+    /* host wall time of plan creation, ms: [0] tables before the bound pass, [1] the bound
+     * pass (upload, kernels, read-back), [2] screening and work queues, [3] upload */
+    double plan_ms[4];
 } molints_stats;
 
 typedef struct molints_ctx molints_ctx;

@@ -77,154 +77,154 @@ void launch_eri_fdps(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
 int occupancy_eri_fdps(int mixed);
 void launch_eri_ffss(const EriQueue &Q, int mixed, int grid, cudaStream_t s);
 int occupancy_eri_ffss(int mixed);
-void launch_rys_ssss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ssss();
+void launch_rys_ssss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ssss(int mixed);
 void launch_rys_bound_ssss(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_psss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_psss();
-void launch_rys_psps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_psps();
+void launch_rys_psss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_psss(int mixed);
+void launch_rys_psps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_psps(int mixed);
 void launch_rys_bound_psps(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_ppss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ppss();
-void launch_rys_ppps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ppps();
-void launch_rys_pppp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_pppp();
+void launch_rys_ppss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ppss(int mixed);
+void launch_rys_ppps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ppps(int mixed);
+void launch_rys_pppp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_pppp(int mixed);
 void launch_rys_bound_pppp(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_dsss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dsss();
-void launch_rys_dsps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dsps();
-void launch_rys_dspp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dspp();
-void launch_rys_dsds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dsds();
+void launch_rys_dsss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dsss(int mixed);
+void launch_rys_dsps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dsps(int mixed);
+void launch_rys_dspp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dspp(int mixed);
+void launch_rys_dsds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dsds(int mixed);
 void launch_rys_bound_dsds(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_dpss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dpss();
-void launch_rys_dpps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dpps();
-void launch_rys_dppp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dppp();
-void launch_rys_dpds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dpds();
-void launch_rys_dpdp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dpdp();
+void launch_rys_dpss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dpss(int mixed);
+void launch_rys_dpps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dpps(int mixed);
+void launch_rys_dppp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dppp(int mixed);
+void launch_rys_dpds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dpds(int mixed);
+void launch_rys_dpdp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dpdp(int mixed);
 void launch_rys_bound_dpdp(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_fsss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fsss();
-void launch_rys_fsps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fsps();
-void launch_rys_fspp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fspp();
-void launch_rys_fsds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fsds();
-void launch_rys_fsdp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fsdp();
-void launch_rys_fsfs(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fsfs();
+void launch_rys_fsss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fsss(int mixed);
+void launch_rys_fsps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fsps(int mixed);
+void launch_rys_fspp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fspp(int mixed);
+void launch_rys_fsds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fsds(int mixed);
+void launch_rys_fsdp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fsdp(int mixed);
+void launch_rys_fsfs(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fsfs(int mixed);
 void launch_rys_bound_fsfs(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_ddss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ddss();
-void launch_rys_ddps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ddps();
-void launch_rys_ddpp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ddpp();
-void launch_rys_ddds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ddds();
-void launch_rys_dddp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dddp();
-void launch_rys_ddfs(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ddfs();
-void launch_rys_dddd(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dddd();
+void launch_rys_ddss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ddss(int mixed);
+void launch_rys_ddps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ddps(int mixed);
+void launch_rys_ddpp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ddpp(int mixed);
+void launch_rys_ddds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ddds(int mixed);
+void launch_rys_dddp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dddp(int mixed);
+void launch_rys_ddfs(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ddfs(int mixed);
+void launch_rys_dddd(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dddd(int mixed);
 void launch_rys_bound_dddd(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_fpss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fpss();
-void launch_rys_fpps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fpps();
-void launch_rys_fppp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fppp();
-void launch_rys_fpds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fpds();
-void launch_rys_fpdp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fpdp();
-void launch_rys_fpfs(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fpfs();
-void launch_rys_fpdd(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fpdd();
-void launch_rys_fpfp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fpfp();
+void launch_rys_fpss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fpss(int mixed);
+void launch_rys_fpps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fpps(int mixed);
+void launch_rys_fppp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fppp(int mixed);
+void launch_rys_fpds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fpds(int mixed);
+void launch_rys_fpdp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fpdp(int mixed);
+void launch_rys_fpfs(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fpfs(int mixed);
+void launch_rys_fpdd(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fpdd(int mixed);
+void launch_rys_fpfp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fpfp(int mixed);
 void launch_rys_bound_fpfp(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_dfss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dfss();
-void launch_rys_dfps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dfps();
-void launch_rys_dfpp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dfpp();
-void launch_rys_dfds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dfds();
-void launch_rys_dfdp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dfdp();
-void launch_rys_dffs(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dffs();
-void launch_rys_dfdd(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dfdd();
-void launch_rys_dffp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dffp();
-void launch_rys_dfdf(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_dfdf();
+void launch_rys_dfss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dfss(int mixed);
+void launch_rys_dfps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dfps(int mixed);
+void launch_rys_dfpp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dfpp(int mixed);
+void launch_rys_dfds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dfds(int mixed);
+void launch_rys_dfdp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dfdp(int mixed);
+void launch_rys_dffs(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dffs(int mixed);
+void launch_rys_dfdd(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dfdd(int mixed);
+void launch_rys_dffp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dffp(int mixed);
+void launch_rys_dfdf(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_dfdf(int mixed);
 void launch_rys_bound_dfdf(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_fdss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fdss();
-void launch_rys_fdps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fdps();
-void launch_rys_fdpp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fdpp();
-void launch_rys_fdds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fdds();
-void launch_rys_fddp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fddp();
-void launch_rys_fdfs(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fdfs();
-void launch_rys_fddd(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fddd();
-void launch_rys_fdfp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fdfp();
-void launch_rys_fddf(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fddf();
-void launch_rys_fdfd(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fdfd();
+void launch_rys_fdss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fdss(int mixed);
+void launch_rys_fdps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fdps(int mixed);
+void launch_rys_fdpp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fdpp(int mixed);
+void launch_rys_fdds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fdds(int mixed);
+void launch_rys_fddp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fddp(int mixed);
+void launch_rys_fdfs(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fdfs(int mixed);
+void launch_rys_fddd(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fddd(int mixed);
+void launch_rys_fdfp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fdfp(int mixed);
+void launch_rys_fddf(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fddf(int mixed);
+void launch_rys_fdfd(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fdfd(int mixed);
 void launch_rys_bound_fdfd(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
-void launch_rys_ffss(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffss();
-void launch_rys_ffps(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffps();
-void launch_rys_ffpp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffpp();
-void launch_rys_ffds(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffds();
-void launch_rys_ffdp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffdp();
-void launch_rys_fffs(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fffs();
-void launch_rys_ffdd(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffdd();
-void launch_rys_fffp(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fffp();
-void launch_rys_ffdf(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffdf();
-void launch_rys_fffd(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_fffd();
-void launch_rys_ffff(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);
-int occupancy_rys_ffff();
+void launch_rys_ffss(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffss(int mixed);
+void launch_rys_ffps(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffps(int mixed);
+void launch_rys_ffpp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffpp(int mixed);
+void launch_rys_ffds(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffds(int mixed);
+void launch_rys_ffdp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffdp(int mixed);
+void launch_rys_fffs(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fffs(int mixed);
+void launch_rys_ffdd(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffdd(int mixed);
+void launch_rys_fffp(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fffp(int mixed);
+void launch_rys_ffdf(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffdf(int mixed);
+void launch_rys_fffd(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_fffd(int mixed);
+void launch_rys_ffff(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);
+int occupancy_rys_ffff(int mixed);
 void launch_rys_bound_ffff(const PairTab &P, const RysTab &R, int p0, int np, double2 *pbound, double *qout, int full, cudaStream_t s);
 typedef void (*EriLauncher)(const EriQueue &, int, int, cudaStream_t);
 typedef int (*EriOccupancy)(int);
 typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, double2 *, double *, int, cudaStream_t);
-typedef void (*RysLauncher)(const EriQueue &, const RysTab &, int, cudaStream_t);
-typedef int (*RysOccupancy)();
+typedef void (*RysLauncher)(const EriQueue &, const RysTab &, int, int, cudaStream_t);
+typedef int (*RysOccupancy)(int);
 typedef void (*RysBoundLauncher)(const PairTab &, const RysTab &, int, int, double2 *, double *, int, cudaStream_t);
 constexpr int kLmax = 3;      // shells up to f (Rys)
 constexpr int kLmaxHgp = 2;   // every class pair up to d has an HGP kernel

@@ -492,8 +492,8 @@ def emit_dispatch(pairs):
                          f"int np, double2 *pbound, double *qout, int full, cudaStream_t s);")
     for X, Y in gen_rys.class_pairs():
         t = tag_of(X, Y)
-        lines.append(f"void launch_rys_{t}(const EriQueue &Q, const RysTab &R, int grid, cudaStream_t s);")
-        lines.append(f"int occupancy_rys_{t}();")
+        lines.append(f"void launch_rys_{t}(const EriQueue &Q, const RysTab &R, int mixed, int grid, cudaStream_t s);")
+        lines.append(f"int occupancy_rys_{t}(int mixed);")
         if X == Y:
             lines.append(f"void launch_rys_bound_{t}(const PairTab &P, const RysTab &R, int p0, int np, "
                          f"double2 *pbound, double *qout, int full, cudaStream_t s);")
@@ -501,8 +501,8 @@ def emit_dispatch(pairs):
     lines.append("typedef int (*EriOccupancy)(int);")
     lines.append("typedef void (*SchwarzLauncher)(const PairTab &, const BoysTab &, int, int, "
                  "double2 *, double *, int, cudaStream_t);")
-    lines.append("typedef void (*RysLauncher)(const EriQueue &, const RysTab &, int, cudaStream_t);")
-    lines.append("typedef int (*RysOccupancy)();")
+    lines.append("typedef void (*RysLauncher)(const EriQueue &, const RysTab &, int, int, cudaStream_t);")
+    lines.append("typedef int (*RysOccupancy)(int);")
     lines.append("typedef void (*RysBoundLauncher)(const PairTab &, const RysTab &, int, int, "
                  "double2 *, double *, int, cudaStream_t);")
     lines.append(f"constexpr int kLmax = {gen_rys.LMAX};      // shells up to f (Rys)")

@@ -38,6 +38,10 @@ HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE / "generated"
 LMAX = 3             # shells up to f
 NMONO = 20           # monomials AB^(px,py,pz), px+py+pz <= 3
+# Classes with at least this many block entries and at most MIXED_MAX_ACC accumulators per
+# thread get an FP32 variant for MIXED quartets (stage-2 products summed in FP32 per batch).
+MIXED_MIN_NBLK = 100
+MIXED_MAX_ACC = 24
 
 
 def shell_components(l):
@@ -156,10 +160,11 @@ def class_tables(X, Y):
     nslot = max(1, min(npb, G // nblk)) if 2 * nblk <= G else 1
     acc = 1 if nslot > 1 else (nblk + G - 1) // G
     smem_group = 2 * NMONO + max(npb * nr * 3 * S, nblk + nab * nc, nslot * nblk)
+    mixed = nblk >= MIXED_MIN_NBLK and acc <= MIXED_MAX_ACC
     return dict(la=la, lb=lb, lc=lc, ld=ld, e=e, f=f, nr=nr, rows=rows, cols=cols, S=S,
                 blk=blk, bra=bra, ket=ket, norm_ab=norm_ab, norm_cd=norm_cd, na=na, nc=nc,
                 nblk=nblk, nab=nab, ncd=ncd, G=G, npb=npb, nslot=nslot, acc=acc,
-                smem_group=smem_group)
+                smem_group=smem_group, mixed=mixed)
 
 
 def _flat_terms(lists):
@@ -205,6 +210,16 @@ void launch_rys_bound_{tag}(const PairTab &P, const RysTab &R, int p0, int np, d
     rys_bound_kernel_{tag}<<<(np + ng - 1) / ng, 128, {smem_block}, s>>>(P, R, p0, np, pbound, qout, full);
 }}
 """
+    if t["mixed"]:
+        mixed_dispatch = (f"    if (mixed) rys_queue_{tag}<1><<<grid, 128, {smem_block}, s>>>(Q, R);\n"
+                          f"    else rys_queue_{tag}<0><<<grid, 128, {smem_block}, s>>>(Q, R);")
+        occ_dispatch = (f"    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_{tag}<1>, 128, {smem_block});\n"
+                        f"    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_{tag}<0>, 128, {smem_block});")
+    else:
+        mixed_dispatch = (f"    (void)mixed;  // no FP32 variant for this class\n"
+                          f"    rys_queue_{tag}<0><<<grid, 128, {smem_block}, s>>>(Q, R);")
+        occ_dispatch = (f"    (void)mixed;\n"
+                        f"    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_{tag}<0>, 128, {smem_block});")
     return f"""// Generated by gen_rys.py -- Rys class ({tag[0]}{tag[1]}|{tag[2]}{tag[3]}).  Do not edit.
 // roots {t['nr']}, block {t['na']} x {t['nc']}, outputs {t['nab']} x {t['ncd']}, group {t['G']} threads,
 // {t['npb']} primitive quartets per batch, {t['nslot']} slot(s), {t['acc']} accumulators per thread, {smem_block} B shared per block.
@@ -252,8 +267,9 @@ __device__ __forceinline__ RysClassTabs tabs_{tag}() {{
                         kNormAB_{tag}, kNormCD_{tag}}};
 }}
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_{tag}(const EriQueue Q, const RysTab R) {{
-    rys_queue_body<C_{tag}>(Q, R, tabs_{tag}());
+    rys_queue_body<C_{tag}, MIXED>(Q, R, tabs_{tag}());
 }}
 {bound_kernel}
 static void rys_prepare_{tag}() {{
@@ -261,26 +277,27 @@ static void rys_prepare_{tag}() {{
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {{
-        cudaFuncSetAttribute(rys_queue_{tag}, cudaFuncAttributeMaxDynamicSharedMemorySize, {smem_block});
+        cudaFuncSetAttribute(rys_queue_{tag}<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, {smem_block});
+{"        cudaFuncSetAttribute(rys_queue_" + tag + "<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, " + str(smem_block) + ");" if t["mixed"] else ""}
 {"        cudaFuncSetAttribute(rys_bound_kernel_" + tag + ", cudaFuncAttributeMaxDynamicSharedMemorySize, " + str(smem_block) + ");" if diag else ""}
         done[dev] = true;
     }}
 }}
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_{tag}(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {{
+void launch_rys_{tag}(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {{
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_{tag}();
     constexpr int ng = 128 / C_{tag}::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_{tag}<<<grid, 128, {smem_block}, s>>>(Q, R);
+{mixed_dispatch}
 }}
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_{tag}() {{
+int occupancy_rys_{tag}(int mixed) {{
     rys_prepare_{tag}();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_{tag}, 128, {smem_block});
+{occ_dispatch}
     return n;
 }}
 {bound_launch}

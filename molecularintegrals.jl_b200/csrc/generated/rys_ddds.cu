@@ -82,8 +82,9 @@ __device__ __forceinline__ RysClassTabs tabs_ddds() {
                         kNormAB_ddds, kNormCD_ddds};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_ddds(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_ddds>(Q, R, tabs_ddds());
+    rys_queue_body<C_ddds, MIXED>(Q, R, tabs_ddds());
 }
 
 static void rys_prepare_ddds() {
@@ -91,26 +92,29 @@ static void rys_prepare_ddds() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ddds, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
+        cudaFuncSetAttribute(rys_queue_ddds<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
+        cudaFuncSetAttribute(rys_queue_ddds<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_ddds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_ddds(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_ddds();
     constexpr int ng = 128 / C_ddds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ddds<<<grid, 128, 46720, s>>>(Q, R);
+    if (mixed) rys_queue_ddds<1><<<grid, 128, 46720, s>>>(Q, R);
+    else rys_queue_ddds<0><<<grid, 128, 46720, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_ddds() {
+int occupancy_rys_ddds(int mixed) {
     rys_prepare_ddds();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddds, 128, 46720);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddds<1>, 128, 46720);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddds<0>, 128, 46720);
     return n;
 }
 

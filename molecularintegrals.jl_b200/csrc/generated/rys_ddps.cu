@@ -73,8 +73,9 @@ __device__ __forceinline__ RysClassTabs tabs_ddps() {
                         kNormAB_ddps, kNormCD_ddps};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_ddps(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_ddps>(Q, R, tabs_ddps());
+    rys_queue_body<C_ddps, MIXED>(Q, R, tabs_ddps());
 }
 
 static void rys_prepare_ddps() {
@@ -82,26 +83,29 @@ static void rys_prepare_ddps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ddps, cudaFuncAttributeMaxDynamicSharedMemorySize, 30080);
+        cudaFuncSetAttribute(rys_queue_ddps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 30080);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_ddps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_ddps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_ddps();
     constexpr int ng = 128 / C_ddps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ddps<<<grid, 128, 30080, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_ddps<0><<<grid, 128, 30080, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_ddps() {
+int occupancy_rys_ddps(int mixed) {
     rys_prepare_ddps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddps, 128, 30080);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddps<0>, 128, 30080);
     return n;
 }
 

@@ -68,8 +68,9 @@ __device__ __forceinline__ RysClassTabs tabs_ddss() {
                         kNormAB_ddss, kNormCD_ddss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_ddss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_ddss>(Q, R, tabs_ddss());
+    rys_queue_body<C_ddss, MIXED>(Q, R, tabs_ddss());
 }
 
 static void rys_prepare_ddss() {
@@ -77,26 +78,29 @@ static void rys_prepare_ddss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ddss, cudaFuncAttributeMaxDynamicSharedMemorySize, 15680);
+        cudaFuncSetAttribute(rys_queue_ddss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 15680);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_ddss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_ddss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_ddss();
     constexpr int ng = 128 / C_ddss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ddss<<<grid, 128, 15680, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_ddss<0><<<grid, 128, 15680, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_ddss() {
+int occupancy_rys_ddss(int mixed) {
     rys_prepare_ddss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddss, 128, 15680);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ddss<0>, 128, 15680);
     return n;
 }
 

@@ -80,8 +80,9 @@ __device__ __forceinline__ RysClassTabs tabs_dpdp() {
                         kNormAB_dpdp, kNormCD_dpdp};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dpdp(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dpdp>(Q, R, tabs_dpdp());
+    rys_queue_body<C_dpdp, MIXED>(Q, R, tabs_dpdp());
 }
 
 __global__ void __launch_bounds__(128) rys_bound_kernel_dpdp(PairTab P, RysTab R, int p0, int np,
@@ -94,26 +95,29 @@ static void rys_prepare_dpdp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
+        cudaFuncSetAttribute(rys_queue_dpdp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
+        cudaFuncSetAttribute(rys_queue_dpdp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
         cudaFuncSetAttribute(rys_bound_kernel_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dpdp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dpdp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dpdp();
     constexpr int ng = 128 / C_dpdp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dpdp<<<grid, 128, 49792, s>>>(Q, R);
+    if (mixed) rys_queue_dpdp<1><<<grid, 128, 49792, s>>>(Q, R);
+    else rys_queue_dpdp<0><<<grid, 128, 49792, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dpdp() {
+int occupancy_rys_dpdp(int mixed) {
     rys_prepare_dpdp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp, 128, 49792);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp<1>, 128, 49792);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp<0>, 128, 49792);
     return n;
 }
 

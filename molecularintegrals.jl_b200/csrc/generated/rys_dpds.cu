@@ -60,8 +60,9 @@ __device__ __forceinline__ RysClassTabs tabs_dpds() {
                         kNormAB_dpds, kNormCD_dpds};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dpds(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dpds>(Q, R, tabs_dpds());
+    rys_queue_body<C_dpds, MIXED>(Q, R, tabs_dpds());
 }
 
 static void rys_prepare_dpds() {
@@ -69,26 +70,29 @@ static void rys_prepare_dpds() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpds, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
+        cudaFuncSetAttribute(rys_queue_dpds<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dpds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dpds(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dpds();
     constexpr int ng = 128 / C_dpds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dpds<<<grid, 128, 35840, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_dpds<0><<<grid, 128, 35840, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dpds() {
+int occupancy_rys_dpds(int mixed) {
     rys_prepare_dpds();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpds, 128, 35840);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpds<0>, 128, 35840);
     return n;
 }
 

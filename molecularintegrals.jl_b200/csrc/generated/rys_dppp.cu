@@ -66,8 +66,9 @@ __device__ __forceinline__ RysClassTabs tabs_dppp() {
                         kNormAB_dppp, kNormCD_dppp};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dppp(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dppp>(Q, R, tabs_dppp());
+    rys_queue_body<C_dppp, MIXED>(Q, R, tabs_dppp());
 }
 
 static void rys_prepare_dppp() {
@@ -75,26 +76,29 @@ static void rys_prepare_dppp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 36928);
+        cudaFuncSetAttribute(rys_queue_dppp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 36928);
+        cudaFuncSetAttribute(rys_queue_dppp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 36928);
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dppp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dppp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dppp();
     constexpr int ng = 128 / C_dppp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dppp<<<grid, 128, 36928, s>>>(Q, R);
+    if (mixed) rys_queue_dppp<1><<<grid, 128, 36928, s>>>(Q, R);
+    else rys_queue_dppp<0><<<grid, 128, 36928, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dppp() {
+int occupancy_rys_dppp(int mixed) {
     rys_prepare_dppp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dppp, 128, 36928);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dppp<1>, 128, 36928);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dppp<0>, 128, 36928);
     return n;
 }
 

@@ -55,8 +55,9 @@ __device__ __forceinline__ RysClassTabs tabs_dpps() {
                         kNormAB_dpps, kNormCD_dpps};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dpps(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dpps>(Q, R, tabs_dpps());
+    rys_queue_body<C_dpps, MIXED>(Q, R, tabs_dpps());
 }
 
 static void rys_prepare_dpps() {
@@ -64,26 +65,29 @@ static void rys_prepare_dpps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpps, cudaFuncAttributeMaxDynamicSharedMemorySize, 24320);
+        cudaFuncSetAttribute(rys_queue_dpps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 24320);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dpps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dpps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dpps();
     constexpr int ng = 128 / C_dpps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dpps<<<grid, 128, 24320, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_dpps<0><<<grid, 128, 24320, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dpps() {
+int occupancy_rys_dpps(int mixed) {
     rys_prepare_dpps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpps, 128, 24320);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpps<0>, 128, 24320);
     return n;
 }
 

@@ -53,8 +53,9 @@ __device__ __forceinline__ RysClassTabs tabs_dpss() {
                         kNormAB_dpss, kNormCD_dpss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dpss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dpss>(Q, R, tabs_dpss());
+    rys_queue_body<C_dpss, MIXED>(Q, R, tabs_dpss());
 }
 
 static void rys_prepare_dpss() {
@@ -62,26 +63,29 @@ static void rys_prepare_dpss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpss, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+        cudaFuncSetAttribute(rys_queue_dpss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dpss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dpss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dpss();
     constexpr int ng = 128 / C_dpss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dpss<<<grid, 128, 13568, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_dpss<0><<<grid, 128, 13568, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dpss() {
+int occupancy_rys_dpss(int mixed) {
     rys_prepare_dpss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpss, 128, 13568);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpss<0>, 128, 13568);
     return n;
 }
 

@@ -53,8 +53,9 @@ __device__ __forceinline__ RysClassTabs tabs_dspp() {
                         kNormAB_dspp, kNormCD_dspp};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dspp(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dspp>(Q, R, tabs_dspp());
+    rys_queue_body<C_dspp, MIXED>(Q, R, tabs_dspp());
 }
 
 static void rys_prepare_dspp() {
@@ -62,26 +63,29 @@ static void rys_prepare_dspp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dspp, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
+        cudaFuncSetAttribute(rys_queue_dspp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dspp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dspp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dspp();
     constexpr int ng = 128 / C_dspp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dspp<<<grid, 128, 27200, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_dspp<0><<<grid, 128, 27200, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dspp() {
+int occupancy_rys_dspp(int mixed) {
     rys_prepare_dspp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp, 128, 27200);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp<0>, 128, 27200);
     return n;
 }
 

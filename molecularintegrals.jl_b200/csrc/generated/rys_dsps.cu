@@ -47,8 +47,9 @@ __device__ __forceinline__ RysClassTabs tabs_dsps() {
                         kNormAB_dsps, kNormCD_dsps};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dsps(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dsps>(Q, R, tabs_dsps());
+    rys_queue_body<C_dsps, MIXED>(Q, R, tabs_dsps());
 }
 
 static void rys_prepare_dsps() {
@@ -56,26 +57,29 @@ static void rys_prepare_dsps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dsps, cudaFuncAttributeMaxDynamicSharedMemorySize, 19712);
+        cudaFuncSetAttribute(rys_queue_dsps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 19712);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dsps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dsps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dsps();
     constexpr int ng = 128 / C_dsps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dsps<<<grid, 128, 19712, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_dsps<0><<<grid, 128, 19712, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dsps() {
+int occupancy_rys_dsps(int mixed) {
     rys_prepare_dsps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsps, 128, 19712);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsps<0>, 128, 19712);
     return n;
 }
 

@@ -46,8 +46,9 @@ __device__ __forceinline__ RysClassTabs tabs_dsss() {
                         kNormAB_dsss, kNormCD_dsss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_dsss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_dsss>(Q, R, tabs_dsss());
+    rys_queue_body<C_dsss, MIXED>(Q, R, tabs_dsss());
 }
 
 static void rys_prepare_dsss() {
@@ -55,26 +56,29 @@ static void rys_prepare_dsss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dsss, cudaFuncAttributeMaxDynamicSharedMemorySize, 10496);
+        cudaFuncSetAttribute(rys_queue_dsss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 10496);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_dsss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_dsss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_dsss();
     constexpr int ng = 128 / C_dsss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_dsss<<<grid, 128, 10496, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_dsss<0><<<grid, 128, 10496, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_dsss() {
+int occupancy_rys_dsss(int mixed) {
     rys_prepare_dsss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsss, 128, 10496);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dsss<0>, 128, 10496);
     return n;
 }
 

@@ -84,8 +84,9 @@ __device__ __forceinline__ RysClassTabs tabs_fdss() {
                         kNormAB_fdss, kNormCD_fdss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fdss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fdss>(Q, R, tabs_fdss());
+    rys_queue_body<C_fdss, MIXED>(Q, R, tabs_fdss());
 }
 
 static void rys_prepare_fdss() {
@@ -93,26 +94,29 @@ static void rys_prepare_fdss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fdss, cudaFuncAttributeMaxDynamicSharedMemorySize, 18560);
+        cudaFuncSetAttribute(rys_queue_fdss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 18560);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fdss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fdss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fdss();
     constexpr int ng = 128 / C_fdss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fdss<<<grid, 128, 18560, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_fdss<0><<<grid, 128, 18560, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fdss() {
+int occupancy_rys_fdss(int mixed) {
     rys_prepare_fdss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fdss, 128, 18560);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fdss<0>, 128, 18560);
     return n;
 }
 

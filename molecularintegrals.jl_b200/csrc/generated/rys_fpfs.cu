@@ -80,8 +80,9 @@ __device__ __forceinline__ RysClassTabs tabs_fpfs() {
                         kNormAB_fpfs, kNormCD_fpfs};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fpfs(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fpfs>(Q, R, tabs_fpfs());
+    rys_queue_body<C_fpfs, MIXED>(Q, R, tabs_fpfs());
 }
 
 static void rys_prepare_fpfs() {
@@ -89,26 +90,29 @@ static void rys_prepare_fpfs() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fpfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 62080);
+        cudaFuncSetAttribute(rys_queue_fpfs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 62080);
+        cudaFuncSetAttribute(rys_queue_fpfs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 62080);
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fpfs(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fpfs(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fpfs();
     constexpr int ng = 128 / C_fpfs::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fpfs<<<grid, 128, 62080, s>>>(Q, R);
+    if (mixed) rys_queue_fpfs<1><<<grid, 128, 62080, s>>>(Q, R);
+    else rys_queue_fpfs<0><<<grid, 128, 62080, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fpfs() {
+int occupancy_rys_fpfs(int mixed) {
     rys_prepare_fpfs();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpfs, 128, 62080);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpfs<1>, 128, 62080);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpfs<0>, 128, 62080);
     return n;
 }
 

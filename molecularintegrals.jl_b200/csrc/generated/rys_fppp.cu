@@ -79,8 +79,9 @@ __device__ __forceinline__ RysClassTabs tabs_fppp() {
                         kNormAB_fppp, kNormCD_fppp};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fppp(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fppp>(Q, R, tabs_fppp());
+    rys_queue_body<C_fppp, MIXED>(Q, R, tabs_fppp());
 }
 
 static void rys_prepare_fppp() {
@@ -88,26 +89,29 @@ static void rys_prepare_fppp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
+        cudaFuncSetAttribute(rys_queue_fppp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
+        cudaFuncSetAttribute(rys_queue_fppp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 46720);
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fppp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fppp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fppp();
     constexpr int ng = 128 / C_fppp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fppp<<<grid, 128, 46720, s>>>(Q, R);
+    if (mixed) rys_queue_fppp<1><<<grid, 128, 46720, s>>>(Q, R);
+    else rys_queue_fppp<0><<<grid, 128, 46720, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fppp() {
+int occupancy_rys_fppp(int mixed) {
     rys_prepare_fppp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fppp, 128, 46720);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fppp<1>, 128, 46720);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fppp<0>, 128, 46720);
     return n;
 }
 

@@ -64,8 +64,9 @@ __device__ __forceinline__ RysClassTabs tabs_fpps() {
                         kNormAB_fpps, kNormCD_fpps};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fpps(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fpps>(Q, R, tabs_fpps());
+    rys_queue_body<C_fpps, MIXED>(Q, R, tabs_fpps());
 }
 
 static void rys_prepare_fpps() {
@@ -73,26 +74,29 @@ static void rys_prepare_fpps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fpps, cudaFuncAttributeMaxDynamicSharedMemorySize, 30080);
+        cudaFuncSetAttribute(rys_queue_fpps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 30080);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fpps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fpps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fpps();
     constexpr int ng = 128 / C_fpps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fpps<<<grid, 128, 30080, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_fpps<0><<<grid, 128, 30080, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fpps() {
+int occupancy_rys_fpps(int mixed) {
     rys_prepare_fpps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpps, 128, 30080);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpps<0>, 128, 30080);
     return n;
 }
 

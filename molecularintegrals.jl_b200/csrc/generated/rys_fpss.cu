@@ -60,8 +60,9 @@ __device__ __forceinline__ RysClassTabs tabs_fpss() {
                         kNormAB_fpss, kNormCD_fpss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fpss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fpss>(Q, R, tabs_fpss());
+    rys_queue_body<C_fpss, MIXED>(Q, R, tabs_fpss());
 }
 
 static void rys_prepare_fpss() {
@@ -69,26 +70,29 @@ static void rys_prepare_fpss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fpss, cudaFuncAttributeMaxDynamicSharedMemorySize, 15680);
+        cudaFuncSetAttribute(rys_queue_fpss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 15680);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fpss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fpss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fpss();
     constexpr int ng = 128 / C_fpss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fpss<<<grid, 128, 15680, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_fpss<0><<<grid, 128, 15680, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fpss() {
+int occupancy_rys_fpss(int mixed) {
     rys_prepare_fpss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpss, 128, 15680);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpss<0>, 128, 15680);
     return n;
 }
 

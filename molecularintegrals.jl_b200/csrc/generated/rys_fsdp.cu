@@ -67,8 +67,9 @@ __device__ __forceinline__ RysClassTabs tabs_fsdp() {
                         kNormAB_fsdp, kNormCD_fsdp};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fsdp(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fsdp>(Q, R, tabs_fsdp());
+    rys_queue_body<C_fsdp, MIXED>(Q, R, tabs_fsdp());
 }
 
 static void rys_prepare_fsdp() {
@@ -76,26 +77,29 @@ static void rys_prepare_fsdp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
+        cudaFuncSetAttribute(rys_queue_fsdp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
+        cudaFuncSetAttribute(rys_queue_fsdp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fsdp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fsdp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fsdp();
     constexpr int ng = 128 / C_fsdp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsdp<<<grid, 128, 49792, s>>>(Q, R);
+    if (mixed) rys_queue_fsdp<1><<<grid, 128, 49792, s>>>(Q, R);
+    else rys_queue_fsdp<0><<<grid, 128, 49792, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fsdp() {
+int occupancy_rys_fsdp(int mixed) {
     rys_prepare_fsdp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsdp, 128, 49792);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsdp<1>, 128, 49792);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsdp<0>, 128, 49792);
     return n;
 }
 

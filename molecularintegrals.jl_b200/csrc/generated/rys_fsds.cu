@@ -52,8 +52,9 @@ __device__ __forceinline__ RysClassTabs tabs_fsds() {
                         kNormAB_fsds, kNormCD_fsds};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fsds(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fsds>(Q, R, tabs_fsds());
+    rys_queue_body<C_fsds, MIXED>(Q, R, tabs_fsds());
 }
 
 static void rys_prepare_fsds() {
@@ -61,26 +62,29 @@ static void rys_prepare_fsds() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsds, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
+        cudaFuncSetAttribute(rys_queue_fsds<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fsds(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fsds(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fsds();
     constexpr int ng = 128 / C_fsds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsds<<<grid, 128, 35840, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_fsds<0><<<grid, 128, 35840, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fsds() {
+int occupancy_rys_fsds(int mixed) {
     rys_prepare_fsds();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsds, 128, 35840);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsds<0>, 128, 35840);
     return n;
 }
 

@@ -57,8 +57,9 @@ __device__ __forceinline__ RysClassTabs tabs_fsfs() {
                         kNormAB_fsfs, kNormCD_fsfs};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fsfs(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fsfs>(Q, R, tabs_fsfs());
+    rys_queue_body<C_fsfs, MIXED>(Q, R, tabs_fsfs());
 }
 
 __global__ void __launch_bounds__(128) rys_bound_kernel_fsfs(PairTab P, RysTab R, int p0, int np,
@@ -71,26 +72,29 @@ static void rys_prepare_fsfs() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
+        cudaFuncSetAttribute(rys_queue_fsfs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
+        cudaFuncSetAttribute(rys_queue_fsfs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
         cudaFuncSetAttribute(rys_bound_kernel_fsfs, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fsfs(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fsfs(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fsfs();
     constexpr int ng = 128 / C_fsfs::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsfs<<<grid, 128, 50432, s>>>(Q, R);
+    if (mixed) rys_queue_fsfs<1><<<grid, 128, 50432, s>>>(Q, R);
+    else rys_queue_fsfs<0><<<grid, 128, 50432, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fsfs() {
+int occupancy_rys_fsfs(int mixed) {
     rys_prepare_fsfs();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsfs, 128, 50432);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsfs<1>, 128, 50432);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsfs<0>, 128, 50432);
     return n;
 }
 

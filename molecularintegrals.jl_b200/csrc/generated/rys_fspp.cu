@@ -57,8 +57,9 @@ __device__ __forceinline__ RysClassTabs tabs_fspp() {
                         kNormAB_fspp, kNormCD_fspp};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fspp(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fspp>(Q, R, tabs_fspp());
+    rys_queue_body<C_fspp, MIXED>(Q, R, tabs_fspp());
 }
 
 static void rys_prepare_fspp() {
@@ -66,26 +67,29 @@ static void rys_prepare_fspp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fspp, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
+        cudaFuncSetAttribute(rys_queue_fspp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fspp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fspp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fspp();
     constexpr int ng = 128 / C_fspp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fspp<<<grid, 128, 35840, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_fspp<0><<<grid, 128, 35840, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fspp() {
+int occupancy_rys_fspp(int mixed) {
     rys_prepare_fspp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fspp, 128, 35840);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fspp<0>, 128, 35840);
     return n;
 }
 

@@ -49,8 +49,9 @@ __device__ __forceinline__ RysClassTabs tabs_fsps() {
                         kNormAB_fsps, kNormCD_fsps};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fsps(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fsps>(Q, R, tabs_fsps());
+    rys_queue_body<C_fsps, MIXED>(Q, R, tabs_fsps());
 }
 
 static void rys_prepare_fsps() {
@@ -58,26 +59,29 @@ static void rys_prepare_fsps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsps, cudaFuncAttributeMaxDynamicSharedMemorySize, 24320);
+        cudaFuncSetAttribute(rys_queue_fsps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 24320);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fsps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fsps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fsps();
     constexpr int ng = 128 / C_fsps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsps<<<grid, 128, 24320, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_fsps<0><<<grid, 128, 24320, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fsps() {
+int occupancy_rys_fsps(int mixed) {
     rys_prepare_fsps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsps, 128, 24320);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsps<0>, 128, 24320);
     return n;
 }
 

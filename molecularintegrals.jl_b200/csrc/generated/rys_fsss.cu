@@ -47,8 +47,9 @@ __device__ __forceinline__ RysClassTabs tabs_fsss() {
                         kNormAB_fsss, kNormCD_fsss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_fsss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_fsss>(Q, R, tabs_fsss());
+    rys_queue_body<C_fsss, MIXED>(Q, R, tabs_fsss());
 }
 
 static void rys_prepare_fsss() {
@@ -56,26 +57,29 @@ static void rys_prepare_fsss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_fsss, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+        cudaFuncSetAttribute(rys_queue_fsss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_fsss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_fsss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_fsss();
     constexpr int ng = 128 / C_fsss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_fsss<<<grid, 128, 13568, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_fsss<0><<<grid, 128, 13568, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_fsss() {
+int occupancy_rys_fsss(int mixed) {
     rys_prepare_fsss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsss, 128, 13568);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fsss<0>, 128, 13568);
     return n;
 }
 

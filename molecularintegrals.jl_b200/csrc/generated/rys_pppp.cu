@@ -57,8 +57,9 @@ __device__ __forceinline__ RysClassTabs tabs_pppp() {
                         kNormAB_pppp, kNormCD_pppp};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_pppp(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_pppp>(Q, R, tabs_pppp());
+    rys_queue_body<C_pppp, MIXED>(Q, R, tabs_pppp());
 }
 
 __global__ void __launch_bounds__(128) rys_bound_kernel_pppp(PairTab P, RysTab R, int p0, int np,
@@ -71,26 +72,29 @@ static void rys_prepare_pppp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_pppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
+        cudaFuncSetAttribute(rys_queue_pppp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
+
         cudaFuncSetAttribute(rys_bound_kernel_pppp, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_pppp(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_pppp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_pppp();
     constexpr int ng = 128 / C_pppp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_pppp<<<grid, 128, 27200, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_pppp<0><<<grid, 128, 27200, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_pppp() {
+int occupancy_rys_pppp(int mixed) {
     rys_prepare_pppp();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_pppp, 128, 27200);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_pppp<0>, 128, 27200);
     return n;
 }
 

@@ -50,8 +50,9 @@ __device__ __forceinline__ RysClassTabs tabs_ppps() {
                         kNormAB_ppps, kNormCD_ppps};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_ppps(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_ppps>(Q, R, tabs_ppps());
+    rys_queue_body<C_ppps, MIXED>(Q, R, tabs_ppps());
 }
 
 static void rys_prepare_ppps() {
@@ -59,26 +60,29 @@ static void rys_prepare_ppps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ppps, cudaFuncAttributeMaxDynamicSharedMemorySize, 19712);
+        cudaFuncSetAttribute(rys_queue_ppps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 19712);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_ppps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_ppps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_ppps();
     constexpr int ng = 128 / C_ppps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ppps<<<grid, 128, 19712, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_ppps<0><<<grid, 128, 19712, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_ppps() {
+int occupancy_rys_ppps(int mixed) {
     rys_prepare_ppps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppps, 128, 19712);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppps<0>, 128, 19712);
     return n;
 }
 

@@ -48,8 +48,9 @@ __device__ __forceinline__ RysClassTabs tabs_ppss() {
                         kNormAB_ppss, kNormCD_ppss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_ppss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_ppss>(Q, R, tabs_ppss());
+    rys_queue_body<C_ppss, MIXED>(Q, R, tabs_ppss());
 }
 
 static void rys_prepare_ppss() {
@@ -57,26 +58,29 @@ static void rys_prepare_ppss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ppss, cudaFuncAttributeMaxDynamicSharedMemorySize, 10496);
+        cudaFuncSetAttribute(rys_queue_ppss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 10496);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_ppss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_ppss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_ppss();
     constexpr int ng = 128 / C_ppss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ppss<<<grid, 128, 10496, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_ppss<0><<<grid, 128, 10496, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_ppss() {
+int occupancy_rys_ppss(int mixed) {
     rys_prepare_ppss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppss, 128, 10496);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ppss<0>, 128, 10496);
     return n;
 }
 

@@ -45,8 +45,9 @@ __device__ __forceinline__ RysClassTabs tabs_psps() {
                         kNormAB_psps, kNormCD_psps};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_psps(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_psps>(Q, R, tabs_psps());
+    rys_queue_body<C_psps, MIXED>(Q, R, tabs_psps());
 }
 
 __global__ void __launch_bounds__(128) rys_bound_kernel_psps(PairTab P, RysTab R, int p0, int np,
@@ -59,26 +60,29 @@ static void rys_prepare_psps() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_psps, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+        cudaFuncSetAttribute(rys_queue_psps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
+
         cudaFuncSetAttribute(rys_bound_kernel_psps, cudaFuncAttributeMaxDynamicSharedMemorySize, 13568);
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_psps(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_psps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_psps();
     constexpr int ng = 128 / C_psps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_psps<<<grid, 128, 13568, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_psps<0><<<grid, 128, 13568, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_psps() {
+int occupancy_rys_psps(int mixed) {
     rys_prepare_psps();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psps, 128, 13568);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psps<0>, 128, 13568);
     return n;
 }
 

@@ -45,8 +45,9 @@ __device__ __forceinline__ RysClassTabs tabs_psss() {
                         kNormAB_psss, kNormCD_psss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_psss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_psss>(Q, R, tabs_psss());
+    rys_queue_body<C_psss, MIXED>(Q, R, tabs_psss());
 }
 
 static void rys_prepare_psss() {
@@ -54,26 +55,29 @@ static void rys_prepare_psss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_psss, cudaFuncAttributeMaxDynamicSharedMemorySize, 7424);
+        cudaFuncSetAttribute(rys_queue_psss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 7424);
+
 
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_psss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_psss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_psss();
     constexpr int ng = 128 / C_psss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_psss<<<grid, 128, 7424, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_psss<0><<<grid, 128, 7424, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_psss() {
+int occupancy_rys_psss(int mixed) {
     rys_prepare_psss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psss, 128, 7424);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_psss<0>, 128, 7424);
     return n;
 }
 

@@ -45,8 +45,9 @@ __device__ __forceinline__ RysClassTabs tabs_ssss() {
                         kNormAB_ssss, kNormCD_ssss};
 }
 
+template <int MIXED>
 __global__ void __launch_bounds__(128) rys_queue_ssss(const EriQueue Q, const RysTab R) {
-    rys_queue_body<C_ssss>(Q, R, tabs_ssss());
+    rys_queue_body<C_ssss, MIXED>(Q, R, tabs_ssss());
 }
 
 __global__ void __launch_bounds__(128) rys_bound_kernel_ssss(PairTab P, RysTab R, int p0, int np,
@@ -59,26 +60,29 @@ static void rys_prepare_ssss() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_ssss, cudaFuncAttributeMaxDynamicSharedMemorySize, 4352);
+        cudaFuncSetAttribute(rys_queue_ssss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4352);
+
         cudaFuncSetAttribute(rys_bound_kernel_ssss, cudaFuncAttributeMaxDynamicSharedMemorySize, 4352);
         done[dev] = true;
     }
 }
 
 // grid_max: resident blocks on the device; the grid is cut to the chunks' groups.
-void launch_rys_ssss(const EriQueue &Q, const RysTab &R, int grid_max, cudaStream_t s) {
+void launch_rys_ssss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid_max <= 0) return;
     rys_prepare_ssss();
     constexpr int ng = 128 / C_ssss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    rys_queue_ssss<<<grid, 128, 4352, s>>>(Q, R);
+    (void)mixed;  // no FP32 variant for this class
+    rys_queue_ssss<0><<<grid, 128, 4352, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
-int occupancy_rys_ssss() {
+int occupancy_rys_ssss(int mixed) {
     rys_prepare_ssss();
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ssss, 128, 4352);
+    (void)mixed;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_ssss<0>, 128, 4352);
     return n;
 }
 

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -45,8 +46,9 @@ struct molints_ctx {
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork = nullptr, join[kSide] = {};
     int num_sms = 0;
-    // blocks/SM of the queue kernels, 0 = not queried: [x][y][HGP FP64, HGP MIXED, Rys]
-    int occupancy[kNumPairClasses][kNumPairClasses][3] = {};
+    // blocks/SM of the queue kernels, 0 = not queried: [x][y][HGP FP64, HGP MIXED, Rys FP64,
+    // Rys MIXED]
+    int occupancy[kNumPairClasses][kNumPairClasses][4] = {};
     RysTab rys{};  // device addresses of the Rys root/weight tables on this device
     int32_t class_method[kNumPairClasses][kNumPairClasses] = {};  // AUTO choices (0 = default)
     std::string err;
@@ -88,6 +90,7 @@ struct molints_plan {
     double *qcon = nullptr;  // contracted Schwarz bounds, filled on demand by plan_schwarz
     int64_t bytes = 0;
     int n_launches = 0;
+    double plan_ms[4] = {0, 0, 0, 0};  // plan creation phases (molints_stats.plan_ms)
     // per-launch profiling (molints_plan_set_profiling)
     int profiling = 0;
     std::vector<cudaEvent_t> prof_ev;
@@ -573,6 +576,11 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown method");
     if (!(opts.fp32_cutoff >= 0.0) || !(opts.screen_cutoff >= 0.0) || !(opts.prim_cutoff >= 0.0))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: cutoffs must be >= 0");
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point t0) {
+        return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+    };
+    clk::time_point t_phase = clk::now();
 
     // ---- molecules: validation, output offsets, global shell and primitive arrays
     std::vector<int> shell_off(nmol + 1, 0), prim_base(nmol + 1, 0);
@@ -713,6 +721,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     const int64_t nall = (int64_t)src_h.size();
     p->nprim_pair_all = nall;
 
+    p->plan_ms[0] = ms_since(t_phase);
+    t_phase = clk::now();
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) { plan_free(p); return cuda_fail(ctx, e, "cudaSetDevice"); }
     double2 *pbound = nullptr;
@@ -772,6 +782,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     dev_free(ctx, pbound);
     ctx->held -= scratch;
 
+    p->plan_ms[1] = ms_since(t_phase);
+    t_phase = clk::now();
     // ---- stage 2: drop primitive pairs i with b_i * max Qabs (of the same molecule) below
     // prim_cutoff -- each dropped term of any integral is below prim_cutoff by the Schwarz
     // inequality -- and record each pair's bounds.
@@ -918,6 +930,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         }
     std::vector<long long> mol_out_ll(std::max(nmol, 1), 0);
     for (int m = 0; m < nmol; ++m) mol_out_ll[m] = (long long)p->mol_out_h[m];
+    p->plan_ms[2] = ms_since(t_phase);
+    t_phase = clk::now();
     rc = dev_alloc(ctx, &p->chunks, chunks.size(), &p->bytes);
     if (rc) { plan_free(p); return rc; }
     if ((e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
@@ -934,6 +948,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         return cuda_fail(ctx, e, "plan_create upload");
     }
     (void)mol_cls_start;
+    p->plan_ms[3] = ms_since(t_phase);
     *out = p;
     return MOLINTS_OK;
 }
@@ -996,8 +1011,8 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         const int x = jobs[k].x, y = jobs[k].y;
         cudaStream_t st = nside ? ctx->side[k % nside] : s;
         const bool rys = p->method[x][y] == MOLINTS_METHOD_RYS;
-        int &occ = ctx->occupancy[x][y][rys ? 2 : mixed];
-        if (occ == 0) occ = std::max(1, rys ? kRysOccupancy[x][y]() : kEriOccupancy[x][y](mixed));
+        int &occ = ctx->occupancy[x][y][(rys ? 2 : 0) + mixed];
+        if (occ == 0) occ = std::max(1, rys ? kRysOccupancy[x][y](mixed) : kEriOccupancy[x][y](mixed));
         EriQueue Q{};
         Q.pairs = P;
         Q.boys = B;
@@ -1013,7 +1028,7 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
                              : (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);
         const char *name = rys ? kRysNames[x][y] : kEriNames[x][y];
         if (int rc = mark(launches, name, 0, st)) return rc;
-        if (rys) kRysLaunchers[x][y](Q, ctx->rys, grid, st);
+        if (rys) kRysLaunchers[x][y](Q, ctx->rys, mixed, grid, st);
         else kEriLaunchers[x][y](Q, mixed, grid, st);
         if (int rc = mark(launches, name, 1, st)) return rc;
         ++launches;
@@ -1036,6 +1051,7 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
     st->n_kernel_launches = p->n_launches;
     st->n_prim_pairs = p->nprim_pair_all;
     st->n_prim_pairs_kept = p->nprim_pair_kept;
+    for (int k = 0; k < 4; ++k) st->plan_ms[k] = p->plan_ms[k];
     // per molecule: its pairs are interleaved by class, so gather them first
     std::vector<std::vector<int>> by_mol(std::max(p->nmol, 1));
     for (int k = 0; k < p->npair; ++k) by_mol[p->pair_mol[k]].push_back(k);

@@ -15,6 +15,7 @@
 // src/Rys.jl:59-156.
 #pragma once
 #include <algorithm>
+#include <type_traits>
 
 #include "eri_common.cuh"
 
@@ -117,12 +118,17 @@ __device__ __forceinline__ double group_max(double v, double *red, int gid) {
 
 // The contracted [e0|f0] block of bra pair ib (primitive pairs [i0, i1)) and ket pair ik
 // ([j0, j1)) into work[0 .. NBLK).  All G threads of the group call it; it ends with a barrier.
-template <class C>
+// F32 (MIXED quartets below the FP32 cutoff): the 2-D tables are stored in FP32 and a batch's
+// products are summed in FP32, then added to the FP64 accumulators (roots, weights and the
+// recurrences stay FP64).
+template <class C, bool F32 = false>
 __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, const RysClassTabs &T,
                                              const int4 ib, const int4 ik, int i0, int i1, int j0,
                                              int j1, double *__restrict__ work, int lane, int gid) {
     constexpr int S = C::S, F1 = C::F + 1, NR = C::NR, E = C::E, F = C::F;
     constexpr int NSLOT = C::NSLOT;
+    using TT = typename std::conditional<F32, float, double>::type;
+    TT *__restrict__ tabs = reinterpret_cast<TT *>(work);
     double acc[C::ACC];
     uint32_t off[C::ACC];
     // slot layout (NSLOT > 1): thread = slot * NBLK + entry, ACC == 1
@@ -157,7 +163,7 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
             for (int ax = 0; ax < 3; ++ax) {
                 const double c00 = fma(-ez * PQv[ax], u, PAv[ax]);
                 const double d00 = fma(zz * PQv[ax], u, QCv[ax]);
-                double *tab = work + ((tb * NR + tr) * 3 + ax) * S;
+                TT *tab = tabs + ((tb * NR + tr) * 3 + ax) * S;
                 // column c = 0 by the a-recurrence, then column c+1 from columns c and c-1
                 double cur[E + 1], prev[E + 1];
                 cur[0] = ax == 0 ? bra.kab * ket.kab * rz * w : 1.0;
@@ -166,7 +172,7 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
                 for (int a = 1; a < E; ++a) cur[a + 1] = fma(c00, cur[a], (double)a * b10 * cur[a - 1]);
 #pragma unroll
                 for (int a = 0; a <= E; ++a) {
-                    tab[a * F1] = cur[a];
+                    tab[a * F1] = (TT)cur[a];
                     prev[a] = 0.0;
                 }
 #pragma unroll
@@ -183,24 +189,29 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
                     for (int a = 0; a <= E; ++a) {
                         prev[a] = cur[a];
                         cur[a] = nxt[a];
-                        tab[a * F1 + c + 1] = nxt[a];
+                        tab[a * F1 + c + 1] = (TT)nxt[a];
                     }
                 }
             }
         }
         group_sync<C::G>(gid);
         if (slot < NSLOT) {
+            TT bacc[C::ACC];
+#pragma unroll
+            for (int k = 0; k < C::ACC; ++k) bacc[k] = (TT)0;
             for (int b = slot; b < nb; b += NSLOT) {
 #pragma unroll 1
                 for (int r = 0; r < NR; ++r) {
-                    const double *__restrict__ tx = work + (b * NR + r) * 3 * S;
+                    const TT *__restrict__ tx = tabs + (b * NR + r) * 3 * S;
 #pragma unroll
                     for (int k = 0; k < C::ACC; ++k) {
                         const uint32_t o = off[k];
-                        acc[k] = fma(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], acc[k]);
+                        bacc[k] = fma(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], bacc[k]);
                     }
                 }
             }
+#pragma unroll
+            for (int k = 0; k < C::ACC; ++k) acc[k] += (double)bacc[k];
         }
         group_sync<C::G>(gid);
     }
@@ -268,7 +279,7 @@ __device__ __forceinline__ void rys_hrr(const RysClassTabs &T, const double *__r
 
 // Persistent work-queue kernel body: each group takes chunks (one bra pair, a run of ket pairs
 // of one molecule) from the class pair's counter and computes their quartets one by one.
-template <class C>
+template <class C, int MIXED = 0>
 __device__ __forceinline__ void rys_queue_body(const EriQueue &Q, const RysTab &R, const RysClassTabs &T) {
     extern __shared__ __align__(16) double rys_smem[];
     __shared__ int s_chunk[128 / C::G];
@@ -291,7 +302,10 @@ __device__ __forceinline__ void rys_queue_body(const EriQueue &Q, const RysTab &
             const int4 ik = __ldg(&Q.pairs.info[q]);
             const double2 bq = __ldg(&Q.pairs.bnd[q]);
             const int nbp = (bp.x * bq.x < Q.screen_cut) ? 0 : ib.y;  // screened: written as 0
-            rys_contract<C>(Q.pairs, R, T, ib, ik, 0, nbp, 0, ik.y, work, lane, gid);
+            if (MIXED && bp.y * bq.y < Q.fp32_cut)
+                rys_contract<C, true>(Q.pairs, R, T, ib, ik, 0, nbp, 0, ik.y, work, lane, gid);
+            else
+                rys_contract<C, false>(Q.pairs, R, T, ib, ik, 0, nbp, 0, ik.y, work, lane, gid);
             const double4 gk = ldg4(&Q.pairs.geo[q]);
             for (int m = lane; m < 2 * kRysNmono; m += C::G)
                 mono[m] = m < kRysNmono ? rys_monomial(m, gb.x, gb.y, gb.z)

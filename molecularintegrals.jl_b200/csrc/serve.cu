@@ -25,6 +25,11 @@
 
 #include "../../include/molints.h"
 
+namespace molints {
+int ctx_device_of(const molints_ctx *ctx);                          // molints.cu
+void ctx_copy_methods(molints_ctx *dst, const molints_ctx *src);    // molints.cu
+}  // namespace molints
+
 namespace {
 
 double now_s() {
@@ -228,11 +233,6 @@ Server *server_start(molints_ctx *ctx, int device, int nslots, int64_t budget, s
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
-namespace molints {
-int ctx_device_of(const molints_ctx *ctx);                          // molints.cu
-void ctx_copy_methods(molints_ctx *dst, const molints_ctx *src);    // molints.cu
-}
-
 namespace {
 std::mutex g_srv_mu;
 std::vector<std::pair<molints_ctx *, Server *>> g_servers;

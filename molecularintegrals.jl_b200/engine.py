@@ -72,10 +72,13 @@ class Stats(ctypes.Structure):
                 ("n_prim_quartets", ctypes.c_int64), ("n_fp32_quartets", ctypes.c_int64),
                 ("n_screened", ctypes.c_int64), ("n_kernel_launches", ctypes.c_int32),
                 ("reserved", ctypes.c_int32), ("device_ms", ctypes.c_double),
-                ("n_prim_pairs", ctypes.c_int64), ("n_prim_pairs_kept", ctypes.c_int64)]
+                ("n_prim_pairs", ctypes.c_int64), ("n_prim_pairs_kept", ctypes.c_int64),
+                ("plan_ms", ctypes.c_double * 4)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "plan_ms")}
+        d["plan_ms"] = list(self.plan_ms)
+        return d
 
 
 _lib = None
