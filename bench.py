@@ -267,13 +267,17 @@ def run_ours(args):
             eng, [mi.config3_molecule(m) for m in range(1, 16, 2)] + [mi.config4_request(r) for r in range(4)])
         t_tune = time.perf_counter() - t_tune
         eng.set_class_methods(class_table)
+        # FP32 cutoff for l <= 3 molecules under the tuned methods (FP32 Rys tables and FP32
+        # HGP VRR), on a serving-shaped molecule with f shells
+        fp32_cut_l3, tune_l3 = AT.tune_fp32_cutoff(eng, mi.config4_request(6))
         eng.set_stream(stream.cuda_stream)
         tuned = {"seconds": t_tune, "rys_classes": sorted(
-            t for t, (h, r) in class_timings.items() if class_table[AT._class_index(t)] == E.METHOD_RYS)}
+            t for t, (h, r) in class_timings.items() if class_table[AT._class_index(t)] == E.METHOD_RYS),
+            "fp32_cutoff_l3": fp32_cut_l3, "fp32_cutoff_l3_tuning": tune_l3}
         if "batch" in parts:
-            batch = measure_batch(eng, stream, dev, fp32_cut, rank, world)
+            batch = measure_batch(eng, stream, dev, fp32_cut_l3, rank, world)
         if "serve" in parts:
-            serving = measure_serving(local, fp32_cut, args.serve_window, rank, class_table=class_table)
+            serving = measure_serving(local, fp32_cut_l3, args.serve_window, rank, class_table=class_table)
 
     cpu = None
     if rank == 0 and world == 1 and "cpu" in parts:
@@ -369,6 +373,13 @@ def measure_batch(eng, stream, dev, fp32_cut, rank, world, cap=1.5e9):
         res[name] = {"value": tot_eri / t_max, "unit": UNIT, "exec_s_max_over_ranks": t_max,
                      "plan_s": t_plan}
     res["fp32_cutoff"] = fp32_cut
+    # accuracy of MIXED against FP64 on a sample of the batch's molecules
+    errs = []
+    for i in mine[len(mine) // 2:len(mine) // 2 + 2] + mine[-2:]:
+        a = eng.eri_packed(mols[i])
+        b = eng.eri_packed(mols[i], precision=E.MIXED, fp32_cutoff=fp32_cut)
+        errs.append(float(np.max(np.abs(a - b))))
+    res["max_abs_err_mixed_vs_fp64_sample"] = max(errs)
     return res
 
 

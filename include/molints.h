@@ -180,6 +180,11 @@ int molints_plan_create_shard(molints_ctx *ctx, const molints_basis *basis,
  * status. */
 int64_t molints_plan_npacked(const molints_plan *plan);
 int molints_plan_execute(molints_plan *plan, double *out_device);
+/* enable != 0: the next execute captures the plan's whole device path (pair build, counter
+ * reset, every class-pair kernel on the forked side streams) into a CUDA graph on the
+ * context's stream, and later executes into the same out_device launch that graph (a new
+ * out_device recaptures).  Not combined with profiling.  No reference counterpart. */
+int molints_plan_set_graph(molints_plan *plan, int enable);
 int molints_plan_stats(const molints_plan *plan, molints_stats *stats);
 int molints_plan_destroy(molints_plan *plan);
 

@@ -14,23 +14,24 @@ LADDER = tuple(10.0 ** k for k in range(-6, 5))
 
 
 def tune_fp32_cutoff(engine, shells, target: float = 1e-9, safety: float = 0.25,
-                     ladder=LADDER, boys=None):
+                     ladder=LADDER, boys=None, method=None):
     import torch
     from . import engine as E
     boys = E.BOYS_REFERENCE if boys is None else boys
+    method = E.METHOD_AUTO if method is None else method
     dev = torch.device("cuda", engine.device)
     ref = torch.empty(shells.npacked, dtype=torch.float64, device=dev)
     out = torch.empty_like(ref)
     stream = torch.cuda.current_stream(dev)
     engine.set_stream(stream.cuda_stream)
     try:
-        p64 = engine.plan(shells, precision=E.FP64, boys=boys)
+        p64 = engine.plan(shells, precision=E.FP64, boys=boys, method=method)
         p64.execute(ref.data_ptr())
         p64.close()
         table = []
         best = 0.0
         for c in sorted(ladder):
-            pm = engine.plan(shells, precision=E.MIXED, boys=boys, fp32_cutoff=c)
+            pm = engine.plan(shells, precision=E.MIXED, boys=boys, fp32_cutoff=c, method=method)
             pm.execute(out.data_ptr())
             st = pm.stats()
             pm.close()

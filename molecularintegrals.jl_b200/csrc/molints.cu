@@ -12,12 +12,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/molints.h"
@@ -91,6 +93,10 @@ struct molints_plan {
     int64_t bytes = 0;
     int n_launches = 0;
     double plan_ms[4] = {0, 0, 0, 0};  // plan creation phases (molints_stats.plan_ms)
+    // CUDA graph of one execute (molints_plan_set_graph), valid for graph_out
+    int use_graph = 0;
+    cudaGraphExec_t gexec = nullptr;
+    double *graph_out = nullptr;
     // per-launch profiling (molints_plan_set_profiling)
     int profiling = 0;
     std::vector<cudaEvent_t> prof_ev;
@@ -449,6 +455,7 @@ int molints_boys_eval(molints_ctx *ctx, int32_t mode, int32_t mmax, const double
 
 static void plan_free(molints_plan *p) {
     if (!p) return;
+    if (p->gexec) cudaGraphExecDestroy(p->gexec);
     for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon};
@@ -850,9 +857,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<int64_t> npp_prefix(npair + 1, 0);  // kept primitive pairs of pairs [0, k)
     for (int k = 0; k < npair; ++k) npp_prefix[k + 1] = npp_prefix[k] + p->npp_h[k];
     std::vector<int4> chunks;
-    struct CostedChunk { double cost; int4 c; };
-    std::vector<CostedChunk> tmp;
-    chunks.reserve(1 << 16);
     // chunk width: 32 ket pairs (one per lane), widened in steps of 32 for large batches so
     // that the queues stay near kMaxChunks entries
     constexpr double kMaxChunks = 4.0e6;
@@ -870,64 +874,92 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     // A Rys group computes a chunk's quartets one after another, so its chunks are short
     // (kRysChunk ket pairs) to spread small classes over many groups.
     constexpr int kRysChunk = 4;
+    // Class pairs are independent: their queues are built on host threads, then concatenated.
+    struct ClassQueue { std::vector<int4> q; double total = 0.0; };
+    std::vector<std::pair<int, int>> cps;
     for (int x = 0; x < kNumPairClasses; ++x)
-        for (int y = 0; y <= x; ++y) {
-            tmp.clear();
-            const int width = (p->method[x][y] == MOLINTS_METHOD_RYS ? kRysChunk : 32) * widen;
-            const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
-            const double w = 1.0 + lsum * lsum;
-            double total = 0.0;
-            for (int m = 0; m < nmol; ++m) {
-                int b0, b1, k0, k1;
-                range_of(x, m, b0, b1);
-                range_of(y, m, k0, k1);
-                for (int pb = b0; pb < b1; ++pb) {
-                    int kbeg = k0, kend = (x == y) ? pb + 1 : k1;
-                    if (sharded) {
-                        // quartet owner: the higher of the two pairs' max shells
-                        const int mp = pr[pb].ms;
-                        auto first_ms_at_least = [&](int v) {
-                            return (int)(std::partition_point(pr.begin() + k0, pr.begin() + k1,
-                                                              [v](const PairRec &r) { return r.ms < v; }) -
-                                         pr.begin());
-                        };
-                        if (mp >= shard_s1) continue;
-                        if (x == y) {
-                            if (mp < shard_s0) continue;  // q <= pb in list order: owner is mp
-                        } else if (mp >= shard_s0) {
-                            kend = first_ms_at_least(shard_s1);
-                        } else {
-                            kbeg = first_ms_at_least(shard_s0);
-                            kend = first_ms_at_least(shard_s1);
-                        }
-                    }
-                    for (int q0 = kbeg; q0 < kend; q0 += width) {
-                        const int n = std::min(width, kend - q0);
-                        const double kq = (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
-                        const double cost = w * p->npp_h[pb] * kq;
-                        total += cost;
-                        tmp.push_back({cost, make_int4(pb, q0, n, m)});
+        for (int y = 0; y <= x; ++y) cps.push_back({x, y});
+    std::vector<ClassQueue> cq(cps.size());
+    auto build_queue = [&](size_t ci) {
+        const int x = cps[ci].first, y = cps[ci].second;
+        const int width = (p->method[x][y] == MOLINTS_METHOD_RYS ? kRysChunk : 32) * widen;
+        const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
+        const double w = 1.0 + lsum * lsum;
+        // heaviest first, bucketed by the binary exponent of the cost: an O(n) order that is
+        // all the load balance needs (a full sort of millions of chunks dominated batches)
+        constexpr int kBuckets = 64;
+        auto bucket = [](double c) {
+            uint64_t bits;
+            std::memcpy(&bits, &c, sizeof bits);
+            const int e2 = c > 0.0 ? (int)((bits >> 52) & 0x7ff) - 1022 : 1;
+            return std::max(0, std::min(kBuckets - 1, kBuckets - 1 - (e2 + 8)));
+        };
+        std::vector<int4> raw;
+        std::vector<unsigned char> bk;
+        int cnt[kBuckets + 1] = {0};
+        double total = 0.0;
+        for (int m = 0; m < nmol; ++m) {
+            int b0, b1, k0, k1;
+            range_of(x, m, b0, b1);
+            range_of(y, m, k0, k1);
+            for (int pb = b0; pb < b1; ++pb) {
+                int kbeg = k0, kend = (x == y) ? pb + 1 : k1;
+                if (sharded) {
+                    // quartet owner: the higher of the two pairs' max shells
+                    const int mp = pr[pb].ms;
+                    auto first_ms_at_least = [&](int v) {
+                        return (int)(std::partition_point(pr.begin() + k0, pr.begin() + k1,
+                                                          [v](const PairRec &r) { return r.ms < v; }) -
+                                     pr.begin());
+                    };
+                    if (mp >= shard_s1) continue;
+                    if (x == y) {
+                        if (mp < shard_s0) continue;  // q <= pb in list order: owner is mp
+                    } else if (mp >= shard_s0) {
+                        kend = first_ms_at_least(shard_s1);
+                    } else {
+                        kbeg = first_ms_at_least(shard_s0);
+                        kend = first_ms_at_least(shard_s1);
                     }
                 }
+                const double wp = w * p->npp_h[pb];
+                for (int q0 = kbeg; q0 < kend; q0 += width) {
+                    const int n = std::min(width, kend - q0);
+                    const double cost = wp * (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
+                    total += cost;
+                    const int b = bucket(cost);
+                    raw.push_back(make_int4(pb, q0, n, m));
+                    bk.push_back((unsigned char)b);
+                    ++cnt[b + 1];
+                }
             }
-            // heaviest first, bucketed by log2(cost): an O(n) order that is all the load
-            // balance needs (a full sort of millions of chunks dominated large batches)
-            constexpr int kBuckets = 64;
-            int cnt[kBuckets + 1] = {0};
-            auto bucket = [](double c) {
-                int e2 = 0;
-                std::frexp(c > 0 ? c : 1.0, &e2);
-                return std::max(0, std::min(kBuckets - 1, kBuckets - 1 - (e2 + 8)));
-            };
-            for (const CostedChunk &cc : tmp) ++cnt[bucket(cc.cost) + 1];
-            for (int k = 1; k <= kBuckets; ++k) cnt[k] += cnt[k - 1];
-            p->q_off[x][y] = (int)chunks.size();
-            p->q_len[x][y] = (int)tmp.size();
-            p->class_cost[x][y] = total;
-            chunks.resize(chunks.size() + tmp.size());
-            int4 *dst = chunks.data() + p->q_off[x][y];
-            for (const CostedChunk &cc : tmp) dst[cnt[bucket(cc.cost)]++] = cc.c;
         }
+        for (int k = 1; k <= kBuckets; ++k) cnt[k] += cnt[k - 1];
+        cq[ci].q.resize(raw.size());
+        for (size_t i = 0; i < raw.size(); ++i) cq[ci].q[cnt[bk[i]]++] = raw[i];
+        cq[ci].total = total;
+    };
+    {
+        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::atomic<size_t> next{0};
+        auto worker = [&] {
+            for (size_t ci; (ci = next.fetch_add(1)) < cps.size();) build_queue(ci);
+        };
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < std::min<unsigned>(hw, (unsigned)cps.size()); ++t) pool.emplace_back(worker);
+        worker();
+        for (std::thread &t : pool) t.join();
+    }
+    size_t nq = 0;
+    for (const ClassQueue &c : cq) nq += c.q.size();
+    chunks.reserve(nq);
+    for (size_t ci = 0; ci < cps.size(); ++ci) {
+        const int x = cps[ci].first, y = cps[ci].second;
+        p->q_off[x][y] = (int)chunks.size();
+        p->q_len[x][y] = (int)cq[ci].q.size();
+        p->class_cost[x][y] = cq[ci].total;
+        chunks.insert(chunks.end(), cq[ci].q.begin(), cq[ci].q.end());
+    }
     std::vector<long long> mol_out_ll(std::max(nmol, 1), 0);
     for (int m = 0; m < nmol; ++m) mol_out_ll[m] = (long long)p->mol_out_h[m];
     p->plan_ms[2] = ms_since(t_phase);
@@ -961,11 +993,10 @@ int molints_plan_create(molints_ctx *ctx, const molints_basis *b, const molints_
 
 int64_t molints_plan_npacked(const molints_plan *p) { return p ? p->npacked : MOLINTS_ERR_INVALID; }
 
-int molints_plan_execute(molints_plan *p, double *out_device) {
-    if (!p || (!out_device && p->npacked > 0))
-        return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_execute: null argument");
+// Queue the device path of one execute on the context's stream (side streams forked from it
+// and joined back).  timing: record the context's ev0/ev1 around it (not inside a graph).
+static int plan_enqueue(molints_plan *p, double *out_device, bool timing) {
     molints_ctx *ctx = p->ctx;
-    MI_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     int launches = 0;
     // event pair around each launch when profiling (launch k uses events 2k, 2k+1)
@@ -982,7 +1013,7 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         cudaError_t err = cudaEventRecord(p->prof_ev[2 * k + end], st);
         return err == cudaSuccess ? 0 : cuda_fail(ctx, err, "cudaEventRecord");
     };
-    MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
+    if (timing) MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
     MI_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(int) * kNumPairClasses * kNumPairClasses, s));
     if (p->npair > 0) {
         if (int rc = mark(launches, "build_pairs", 0, s)) return rc;
@@ -1038,8 +1069,70 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
         MI_CUDA(ctx, cudaStreamWaitEvent(s, ctx->join[i], 0));
     }
     MI_CUDA(ctx, cudaGetLastError());
-    MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
+    if (timing) MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
     p->n_launches = launches;
+    return MOLINTS_OK;
+}
+
+// Resident blocks per SM of every queue kernel the plan launches (queried once per context,
+// before any graph capture).
+static void plan_occupancy(molints_plan *p) {
+    molints_ctx *ctx = p->ctx;
+    const int mixed = p->opts.precision == MOLINTS_MIXED ? 1 : 0;
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            if (p->q_len[x][y] == 0) continue;
+            const bool rys = p->method[x][y] == MOLINTS_METHOD_RYS;
+            int &occ = ctx->occupancy[x][y][(rys ? 2 : 0) + mixed];
+            if (occ == 0) occ = std::max(1, rys ? kRysOccupancy[x][y](mixed) : kEriOccupancy[x][y](mixed));
+        }
+}
+
+int molints_plan_execute(molints_plan *p, double *out_device) {
+    if (!p || (!out_device && p->npacked > 0))
+        return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_execute: null argument");
+    molints_ctx *ctx = p->ctx;
+    MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (!p->use_graph || p->profiling) return plan_enqueue(p, out_device, true);
+    // CUDA graph: captured once per output pointer, then launched as a whole
+    cudaStream_t s = ctx->stream;
+    if (!p->gexec || p->graph_out != out_device) {
+        if (p->gexec) {
+            cudaGraphExecDestroy(p->gexec);
+            p->gexec = nullptr;
+        }
+        plan_occupancy(p);
+        MI_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int rc = plan_enqueue(p, out_device, false);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&p->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            p->gexec = nullptr;
+            return cuda_fail(ctx, e, "cudaGraphInstantiate");
+        }
+        p->graph_out = out_device;
+    }
+    MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
+    MI_CUDA(ctx, cudaGraphLaunch(p->gexec, s));
+    MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
+    return MOLINTS_OK;
+}
+
+int molints_plan_set_graph(molints_plan *p, int enable) {
+    if (!p) return MOLINTS_ERR_INVALID;
+    p->use_graph = enable ? 1 : 0;
+    if (!enable && p->gexec) {
+        cudaSetDevice(p->ctx->device);
+        cudaGraphExecDestroy(p->gexec);
+        p->gexec = nullptr;
+    }
     return MOLINTS_OK;
 }
 

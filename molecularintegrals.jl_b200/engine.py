@@ -42,6 +42,7 @@ EXPORTED_SYMBOLS = [
     "molints_serve_start", "molints_serve_stop", "molints_submit", "molints_poll",
     "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
     "molints_release", "molints_serve_stats", "molints_shard_range", "molints_plan_create_shard",
+    "molints_plan_set_graph",
 ]
 
 
@@ -128,6 +129,7 @@ def load_library(path: Path | str | None = None):
         "molints_serve_stats": (ctypes.c_int, [P, P, P, P, P]),
         "molints_shard_range": (ctypes.c_int, [P, I32, I32, P, P]),
         "molints_plan_create_shard": (ctypes.c_int, [P, P, P, I32, I32, P]),
+        "molints_plan_set_graph": (ctypes.c_int, [P, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -203,6 +205,10 @@ class Plan:
         st = Stats()
         self.engine._check(self.engine.lib.molints_plan_stats(self.h, ctypes.byref(st)))
         return st.as_dict()
+
+    def set_graph(self, enable: bool = True) -> None:
+        """Launch executes as one captured CUDA graph (recaptured for a new output pointer)."""
+        self.engine._check(self.engine.lib.molints_plan_set_graph(self.h, int(enable)))
 
     def set_profiling(self, enable: bool = True) -> None:
         self.engine._check(self.engine.lib.molints_plan_set_profiling(self.h, int(enable)))

@@ -365,3 +365,59 @@ def test_f_shell_schwarz_bounds(eng, oracle):
                     ab = a * (a + 1) // 2 + b if a >= b else b * (b + 1) // 2 + a
                     m = max(m, abs(diag[ab]))
             assert q[i * (i + 1) // 2 + j] == pytest.approx(np.sqrt(m), rel=1e-12)
+
+
+def test_rys_mixed_error_bound(eng):
+    """MIXED with the Rys kernels (FP32 2-D tables and batch sums, FP64 accumulation): the
+    tuned cutoff keeps max |MIXED - FP64| below 1e-9 Eh on config 2 and an f molecule."""
+    from molints_b200 import autotune, engine
+    for sh in (mi.config2(), _f_molecule(12)):
+        cut, table = autotune.tune_fp32_cutoff(eng, sh, method=engine.METHOD_RYS)
+        assert cut > 0, table
+        ref = eng.eri_packed(sh, method=engine.METHOD_RYS)
+        got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cut, method=engine.METHOD_RYS,
+                                 with_stats=True)
+        assert st["n_fp32_quartets"] > 0
+        assert np.max(np.abs(got - ref)) < TOL_MIXED
+
+
+def test_class_method_tuner(eng):
+    """tune_class_methods times both kernels of every HGP-capable class pair present and
+    returns a valid table; plans under it stay within 1e-12 of the HGP result (exact Boys)."""
+    from molints_b200 import autotune, engine
+    mols = [mi.config2(), _f_molecule(14)]
+    table, timings = autotune.tune_class_methods(eng, mols, repeats=2)
+    assert timings and set(table.values()) <= {engine.METHOD_HGP, engine.METHOD_RYS}
+    assert all(h > 0 and r > 0 for h, r in timings.values())
+    eng.set_class_methods(table)
+    try:
+        for sh in mols:
+            got = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
+            ref = eng.eri_packed(sh, boys=engine.BOYS_EXACT, method=engine.METHOD_HGP)
+            assert np.max(np.abs(got - ref)) < TOL_FP64
+    finally:
+        eng.set_class_methods(None)
+
+
+def test_plan_cuda_graph(eng):
+    """An execute captured as a CUDA graph (side streams included) gives the eager result
+    bit for bit, on repeat launches and after a recapture for a new output vector."""
+    import torch
+    from molints_b200 import engine
+    sh = _f_molecule(15)
+    eng.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        plan = eng.plan(sh, precision=engine.MIXED, fp32_cutoff=1e-4)
+        ref = torch.empty(sh.npacked, dtype=torch.float64, device="cuda")
+        plan.execute(ref.data_ptr())
+        plan.set_graph(True)
+        outs = [torch.full_like(ref, float("nan")) for _ in range(2)]
+        for out in (outs[0], outs[0], outs[1]):
+            out.fill_(float("nan"))
+            plan.execute(out.data_ptr())
+            torch.cuda.synchronize()
+            assert torch.equal(out, ref)
+        assert plan.stats()["device_ms"] > 0
+        plan.close()
+    finally:
+        eng.set_stream(None)
