@@ -180,6 +180,16 @@ int molints_plan_create_shard(molints_ctx *ctx, const molints_basis *basis,
  * status. */
 int64_t molints_plan_npacked(const molints_plan *plan);
 int molints_plan_execute(molints_plan *plan, double *out_device);
+/* Coulomb and exchange matrices instead of the packed vector: one execute of a one-molecule
+ * plan (or of a shard plan: that shard's share) digests every unique integral into
+ * J_pq = sum_rs D_rs (pq|rs) and K_pr = sum_qs D_qs (pq|rs), n x n row-major device arrays
+ * (zeroed by the call) for a symmetric device density D, on the context's stream.  No packed
+ * vector is written.  The reference consumer is make2JmK (src/ERI.jl:114-128), which forms
+ * 2J - K from the packed vector. */
+int molints_plan_jk(molints_plan *plan, const double *D_device, double *J_device, double *K_device);
+/* The same from host arrays in one synchronous call (plan, device buffers, copies). */
+int molints_jk(molints_ctx *ctx, const molints_basis *basis, const molints_options *opts,
+               const double *D_host, double *J_host, double *K_host);
 /* enable != 0: the next execute captures the plan's whole device path (pair build, counter
  * reset, every class-pair kernel on the forked side streams) into a CUDA graph on the
  * context's stream, and later executes into the same out_device launch that graph (a new

@@ -63,12 +63,21 @@ struct RysTab {
 };
 int rys_tables(RysTab *t);  // device addresses on the current device; 0 on success
 
+// Coulomb and exchange digestion (molints_plan_jk): J_pq = sum_rs D_rs (pq|rs) and
+// K_pr = sum_qs D_qs (pq|rs), full n x n row-major, accumulated with FP64 atomics.
+struct JKOut {
+    const double *D;   // symmetric density, n x n
+    double *J, *K;     // zeroed before the execute
+    int n;
+};
+
 // The chunk queue of one class pair: chunk c = {bra pair, first ket pair, ket count,
 // molecule}; lane l of the warp that takes it computes (bra | first + l + 32 i).  Chunks never
 // cross a bra pair, a molecule or, when bra and ket class coincide, the triangle q <= p.
 struct EriQueue {
     PairTab pairs;
     BoysTab boys;
+    JKOut jk;                     // jk.J != nullptr: digest into J and K instead of storing
     double *out;                  // packed outputs of all molecules (device)
     const long long *mol_out;     // offset of each molecule's packed vector in out
     const int4 *chunks;
@@ -147,6 +156,36 @@ __device__ __forceinline__ double4 ldg4(const double4 *p) {
 }
 
 __device__ __forceinline__ long long tri_ll(long long i) { return i * (i + 1) / 2; }
+
+// One unique integral v = (ij|kl) into J and K: every distinct index permutation (pq|rs) of
+// the 8-fold symmetry adds D_rs v to J_pq and D_qs v to K_pr (the Fock-build contraction that
+// make2JmK, src/ERI.jl:114-128, performs on the packed vector).
+__device__ __forceinline__ void jk_add(const JKOut &jk, int i, int j, int k, int l, double v) {
+    if (v == 0.0) return;
+    if (i < j) { const int t = i; i = j; j = t; }
+    if (k < l) { const int t = k; k = l; l = t; }
+    const long long n = jk.n;
+    const bool dij = i != j, dkl = k != l;
+    const bool dbk = (tri_ll(i) + j) != (tri_ll(k) + l);
+    const double *__restrict__ D = jk.D;
+    // J: J_ij (and J_ji) += (1 + [k != l]) D_kl v; J_kl (and J_lk) += (1 + [i != j]) D_ij v
+    const double jkl = (dkl ? 2.0 : 1.0) * __ldg(&D[k * n + l]) * v;
+    atomicAdd(&jk.J[i * n + j], jkl);
+    if (dij) atomicAdd(&jk.J[j * n + i], jkl);
+    if (dbk) {
+        const double jij = (dij ? 2.0 : 1.0) * __ldg(&D[i * n + j]) * v;
+        atomicAdd(&jk.J[k * n + l], jij);
+        if (dkl) atomicAdd(&jk.J[l * n + k], jij);
+    }
+    // K: (pq|rs) -> K_pr += D_qs v over the distinct permutations
+    const int pq[2][2] = {{i, j}, {j, i}}, rs[2][2] = {{k, l}, {l, k}};
+    for (int a = 0; a < (dij ? 2 : 1); ++a)
+        for (int b = 0; b < (dkl ? 2 : 1); ++b) {
+            const int p0 = pq[a][0], q0 = pq[a][1], r0 = rs[b][0], s0 = rs[b][1];
+            atomicAdd(&jk.K[p0 * n + r0], __ldg(&D[q0 * n + s0]) * v);
+            if (dbk) atomicAdd(&jk.K[r0 * n + p0], __ldg(&D[s0 * n + q0]) * v);
+        }
+}
 
 // 0-based packed index of the function-pair indices ij, kl (iindex, src/Utils.jl:19).
 __device__ __forceinline__ long long packed_index(long long ij, long long kl) {

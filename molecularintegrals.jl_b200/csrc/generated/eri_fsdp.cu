@@ -1453,6 +1453,19 @@ __device__ __forceinline__ void store_fsdp(double *__restrict__ out, const int4 
       if (true && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[179]; }
 }
 
+// The quartet's unique integrals digested into J and K (molints_plan_jk) instead of stored.
+__device__ __noinline__ void jk_fsdp(const JKOut &jk, const int4 ib_, const int4 ik_, bool same,
+                                      const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    for (int x = 0; x < 180; ++x) {
+        const int ia = x / 18, ibb = (x / 18) % 1, ic = (x / 3) % 6, id = x % 3;
+        if ((dab && ia < ibb) || (dcd && ic < id)) continue;
+        const int i = ib_.z + ia, j = ib_.w + ibb, k = ik_.z + ic, l = ik_.w + id;
+        if (same && pair_index(i, j) < pair_index(k, l)) continue;
+        jk_add(jk, i, j, k, l, res[x]);
+    }
+}
+
 // Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
 // ket pairs of one molecule) from a shared counter until the chunk list, ordered by
 // decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
@@ -1477,8 +1490,9 @@ __global__ void __launch_bounds__(128) eri_queue_fsdp(const EriQueue Q) {
             if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_fsdp<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
             else quartet_fsdp<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
         }
-        store_fsdp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                    p == q, res);
+        if (Q.jk.J) jk_fsdp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+        else store_fsdp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                         p == q, res);
         }
     }
 }

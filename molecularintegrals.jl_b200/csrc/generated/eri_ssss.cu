@@ -67,6 +67,19 @@ __device__ __forceinline__ void store_ssss(double *__restrict__ out, const int4 
       if ((!dab || 0 >= 0) && (!dcd || 0 >= 0) && (!same || ij >= kl)) out[packed_index(ij, kl)] = res[0]; }
 }
 
+// The quartet's unique integrals digested into J and K (molints_plan_jk) instead of stored.
+__device__ __noinline__ void jk_ssss(const JKOut &jk, const int4 ib_, const int4 ik_, bool same,
+                                      const double *__restrict__ res) {
+    const bool dab = ib_.z == ib_.w, dcd = ik_.z == ik_.w;
+    for (int x = 0; x < 1; ++x) {
+        const int ia = x / 1, ibb = (x / 1) % 1, ic = (x / 1) % 1, id = x % 1;
+        if ((dab && ia < ibb) || (dcd && ic < id)) continue;
+        const int i = ib_.z + ia, j = ib_.w + ibb, k = ik_.z + ic, l = ik_.w + id;
+        if (same && pair_index(i, j) < pair_index(k, l)) continue;
+        jk_add(jk, i, j, k, l, res[x]);
+    }
+}
+
 // Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
 // ket pairs of one molecule) from a shared counter until the chunk list, ordered by
 // decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
@@ -91,8 +104,9 @@ __global__ void __launch_bounds__(128) eri_queue_ssss(const EriQueue Q) {
             if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_ssss<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
             else quartet_ssss<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
         }
-        store_ssss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                    p == q, res);
+        if (Q.jk.J) jk_ssss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+        else store_ssss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                         p == q, res);
         }
     }
 }

@@ -61,6 +61,7 @@ struct molints_plan {
     molints_options opts{};
     int nmol = 0;
     int nshell = 0;
+    int64_t nbf0 = 0;                  // functions of molecule 0 (J/K dimension)
     int64_t npacked = 0;               // all molecules
     std::vector<int64_t> mol_out_h;    // offset of each molecule's packed vector
     std::vector<int> mol_nshell;
@@ -619,6 +620,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         p->mol_out_h[0] = -shard_lo;  // kernels write out[iindex - lo]
     }
     p->mol_nshell.resize(nmol);
+    p->nbf0 = nmol > 0 ? mol_nbf[0] : 0;
     // method per class pair: Rys where no HGP kernel exists (an f shell), else the request
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
@@ -995,7 +997,7 @@ int64_t molints_plan_npacked(const molints_plan *p) { return p ? p->npacked : MO
 
 // Queue the device path of one execute on the context's stream (side streams forked from it
 // and joined back).  timing: record the context's ev0/ev1 around it (not inside a graph).
-static int plan_enqueue(molints_plan *p, double *out_device, bool timing) {
+static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut jk = JKOut{}) {
     molints_ctx *ctx = p->ctx;
     cudaStream_t s = ctx->stream;
     int launches = 0;
@@ -1047,6 +1049,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing) {
         EriQueue Q{};
         Q.pairs = P;
         Q.boys = B;
+        Q.jk = jk;
         Q.out = out_device;
         Q.mol_out = p->mol_out;
         Q.chunks = p->chunks + p->q_off[x][y];
@@ -1123,6 +1126,52 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
     MI_CUDA(ctx, cudaGraphLaunch(p->gexec, s));
     MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
     return MOLINTS_OK;
+}
+
+int molints_plan_jk(molints_plan *p, const double *D_device, double *J_device, double *K_device) {
+    if (!p || !D_device || !J_device || !K_device)
+        return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_jk: null argument");
+    molints_ctx *ctx = p->ctx;
+    if (p->nmol != 1) return fail(ctx, MOLINTS_ERR_INVALID, "plan_jk: one molecule per plan");
+    MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int64_t n = p->nbf0;
+    const size_t bytes = (size_t)n * n * sizeof(double);
+    MI_CUDA(ctx, cudaMemsetAsync(J_device, 0, bytes, ctx->stream));
+    MI_CUDA(ctx, cudaMemsetAsync(K_device, 0, bytes, ctx->stream));
+    JKOut jk;
+    jk.D = D_device;
+    jk.J = J_device;
+    jk.K = K_device;
+    jk.n = (int)n;
+    return plan_enqueue(p, nullptr, true, jk);
+}
+
+int molints_jk(molints_ctx *ctx, const molints_basis *b, const molints_options *opts,
+               const double *D_host, double *J_host, double *K_host) {
+    if (!ctx || !b || !D_host || !J_host || !K_host) return fail(ctx, MOLINTS_ERR_INVALID, "jk: null argument");
+    const int64_t n = molints_nbf(b);
+    if (n < 0) return fail(ctx, MOLINTS_ERR_INVALID, "jk: malformed basis");
+    molints_plan *p = nullptr;
+    int rc = molints_plan_create(ctx, b, opts, &p);
+    if (rc) return rc;
+    if (n == 0) { molints_plan_destroy(p); return MOLINTS_OK; }
+    double *d = nullptr;
+    int64_t held = 0;
+    rc = dev_alloc(ctx, &d, (size_t)3 * n * n, &held);
+    if (!rc) {
+        const size_t bytes = (size_t)n * n * sizeof(double);
+        cudaError_t e = cudaMemcpyAsync(d, D_host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) rc = molints_plan_jk(p, d, d + n * n, d + 2 * n * n);
+        else rc = cuda_fail(ctx, e, "jk upload");
+        if (!rc && (e = cudaMemcpyAsync(J_host, d + n * n, bytes, cudaMemcpyDeviceToHost, ctx->stream)) == cudaSuccess)
+            e = cudaMemcpyAsync(K_host, d + 2 * n * n, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "jk");
+        dev_free(ctx, d);
+        ctx->held -= held;
+    }
+    molints_plan_destroy(p);
+    return rc;
 }
 
 int molints_plan_set_graph(molints_plan *p, int enable) {

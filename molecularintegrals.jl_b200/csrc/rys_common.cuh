@@ -317,7 +317,8 @@ __device__ __forceinline__ void rys_queue_body(const EriQueue &Q, const RysTab &
                 if ((dab && ia < jb) || (dcd && ic < jd)) return;
                 const long long ij = pair_index(ib.z + ia, ib.w + jb), kl = pair_index(ik.z + ic, ik.w + jd);
                 if (same && ij < kl) return;
-                out[packed_index(ij, kl)] = v;
+                if (Q.jk.J) jk_add(Q.jk, ib.z + ia, ib.w + jb, ik.z + ic, ik.w + jd, v);
+                else out[packed_index(ij, kl)] = v;
             });
             group_sync<C::G>(gid);
         }

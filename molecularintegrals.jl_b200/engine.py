@@ -42,7 +42,7 @@ EXPORTED_SYMBOLS = [
     "molints_serve_start", "molints_serve_stop", "molints_submit", "molints_poll",
     "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
     "molints_release", "molints_serve_stats", "molints_shard_range", "molints_plan_create_shard",
-    "molints_plan_set_graph",
+    "molints_plan_set_graph", "molints_plan_jk", "molints_jk",
 ]
 
 
@@ -130,6 +130,8 @@ def load_library(path: Path | str | None = None):
         "molints_shard_range": (ctypes.c_int, [P, I32, I32, P, P]),
         "molints_plan_create_shard": (ctypes.c_int, [P, P, P, I32, I32, P]),
         "molints_plan_set_graph": (ctypes.c_int, [P, ctypes.c_int]),
+        "molints_plan_jk": (ctypes.c_int, [P, P, P, P]),
+        "molints_jk": (ctypes.c_int, [P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -205,6 +207,11 @@ class Plan:
         st = Stats()
         self.engine._check(self.engine.lib.molints_plan_stats(self.h, ctypes.byref(st)))
         return st.as_dict()
+
+    def jk(self, D_ptr: int, J_ptr: int, K_ptr: int) -> None:
+        """Queue J and K (n x n device arrays) for the symmetric device density at D_ptr."""
+        self.engine._check(self.engine.lib.molints_plan_jk(self.h, ctypes.c_void_p(D_ptr),
+                                                           ctypes.c_void_p(J_ptr), ctypes.c_void_p(K_ptr)))
 
     def set_graph(self, enable: bool = True) -> None:
         """Launch executes as one captured CUDA graph (recaptured for a new output pointer)."""
@@ -394,6 +401,22 @@ class Engine:
             msg = self.lib.molints_request_error(req.h)
             raise MolintsError(rc, msg.decode() if msg else "")
 
+    def jk(self, shells, D, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
+           method=METHOD_AUTO):
+        """(J, K) for the symmetric density D (n x n host array), digested on the device
+        without storing the integrals."""
+        arrs = _BasisArrays(shells)
+        n = shells.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        if D.shape != (n, n):
+            raise ValueError(f"D must be {n} x {n}")
+        J = np.empty((n, n))
+        K = np.empty((n, n))
+        opts = make_options(precision, boys, fp32_cutoff, 0.0, method)
+        self._check(self.lib.molints_jk(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
+                                        _ptr(D), _ptr(J), _ptr(K)))
+        return J, K
+
     def boys(self, mmax: int, T, mode=BOYS_REFERENCE) -> np.ndarray:
         T = np.ascontiguousarray(T, dtype=np.float64)
         out = np.empty((T.size, mmax))
@@ -444,6 +467,13 @@ def all_twoe_ints_chrr(shells) -> np.ndarray:
     """Drop-in for all_twoe_ints_chrr(bfs) (src/HGP.jl:22-34), with its layout and
     normalisation defects fixed: the same vector as all_twoe_ints."""
     return default_engine().eri_packed(shells, method=METHOD_HGP)
+
+
+def make2JmK(D, shells) -> np.ndarray:
+    """2J - K for the density D (make2JmK(D, Ints), src/ERI.jl:114-128), with the integrals
+    digested on the device instead of read from a packed vector."""
+    J, K = default_engine().jk(shells, D)
+    return 2.0 * J - K
 
 
 def all_twoe_ints_rys(shells) -> np.ndarray:

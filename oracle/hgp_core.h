@@ -260,10 +260,16 @@ static int64_t PFX(eri_packed_hgp_impl)(int nshell, const double *xyz, const int
         while (tri64(p1 + 1) <= q) ++p1;
         int64_t p2 = q - tri64(p1);
         int I = pi[p1], J = pj[p1], K = pi[p2], Lsh = pj[p2];
-        if (g_orient == 1) {
+        if (g_orient == 1 || g_orient == 2) {
             int t;
-            if (L[I] < L[J]) { t = I; I = J; J = t; }
-            if (L[K] < L[Lsh]) { t = K; K = Lsh; Lsh = t; }
+            if (g_orient == 2) {
+                /* larger L first; equal L, and an f-d pair, put the tighter shell first */
+                if (oracle_a_first(&b, J, I)) { t = I; I = J; J = t; }
+                if (oracle_a_first(&b, Lsh, K)) { t = K; K = Lsh; Lsh = t; }
+            } else {
+                if (L[I] < L[J]) { t = I; I = J; J = t; }
+                if (L[K] < L[Lsh]) { t = K; K = Lsh; Lsh = t; }
+            }
             int sb = L[I] + L[J], sk = L[K] + L[Lsh];
             if (sk > sb || (sk == sb && L[K] > L[I])) {
                 t = I; I = K; K = t; t = J; J = Lsh; Lsh = t;

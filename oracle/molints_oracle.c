@@ -193,6 +193,24 @@ static int g_orient = 0;
 void oracle_set_orientation(int mode) { g_orient = mode; }
 int oracle_get_orientation(void) { return g_orient; }
 
+/* Orientation 2 (the engine's present rule): shell x goes first in the pair (x, y) if it has
+ * the larger L, or, for equal L and for an f-d pair, the larger sqrt(min * max exponent).
+ * Moving angular momentum away from the tighter shell keeps the HRR from cancelling. */
+static double oracle_tightness(const double *expn, const int *nprim, const int *prim_off, int s) {
+    double lo = expn[prim_off[s]], hi = lo;
+    for (int i = 1; i < nprim[s]; ++i) {
+        const double e = expn[prim_off[s] + i];
+        if (e < lo) lo = e;
+        if (e > hi) hi = e;
+    }
+    return sqrt(lo * hi);
+}
+#define oracle_a_first(bp, x, y)                                                                     \
+    (((bp)->L[x] == (bp)->L[y] || ((bp)->L[x] >= 2 && (bp)->L[y] >= 2 && (bp)->L[x] + (bp)->L[y] == 5)) \
+         ? oracle_tightness((bp)->expn_in, (bp)->nprim, (bp)->prim_off, x) >                            \
+               oracle_tightness((bp)->expn_in, (bp)->nprim, (bp)->prim_off, y)                          \
+         : (bp)->L[x] > (bp)->L[y])
+
 /* ---------------------------------------------------------------- the HGP core, twice */
 
 static inline int64_t tri64(int64_t i) { return i * (i + 1) / 2; }

@@ -140,6 +140,20 @@ class engine_orientation:
         lib().oracle_set_orientation(self._old)
 
 
+class stable_orientation:
+    """Context manager: the HGP driver orients each pair as the engine does now (larger L
+    first; for equal L and for an f-d pair the tighter shell first), the orientation in
+    which the HRR does not cancel.  The long-double oracle in this mode is the near-exact
+    reference for bases with tight and diffuse shells of the same L."""
+
+    def __enter__(self):
+        self._old = lib().oracle_get_orientation()
+        lib().oracle_set_orientation(2)
+
+    def __exit__(self, *exc):
+        lib().oracle_set_orientation(self._old)
+
+
 def boys_mpmath(m: int, T: float, dps: int = 40) -> float:
     """Exact F_m(T) = 1/2 T^-(m+1/2) gamma_lower(m+1/2, T), in mpmath."""
     import mpmath
@@ -431,3 +445,19 @@ def eri_packed_rys(shells, nthreads: int = 1) -> np.ndarray:
     if rc != 0:
         raise ValueError("oracle_eri_packed_rys: unsupported shell")
     return out
+
+
+# ------------------------------------------------------------------ J/K
+def make2JmK(D: np.ndarray, ints: np.ndarray) -> np.ndarray:
+    """make2JmK(D, Ints) of src/ERI.jl:114-128 on a packed vector (0-based iindex):
+    G_ij = sum_kl D_kl (2 (ij|kl) - (ik|jl)).  Returns (G, J, K)."""
+    n = D.shape[0]
+    i, j, k, l = np.meshgrid(*[np.arange(n)] * 4, indexing="ij")
+    def tri(x):
+        return x * (x + 1) // 2
+    ij = np.where(i >= j, tri(i) + j, tri(j) + i)
+    kl = np.where(k >= l, tri(k) + l, tri(l) + k)
+    full = ints[np.where(ij >= kl, tri(ij) + kl, tri(kl) + ij)]
+    J = np.einsum("ijkl,kl->ij", full, D)
+    K = np.einsum("ikjl,kl->ij", full, D)
+    return 2 * J - K, J, K

@@ -214,3 +214,39 @@ def test_rys_equals_hgp_random_classes(oracle, lmax, seed):
     with oracle.exact_boys():
         h = oracle.eri_packed_hgp_ld(sh, nthreads=8)
     assert np.max(np.abs(r - h)) < 1e-13 * max(1.0, np.max(np.abs(h)))
+
+
+def test_make2JmK_restatement_matches_loops(oracle):
+    """The oracle's make2JmK (src/ERI.jl:114-128) against explicit loops on ethane/STO-3G."""
+    sh = mi.config0()
+    ints = oracle.eri_packed_hgp(sh, nthreads=4)
+    n = sh.nbf
+    rng = np.random.default_rng(1)
+    A = rng.normal(size=(n, n))
+    D = A + A.T
+    G, J, K = oracle.make2JmK(D, ints)
+    for i in (0, 3, 9, 15):
+        for j in (0, 7, 15):
+            g = sum(D[k, l] * (2 * ints[oracle.iindex(i, j, k, l)] - ints[oracle.iindex(i, k, j, l)])
+                    for k in range(n) for l in range(n))
+            assert G[i, j] == pytest.approx(g, rel=1e-12, abs=1e-12)
+
+
+def test_hrr_orientation_tight_first(oracle):
+    """D6: a diffuse s shell (0.108) before a tight f (1009), 6.8 bohr apart.  The reference
+    orientation chrr(I,J,...) with I >= J by shell index transfers angular momentum onto the
+    tight f and cancels: its FP64 value is off by ~4e-9 Eh, and even long double by ~5e-12.
+    With the tight shell first (the engine's orientation) FP64 agrees with Huzinaga."""
+    A = np.array([1.3, -2.0, 0.4])
+    B = A + np.array([4.1, 3.9, -3.6])
+    sub = mi.Shells.from_list([(A, 3, [(1008.9973033479797, 1.0)]), (B, 0, [(0.10849250091461012, 1.0)])])
+    huz = oracle.eri_packed_huzinaga(sub, nthreads=2)
+    with oracle.exact_boys():
+        ref_f64 = oracle.eri_packed_hgp(sub, nthreads=2)
+        ref_ld = oracle.eri_packed_hgp_ld(sub, nthreads=2)
+        with oracle.stable_orientation():
+            st_f64 = oracle.eri_packed_hgp(sub, nthreads=2)
+            st_ld = oracle.eri_packed_hgp_ld(sub, nthreads=2)
+    assert np.max(np.abs(ref_f64 - huz)) > 1e-10
+    assert np.max(np.abs(st_f64 - huz)) < 1e-13 * max(1.0, np.max(np.abs(huz)))
+    assert np.max(np.abs(st_ld - huz)) < np.max(np.abs(ref_ld - huz))
