@@ -33,10 +33,12 @@ constexpr double kBoysReferenceSwitch = 30.0;  // farray's Tmax, src/Boys.jl:19
 //   oo2z = 1 / (2 zeta)
 //   P    = (a A + b B) / zeta (gaussian_product_center, src/OneInts.jl:78-83)
 //   PA   = P - A
+//   b    = sqrt(max |(ab|ab)|) of this primitive pair (its Schwarz bound; 0 before the plan's
+//          bound pass); a shell pair's kept primitive pairs are sorted by b, largest first
 // so that kab_bra * kab_ket / sqrt(zeta+eta) is the [00|00] prefactor of HGP eq. 12,
 // 2 pi^(5/2) / (zeta eta sqrt(zeta+eta)) x exp(...) x coefficients.
 struct PrimPair {
-    double zeta, kab, oo2z, px, py, pz, pax, pay, paz, pad;
+    double zeta, kab, oo2z, px, py, pz, pax, pay, paz, b;
 };
 static_assert(sizeof(PrimPair) == 80, "PrimPair is 5 x 16 bytes");
 
@@ -85,6 +87,7 @@ struct EriQueue {
     int *counter;                 // next chunk; zero at launch
     double screen_cut;            // Qabs_p Qabs_q below this: written as 0
     double fp32_cut;              // R_p R_q below this (MIXED kernels): FP32 VRR
+    double prim_cut;              // primitive quartets with b_i b_j below this are skipped
 };
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {
@@ -93,7 +96,7 @@ __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, i
                   e = __ldg(v + 4);
     PrimPair r;
     r.zeta = a.x; r.kab = a.y; r.oo2z = b.x; r.px = b.y; r.py = c.x; r.pz = c.y;
-    r.pax = d.x; r.pay = d.y; r.paz = e.x; r.pad = e.y;
+    r.pax = d.x; r.pay = d.y; r.paz = e.x; r.b = e.y;
     return r;
 }
 

@@ -31,6 +31,8 @@ using namespace molints;
 struct molints_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
+    cudaStream_t cap_stream = nullptr;  // CUDA-graph capture (the legacy stream cannot capture)
+    std::vector<molints_plan *> plans;  // live plans, orphaned when the context goes first
     cudaStream_t stream = nullptr;
     int64_t budget = 0;        // bytes, 0 = unbounded
     int64_t held = 0;          // bytes currently allocated by this context and its plans
@@ -84,6 +86,7 @@ struct molints_plan {
     int2 *pair_ab = nullptr;
     int4 *info = nullptr;
     int *pp_src = nullptr;             // primitive pair k -> (ia << 8) | ib within its shells
+    double *pbk = nullptr;             // primitive pair k -> its Schwarz bound b_k (kept order)
     double4 *geo = nullptr;
     PrimPair *pp = nullptr;
     double2 *bnd = nullptr;
@@ -174,6 +177,7 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
                                    const double *__restrict__ xyz, const int *__restrict__ poff,
                                    const double *__restrict__ expn,
                                    const double *__restrict__ ncoef, double c0,
+                                   const double *__restrict__ pb,
                                    PrimPair *__restrict__ pp, double4 *__restrict__ geo) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npair) return;
@@ -202,7 +206,7 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
         r.px = Ax + r.pax;
         r.py = Ay + r.pay;
         r.pz = Az + r.paz;
-        r.pad = 0.0;
+        r.b = pb ? pb[k] : 0.0;
         pp[k] = r;
     }
     geo[p] = make_double4(ABx, ABy, ABz, 0.0);
@@ -237,7 +241,7 @@ void launch_build_pairs(int npair, const int2 *pair_ab, const int4 *info, const 
     if (npair <= 0) return;
     build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, pair_ab, info, pp_src, xyz, poff,
                                                           expn, ncoef, std::sqrt(2.0) * std::pow(M_PI, 1.25),
-                                                          pp, geo);
+                                                          nullptr, pp, geo);
 }
 
 // The scaled Boys tables of the kernels for M = 0..nM-1: row n of table M holds
@@ -307,6 +311,7 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) { delete ctx; return MOLINTS_ERR_CUDA; }
     bool ok = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreate(&ctx->ev0) == cudaSuccess && cudaEventCreate(&ctx->ev1) == cudaSuccess &&
               cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; ok && i < molints_ctx::kSide; ++i)
@@ -360,10 +365,16 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
     return MOLINTS_OK;
 }
 
+static void plan_release_device(molints_plan *p);
+
 int molints_destroy(molints_ctx *ctx) {
     if (!ctx) return MOLINTS_OK;
     molints_serve_stop(ctx);
     cudaSetDevice(ctx->device);
+    // Plans the caller has not destroyed lose their device state now; destroying one later
+    // only frees its host record.
+    for (molints_plan *p : ctx->plans) plan_release_device(p);
+    ctx->plans.clear();
     if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->stream = ctx->own_stream;
@@ -383,6 +394,7 @@ int molints_destroy(molints_ctx *ctx) {
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     delete ctx;
     return MOLINTS_OK;
 }
@@ -454,21 +466,35 @@ int molints_boys_eval(molints_ctx *ctx, int32_t mode, int32_t mmax, const double
     return MOLINTS_OK;
 }
 
-static void plan_free(molints_plan *p) {
-    if (!p) return;
+// The plan's CUDA objects and device buffers (stream-ordered frees after its queued work);
+// the plan is left orphaned (ctx == nullptr).
+static void plan_release_device(molints_plan *p) {
+    if (!p || !p->ctx) return;
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
     for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
-    void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src,
+    p->prof_ev.clear();
+    void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon};
     for (void *b : bufs) dev_free(p->ctx, b);
-    if (p->ctx) p->ctx->held -= p->bytes;
+    p->ctx->held -= p->bytes;
+    p->ctx = nullptr;
+}
+
+static void plan_free(molints_plan *p) {
+    if (!p) return;
+    if (p->ctx) {
+        std::vector<molints_plan *> &v = p->ctx->plans;
+        v.erase(std::remove(v.begin(), v.end(), p), v.end());
+    }
+    plan_release_device(p);
     delete p;
 }
 
 int molints_plan_destroy(molints_plan *p) {
     if (!p) return MOLINTS_OK;
-    cudaSetDevice(p->ctx->device);
-    plan_free(p);  // stream-ordered frees after the plan's queued work
+    if (p->ctx) cudaSetDevice(p->ctx->device);
+    plan_free(p);
     return MOLINTS_OK;
 }
 
@@ -708,15 +734,22 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<int4> info_h(npair);
     std::vector<int> src_h;
     std::vector<int> cls_start(kNumPairClasses + 1, 0);
-    std::vector<std::vector<int>> kept;  // indexed by position in the stage-1 order
+    // kept primitive pairs of each pair, (b_k, source) sorted by b_k descending; indexed by
+    // position in the stage-1 order
+    std::vector<std::vector<std::pair<double, int>>> kept;
+    std::vector<double> pbk_h;
     auto fill_tables = [&](const std::vector<int> *stage1_pos) {
         src_h.clear();
+        pbk_h.clear();
         std::fill(cls_start.begin(), cls_start.end(), 0);
         for (int k = 0; k < npair; ++k) {
             ab_h[k] = make_int2(pr[k].a, pr[k].b);
             const int off = (int)src_h.size();
             if (stage1_pos) {
-                for (int x : kept[(*stage1_pos)[k]]) src_h.push_back(x);
+                for (const auto &x : kept[(*stage1_pos)[k]]) {
+                    src_h.push_back(x.second);
+                    pbk_h.push_back(x.first);
+                }
             } else {
                 for (int ia = 0; ia < K[pr[k].a]; ++ia)
                     for (int ib = 0; ib < K[pr[k].b]; ++ib) src_h.push_back((ia << 8) | ib);
@@ -774,7 +807,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     if (npair > 0) {
         build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, p->pair_ab, p->info, p->pp_src,
                                                                p->sh_xyz, p->sh_poff, p->expn,
-                                                               p->ncoef, c0, p->pp, p->geo);
+                                                               p->ncoef, c0, nullptr, p->pp, p->geo);
         for (int c = 0; c < kNumPairClasses; ++c) {
             const int n = cls_start[c + 1] - cls_start[c];
             if (kSchwarzLaunchers[c]) kSchwarzLaunchers[c](P, Bt, cls_start[c], n, pbound, nullptr, 0, s);
@@ -810,10 +843,13 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         for (int x = 0; x < info_h[k].y; ++x) {
             const double2 bb = pb_h[info_h[k].x + x];
             if (opts.prim_cutoff > 0.0 && bb.x * qmax[pr[k].mol] < opts.prim_cutoff) continue;
-            kept[k].push_back(src_h[info_h[k].x + x]);
+            kept[k].push_back({bb.x, src_h[info_h[k].x + x]});
             qa += bb.x;
             wa += bb.y;
         }
+        // largest bound first: the kernels stop a primitive loop once b_i b_j < prim_cutoff
+        std::stable_sort(kept[k].begin(), kept[k].end(),
+                         [](const std::pair<double, int> &u, const std::pair<double, int> &v) { return u.first > v.first; });
         const double *A = &xyz[3 * pr[k].a], *Bc = &xyz[3 * pr[k].b];
         const double dab = std::sqrt((A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
                                      (A[2] - Bc[2]) * (A[2] - Bc[2]));
@@ -967,11 +1003,14 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     p->plan_ms[2] = ms_since(t_phase);
     t_phase = clk::now();
     rc = dev_alloc(ctx, &p->chunks, chunks.size(), &p->bytes);
+    if (!rc) rc = dev_alloc(ctx, &p->pbk, (size_t)std::max<int64_t>(nkept, 1), &p->bytes);
     if (rc) { plan_free(p); return rc; }
     if ((e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->bnd, p->bnd_h.data(), npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
         (nkept > 0 && (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nkept * sizeof(int),
+                                           cudaMemcpyHostToDevice, s))) ||
+        (nkept > 0 && (e = cudaMemcpyAsync(p->pbk, pbk_h.data(), nkept * sizeof(double),
                                            cudaMemcpyHostToDevice, s))) ||
         (chunks.size() > 0 && (e = cudaMemcpyAsync(p->chunks, chunks.data(), chunks.size() * sizeof(int4),
                                                    cudaMemcpyHostToDevice, s))) ||
@@ -983,6 +1022,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     }
     (void)mol_cls_start;
     p->plan_ms[3] = ms_since(t_phase);
+    ctx->plans.push_back(p);
     *out = p;
     return MOLINTS_OK;
 }
@@ -1021,7 +1061,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         if (int rc = mark(launches, "build_pairs", 0, s)) return rc;
         build_pairs_kernel<<<(p->npair + 127) / 128, 128, 0, s>>>(
             p->npair, p->pair_ab, p->info, p->pp_src, p->sh_xyz, p->sh_poff, p->expn, p->ncoef,
-            std::sqrt(2.0) * std::pow(M_PI, 1.25), p->pp, p->geo);
+            std::sqrt(2.0) * std::pow(M_PI, 1.25), p->pbk, p->pp, p->geo);
         if (int rc = mark(launches, "build_pairs", 1, s)) return rc;
         ++launches;
     }
@@ -1057,6 +1097,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         Q.counter = p->counters + x * kNumPairClasses + y;
         Q.screen_cut = p->opts.screen_cutoff;
         Q.fp32_cut = p->opts.fp32_cutoff;
+        Q.prim_cut = p->opts.prim_cutoff;
         // HGP: one warp per chunk, four per block; Rys: the launcher divides by its groups/block
         const int grid = rys ? occ * ctx->num_sms
                              : (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);
@@ -1094,6 +1135,7 @@ static void plan_occupancy(molints_plan *p) {
 int molints_plan_execute(molints_plan *p, double *out_device) {
     if (!p || (!out_device && p->npacked > 0))
         return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_execute: null argument");
+    if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
     if (!p->use_graph || p->profiling) return plan_enqueue(p, out_device, true);
@@ -1105,10 +1147,13 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
             p->gexec = nullptr;
         }
         plan_occupancy(p);
-        MI_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        // captured on the context's capture stream, launched on its current stream
+        MI_CUDA(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+        ctx->stream = ctx->cap_stream;
         const int rc = plan_enqueue(p, out_device, false);
+        ctx->stream = s;
         cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamEndCapture(s, &g);
+        cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);
         if (rc) {
             if (g) cudaGraphDestroy(g);
             return rc;
@@ -1131,6 +1176,7 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
 int molints_plan_jk(molints_plan *p, const double *D_device, double *J_device, double *K_device) {
     if (!p || !D_device || !J_device || !K_device)
         return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_jk: null argument");
+    if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     if (p->nmol != 1) return fail(ctx, MOLINTS_ERR_INVALID, "plan_jk: one molecule per plan");
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -1187,6 +1233,7 @@ int molints_plan_set_graph(molints_plan *p, int enable) {
 
 int molints_plan_stats(const molints_plan *p, molints_stats *st) {
     if (!p || !st) return MOLINTS_ERR_INVALID;
+    if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     std::memset(st, 0, sizeof(*st));
     st->n_eri = p->npacked;
@@ -1245,6 +1292,7 @@ int molints_plan_set_profiling(molints_plan *p, int enable) {
 
 int molints_plan_launch_times(molints_plan *p, const char **names, float *ms, int cap) {
     if (!p || cap < 0 || (cap > 0 && (!names || !ms))) return MOLINTS_ERR_INVALID;
+    if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     if (!p->profiling) return fail(ctx, MOLINTS_ERR_INVALID, "launch_times: profiling is off");
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -1259,6 +1307,7 @@ int molints_plan_launch_times(molints_plan *p, const char **names, float *ms, in
 
 int molints_plan_schwarz(molints_plan *p, double *out) {
     if (!p || !out) return MOLINTS_ERR_INVALID;
+    if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
     if (p->npair == 0) return MOLINTS_OK;

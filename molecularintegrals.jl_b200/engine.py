@@ -300,7 +300,7 @@ class Engine:
 
     def _check(self, rc: int):
         if rc != 0:
-            msg = self.lib.molints_last_error(self.ctx)
+            msg = self.lib.molints_last_error(self.ctx) if self.ctx else b"context closed"
             raise MolintsError(rc, msg.decode() if msg else "")
 
     def set_stream(self, stream_handle: int | None):

@@ -470,3 +470,21 @@ def test_jk_digestion_matches_make2JmK(eng, oracle, which):
         Ks += Kd.cpu().numpy()
         plan.close()
     assert np.max(np.abs(Js - Jr)) < 1e-11 * scale and np.max(np.abs(Ks - Kr)) < 1e-11 * scale
+
+
+def test_plan_outliving_its_engine():
+    """A plan whose engine was closed first fails cleanly (invalid argument) and can still be
+    destroyed: the context's destruction released the plan's device state."""
+    import torch
+    from molints_b200 import engine
+    e = engine.Engine(0)
+    sh = mi.config0()
+    plan = e.plan(sh)
+    out = torch.empty(sh.npacked, dtype=torch.float64, device="cuda")
+    plan.execute(out.data_ptr())
+    torch.cuda.synchronize()
+    e.close()
+    with pytest.raises(engine.MolintsError) as err:
+        plan.execute(out.data_ptr())
+    assert err.value.status == -1
+    plan.close()
