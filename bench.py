@@ -257,8 +257,10 @@ def run_ours(args):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": npacked * 8,
            "timing": "host wall clock around molints_eri_packed (synchronous call)"}
 
-    batch = serving = tuned = None
+    batch = serving = tuned = jk = None
     parts = set(args.parts.split(","))
+    if "jk" in parts:
+        jk = measure_jk(eng, stream, dev, sh, plan64, flush)
     if parts & {"batch", "serve"}:
         # per-class HGP/Rys choice for the batch and serving workloads (l <= 3 molecules)
         from molints_b200 import autotune as AT
@@ -308,6 +310,7 @@ def run_ours(args):
             "e2e": e2e,
             "batch_config3": batch,
             "serving_config4": serving,
+            "jk_config1": jk,
             "class_method_tuning": tuned,
             "gpu_launches": args.steps * 2 * plan64.stats()["n_kernel_launches"],
             "clocks": clocks,
@@ -456,6 +459,33 @@ def measure_serving(device, fp32_cut, window_s, rank, rate=200.0, nslots=8,
     return out
 
 
+def measure_jk(eng, stream, dev, sh, plan, flush, k=5):
+    """Coulomb and exchange matrices of the headline workload for a random symmetric
+    density, digested in the integral kernels (molints_plan_jk: no packed vector written):
+    device time per build and the rate in integrals digested per second."""
+    import torch
+    n = sh.nbf
+    g = torch.Generator(device="cpu").manual_seed(0)
+    A = torch.randn(n, n, generator=g, dtype=torch.float64)
+    D = ((A + A.T) / n).to(dev)
+    J = torch.empty_like(D)
+    K = torch.empty_like(D)
+    plan.jk(D.data_ptr(), J.data_ptr(), K.data_ptr())
+    torch.cuda.synchronize(dev)
+    ts = []
+    for _ in range(k):
+        flush_l2(flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        plan.jk(D.data_ptr(), J.data_ptr(), K.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ts.append(a.elapsed_time(b))
+    ms = float(np.median(ts))
+    return {"ms_per_build": ms, "eri_digested_per_s": sh.npacked / (ms * 1e-3),
+            "note": "J and K (n x n) from one execute with the digestion sink; FP64 atomics"}
+
+
 def measure_fp64_peak(dev) -> float:
     import torch
     a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
@@ -481,7 +511,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--serve-window", type=float, default=5.0,
                     help="seconds of Poisson arrivals in the serving measurement")
-    ap.add_argument("--parts", default="batch,serve,cpu",
+    ap.add_argument("--parts", default="batch,serve,cpu,jk",
                     help="extra measurements beside the headline workload (profiling runs "
                          "pass an empty string)")
     args = ap.parse_args()

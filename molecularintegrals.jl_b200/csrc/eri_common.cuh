@@ -34,7 +34,7 @@ constexpr double kBoysReferenceSwitch = 30.0;  // farray's Tmax, src/Boys.jl:19
 //   P    = (a A + b B) / zeta (gaussian_product_center, src/OneInts.jl:78-83)
 //   PA   = P - A
 //   b    = sqrt(max |(ab|ab)|) of this primitive pair (its Schwarz bound; 0 before the plan's
-//          bound pass); a shell pair's kept primitive pairs are sorted by b, largest first
+//          bound pass); a shell pair's kept primitive pairs are stored by b, largest first
 // so that kab_bra * kab_ket / sqrt(zeta+eta) is the [00|00] prefactor of HGP eq. 12,
 // 2 pi^(5/2) / (zeta eta sqrt(zeta+eta)) x exp(...) x coefficients.
 struct PrimPair {
@@ -87,7 +87,6 @@ struct EriQueue {
     int *counter;                 // next chunk; zero at launch
     double screen_cut;            // Qabs_p Qabs_q below this: written as 0
     double fp32_cut;              // R_p R_q below this (MIXED kernels): FP32 VRR
-    double prim_cut;              // primitive quartets with b_i b_j below this are skipped
 };
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {

@@ -13,22 +13,16 @@ template <typename VT>
 __device__ __forceinline__ void quartet_fppp(const PairTab &P, const BoysTab &B, int p, int q,
                                               int i0, int i1, int j0, int j1,
                                               double *__restrict__ res,
-                                              double *__restrict__ acc_out = nullptr,
-                                              double pcut = 0.0) {
+                                              double *__restrict__ acc_out = nullptr) {
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
     double acc[225];
 #pragma unroll
     for (int x = 0; x < 225; ++x) acc[x] = 0.0;
-    // primitive pairs are sorted by their bound b (largest first): once b_i b_j < pcut the
-    // rest of the loop only holds smaller terms (each below pcut by the Schwarz inequality)
-    const double bmax = i1 > i0 ? __ldg(&P.pp[ib_.x + i0].b) : 0.0;
     for (int j = j0; j < j1; ++j) {
         const PrimPair ket = load_pp(P.pp, ik_.x + j);
-        if (bmax * ket.b < pcut) break;
         for (int i = i0; i < i1; ++i) {
             const PrimPair bra = load_pp(P.pp, ib_.x + i);
-            if (bra.b * ket.b < pcut) break;
             const double r = rsqrt(bra.zeta + ket.zeta);
             const double r2 = r * r;
             const double PQx = bra.px - ket.px, PQy = bra.py - ket.py, PQz = bra.pz - ket.pz;
@@ -2171,8 +2165,8 @@ __global__ void __launch_bounds__(128) eri_queue_fppp(const EriQueue Q) {
             for (int x = 0; x < 270; ++x) res[x] = 0.0;
         } else {
             const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
-            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_fppp<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res, nullptr, Q.prim_cut);
-            else quartet_fppp<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res, nullptr, Q.prim_cut);
+            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_fppp<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+            else quartet_fppp<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
         }
         if (Q.jk.J) jk_fppp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
         else store_fppp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),

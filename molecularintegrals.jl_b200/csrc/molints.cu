@@ -847,7 +847,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             qa += bb.x;
             wa += bb.y;
         }
-        // largest bound first: the kernels stop a primitive loop once b_i b_j < prim_cutoff
+        // largest bound first (the order of the primitive loops)
         std::stable_sort(kept[k].begin(), kept[k].end(),
                          [](const std::pair<double, int> &u, const std::pair<double, int> &v) { return u.first > v.first; });
         const double *A = &xyz[3 * pr[k].a], *Bc = &xyz[3 * pr[k].b];
@@ -1097,7 +1097,6 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         Q.counter = p->counters + x * kNumPairClasses + y;
         Q.screen_cut = p->opts.screen_cutoff;
         Q.fp32_cut = p->opts.fp32_cutoff;
-        Q.prim_cut = p->opts.prim_cutoff;
         // HGP: one warp per chunk, four per block; Rys: the launcher divides by its groups/block
         const int grid = rys ? occ * ctx->num_sms
                              : (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);

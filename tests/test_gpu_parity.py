@@ -113,7 +113,9 @@ def test_split_valence_24_full(eng, oracle):
     ij = np.repeat(np.arange(npair), np.arange(1, npair + 1))
     kl = np.arange(len(got)) - ij * (ij + 1) // 2
     bound = np.sqrt(np.abs(diag[ij] * diag[kl]))
-    assert np.all(np.abs(got) <= bound * (1 + 1e-10) + 1e-14)
+    # each value carries up to the parity tolerance, so equality cases may exceed by that much
+    excess = np.abs(got) - bound * (1 + 1e-10)
+    assert excess.max() < TOL_FP64, (excess.max(), int(np.argmax(excess)))
 
 
 @pytest.mark.parametrize("seed,lmax", [(101, 0), (102, 1), (103, 2), (104, 2)])
