@@ -490,3 +490,25 @@ def test_plan_outliving_its_engine():
         plan.execute(out.data_ptr())
     assert err.value.status == -1
     plan.close()
+
+
+@pytest.mark.parametrize("method", ["hgp", "rys"])
+def test_reference_coulomb_pins_on_device(eng, golden, oracle, method):
+    """The known answers of test/runtests.jl (coulomb and coulomb_rys cases: (ss|ss), (ss|pxpx)
+    and the s-s distance sweep on unit-exponent primitives) computed by the device path with
+    either method, at the reference's own tolerance (rtol 1.5e-8)."""
+    from molints_b200 import engine
+    m = engine.METHOD_HGP if method == "hgp" else engine.METHOD_RYS
+    o = (0.0, 0.0, 0.0)
+    g = golden["coulomb"]
+    one_s = mi.Shells.from_list([(o, 0, [(1.0, 1.0)])])
+    assert eng.eri_packed(one_s, method=m, boys=engine.BOYS_EXACT)[0] == pytest.approx(
+        g["c,c,c,c"]["value"], rel=1.5e-8)
+    sp = mi.Shells.from_list([(o, 0, [(1.0, 1.0)]), (o, 1, [(1.0, 1.0)])])
+    v = eng.eri_packed(sp, method=m, boys=engine.BOYS_EXACT)
+    assert v[oracle.iindex(0, 0, 1, 1)] == pytest.approx(g["s,s,px,px"]["value"], rel=1.5e-8)
+    assert abs(v[oracle.iindex(0, 0, 0, 1)]) < 1e-17
+    for case in golden["ss_distance_sweep"]:
+        two = mi.Shells.from_list([(o, 0, [(1.0, 1.0)]), ((0.0, 0.0, case["r"]), 0, [(1.0, 1.0)])])
+        w = eng.eri_packed(two, method=m, boys=engine.BOYS_EXACT)
+        assert w[oracle.iindex(0, 0, 1, 1)] == pytest.approx(case["value"], rel=1.5e-8)
