@@ -34,7 +34,7 @@ constexpr double kBoysReferenceSwitch = 30.0;  // farray's Tmax, src/Boys.jl:19
 //   P    = (a A + b B) / zeta (gaussian_product_center, src/OneInts.jl:78-83)
 //   PA   = P - A
 //   b    = sqrt(max |(ab|ab)|) of this primitive pair (its Schwarz bound; 0 before the plan's
-//          bound pass); a shell pair's kept primitive pairs are stored by b, largest first
+//          bound pass)
 // so that kab_bra * kab_ket / sqrt(zeta+eta) is the [00|00] prefactor of HGP eq. 12,
 // 2 pi^(5/2) / (zeta eta sqrt(zeta+eta)) x exp(...) x coefficients.
 struct PrimPair {

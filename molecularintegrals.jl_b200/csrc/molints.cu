@@ -734,8 +734,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<int4> info_h(npair);
     std::vector<int> src_h;
     std::vector<int> cls_start(kNumPairClasses + 1, 0);
-    // kept primitive pairs of each pair, (b_k, source) sorted by b_k descending; indexed by
-    // position in the stage-1 order
+    // kept primitive pairs of each pair, (b_k, source) in source order; indexed by position in
+    // the stage-1 order
     std::vector<std::vector<std::pair<double, int>>> kept;
     std::vector<double> pbk_h;
     auto fill_tables = [&](const std::vector<int> *stage1_pos) {
@@ -847,9 +847,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             qa += bb.x;
             wa += bb.y;
         }
-        // largest bound first (the order of the primitive loops)
-        std::stable_sort(kept[k].begin(), kept[k].end(),
-                         [](const std::pair<double, int> &u, const std::pair<double, int> &v) { return u.first > v.first; });
         const double *A = &xyz[3 * pr[k].a], *Bc = &xyz[3 * pr[k].b];
         const double dab = std::sqrt((A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
                                      (A[2] - Bc[2]) * (A[2] - Bc[2]));
