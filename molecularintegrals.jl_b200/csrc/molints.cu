@@ -906,9 +906,10 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 nchunk32 += (x == y) ? nb * (nb + 1) / 64.0 + nb : nb * (nk / 32.0 + 1.0);
             }
     const int widen = std::max(1, (int)std::ceil(nchunk32 / kMaxChunks));
-    // A Rys group computes a chunk's quartets one after another, so its chunks are short
-    // (kRysChunk ket pairs) to spread small classes over many groups.
-    constexpr int kRysChunk = 4;
+    // A Rys group computes a chunk's quartets one after another, so its chunks hold one ket
+    // pair: the large classes have few quartets (e.g. 231 (ff|ff) quartets for six f shells),
+    // and a quartet is microseconds of work beside one atomic on the queue counter.
+    constexpr int kRysChunk = 1;
     // Class pairs are independent: their queues are built on host threads, then concatenated.
     struct ClassQueue { std::vector<int4> q; double total = 0.0; };
     std::vector<std::pair<int, int>> cps;
