@@ -880,7 +880,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
 
     // ---- work queues: per class pair, chunks of one bra pair and <= 32 ket pairs of the same
     // molecule, ordered by decreasing estimated cost (kept primitive quartets x class weight)
-    std::vector<int> mol_cls_start((size_t)(nmol + 1) * kNumPairClasses, 0);  // [cls][mol] ranges
     auto range_of = [&](int cls, int m, int &b0, int &b1) {
         b0 = b1 = cls_start[cls];
         // pairs of class cls are sorted by molecule: binary search the molecule's run
@@ -906,10 +905,22 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 nchunk32 += (x == y) ? nb * (nb + 1) / 64.0 + nb : nb * (nk / 32.0 + 1.0);
             }
     const int widen = std::max(1, (int)std::ceil(nchunk32 / kMaxChunks));
-    // A Rys group computes a chunk's quartets one after another, so its chunks hold one ket
-    // pair: the large classes have few quartets (e.g. 231 (ff|ff) quartets for six f shells),
-    // and a quartet is microseconds of work beside one atomic on the queue counter.
-    constexpr int kRysChunk = 1;
+    // A Rys group computes a chunk's quartets one after another.  Its chunks are as long as
+    // keeps about kRysMinChunks chunks in the class queue (1..8 ket pairs): the large classes
+    // have few quartets (e.g. 231 (ff|ff) quartets for six f shells) and need one group per
+    // quartet, while the many small quartets of the low classes amortise the queue atomic.
+    constexpr double kRysMinChunks = 4096.0;
+    auto rys_width = [&](int x, int y) {
+        double nq = 0.0;
+        for (int m = 0; m < nmol; ++m) {
+            int b0, b1, k0, k1;
+            range_of(x, m, b0, b1);
+            range_of(y, m, k0, k1);
+            const double nb = b1 - b0, nk = k1 - k0;
+            nq += (x == y) ? nb * (nb + 1) / 2 : nb * nk;
+        }
+        return std::max(1, std::min(8, (int)(nq / kRysMinChunks)));
+    };
     // Class pairs are independent: their queues are built on host threads, then concatenated.
     struct ClassQueue { std::vector<int4> q; double total = 0.0; };
     std::vector<std::pair<int, int>> cps;
@@ -918,7 +929,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<ClassQueue> cq(cps.size());
     auto build_queue = [&](size_t ci) {
         const int x = cps[ci].first, y = cps[ci].second;
-        const int width = (p->method[x][y] == MOLINTS_METHOD_RYS ? kRysChunk : 32) * widen;
+        const int width = (p->method[x][y] == MOLINTS_METHOD_RYS ? rys_width(x, y) : 32) * widen;
         const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
         const double w = 1.0 + lsum * lsum;
         // heaviest first, bucketed by the binary exponent of the cost: an O(n) order that is
@@ -1018,7 +1029,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
     }
-    (void)mol_cls_start;
     p->plan_ms[3] = ms_since(t_phase);
     ctx->plans.push_back(p);
     *out = p;

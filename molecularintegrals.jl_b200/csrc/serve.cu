@@ -12,10 +12,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <chrono>
 #include <condition_variable>
-#include <cstring>
 #include <deque>
 #include <mutex>
 #include <new>
@@ -36,8 +34,6 @@ double now_s() {
     using namespace std::chrono;
     return duration_cast<duration<double>>(steady_clock::now().time_since_epoch()).count();
 }
-
-int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
 struct Server;
 
