@@ -40,7 +40,7 @@ LMAX = 3             # shells up to f
 NMONO = 20           # monomials AB^(px,py,pz), px+py+pz <= 3
 # Classes with at least this many block entries and at most MIXED_MAX_ACC accumulators per
 # thread get an FP32 variant for MIXED quartets (stage-2 products summed in FP32 per batch).
-MIXED_MIN_NBLK = 100
+MIXED_MIN_NBLK = 32
 MIXED_MAX_ACC = 24
 
 

@@ -71,7 +71,7 @@ static void rys_prepare_dpds() {
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
         cudaFuncSetAttribute(rys_queue_dpds<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
-
+        cudaFuncSetAttribute(rys_queue_dpds<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 35840);
 
         done[dev] = true;
     }
@@ -83,16 +83,16 @@ void launch_rys_dpds(const EriQueue &Q, const RysTab &R, int mixed, int grid_max
     rys_prepare_dpds();
     constexpr int ng = 128 / C_dpds::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    (void)mixed;  // no FP32 variant for this class
-    rys_queue_dpds<0><<<grid, 128, 35840, s>>>(Q, R);
+    if (mixed) rys_queue_dpds<1><<<grid, 128, 35840, s>>>(Q, R);
+    else rys_queue_dpds<0><<<grid, 128, 35840, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dpds(int mixed) {
     rys_prepare_dpds();
     int n = 0;
-    (void)mixed;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpds<0>, 128, 35840);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpds<1>, 128, 35840);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpds<0>, 128, 35840);
     return n;
 }
 

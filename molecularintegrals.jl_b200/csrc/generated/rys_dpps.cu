@@ -66,7 +66,7 @@ static void rys_prepare_dpps() {
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
         cudaFuncSetAttribute(rys_queue_dpps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 24320);
-
+        cudaFuncSetAttribute(rys_queue_dpps<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 24320);
 
         done[dev] = true;
     }
@@ -78,16 +78,16 @@ void launch_rys_dpps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max
     rys_prepare_dpps();
     constexpr int ng = 128 / C_dpps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    (void)mixed;  // no FP32 variant for this class
-    rys_queue_dpps<0><<<grid, 128, 24320, s>>>(Q, R);
+    if (mixed) rys_queue_dpps<1><<<grid, 128, 24320, s>>>(Q, R);
+    else rys_queue_dpps<0><<<grid, 128, 24320, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dpps(int mixed) {
     rys_prepare_dpps();
     int n = 0;
-    (void)mixed;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpps<0>, 128, 24320);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpps<1>, 128, 24320);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpps<0>, 128, 24320);
     return n;
 }
 

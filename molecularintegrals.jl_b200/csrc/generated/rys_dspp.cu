@@ -64,7 +64,7 @@ static void rys_prepare_dspp() {
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
         cudaFuncSetAttribute(rys_queue_dspp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
-
+        cudaFuncSetAttribute(rys_queue_dspp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 27200);
 
         done[dev] = true;
     }
@@ -76,16 +76,16 @@ void launch_rys_dspp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max
     rys_prepare_dspp();
     constexpr int ng = 128 / C_dspp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    (void)mixed;  // no FP32 variant for this class
-    rys_queue_dspp<0><<<grid, 128, 27200, s>>>(Q, R);
+    if (mixed) rys_queue_dspp<1><<<grid, 128, 27200, s>>>(Q, R);
+    else rys_queue_dspp<0><<<grid, 128, 27200, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dspp(int mixed) {
     rys_prepare_dspp();
     int n = 0;
-    (void)mixed;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp<0>, 128, 27200);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp<1>, 128, 27200);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dspp<0>, 128, 27200);
     return n;
 }
 

@@ -95,7 +95,7 @@ static void rys_prepare_fdss() {
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
         cudaFuncSetAttribute(rys_queue_fdss<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 18560);
-
+        cudaFuncSetAttribute(rys_queue_fdss<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 18560);
 
         done[dev] = true;
     }
@@ -107,16 +107,16 @@ void launch_rys_fdss(const EriQueue &Q, const RysTab &R, int mixed, int grid_max
     rys_prepare_fdss();
     constexpr int ng = 128 / C_fdss::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    (void)mixed;  // no FP32 variant for this class
-    rys_queue_fdss<0><<<grid, 128, 18560, s>>>(Q, R);
+    if (mixed) rys_queue_fdss<1><<<grid, 128, 18560, s>>>(Q, R);
+    else rys_queue_fdss<0><<<grid, 128, 18560, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fdss(int mixed) {
     rys_prepare_fdss();
     int n = 0;
-    (void)mixed;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fdss<0>, 128, 18560);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fdss<1>, 128, 18560);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fdss<0>, 128, 18560);
     return n;
 }
 

@@ -75,7 +75,7 @@ static void rys_prepare_fpps() {
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
         cudaFuncSetAttribute(rys_queue_fpps<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 30080);
-
+        cudaFuncSetAttribute(rys_queue_fpps<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 30080);
 
         done[dev] = true;
     }
@@ -87,16 +87,16 @@ void launch_rys_fpps(const EriQueue &Q, const RysTab &R, int mixed, int grid_max
     rys_prepare_fpps();
     constexpr int ng = 128 / C_fpps::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    (void)mixed;  // no FP32 variant for this class
-    rys_queue_fpps<0><<<grid, 128, 30080, s>>>(Q, R);
+    if (mixed) rys_queue_fpps<1><<<grid, 128, 30080, s>>>(Q, R);
+    else rys_queue_fpps<0><<<grid, 128, 30080, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_fpps(int mixed) {
     rys_prepare_fpps();
     int n = 0;
-    (void)mixed;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpps<0>, 128, 30080);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpps<1>, 128, 30080);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_fpps<0>, 128, 30080);
     return n;
 }
 
