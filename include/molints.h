@@ -234,6 +234,13 @@ int molints_boys_eval(molints_ctx *ctx, int32_t boys_mode, int32_t mmax, const d
 int molints_eri_packed_noalloc(const molints_basis *basis, const molints_options *opts,
                                double *out_device, void *stream, char *err, size_t err_len);
 
+/* The one-electron matrices of the basis, the drop-in for all_1e_ints(bfs, mol)
+ * (src/OneInts.jl:267-290): overlap S, kinetic energy T and nuclear attraction V (summed over
+ * natom point charges atom_charge[c] at atom_xyz[3c..3c+2], bohr), each n x n row-major in host
+ * memory, for the same normalised functions as the ERIs.  Shells up to f.  Synchronous. */
+int molints_one_e(molints_ctx *ctx, const molints_basis *basis, int32_t natom,
+                  const double *atom_xyz, const double *atom_charge, double *S, double *T, double *V);
+
 /* ------------------------------------------------------------------------------------------
  * Serving: molecules submitted as they arrive, computed concurrently, results kept on the
  * device until released.  No reference counterpart (the reference computes one basis per

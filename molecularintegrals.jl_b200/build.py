@@ -42,7 +42,7 @@ def sources():
     finally:
         sys.path.pop(0)
     gen = gen_eri.generate()
-    return ([CSRC / "molints.cu", CSRC / "noalloc.cu", CSRC / "serve.cu",
+    return ([CSRC / "molints.cu", CSRC / "noalloc.cu", CSRC / "serve.cu", CSRC / "one_e.cu",
              CSRC / "generated" / "rys_tables.cu"] +
             sorted(gen))
 

@@ -265,6 +265,39 @@ void fill_boys_scaled(double *sc, int nM) {
 
 namespace molints {
 int ctx_device_of(const molints_ctx *ctx) { return ctx->device; }
+RysTab ctx_rys(const molints_ctx *ctx) { return ctx->rys; }
+
+// Normalised contraction coefficients of a basis (indexed like its primitives): raw coef x
+// (2a/pi)^(3/4) (4a)^(L/2) x the CGBF norm (PGBF/CGBF normalize!, src/Basis.jl:42-83).
+int basis_ncoef(const molints_basis *b, std::vector<double> &ncoef, std::string &err) {
+    int nprim = 0;
+    for (int s = 0; s < b->nshell; ++s) {
+        if (b->nprim[s] < 1 || b->prim_off[s] < 0) { err = "shell without primitives"; return MOLINTS_ERR_INVALID; }
+        nprim = std::max(nprim, b->prim_off[s] + b->nprim[s]);
+    }
+    for (int k = 0; k < nprim; ++k)
+        if (!(b->expn[k] > 0.0) || !std::isfinite(b->expn[k]) || !std::isfinite(b->coef[k])) {
+            err = "exponents must be finite and > 0";
+            return MOLINTS_ERR_INVALID;
+        }
+    ncoef.assign(std::max(nprim, 1), 0.0);
+    for (int s = 0; s < b->nshell; ++s) {
+        const int p0 = b->prim_off[s], K = b->nprim[s], Ls = b->L[s];
+        double S = 0;
+        for (int i = 0; i < K; ++i)
+            for (int j = 0; j < K; ++j) {
+                const double x = b->expn[p0 + i], y = b->expn[p0 + j];
+                S += b->coef[p0 + i] * b->coef[p0 + j] * std::pow(2 * std::sqrt(x * y) / (x + y), Ls + 1.5);
+            }
+        if (!(S > 0.0)) { err = "zero contracted function"; return MOLINTS_ERR_INVALID; }
+        const double cn = 1.0 / std::sqrt(S);
+        for (int i = 0; i < K; ++i) {
+            const double a = b->expn[p0 + i];
+            ncoef[p0 + i] = b->coef[p0 + i] * cn * std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * Ls);
+        }
+    }
+    return MOLINTS_OK;
+}
 // The AUTO method table of src, given to dst (the serving slots inherit their owner's table).
 void ctx_copy_methods(molints_ctx *dst, const molints_ctx *src) {
     std::memcpy(dst->class_method, src->class_method, sizeof(dst->class_method));

@@ -42,7 +42,7 @@ EXPORTED_SYMBOLS = [
     "molints_serve_start", "molints_serve_stop", "molints_submit", "molints_poll",
     "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
     "molints_release", "molints_serve_stats", "molints_shard_range", "molints_plan_create_shard",
-    "molints_plan_set_graph", "molints_plan_jk", "molints_jk",
+    "molints_plan_set_graph", "molints_plan_jk", "molints_jk", "molints_one_e",
 ]
 
 
@@ -132,6 +132,7 @@ def load_library(path: Path | str | None = None):
         "molints_plan_set_graph": (ctypes.c_int, [P, ctypes.c_int]),
         "molints_plan_jk": (ctypes.c_int, [P, P, P, P]),
         "molints_jk": (ctypes.c_int, [P, P, P, P, P, P]),
+        "molints_one_e": (ctypes.c_int, [P, P, I32, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -417,6 +418,20 @@ class Engine:
                                         _ptr(D), _ptr(J), _ptr(K)))
         return J, K
 
+    def one_e(self, shells, atom_xyz, atom_charge):
+        """(S, T, V): overlap, kinetic energy and nuclear attraction (point charges
+        atom_charge at atom_xyz, bohr) of the basis, n x n each."""
+        arrs = _BasisArrays(shells)
+        n = shells.nbf
+        xyz = np.ascontiguousarray(atom_xyz, dtype=np.float64).reshape(-1)
+        z = np.ascontiguousarray(atom_charge, dtype=np.float64).reshape(-1)
+        if xyz.size != 3 * z.size:
+            raise ValueError("atom_xyz must hold 3 coordinates per charge")
+        S, T, V = (np.zeros((n, n)) for _ in range(3))
+        self._check(self.lib.molints_one_e(self.ctx, ctypes.byref(arrs.c), z.size, _ptr(xyz), _ptr(z),
+                                           _ptr(S), _ptr(T), _ptr(V)))
+        return S, T, V
+
     def boys(self, mmax: int, T, mode=BOYS_REFERENCE) -> np.ndarray:
         T = np.ascontiguousarray(T, dtype=np.float64)
         out = np.empty((T.size, mmax))
@@ -467,6 +482,14 @@ def all_twoe_ints_chrr(shells) -> np.ndarray:
     """Drop-in for all_twoe_ints_chrr(bfs) (src/HGP.jl:22-34), with its layout and
     normalisation defects fixed: the same vector as all_twoe_ints."""
     return default_engine().eri_packed(shells, method=METHOD_HGP)
+
+
+def all_1e_ints(shells, atoms):
+    """Drop-in for all_1e_ints(bfs, mol) (src/OneInts.jl:267-290): (S, T, V) for the basis and
+    the atoms (objects with ``atno`` and ``xyz`` in bohr, as ``basis.atom`` makes)."""
+    xyz = np.array([a.xyz for a in atoms], dtype=np.float64).reshape(-1, 3)
+    z = np.array([a.atno for a in atoms], dtype=np.float64)
+    return default_engine().one_e(shells, xyz, z)
 
 
 def make2JmK(D, shells) -> np.ndarray:

@@ -461,3 +461,111 @@ def make2JmK(D: np.ndarray, ints: np.ndarray) -> np.ndarray:
     J = np.einsum("ijkl,kl->ij", full, D)
     K = np.einsum("ikjl,kl->ij", full, D)
     return 2 * J - K, J, K
+
+
+# ------------------------------------------------------------------ one-electron integrals
+def _fact2(n: int) -> float:
+    r = 1
+    while n > 1:
+        r *= n
+        n -= 2
+    return float(r)
+
+
+def _binomial_prefactor(s, ia, ib, xpa, xpb):
+    """binomial_prefactor of src/OneInts.jl:94-95."""
+    from math import comb
+    tot = 0.0
+    for t in range(s + 1):
+        if s - ia <= t <= ib:
+            tot += comb(ia, s - t) * xpa ** (ia - s + t) * comb(ib, t) * xpb ** (ib - t)
+    return tot
+
+
+def _overlap1d(la, lb, ax, bx, g):
+    """overlap1d, src/OneInts.jl:86-92."""
+    return sum(_binomial_prefactor(2 * i, la, lb, ax, bx) * _fact2(2 * i - 1) / (2 * g) ** i
+               for i in range((la + lb) // 2 + 1)) if la >= 0 and lb >= 0 else 0.0
+
+
+def overlap_prim(a, A, ia, b, B, ib) -> float:
+    """overlap(aexpn,axyz,aI,aJ,aK,bexpn,bxyz,bI,bJ,bK), src/OneInts.jl:41-52 (no norms)."""
+    A, B = np.asarray(A, float), np.asarray(B, float)
+    g = a + b
+    P = (a * A + b * B) / g
+    pre = (np.pi / g) ** 1.5 * np.exp(-a * b * np.sum((A - B) ** 2) / g)
+    return pre * np.prod([_overlap1d(ia[t], ib[t], P[t] - A[t], P[t] - B[t], g) for t in range(3)])
+
+
+def kinetic_prim(a, A, ia, b, B, ib) -> float:
+    """kinetic(...) of src/OneInts.jl:124-135 (no norms)."""
+    def ov(db):
+        return overlap_prim(a, A, ia, b, B, [ib[t] + db[t] for t in range(3)])
+    t0 = b * (2 * sum(ib) + 3) * ov((0, 0, 0))
+    t1 = -2 * b * b * (ov((2, 0, 0)) + ov((0, 2, 0)) + ov((0, 0, 2)))
+    t2 = -0.5 * sum(ib[t] * (ib[t] - 1) * ov(tuple(-2 if u == t else 0 for u in range(3))) for t in range(3))
+    return t0 + t1 + t2
+
+
+def nuclear_prim(a, A, ia, b, B, ib, C) -> float:
+    """nuclear_attraction(...) of src/OneInts.jl:208-227 via Aarray (:143-165), exact Boys
+    function for Fgamma (no norms, unit charge)."""
+    from math import factorial
+    A, B, C = (np.asarray(v, float) for v in (A, B, C))
+    g = a + b
+    P = (a * A + b * B) / g
+    PA, PB, PC = P - A, P - B, P - C
+
+    def aarray(l1, l2, pa, pb, pc):
+        out = np.zeros(l1 + l2 + 1)
+        for i in range(l1 + l2 + 1):
+            for r in range(i // 2 + 1):
+                for u in range((i - 2 * r) // 2 + 1):
+                    I = i - 2 * r - u
+                    out[I] += ((-1) ** i * _binomial_prefactor(i, l1, l2, pa, pb) * (-1) ** u * factorial(i)
+                               * pc ** (i - 2 * r - 2 * u) * (0.25 / g) ** (r + u)
+                               / (factorial(r) * factorial(u) * factorial(i - 2 * r - 2 * u)))
+        return out
+    Ax, Ay, Az = (aarray(ia[t], ib[t], PA[t], PB[t], PC[t]) for t in range(3))
+    T = g * float(PC @ PC)
+    tot = 0.0
+    for I in range(len(Ax)):
+        for J in range(len(Ay)):
+            for K in range(len(Az)):
+                tot += Ax[I] * Ay[J] * Az[K] * boys(I + J + K, T)
+    return -2 * np.pi * np.exp(-a * b * np.sum((A - B) ** 2) / g) * tot / g
+
+
+def all_1e_ints(shells, atom_xyz, atom_charge):
+    """all_1e_ints(bfs, mol), src/OneInts.jl:267-290, for normalised contracted functions:
+    (S, T, V), V summed over point charges."""
+    from molints_b200 import basis as B_
+    n = shells.nbf
+    funcs = []  # (centre, ijk, [(expn, normalised coefficient)])
+    for s in range(shells.nshell):
+        l = int(shells.L[s])
+        p0, k = int(shells.prim_off[s]), int(shells.nprim[s])
+        ex, co = shells.expn[p0:p0 + k], shells.coef[p0:p0 + k]
+        S0 = sum(co[i] * co[j] * (2 * np.sqrt(ex[i] * ex[j]) / (ex[i] + ex[j])) ** (l + 1.5)
+                 for i in range(k) for j in range(k))
+        for c in B_.shell_components(l):
+            g = 1 / np.sqrt(_fact2(2 * c[0] - 1) * _fact2(2 * c[1] - 1) * _fact2(2 * c[2] - 1))
+            prims = [(e, cf / np.sqrt(S0) * (2 * e / np.pi) ** 0.75 * (4 * e) ** (l / 2) * g)
+                     for e, cf in zip(ex, co)]
+            funcs.append((shells.xyz[s], c, prims))
+    S, T, V = (np.zeros((n, n)) for _ in range(3))
+    atoms = list(zip(np.asarray(atom_xyz, float).reshape(-1, 3), np.asarray(atom_charge, float)))
+    for i in range(n):
+        for j in range(i + 1):
+            A, ia, pa = funcs[i]
+            Bc, ib, pb = funcs[j]
+            s = t = v = 0.0
+            for a, ca in pa:
+                for b, cb in pb:
+                    s += ca * cb * overlap_prim(a, A, ia, b, Bc, ib)
+                    t += ca * cb * kinetic_prim(a, A, ia, b, Bc, ib)
+                    v += ca * cb * sum(z * nuclear_prim(a, A, ia, b, Bc, ib, C) for C, z in atoms)
+            S[i, j] = S[j, i] = s
+            T[i, j] = T[j, i] = t
+            V[i, j] = V[j, i] = v
+    return S, T, V

@@ -512,3 +512,25 @@ def test_reference_coulomb_pins_on_device(eng, golden, oracle, method):
         two = mi.Shells.from_list([(o, 0, [(1.0, 1.0)]), ((0.0, 0.0, case["r"]), 0, [(1.0, 1.0)])])
         w = eng.eri_packed(two, method=m, boys=engine.BOYS_EXACT)
         assert w[oracle.iindex(0, 0, 1, 1)] == pytest.approx(case["value"], rel=1.5e-8)
+
+
+def test_one_electron_matrices(eng, oracle):
+    """S, T and V on the device (molints_one_e, the drop-in for all_1e_ints) against the
+    oracle's restatement of src/OneInts.jl: H2/STO-3G pins of test/runtests.jl:42-47, staggered
+    ethane in STO-3G, and a random basis with shells up to f around four point charges."""
+    from molints_b200 import engine
+    h2 = mi.h2()
+    S, T, V = engine.all_1e_ints(mi.build_basis(h2), h2)
+    assert S[0, 1] == pytest.approx(0.6647387449282997, rel=1.5e-8)
+    assert T[0, 0] == pytest.approx(0.76003188, rel=1.5e-8)
+    assert T[0, 1] == pytest.approx(0.24141861181119084, rel=1.5e-8)
+    eth = mi.ethane_staggered()
+    cases = [(mi.config0(), [a.xyz for a in eth], [a.atno for a in eth])]
+    rng = np.random.default_rng(9)
+    cases.append((_rand_basis(301, 3, natom=2, kmax=2), rng.uniform(-2, 2, (4, 3)), [1.0, 6.0, 8.0, 1.0]))
+    for sh, xyz, z in cases:
+        S, T, V = eng.one_e(sh, xyz, z)
+        Sr, Tr, Vr = oracle.all_1e_ints(sh, xyz, z)
+        for got, ref in ((S, Sr), (T, Tr), (V, Vr)):
+            assert np.max(np.abs(got - ref)) < 1e-12 * max(1.0, np.max(np.abs(ref)))
+        assert np.allclose(np.diag(S), 1.0, atol=1e-13)

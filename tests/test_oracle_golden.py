@@ -250,3 +250,23 @@ def test_hrr_orientation_tight_first(oracle):
     assert np.max(np.abs(ref_f64 - huz)) > 1e-10
     assert np.max(np.abs(st_f64 - huz)) < 1e-13 * max(1.0, np.max(np.abs(huz)))
     assert np.max(np.abs(st_ld - huz)) < np.max(np.abs(ref_ld - huz))
+
+
+def test_one_electron_restatement_pins(oracle):
+    """The one-electron known answers of test/runtests.jl:42-88 on the oracle's restatement of
+    src/OneInts.jl (unit-exponent primitives at the origin, and H2/STO-3G)."""
+    o = (0.0, 0.0, 0.0)
+    ns = oracle.pgbf_norm(1.0, 0, 0, 0)
+    npx = oracle.pgbf_norm(1.0, 1, 0, 0)
+    assert ns ** 2 * oracle.kinetic_prim(1.0, o, (0, 0, 0), 1.0, o, (0, 0, 0)) == pytest.approx(1.5, rel=1e-12)
+    assert oracle.kinetic_prim(1.0, o, (0, 0, 0), 1.0, o, (0, 0, 0)) == pytest.approx(2.9530518648229536, rel=1e-12)
+    assert ns ** 2 * oracle.nuclear_prim(1.0, o, (0, 0, 0), 1.0, o, (0, 0, 0), o) == pytest.approx(-1.59576912, rel=1.5e-8)
+    assert npx ** 2 * oracle.nuclear_prim(1.0, o, (1, 0, 0), 1.0, o, (1, 0, 0), o) == pytest.approx(-1.06384608, rel=1.5e-8)
+    assert oracle.nuclear_prim(1.0, o, (0, 0, 0), 1.0, o, (0, 0, 0), o) == pytest.approx(-np.pi, rel=1e-12)
+    assert oracle.overlap_prim(1.0, o, (0, 0, 0), 1.0, o, (0, 0, 0)) == pytest.approx(1.9687012432, rel=1.5e-8)
+    h2 = mi.h2()
+    S, T, V = oracle.all_1e_ints(mi.build_basis(h2), [a.xyz for a in h2], [a.atno for a in h2])
+    assert S[0, 0] == pytest.approx(1.0, rel=1e-12) and S[1, 1] == pytest.approx(1.0, rel=1e-12)
+    assert S[0, 1] == pytest.approx(0.6647387449282997, rel=1.5e-8)
+    assert T[0, 0] == pytest.approx(0.76003188, rel=1.5e-8)
+    assert T[0, 1] == pytest.approx(0.24141861181119084, rel=1.5e-8)
