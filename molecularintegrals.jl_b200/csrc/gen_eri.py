@@ -353,15 +353,19 @@ void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, do
 }}
 """
     if len(entries) >= MIXED_MIN_VRR:
-        mixed_dispatch = ("    if (mixed) eri_queue_{t}<1><<<grid, 128, 0, s>>>(Q);\n"
-                          "    else eri_queue_{t}<0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
-        occ_dispatch = ("    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<1>, 128, 0);\n"
-                        "    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0>, 128, 0);").format(t=tag)
+        mixed_dispatch = ("    const bool jk = Q.jk.J != nullptr;\n"
+                          "    if (mixed) {{ if (jk) eri_queue_{t}<1, 1><<<grid, 128, 0, s>>>(Q); "
+                          "else eri_queue_{t}<1, 0><<<grid, 128, 0, s>>>(Q); }}\n"
+                          "    else if (jk) eri_queue_{t}<0, 1><<<grid, 128, 0, s>>>(Q);\n"
+                          "    else eri_queue_{t}<0, 0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
+        occ_dispatch = ("    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<1, 0>, 128, 0);\n"
+                        "    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0, 0>, 128, 0);").format(t=tag)
     else:
         mixed_dispatch = ("    (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)\n"
-                          "    eri_queue_{t}<0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
+                          "    if (Q.jk.J) eri_queue_{t}<0, 1><<<grid, 128, 0, s>>>(Q);\n"
+                          "    else eri_queue_{t}<0, 0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
         occ_dispatch = ("    (void)mixed;\n"
-                        "    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0>, 128, 0);").format(t=tag)
+                        "    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0, 0>, 128, 0);").format(t=tag)
     return f"""// Generated by gen_eri.py -- class ({'spdfg'[la]}{'spdfg'[lb]}|{'spdfg'[lc]}{'spdfg'[ld]}).  Do not edit.
 // VRR entries: {len(entries)}, contracted block: {nacc}, HRR lines: {len(hp.lines)}, outputs: {nout}.
 #include "../eri_common.cuh"
@@ -446,7 +450,9 @@ __device__ __noinline__ void jk_{tag}(const JKOut &jk, const int4 ib_, const int
 // Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
 // ket pairs of one molecule) from a shared counter until the chunk list, ordered by
 // decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
-template <int MIXED>
+// JK: digest into J and K (molints_plan_jk) instead of storing the packed integrals; a separate
+// instantiation, so that the store kernels carry none of the digestion code.
+template <int MIXED, int JK>
 __global__ void __launch_bounds__(128) eri_queue_{tag}(const EriQueue Q) {{
     const int lane = threadIdx.x & 31;
     for (;;) {{
@@ -467,7 +473,7 @@ __global__ void __launch_bounds__(128) eri_queue_{tag}(const EriQueue Q) {{
             if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_{tag}<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
             else quartet_{tag}<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
         }}
-        if (Q.jk.J) jk_{tag}(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+        if constexpr (JK) jk_{tag}(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
         else store_{tag}(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
                          p == q, res);
         }}

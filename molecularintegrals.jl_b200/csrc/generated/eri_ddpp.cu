@@ -2927,7 +2927,9 @@ __device__ __noinline__ void jk_ddpp(const JKOut &jk, const int4 ib_, const int4
 // Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
 // ket pairs of one molecule) from a shared counter until the chunk list, ordered by
 // decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
-template <int MIXED>
+// JK: digest into J and K (molints_plan_jk) instead of storing the packed integrals; a separate
+// instantiation, so that the store kernels carry none of the digestion code.
+template <int MIXED, int JK>
 __global__ void __launch_bounds__(128) eri_queue_ddpp(const EriQueue Q) {
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -2948,7 +2950,7 @@ __global__ void __launch_bounds__(128) eri_queue_ddpp(const EriQueue Q) {
             if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_ddpp<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
             else quartet_ddpp<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
         }
-        if (Q.jk.J) jk_ddpp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+        if constexpr (JK) jk_ddpp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
         else store_ddpp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
                          p == q, res);
         }
@@ -2957,15 +2959,17 @@ __global__ void __launch_bounds__(128) eri_queue_ddpp(const EriQueue Q) {
 
 void launch_eri_ddpp(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
-    if (mixed) eri_queue_ddpp<1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_ddpp<0><<<grid, 128, 0, s>>>(Q);
+    const bool jk = Q.jk.J != nullptr;
+    if (mixed) { if (jk) eri_queue_ddpp<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_ddpp<1, 0><<<grid, 128, 0, s>>>(Q); }
+    else if (jk) eri_queue_ddpp<0, 1><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_ddpp<0, 0><<<grid, 128, 0, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_ddpp(int mixed) {
     int n = 0;
-    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ddpp<1>, 128, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ddpp<0>, 128, 0);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ddpp<1, 0>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ddpp<0, 0>, 128, 0);
     return n;
 }
 

@@ -463,7 +463,9 @@ __device__ __noinline__ void jk_dpps(const JKOut &jk, const int4 ib_, const int4
 // Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
 // ket pairs of one molecule) from a shared counter until the chunk list, ordered by
 // decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
-template <int MIXED>
+// JK: digest into J and K (molints_plan_jk) instead of storing the packed integrals; a separate
+// instantiation, so that the store kernels carry none of the digestion code.
+template <int MIXED, int JK>
 __global__ void __launch_bounds__(128) eri_queue_dpps(const EriQueue Q) {
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(128) eri_queue_dpps(const EriQueue Q) {
             if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_dpps<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
             else quartet_dpps<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
         }
-        if (Q.jk.J) jk_dpps(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+        if constexpr (JK) jk_dpps(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
         else store_dpps(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
                          p == q, res);
         }
@@ -493,15 +495,17 @@ __global__ void __launch_bounds__(128) eri_queue_dpps(const EriQueue Q) {
 
 void launch_eri_dpps(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
-    if (mixed) eri_queue_dpps<1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_dpps<0><<<grid, 128, 0, s>>>(Q);
+    const bool jk = Q.jk.J != nullptr;
+    if (mixed) { if (jk) eri_queue_dpps<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_dpps<1, 0><<<grid, 128, 0, s>>>(Q); }
+    else if (jk) eri_queue_dpps<0, 1><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_dpps<0, 0><<<grid, 128, 0, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_dpps(int mixed) {
     int n = 0;
-    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpps<1>, 128, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpps<0>, 128, 0);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpps<1, 0>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpps<0, 0>, 128, 0);
     return n;
 }
 
