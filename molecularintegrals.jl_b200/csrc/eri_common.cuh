@@ -161,7 +161,9 @@ __device__ __forceinline__ long long tri_ll(long long i) { return i * (i + 1) / 
 
 // One unique integral v = (ij|kl) into J and K: every distinct index permutation (pq|rs) of
 // the 8-fold symmetry adds D_rs v to J_pq and D_qs v to K_pr (the Fock-build contraction that
-// make2JmK, src/ERI.jl:114-128, performs on the packed vector).
+// make2JmK, src/ERI.jl:114-128, performs on the packed vector).  J and K are symmetric, so only
+// the targets on or below the diagonal are accumulated (half the atomics); molints_plan_jk
+// mirrors the lower triangles afterwards.
 __device__ __forceinline__ void jk_add(const JKOut &jk, int i, int j, int k, int l, double v) {
     if (v == 0.0) return;
     if (i < j) { const int t = i; i = j; j = t; }
@@ -170,22 +172,16 @@ __device__ __forceinline__ void jk_add(const JKOut &jk, int i, int j, int k, int
     const bool dij = i != j, dkl = k != l;
     const bool dbk = (tri_ll(i) + j) != (tri_ll(k) + l);
     const double *__restrict__ D = jk.D;
-    // J: J_ij (and J_ji) += (1 + [k != l]) D_kl v; J_kl (and J_lk) += (1 + [i != j]) D_ij v
-    const double jkl = (dkl ? 2.0 : 1.0) * __ldg(&D[k * n + l]) * v;
-    atomicAdd(&jk.J[i * n + j], jkl);
-    if (dij) atomicAdd(&jk.J[j * n + i], jkl);
-    if (dbk) {
-        const double jij = (dij ? 2.0 : 1.0) * __ldg(&D[i * n + j]) * v;
-        atomicAdd(&jk.J[k * n + l], jij);
-        if (dkl) atomicAdd(&jk.J[l * n + k], jij);
-    }
-    // K: (pq|rs) -> K_pr += D_qs v over the distinct permutations
+    // J: J_ij += (1 + [k != l]) D_kl v (i >= j); J_kl += (1 + [i != j]) D_ij v (k >= l)
+    atomicAdd(&jk.J[i * n + j], (dkl ? 2.0 : 1.0) * __ldg(&D[k * n + l]) * v);
+    if (dbk) atomicAdd(&jk.J[k * n + l], (dij ? 2.0 : 1.0) * __ldg(&D[i * n + j]) * v);
+    // K: (pq|rs) -> K_pr += D_qs v over the distinct permutations, targets with p >= r only
     const int pq[2][2] = {{i, j}, {j, i}}, rs[2][2] = {{k, l}, {l, k}};
     for (int a = 0; a < (dij ? 2 : 1); ++a)
         for (int b = 0; b < (dkl ? 2 : 1); ++b) {
             const int p0 = pq[a][0], q0 = pq[a][1], r0 = rs[b][0], s0 = rs[b][1];
-            atomicAdd(&jk.K[p0 * n + r0], __ldg(&D[q0 * n + s0]) * v);
-            if (dbk) atomicAdd(&jk.K[r0 * n + p0], __ldg(&D[s0 * n + q0]) * v);
+            if (p0 >= r0) atomicAdd(&jk.K[p0 * n + r0], __ldg(&D[q0 * n + s0]) * v);
+            if (dbk && r0 >= p0) atomicAdd(&jk.K[r0 * n + p0], __ldg(&D[s0 * n + q0]) * v);
         }
 }
 

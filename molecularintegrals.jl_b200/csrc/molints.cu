@@ -212,6 +212,17 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
     geo[p] = make_double4(ABx, ABy, ABz, 0.0);
 }
 
+// Copy the lower triangles of J and K (the digestion accumulates only those) to the upper.
+__global__ void mirror_lower_kernel(double *__restrict__ J, double *__restrict__ K, int n) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const int r = (int)(t / n), c = (int)(t - (long long)r * n);
+    if (r < c) {
+        J[(long long)r * n + c] = J[(long long)c * n + r];
+        K[(long long)r * n + c] = K[(long long)c * n + r];
+    }
+}
+
 __global__ void boys_eval_kernel(BoysTab bt, int mmax, const double *__restrict__ T, long long n,
                                  double *__restrict__ out) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1229,7 +1240,14 @@ int molints_plan_jk(molints_plan *p, const double *D_device, double *J_device, d
     jk.J = J_device;
     jk.K = K_device;
     jk.n = (int)n;
-    return plan_enqueue(p, nullptr, true, jk);
+    const int rc = plan_enqueue(p, nullptr, true, jk);
+    if (rc) return rc;
+    if (n > 1) {
+        const long long nn = (long long)n * n;
+        mirror_lower_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, ctx->stream>>>(J_device, K_device, (int)n);
+        MI_CUDA(ctx, cudaGetLastError());
+    }
+    return MOLINTS_OK;
 }
 
 int molints_jk(molints_ctx *ctx, const molints_basis *b, const molints_options *opts,

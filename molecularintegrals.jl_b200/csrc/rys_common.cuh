@@ -196,22 +196,37 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
         }
         group_sync<C::G>(gid);
         if (slot < NSLOT) {
-            TT bacc[C::ACC];
+            if constexpr (F32) {
+                // the batch's products summed in FP32, then added to the FP64 accumulators
+                float bacc[C::ACC];
 #pragma unroll
-            for (int k = 0; k < C::ACC; ++k) bacc[k] = (TT)0;
-            for (int b = slot; b < nb; b += NSLOT) {
+                for (int k = 0; k < C::ACC; ++k) bacc[k] = 0.0f;
+                for (int b = slot; b < nb; b += NSLOT) {
 #pragma unroll 1
-                for (int r = 0; r < NR; ++r) {
-                    const TT *__restrict__ tx = tabs + (b * NR + r) * 3 * S;
+                    for (int r = 0; r < NR; ++r) {
+                        const TT *__restrict__ tx = tabs + (b * NR + r) * 3 * S;
 #pragma unroll
-                    for (int k = 0; k < C::ACC; ++k) {
-                        const uint32_t o = off[k];
-                        bacc[k] = fma(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], bacc[k]);
+                        for (int k = 0; k < C::ACC; ++k) {
+                            const uint32_t o = off[k];
+                            bacc[k] = fmaf(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], bacc[k]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < C::ACC; ++k) acc[k] += (double)bacc[k];
+            } else {
+                for (int b = slot; b < nb; b += NSLOT) {
+#pragma unroll 1
+                    for (int r = 0; r < NR; ++r) {
+                        const TT *__restrict__ tx = tabs + (b * NR + r) * 3 * S;
+#pragma unroll
+                        for (int k = 0; k < C::ACC; ++k) {
+                            const uint32_t o = off[k];
+                            acc[k] = fma(tx[o & 255u] * tx[S + ((o >> 8) & 255u)], tx[2 * S + (o >> 16)], acc[k]);
+                        }
                     }
                 }
             }
-#pragma unroll
-            for (int k = 0; k < C::ACC; ++k) acc[k] += (double)bacc[k];
         }
         group_sync<C::G>(gid);
     }
