@@ -176,6 +176,14 @@ def run_ours(args):
     flush = torch.zeros(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     from molints_b200 import autotune
     fp32_cut, tune_table = autotune.tune_fp32_cutoff(eng, sh)
+    # per class pair: HGP or Rys, and whether MIXED plans use the FP32 variant, timed on a
+    # sample of the batch and serving molecules (l <= 3) at the tuned cutoff
+    t_tune = time.perf_counter()
+    class_table, class_timings = autotune.tune_class_methods(
+        eng, [mi.config3_molecule(m) for m in range(1, 16, 2)] + [mi.config4_request(r) for r in range(4)],
+        fp32_cutoff=fp32_cut)
+    t_tune = time.perf_counter() - t_tune
+    eng.set_class_methods(class_table)
     eng.set_stream(stream.cuda_stream)
     plan64 = eng.plan(sh, precision=E.FP64)
     planmx = eng.plan(sh, precision=E.MIXED, fp32_cutoff=fp32_cut)
@@ -262,19 +270,16 @@ def run_ours(args):
     if "jk" in parts:
         jk = measure_jk(eng, stream, dev, sh, plan64, flush)
     if parts & {"batch", "serve"}:
-        # per-class HGP/Rys choice for the batch and serving workloads (l <= 3 molecules)
-        from molints_b200 import autotune as AT
-        t_tune = time.perf_counter()
-        class_table, class_timings = AT.tune_class_methods(
-            eng, [mi.config3_molecule(m) for m in range(1, 16, 2)] + [mi.config4_request(r) for r in range(4)])
-        t_tune = time.perf_counter() - t_tune
-        eng.set_class_methods(class_table)
+        AT = autotune
         # FP32 cutoff for l <= 3 molecules under the tuned methods (FP32 Rys tables and FP32
         # HGP VRR), on a serving-shaped molecule with f shells
         fp32_cut_l3, tune_l3 = AT.tune_fp32_cutoff(eng, mi.config4_request(6))
         eng.set_stream(stream.cuda_stream)
-        tuned = {"seconds": t_tune, "rys_classes": sorted(
-            t for t, (h, r) in class_timings.items() if class_table[AT._class_index(t)] == E.METHOD_RYS),
+        tuned = {"seconds": t_tune,
+                 "rys_classes": sorted(t for t in class_timings
+                                       if class_table[AT._class_index(t)] & 3 == E.METHOD_RYS),
+                 "fp32_classes": sorted(t for t in class_timings
+                                        if not class_table[AT._class_index(t)] & E.CLASS_NO_FP32),
             "fp32_cutoff_l3": fp32_cut_l3, "fp32_cutoff_l3_tuning": tune_l3}
         if "batch" in parts:
             batch = measure_batch(eng, stream, dev, fp32_cut_l3, rank, world)
@@ -286,6 +291,9 @@ def run_ours(args):
         r, dt, passes = cpu_reference_rate(sh, os.cpu_count() or 1, CPU_SAMPLE_SECONDS)
         cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                "sample": f"{passes} full passes over the workload in {dt:.1f} s (oracle HGP, OpenMP)"}
+        r1, dt1, passes1 = cpu_reference_rate(sh, 1, 3.0)
+        cpu["one_core"] = {"value": r1, "unit": UNIT, "cores": 1,
+                           "sample": f"{passes1} full pass(es) in {dt1:.1f} s"}
 
     if rank == 0:
         line = {

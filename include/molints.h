@@ -136,6 +136,9 @@ const char *molints_last_error(const molints_ctx *ctx);
  * MOLINTS_NUM_PAIR_CLASSES^2.  No reference counterpart (the reference picks its driver by
  * function name). */
 int molints_set_class_methods(molints_ctx *ctx, const int32_t *methods, int32_t n);
+/* Flag OR'ed into a molints_set_class_methods entry: MIXED plans run that class pair's FP64
+ * kernel (its FP32 variant measured no faster). */
+#define MOLINTS_CLASS_NO_FP32 4
 
 /* Set the CUDA stream (a cudaStream_t passed as void*) the context launches on.
  * NULL selects the context's own (non-blocking) stream; to launch on the legacy default

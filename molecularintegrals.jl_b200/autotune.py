@@ -56,12 +56,16 @@ def _class_index(tag: str):
     return E.PAIR_CLASSES.index(bra), E.PAIR_CLASSES.index(ket)
 
 
-def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95):
+def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95,
+                       fp32_cutoff: float | None = None):
     """Per class pair, HGP or Rys, whichever kernel is faster on `molecules` (one batch plan
     per method; each launch timed alone with CUDA events in profiling mode, best of
-    `repeats`).  Rys is taken only where it is faster by `margin`.  Returns (table, timings):
-    table[(x, y)] = METHOD_HGP or METHOD_RYS for engine.set_class_methods; timings maps the
-    class tag to (HGP ms, Rys ms).  Classes with an f shell have only Rys and are not listed."""
+    `repeats`).  Rys is taken only where it is faster by `margin`.  With `fp32_cutoff`, the
+    MIXED kernels of the chosen method are timed too, and classes whose FP32 variant is not
+    faster get the MOLINTS_CLASS_NO_FP32 flag (MIXED plans then run their FP64 kernel).
+    Returns (table, timings): table[(x, y)] for engine.set_class_methods; timings maps the class
+    tag to (HGP ms, Rys ms[, mixed ms of the chosen method]).  Classes with an f shell and no
+    HGP kernel have only Rys and are listed only for the FP32 decision."""
     import torch
     from . import engine as E
     mols = list(molecules)
@@ -71,24 +75,42 @@ def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95
     stream = torch.cuda.current_stream(dev)
     engine.set_stream(stream.cuda_stream)
     best = {}
+    runs = [(E.METHOD_HGP, E.FP64), (E.METHOD_RYS, E.FP64)]
+    if fp32_cutoff:
+        runs += [(E.METHOD_HGP, E.MIXED), (E.METHOD_RYS, E.MIXED)]
     try:
-        for meth, prefix in ((E.METHOD_HGP, "eri_"), (E.METHOD_RYS, "rys_")):
-            plan = engine.plan_batch(mols, method=meth, boys=E.BOYS_EXACT)
+        for meth, prec in runs:
+            plan = engine.plan_batch(mols, method=meth, boys=E.BOYS_EXACT, precision=prec,
+                                     fp32_cutoff=fp32_cutoff or 0.0)
             plan.set_profiling(True)
             for _ in range(repeats):
                 plan.execute(out.data_ptr())
                 for name, ms in plan.launch_times():
-                    if name.startswith(prefix):
-                        key = (name[4:], meth)
+                    if name.startswith("eri_") or name.startswith("rys_"):
+                        key = (name[4:], name[:3], prec)
                         best[key] = min(best.get(key, float("inf")), ms)
             plan.close()
     finally:
         engine.set_stream(None)
     table, timings = {}, {}
-    for (tag, meth), ms in best.items():
-        if meth != E.METHOD_HGP or (tag, E.METHOD_RYS) not in best:
-            continue
-        rys = best[(tag, E.METHOD_RYS)]
-        timings[tag] = (ms, rys)
-        table[_class_index(tag)] = E.METHOD_RYS if rys < margin * ms else E.METHOD_HGP
+    for tag in sorted({k[0] for k in best}):
+        h = best.get((tag, "eri", E.FP64))
+        r = best.get((tag, "rys", E.FP64))
+        if h is not None and r is not None:
+            meth = E.METHOD_RYS if r < margin * h else E.METHOD_HGP
+        elif h is not None:
+            meth = E.METHOD_HGP
+        else:
+            meth = E.METHOD_RYS
+        entry = meth
+        t = (h, r)
+        if fp32_cutoff:
+            fam = "eri" if meth == E.METHOD_HGP else "rys"
+            m64, mmx = best.get((tag, fam, E.FP64)), best.get((tag, fam, E.MIXED))
+            if m64 is not None and mmx is not None:
+                t = (h, r, mmx)
+                if not mmx < margin * m64:
+                    entry |= E.CLASS_NO_FP32
+        timings[tag] = t
+        table[_class_index(tag)] = entry
     return table, timings

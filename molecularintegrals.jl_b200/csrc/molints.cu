@@ -75,6 +75,7 @@ struct molints_plan {
     int q_len[kNumPairClasses][kNumPairClasses] = {};
     double class_cost[kNumPairClasses][kNumPairClasses] = {};  // kept primitive quartets
     int method[kNumPairClasses][kNumPairClasses] = {};  // MOLINTS_METHOD_HGP or _RYS
+    int fp32[kNumPairClasses][kNumPairClasses] = {};    // MIXED and this class's FP32 variant used
     // host copies (final, screened order)
     std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
     std::vector<int> pair_mol;         // canonical pair -> molecule
@@ -455,7 +456,7 @@ int molints_set_class_methods(molints_ctx *ctx, const int32_t *methods, int32_t 
         return fail(ctx, MOLINTS_ERR_INVALID, "set_class_methods: n must be MOLINTS_NUM_PAIR_CLASSES^2");
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
-            const int32_t m = methods[x * kNumPairClasses + y];
+            const int32_t m = methods[x * kNumPairClasses + y] & ~MOLINTS_CLASS_NO_FP32;
             if (m != MOLINTS_METHOD_AUTO && m != MOLINTS_METHOD_HGP && m != MOLINTS_METHOD_RYS)
                 return fail(ctx, MOLINTS_ERR_INVALID, "set_class_methods: unknown method");
         }
@@ -694,11 +695,14 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     // method per class pair: Rys where no HGP kernel exists (an f shell), else the request
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
+            const int32_t entry = ctx->class_method[x][y];
             int m = opts.method;
-            if (m == MOLINTS_METHOD_AUTO) m = ctx->class_method[x][y];
+            if (m == MOLINTS_METHOD_AUTO) m = entry & ~MOLINTS_CLASS_NO_FP32;
             if (m == MOLINTS_METHOD_AUTO) m = MOLINTS_METHOD_HGP;
             if (!kEriLaunchers[x][y]) m = MOLINTS_METHOD_RYS;
             p->method[x][y] = m;
+            // MIXED plans run this class's FP32 variant unless the table says it is no faster
+            p->fp32[x][y] = opts.precision == MOLINTS_MIXED && !(entry & MOLINTS_CLASS_NO_FP32);
         }
 
     // Normalised coefficients: raw coef x (2a/pi)^(3/4) (4a)^(L/2) x CGBF norm; the component
@@ -1119,7 +1123,6 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     }
     PairTab P{p->info, p->geo, p->pp, p->bnd};
     BoysTab B = boys_of(ctx, p->opts.boys);
-    const int mixed = p->opts.precision == MOLINTS_MIXED ? 1 : 0;
     // Class-pair queues, largest estimated work first, spread over the side streams so that
     // small classes fill the SMs next to large ones.
     struct Job { double cost; int x, y; };
@@ -1136,6 +1139,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         const int x = jobs[k].x, y = jobs[k].y;
         cudaStream_t st = nside ? ctx->side[k % nside] : s;
         const bool rys = p->method[x][y] == MOLINTS_METHOD_RYS;
+        const int mixed = p->fp32[x][y];
         int &occ = ctx->occupancy[x][y][(rys ? 2 : 0) + mixed];
         if (occ == 0) occ = std::max(1, rys ? kRysOccupancy[x][y](mixed) : kEriOccupancy[x][y](mixed));
         EriQueue Q{};
@@ -1173,10 +1177,10 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
 // before any graph capture).
 static void plan_occupancy(molints_plan *p) {
     molints_ctx *ctx = p->ctx;
-    const int mixed = p->opts.precision == MOLINTS_MIXED ? 1 : 0;
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
             if (p->q_len[x][y] == 0) continue;
+            const int mixed = p->fp32[x][y];
             const bool rys = p->method[x][y] == MOLINTS_METHOD_RYS;
             int &occ = ctx->occupancy[x][y][(rys ? 2 : 0) + mixed];
             if (occ == 0) occ = std::max(1, rys ? kRysOccupancy[x][y](mixed) : kEriOccupancy[x][y](mixed));

@@ -24,6 +24,7 @@ LIB_PATH = HERE / "libmolints_cuda.so"
 FP64, MIXED = 0, 1
 BOYS_REFERENCE, BOYS_EXACT = 0, 1
 METHOD_AUTO, METHOD_HGP, METHOD_RYS = 0, 1, 2
+CLASS_NO_FP32 = 4   # flag in a set_class_methods entry: MIXED plans run the FP64 kernel
 LMAX = 3
 # shell-pair classes in the engine's order (la+lb, then la): index -> (la, lb)
 PAIR_CLASSES = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (3, 0), (2, 2), (3, 1), (2, 3), (3, 2), (3, 3)]

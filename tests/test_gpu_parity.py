@@ -400,9 +400,9 @@ def test_class_method_tuner(eng, oracle):
     basis's FP64 floor) of the long-double oracle."""
     from molints_b200 import autotune, engine
     mols = [mi.config2(), _f_molecule(14)]
-    table, timings = autotune.tune_class_methods(eng, mols, repeats=2)
-    assert timings and set(table.values()) <= {engine.METHOD_HGP, engine.METHOD_RYS}
-    assert all(h > 0 and r > 0 for h, r in timings.values())
+    table, timings = autotune.tune_class_methods(eng, mols, repeats=2, fp32_cutoff=1e-3)
+    assert timings and {v & 3 for v in table.values()} <= {engine.METHOD_HGP, engine.METHOD_RYS}
+    assert all(t is None or t > 0 for ts in timings.values() for t in ts)
     eng.set_class_methods(table)
     try:
         for sh in mols:
