@@ -272,8 +272,10 @@ def run_ours(args):
     if parts & {"batch", "serve"}:
         AT = autotune
         # FP32 cutoff for l <= 3 molecules under the tuned methods (FP32 Rys tables and FP32
-        # HGP VRR), on a serving-shaped molecule with f shells
-        fp32_cut_l3, tune_l3 = AT.tune_fp32_cutoff(eng, mi.config4_request(6))
+        # HGP VRR): the smallest of the cutoffs tuned on three serving-shaped molecules
+        tunes = [AT.tune_fp32_cutoff(eng, mi.config4_request(r)) for r in (6, 1, 7)]
+        fp32_cut_l3 = min(c for c, _ in tunes)
+        tune_l3 = [t for _, t in tunes]
         eng.set_stream(stream.cuda_stream)
         tuned = {"seconds": t_tune,
                  "rys_classes": sorted(t for t in class_timings
