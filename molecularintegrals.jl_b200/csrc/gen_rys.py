@@ -42,6 +42,8 @@ NMONO = 20           # monomials AB^(px,py,pz), px+py+pz <= 3
 # thread get an FP32 variant for MIXED quartets (stage-2 products summed in FP32 per batch).
 MIXED_MIN_NBLK = 32
 MIXED_MAX_ACC = 24
+COL_MIN_NC = 16
+COL_MAX_NA = 48
 
 
 def shell_components(l):
@@ -145,7 +147,13 @@ def class_tables(X, Y):
     na, nc = len(rows), len(cols)
     nblk = na * nc
     nab, ncd = ncart(la) * ncart(lb), ncart(lc) * ncart(ld)
-    if nblk <= 128:
+    # column mode: one stage-2 thread per block column holds that column's three 2-D table
+    # columns and all NA row accumulators in registers (3(E+1) shared loads per root instead
+    # of 3 per entry); for blocks with at least COL_MIN_NC columns and at most COL_MAX_NA rows
+    col = nc >= COL_MIN_NC and na <= COL_MAX_NA
+    if col:
+        G = 32 * ((nc + 31) // 32)
+    elif nblk <= 128:
         G = 32
     elif nblk <= 1024:
         G = 64
@@ -157,14 +165,14 @@ def class_tables(X, Y):
     npb = max(1, min(G // nr, hrr_room // (3 * nr * S)))
     # stage-2 slots: a small block is accumulated by NSLOT threads per entry, each taking every
     # NSLOT-th quartet of a batch, and the slots are summed after the primitive loop
-    nslot = max(1, min(npb, G // nblk)) if 2 * nblk <= G else 1
-    acc = 1 if nslot > 1 else (nblk + G - 1) // G
+    nslot = max(1, min(npb, G // nblk)) if (2 * nblk <= G and not col) else 1
+    acc = 1 if (nslot > 1 or col) else (nblk + G - 1) // G
     smem_group = 2 * NMONO + max(npb * nr * 3 * S, nblk + nab * nc, nslot * nblk)
-    mixed = nblk >= MIXED_MIN_NBLK and acc <= MIXED_MAX_ACC
+    mixed = nblk >= MIXED_MIN_NBLK and (acc <= MIXED_MAX_ACC or col)
     return dict(la=la, lb=lb, lc=lc, ld=ld, e=e, f=f, nr=nr, rows=rows, cols=cols, S=S,
                 blk=blk, bra=bra, ket=ket, norm_ab=norm_ab, norm_cd=norm_cd, na=na, nc=nc,
                 nblk=nblk, nab=nab, ncd=ncd, G=G, npb=npb, nslot=nslot, acc=acc,
-                smem_group=smem_group, mixed=mixed)
+                smem_group=smem_group, mixed=mixed, col=col)
 
 
 def _flat_terms(lists):
@@ -220,9 +228,24 @@ void launch_rys_bound_{tag}(const PairTab &P, const RysTab &R, int p0, int np, d
                           f"    rys_queue_{tag}<0><<<grid, 128, {smem_block}, s>>>(Q, R);")
         occ_dispatch = (f"    (void)mixed;\n"
                         f"    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_{tag}<0>, 128, {smem_block});")
+    if t["col"]:
+        F1 = t["f"] + 1
+        lines = []
+        for ia, a in enumerate(t["rows"]):
+            lines.append(f"        acc[{ia}] = fma(x[{a[0]}] * y[{a[1]}], z[{a[2]}], acc[{ia}]);")
+        col_code = ("    // stage 2, column mode: acc[row] += x[ax] y[ay] z[az] for the column's table columns\n"
+                    "    template <typename T, typename A>\n"
+                    "    __device__ __forceinline__ static void col_update(const T *x, const T *y, const T *z, A *acc) {\n"
+                    + "\n".join(lines) + "\n    }")
+        colpow = ", ".join(str(c[0] | (c[1] << 4) | (c[2] << 8)) for c in t["cols"])
+        col_code += f"\n    static constexpr int NCOLS = {t['nc']};"
+        col_tab = f"\n// column components cx | cy << 4 | cz << 8\n__device__ const uint16_t kCol_{tag}[{t['nc']}] = {{ {colpow} }};\n"
+    else:
+        col_code = "    template <typename T, typename A>\n    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}"
+        col_tab = ""
     return f"""// Generated by gen_rys.py -- Rys class ({tag[0]}{tag[1]}|{tag[2]}{tag[3]}).  Do not edit.
 // roots {t['nr']}, block {t['na']} x {t['nc']}, outputs {t['nab']} x {t['ncd']}, group {t['G']} threads,
-// {t['npb']} primitive quartets per batch, {t['nslot']} slot(s), {t['acc']} accumulators per thread, {smem_block} B shared per block.
+// {t['npb']} primitive quartets per batch, {t['nslot']} slot(s), {t['acc']} accumulators per thread, {smem_block} B shared per block{", column mode" if t["col"] else ""}.
 #include "../rys_common.cuh"
 
 namespace molints {{
@@ -236,6 +259,8 @@ struct C_{tag} {{
     static constexpr int G = {t['G']}, NPB = {t['npb']}, NSLOT = {t['nslot']}, ACC = {t['acc']};
     static constexpr int S = {t['S']};
     static constexpr int SMEM_GROUP = {t['smem_group']};
+    static constexpr bool COL = {'true' if t['col'] else 'false'};
+{col_code}
 }};
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -262,9 +287,10 @@ __device__ const double kNormCD_{tag}[{len(t['norm_cd'])}] = {{
 {_arr(t['norm_cd'], repr, 4)}
 }};
 
+{col_tab}
 __device__ __forceinline__ RysClassTabs tabs_{tag}() {{
     return RysClassTabs{{kBlk_{tag}, kBraOff_{tag}, kBraTerm_{tag}, kKetOff_{tag}, kKetTerm_{tag},
-                        kNormAB_{tag}, kNormCD_{tag}}};
+                        kNormAB_{tag}, kNormCD_{tag}, {"kCol_" + tag if t["col"] else "nullptr"}}};
 }}
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_ddds {
     static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 3;
     static constexpr int S = 15;
     static constexpr int SMEM_GROUP = 2920;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -77,9 +80,10 @@ __device__ const double kNormCD_ddds[6] = {
     1.0, 0.5773502691896258,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_ddds() {
     return RysClassTabs{kBlk_ddds, kBraOff_ddds, kBraTerm_ddds, kKetOff_ddds, kKetTerm_ddds,
-                        kNormAB_ddds, kNormCD_ddds};
+                        kNormAB_ddds, kNormCD_ddds, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_ddpp {
     static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 5;
     static constexpr int S = 15;
     static constexpr int SMEM_GROUP = 2920;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -87,9 +90,10 @@ __device__ const double kNormCD_ddpp[9] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_ddpp() {
     return RysClassTabs{kBlk_ddpp, kBraOff_ddpp, kBraTerm_ddpp, kKetOff_ddpp, kKetTerm_ddpp,
-                        kNormAB_ddpp, kNormCD_ddpp};
+                        kNormAB_ddpp, kNormCD_ddpp, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_ddps {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 3;
     static constexpr int S = 10;
     static constexpr int SMEM_GROUP = 940;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -68,9 +71,10 @@ __device__ const double kNormCD_ddps[3] = {
     1.0, 1.0, 1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_ddps() {
     return RysClassTabs{kBlk_ddps, kBraOff_ddps, kBraTerm_ddps, kKetOff_ddps, kKetTerm_ddps,
-                        kNormAB_ddps, kNormCD_ddps};
+                        kNormAB_ddps, kNormCD_ddps, nullptr};
 }
 
 template <int MIXED>

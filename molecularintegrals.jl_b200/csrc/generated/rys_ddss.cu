@@ -14,6 +14,9 @@ struct C_ddss {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 1;
     static constexpr int S = 5;
     static constexpr int SMEM_GROUP = 490;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -63,9 +66,10 @@ __device__ const double kNormCD_ddss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_ddss() {
     return RysClassTabs{kBlk_ddss, kBraOff_ddss, kBraTerm_ddss, kKetOff_ddss, kKetTerm_ddss,
-                        kNormAB_ddss, kNormCD_ddss};
+                        kNormAB_ddss, kNormCD_ddss, nullptr};
 }
 
 template <int MIXED>

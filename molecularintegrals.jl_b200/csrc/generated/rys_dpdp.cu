@@ -1,6 +1,6 @@
 // Generated by gen_rys.py -- Rys class (dp|dp).  Do not edit.
-// roots 4, block 16 x 16, outputs 18 x 18, group 64 threads,
-// 16 primitive quartets per batch, 1 slot(s), 4 accumulators per thread, 49792 B shared per block.
+// roots 4, block 16 x 16, outputs 18 x 18, group 32 threads,
+// 8 primitive quartets per batch, 1 slot(s), 1 accumulators per thread, 50432 B shared per block, column mode.
 #include "../rys_common.cuh"
 
 namespace molints {
@@ -11,9 +11,31 @@ struct C_dpdp {
     static constexpr int NA = 16, NC = 16, NBLK = 256;
     static constexpr int NB = 3, ND = 3;
     static constexpr int NAB = 18, NCD = 18;
-    static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 4;
+    static constexpr int G = 32, NPB = 8, NSLOT = 1, ACC = 1;
     static constexpr int S = 16;
-    static constexpr int SMEM_GROUP = 3112;
+    static constexpr int SMEM_GROUP = 1576;
+    static constexpr bool COL = true;
+    // stage 2, column mode: acc[row] += x[ax] y[ay] z[az] for the column's table columns
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *x, const T *y, const T *z, A *acc) {
+        acc[0] = fma(x[2] * y[0], z[0], acc[0]);
+        acc[1] = fma(x[1] * y[1], z[0], acc[1]);
+        acc[2] = fma(x[1] * y[0], z[1], acc[2]);
+        acc[3] = fma(x[0] * y[2], z[0], acc[3]);
+        acc[4] = fma(x[0] * y[1], z[1], acc[4]);
+        acc[5] = fma(x[0] * y[0], z[2], acc[5]);
+        acc[6] = fma(x[3] * y[0], z[0], acc[6]);
+        acc[7] = fma(x[2] * y[1], z[0], acc[7]);
+        acc[8] = fma(x[2] * y[0], z[1], acc[8]);
+        acc[9] = fma(x[1] * y[2], z[0], acc[9]);
+        acc[10] = fma(x[1] * y[0], z[2], acc[10]);
+        acc[11] = fma(x[1] * y[1], z[1], acc[11]);
+        acc[12] = fma(x[0] * y[3], z[0], acc[12]);
+        acc[13] = fma(x[0] * y[2], z[1], acc[13]);
+        acc[14] = fma(x[0] * y[1], z[2], acc[14]);
+        acc[15] = fma(x[0] * y[0], z[3], acc[15]);
+    }
+    static constexpr int NCOLS = 16;
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -75,9 +97,13 @@ __device__ const double kNormCD_dpdp[18] = {
     0.5773502691896258, 0.5773502691896258,
 };
 
+
+// column components cx | cy << 4 | cz << 8
+__device__ const uint16_t kCol_dpdp[16] = { 2, 17, 257, 32, 272, 512, 3, 18, 258, 33, 513, 273, 48, 288, 528, 768 };
+
 __device__ __forceinline__ RysClassTabs tabs_dpdp() {
     return RysClassTabs{kBlk_dpdp, kBraOff_dpdp, kBraTerm_dpdp, kKetOff_dpdp, kKetTerm_dpdp,
-                        kNormAB_dpdp, kNormCD_dpdp};
+                        kNormAB_dpdp, kNormCD_dpdp, kCol_dpdp};
 }
 
 template <int MIXED>
@@ -95,9 +121,9 @@ static void rys_prepare_dpdp() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(rys_queue_dpdp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
-        cudaFuncSetAttribute(rys_queue_dpdp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
-        cudaFuncSetAttribute(rys_bound_kernel_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 49792);
+        cudaFuncSetAttribute(rys_queue_dpdp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
+        cudaFuncSetAttribute(rys_queue_dpdp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
+        cudaFuncSetAttribute(rys_bound_kernel_dpdp, cudaFuncAttributeMaxDynamicSharedMemorySize, 50432);
         done[dev] = true;
     }
 }
@@ -108,16 +134,16 @@ void launch_rys_dpdp(const EriQueue &Q, const RysTab &R, int mixed, int grid_max
     rys_prepare_dpdp();
     constexpr int ng = 128 / C_dpdp::G;
     const int grid = (int)std::min<long long>(grid_max, ((long long)Q.nchunks + ng - 1) / ng);
-    if (mixed) rys_queue_dpdp<1><<<grid, 128, 49792, s>>>(Q, R);
-    else rys_queue_dpdp<0><<<grid, 128, 49792, s>>>(Q, R);
+    if (mixed) rys_queue_dpdp<1><<<grid, 128, 50432, s>>>(Q, R);
+    else rys_queue_dpdp<0><<<grid, 128, 50432, s>>>(Q, R);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_rys_dpdp(int mixed) {
     rys_prepare_dpdp();
     int n = 0;
-    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp<1>, 128, 49792);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp<0>, 128, 49792);
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp<1>, 128, 50432);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rys_queue_dpdp<0>, 128, 50432);
     return n;
 }
 
@@ -126,7 +152,7 @@ void launch_rys_bound_dpdp(const PairTab &P, const RysTab &R, int p0, int np, do
     if (np <= 0) return;
     rys_prepare_dpdp();
     constexpr int ng = 128 / C_dpdp::G;
-    rys_bound_kernel_dpdp<<<(np + ng - 1) / ng, 128, 49792, s>>>(P, R, p0, np, pbound, qout, full);
+    rys_bound_kernel_dpdp<<<(np + ng - 1) / ng, 128, 50432, s>>>(P, R, p0, np, pbound, qout, full);
 }
 
 }  // namespace molints

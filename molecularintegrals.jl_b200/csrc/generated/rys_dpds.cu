@@ -14,6 +14,9 @@ struct C_dpds {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 3;
     static constexpr int S = 12;
     static constexpr int SMEM_GROUP = 1120;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -55,9 +58,10 @@ __device__ const double kNormCD_dpds[6] = {
     1.0, 0.5773502691896258,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dpds() {
     return RysClassTabs{kBlk_dpds, kBraOff_dpds, kBraTerm_dpds, kKetOff_dpds, kKetTerm_dpds,
-                        kNormAB_dpds, kNormCD_dpds};
+                        kNormAB_dpds, kNormCD_dpds, nullptr};
 }
 
 template <int MIXED>

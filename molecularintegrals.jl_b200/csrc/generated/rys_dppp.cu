@@ -14,6 +14,9 @@ struct C_dppp {
     static constexpr int G = 64, NPB = 21, NSLOT = 1, ACC = 3;
     static constexpr int S = 12;
     static constexpr int SMEM_GROUP = 2308;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -61,9 +64,10 @@ __device__ const double kNormCD_dppp[9] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dppp() {
     return RysClassTabs{kBlk_dppp, kBraOff_dppp, kBraTerm_dppp, kKetOff_dppp, kKetTerm_dppp,
-                        kNormAB_dppp, kNormCD_dppp};
+                        kNormAB_dppp, kNormCD_dppp, nullptr};
 }
 
 template <int MIXED>

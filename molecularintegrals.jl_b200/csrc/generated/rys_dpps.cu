@@ -14,6 +14,9 @@ struct C_dpps {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 8;
     static constexpr int SMEM_GROUP = 760;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -50,9 +53,10 @@ __device__ const double kNormCD_dpps[3] = {
     1.0, 1.0, 1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dpps() {
     return RysClassTabs{kBlk_dpps, kBraOff_dpps, kBraTerm_dpps, kKetOff_dpps, kKetTerm_dpps,
-                        kNormAB_dpps, kNormCD_dpps};
+                        kNormAB_dpps, kNormCD_dpps, nullptr};
 }
 
 template <int MIXED>

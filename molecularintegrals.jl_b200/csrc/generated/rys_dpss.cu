@@ -14,6 +14,9 @@ struct C_dpss {
     static constexpr int G = 32, NPB = 16, NSLOT = 2, ACC = 1;
     static constexpr int S = 4;
     static constexpr int SMEM_GROUP = 424;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -48,9 +51,10 @@ __device__ const double kNormCD_dpss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dpss() {
     return RysClassTabs{kBlk_dpss, kBraOff_dpss, kBraTerm_dpss, kKetOff_dpss, kKetTerm_dpss,
-                        kNormAB_dpss, kNormCD_dpss};
+                        kNormAB_dpss, kNormCD_dpss, nullptr};
 }
 
 template <int MIXED>

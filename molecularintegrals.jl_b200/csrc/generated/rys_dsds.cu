@@ -14,6 +14,9 @@ struct C_dsds {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 9;
     static constexpr int SMEM_GROUP = 850;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -44,9 +47,10 @@ __device__ const double kNormCD_dsds[6] = {
     1.0, 0.5773502691896258,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dsds() {
     return RysClassTabs{kBlk_dsds, kBraOff_dsds, kBraTerm_dsds, kKetOff_dsds, kKetTerm_dsds,
-                        kNormAB_dsds, kNormCD_dsds};
+                        kNormAB_dsds, kNormCD_dsds, nullptr};
 }
 
 template <int MIXED>

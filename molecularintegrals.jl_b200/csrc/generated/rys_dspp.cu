@@ -14,6 +14,9 @@ struct C_dspp {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 9;
     static constexpr int SMEM_GROUP = 850;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -48,9 +51,10 @@ __device__ const double kNormCD_dspp[9] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dspp() {
     return RysClassTabs{kBlk_dspp, kBraOff_dspp, kBraTerm_dspp, kKetOff_dspp, kKetTerm_dspp,
-                        kNormAB_dspp, kNormCD_dspp};
+                        kNormAB_dspp, kNormCD_dspp, nullptr};
 }
 
 template <int MIXED>

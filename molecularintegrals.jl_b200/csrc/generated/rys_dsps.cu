@@ -14,6 +14,9 @@ struct C_dsps {
     static constexpr int G = 32, NPB = 16, NSLOT = 1, ACC = 1;
     static constexpr int S = 6;
     static constexpr int SMEM_GROUP = 616;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -42,9 +45,10 @@ __device__ const double kNormCD_dsps[3] = {
     1.0, 1.0, 1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dsps() {
     return RysClassTabs{kBlk_dsps, kBraOff_dsps, kBraTerm_dsps, kKetOff_dsps, kKetTerm_dsps,
-                        kNormAB_dsps, kNormCD_dsps};
+                        kNormAB_dsps, kNormCD_dsps, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_dsss {
     static constexpr int G = 32, NPB = 16, NSLOT = 5, ACC = 1;
     static constexpr int S = 3;
     static constexpr int SMEM_GROUP = 328;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -41,9 +44,10 @@ __device__ const double kNormCD_dsss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_dsss() {
     return RysClassTabs{kBlk_dsss, kBraOff_dsss, kBraTerm_dsss, kKetOff_dsss, kKetTerm_dsss,
-                        kNormAB_dsss, kNormCD_dsss};
+                        kNormAB_dsss, kNormCD_dsss, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fdps {
     static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 3;
     static constexpr int S = 12;
     static constexpr int SMEM_GROUP = 2344;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -87,9 +90,10 @@ __device__ const double kNormCD_fdps[3] = {
     1.0, 1.0, 1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fdps() {
     return RysClassTabs{kBlk_fdps, kBraOff_fdps, kBraTerm_fdps, kKetOff_fdps, kKetTerm_fdps,
-                        kNormAB_fdps, kNormCD_fdps};
+                        kNormAB_fdps, kNormCD_fdps, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fdss {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 6;
     static constexpr int SMEM_GROUP = 580;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -79,9 +82,10 @@ __device__ const double kNormCD_fdss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fdss() {
     return RysClassTabs{kBlk_fdss, kBraOff_fdss, kBraTerm_fdss, kKetOff_fdss, kKetTerm_fdss,
-                        kNormAB_fdss, kNormCD_fdss};
+                        kNormAB_fdss, kNormCD_fdss, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fpfs {
     static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 4;
     static constexpr int S = 20;
     static constexpr int SMEM_GROUP = 3880;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -75,9 +78,10 @@ __device__ const double kNormCD_fpfs[10] = {
     0.5773502691896258, 0.2581988897471611,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fpfs() {
     return RysClassTabs{kBlk_fpfs, kBraOff_fpfs, kBraTerm_fpfs, kKetOff_fpfs, kKetTerm_fpfs,
-                        kNormAB_fpfs, kNormCD_fpfs};
+                        kNormAB_fpfs, kNormCD_fpfs, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fppp {
     static constexpr int G = 64, NPB = 16, NSLOT = 1, ACC = 4;
     static constexpr int S = 15;
     static constexpr int SMEM_GROUP = 2920;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -74,9 +77,10 @@ __device__ const double kNormCD_fppp[9] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fppp() {
     return RysClassTabs{kBlk_fppp, kBraOff_fppp, kBraTerm_fppp, kKetOff_fppp, kKetTerm_fppp,
-                        kNormAB_fppp, kNormCD_fppp};
+                        kNormAB_fppp, kNormCD_fppp, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fpps {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 3;
     static constexpr int S = 10;
     static constexpr int SMEM_GROUP = 940;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -59,9 +62,10 @@ __device__ const double kNormCD_fpps[3] = {
     1.0, 1.0, 1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fpps() {
     return RysClassTabs{kBlk_fpps, kBraOff_fpps, kBraTerm_fpps, kKetOff_fpps, kKetTerm_fpps,
-                        kNormAB_fpps, kNormCD_fpps};
+                        kNormAB_fpps, kNormCD_fpps, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fpss {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 1;
     static constexpr int S = 5;
     static constexpr int SMEM_GROUP = 490;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -55,9 +58,10 @@ __device__ const double kNormCD_fpss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fpss() {
     return RysClassTabs{kBlk_fpss, kBraOff_fpss, kBraTerm_fpss, kKetOff_fpss, kKetTerm_fpss,
-                        kNormAB_fpss, kNormCD_fpss};
+                        kNormAB_fpss, kNormCD_fpss, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fsds {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 2;
     static constexpr int S = 12;
     static constexpr int SMEM_GROUP = 1120;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -47,9 +50,10 @@ __device__ const double kNormCD_fsds[6] = {
     1.0, 0.5773502691896258,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fsds() {
     return RysClassTabs{kBlk_fsds, kBraOff_fsds, kBraTerm_fsds, kKetOff_fsds, kKetTerm_fsds,
-                        kNormAB_fsds, kNormCD_fsds};
+                        kNormAB_fsds, kNormCD_fsds, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fsfs {
     static constexpr int G = 32, NPB = 8, NSLOT = 1, ACC = 4;
     static constexpr int S = 16;
     static constexpr int SMEM_GROUP = 1576;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -52,9 +55,10 @@ __device__ const double kNormCD_fsfs[10] = {
     0.5773502691896258, 0.2581988897471611,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fsfs() {
     return RysClassTabs{kBlk_fsfs, kBraOff_fsfs, kBraTerm_fsfs, kKetOff_fsfs, kKetTerm_fsfs,
-                        kNormAB_fsfs, kNormCD_fsfs};
+                        kNormAB_fsfs, kNormCD_fsfs, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fspp {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 3;
     static constexpr int S = 12;
     static constexpr int SMEM_GROUP = 1120;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -52,9 +55,10 @@ __device__ const double kNormCD_fspp[9] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fspp() {
     return RysClassTabs{kBlk_fspp, kBraOff_fspp, kBraTerm_fspp, kKetOff_fspp, kKetTerm_fspp,
-                        kNormAB_fspp, kNormCD_fspp};
+                        kNormAB_fspp, kNormCD_fspp, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fsps {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 1;
     static constexpr int S = 8;
     static constexpr int SMEM_GROUP = 760;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -44,9 +47,10 @@ __device__ const double kNormCD_fsps[3] = {
     1.0, 1.0, 1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fsps() {
     return RysClassTabs{kBlk_fsps, kBraOff_fsps, kBraTerm_fsps, kKetOff_fsps, kKetTerm_fsps,
-                        kNormAB_fsps, kNormCD_fsps};
+                        kNormAB_fsps, kNormCD_fsps, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_fsss {
     static constexpr int G = 32, NPB = 16, NSLOT = 3, ACC = 1;
     static constexpr int S = 4;
     static constexpr int SMEM_GROUP = 424;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -42,9 +45,10 @@ __device__ const double kNormCD_fsss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_fsss() {
     return RysClassTabs{kBlk_fsss, kBraOff_fsss, kBraTerm_fsss, kKetOff_fsss, kKetTerm_fsss,
-                        kNormAB_fsss, kNormCD_fsss};
+                        kNormAB_fsss, kNormCD_fsss, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_pppp {
     static constexpr int G = 32, NPB = 10, NSLOT = 1, ACC = 3;
     static constexpr int S = 9;
     static constexpr int SMEM_GROUP = 850;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -52,9 +55,10 @@ __device__ const double kNormCD_pppp[9] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_pppp() {
     return RysClassTabs{kBlk_pppp, kBraOff_pppp, kBraTerm_pppp, kKetOff_pppp, kKetTerm_pppp,
-                        kNormAB_pppp, kNormCD_pppp};
+                        kNormAB_pppp, kNormCD_pppp, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_ppss {
     static constexpr int G = 32, NPB = 16, NSLOT = 3, ACC = 1;
     static constexpr int S = 3;
     static constexpr int SMEM_GROUP = 328;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -43,9 +46,10 @@ __device__ const double kNormCD_ppss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_ppss() {
     return RysClassTabs{kBlk_ppss, kBraOff_ppss, kBraTerm_ppss, kKetOff_ppss, kKetTerm_ppss,
-                        kNormAB_ppss, kNormCD_ppss};
+                        kNormAB_ppss, kNormCD_ppss, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_psps {
     static constexpr int G = 32, NPB = 16, NSLOT = 3, ACC = 1;
     static constexpr int S = 4;
     static constexpr int SMEM_GROUP = 424;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -40,9 +43,10 @@ __device__ const double kNormCD_psps[3] = {
     1.0, 1.0, 1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_psps() {
     return RysClassTabs{kBlk_psps, kBraOff_psps, kBraTerm_psps, kKetOff_psps, kKetTerm_psps,
-                        kNormAB_psps, kNormCD_psps};
+                        kNormAB_psps, kNormCD_psps, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_psss {
     static constexpr int G = 32, NPB = 32, NSLOT = 10, ACC = 1;
     static constexpr int S = 2;
     static constexpr int SMEM_GROUP = 232;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -40,9 +43,10 @@ __device__ const double kNormCD_psss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_psss() {
     return RysClassTabs{kBlk_psss, kBraOff_psss, kBraTerm_psss, kKetOff_psss, kKetTerm_psss,
-                        kNormAB_psss, kNormCD_psss};
+                        kNormAB_psss, kNormCD_psss, nullptr};
 }
 
 template <int MIXED>

@@ -14,6 +14,9 @@ struct C_ssss {
     static constexpr int G = 32, NPB = 32, NSLOT = 32, ACC = 1;
     static constexpr int S = 1;
     static constexpr int SMEM_GROUP = 136;
+    static constexpr bool COL = false;
+    template <typename T, typename A>
+    __device__ __forceinline__ static void col_update(const T *, const T *, const T *, A *) {}
 };
 
 // block entry (row, col) -> 2-D table offsets x | y << 8 | z << 16
@@ -40,9 +43,10 @@ __device__ const double kNormCD_ssss[1] = {
     1.0,
 };
 
+
 __device__ __forceinline__ RysClassTabs tabs_ssss() {
     return RysClassTabs{kBlk_ssss, kBraOff_ssss, kBraTerm_ssss, kKetOff_ssss, kKetTerm_ssss,
-                        kNormAB_ssss, kNormCD_ssss};
+                        kNormAB_ssss, kNormCD_ssss, nullptr};
 }
 
 template <int MIXED>

@@ -34,6 +34,7 @@ struct RysClassTabs {
     const uint32_t *ket_term;  // block column | monomial << 8 | binomial << 16
     const double *norm_ab;     // [NAB] component norms of a and b
     const double *norm_cd;     // [NCD]
+    const uint16_t *col;       // column mode: [NC] column components cx | cy << 4 | cz << 8
 };
 
 // (px, py, pz) of monomial m, packed px | py << 2 | pz << 4, in gen_rys.MONOS order.
@@ -116,6 +117,130 @@ __device__ __forceinline__ double group_max(double v, double *red, int gid) {
     }
 }
 
+// Stage 1 of a primitive batch: thread tb*NR + tr (tb < nb) evaluates root tr of primitive
+// quartet g0 + tb and writes the three 2-D tables of that root into tabs.
+template <class C, typename TT>
+__device__ __forceinline__ void rys_stage1(const PairTab &P, const RysTab &R, const int4 ib, const int4 ik,
+                                           int i0, int j0, int nbp, int g0, int nb, int tb, int tr,
+                                           TT *__restrict__ tabs) {
+    constexpr int S = C::S, F1 = C::F + 1, NR = C::NR, E = C::E, F = C::F;
+    if (tb < nb) {
+        const int g = g0 + tb;
+        const int gj = g / nbp;
+        const PrimPair bra = load_pp(P.pp, ib.x + i0 + (g - gj * nbp));
+        const PrimPair ket = load_pp(P.pp, ik.x + j0 + gj);
+        const double rz = rsqrt(bra.zeta + ket.zeta);
+        const double r2 = rz * rz;
+        const double PQv[3] = {bra.px - ket.px, bra.py - ket.py, bra.pz - ket.pz};
+        const double X = bra.zeta * ket.zeta * r2 * (PQv[0] * PQv[0] + PQv[1] * PQv[1] + PQv[2] * PQv[2]);
+        double u, w;
+        rys_root<NR>(R, X, tr, u, w);
+        const double ez = ket.zeta * r2, zz = bra.zeta * r2;
+        const double PAv[3] = {bra.pax, bra.pay, bra.paz}, QCv[3] = {ket.pax, ket.pay, ket.paz};
+        const double b10 = bra.oo2z * fma(-ez, u, 1.0);
+        const double b01 = ket.oo2z * fma(-zz, u, 1.0);
+        const double b00 = 0.5 * r2 * u;
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const double c00 = fma(-ez * PQv[ax], u, PAv[ax]);
+            const double d00 = fma(zz * PQv[ax], u, QCv[ax]);
+            TT *tab = tabs + ((tb * NR + tr) * 3 + ax) * S;
+            // column c = 0 by the a-recurrence, then column c+1 from columns c and c-1
+            double cur[E + 1], prev[E + 1];
+            cur[0] = ax == 0 ? bra.kab * ket.kab * rz * w : 1.0;
+            if (E > 0) cur[1] = c00 * cur[0];
+#pragma unroll
+            for (int a = 1; a < E; ++a) cur[a + 1] = fma(c00, cur[a], (double)a * b10 * cur[a - 1]);
+#pragma unroll
+            for (int a = 0; a <= E; ++a) {
+                tab[a * F1] = (TT)cur[a];
+                prev[a] = 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < F; ++c) {
+                double nxt[E + 1];
+#pragma unroll
+                for (int a = 0; a <= E; ++a) {
+                    double v = d00 * cur[a];
+                    if (c > 0) v = fma((double)c * b01, prev[a], v);
+                    if (a > 0) v = fma((double)a * b00, cur[a - 1], v);
+                    nxt[a] = v;
+                }
+#pragma unroll
+                for (int a = 0; a <= E; ++a) {
+                    prev[a] = cur[a];
+                    cur[a] = nxt[a];
+                    tab[a * F1 + c + 1] = (TT)nxt[a];
+                }
+            }
+        }
+    }
+}
+
+// Column mode of rys_contract (classes with C::COL): stage-2 thread `lane` < NC owns block
+// column lane; per primitive quartet and root it loads the column's three 2-D table columns
+// (3 (E+1) values) into registers and updates all NA row accumulators of the column
+// (C::col_update, generated with literal indices), so shared memory is read 3(E+1) times per
+// root instead of 3 times per block entry.
+template <class C, bool F32>
+__device__ __forceinline__ void rys_contract_col(const PairTab &P, const RysTab &R, const int4 ib,
+                                                 const int4 ik, int i0, int i1, int j0, int j1,
+                                                 double *__restrict__ work, const uint16_t *__restrict__ colpow,
+                                                 int lane, int gid) {
+    constexpr int S = C::S, F1 = C::F + 1, NR = C::NR, E = C::E, NA = C::NA, NC = C::NC;
+    using TT = typename std::conditional<F32, float, double>::type;
+    TT *__restrict__ tabs = reinterpret_cast<TT *>(work);
+    double acc[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) acc[a] = 0.0;
+    int cx = 0, cy = 0, cz = 0;
+    if (lane < NC) {
+        const unsigned cp = __ldg(&colpow[lane]);
+        cx = cp & 15u;
+        cy = (cp >> 4) & 15u;
+        cz = cp >> 8;
+    }
+    const int nbp = i1 - i0, nq = nbp * (j1 - j0);
+    const int tb = lane / NR, tr = lane - tb * NR;
+    for (int g0 = 0; g0 < nq; g0 += C::NPB) {
+        const int nb = min(C::NPB, nq - g0);
+        rys_stage1<C, TT>(P, R, ib, ik, i0, j0, nbp, g0, nb, tb, tr, tabs);
+        group_sync<C::G>(gid);
+        if (lane < NC) {
+            TT bacc[F32 ? NA : 1];
+            if constexpr (F32) {
+#pragma unroll
+                for (int a = 0; a < NA; ++a) bacc[a] = (TT)0;
+            }
+            for (int b = 0; b < nb; ++b) {
+#pragma unroll 1
+                for (int r = 0; r < NR; ++r) {
+                    const TT *__restrict__ t0 = tabs + (b * NR + r) * 3 * S;
+                    TT x[E + 1], y[E + 1], z[E + 1];
+#pragma unroll
+                    for (int a = 0; a <= E; ++a) {
+                        x[a] = t0[a * F1 + cx];
+                        y[a] = t0[S + a * F1 + cy];
+                        z[a] = t0[2 * S + a * F1 + cz];
+                    }
+                    if constexpr (F32) C::col_update(x, y, z, bacc);
+                    else C::col_update(x, y, z, acc);
+                }
+            }
+            if constexpr (F32) {
+#pragma unroll
+                for (int a = 0; a < NA; ++a) acc[a] += (double)bacc[a];
+            }
+        }
+        group_sync<C::G>(gid);
+    }
+    if (lane < NC) {
+#pragma unroll
+        for (int a = 0; a < NA; ++a) work[a * NC + lane] = acc[a];
+    }
+    group_sync<C::G>(gid);
+}
+
 // The contracted [e0|f0] block of bra pair ib (primitive pairs [i0, i1)) and ket pair ik
 // ([j0, j1)) into work[0 .. NBLK).  All G threads of the group call it; it ends with a barrier.
 // F32 (MIXED quartets below the FP32 cutoff): the 2-D tables are stored in FP32 and a batch's
@@ -129,6 +254,10 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
     constexpr int NSLOT = C::NSLOT;
     using TT = typename std::conditional<F32, float, double>::type;
     TT *__restrict__ tabs = reinterpret_cast<TT *>(work);
+    if constexpr (C::COL) {
+        rys_contract_col<C, F32>(P, R, ib, ik, i0, i1, j0, j1, work, T.col, lane, gid);
+        return;
+    }
     double acc[C::ACC];
     uint32_t off[C::ACC];
     // slot layout (NSLOT > 1): thread = slot * NBLK + entry, ACC == 1
@@ -143,57 +272,7 @@ __device__ __forceinline__ void rys_contract(const PairTab &P, const RysTab &R, 
     const int tb = lane / NR, tr = lane - tb * NR;
     for (int g0 = 0; g0 < nq; g0 += C::NPB) {
         const int nb = min(C::NPB, nq - g0);
-        if (tb < nb) {
-            const int g = g0 + tb;
-            const int gj = g / nbp;
-            const PrimPair bra = load_pp(P.pp, ib.x + i0 + (g - gj * nbp));
-            const PrimPair ket = load_pp(P.pp, ik.x + j0 + gj);
-            const double rz = rsqrt(bra.zeta + ket.zeta);
-            const double r2 = rz * rz;
-            const double PQv[3] = {bra.px - ket.px, bra.py - ket.py, bra.pz - ket.pz};
-            const double X = bra.zeta * ket.zeta * r2 * (PQv[0] * PQv[0] + PQv[1] * PQv[1] + PQv[2] * PQv[2]);
-            double u, w;
-            rys_root<NR>(R, X, tr, u, w);
-            const double ez = ket.zeta * r2, zz = bra.zeta * r2;
-            const double PAv[3] = {bra.pax, bra.pay, bra.paz}, QCv[3] = {ket.pax, ket.pay, ket.paz};
-            const double b10 = bra.oo2z * fma(-ez, u, 1.0);
-            const double b01 = ket.oo2z * fma(-zz, u, 1.0);
-            const double b00 = 0.5 * r2 * u;
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-                const double c00 = fma(-ez * PQv[ax], u, PAv[ax]);
-                const double d00 = fma(zz * PQv[ax], u, QCv[ax]);
-                TT *tab = tabs + ((tb * NR + tr) * 3 + ax) * S;
-                // column c = 0 by the a-recurrence, then column c+1 from columns c and c-1
-                double cur[E + 1], prev[E + 1];
-                cur[0] = ax == 0 ? bra.kab * ket.kab * rz * w : 1.0;
-                if (E > 0) cur[1] = c00 * cur[0];
-#pragma unroll
-                for (int a = 1; a < E; ++a) cur[a + 1] = fma(c00, cur[a], (double)a * b10 * cur[a - 1]);
-#pragma unroll
-                for (int a = 0; a <= E; ++a) {
-                    tab[a * F1] = (TT)cur[a];
-                    prev[a] = 0.0;
-                }
-#pragma unroll
-                for (int c = 0; c < F; ++c) {
-                    double nxt[E + 1];
-#pragma unroll
-                    for (int a = 0; a <= E; ++a) {
-                        double v = d00 * cur[a];
-                        if (c > 0) v = fma((double)c * b01, prev[a], v);
-                        if (a > 0) v = fma((double)a * b00, cur[a - 1], v);
-                        nxt[a] = v;
-                    }
-#pragma unroll
-                    for (int a = 0; a <= E; ++a) {
-                        prev[a] = cur[a];
-                        cur[a] = nxt[a];
-                        tab[a * F1 + c + 1] = (TT)nxt[a];
-                    }
-                }
-            }
-        }
+        rys_stage1<C, TT>(P, R, ib, ik, i0, j0, nbp, g0, nb, tb, tr, tabs);
         group_sync<C::G>(gid);
         if (slot < NSLOT) {
             if constexpr (F32) {

@@ -171,7 +171,10 @@ def test_class_kernel_limits():
         assert (128 // t["G"]) * t["smem_group"] * 8 <= 227 * 1024
         assert t["npb"] * t["nr"] <= t["G"]
         assert t["nslot"] == 1 or (t["nslot"] <= t["npb"] and t["nslot"] * t["nblk"] <= t["G"])
-        assert (t["acc"] == 1) if t["nslot"] > 1 else (t["acc"] * t["G"] >= t["nblk"])
+        if t["col"]:  # column mode: one stage-2 thread per block column, all rows in registers
+            assert t["nc"] <= t["G"] and t["na"] <= gen_rys.COL_MAX_NA and t["nslot"] == 1
+        else:
+            assert (t["acc"] == 1) if t["nslot"] > 1 else (t["acc"] * t["G"] >= t["nblk"])
         assert max(max(o) for o in t["blk"]) < t["S"] < 256
         assert t["na"] < 256 and t["nc"] < 256
 
