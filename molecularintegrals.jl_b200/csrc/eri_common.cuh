@@ -73,9 +73,11 @@ struct JKOut {
     int n;
 };
 
-// The chunk queue of one class pair: chunk c = {bra pair, first ket pair, ket count,
-// molecule}; lane l of the warp that takes it computes (bra | first + l + 32 i).  Chunks never
-// cross a bra pair, a molecule or, when bra and ket class coincide, the triangle q <= p.
+// The chunk queue of one class pair: chunk c = {bra pair, first ket pair, ket count |
+// lg << 16, molecule}.  HGP: S = 2^lg lanes share each quartet, lane l of the warp that takes
+// the chunk computes (bra | first + l % (32/S) + (32/S) i) over every S-th ket primitive
+// (lg = 0: one lane per quartet).  Rys chunks have lg = 0.  Chunks never cross a bra pair, a
+// molecule or, when bra and ket class coincide, the triangle q <= p.
 struct EriQueue {
     PairTab pairs;
     BoysTab boys;

@@ -372,22 +372,21 @@ void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, do
 
 namespace molints {{
 
-// Contracted, normalised (ab|cd) for bra pair p and ket pair q into res[{nout}]
-// (ma, mb, mc, md row-major), summed over the bra primitive pairs [i0, i1) and the ket
-// primitive pairs [j0, j1) of the two shell pairs.  VT is the VRR arithmetic type (double,
-// or float for MIXED).  The ket loop is outside: a warp shares its bra pair, so the inner
-// bra loads are warp-uniform broadcasts and each lane's ket record is loaded once.
+// The contracted [e0|f0] block of bra pair p and ket pair q into acc[{nacc}], summed over
+// the bra primitive pairs [i0, i1) and the ket primitive pairs j0, j0 + jstep, ... < j1 of the
+// two shell pairs.  VT is the VRR arithmetic type (double, or float for MIXED).  The ket loop
+// is outside: a warp shares its bra pair, so the inner bra loads are warp-uniform broadcasts
+// and each lane's ket record is loaded once.  jstep > 1 splits one quartet's ket primitives
+// over the lanes of a split group (their blocks are summed before the HRR).
 template <typename VT>
-__device__ __forceinline__ void quartet_{tag}(const PairTab &P, const BoysTab &B, int p, int q,
-                                              int i0, int i1, int j0, int j1,
-                                              double *__restrict__ res,
-                                              double *__restrict__ acc_out = nullptr) {{
+__device__ __forceinline__ void vrr_{tag}(const PairTab &P, const BoysTab &B, int p, int q,
+                                          int i0, int i1, int j0, int j1, int jstep,
+                                          double *__restrict__ acc) {{
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
-    double acc[{nacc}];
 #pragma unroll
     for (int x = 0; x < {nacc}; ++x) acc[x] = 0.0;
-    for (int j = j0; j < j1; ++j) {{
+    for (int j = j0; j < j1; j += jstep) {{
         const PrimPair ket = load_pp(P.pp, ik_.x + j);
         for (int i = i0; i < i1; ++i) {{
             const PrimPair bra = load_pp(P.pp, ib_.x + i);
@@ -412,10 +411,13 @@ __device__ __forceinline__ void quartet_{tag}(const PairTab &P, const BoysTab &B
 {acc_code}
         }}
     }}
-    if (acc_out) {{
-#pragma unroll
-        for (int x = 0; x < {nacc}; ++x) acc_out[x] = acc[x];
-    }}
+}}
+
+// Bra and ket HRR of the contracted block (src/HGP.jl:92-114), then the component norms:
+// the normalised (ab|cd) of bra pair p and ket pair q into res[{nout}] (ma, mb, mc, md
+// row-major).
+__device__ __forceinline__ void hrr_{tag}(const PairTab &P, int p, int q, const double *__restrict__ acc,
+                                          double *__restrict__ res) {{
     const double4 gb = ldg4(&P.geo[p]);
     const double4 gk = ldg4(&P.geo[q]);
     const double ABx = gb.x, ABy = gb.y, ABz = gb.z;
@@ -423,6 +425,22 @@ __device__ __forceinline__ void quartet_{tag}(const PairTab &P, const BoysTab &B
     (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;
 {hrr_code}
 {out_code}
+}}
+
+// (ab|cd) over the bra primitive pairs [i0, i1) and ket primitive pairs [j0, j1) into
+// res[{nout}]; the contracted block also into acc_out when given (the bound kernels).
+template <typename VT>
+__device__ __forceinline__ void quartet_{tag}(const PairTab &P, const BoysTab &B, int p, int q,
+                                              int i0, int i1, int j0, int j1,
+                                              double *__restrict__ res,
+                                              double *__restrict__ acc_out = nullptr) {{
+    double acc[{nacc}];
+    vrr_{tag}<VT>(P, B, p, q, i0, i1, j0, j1, 1, acc);
+    if (acc_out) {{
+#pragma unroll
+        for (int x = 0; x < {nacc}; ++x) acc_out[x] = acc[x];
+    }}
+    hrr_{tag}(P, p, q, acc, res);
 }}
 
 __device__ __forceinline__ void store_{tag}(double *__restrict__ out, const int4 ib_, const int4 ik_,
@@ -449,7 +467,12 @@ __device__ __noinline__ void jk_{tag}(const JKOut &jk, const int4 ib_, const int
 
 // Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
 // ket pairs of one molecule) from a shared counter until the chunk list, ordered by
-// decreasing estimated cost, is exhausted; lane l computes the quartets (p, q0 + l + 32 i).
+// decreasing estimated cost, is exhausted.  A chunk's count field carries the split
+// log2(S) in bits 16+: S lanes share each quartet, lane l takes ket pair q0 + l % (32/S)
+// (+ 32/S per round) and every S-th of its ket primitives from l / (32/S); the S partial
+// blocks are summed by a fixed butterfly (the result depends on S alone, not on the chunk),
+// and the group's first lane runs the HRR and stores.  Heavy quartets (many primitive
+// quartets) are split so that no single lane's serial primitive loop sets the kernel time.
 // JK: digest into J and K (molints_plan_jk) instead of storing the packed integrals; a separate
 // instantiation, so that the store kernels carry none of the digestion code.
 template <int MIXED, int JK>
@@ -461,21 +484,38 @@ __global__ void __launch_bounds__(128) eri_queue_{tag}(const EriQueue Q) {{
         c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= Q.nchunks) return;
         const int4 ch = __ldg(&Q.chunks[c]);
-        for (int q = ch.y + lane; q < ch.y + ch.z; q += 32) {{
-        const int p = ch.x;
-        const double2 bp = __ldg(&Q.pairs.bnd[p]), bq = __ldg(&Q.pairs.bnd[q]);
-        double res[{nout}];
-        if (bp.x * bq.x < Q.screen_cut) {{
+        const int p = ch.x, cnt = ch.z & 0xffff, lg = ch.z >> 16;
+        const int W = 32 >> lg, kq = lane & (W - 1), s = lane >> (5 - lg);
+        for (int base = 0; base < cnt; base += W) {{
+        const int q = ch.y + base + kq;
+        const bool live = base + kq < cnt;
+        double acc[{nacc}];
+        double2 bp = make_double2(0.0, 0.0), bq = bp;
+        if (live) {{
+            bp = __ldg(&Q.pairs.bnd[p]);
+            bq = __ldg(&Q.pairs.bnd[q]);
+        }}
+        if (!live || bp.x * bq.x < Q.screen_cut) {{
 #pragma unroll
-            for (int x = 0; x < {nout}; ++x) res[x] = 0.0;
+            for (int x = 0; x < {nacc}; ++x) acc[x] = 0.0;
         }} else {{
             const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
-            if (MIXED && bp.y * bq.y < Q.fp32_cut) quartet_{tag}<float>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
-            else quartet_{tag}<double>(Q.pairs, Q.boys, p, q, 0, nb, 0, nk, res);
+            if (MIXED && bp.y * bq.y < Q.fp32_cut) vrr_{tag}<float>(Q.pairs, Q.boys, p, q, 0, nb, s, nk, 1 << lg, acc);
+            else vrr_{tag}<double>(Q.pairs, Q.boys, p, q, 0, nb, s, nk, 1 << lg, acc);
         }}
-        if constexpr (JK) jk_{tag}(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-        else store_{tag}(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                         p == q, res);
+        if (lg) {{
+            for (int off = W; off < 32; off <<= 1) {{
+#pragma unroll
+                for (int x = 0; x < {nacc}; ++x) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], off);
+            }}
+        }}
+        if (live && s == 0) {{
+            double res[{nout}];
+            hrr_{tag}(Q.pairs, p, q, acc, res);
+            if constexpr (JK) jk_{tag}(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            else store_{tag}(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                             p == q, res);
+        }}
         }}
     }}
 }}

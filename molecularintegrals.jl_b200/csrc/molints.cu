@@ -152,6 +152,19 @@ int pair_class_of(int la, int lb) {
     return -1;
 }
 
+// Lanes per quartet (log2) of an HGP work-queue chunk whose bra pair has nb and ket pair nk
+// kept primitive pairs.  A lane evaluates its quartet's nb x nk primitive quartets one after
+// another; a heavy quartet (six-primitive core shells: 36 x 36) on one lane outlasts the rest
+// of the launch, so its ket primitives are split over S = 2^lg lanes (S <= 16, S <= nk) until a
+// lane's share nb x ceil(nk / S) is at most kLaneWork.  A pure function of (nb, nk): the same
+// quartet gets the same split, and so the same rounding, in every plan.
+constexpr int kLaneWork = 64;
+int hgp_split_log2(int nb, int nk) {
+    int lg = 0;
+    while (lg < 4 && (int64_t)nb * ((nk + (1 << lg) - 1) >> lg) > kLaneWork && (nk >> lg) >= 2) ++lg;
+    return lg;
+}
+
 template <typename T>
 int dev_alloc(molints_ctx *ctx, T **p, size_t count, int64_t *tally) {
     size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
@@ -977,7 +990,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<ClassQueue> cq(cps.size());
     auto build_queue = [&](size_t ci) {
         const int x = cps[ci].first, y = cps[ci].second;
-        const int width = (p->method[x][y] == MOLINTS_METHOD_RYS ? rys_width(x, y) : 32) * widen;
+        const bool hgp = p->method[x][y] != MOLINTS_METHOD_RYS;
+        const int width = (hgp ? 32 : rys_width(x, y)) * widen;
         const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
         const double w = 1.0 + lsum * lsum;
         // heaviest first, bucketed by the binary exponent of the cost: an O(n) order that is
@@ -1018,12 +1032,25 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                     }
                 }
                 const double wp = w * p->npp_h[pb];
-                for (int q0 = kbeg; q0 < kend; q0 += width) {
-                    const int n = std::min(width, kend - q0);
+                for (int q0 = kbeg; q0 < kend;) {
+                    int n = std::min(width, kend - q0), lg = 0;
+                    if (hgp) {
+                        // the kets of a molecule's class run are in descending primitive-pair
+                        // count, so the split only falls along the run: a chunk that starts
+                        // unsplit stays unsplit, and a split chunk ends where the split changes
+                        // (shard plans order by highest shell first; there a heavy ket inside
+                        // an unsplit chunk only runs unsplit)
+                        lg = hgp_split_log2(p->npp_h[pb], p->npp_h[q0]);
+                        n = std::min((32 >> lg) * widen, kend - q0);
+                        if (lg)
+                            for (int k = 1; k < n; ++k)
+                                if (hgp_split_log2(p->npp_h[pb], p->npp_h[q0 + k]) != lg) { n = k; break; }
+                    }
                     const double cost = wp * (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
                     total += cost;
                     const int b = bucket(cost);
-                    raw.push_back(make_int4(pb, q0, n, m));
+                    raw.push_back(make_int4(pb, q0, n | (lg << 16), m));
+                    q0 += n;
                     bk.push_back((unsigned char)b);
                     ++cnt[b + 1];
                 }
