@@ -74,9 +74,10 @@ struct JKOut {
 };
 
 // The chunk queue of one class pair: chunk c = {bra pair, first ket pair, ket count |
-// lg << 16, molecule}.  HGP: S = 2^lg lanes share each quartet, lane l of the warp that takes
-// the chunk computes (bra | first + l % (32/S) + (32/S) i) over every S-th ket primitive
-// (lg = 0: one lane per quartet).  Rys chunks have lg = 0.  Chunks never cross a bra pair, a
+// split << 16, molecule}.  HGP: split = lg | lgj << 4, S = 2^lg lanes share each quartet and
+// lane l of the warp that takes the chunk computes its share of (bra | first + l % (32/S) +
+// (32/S) i), the ket primitives split over 2^lgj lanes and the bra primitives over the rest
+// (split 0: one lane per quartet).  Rys chunks have split 0.  Chunks never cross a bra pair, a
 // molecule or, when bra and ket class coincide, the triangle q <= p.
 struct EriQueue {
     PairTab pairs;

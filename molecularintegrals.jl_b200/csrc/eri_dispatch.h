@@ -272,6 +272,21 @@ static const char *const kEriNames[11][11] = {
     {"eri_fdss", "eri_fdps", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {"eri_ffss", nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
 };
+// relative cost of one primitive quartet of the HGP kernel, 1 + VRR entries / 4 (the
+// (ss|ss) quartet ~ 1); sizes the lane split of heavy quartets; 0 where no HGP kernel
+static const float kEriPrimCost[11][11] = {
+    {1.25f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {2.25f, 5.5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {4.75f, 14.0f, 37.5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {4.75f, 11.75f, 30.0f, 30.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {9.75f, 26.75f, 70.0f, 70.0f, 158.5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {9.75f, 22.25f, 54.25f, 54.25f, 122.5f, 122.5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {18.5f, 50.5f, 131.25f, 131.25f, 294.75f, 0.0f, 583.5f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {18.5f, 46.0f, 115.5f, 115.5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {32.5f, 81.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {53.5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+};
 static const RysLauncher kRysLaunchers[11][11] = {
     {launch_rys_ssss, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},
     {launch_rys_psss, launch_rys_psps, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr},

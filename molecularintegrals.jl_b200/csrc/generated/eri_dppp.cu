@@ -5,14 +5,14 @@
 namespace molints {
 
 // The contracted [e0|f0] block of bra pair p and ket pair q into acc[144], summed over
-// the bra primitive pairs [i0, i1) and the ket primitive pairs j0, j0 + jstep, ... < j1 of the
-// two shell pairs.  VT is the VRR arithmetic type (double, or float for MIXED).  The ket loop
-// is outside: a warp shares its bra pair, so the inner bra loads are warp-uniform broadcasts
-// and each lane's ket record is loaded once.  jstep > 1 splits one quartet's ket primitives
-// over the lanes of a split group (their blocks are summed before the HRR).
+// the bra primitive pairs i0, i0 + istep, ... < i1 and the ket primitive pairs j0, j0 + jstep,
+// ... < j1 of the two shell pairs.  VT is the VRR arithmetic type (double, or float for MIXED).
+// The ket loop is outside: a warp shares its bra pair, so the inner bra loads are broadcasts
+// and each lane's ket record is loaded once.  Steps above 1 split one quartet's primitive
+// quartets over the lanes of a split group (their blocks are summed before the HRR).
 template <typename VT>
 __device__ __forceinline__ void vrr_dppp(const PairTab &P, const BoysTab &B, int p, int q,
-                                          int i0, int i1, int j0, int j1, int jstep,
+                                          int i0, int i1, int istep, int j0, int j1, int jstep,
                                           double *__restrict__ acc) {
     const int4 ib_ = __ldg(&P.info[p]);
     const int4 ik_ = __ldg(&P.info[q]);
@@ -20,7 +20,7 @@ __device__ __forceinline__ void vrr_dppp(const PairTab &P, const BoysTab &B, int
     for (int x = 0; x < 144; ++x) acc[x] = 0.0;
     for (int j = j0; j < j1; j += jstep) {
         const PrimPair ket = load_pp(P.pp, ik_.x + j);
-        for (int i = i0; i < i1; ++i) {
+        for (int i = i0; i < i1; i += istep) {
             const PrimPair bra = load_pp(P.pp, ib_.x + i);
             const double r = rsqrt(bra.zeta + ket.zeta);
             const double r2 = r * r;
@@ -969,7 +969,7 @@ __device__ __forceinline__ void quartet_dppp(const PairTab &P, const BoysTab &B,
                                               double *__restrict__ res,
                                               double *__restrict__ acc_out = nullptr) {
     double acc[144];
-    vrr_dppp<VT>(P, B, p, q, i0, i1, j0, j1, 1, acc);
+    vrr_dppp<VT>(P, B, p, q, i0, i1, 1, j0, j1, 1, acc);
     if (acc_out) {
 #pragma unroll
         for (int x = 0; x < 144; ++x) acc_out[x] = acc[x];
@@ -1349,12 +1349,13 @@ __device__ __noinline__ void jk_dppp(const JKOut &jk, const int4 ib_, const int4
 
 // Persistent work-queue kernel: each warp takes chunks (one bra pair, a run of consecutive
 // ket pairs of one molecule) from a shared counter until the chunk list, ordered by
-// decreasing estimated cost, is exhausted.  A chunk's count field carries the split
-// log2(S) in bits 16+: S lanes share each quartet, lane l takes ket pair q0 + l % (32/S)
-// (+ 32/S per round) and every S-th of its ket primitives from l / (32/S); the S partial
-// blocks are summed by a fixed butterfly (the result depends on S alone, not on the chunk),
-// and the group's first lane runs the HRR and stores.  Heavy quartets (many primitive
-// quartets) are split so that no single lane's serial primitive loop sets the kernel time.
+// decreasing estimated cost, is exhausted.  A chunk's count field carries the split in bits
+// 16+: lg = log2 S (bits 16-18) and lgj = log2 Sj (bits 20-22).  S lanes share each quartet:
+// lane l takes ket pair q0 + l % (32/S) (+ 32/S per round); its group rank s = l / (32/S)
+// takes every Sj-th ket primitive from s % Sj and every (S/Sj)-th bra primitive from s / Sj.
+// The S partial blocks are summed by a fixed butterfly (the result depends on the split
+// alone, not on the chunk), and the group's first lane runs the HRR and stores.  Heavy
+// quartets are split so that no single lane's serial primitive loop sets the kernel time.
 // JK: digest into J and K (molints_plan_jk) instead of storing the packed integrals; a separate
 // instantiation, so that the store kernels carry none of the digestion code.
 template <int MIXED, int JK>
@@ -1366,8 +1367,9 @@ __global__ void __launch_bounds__(128) eri_queue_dppp(const EriQueue Q) {
         c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= Q.nchunks) return;
         const int4 ch = __ldg(&Q.chunks[c]);
-        const int p = ch.x, cnt = ch.z & 0xffff, lg = ch.z >> 16;
+        const int p = ch.x, cnt = ch.z & 0xffff, lg = (ch.z >> 16) & 7, lgj = (ch.z >> 20) & 7;
         const int W = 32 >> lg, kq = lane & (W - 1), s = lane >> (5 - lg);
+        const int js = s & ((1 << lgj) - 1), is = s >> lgj;
         for (int base = 0; base < cnt; base += W) {
         const int q = ch.y + base + kq;
         const bool live = base + kq < cnt;
@@ -1382,8 +1384,9 @@ __global__ void __launch_bounds__(128) eri_queue_dppp(const EriQueue Q) {
             for (int x = 0; x < 144; ++x) acc[x] = 0.0;
         } else {
             const int nb = __ldg(&Q.pairs.info[p]).y, nk = __ldg(&Q.pairs.info[q]).y;
-            if (MIXED && bp.y * bq.y < Q.fp32_cut) vrr_dppp<float>(Q.pairs, Q.boys, p, q, 0, nb, s, nk, 1 << lg, acc);
-            else vrr_dppp<double>(Q.pairs, Q.boys, p, q, 0, nb, s, nk, 1 << lg, acc);
+            if (MIXED && bp.y * bq.y < Q.fp32_cut)
+                vrr_dppp<float>(Q.pairs, Q.boys, p, q, is, nb, 1 << (lg - lgj), js, nk, 1 << lgj, acc);
+            else vrr_dppp<double>(Q.pairs, Q.boys, p, q, is, nb, 1 << (lg - lgj), js, nk, 1 << lgj, acc);
         }
         if (lg) {
             for (int off = W; off < 32; off <<= 1) {

@@ -15,8 +15,12 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -55,6 +59,8 @@ struct molints_ctx {
     int occupancy[kNumPairClasses][kNumPairClasses][4] = {};
     RysTab rys{};  // device addresses of the Rys root/weight tables on this device
     int32_t class_method[kNumPairClasses][kNumPairClasses] = {};  // AUTO choices (0 = default)
+    char *stage = nullptr;     // pinned host buffer of plan uploads (work queues, pair tables)
+    size_t stage_bytes = 0;
     std::string err;
 };
 
@@ -152,17 +158,27 @@ int pair_class_of(int la, int lb) {
     return -1;
 }
 
-// Lanes per quartet (log2) of an HGP work-queue chunk whose bra pair has nb and ket pair nk
-// kept primitive pairs.  A lane evaluates its quartet's nb x nk primitive quartets one after
-// another; a heavy quartet (six-primitive core shells: 36 x 36) on one lane outlasts the rest
-// of the launch, so its ket primitives are split over S = 2^lg lanes (S <= 16, S <= nk) until a
-// lane's share nb x ceil(nk / S) is at most kLaneWork.  A pure function of (nb, nk): the same
-// quartet gets the same split, and so the same rounding, in every plan.
-constexpr int kLaneWork = 64;
-int hgp_split_log2(int nb, int nk) {
-    int lg = 0;
-    while (lg < 4 && (int64_t)nb * ((nk + (1 << lg) - 1) >> lg) > kLaneWork && (nk >> lg) >= 2) ++lg;
-    return lg;
+// Lane split of an HGP work-queue chunk whose bra pair has nb and ket pair nk kept primitive
+// pairs, in a class whose primitive quartet costs `cost` (kEriPrimCost; (ss|ss) ~ 1).  A lane
+// evaluates its quartet's primitive quartets one after another; a heavy quartet (six-primitive
+// core shells: 36 x 36) on one lane outlasts the rest of the launch.  Its primitive quartets
+// are therefore split over S = 2^lg lanes (S <= 32) -- ket primitives over Sj = 2^lgj of them
+// first (Sj <= nk), then bra primitives over S / Sj -- until a lane's share costs at most
+// kLaneCost.  Returns lg | lgj << 4, the chunk's split field.  A pure function of
+// (nb, nk, class): the same quartet gets the same split, and so the same rounding, in every
+// plan.
+constexpr double kLaneCost = 80.0;
+int hgp_split(int nb, int nk, double cost) {
+    int lg = 0, lgj = 0;
+    auto share = [&](int gj, int gi) {
+        return cost * (double)((nk + (1 << gj) - 1) >> gj) * (double)((nb + (1 << gi) - 1) >> gi);
+    };
+    while (lg < 5 && share(lgj, lg - lgj) > kLaneCost) {
+        if ((nk >> lgj) >= 2) ++lgj;
+        else if ((nb >> (lg - lgj)) < 2) break;
+        ++lg;
+    }
+    return lg | (lgj << 4);
 }
 
 template <typename T>
@@ -180,6 +196,103 @@ int dev_alloc(molints_ctx *ctx, T **p, size_t count, int64_t *tally) {
 void dev_free(molints_ctx *ctx, void *p) {
     if (p) cudaFreeAsync(p, ctx->stream);
 }
+
+// The pinned upload buffer of the context, grown to at least `bytes` (a pinned source makes
+// the plan uploads asynchronous DMA at full link speed; every plan creation ends with a
+// stream synchronise, so the buffer is free again when the next one starts).
+int ctx_stage(molints_ctx *ctx, size_t bytes) {
+    if (ctx->stage_bytes >= bytes) return MOLINTS_OK;
+    if (ctx->stage) cudaFreeHost(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    const size_t want = std::max<size_t>(bytes + bytes / 4, (size_t)1 << 20);
+    cudaError_t e = cudaHostAlloc((void **)&ctx->stage, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        ctx->stage = nullptr;
+        return cuda_fail(ctx, e, "cudaHostAlloc (plan upload buffer)");
+    }
+    ctx->stage_bytes = want;
+    return MOLINTS_OK;
+}
+
+// Host worker threads shared by every context of the process (the serving slots create plans
+// concurrently and share them).  Created on first use and kept until the process exits, so a
+// plan creation pays no thread start-up.  run(n, fn) calls fn(0..n-1) on the workers and the
+// calling thread and returns when all calls are done; concurrent run()s from several threads
+// interleave on the same workers.
+class HostPool {
+  public:
+    static HostPool &instance() {
+        static HostPool *pool = new HostPool();  // never destroyed: its threads outlive main
+        return *pool;
+    }
+    void run(int n, const std::function<void(int)> &fn) {
+        if (n <= 0) return;
+        if (n == 1 || nthreads_ == 0) {
+            for (int i = 0; i < n; ++i) fn(i);
+            return;
+        }
+        Job job;
+        job.fn = &fn;
+        job.n = n;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            jobs_.push_back(&job);
+        }
+        cv_.notify_all();
+        work(job);
+        std::unique_lock<std::mutex> lk(mu_);
+        auto it = std::find(jobs_.begin(), jobs_.end(), &job);
+        if (it != jobs_.end()) jobs_.erase(it);
+        // no worker can pick the job up any more; wait for those inside it
+        done_cv_.wait(lk, [&] { return job.users == 0 && job.done.load() == n; });
+    }
+
+  private:
+    struct Job {
+        const std::function<void(int)> *fn = nullptr;
+        int n = 0;
+        std::atomic<int> next{0}, done{0};
+        int users = 0;  // workers inside work(); guarded by mu_
+    };
+    static void work(Job &j) {
+        for (int i; (i = j.next.fetch_add(1)) < j.n;) {
+            (*j.fn)(i);
+            j.done.fetch_add(1);
+        }
+    }
+    HostPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        nthreads_ = (int)std::min(15u, hw > 1 ? hw - 1 : 0u);
+        for (int t = 0; t < nthreads_; ++t) std::thread([this] { loop(); }).detach();
+    }
+    void loop() {
+        for (;;) {
+            Job *j = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return !jobs_.empty(); });
+                j = jobs_.front();
+                if (j->next.load() >= j->n) {  // all calls handed out: move on
+                    jobs_.pop_front();
+                    continue;
+                }
+                ++j->users;
+            }
+            work(*j);
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                --j->users;
+                if (!jobs_.empty() && jobs_.front() == j && j->next.load() >= j->n) jobs_.pop_front();
+            }
+            done_cv_.notify_all();
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    std::deque<Job *> jobs_;
+    int nthreads_ = 0;
+};
 
 }  // namespace
 
@@ -453,6 +566,7 @@ int molints_destroy(molints_ctx *ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->stage) cudaFreeHost(ctx->stage);
     delete ctx;
     return MOLINTS_OK;
 }
@@ -795,9 +909,11 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<int4> info_h(npair);
     std::vector<int> src_h;
     std::vector<int> cls_start(kNumPairClasses + 1, 0);
-    // kept primitive pairs of each pair, (b_k, source) in source order; indexed by position in
-    // the stage-1 order
-    std::vector<std::vector<std::pair<double, int>>> kept;
+    // kept primitive pairs of each pair, b_k and source in source order, flat: those of the
+    // pair at stage-1 position k are [kept_off[k], kept_off[k + 1])
+    std::vector<int64_t> kept_off;
+    std::vector<double> kept_b;
+    std::vector<int> kept_src;
     std::vector<double> pbk_h;
     auto fill_tables = [&](const std::vector<int> *stage1_pos) {
         src_h.clear();
@@ -807,9 +923,10 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             ab_h[k] = make_int2(pr[k].a, pr[k].b);
             const int off = (int)src_h.size();
             if (stage1_pos) {
-                for (const auto &x : kept[(*stage1_pos)[k]]) {
-                    src_h.push_back(x.second);
-                    pbk_h.push_back(x.first);
+                const int k1 = (*stage1_pos)[k];
+                for (int64_t x = kept_off[k1]; x < kept_off[k1 + 1]; ++x) {
+                    src_h.push_back(kept_src[x]);
+                    pbk_h.push_back(kept_b[x]);
                 }
             } else {
                 for (int ia = 0; ia < K[pr[k].a]; ++ia)
@@ -896,15 +1013,20 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         for (int x = 0; x < info_h[k].y; ++x) q += pb_h[info_h[k].x + x].x;
         qmax[pr[k].mol] = std::max(qmax[pr[k].mol], q);
     }
-    kept.assign(npair, {});
+    kept_off.assign(npair + 1, 0);
+    kept_b.resize(nall);
+    kept_src.resize(nall);
     std::vector<double2> bnd1(npair);
     int64_t nkept = 0;
     for (int k = 0; k < npair; ++k) {
         double qa = 0.0, wa = 0.0;
+        kept_off[k] = nkept;
         for (int x = 0; x < info_h[k].y; ++x) {
             const double2 bb = pb_h[info_h[k].x + x];
             if (opts.prim_cutoff > 0.0 && bb.x * qmax[pr[k].mol] < opts.prim_cutoff) continue;
-            kept[k].push_back({bb.x, src_h[info_h[k].x + x]});
+            kept_b[nkept] = bb.x;
+            kept_src[nkept] = src_h[info_h[k].x + x];
+            ++nkept;
             qa += bb.x;
             wa += bb.y;
         }
@@ -912,12 +1034,12 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         const double dab = std::sqrt((A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
                                      (A[2] - Bc[2]) * (A[2] - Bc[2]));
         bnd1[k] = make_double2(qa, wa * std::pow(1.0 + dab, L[pr[k].b]));
-        nkept += (int64_t)kept[k].size();
     }
+    kept_off[npair] = nkept;
     p->nprim_pair_kept = nkept;
     // re-sort by kept count, remembering each pair's stage-1 position
     std::vector<int> pos1(npair);
-    for (int k = 0; k < npair; ++k) { pos1[k] = k; pr[k].npp = (int)kept[k].size(); }
+    for (int k = 0; k < npair; ++k) { pos1[k] = k; pr[k].npp = (int)(kept_off[k + 1] - kept_off[k]); }
     std::vector<int> perm(npair);
     for (int k = 0; k < npair; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return order(pr[x], pr[y]); });
@@ -951,7 +1073,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     };
     std::vector<int64_t> npp_prefix(npair + 1, 0);  // kept primitive pairs of pairs [0, k)
     for (int k = 0; k < npair; ++k) npp_prefix[k + 1] = npp_prefix[k] + p->npp_h[k];
-    std::vector<int4> chunks;
     // chunk width: 32 ket pairs (one per lane), widened in steps of 32 for large batches so
     // that the queues stay near kMaxChunks entries
     constexpr double kMaxChunks = 4.0e6;
@@ -982,123 +1103,171 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         }
         return std::max(1, std::min(8, (int)(nq / kRysMinChunks)));
     };
-    // Class pairs are independent: their queues are built on host threads, then concatenated.
-    struct ClassQueue { std::vector<int4> q; double total = 0.0; };
+    // Class pairs are independent, and so are the bra pairs of one class pair: the queues are
+    // built as tasks of consecutive bra pairs on the process's host worker threads.  Phase 1:
+    // each task's chunks, in (bra, ket) order, and its count per cost bucket.  Phase 2: every
+    // chunk goes straight to its place in the pinned upload buffer -- class pairs in order, in a
+    // class pair the heaviest bucket first, in a bucket the task and chunk order.
+    constexpr int kBuckets = 64;
+    struct QueueTask {
+        int ci = 0, pb0 = 0, pb1 = 0;
+        std::vector<int4> raw;
+        std::vector<unsigned char> bk;
+        int64_t cnt[kBuckets] = {};
+        int64_t base[kBuckets] = {};
+        double total = 0.0;
+    };
     std::vector<std::pair<int, int>> cps;
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) cps.push_back({x, y});
-    std::vector<ClassQueue> cq(cps.size());
-    auto build_queue = [&](size_t ci) {
-        const int x = cps[ci].first, y = cps[ci].second;
-        const bool hgp = p->method[x][y] != MOLINTS_METHOD_RYS;
-        const int width = (hgp ? 32 : rys_width(x, y)) * widen;
-        const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
-        const double w = 1.0 + lsum * lsum;
-        // heaviest first, bucketed by the binary exponent of the cost: an O(n) order that is
-        // all the load balance needs (a full sort of millions of chunks dominated batches)
-        constexpr int kBuckets = 64;
-        auto bucket = [](double c) {
-            uint64_t bits;
-            std::memcpy(&bits, &c, sizeof bits);
-            const int e2 = c > 0.0 ? (int)((bits >> 52) & 0x7ff) - 1022 : 1;
-            return std::max(0, std::min(kBuckets - 1, kBuckets - 1 - (e2 + 8)));
-        };
-        std::vector<int4> raw;
-        std::vector<unsigned char> bk;
-        int cnt[kBuckets + 1] = {0};
-        double total = 0.0;
-        for (int m = 0; m < nmol; ++m) {
-            int b0, b1, k0, k1;
-            range_of(x, m, b0, b1);
-            range_of(y, m, k0, k1);
-            for (int pb = b0; pb < b1; ++pb) {
-                int kbeg = k0, kend = (x == y) ? pb + 1 : k1;
-                if (sharded) {
-                    // quartet owner: the higher of the two pairs' max shells
-                    const int mp = pr[pb].ms;
-                    auto first_ms_at_least = [&](int v) {
-                        return (int)(std::partition_point(pr.begin() + k0, pr.begin() + k1,
-                                                          [v](const PairRec &r) { return r.ms < v; }) -
-                                     pr.begin());
-                    };
-                    if (mp >= shard_s1) continue;
-                    if (x == y) {
-                        if (mp < shard_s0) continue;  // q <= pb in list order: owner is mp
-                    } else if (mp >= shard_s0) {
-                        kend = first_ms_at_least(shard_s1);
-                    } else {
-                        kbeg = first_ms_at_least(shard_s0);
-                        kend = first_ms_at_least(shard_s1);
-                    }
-                }
-                const double wp = w * p->npp_h[pb];
-                for (int q0 = kbeg; q0 < kend;) {
-                    int n = std::min(width, kend - q0), lg = 0;
-                    if (hgp) {
-                        // the kets of a molecule's class run are in descending primitive-pair
-                        // count, so the split only falls along the run: a chunk that starts
-                        // unsplit stays unsplit, and a split chunk ends where the split changes
-                        // (shard plans order by highest shell first; there a heavy ket inside
-                        // an unsplit chunk only runs unsplit)
-                        lg = hgp_split_log2(p->npp_h[pb], p->npp_h[q0]);
-                        n = std::min((32 >> lg) * widen, kend - q0);
-                        if (lg)
-                            for (int k = 1; k < n; ++k)
-                                if (hgp_split_log2(p->npp_h[pb], p->npp_h[q0 + k]) != lg) { n = k; break; }
-                    }
-                    const double cost = wp * (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
-                    total += cost;
-                    const int b = bucket(cost);
-                    raw.push_back(make_int4(pb, q0, n | (lg << 16), m));
-                    q0 += n;
-                    bk.push_back((unsigned char)b);
-                    ++cnt[b + 1];
-                }
-            }
-        }
-        for (int k = 1; k <= kBuckets; ++k) cnt[k] += cnt[k - 1];
-        cq[ci].q.resize(raw.size());
-        for (size_t i = 0; i < raw.size(); ++i) cq[ci].q[cnt[bk[i]]++] = raw[i];
-        cq[ci].total = total;
-    };
-    {
-        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        std::atomic<size_t> next{0};
-        auto worker = [&] {
-            for (size_t ci; (ci = next.fetch_add(1)) < cps.size();) build_queue(ci);
-        };
-        std::vector<std::thread> pool;
-        for (unsigned t = 1; t < std::min<unsigned>(hw, (unsigned)cps.size()); ++t) pool.emplace_back(worker);
-        worker();
-        for (std::thread &t : pool) t.join();
-    }
-    size_t nq = 0;
-    for (const ClassQueue &c : cq) nq += c.q.size();
-    chunks.reserve(nq);
+    std::vector<QueueTask> tasks;
+    std::vector<int> task_end(cps.size(), 0), cp_width(cps.size(), 32 * widen);
+    for (size_t ci = 0; ci < cps.size(); ++ci)
+        if (p->method[cps[ci].first][cps[ci].second] == MOLINTS_METHOD_RYS)
+            cp_width[ci] = rys_width(cps[ci].first, cps[ci].second) * widen;
     for (size_t ci = 0; ci < cps.size(); ++ci) {
         const int x = cps[ci].first, y = cps[ci].second;
-        p->q_off[x][y] = (int)chunks.size();
-        p->q_len[x][y] = (int)cq[ci].q.size();
-        p->class_cost[x][y] = cq[ci].total;
-        chunks.insert(chunks.end(), cq[ci].q.begin(), cq[ci].q.end());
+        const int b0 = cls_start[x], b1 = cls_start[x + 1];
+        const double nb = b1 - b0, nk = cls_start[y + 1] - cls_start[y];
+        // about kTaskChunks 32-ket chunks per task
+        constexpr double kTaskChunks = 2048.0;
+        const double est = (x == y ? nb * nb / 2.0 : nb * nk) / std::max(nmol, 1) / 32.0;
+        const int nt = b1 > b0 ? (int)std::max(1.0, std::min(std::min(nb, 256.0), std::ceil(est / kTaskChunks))) : 0;
+        for (int t = 0; t < nt; ++t) {
+            QueueTask T;
+            T.ci = (int)ci;
+            T.pb0 = b0 + (int)((int64_t)(b1 - b0) * t / nt);
+            T.pb1 = b0 + (int)((int64_t)(b1 - b0) * (t + 1) / nt);
+            tasks.push_back(std::move(T));
+        }
+        task_end[ci] = (int)tasks.size();
     }
-    std::vector<long long> mol_out_ll(std::max(nmol, 1), 0);
+    // heaviest first, bucketed by the binary exponent of the cost: an O(n) order that is all
+    // the load balance needs (a full sort of millions of chunks dominated batches)
+    auto bucket = [](double c) {
+        uint64_t bits;
+        std::memcpy(&bits, &c, sizeof bits);
+        const int e2 = c > 0.0 ? (int)((bits >> 52) & 0x7ff) - 1022 : 1;
+        return std::max(0, std::min(kBuckets - 1, kBuckets - 1 - (e2 + 8)));
+    };
+    auto build_task = [&](QueueTask &T) {
+        const int x = cps[T.ci].first, y = cps[T.ci].second;
+        const bool hgp = p->method[x][y] != MOLINTS_METHOD_RYS;
+        const int width = cp_width[T.ci];
+        const double pcost = kEriPrimCost[x][y];
+        const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
+        const double w = 1.0 + lsum * lsum;
+        int mcur = -1, k0 = 0, k1 = 0;
+        for (int pb = T.pb0; pb < T.pb1; ++pb) {
+            const int m = p->pair_mol[pb];
+            if (m != mcur) {
+                range_of(y, m, k0, k1);
+                mcur = m;
+            }
+            int kbeg = k0, kend = (x == y) ? pb + 1 : k1;
+            if (sharded) {
+                // quartet owner: the higher of the two pairs' max shells
+                const int mp = pr[pb].ms;
+                auto first_ms_at_least = [&](int v) {
+                    return (int)(std::partition_point(pr.begin() + k0, pr.begin() + k1,
+                                                      [v](const PairRec &r) { return r.ms < v; }) -
+                                 pr.begin());
+                };
+                if (mp >= shard_s1) continue;
+                if (x == y) {
+                    if (mp < shard_s0) continue;  // q <= pb in list order: owner is mp
+                } else if (mp >= shard_s0) {
+                    kend = first_ms_at_least(shard_s1);
+                } else {
+                    kbeg = first_ms_at_least(shard_s0);
+                    kend = first_ms_at_least(shard_s1);
+                }
+            }
+            const double wp = w * p->npp_h[pb];
+            bool heavy = hgp;  // this bra's remaining kets may still need a split
+            for (int q0 = kbeg; q0 < kend;) {
+                int n = std::min(width, kend - q0), lg = 0;
+                if (heavy) {
+                    // the kets of a molecule's class run are in descending primitive-pair
+                    // count, so the split only falls along the run: a chunk that starts
+                    // unsplit stays unsplit, and a split chunk ends where the split changes
+                    // (shard plans order by highest shell first; there a heavy ket inside
+                    // an unsplit chunk only runs unsplit)
+                    lg = hgp_split(p->npp_h[pb], p->npp_h[q0], pcost);
+                    n = std::min((32 >> (lg & 7)) * widen, kend - q0);
+                    if (lg)
+                        for (int k = 1; k < n; ++k)
+                            if (hgp_split(p->npp_h[pb], p->npp_h[q0 + k], pcost) != lg) { n = k; break; }
+                    heavy = lg != 0 || sharded;
+                }
+                const double cost = wp * (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
+                T.total += cost;
+                const int b = bucket(cost);
+                T.raw.push_back(make_int4(pb, q0, n | (lg << 16), m));
+                T.bk.push_back((unsigned char)b);
+                ++T.cnt[b];
+                q0 += n;
+            }
+        }
+    };
+    HostPool &hp = HostPool::instance();
+    hp.run((int)tasks.size(), [&](int t) { build_task(tasks[t]); });
+    int64_t nq = 0;
+    for (size_t ci = 0, t0 = 0; ci < cps.size(); t0 = task_end[ci], ++ci) {
+        const int x = cps[ci].first, y = cps[ci].second;
+        p->q_off[x][y] = (int)nq;
+        double total = 0.0;
+        for (int b = 0; b < kBuckets; ++b)
+            for (size_t t = t0; t < (size_t)task_end[ci]; ++t) {
+                tasks[t].base[b] = nq;
+                nq += tasks[t].cnt[b];
+            }
+        for (size_t t = t0; t < (size_t)task_end[ci]; ++t) total += tasks[t].total;
+        p->q_len[x][y] = (int)(nq - p->q_off[x][y]);
+        p->class_cost[x][y] = total;
+    }
+    if (nq > INT32_MAX) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: work queue too long"); }
+    // pinned upload buffer: chunks, then the final pair tables
+    auto al16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t o_info = al16((size_t)nq * sizeof(int4));
+    const size_t o_bnd = o_info + al16((size_t)npair * sizeof(int4));
+    const size_t o_ab = o_bnd + al16((size_t)npair * sizeof(double2));
+    const size_t o_src = o_ab + al16((size_t)npair * sizeof(int2));
+    const size_t o_pbk = o_src + al16((size_t)nkept * sizeof(int));
+    const size_t o_mol = o_pbk + al16((size_t)nkept * sizeof(double));
+    const size_t stage_bytes = o_mol + al16((size_t)std::max(nmol, 1) * sizeof(long long));
+    if ((rc = ctx_stage(ctx, stage_bytes))) { plan_free(p); return rc; }
+    char *stage = ctx->stage;
+    int4 *chunks = reinterpret_cast<int4 *>(stage);
+    hp.run((int)tasks.size(), [&](int t) {
+        QueueTask &T = tasks[t];
+        for (size_t i = 0; i < T.raw.size(); ++i) chunks[T.base[T.bk[i]]++] = T.raw[i];
+    });
+    std::memcpy(stage + o_info, info_h.data(), npair * sizeof(int4));
+    std::memcpy(stage + o_bnd, p->bnd_h.data(), npair * sizeof(double2));
+    std::memcpy(stage + o_ab, ab_h.data(), npair * sizeof(int2));
+    if (nkept > 0) {
+        std::memcpy(stage + o_src, src_h.data(), nkept * sizeof(int));
+        std::memcpy(stage + o_pbk, pbk_h.data(), nkept * sizeof(double));
+    }
+    long long *mol_out_ll = reinterpret_cast<long long *>(stage + o_mol);
+    mol_out_ll[0] = 0;
     for (int m = 0; m < nmol; ++m) mol_out_ll[m] = (long long)p->mol_out_h[m];
     p->plan_ms[2] = ms_since(t_phase);
     t_phase = clk::now();
-    rc = dev_alloc(ctx, &p->chunks, chunks.size(), &p->bytes);
+    rc = dev_alloc(ctx, &p->chunks, (size_t)nq, &p->bytes);
     if (!rc) rc = dev_alloc(ctx, &p->pbk, (size_t)std::max<int64_t>(nkept, 1), &p->bytes);
     if (rc) { plan_free(p); return rc; }
-    if ((e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->bnd, p->bnd_h.data(), npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
-        (nkept > 0 && (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nkept * sizeof(int),
+    if ((e = cudaMemcpyAsync(p->pair_ab, stage + o_ab, npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->info, stage + o_info, npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->bnd, stage + o_bnd, npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
+        (nkept > 0 && (e = cudaMemcpyAsync(p->pp_src, stage + o_src, nkept * sizeof(int),
                                            cudaMemcpyHostToDevice, s))) ||
-        (nkept > 0 && (e = cudaMemcpyAsync(p->pbk, pbk_h.data(), nkept * sizeof(double),
+        (nkept > 0 && (e = cudaMemcpyAsync(p->pbk, stage + o_pbk, nkept * sizeof(double),
                                            cudaMemcpyHostToDevice, s))) ||
-        (chunks.size() > 0 && (e = cudaMemcpyAsync(p->chunks, chunks.data(), chunks.size() * sizeof(int4),
-                                                   cudaMemcpyHostToDevice, s))) ||
-        (e = cudaMemcpyAsync(p->mol_out, mol_out_ll.data(), mol_out_ll.size() * sizeof(long long),
+        (nq > 0 && (e = cudaMemcpyAsync(p->chunks, chunks, (size_t)nq * sizeof(int4),
+                                        cudaMemcpyHostToDevice, s))) ||
+        (e = cudaMemcpyAsync(p->mol_out, mol_out_ll, std::max(nmol, 1) * sizeof(long long),
                              cudaMemcpyHostToDevice, s)) ||
         (e = cudaStreamSynchronize(s))) {
         plan_free(p);
