@@ -306,7 +306,9 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
                                    const double *__restrict__ ncoef, double c0,
                                    const double *__restrict__ pb,
                                    PrimPair *__restrict__ pp, double4 *__restrict__ geo) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    // one warp per shell pair, its lanes over the pair's primitive pairs (up to 7 x 7)
+    const int p = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (p >= npair) return;
     const int2 ab = pair_ab[p];
     const int4 in = info[p];
@@ -315,7 +317,7 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
     const double ABx = Ax - Bx, ABy = Ay - By, ABz = Az - Bz;
     const double rab2 = ABx * ABx + ABy * ABy + ABz * ABz;
     const int pa0 = poff[ab.x], pb0 = poff[ab.y];
-    for (int k = in.x; k < in.x + in.y; ++k) {
+    for (int k = in.x + lane; k < in.x + in.y; k += 32) {
         const int src = pp_src[k];
         const double a = expn[pa0 + (src >> 8)], ca = ncoef[pa0 + (src >> 8)];
         const double b = expn[pb0 + (src & 255)], cb = ncoef[pb0 + (src & 255)];
@@ -336,8 +338,11 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
         r.b = pb ? pb[k] : 0.0;
         pp[k] = r;
     }
-    geo[p] = make_double4(ABx, ABy, ABz, 0.0);
+    if (lane == 0) geo[p] = make_double4(ABx, ABy, ABz, 0.0);
 }
+
+// Blocks of 128 threads for build_pairs_kernel over npair shell pairs (a warp each).
+inline int build_pairs_blocks(int npair) { return (int)(((long long)npair + 3) / 4); }
 
 // Copy the lower triangles of J and K (the digestion accumulates only those) to the upper.
 __global__ void mirror_lower_kernel(double *__restrict__ J, double *__restrict__ K, int n) {
@@ -377,7 +382,7 @@ void launch_build_pairs(int npair, const int2 *pair_ab, const int4 *info, const 
                         const double *xyz, const int *poff, const double *expn,
                         const double *ncoef, PrimPair *pp, double4 *geo, cudaStream_t s) {
     if (npair <= 0) return;
-    build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, pair_ab, info, pp_src, xyz, poff,
+    build_pairs_kernel<<<build_pairs_blocks(npair), 128, 0, s>>>(npair, pair_ab, info, pp_src, xyz, poff,
                                                           expn, ncoef, std::sqrt(2.0) * std::pow(M_PI, 1.25),
                                                           nullptr, pp, geo);
 }
@@ -983,7 +988,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         return cuda_fail(ctx, e, "plan_create upload");
     }
     if (npair > 0) {
-        build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, p->pair_ab, p->info, p->pp_src,
+        build_pairs_kernel<<<build_pairs_blocks(npair), 128, 0, s>>>(npair, p->pair_ab, p->info, p->pp_src,
                                                                p->sh_xyz, p->sh_poff, p->expn,
                                                                p->ncoef, c0, nullptr, p->pp, p->geo);
         for (int c = 0; c < kNumPairClasses; ++c) {
@@ -1311,7 +1316,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     MI_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(int) * kNumPairClasses * kNumPairClasses, s));
     if (p->npair > 0) {
         if (int rc = mark(launches, "build_pairs", 0, s)) return rc;
-        build_pairs_kernel<<<(p->npair + 127) / 128, 128, 0, s>>>(
+        build_pairs_kernel<<<build_pairs_blocks(p->npair), 128, 0, s>>>(
             p->npair, p->pair_ab, p->info, p->pp_src, p->sh_xyz, p->sh_poff, p->expn, p->ncoef,
             std::sqrt(2.0) * std::pow(M_PI, 1.25), p->pbk, p->pp, p->geo);
         if (int rc = mark(launches, "build_pairs", 1, s)) return rc;
