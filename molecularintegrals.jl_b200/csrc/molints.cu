@@ -61,6 +61,8 @@ struct molints_ctx {
     int32_t class_method[kNumPairClasses][kNumPairClasses] = {};  // AUTO choices (0 = default)
     char *stage = nullptr;     // pinned host buffer of plan uploads (work queues, pair tables)
     size_t stage_bytes = 0;
+    cudaEvent_t stage_ev = nullptr;  // recorded after uploads that a plan creation left in flight
+    bool stage_busy = false;
     std::string err;
 };
 
@@ -198,9 +200,14 @@ void dev_free(molints_ctx *ctx, void *p) {
 }
 
 // The pinned upload buffer of the context, grown to at least `bytes` (a pinned source makes
-// the plan uploads asynchronous DMA at full link speed; every plan creation ends with a
-// stream synchronise, so the buffer is free again when the next one starts).
+// the plan uploads asynchronous DMA at full link speed).  A plan creation that returns with its
+// uploads in flight marks the buffer busy; the next one waits for them before writing it.
 int ctx_stage(molints_ctx *ctx, size_t bytes) {
+    if (ctx->stage_busy) {  // the previous plan's uploads may still read the buffer
+        cudaError_t e = cudaEventSynchronize(ctx->stage_ev);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "plan upload buffer");
+        ctx->stage_busy = false;
+    }
     if (ctx->stage_bytes >= bytes) return MOLINTS_OK;
     if (ctx->stage) cudaFreeHost(ctx->stage);
     ctx->stage = nullptr;
@@ -493,6 +500,7 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
     for (int i = 0; ok && i < molints_ctx::kSide; ++i)
         ok = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&ctx->join[i], cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         molints_destroy(ctx);
         return MOLINTS_ERR_CUDA;
@@ -571,6 +579,7 @@ int molints_destroy(molints_ctx *ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
     if (ctx->stage) cudaFreeHost(ctx->stage);
     delete ctx;
     return MOLINTS_OK;
@@ -745,9 +754,11 @@ static void shard_bounds(const molints_basis *b, int shard, int nshards, int *s_
     *hi = tri(tri(first_fn(*s_hi)));
 }
 
+// sync_end == false: return with the final uploads in flight on the context's stream (work
+// queued on that stream afterwards is ordered after them); molints_eri_packed uses it.
 static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                             const molints_options *opts_in, int shard, int nshards,
-                            molints_plan **out);
+                            molints_plan **out, bool sync_end = true);
 
 int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                               const molints_options *opts_in, molints_plan **out) {
@@ -772,7 +783,7 @@ int molints_plan_create_shard(molints_ctx *ctx, const molints_basis *b, const mo
 
 static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                             const molints_options *opts_in, int shard, int nshards,
-                            molints_plan **out) {
+                            molints_plan **out, bool sync_end) {
     if (!ctx || !out || nmol < 0 || (nmol > 0 && !bases))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null argument");
     *out = nullptr;
@@ -1135,7 +1146,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         const int b0 = cls_start[x], b1 = cls_start[x + 1];
         const double nb = b1 - b0, nk = cls_start[y + 1] - cls_start[y];
         // about kTaskChunks 32-ket chunks per task
-        constexpr double kTaskChunks = 2048.0;
+        constexpr double kTaskChunks = 1024.0;
         const double est = (x == y ? nb * nb / 2.0 : nb * nk) / std::max(nmol, 1) / 32.0;
         const int nt = b1 > b0 ? (int)std::max(1.0, std::min(std::min(nb, 256.0), std::ceil(est / kTaskChunks))) : 0;
         for (int t = 0; t < nt; ++t) {
@@ -1143,6 +1154,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             T.ci = (int)ci;
             T.pb0 = b0 + (int)((int64_t)(b1 - b0) * t / nt);
             T.pb1 = b0 + (int)((int64_t)(b1 - b0) * (t + 1) / nt);
+            const size_t guess = (size_t)(1.25 * est / nt) + 64;
+            T.raw.reserve(guess);
+            T.bk.reserve(guess);
             tasks.push_back(std::move(T));
         }
         task_end[ci] = (int)tasks.size();
@@ -1274,10 +1288,11 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                                         cudaMemcpyHostToDevice, s))) ||
         (e = cudaMemcpyAsync(p->mol_out, mol_out_ll, std::max(nmol, 1) * sizeof(long long),
                              cudaMemcpyHostToDevice, s)) ||
-        (e = cudaStreamSynchronize(s))) {
+        (sync_end ? (e = cudaStreamSynchronize(s)) : (e = cudaEventRecord(ctx->stage_ev, s)))) {
         plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
     }
+    if (!sync_end) ctx->stage_busy = true;
     p->plan_ms[3] = ms_since(t_phase);
     ctx->plans.push_back(p);
     *out = p;
@@ -1605,7 +1620,7 @@ int molints_eri_packed(molints_ctx *ctx, const molints_basis *b, const molints_o
     if (nbf < 0) return fail(ctx, MOLINTS_ERR_INVALID, "eri_packed: malformed basis");
     if (!out && molints_npacked(nbf) > 0) return fail(ctx, MOLINTS_ERR_INVALID, "eri_packed: null output");
     molints_plan *p = nullptr;
-    int rc = molints_plan_create(ctx, b, opts, &p);
+    int rc = plan_create_impl(ctx, 1, b, opts, 0, 1, &p, false);
     if (rc) return rc;
     if (p->npacked == 0) {
         if (stats) rc = molints_plan_stats(p, stats);
