@@ -50,6 +50,13 @@ enum molints_boys {
     /* exact F_m (table + Taylor + downward recursion) up to T = 40, asymptotic beyond. */
     MOLINTS_BOYS_EXACT = 1
 };
+/* How the class kernels reach the packed vector.  DIRECT: each integral is stored at its
+ * iindex position.  For an output larger than L2 that costs one read-modify-write of a DRAM
+ * sector per 8-byte store.  TWO_PHASE: each shell quartet's block is stored whole, coalesced,
+ * into a class-major scratch held by the plan (about npacked doubles more); then one pass
+ * writes the packed vector in order from it (whole-molecule plans; shard plans stay DIRECT).
+ * AUTO is DIRECT.  The values are the same either way, bit for bit. */
+enum molints_output { MOLINTS_OUTPUT_AUTO = 0, MOLINTS_OUTPUT_DIRECT = 1, MOLINTS_OUTPUT_TWO_PHASE = 2 };
 
 /* Largest shell angular momentum the engine accepts (f = 3).  Class pairs with an f shell run
  * the Rys kernels (n <= 7 roots). */
@@ -78,7 +85,7 @@ typedef struct molints_options {
     int32_t precision;       /* enum molints_precision */
     int32_t boys;            /* enum molints_boys; the Rys kernels always evaluate the exact
                                 quadrature (there is no T >= 30 branch to follow) */
-    int32_t reserved;
+    int32_t output;          /* enum molints_output */
     /* Both cutoffs compare against B = Qabs_ab * Qabs_cd, where Qabs_ab is the sum over the
      * pair's primitive pairs i of sqrt(max |(a_i b_i|a_i b_i)|).  B bounds the sum of the
      * magnitudes of all primitive contributions to (ab|cd), not only |(ab|cd)|. */

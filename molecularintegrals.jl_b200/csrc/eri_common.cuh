@@ -90,6 +90,11 @@ struct EriQueue {
     int *counter;                 // next chunk; zero at launch
     double screen_cut;            // Qabs_p Qabs_q below this: written as 0
     double fp32_cut;              // R_p R_q below this (MIXED kernels): FP32 VRR
+    // two-phase output (scratch != nullptr): quartet (p, q0 + t) of chunk c stores its whole
+    // block (ma, mb, mc, md row-major) at scratch[chunk_slot[c] + t * block size]; a gather
+    // pass writes the packed vector from the scratch afterwards
+    double *scratch;
+    const long long *chunk_slot;
 };
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {

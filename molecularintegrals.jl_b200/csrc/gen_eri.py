@@ -515,9 +515,16 @@ __global__ void __launch_bounds__(128) eri_queue_{tag}(const EriQueue Q) {{
         if (live && s == 0) {{
             double res[{nout}];
             hrr_{tag}(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_{tag}(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_{tag}(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {{
+                jk_{tag}(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            }} else if (Q.scratch) {{
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * {nout};
+#pragma unroll
+                for (int x = 0; x < {nout}; ++x) dst[x] = res[x];
+            }} else {{
+                store_{tag}(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }}
         }}
         }}
     }}

@@ -12684,9 +12684,16 @@ __global__ void __launch_bounds__(128) eri_queue_dddd(const EriQueue Q) {
         if (live && s == 0) {
             double res[1296];
             hrr_dddd(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_dddd(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_dddd(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_dddd(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 1296;
+#pragma unroll
+                for (int x = 0; x < 1296; ++x) dst[x] = res[x];
+            } else {
+                store_dddd(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

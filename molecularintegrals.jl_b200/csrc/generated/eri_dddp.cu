@@ -5721,9 +5721,16 @@ __global__ void __launch_bounds__(128) eri_queue_dddp(const EriQueue Q) {
         if (live && s == 0) {
             double res[648];
             hrr_dddp(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_dddp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_dddp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_dddp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 648;
+#pragma unroll
+                for (int x = 0; x < 648; ++x) dst[x] = res[x];
+            } else {
+                store_dddp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

@@ -2992,9 +2992,16 @@ __global__ void __launch_bounds__(128) eri_queue_ddpp(const EriQueue Q) {
         if (live && s == 0) {
             double res[324];
             hrr_ddpp(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_ddpp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_ddpp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_ddpp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 324;
+#pragma unroll
+                for (int x = 0; x < 324; ++x) dst[x] = res[x];
+            } else {
+                store_ddpp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

@@ -465,9 +465,16 @@ __global__ void __launch_bounds__(128) eri_queue_ddss(const EriQueue Q) {
         if (live && s == 0) {
             double res[36];
             hrr_ddss(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_ddss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_ddss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_ddss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 36;
+#pragma unroll
+                for (int x = 0; x < 36; ++x) dst[x] = res[x];
+            } else {
+                store_ddss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

@@ -282,9 +282,16 @@ __global__ void __launch_bounds__(128) eri_queue_dpss(const EriQueue Q) {
         if (live && s == 0) {
             double res[18];
             hrr_dpss(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_dpss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_dpss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_dpss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 18;
+#pragma unroll
+                for (int x = 0; x < 18; ++x) dst[x] = res[x];
+            } else {
+                store_dpss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

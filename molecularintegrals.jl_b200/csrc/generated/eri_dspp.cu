@@ -541,9 +541,16 @@ __global__ void __launch_bounds__(128) eri_queue_dspp(const EriQueue Q) {
         if (live && s == 0) {
             double res[54];
             hrr_dspp(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_dspp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_dspp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_dspp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 54;
+#pragma unroll
+                for (int x = 0; x < 54; ++x) dst[x] = res[x];
+            } else {
+                store_dspp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

@@ -682,9 +682,16 @@ __global__ void __launch_bounds__(128) eri_queue_fdss(const EriQueue Q) {
         if (live && s == 0) {
             double res[60];
             hrr_fdss(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_fdss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_fdss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_fdss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 60;
+#pragma unroll
+                for (int x = 0; x < 60; ++x) dst[x] = res[x];
+            } else {
+                store_fdss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

@@ -1176,9 +1176,16 @@ __global__ void __launch_bounds__(128) eri_queue_ffss(const EriQueue Q) {
         if (live && s == 0) {
             double res[100];
             hrr_ffss(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_ffss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_ffss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_ffss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 100;
+#pragma unroll
+                for (int x = 0; x < 100; ++x) dst[x] = res[x];
+            } else {
+                store_ffss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

@@ -227,9 +227,16 @@ __global__ void __launch_bounds__(128) eri_queue_fsss(const EriQueue Q) {
         if (live && s == 0) {
             double res[10];
             hrr_fsss(Q.pairs, p, q, acc, res);
-            if constexpr (JK) jk_fsss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            else store_fsss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
-                             p == q, res);
+            if constexpr (JK) {
+                jk_fsss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
+            } else if (Q.scratch) {
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 10;
+#pragma unroll
+                for (int x = 0; x < 10; ++x) dst[x] = res[x];
+            } else {
+                store_fsss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
+                            p == q, res);
+            }
         }
         }
     }

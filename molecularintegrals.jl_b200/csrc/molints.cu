@@ -103,6 +103,15 @@ struct molints_plan {
     int *counters = nullptr;           // one per class pair, zeroed by every execute
     long long *mol_out = nullptr;
     double *qcon = nullptr;  // contracted Schwarz bounds, filled on demand by plan_schwarz
+    // two-phase output (molints_output): the class kernels store whole quartet blocks into a
+    // class-major scratch, a gather pass writes the packed vector in order from it
+    int two_phase = 0;
+    double *scratch = nullptr;         // per (class pair, molecule) region of quartet blocks
+    long long *chunk_slot = nullptr;   // per chunk: scratch offset of its first quartet's block
+    int2 *g_fn = nullptr;              // per function (all molecules): {shell in molecule, component}
+    int *g_pair = nullptr;             // per molecule shell pair I >= J: pos << 5 | class << 1 | A == J
+    long long *g_region = nullptr;     // per (x, y, molecule): {scratch offset, first bra, first ket, kets}
+    long long *g_mol = nullptr;        // per molecule: {first function, first pair entry, packed offset, packed}
     int64_t bytes = 0;
     int n_launches = 0;
     double plan_ms[4] = {0, 0, 0, 0};  // plan creation phases (molints_stats.plan_ms)
@@ -350,6 +359,99 @@ __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
 
 // Blocks of 128 threads for build_pairs_kernel over npair shell pairs (a warp each).
 inline int build_pairs_blocks(int npair) { return (int)(((long long)npair + 3) / 4); }
+
+// Cartesian components of each pair class's two shells, for the gather pass.
+__constant__ int c_pair_na[kNumPairClasses] = {
+#define MI_NC(c) (kPairClassLa[c] + 1) * (kPairClassLa[c] + 2) / 2
+    MI_NC(0), MI_NC(1), MI_NC(2), MI_NC(3), MI_NC(4), MI_NC(5), MI_NC(6), MI_NC(7), MI_NC(8), MI_NC(9), MI_NC(10)};
+#undef MI_NC
+__constant__ int c_pair_nb[kNumPairClasses] = {
+#define MI_NC(c) (kPairClassLb[c] + 1) * (kPairClassLb[c] + 2) / 2
+    MI_NC(0), MI_NC(1), MI_NC(2), MI_NC(3), MI_NC(4), MI_NC(5), MI_NC(6), MI_NC(7), MI_NC(8), MI_NC(9), MI_NC(10)};
+#undef MI_NC
+static_assert(kNumPairClasses == 11, "c_pair_na / c_pair_nb list every pair class");
+
+// n with n(n+1)/2 <= t < (n+1)(n+2)/2, from an FP32 square root and an exact integer fix-up
+// (t < 2^31 is off by at most a few units in n).
+__device__ __forceinline__ long long untri_f(long long t) {
+    long long n = (long long)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+    while ((n + 1) * (n + 2) / 2 <= t) ++n;
+    while (n > 0 && n * (n + 1) / 2 > t) --n;
+    return n;
+}
+
+constexpr int kGatherThreads = 256, kGatherPerThread = 8;
+
+// Second phase of the two-phase output: every packed entry t (in order, so the stores are
+// coalesced) from the scratch block of the quartet and component the direct path would have
+// stored it from.  Row ij >= column kl; their shell pairs P (from ij) and Q (from kl); the
+// quartet's bra is the pair of the higher class, or of the later list position within a class
+// (P for the diagonal quartet P == Q); a pair's components are taken in its A, B orientation,
+// with the larger component first within a same-shell pair, as the direct store conditions pick.
+// A block covers kGatherThreads * kGatherPerThread consecutive entries; its first row comes
+// from one FP64 square root, and each thread walks its entries' rows forward from there.
+__global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
+    double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ fn,
+    const int *__restrict__ pairs, const long long *__restrict__ region, const long long *__restrict__ mol,
+    int nmol, long long npacked) {
+    constexpr long long kTile = (long long)kGatherThreads * kGatherPerThread;
+    for (long long t0 = (long long)blockIdx.x * kTile; t0 < npacked; t0 += (long long)gridDim.x * kTile) {
+        // the tile's first molecule (binary search over the molecules' packed offsets)
+        int m = 0;
+        if (nmol > 1) {
+            int lo = 0, hi = nmol - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&mol[4 * mid + 2]) <= t0) lo = mid; else hi = mid - 1;
+            }
+            m = lo;
+        }
+        long long mol_lo = __ldg(&mol[4 * m + 2]), mol_hi = mol_lo + __ldg(&mol[4 * m + 3]);
+        long long row = -1, i = 0, j = 0;
+        for (int e = 0; e < kGatherPerThread; ++e) {
+            const long long t = t0 + threadIdx.x + (long long)e * kGatherThreads;
+            if (t >= npacked) break;
+            while (t >= mol_hi) {  // next molecule
+                ++m;
+                mol_lo = mol_hi;
+                mol_hi = mol_lo + __ldg(&mol[4 * m + 3]);
+                row = -1;
+            }
+            const long long tl = t - mol_lo;
+            if (row < 0) {
+                row = (long long)((sqrt(8.0 * (double)tl + 1.0) - 1.0) * 0.5);
+                while ((row + 1) * (row + 2) / 2 <= tl) ++row;
+                while (row * (row + 1) / 2 > tl) --row;
+                i = untri_f(row);
+                j = row - i * (i + 1) / 2;
+            }
+            while ((row + 1) * (row + 2) / 2 <= tl) {  // rows grow: a step or two at most
+                ++row;
+                if (++j > i) { ++i; j = 0; }
+            }
+            const long long kl = tl - row * (row + 1) / 2;
+            const long long k = untri_f(kl), l = kl - k * (k + 1) / 2;
+            const long long fb = __ldg(&mol[4 * m]), pb = __ldg(&mol[4 * m + 1]);
+            const int2 fi = __ldg(&fn[fb + i]), fj = __ldg(&fn[fb + j]), fk = __ldg(&fn[fb + k]), fl = __ldg(&fn[fb + l]);
+            const int P = __ldg(&pairs[pb + (long long)fi.x * (fi.x + 1) / 2 + fj.x]);
+            const int Q = __ldg(&pairs[pb + (long long)fk.x * (fk.x + 1) / 2 + fl.x]);
+            const int posP = P >> 5, clsP = (P >> 1) & 15, posQ = Q >> 5, clsQ = (Q >> 1) & 15;
+            // components in each pair's A, B orientation
+            const int pa = (P & 1) ? fj.y : fi.y, pbc = (P & 1) ? fi.y : fj.y;
+            const int qa = (Q & 1) ? fl.y : fk.y, qb = (Q & 1) ? fk.y : fl.y;
+            const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
+            const int x = braP ? clsP : clsQ, y = braP ? clsQ : clsP;
+            const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
+            const int ma = braP ? pa : qa, mb = braP ? pbc : qb, mc = braP ? qa : pa, md = braP ? qb : pbc;
+            const long long *rg = region + 4 * (((long long)x * kNumPairClasses + y) * nmol + m);
+            const long long db = bpos - __ldg(&rg[1]), dk = kpos - __ldg(&rg[2]);
+            const long long slot = (x == y) ? db * (db + 1) / 2 + dk : db * __ldg(&rg[3]) + dk;
+            const int na = c_pair_na[x], nb = c_pair_nb[x], nc = c_pair_na[y], nd = c_pair_nb[y];
+            const long long blk = (long long)na * nb * nc * nd;
+            out[t] = __ldg(&scratch[__ldg(&rg[0]) + slot * blk + ((ma * nb + mb) * nc + mc) * nd + md]);
+        }
+    }
+}
 
 // Copy the lower triangles of J and K (the digestion accumulates only those) to the upper.
 __global__ void mirror_lower_kernel(double *__restrict__ J, double *__restrict__ K, int n) {
@@ -661,7 +763,8 @@ static void plan_release_device(molints_plan *p) {
     for (cudaEvent_t e : p->prof_ev) cudaEventDestroy(e);
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
-                    p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon};
+                    p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
+                    p->scratch, p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
     p->ctx = nullptr;
@@ -798,6 +901,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown method");
     if (!(opts.fp32_cutoff >= 0.0) || !(opts.screen_cutoff >= 0.0) || !(opts.prim_cutoff >= 0.0))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: cutoffs must be >= 0");
+    if (opts.output != MOLINTS_OUTPUT_AUTO && opts.output != MOLINTS_OUTPUT_DIRECT &&
+        opts.output != MOLINTS_OUTPUT_TWO_PHASE)
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: unknown output mode");
     using clk = std::chrono::steady_clock;
     auto ms_since = [](clk::time_point t0) {
         return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
@@ -835,6 +941,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     }
     p->mol_nshell.resize(nmol);
     p->nbf0 = nmol > 0 ? mol_nbf[0] : 0;
+    // two-phase output on request (whole-molecule plans only); AUTO is DIRECT: with the
+    // scratch in bra-major, primitive-count order the gather pass costs what it saves
+    p->two_phase = nshards == 1 && nmol > 0 && opts.output == MOLINTS_OUTPUT_TWO_PHASE;
     // method per class pair: Rys where no HGP kernel exists (an f shell), else the request
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
@@ -1129,6 +1238,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         int ci = 0, pb0 = 0, pb1 = 0;
         std::vector<int4> raw;
         std::vector<unsigned char> bk;
+        std::vector<long long> slot;  // two-phase: scratch offset of each chunk's first block
         int64_t cnt[kBuckets] = {};
         int64_t base[kBuckets] = {};
         double total = 0.0;
@@ -1136,6 +1246,32 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<std::pair<int, int>> cps;
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) cps.push_back({x, y});
+    // two-phase scratch: per (class pair, molecule) a region of quartet blocks, bra-major
+    // (the triangle q <= p for equal classes); region_h[((x nc + y) nmol + m) 4 ..] =
+    // {offset in doubles, first bra pair, first ket pair, ket pairs}
+    if (npair >= (1 << 26)) p->two_phase = 0;  // the gather's pair entries hold the position in 26 bits
+    auto ncomp_of = [](int x, int y) {
+        return (int64_t)ncart(kPairClassLa[x]) * ncart(kPairClassLb[x]) * ncart(kPairClassLa[y]) * ncart(kPairClassLb[y]);
+    };
+    std::vector<long long> region_h;
+    int64_t scratch_len = 0;
+    if (p->two_phase) {
+        region_h.assign((size_t)kNumPairClasses * kNumPairClasses * nmol * 4, 0);
+        for (const auto &cp : cps)
+            for (int m = 0; m < nmol; ++m) {
+                const int x = cp.first, y = cp.second;
+                int b0, b1, k0, k1;
+                range_of(x, m, b0, b1);
+                range_of(y, m, k0, k1);
+                const int64_t nb = b1 - b0, nk = k1 - k0;
+                long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * 4];
+                rg[0] = scratch_len;
+                rg[1] = b0;
+                rg[2] = k0;
+                rg[3] = nk;
+                scratch_len += (x == y ? nb * (nb + 1) / 2 : nb * nk) * ncomp_of(x, y);
+            }
+    }
     std::vector<QueueTask> tasks;
     std::vector<int> task_end(cps.size(), 0), cp_width(cps.size(), 32 * widen);
     for (size_t ci = 0; ci < cps.size(); ++ci)
@@ -1157,6 +1293,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             const size_t guess = (size_t)(1.25 * est / nt) + 64;
             T.raw.reserve(guess);
             T.bk.reserve(guess);
+            if (p->two_phase) T.slot.reserve(guess);
             tasks.push_back(std::move(T));
         }
         task_end[ci] = (int)tasks.size();
@@ -1224,6 +1361,11 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 const int b = bucket(cost);
                 T.raw.push_back(make_int4(pb, q0, n | (lg << 16), m));
                 T.bk.push_back((unsigned char)b);
+                if (p->two_phase) {
+                    const long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * 4];
+                    const long long db = pb - rg[1], dk = q0 - rg[2];
+                    T.slot.push_back(rg[0] + (x == y ? db * (db + 1) / 2 + dk : db * rg[3] + dk) * ncomp_of(x, y));
+                }
                 ++T.cnt[b];
                 q0 += n;
             }
@@ -1254,14 +1396,55 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     const size_t o_src = o_ab + al16((size_t)npair * sizeof(int2));
     const size_t o_pbk = o_src + al16((size_t)nkept * sizeof(int));
     const size_t o_mol = o_pbk + al16((size_t)nkept * sizeof(double));
-    const size_t stage_bytes = o_mol + al16((size_t)std::max(nmol, 1) * sizeof(long long));
+    // two-phase: chunk slots and the gather tables (functions, shell pairs, regions, molecules)
+    int64_t nfn_all = 0, npe_all = 0;
+    for (int m = 0; m < nmol; ++m) {
+        nfn_all += mol_nbf[m];
+        npe_all += (int64_t)bases[m].nshell * (bases[m].nshell + 1) / 2;
+    }
+    const bool tp = p->two_phase != 0;
+    const size_t o_slot = o_mol + al16((size_t)std::max(nmol, 1) * sizeof(long long));
+    const size_t o_gfn = o_slot + (tp ? al16((size_t)nq * sizeof(long long)) : 0);
+    const size_t o_gpair = o_gfn + (tp ? al16((size_t)nfn_all * sizeof(int2)) : 0);
+    const size_t o_greg = o_gpair + (tp ? al16((size_t)npe_all * sizeof(int)) : 0);
+    const size_t o_gmol = o_greg + (tp ? al16(region_h.size() * sizeof(long long)) : 0);
+    const size_t stage_bytes = o_gmol + (tp ? al16((size_t)nmol * 4 * sizeof(long long)) : 0);
     if ((rc = ctx_stage(ctx, stage_bytes))) { plan_free(p); return rc; }
     char *stage = ctx->stage;
     int4 *chunks = reinterpret_cast<int4 *>(stage);
+    long long *slots = tp ? reinterpret_cast<long long *>(stage + o_slot) : nullptr;
     hp.run((int)tasks.size(), [&](int t) {
         QueueTask &T = tasks[t];
-        for (size_t i = 0; i < T.raw.size(); ++i) chunks[T.base[T.bk[i]]++] = T.raw[i];
+        for (size_t i = 0; i < T.raw.size(); ++i) {
+            const int64_t d = T.base[T.bk[i]]++;
+            chunks[d] = T.raw[i];
+            if (slots) slots[d] = T.slot[i];
+        }
     });
+    if (tp) {
+        int2 *gfn = reinterpret_cast<int2 *>(stage + o_gfn);
+        int *gpair = reinterpret_cast<int *>(stage + o_gpair);
+        long long *gmol = reinterpret_cast<long long *>(stage + o_gmol);
+        std::vector<int64_t> pbase(nmol + 1, 0);
+        for (int m = 0, fb = 0; m < nmol; ++m) {
+            pbase[m + 1] = pbase[m] + (int64_t)bases[m].nshell * (bases[m].nshell + 1) / 2;
+            for (int sl = 0; sl < bases[m].nshell; ++sl) {
+                const int g = shell_off[m] + sl;
+                for (int c = 0; c < ncart(L[g]); ++c) gfn[fb + fn_off[g] + c] = make_int2(sl, c);
+            }
+            gmol[4 * m] = fb;
+            gmol[4 * m + 1] = pbase[m];
+            gmol[4 * m + 2] = (long long)p->mol_out_h[m];
+            gmol[4 * m + 3] = (long long)molints_npacked(mol_nbf[m]);
+            fb += (int)mol_nbf[m];
+        }
+        for (int k = 0; k < npair; ++k) {
+            const int m = pr[k].mol;
+            const int swapped = (pr[k].a - shell_off[m]) != pr[k].ms;  // A is the lower shell J
+            gpair[pbase[m] + pr[k].ref] = (k << 5) | (pr[k].cls << 1) | swapped;
+        }
+        std::memcpy(stage + o_greg, region_h.data(), region_h.size() * sizeof(long long));
+    }
     std::memcpy(stage + o_info, info_h.data(), npair * sizeof(int4));
     std::memcpy(stage + o_bnd, p->bnd_h.data(), npair * sizeof(double2));
     std::memcpy(stage + o_ab, ab_h.data(), npair * sizeof(int2));
@@ -1276,7 +1459,28 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     t_phase = clk::now();
     rc = dev_alloc(ctx, &p->chunks, (size_t)nq, &p->bytes);
     if (!rc) rc = dev_alloc(ctx, &p->pbk, (size_t)std::max<int64_t>(nkept, 1), &p->bytes);
+    if (!rc && tp) {
+        rc = dev_alloc(ctx, &p->scratch, (size_t)std::max<int64_t>(scratch_len, 1), &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->chunk_slot, (size_t)std::max<int64_t>(nq, 1), &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->g_fn, (size_t)std::max<int64_t>(nfn_all, 1), &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->g_pair, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
+    }
     if (rc) { plan_free(p); return rc; }
+    if (tp && ((nq > 0 && (e = cudaMemcpyAsync(p->chunk_slot, stage + o_slot, (size_t)nq * sizeof(long long),
+                                                cudaMemcpyHostToDevice, s))) ||
+               (nfn_all > 0 && (e = cudaMemcpyAsync(p->g_fn, stage + o_gfn, (size_t)nfn_all * sizeof(int2),
+                                                     cudaMemcpyHostToDevice, s))) ||
+               (npe_all > 0 && (e = cudaMemcpyAsync(p->g_pair, stage + o_gpair, (size_t)npe_all * sizeof(int),
+                                                     cudaMemcpyHostToDevice, s))) ||
+               (e = cudaMemcpyAsync(p->g_region, stage + o_greg, region_h.size() * sizeof(long long),
+                                    cudaMemcpyHostToDevice, s)) ||
+               (e = cudaMemcpyAsync(p->g_mol, stage + o_gmol, (size_t)nmol * 4 * sizeof(long long),
+                                    cudaMemcpyHostToDevice, s)))) {
+        plan_free(p);
+        return cuda_fail(ctx, e, "plan_create upload");
+    }
     if ((e = cudaMemcpyAsync(p->pair_ab, stage + o_ab, npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, stage + o_info, npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->bnd, stage + o_bnd, npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
@@ -1369,6 +1573,10 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         Q.counter = p->counters + x * kNumPairClasses + y;
         Q.screen_cut = p->opts.screen_cutoff;
         Q.fp32_cut = p->opts.fp32_cutoff;
+        if (p->two_phase && !jk.J) {
+            Q.scratch = p->scratch;
+            Q.chunk_slot = p->chunk_slot + p->q_off[x][y];
+        }
         // HGP: one warp per chunk, four per block; Rys: the launcher divides by its groups/block
         const int grid = rys ? occ * ctx->num_sms
                              : (int)std::min<long long>((long long)occ * ctx->num_sms, (Q.nchunks + 3) / 4);
@@ -1382,6 +1590,16 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     for (int i = 0; i < nside; ++i) {
         MI_CUDA(ctx, cudaEventRecord(ctx->join[i], ctx->side[i]));
         MI_CUDA(ctx, cudaStreamWaitEvent(s, ctx->join[i], 0));
+    }
+    if (p->two_phase && !jk.J && p->npacked > 0) {
+        // second phase: the packed vector in order from the scratch blocks
+        if (int rc = mark(launches, "gather_packed", 0, s)) return rc;
+        constexpr long long kTile = (long long)kGatherThreads * kGatherPerThread;
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, (p->npacked + kTile - 1) / kTile);
+        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, p->scratch, p->g_fn, p->g_pair,
+                                                             p->g_region, p->g_mol, p->nmol, p->npacked);
+        if (int rc = mark(launches, "gather_packed", 1, s)) return rc;
+        ++launches;
     }
     MI_CUDA(ctx, cudaGetLastError());
     if (timing) MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));

@@ -406,7 +406,11 @@ __device__ __forceinline__ void rys_queue_body(const EriQueue &Q, const RysTab &
                                         : rys_monomial(m - kRysNmono, gk.x, gk.y, gk.z);
             group_sync<C::G>(gid);
             const bool dab = ib.z == ib.w, dcd = ik.z == ik.w, same = p == q;
+            // two-phase output: the quartet's whole block, (bra component, ket component) row-major
+            double *__restrict__ blk = (Q.scratch && !Q.jk.J)
+                ? Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(q - ch.y) * (C::NAB * C::NCD) : nullptr;
             rys_hrr<C, false>(T, work, work + C::NBLK, mono, lane, gid, [&](int r, int s, double v) {
+                if (blk) { blk[r * C::NCD + s] = v; return; }
                 const int ia = r / C::NB, jb = r - ia * C::NB, ic = s / C::ND, jd = s - ic * C::ND;
                 if ((dab && ia < jb) || (dcd && ic < jd)) return;
                 const long long ij = pair_index(ib.z + ia, ib.w + jb), kl = pair_index(ik.z + ic, ik.w + jd);

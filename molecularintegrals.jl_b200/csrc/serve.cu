@@ -91,15 +91,26 @@ void Server::destroy_resources() {
 }
 
 // Device bytes a plan of this basis holds (an upper bound of molints_plan_create's tables:
-// shells, primitives, pairs, primitive pairs, chunk queues).
-int64_t plan_bytes(const molints_basis &b) {
+// shells, primitives, pairs, primitive pairs, chunk queues, and for a two-phase output the
+// scratch of quartet blocks: the sum over shell-pair pairs P >= Q of n_P n_Q components, at
+// most (S^2 + S n_max) / 2 with S = sum_P n_P).
+int64_t plan_bytes(const molints_basis &b, const molints_options &o, int64_t npacked) {
     int64_t nprim = 0, nall = 0;
     for (int s = 0; s < b.nshell; ++s) nprim = std::max<int64_t>(nprim, b.prim_off[s] + b.nprim[s]);
     for (int i = 0; i < b.nshell; ++i)
         for (int j = 0; j <= i; ++j) nall += (int64_t)b.nprim[i] * b.nprim[j];
     const int64_t npair = (int64_t)b.nshell * (b.nshell + 1) / 2;
     const int64_t nchunk = npair * (npair + 1) / 2 / 32 + npair * 2;
-    return 40 * (int64_t)b.nshell + 24 * nprim + 88 * npair + 100 * nall + 16 * nchunk + (4 << 20);
+    int64_t scratch = 0;
+    (void)npacked;
+    if (o.output == MOLINTS_OUTPUT_TWO_PHASE) {
+        double S = 0.0;
+        for (int i = 0; i < b.nshell; ++i)
+            for (int j = 0; j <= i; ++j)
+                S += (double)((b.L[i] + 1) * (b.L[i] + 2) / 2) * ((b.L[j] + 1) * (b.L[j] + 2) / 2);
+        scratch = (int64_t)(8.0 * (S * S + S * 100.0) / 2.0) + 8 * nchunk;
+    }
+    return 40 * (int64_t)b.nshell + 24 * nprim + 88 * npair + 100 * nall + 16 * nchunk + scratch + (4 << 20);
 }
 
 void Server::worker(int slot) {
@@ -333,7 +344,7 @@ int molints_submit(molints_ctx *ctx, const molints_basis *b, const molints_optio
     if (opts) r->opts = *opts; else molints_default_options(&r->opts);
     r->npacked = molints_npacked(nbf);
     r->need_out = r->npacked * (int64_t)sizeof(double);
-    r->need_plan = plan_bytes(r->basis);
+    r->need_plan = plan_bytes(r->basis, r->opts, r->npacked);
     r->t_submit = now_s();
     {
         std::lock_guard<std::mutex> lk(S->mu);

@@ -61,12 +61,14 @@ class Basis(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("boys", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("boys", ctypes.c_int32), ("output", ctypes.c_int32),
                 ("fp32_cutoff", ctypes.c_double), ("screen_cutoff", ctypes.c_double),
                 ("prim_cutoff", ctypes.c_double)]
 
 
 PRIM_CUTOFF = 1e-18
+# enum molints_output: how the class kernels reach the packed vector
+OUTPUT_AUTO, OUTPUT_DIRECT, OUTPUT_TWO_PHASE = 0, 1, 2
 
 
 class Stats(ctypes.Structure):
@@ -163,8 +165,8 @@ class _BasisArrays:
 
 
 def make_options(precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0, screen_cutoff=0.0,
-                 method=METHOD_AUTO, prim_cutoff=PRIM_CUTOFF) -> Options:
-    return Options(method, precision, boys, 0, float(fp32_cutoff), float(screen_cutoff),
+                 method=METHOD_AUTO, prim_cutoff=PRIM_CUTOFF, output=OUTPUT_AUTO) -> Options:
+    return Options(method, precision, boys, int(output), float(fp32_cutoff), float(screen_cutoff),
                    float(prim_cutoff))
 
 
@@ -318,7 +320,7 @@ class Engine:
 
     def eri_packed(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
                    screen_cutoff=0.0, out: np.ndarray | None = None, with_stats=False,
-                   prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO):
+                   prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO, output=OUTPUT_AUTO):
         """The packed iindex vector of all unique integrals, into a host array."""
         arrs = _BasisArrays(shells)
         if out is None:
@@ -330,7 +332,7 @@ class Engine:
             return (out, st.as_dict()) if with_stats else out
         if out.dtype != np.float64 or out.size != shells.npacked or not out.flags.c_contiguous:
             raise ValueError("out must be a contiguous float64 array of npacked elements")
-        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff, output)
         st = Stats()
         self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
                                                 _ptr(out), 0, ctypes.byref(st) if with_stats else None))
@@ -338,18 +340,19 @@ class Engine:
 
     def eri_packed_device(self, shells, out_device_ptr: int, precision=FP64, boys=BOYS_REFERENCE,
                           fp32_cutoff=0.0, screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF,
-                          method=METHOD_AUTO):
+                          method=METHOD_AUTO, output=OUTPUT_AUTO):
         arrs = _BasisArrays(shells)
-        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff)
+        opts = make_options(precision, boys, fp32_cutoff, screen_cutoff, method, prim_cutoff, output)
         st = Stats()
         self._check(self.lib.molints_eri_packed(self.ctx, ctypes.byref(arrs.c), ctypes.byref(opts),
                                                 ctypes.c_void_p(out_device_ptr), 1, ctypes.byref(st)))
         return st.as_dict()
 
     def plan(self, shells, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
-             screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO) -> Plan:
+             screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO,
+             output=OUTPUT_AUTO) -> Plan:
         return Plan(self, shells, make_options(precision, boys, fp32_cutoff, screen_cutoff,
-                                               method, prim_cutoff))
+                                               method, prim_cutoff, output))
 
     def plan_shard(self, shells, shard: int, nshards: int, precision=FP64, boys=BOYS_REFERENCE,
                    fp32_cutoff=0.0, screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF,
@@ -360,10 +363,11 @@ class Engine:
                                                method, prim_cutoff), shard=(shard, nshards))
 
     def plan_batch(self, shells_list, precision=FP64, boys=BOYS_REFERENCE, fp32_cutoff=0.0,
-                   screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO) -> Plan:
+                   screen_cutoff=0.0, prim_cutoff=PRIM_CUTOFF, method=METHOD_AUTO,
+                   output=OUTPUT_AUTO) -> Plan:
         """One plan over several molecules: a single execute computes all of them."""
         return Plan(self, list(shells_list), make_options(precision, boys, fp32_cutoff,
-                                                          screen_cutoff, method, prim_cutoff))
+                                                          screen_cutoff, method, prim_cutoff, output))
 
     def set_class_methods(self, table=None):
         """Per class pair method for METHOD_AUTO plans: ``table[(x, y)] = METHOD_HGP or

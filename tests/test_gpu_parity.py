@@ -118,6 +118,52 @@ def test_split_valence_24_full(eng, oracle):
     assert excess.max() < TOL_FP64, (excess.max(), int(np.argmax(excess)))
 
 
+def test_two_phase_output_equals_direct(eng):
+    """The two-phase output (quartet blocks into a class-major scratch, then the packed vector
+    gathered in order) gives the direct path's vector bit for bit: HGP and Rys classes (an f
+    molecule), FP64 and MIXED, a batch plan over several molecules, every entry written (NaN
+    sentinel), and J/K digested from a two-phase plan."""
+    import torch
+    from molints_b200 import engine
+    TP, DIR = engine.OUTPUT_TWO_PHASE, engine.OUTPUT_DIRECT
+    for sh in (mi.config2(), _f_molecule(7), _rand_basis(105, 2)):
+        for prec, cut in ((engine.FP64, 0.0), (engine.MIXED, 1e-3)):
+            a = eng.eri_packed(sh, precision=prec, fp32_cutoff=cut, output=DIR)
+            b = eng.eri_packed(sh, precision=prec, fp32_cutoff=cut, output=TP)
+            assert np.array_equal(a, b)
+    mols = [mi.config2(), mi.config0(), _rand_basis(106, 2), _f_molecule(8)]
+    outs = []
+    for mode in (DIR, TP):
+        plan = eng.plan_batch(mols, output=mode)
+        out = torch.full((plan.npacked,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        eng.set_stream(torch.cuda.current_stream().cuda_stream)
+        try:
+            plan.execute(out.data_ptr())
+            torch.cuda.synchronize()
+        finally:
+            eng.set_stream(None)
+        outs.append(out.cpu().numpy())
+        plan.close()
+    assert not np.isnan(outs[1]).any() and np.array_equal(outs[0], outs[1])
+    sh = _f_molecule(9)
+    n = sh.nbf
+    rng = np.random.default_rng(3)
+    A = rng.normal(size=(n, n))
+    D = torch.from_numpy((A + A.T) / n).cuda()
+    res = []
+    for mode in (DIR, TP):
+        plan = eng.plan(sh, output=mode)
+        J, K = torch.empty_like(D), torch.empty_like(D)
+        plan.jk(D.data_ptr(), J.data_ptr(), K.data_ptr())
+        torch.cuda.synchronize()
+        res.append((J.cpu().numpy(), K.cpu().numpy()))
+        plan.close()
+    scale = max(1.0, np.abs(res[0][0]).max(), np.abs(res[0][1]).max())
+    assert np.max(np.abs(res[0][0] - res[1][0])) < 1e-12 * scale
+    assert np.max(np.abs(res[0][1] - res[1][1])) < 1e-12 * scale
+
+
 @pytest.mark.parametrize("seed,lmax", [(101, 0), (102, 1), (103, 2), (104, 2)])
 def test_random_bases_against_huzinaga(eng, oracle, seed, lmax):
     from molints_b200 import engine
