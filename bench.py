@@ -49,18 +49,57 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """SM clocks and clock-event (throttle) reasons of this process's GPU while the timed region
+    runs.  NVML is polled every millisecond from a thread, so even a timed region of a few
+    milliseconds gets samples; the GPU is found by its UUID, which stays right when
+    CUDA_VISIBLE_DEVICES renumbers the devices.  Without NVML, nvidia-smi is sampled every 200
+    ms instead.  Reads only; no GPU setting is changed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.nvml = None
+        self.thread = None
+        self.stop = False
+        self.samples = []  # (sm MHz, max sm MHz, reason bits)
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def __enter__(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop:
+                    self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
+                                         nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    time.sleep(0.001)
+
+            self.nvml = nv
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -74,6 +113,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop = True
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -82,6 +124,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.nvml is not None:
+            sm = [x[0] for x in self.samples]
+            reasons = {n for n, attr in self.REASONS for x in self.samples
+                       if x[2] & getattr(self.nvml, attr, 0)}
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": max(x[1] for x in self.samples) if sm else None,
+                    "samples": len(sm), "source": "nvml, 1 ms", "reasons": sorted(reasons)}
         if not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
         sm, smax, reasons = [], [], set()
@@ -101,7 +150,7 @@ class ClockSampler:
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms", "reasons": sorted(reasons)}
 
 
 def cpu_reference_rate(shells, threads: int, min_seconds: float):
