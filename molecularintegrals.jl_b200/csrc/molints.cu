@@ -1234,7 +1234,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     // chunk goes straight to its place in the pinned upload buffer -- class pairs in order, in a
     // class pair the heaviest bucket first, in a bucket the task and chunk order.
     constexpr int kBuckets = 64;
-    struct QueueTask {
+    // one cache-line-aligned record per task: the tasks run on different threads and each
+    // bumps its own vectors on every chunk (no line is shared between two tasks)
+    struct alignas(128) QueueTask {
         int ci = 0, pb0 = 0, pb1 = 0;
         std::vector<int4> raw;
         std::vector<unsigned char> bk;
@@ -1314,6 +1316,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
         const double w = 1.0 + lsum * lsum;
         int mcur = -1, k0 = 0, k1 = 0;
+        double total = 0.0;            // accumulated here, stored once at the end
+        int64_t cnt[kBuckets] = {};
         for (int pb = T.pb0; pb < T.pb1; ++pb) {
             const int m = p->pair_mol[pb];
             if (m != mcur) {
@@ -1357,7 +1361,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                     heavy = lg != 0 || sharded;
                 }
                 const double cost = wp * (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
-                T.total += cost;
+                total += cost;
                 const int b = bucket(cost);
                 T.raw.push_back(make_int4(pb, q0, n | (lg << 16), m));
                 T.bk.push_back((unsigned char)b);
@@ -1366,10 +1370,12 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                     const long long db = pb - rg[1], dk = q0 - rg[2];
                     T.slot.push_back(rg[0] + (x == y ? db * (db + 1) / 2 + dk : db * rg[3] + dk) * ncomp_of(x, y));
                 }
-                ++T.cnt[b];
+                ++cnt[b];
                 q0 += n;
             }
         }
+        T.total = total;
+        std::memcpy(T.cnt, cnt, sizeof cnt);
     };
     HostPool &hp = HostPool::instance();
     hp.run((int)tasks.size(), [&](int t) { build_task(tasks[t]); });
