@@ -54,9 +54,13 @@ enum molints_boys {
  * iindex position.  For an output larger than L2 that costs one read-modify-write of a DRAM
  * sector per 8-byte store.  TWO_PHASE: each shell quartet's block is stored whole, coalesced,
  * into a class-major scratch held by the plan (about npacked doubles more); then one pass
- * writes the packed vector in order from it (whole-molecule plans; shard plans stay DIRECT).
- * AUTO is DIRECT.  The values are the same either way, bit for bit. */
+ * writes the packed vector in order from it, an output row per thread block (whole-molecule
+ * plans; shard plans stay DIRECT).  AUTO: TWO_PHASE for outputs of at least
+ * MOLINTS_TWO_PHASE_MIN integrals (256 MB, twice L2), else DIRECT; served requests
+ * (molints_submit) with AUTO run DIRECT.  The values are the same either way, bit for bit. */
 enum molints_output { MOLINTS_OUTPUT_AUTO = 0, MOLINTS_OUTPUT_DIRECT = 1, MOLINTS_OUTPUT_TWO_PHASE = 2 };
+/* Plans of at least this many integrals take TWO_PHASE under MOLINTS_OUTPUT_AUTO. */
+#define MOLINTS_TWO_PHASE_MIN ((int64_t)1 << 25)
 
 /* Largest shell angular momentum the engine accepts (f = 3).  Class pairs with an f shell run
  * the Rys kernels (n <= 7 roots). */

@@ -112,6 +112,8 @@ struct molints_plan {
     int *g_pair = nullptr;             // per molecule shell pair I >= J: pos << 5 | class << 1 | A == J
     long long *g_region = nullptr;     // per (x, y, molecule): {scratch offset, first bra, first ket, kets}
     long long *g_mol = nullptr;        // per molecule: {first function, first pair entry, packed offset, packed}
+    int2 *g_rows = nullptr;            // gather order: {molecule, row ij}, the rows of one shell pair together
+    int64_t n_rows = 0;
     int64_t bytes = 0;
     int n_launches = 0;
     double plan_ms[4] = {0, 0, 0, 0};  // plan creation phases (molints_stats.plan_ms)
@@ -380,64 +382,39 @@ __device__ __forceinline__ long long untri_f(long long t) {
     return n;
 }
 
-constexpr int kGatherThreads = 256, kGatherPerThread = 8;
+constexpr int kGatherThreads = 256;
 
-// Second phase of the two-phase output: every packed entry t (in order, so the stores are
-// coalesced) from the scratch block of the quartet and component the direct path would have
-// stored it from.  Row ij >= column kl; their shell pairs P (from ij) and Q (from kl); the
-// quartet's bra is the pair of the higher class, or of the later list position within a class
-// (P for the diagonal quartet P == Q); a pair's components are taken in its A, B orientation,
-// with the larger component first within a same-shell pair, as the direct store conditions pick.
-// A block covers kGatherThreads * kGatherPerThread consecutive entries; its first row comes
-// from one FP64 square root, and each thread walks its entries' rows forward from there.
+// Second phase of the two-phase output: the packed vector written row by row from the scratch
+// blocks.  A block of threads writes one row ij (function pair i >= j) whole, columns kl =
+// 0..ij in order, so the stores are coalesced; rows[] lists the rows shell pair by shell pair,
+// so the rows of one pair P, which read the same scratch blocks (P's bra row of each class
+// region, or P's column of the regions where P is the ket), run at the same time and find
+// them in L2.  Each entry comes from the block and component the direct path would have
+// stored it from: row ij >= column kl, shell pairs P (from ij) and Q (from kl); the quartet's
+// bra is the pair of the higher class, or of the later list position within a class (P for the
+// diagonal quartet P == Q); a pair's components are taken in its A, B orientation, with the
+// larger component first within a same-shell pair, as the direct store conditions pick.
 __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
     double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ fn,
     const int *__restrict__ pairs, const long long *__restrict__ region, const long long *__restrict__ mol,
-    int nmol, long long npacked) {
-    constexpr long long kTile = (long long)kGatherThreads * kGatherPerThread;
-    for (long long t0 = (long long)blockIdx.x * kTile; t0 < npacked; t0 += (long long)gridDim.x * kTile) {
-        // the tile's first molecule (binary search over the molecules' packed offsets)
-        int m = 0;
-        if (nmol > 1) {
-            int lo = 0, hi = nmol - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (__ldg(&mol[4 * mid + 2]) <= t0) lo = mid; else hi = mid - 1;
-            }
-            m = lo;
-        }
-        long long mol_lo = __ldg(&mol[4 * m + 2]), mol_hi = mol_lo + __ldg(&mol[4 * m + 3]);
-        long long row = -1, i = 0, j = 0;
-        for (int e = 0; e < kGatherPerThread; ++e) {
-            const long long t = t0 + threadIdx.x + (long long)e * kGatherThreads;
-            if (t >= npacked) break;
-            while (t >= mol_hi) {  // next molecule
-                ++m;
-                mol_lo = mol_hi;
-                mol_hi = mol_lo + __ldg(&mol[4 * m + 3]);
-                row = -1;
-            }
-            const long long tl = t - mol_lo;
-            if (row < 0) {
-                row = (long long)((sqrt(8.0 * (double)tl + 1.0) - 1.0) * 0.5);
-                while ((row + 1) * (row + 2) / 2 <= tl) ++row;
-                while (row * (row + 1) / 2 > tl) --row;
-                i = untri_f(row);
-                j = row - i * (i + 1) / 2;
-            }
-            while ((row + 1) * (row + 2) / 2 <= tl) {  // rows grow: a step or two at most
-                ++row;
-                if (++j > i) { ++i; j = 0; }
-            }
-            const long long kl = tl - row * (row + 1) / 2;
-            const long long k = untri_f(kl), l = kl - k * (k + 1) / 2;
-            const long long fb = __ldg(&mol[4 * m]), pb = __ldg(&mol[4 * m + 1]);
-            const int2 fi = __ldg(&fn[fb + i]), fj = __ldg(&fn[fb + j]), fk = __ldg(&fn[fb + k]), fl = __ldg(&fn[fb + l]);
-            const int P = __ldg(&pairs[pb + (long long)fi.x * (fi.x + 1) / 2 + fj.x]);
+    const int2 *__restrict__ rows, int nmol, long long nrows) {
+    for (long long r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int2 mr = __ldg(&rows[r]);
+        const int m = mr.x;
+        const long long ij = mr.y;
+        const long long fb = __ldg(&mol[4 * m]), pb = __ldg(&mol[4 * m + 1]);
+        double *__restrict__ orow = out + __ldg(&mol[4 * m + 2]) + ij * (ij + 1) / 2;
+        const long long i = untri_f(ij), j = ij - i * (i + 1) / 2;
+        const int2 fi = __ldg(&fn[fb + i]), fj = __ldg(&fn[fb + j]);
+        const int P = __ldg(&pairs[pb + (long long)fi.x * (fi.x + 1) / 2 + fj.x]);
+        const int posP = P >> 5, clsP = (P >> 1) & 15;
+        const int pa = (P & 1) ? fj.y : fi.y, pbc = (P & 1) ? fi.y : fj.y;
+        long long k = untri_f(threadIdx.x), l = threadIdx.x - k * (k + 1) / 2;
+        for (long long kl = threadIdx.x; kl <= ij; kl += kGatherThreads) {
+            while (l > k) { l -= k + 1; ++k; }  // kl advanced by kGatherThreads since the last entry
+            const int2 fk = __ldg(&fn[fb + k]), fl = __ldg(&fn[fb + l]);
             const int Q = __ldg(&pairs[pb + (long long)fk.x * (fk.x + 1) / 2 + fl.x]);
-            const int posP = P >> 5, clsP = (P >> 1) & 15, posQ = Q >> 5, clsQ = (Q >> 1) & 15;
-            // components in each pair's A, B orientation
-            const int pa = (P & 1) ? fj.y : fi.y, pbc = (P & 1) ? fi.y : fj.y;
+            const int posQ = Q >> 5, clsQ = (Q >> 1) & 15;
             const int qa = (Q & 1) ? fl.y : fk.y, qb = (Q & 1) ? fk.y : fl.y;
             const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
             const int x = braP ? clsP : clsQ, y = braP ? clsQ : clsP;
@@ -448,7 +425,8 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
             const long long slot = (x == y) ? db * (db + 1) / 2 + dk : db * __ldg(&rg[3]) + dk;
             const int na = c_pair_na[x], nb = c_pair_nb[x], nc = c_pair_na[y], nd = c_pair_nb[y];
             const long long blk = (long long)na * nb * nc * nd;
-            out[t] = __ldg(&scratch[__ldg(&rg[0]) + slot * blk + ((ma * nb + mb) * nc + mc) * nd + md]);
+            orow[kl] = __ldg(&scratch[__ldg(&rg[0]) + slot * blk + ((ma * nb + mb) * nc + mc) * nd + md]);
+            l += kGatherThreads;
         }
     }
 }
@@ -764,7 +742,7 @@ static void plan_release_device(molints_plan *p) {
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
-                    p->scratch, p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol};
+                    p->scratch, p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
     p->ctx = nullptr;
@@ -941,9 +919,12 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     }
     p->mol_nshell.resize(nmol);
     p->nbf0 = nmol > 0 ? mol_nbf[0] : 0;
-    // two-phase output on request (whole-molecule plans only); AUTO is DIRECT: with the
-    // scratch in bra-major, primitive-count order the gather pass costs what it saves
-    p->two_phase = nshards == 1 && nmol > 0 && opts.output == MOLINTS_OUTPUT_TWO_PHASE;
+    // two-phase output (whole-molecule plans only): AUTO takes it for outputs of at least
+    // MOLINTS_TWO_PHASE_MIN integrals (256 MB, twice L2), where the direct stores' sector
+    // read-modify-writes cost more than the gather pass; below, the output stays in L2
+    p->two_phase = nshards == 1 && nmol > 0 &&
+                   (opts.output == MOLINTS_OUTPUT_TWO_PHASE ||
+                    (opts.output == MOLINTS_OUTPUT_AUTO && p->npacked >= MOLINTS_TWO_PHASE_MIN));
     // method per class pair: Rys where no HGP kernel exists (an f shell), else the request
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) {
@@ -1414,7 +1395,10 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     const size_t o_gpair = o_gfn + (tp ? al16((size_t)nfn_all * sizeof(int2)) : 0);
     const size_t o_greg = o_gpair + (tp ? al16((size_t)npe_all * sizeof(int)) : 0);
     const size_t o_gmol = o_greg + (tp ? al16(region_h.size() * sizeof(long long)) : 0);
-    const size_t stage_bytes = o_gmol + (tp ? al16((size_t)nmol * 4 * sizeof(long long)) : 0);
+    int64_t nrows_all = 0;
+    for (int m = 0; m < nmol; ++m) nrows_all += mol_nbf[m] * (mol_nbf[m] + 1) / 2;
+    const size_t o_grows = o_gmol + (tp ? al16((size_t)nmol * 4 * sizeof(long long)) : 0);
+    const size_t stage_bytes = o_grows + (tp ? al16((size_t)nrows_all * sizeof(int2)) : 0);
     if ((rc = ctx_stage(ctx, stage_bytes))) { plan_free(p); return rc; }
     char *stage = ctx->stage;
     int4 *chunks = reinterpret_cast<int4 *>(stage);
@@ -1450,6 +1434,21 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             gpair[pbase[m] + pr[k].ref] = (k << 5) | (pr[k].cls << 1) | swapped;
         }
         std::memcpy(stage + o_greg, region_h.data(), region_h.size() * sizeof(long long));
+        // gather order: per molecule, shell pairs from the last, each pair's rows together
+        int2 *grows = reinterpret_cast<int2 *>(stage + o_grows);
+        int64_t nr = 0;
+        for (int m = 0; m < nmol; ++m)
+            for (int I = bases[m].nshell - 1; I >= 0; --I)
+                for (int J = I; J >= 0; --J) {
+                    const int gI = shell_off[m] + I, gJ = shell_off[m] + J;
+                    for (int ci = 0; ci < ncart(L[gI]); ++ci)
+                        for (int cj = 0; cj < ncart(L[gJ]); ++cj) {
+                            const int64_t fi = fn_off[gI] + ci, fj = fn_off[gJ] + cj;
+                            if (fj > fi) continue;
+                            grows[nr++] = make_int2(m, (int)(fi * (fi + 1) / 2 + fj));
+                        }
+                }
+        p->n_rows = nr;
     }
     std::memcpy(stage + o_info, info_h.data(), npair * sizeof(int4));
     std::memcpy(stage + o_bnd, p->bnd_h.data(), npair * sizeof(double2));
@@ -1472,6 +1471,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         if (!rc) rc = dev_alloc(ctx, &p->g_pair, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->g_rows, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
     }
     if (rc) { plan_free(p); return rc; }
     if (tp && ((nq > 0 && (e = cudaMemcpyAsync(p->chunk_slot, stage + o_slot, (size_t)nq * sizeof(long long),
@@ -1483,7 +1483,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                (e = cudaMemcpyAsync(p->g_region, stage + o_greg, region_h.size() * sizeof(long long),
                                     cudaMemcpyHostToDevice, s)) ||
                (e = cudaMemcpyAsync(p->g_mol, stage + o_gmol, (size_t)nmol * 4 * sizeof(long long),
-                                    cudaMemcpyHostToDevice, s)))) {
+                                    cudaMemcpyHostToDevice, s)) ||
+               (nrows_all > 0 && (e = cudaMemcpyAsync(p->g_rows, stage + o_grows, (size_t)nrows_all * sizeof(int2),
+                                                       cudaMemcpyHostToDevice, s))))) {
         plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
     }
@@ -1600,10 +1602,10 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     if (p->two_phase && !jk.J && p->npacked > 0) {
         // second phase: the packed vector in order from the scratch blocks
         if (int rc = mark(launches, "gather_packed", 0, s)) return rc;
-        constexpr long long kTile = (long long)kGatherThreads * kGatherPerThread;
-        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, (p->npacked + kTile - 1) / kTile);
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, p->n_rows);
         gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, p->scratch, p->g_fn, p->g_pair,
-                                                             p->g_region, p->g_mol, p->nmol, p->npacked);
+                                                             p->g_region, p->g_mol, p->g_rows, p->nmol,
+                                                             p->n_rows);
         if (int rc = mark(launches, "gather_packed", 1, s)) return rc;
         ++launches;
     }

@@ -162,6 +162,26 @@ def test_two_phase_output_equals_direct(eng):
     scale = max(1.0, np.abs(res[0][0]).max(), np.abs(res[0][1]).max())
     assert np.max(np.abs(res[0][0] - res[1][0])) < 1e-12 * scale
     assert np.max(np.abs(res[0][1] - res[1][1])) < 1e-12 * scale
+    # AUTO takes the two-phase output above MOLINTS_TWO_PHASE_MIN (2^25) integrals, for a
+    # batch plan and for one molecule, and keeps a smaller molecule direct
+    big = [mi.config4_request(1), mi.config4_request(7)]
+    total = sum(sh.npacked for sh in big)
+    assert big[0].npacked >= 1 << 25 > big[1].npacked
+    out = torch.empty(total, dtype=torch.float64, device="cuda")
+    for mols, expect in ((big, True), (big[0], True), (big[1], False)):
+        plan = eng.plan_batch(mols) if isinstance(mols, list) else eng.plan(mols)
+        plan.set_profiling(True)
+        plan.execute(out.data_ptr())
+        torch.cuda.synchronize()
+        assert ("gather_packed" in [n for n, _ in plan.launch_times()]) == expect
+        plan.close()
+    plan = eng.plan_batch(big)
+    plan.execute(out.data_ptr())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    plan.close()
+    assert np.array_equal(got[:big[0].npacked], eng.eri_packed(big[0], output=DIR))
+    assert np.array_equal(got[big[0].npacked:total], eng.eri_packed(big[1], output=DIR))
 
 
 @pytest.mark.parametrize("seed,lmax", [(101, 0), (102, 1), (103, 2), (104, 2)])
