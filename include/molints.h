@@ -37,10 +37,11 @@ enum molints_status {
     MOLINTS_ERR_NOMEM = -6         /* host allocation failed */
 };
 
-/* AUTO: per class pair, the context's method table (molints_set_class_methods), else HGP where
- * an HGP kernel exists (shells up to d) and Rys otherwise.  HGP: all_twoe_ints_chrr's
- * algorithm (src/HGP.jl:22-242) wherever it exists, Rys for classes with an f shell.  RYS:
- * all_twoe_ints_rys's algorithm (src/Rys.jl:16-156) for every class pair. */
+/* AUTO: per class pair, the context's method table (molints_set_class_methods; on a B200 the
+ * shipped tuned table by default), else HGP where an HGP kernel exists and Rys otherwise.
+ * HGP: all_twoe_ints_chrr's algorithm (src/HGP.jl:22-242) wherever it exists, Rys for classes
+ * with an f shell.  RYS: all_twoe_ints_rys's algorithm (src/Rys.jl:16-156) for every class
+ * pair. */
 enum molints_method { MOLINTS_METHOD_AUTO = 0, MOLINTS_METHOD_HGP = 1, MOLINTS_METHOD_RYS = 2 };
 enum molints_precision { MOLINTS_FP64 = 0, MOLINTS_MIXED = 1 };
 enum molints_boys {
@@ -56,8 +57,10 @@ enum molints_boys {
  * into a class-major scratch held by the plan (about npacked doubles more); then one pass
  * writes the packed vector in order from it, an output row per thread block (whole-molecule
  * plans; shard plans stay DIRECT).  AUTO: TWO_PHASE for outputs of at least
- * MOLINTS_TWO_PHASE_MIN integrals (256 MB, twice L2), else DIRECT; served requests
- * (molints_submit) with AUTO run DIRECT.  The values are the same either way, bit for bit. */
+ * MOLINTS_TWO_PHASE_MIN integrals (256 MB, twice L2) when its scratch fits the context's
+ * budget and the device, else DIRECT; served requests (molints_submit) with AUTO run DIRECT.
+ * An explicit TWO_PHASE whose scratch does not fit fails.  The values are the same either way,
+ * bit for bit. */
 enum molints_output { MOLINTS_OUTPUT_AUTO = 0, MOLINTS_OUTPUT_DIRECT = 1, MOLINTS_OUTPUT_TWO_PHASE = 2 };
 /* Plans of at least this many integrals take TWO_PHASE under MOLINTS_OUTPUT_AUTO. */
 #define MOLINTS_TWO_PHASE_MIN ((int64_t)1 << 25)
@@ -107,10 +110,13 @@ typedef struct molints_stats {
     int64_t n_eri;            /* packed integrals written */
     int64_t n_shell_quartets; /* unique shell quartets */
     int64_t n_prim_quartets;  /* primitive quartets in those */
-    int64_t n_fp32_quartets;  /* quartets that took the FP32 VRR (counted on the host) */
+    int64_t n_fp32_quartets;  /* quartets that ran an FP32 kernel variant: bound below
+                                 fp32_cutoff, in a class pair whose plan launches its FP32
+                                 variant (counted on the host) */
     int64_t n_screened;       /* quartets skipped by screen_cutoff (counted on the host) */
     int32_t n_kernel_launches;
-    int32_t reserved;
+    int32_t n_fp32_launches;  /* class-pair kernels of the last execute launched as their FP32
+                                 variant (MIXED plans) */
     double device_ms;         /* device time of the last execute (CUDA events) */
     int64_t n_prim_pairs;     /* primitive pairs of all shell pairs */
     int64_t n_prim_pairs_kept;/* primitive pairs left after prim_cutoff */
@@ -142,13 +148,18 @@ const char *molints_last_error(const molints_ctx *ctx);
 
 /* Per class pair method for MOLINTS_METHOD_AUTO plans created afterwards (the autotuner's
  * choice).  methods[x * MOLINTS_NUM_PAIR_CLASSES + y] for bra class x >= ket class y is
- * MOLINTS_METHOD_HGP, MOLINTS_METHOD_RYS or MOLINTS_METHOD_AUTO (default: HGP where it
- * exists); entries with y > x are ignored.  methods == NULL resets the table.  n must be
- * MOLINTS_NUM_PAIR_CLASSES^2.  No reference counterpart (the reference picks its driver by
- * function name). */
+ * MOLINTS_METHOD_HGP, MOLINTS_METHOD_RYS or MOLINTS_METHOD_AUTO (HGP where it exists);
+ * entries with y > x are ignored.  n must be MOLINTS_NUM_PAIR_CLASSES^2.  A new context starts
+ * with the default table: on an NVIDIA B200 the class tuner's measured choices shipped with the
+ * library (Rys for the heavy d and f classes, FP32 variants only where they measured faster),
+ * elsewhere HGP everywhere.  methods == NULL restores that default.  No reference counterpart
+ * (the reference picks its driver by function name). */
 int molints_set_class_methods(molints_ctx *ctx, const int32_t *methods, int32_t n);
+/* The context's current table, in the layout of molints_set_class_methods (n entries). */
+int molints_get_class_methods(const molints_ctx *ctx, int32_t *methods, int32_t n);
 /* Flag OR'ed into a molints_set_class_methods entry: MIXED plans run that class pair's FP64
- * kernel (its FP32 variant measured no faster). */
+ * kernel (its FP32 variant measured no faster).  It applies when the plan runs the entry's own
+ * method (or the entry is AUTO); a plan whose options force the other method ignores it. */
 #define MOLINTS_CLASS_NO_FP32 4
 
 /* Set the CUDA stream (a cudaStream_t passed as void*) the context launches on.
@@ -233,18 +244,20 @@ int molints_boys_eval(molints_ctx *ctx, int32_t boys_mode, int32_t mmax, const d
                       int64_t n, double *out);
 
 /* The ERI path for callers that cannot allocate device memory where they need the
- * integrals: code running inside CUDA stream capture, where cudaMalloc is not allowed, and
- * frameworks whose allocator owns the whole GPU.  There is no counterpart in the reference.
- * It needs no context and allocates nothing: the caller passes the basis (host arrays, as for
- * molints_eri_packed) and its own device vector out_device of molints_npacked(nbf) doubles;
- * the Boys table and the pair tables live in one static device array of 8 MiB that every GPU
- * which loads the library holds until exit.  Bases whose tables do not fit are rejected with
- * MOLINTS_ERR_UNSUPPORTED and a message in err (err may be NULL).  FP64 without screening
- * only (opts NULL = defaults; prim_cutoff is ignored: every primitive pair is kept).  The
- * first call on a device looks the array up with cudaGetSymbolAddress and copies the Boys
- * table into it synchronously, so make that first call before any stream capture.  The call
- * enqueues its work on `stream` (a cudaStream_t; NULL is the legacy default stream) and
- * returns; all calls share the array, so calls whose GPU work overlaps race on it. */
+ * integrals: host programs whose own allocator has reserved the GPU's memory (a framework's
+ * caching allocator, a simulation code's memory manager), and time-critical loops that cannot
+ * take the device synchronisation a cudaMalloc or cudaFree may cause.  There is no counterpart
+ * in the reference.  It needs no context and allocates nothing: the caller passes the basis
+ * (host arrays, as for molints_eri_packed) and its own device vector out_device of
+ * molints_npacked(nbf) doubles; the Boys table, the pair tables and the work queues live in
+ * one static device array of 8 MiB that every GPU which loads the library holds until exit.
+ * Bases whose tables do not fit are rejected with MOLINTS_ERR_UNSUPPORTED and a message in err
+ * (err may be NULL).  FP64 without screening, shells up to d only (opts NULL = defaults;
+ * prim_cutoff is ignored: every primitive pair is kept).  The first call on a device, with
+ * that device current, looks the array up with cudaGetSymbolAddress and copies the Boys table
+ * into it synchronously, so make that first call before any stream capture.  The call enqueues
+ * its work on `stream` (a cudaStream_t; NULL is the legacy default stream) and returns; all
+ * calls share the array, so calls whose GPU work overlaps race on it. */
 int molints_eri_packed_noalloc(const molints_basis *basis, const molints_options *opts,
                                double *out_device, void *stream, char *err, size_t err_len);
 

@@ -26,6 +26,10 @@ def tune_fp32_cutoff(engine, shells, target: float = 1e-9, safety: float = 0.25,
     out = torch.empty_like(ref)
     stream = torch.cuda.current_stream(dev)
     engine.set_stream(stream.cuda_stream)
+    # the error is measured with every class pair's FP32 variant in use (the table's
+    # "FP32 no faster" flags cleared); the context's table is restored afterwards
+    saved = engine.class_methods()
+    engine.set_class_methods({k: v & ~E.CLASS_NO_FP32 for k, v in saved.items()})
     try:
         p64 = engine.plan(shells, precision=E.FP64, boys=boys, method=method)
         p64.execute(ref.data_ptr())
@@ -39,13 +43,15 @@ def tune_fp32_cutoff(engine, shells, target: float = 1e-9, safety: float = 0.25,
             pm.close()
             err = (out - ref).abs().max().item() if shells.npacked else 0.0
             frac = st["n_fp32_quartets"] / max(st["n_shell_quartets"], 1)
-            table.append({"cutoff": c, "max_abs_err": err, "fp32_quartet_fraction": frac})
+            table.append({"cutoff": c, "max_abs_err": err, "fp32_quartet_fraction": frac,
+                          "fp32_launches": st["n_fp32_launches"]})
             if err <= target * safety:
                 best = c
             else:
                 break
         return best, table
     finally:
+        engine.set_class_methods(saved)
         engine.set_stream(None)
 
 
@@ -80,6 +86,9 @@ def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95
     runs = [(E.METHOD_HGP, E.FP64), (E.METHOD_RYS, E.FP64)]
     if fp32_cutoff:
         runs += [(E.METHOD_HGP, E.MIXED), (E.METHOD_RYS, E.MIXED)]
+    # every FP32 variant runs while its time is measured; the table is restored afterwards
+    saved = engine.class_methods()
+    engine.set_class_methods({k: v & ~E.CLASS_NO_FP32 for k, v in saved.items()})
     try:
         for meth, prec in runs:
             plan = engine.plan_batch(mols, method=meth, boys=E.BOYS_EXACT, precision=prec,
@@ -93,6 +102,7 @@ def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95
                         best[key] = min(best.get(key, float("inf")), ms)
             plan.close()
     finally:
+        engine.set_class_methods(saved)
         engine.set_stream(None)
     table, timings = {}, {}
     for tag in sorted({k[0] for k in best}):

@@ -49,7 +49,7 @@ def sources():
 
 def _deps(src: Path):
     return [src, CSRC / "eri_common.cuh", CSRC / "rys_common.cuh", CSRC / "eri_dispatch.h",
-            INCLUDE / "molints.h"]
+            CSRC / "class_table.h", INCLUDE / "molints.h"]
 
 
 def _compile(src: Path, force: bool):

@@ -607,6 +607,16 @@ def emit_dispatch(pairs):
                 row.append("0.0f")
         lines.append("    {" + ", ".join(row) + "},")
     lines.append("};")
+    lines.append("// 1 where the class pair's kernel has an FP32 variant for MIXED quartets (HGP: at least")
+    lines.append(f"// {MIXED_MIN_VRR} VRR entries; Rys: gen_rys's MIXED_MIN_NBLK / MIXED_MAX_ACC rule), else 0")
+    for name, has in (("kEriHasFp32", lambda X, Y: (X, Y) in hgp and
+                       len(vrr_entries(X[0], X[0] + X[1], Y[0], Y[0] + Y[1])) >= MIXED_MIN_VRR),
+                      ("kRysHasFp32", lambda X, Y: gen_rys.class_tables(X, Y)["mixed"])):
+        lines.append(f"static const unsigned char {name}[{n}][{n}] = {{")
+        for i, X in enumerate(cls):
+            lines.append("    {" + ", ".join("1" if (j <= i and has(X, Y)) else "0"
+                                             for j, Y in enumerate(cls)) + "},")
+        lines.append("};")
     table("RysLauncher", "kRysLaunchers", lambda X, Y: f"launch_rys_{tag_of(X, Y)}")
     table("RysOccupancy", "kRysOccupancy", lambda X, Y: f"occupancy_rys_{tag_of(X, Y)}")
     table("char *const", "kRysNames", lambda X, Y: f'"rys_{tag_of(X, Y)}"')
@@ -624,6 +634,41 @@ def emit_dispatch(pairs):
     return "\n".join(lines) + "\n"
 
 
+def emit_class_table(path: Path):
+    """class_table.h: the default per-class-pair method table of MOLINTS_METHOD_AUTO, from the
+    class tuner's result kept in data/class_table_<gpu>.json (the classes it found faster with
+    Rys, and those whose FP32 variant it found faster than FP64)."""
+    import json
+    d = json.loads(path.read_text())
+    cls = gen_rys.pair_classes()
+    lv = {"s": 0, "p": 1, "d": 2, "f": 3}
+
+    def idx(t):
+        return cls.index((lv[t[0]], lv[t[1]])), cls.index((lv[t[2]], lv[t[3]]))
+    n = len(cls)
+    tab = [[0] * n for _ in range(n)]
+    for x in range(n):
+        for y in range(x + 1):
+            tab[x][y] = 1 | 4  # MOLINTS_METHOD_HGP | MOLINTS_CLASS_NO_FP32
+    for t in d["rys"]:
+        x, y = idx(t)
+        tab[x][y] = 2 | (tab[x][y] & 4)
+    for t in d["fp32"]:
+        x, y = idx(t)
+        tab[x][y] &= 3
+    lines = [f"// Generated by gen_eri.py from data/{path.name}.  Do not edit.",
+             "// Default MOLINTS_METHOD_AUTO table of contexts on the device named below:",
+             f"// {d['source']}.",
+             "// Entries: 1 HGP, 2 Rys, | 4 (MOLINTS_CLASS_NO_FP32) where MIXED runs the FP64 kernel.",
+             "#pragma once", "#include <stdint.h>", "namespace molints {",
+             f'constexpr const char *kTunedDevice = "{d["device"]}";',
+             f"static const int32_t kTunedClassMethods[{n}][{n}] = {{"]
+    for x in range(n):
+        lines.append("    {" + ", ".join(str(v) for v in tab[x]) + "},")
+    lines += ["};", "}  // namespace molints", ""]
+    return "\n".join(lines)
+
+
 def generate(out_dir: Path = OUT_DIR):
     out_dir.mkdir(parents=True, exist_ok=True)
     pairs = class_pairs()
@@ -639,6 +684,10 @@ def generate(out_dir: Path = OUT_DIR):
     src = emit_dispatch(pairs)
     if not d.exists() or d.read_text() != src:
         d.write_text(src)
+    t = HERE / "class_table.h"
+    src = emit_class_table(HERE.parent / "data" / "class_table_b200.json")
+    if not t.exists() or t.read_text() != src:
+        t.write_text(src)
     return written
 
 

@@ -28,6 +28,7 @@
 
 #include "../../include/molints.h"
 #include "eri_common.cuh"
+#include "class_table.h"
 #include "eri_dispatch.h"
 
 using namespace molints;
@@ -58,7 +59,10 @@ struct molints_ctx {
     // Rys MIXED]
     int occupancy[kNumPairClasses][kNumPairClasses][4] = {};
     RysTab rys{};  // device addresses of the Rys root/weight tables on this device
-    int32_t class_method[kNumPairClasses][kNumPairClasses] = {};  // AUTO choices (0 = default)
+    int32_t class_method[kNumPairClasses][kNumPairClasses] = {};  // AUTO choices (0 = HGP)
+    // the table molints_set_class_methods(NULL) restores: the tuned table of class_table.h on
+    // the device it was measured on, all zero (HGP everywhere) elsewhere
+    int32_t default_method[kNumPairClasses][kNumPairClasses] = {};
     char *stage = nullptr;     // pinned host buffer of plan uploads (work queues, pair tables)
     size_t stage_bytes = 0;
     cudaEvent_t stage_ev = nullptr;  // recorded after uploads that a plan creation left in flight
@@ -116,6 +120,7 @@ struct molints_plan {
     int64_t n_rows = 0;
     int64_t bytes = 0;
     int n_launches = 0;
+    int n_fp32_launches = 0;           // class-pair launches of the last execute that ran FP32
     double plan_ms[4] = {0, 0, 0, 0};  // plan creation phases (molints_stats.plan_ms)
     // CUDA graph of one execute (molints_plan_set_graph), valid for graph_out
     int use_graph = 0;
@@ -592,6 +597,13 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
     }
     if (cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         ctx->num_sms = 1;
+    {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) == cudaSuccess &&
+            std::strncmp(prop.name, kTunedDevice, std::strlen(kTunedDevice)) == 0)
+            std::memcpy(ctx->default_method, kTunedClassMethods, sizeof(ctx->default_method));
+        std::memcpy(ctx->class_method, ctx->default_method, sizeof(ctx->class_method));
+    }
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -670,7 +682,7 @@ const char *molints_last_error(const molints_ctx *ctx) { return ctx ? ctx->err.c
 int molints_set_class_methods(molints_ctx *ctx, const int32_t *methods, int32_t n) {
     if (!ctx) return MOLINTS_ERR_INVALID;
     if (!methods) {
-        std::memset(ctx->class_method, 0, sizeof(ctx->class_method));
+        std::memcpy(ctx->class_method, ctx->default_method, sizeof(ctx->class_method));
         return MOLINTS_OK;
     }
     if (n != kNumPairClasses * kNumPairClasses)
@@ -683,6 +695,13 @@ int molints_set_class_methods(molints_ctx *ctx, const int32_t *methods, int32_t 
         }
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) ctx->class_method[x][y] = methods[x * kNumPairClasses + y];
+    return MOLINTS_OK;
+}
+
+int molints_get_class_methods(const molints_ctx *ctx, int32_t *methods, int32_t n) {
+    if (!ctx || !methods || n != kNumPairClasses * kNumPairClasses) return MOLINTS_ERR_INVALID;
+    for (int x = 0; x < kNumPairClasses; ++x)
+        for (int y = 0; y < kNumPairClasses; ++y) methods[x * kNumPairClasses + y] = y <= x ? ctx->class_method[x][y] : 0;
     return MOLINTS_OK;
 }
 
@@ -934,8 +953,13 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             if (m == MOLINTS_METHOD_AUTO) m = MOLINTS_METHOD_HGP;
             if (!kEriLaunchers[x][y]) m = MOLINTS_METHOD_RYS;
             p->method[x][y] = m;
-            // MIXED plans run this class's FP32 variant unless the table says it is no faster
-            p->fp32[x][y] = opts.precision == MOLINTS_MIXED && !(entry & MOLINTS_CLASS_NO_FP32);
+            // MIXED plans run this class's FP32 variant where the chosen kernel has one, unless
+            // the table measured that kernel's FP32 variant no faster (the flag speaks for the
+            // table's own method only)
+            const bool has32 = m == MOLINTS_METHOD_RYS ? kRysHasFp32[x][y] : kEriHasFp32[x][y];
+            const int tm = entry & ~MOLINTS_CLASS_NO_FP32;
+            const bool slower32 = (entry & MOLINTS_CLASS_NO_FP32) && (tm == m || tm == MOLINTS_METHOD_AUTO);
+            p->fp32[x][y] = opts.precision == MOLINTS_MIXED && has32 && !slower32;
         }
 
     // Normalised coefficients: raw coef x (2a/pi)^(3/4) (4a)^(L/2) x CGBF norm; the component
@@ -1254,6 +1278,23 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 rg[3] = nk;
                 scratch_len += (x == y ? nb * (nb + 1) / 2 : nb * nk) * ncomp_of(x, y);
             }
+        // The scratch (about npacked doubles) is taken now.  If it does not fit the budget or
+        // the device, AUTO falls back to the direct stores, which need no scratch; only an
+        // explicit MOLINTS_OUTPUT_TWO_PHASE fails.
+        const int64_t held0 = p->bytes;
+        int src = dev_alloc(ctx, &p->scratch, (size_t)std::max<int64_t>(scratch_len, 1), &p->bytes);
+        if (src && opts.output == MOLINTS_OUTPUT_AUTO) {
+            cudaGetLastError();  // an out-of-memory status is not sticky; clear it
+            p->scratch = nullptr;
+            p->bytes = held0;
+            p->two_phase = 0;
+            region_h.clear();
+            scratch_len = 0;
+            ctx->err.clear();
+        } else if (src) {
+            plan_free(p);
+            return src;
+        }
     }
     std::vector<QueueTask> tasks;
     std::vector<int> task_end(cps.size(), 0), cp_width(cps.size(), 32 * widen);
@@ -1465,8 +1506,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     rc = dev_alloc(ctx, &p->chunks, (size_t)nq, &p->bytes);
     if (!rc) rc = dev_alloc(ctx, &p->pbk, (size_t)std::max<int64_t>(nkept, 1), &p->bytes);
     if (!rc && tp) {
-        rc = dev_alloc(ctx, &p->scratch, (size_t)std::max<int64_t>(scratch_len, 1), &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->chunk_slot, (size_t)std::max<int64_t>(nq, 1), &p->bytes);
+        rc = dev_alloc(ctx, &p->chunk_slot, (size_t)std::max<int64_t>(nq, 1), &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_fn, (size_t)std::max<int64_t>(nfn_all, 1), &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_pair, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
@@ -1561,6 +1601,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     std::stable_sort(jobs.begin(), jobs.end(), [](const Job &a, const Job &b) { return a.cost > b.cost; });
     // Profiling runs every launch on the caller's stream, so each event pair times one kernel.
     const int nside = p->profiling ? 0 : std::min<int>(molints_ctx::kSide, (int)jobs.size());
+    int fp32_launches = 0;
     if (nside > 0) MI_CUDA(ctx, cudaEventRecord(ctx->fork, s));
     for (int i = 0; i < nside; ++i) MI_CUDA(ctx, cudaStreamWaitEvent(ctx->side[i], ctx->fork, 0));
     for (size_t k = 0; k < jobs.size(); ++k) {
@@ -1592,6 +1633,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         if (int rc = mark(launches, name, 0, st)) return rc;
         if (rys) kRysLaunchers[x][y](Q, ctx->rys, mixed, grid, st);
         else kEriLaunchers[x][y](Q, mixed, grid, st);
+        fp32_launches += mixed;
         if (int rc = mark(launches, name, 1, st)) return rc;
         ++launches;
     }
@@ -1612,6 +1654,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     MI_CUDA(ctx, cudaGetLastError());
     if (timing) MI_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
     p->n_launches = launches;
+    p->n_fp32_launches = fp32_launches;
     return MOLINTS_OK;
 }
 
@@ -1745,40 +1788,50 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
     st->n_prim_pairs = p->nprim_pair_all;
     st->n_prim_pairs_kept = p->nprim_pair_kept;
     for (int k = 0; k < 4; ++k) st->plan_ms[k] = p->plan_ms[k];
-    // per molecule: its pairs are interleaved by class, so gather them first
-    std::vector<std::vector<int>> by_mol(std::max(p->nmol, 1));
-    for (int k = 0; k < p->npair; ++k) by_mol[p->pair_mol[k]].push_back(k);
+    st->n_fp32_launches = p->n_fp32_launches;
+    // per (molecule, pair class): the pairs, gathered from the class-major list
+    const int nc = kNumPairClasses;
+    std::vector<std::vector<int>> by(std::max(p->nmol, 1) * nc);
+    for (int c = 0; c < nc; ++c)
+        for (int k = p->class_start[c]; k < p->class_start[c + 1]; ++k) by[p->pair_mol[k] * nc + c].push_back(k);
+    const bool mixed = p->opts.precision == MOLINTS_MIXED && p->opts.fp32_cutoff > 0.0;
+    const double cut = p->opts.fp32_cutoff, scut = p->opts.screen_cutoff;
     for (int m = 0; m < p->nmol; ++m) {
-        const std::vector<int> &v = by_mol[m];
-        const int64_t np = (int64_t)v.size();
+        int64_t np = 0, sum = 0, sum2 = 0;
+        for (int c = 0; c < nc; ++c)
+            for (int k : by[m * nc + c]) { ++np; sum += p->npp_h[k]; sum2 += (int64_t)p->npp_h[k] * p->npp_h[k]; }
         st->n_shell_quartets += np * (np + 1) / 2;
-        int64_t sum = 0, sum2 = 0;
-        for (int k : v) { sum += p->npp_h[k]; sum2 += (int64_t)p->npp_h[k] * p->npp_h[k]; }
         st->n_prim_quartets += (sum * sum + sum2) / 2;
-        const bool mixed = p->opts.precision == MOLINTS_MIXED && p->opts.fp32_cutoff > 0.0;
-        if (p->opts.screen_cutoff > 0.0) {
-            // both conditions: the direct count over pair pairs
-            for (size_t a = 0; a < v.size(); ++a)
-                for (size_t c = 0; c <= a; ++c) {
-                    const double2 ba = p->bnd_h[v[a]], bc = p->bnd_h[v[c]];
-                    if (ba.x * bc.x < p->opts.screen_cutoff) ++st->n_screened;
-                    else if (mixed && ba.y * bc.y < p->opts.fp32_cutoff) ++st->n_fp32_quartets;
+        for (int x = 0; x < nc; ++x)
+            for (int y = 0; y <= x; ++y) {
+                const std::vector<int> &A = by[m * nc + x], &Bv = by[m * nc + y];
+                if (A.empty() || Bv.empty()) continue;
+                // only quartets of class pairs whose plan launches an FP32 kernel count as FP32
+                const bool f32 = mixed && p->fp32[x][y];
+                if (scut > 0.0) {
+                    // both conditions: the direct count over the class pair's quartets
+                    for (size_t a = 0; a < A.size(); ++a)
+                        for (size_t c = 0; c < (x == y ? a + 1 : Bv.size()); ++c) {
+                            const double2 ba = p->bnd_h[A[a]], bc = p->bnd_h[Bv[c]];
+                            if (ba.x * bc.x < scut) ++st->n_screened;
+                            else if (f32 && ba.y * bc.y < cut) ++st->n_fp32_quartets;
+                        }
+                } else if (f32) {
+                    // quartets (a, c) with R_a R_c < cut from the sorted R of the ket class; for
+                    // x == y the unordered pairs {a, c}: (ordered + diagonal) / 2
+                    std::vector<double> yk(Bv.size());
+                    for (size_t c = 0; c < Bv.size(); ++c) yk[c] = p->bnd_h[Bv[c]].y;
+                    std::sort(yk.begin(), yk.end());
+                    int64_t ordered = 0, diag = 0;
+                    for (int k : A) {
+                        const double ya = p->bnd_h[k].y;
+                        if (ya <= 0.0) ordered += (int64_t)yk.size();
+                        else ordered += std::lower_bound(yk.begin(), yk.end(), cut / ya) - yk.begin();
+                        if (x == y && ya * ya < cut) ++diag;
+                    }
+                    st->n_fp32_quartets += x == y ? (ordered + diag) / 2 : ordered;
                 }
-        } else if (mixed) {
-            // unordered pairs {a, c} (a == c included) with y_a y_c < cut, from the sorted y:
-            // (sum_a #{c : y_c < cut / y_a} + #{a : y_a^2 < cut}) / 2
-            std::vector<double> y(v.size());
-            for (size_t a = 0; a < v.size(); ++a) y[a] = p->bnd_h[v[a]].y;
-            std::sort(y.begin(), y.end());
-            const double cut = p->opts.fp32_cutoff;
-            int64_t ordered = 0, diag = 0;
-            for (double ya : y) {
-                if (ya <= 0.0) { ordered += (int64_t)y.size(); diag += 1; continue; }
-                ordered += std::lower_bound(y.begin(), y.end(), cut / ya) - y.begin();
-                if (ya * ya < cut) ++diag;
             }
-            st->n_fp32_quartets += (ordered + diag) / 2;
-        }
     }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return MOLINTS_ERR_CUDA;
     if (p->n_launches > 0 && cudaEventSynchronize(ctx->ev1) == cudaSuccess) {

@@ -1,20 +1,24 @@
 // noalloc.cu -- molints_eri_packed_noalloc: the ERI path without any device allocation.
 //
-// Some callers cannot allocate device memory at the point where they need integrals: code
-// running while a CUDA stream is being captured (cudaMalloc is not allowed there), and
-// frameworks whose allocator owns every byte of the GPU and forbid other allocations.  They
-// pass the basis (host arrays) and their own device output vector; everything else the path
-// needs -- the Boys table and the per-call pair tables -- lives in one file-scope device
-// array of kScratchBytes (8 MiB), which every GPU that loads this library holds until exit.
+// Some callers cannot allocate device memory where they need integrals.  A host program whose
+// own allocator has reserved (nearly) all of the GPU's memory -- a framework's caching
+// allocator, or the memory manager of a simulation code that owns the device -- leaves no room
+// for another cudaMalloc and does not want one.  A time-critical loop cannot accept the device
+// synchronisation a cudaMalloc or cudaFree may cause.  Such callers pass the basis (host
+// arrays) and their own device output vector; everything else the path needs -- the Boys table
+// and the per-call pair tables and work queues -- lives in one file-scope device array of
+// kScratchBytes (8 MiB), which every GPU that loads this library holds until the process exits.
 //
-// Set-up: the first call on a device looks up the array's device address with
-// cudaGetSymbolAddress and copies the Boys table into it (a synchronous copy), so that first
-// call should come before any stream capture.  Later calls reuse the address and the table.
+// Set-up: the first call on a device, with that device current, looks up the array's device
+// address with cudaGetSymbolAddress and copies the Boys table into it (a synchronous copy), so
+// that first call should come before any stream capture.  Later calls reuse the address and
+// the table.
 //
 // The call only enqueues work on the caller's stream.  Every call shares the array and
-// overwrites its pair tables, so calls whose GPU work overlaps (different streams, or host
-// threads with no ordering between their streams) race on it; order them on one stream.
-// Host threads are serialised while a call prepares and enqueues its work.
+// overwrites its pair tables and work-queue counters (the counters are cleared by each call's
+// upload), so calls whose GPU work overlaps (different streams, or host threads with no
+// ordering between their streams) race on it; order them on one stream.  Host threads are
+// serialised while a call prepares and enqueues its work.
 #include <cuda_runtime.h>
 
 #include <algorithm>

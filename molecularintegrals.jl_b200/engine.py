@@ -44,6 +44,7 @@ EXPORTED_SYMBOLS = [
     "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
     "molints_release", "molints_serve_stats", "molints_shard_range", "molints_plan_create_shard",
     "molints_plan_set_graph", "molints_plan_jk", "molints_jk", "molints_one_e",
+    "molints_get_class_methods",
 ]
 
 
@@ -75,12 +76,12 @@ class Stats(ctypes.Structure):
     _fields_ = [("n_eri", ctypes.c_int64), ("n_shell_quartets", ctypes.c_int64),
                 ("n_prim_quartets", ctypes.c_int64), ("n_fp32_quartets", ctypes.c_int64),
                 ("n_screened", ctypes.c_int64), ("n_kernel_launches", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("device_ms", ctypes.c_double),
+                ("n_fp32_launches", ctypes.c_int32), ("device_ms", ctypes.c_double),
                 ("n_prim_pairs", ctypes.c_int64), ("n_prim_pairs_kept", ctypes.c_int64),
                 ("plan_ms", ctypes.c_double * 4)]
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "plan_ms")}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "plan_ms"}
         d["plan_ms"] = list(self.plan_ms)
         return d
 
@@ -120,6 +121,7 @@ def load_library(path: Path | str | None = None):
         "molints_plan_create_batch": (ctypes.c_int, [P, I32, P, P, P]),
         "molints_plan_npacked": (I64, [P]),
         "molints_set_class_methods": (ctypes.c_int, [P, P, I32]),
+        "molints_get_class_methods": (ctypes.c_int, [P, P, I32]),
         "molints_serve_start": (ctypes.c_int, [P, I32, I64]),
         "molints_serve_stop": (ctypes.c_int, [P]),
         "molints_submit": (ctypes.c_int, [P, P, P, P]),
@@ -371,7 +373,9 @@ class Engine:
 
     def set_class_methods(self, table=None):
         """Per class pair method for METHOD_AUTO plans: ``table[(x, y)] = METHOD_HGP or
-        METHOD_RYS`` for pair-class indices x >= y (PAIR_CLASSES order); None resets."""
+        METHOD_RYS`` (optionally | CLASS_NO_FP32) for pair-class indices x >= y (PAIR_CLASSES
+        order); missing entries are AUTO (HGP).  None restores the library's default table (the
+        tuned one on a B200)."""
         if table is None:
             self._check(self.lib.molints_set_class_methods(self.ctx, None, 0))
             return
@@ -379,6 +383,13 @@ class Engine:
         for (x, y), m in dict(table).items():
             arr[x * NUM_PAIR_CLASSES + y] = m
         self._check(self.lib.molints_set_class_methods(self.ctx, _ptr(arr), arr.size))
+
+    def class_methods(self) -> dict:
+        """The context's current table as {(x, y): entry} for x >= y."""
+        arr = np.zeros(NUM_PAIR_CLASSES * NUM_PAIR_CLASSES, dtype=np.int32)
+        self._check(self.lib.molints_get_class_methods(self.ctx, _ptr(arr), arr.size))
+        return {(x, y): int(arr[x * NUM_PAIR_CLASSES + y])
+                for x in range(NUM_PAIR_CLASSES) for y in range(x + 1)}
 
     # ---- serving
     def serve_start(self, nslots: int = 4, hbm_budget_bytes: int = 0):

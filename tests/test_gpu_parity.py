@@ -118,6 +118,37 @@ def test_split_valence_24_full(eng, oracle):
     assert excess.max() < TOL_FP64, (excess.max(), int(np.argmax(excess)))
 
 
+def test_auto_output_falls_back_to_direct_under_budget():
+    """AUTO takes the two-phase output for a large molecule (2^25+ integrals), whose scratch is
+    about as large as the output.  Under an HBM budget that the scratch does not fit, AUTO plans
+    still succeed with the direct stores (the same vector bit for bit); an explicit TWO_PHASE
+    plan fails with MOLINTS_ERR_BUDGET."""
+    import torch
+    from molints_b200 import engine
+    sh = mi.config3_molecule(0)  # 134 functions, 40.9 M integrals (327 MB)
+    assert sh.npacked >= 1 << 25
+    small = engine.Engine(0, hbm_budget_bytes=150 * 2**20)
+    big = engine.Engine(0)
+    outs = []
+    try:
+        for e, mode in ((small, engine.OUTPUT_AUTO), (big, engine.OUTPUT_DIRECT)):
+            e.set_stream(torch.cuda.current_stream().cuda_stream)
+            plan = e.plan(sh, output=mode)
+            out = torch.full((sh.npacked,), float("nan"), dtype=torch.float64, device="cuda")
+            plan.execute(out.data_ptr())
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy())
+            plan.close()
+            e.set_stream(None)
+        with pytest.raises(engine.MolintsError) as ex:
+            small.plan(sh, output=engine.OUTPUT_TWO_PHASE)
+        assert ex.value.status == -3
+    finally:
+        small.close()
+        big.close()
+    assert not np.isnan(outs[0]).any() and np.array_equal(outs[0], outs[1])
+
+
 def test_two_phase_output_equals_direct(eng):
     """The two-phase output (quartet blocks into a class-major scratch, then the packed vector
     gathered in order) gives the direct path's vector bit for bit: HGP and Rys classes (an f
@@ -211,9 +242,24 @@ def test_mixed_precision_error_bound(eng, cfg):
     cut, table = autotune.tune_fp32_cutoff(eng, sh)
     assert cut > 0, table
     ref = eng.eri_packed(sh)
-    got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cut, with_stats=True)
-    assert st["n_fp32_quartets"] > 0
+    # HGP everywhere with every FP32 variant enabled, so that FP32 kernels certainly run
+    eng.set_class_methods({})
+    try:
+        got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cut, with_stats=True)
+        plan = eng.plan(sh, precision=engine.MIXED, fp32_cutoff=cut)
+        import torch
+        out = torch.empty(sh.npacked, dtype=torch.float64, device="cuda")
+        plan.execute(out.data_ptr())
+        pst = plan.stats()
+        plan.close()
+    finally:
+        eng.set_class_methods(None)
+    assert st["n_fp32_quartets"] > 0 and st["n_fp32_launches"] > 0, st
+    assert pst["n_fp32_launches"] == st["n_fp32_launches"]
     assert np.max(np.abs(got - ref)) < TOL_MIXED
+    # with the shipped default table, the stats count FP32 quartets only where FP32 kernels run
+    _, st_def = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cut, with_stats=True)
+    assert (st_def["n_fp32_quartets"] > 0) == (st_def["n_fp32_launches"] > 0), st_def
 
 
 def test_primitive_screening_bound(eng, oracle):
@@ -419,6 +465,13 @@ def test_class_method_table(eng):
     finally:
         eng.set_class_methods(None)
     assert any(n.startswith("rys_") for n in names) and any(n.startswith("eri_") for n in names)
+    # None restores the shipped default: on a B200 the tuned table (Rys for (dd|dd))
+    import torch
+    if torch.cuda.get_device_name(0).startswith("NVIDIA B200"):
+        assert eng.class_methods()[(6, 6)] & 3 == engine.METHOD_RYS
+        fresh = engine.Engine(0)
+        assert fresh.class_methods() == eng.class_methods()
+        fresh.close()
     assert np.max(np.abs(mix - hgp)) < TOL_FP64
     with pytest.raises(engine.MolintsError):
         eng.set_class_methods({(0, 0): 7})
@@ -456,9 +509,13 @@ def test_rys_mixed_error_bound(eng):
         cut, table = autotune.tune_fp32_cutoff(eng, sh, method=engine.METHOD_RYS)
         assert cut > 0, table
         ref = eng.eri_packed(sh, method=engine.METHOD_RYS)
-        got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cut, method=engine.METHOD_RYS,
-                                 with_stats=True)
-        assert st["n_fp32_quartets"] > 0
+        eng.set_class_methods({})  # every FP32 variant enabled
+        try:
+            got, st = eng.eri_packed(sh, precision=engine.MIXED, fp32_cutoff=cut,
+                                     method=engine.METHOD_RYS, with_stats=True)
+        finally:
+            eng.set_class_methods(None)
+        assert st["n_fp32_quartets"] > 0 and st["n_fp32_launches"] > 0, st
         assert np.max(np.abs(got - ref)) < TOL_MIXED
 
 
