@@ -49,6 +49,15 @@ struct molints_ctx {
     double *boys_scaled = nullptr;  // per-M tables F_{M+k}(T_n)/k!, k < 8, and e^-T_n
     double *out_cache = nullptr;  // device buffer for host-output calls
     int64_t out_cache_len = 0;
+    // Two-phase output scratch, shared by the context's plans (it is needed only while an
+    // execute runs): grown to the largest plan's need and kept.  scratch_gen counts the
+    // reallocations (a captured graph holds the address); scratch_ev orders the executes that
+    // use it, whatever stream each is launched on.
+    double *scratch = nullptr;
+    int64_t scratch_len = 0;
+    int scratch_gen = 0;
+    cudaEvent_t scratch_ev = nullptr;
+    bool scratch_ev_live = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // class-pair kernels run concurrently on side streams forked from `stream`
     static constexpr int kSide = 6;
@@ -110,7 +119,8 @@ struct molints_plan {
     // two-phase output (molints_output): the class kernels store whole quartet blocks into a
     // class-major scratch, a gather pass writes the packed vector in order from it
     int two_phase = 0;
-    double *scratch = nullptr;         // per (class pair, molecule) region of quartet blocks
+    int64_t scratch_need = 0;          // doubles of the context's scratch an execute uses: per
+                                       // (class pair, molecule) a region of quartet blocks
     long long *chunk_slot = nullptr;   // per chunk: scratch offset of its first quartet's block
     int2 *g_fn = nullptr;              // per function (all molecules): {shell in molecule, component}
     int *g_pair = nullptr;             // per molecule shell pair I >= J: pos << 5 | class << 1 | A == J
@@ -126,6 +136,7 @@ struct molints_plan {
     int use_graph = 0;
     cudaGraphExec_t gexec = nullptr;
     double *graph_out = nullptr;
+    int graph_gen = -1;                // the context's scratch_gen at capture
     // per-launch profiling (molints_plan_set_profiling)
     int profiling = 0;
     std::vector<cudaEvent_t> prof_ev;
@@ -213,6 +224,28 @@ int dev_alloc(molints_ctx *ctx, T **p, size_t count, int64_t *tally) {
 
 void dev_free(molints_ctx *ctx, void *p) {
     if (p) cudaFreeAsync(p, ctx->stream);
+}
+
+// The context's two-phase scratch grown to at least `need` doubles (the old buffer is freed in
+// stream order, after the executes that used it).
+int ctx_scratch(molints_ctx *ctx, int64_t need) {
+    need = std::max<int64_t>(need, 1);
+    if (ctx->scratch_len >= need) return MOLINTS_OK;
+    if (ctx->scratch) {
+        if (ctx->scratch_ev_live) cudaStreamWaitEvent(ctx->stream, ctx->scratch_ev, 0);
+        dev_free(ctx, ctx->scratch);
+        ctx->held -= ctx->scratch_len * (int64_t)sizeof(double);
+        ctx->scratch = nullptr;
+        ctx->scratch_len = 0;
+    }
+    int rc = dev_alloc(ctx, &ctx->scratch, (size_t)need, nullptr);
+    if (rc) {
+        ctx->scratch = nullptr;
+        return rc;
+    }
+    ctx->scratch_len = need;
+    ++ctx->scratch_gen;
+    return MOLINTS_OK;
 }
 
 // The pinned upload buffer of the context, grown to at least `bytes` (a pinned source makes
@@ -586,6 +619,7 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
         ok = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&ctx->join[i], cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&ctx->scratch_ev, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         molints_destroy(ctx);
         return MOLINTS_ERR_CUDA;
@@ -658,6 +692,7 @@ int molints_destroy(molints_ctx *ctx) {
         dev_free(ctx, ctx->boys_tab);
         dev_free(ctx, ctx->boys_scaled);
         dev_free(ctx, ctx->out_cache);
+        dev_free(ctx, ctx->scratch);
         cudaStreamSynchronize(ctx->own_stream);
     }
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
@@ -672,6 +707,7 @@ int molints_destroy(molints_ctx *ctx) {
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
+    if (ctx->scratch_ev) cudaEventDestroy(ctx->scratch_ev);
     if (ctx->stage) cudaFreeHost(ctx->stage);
     delete ctx;
     return MOLINTS_OK;
@@ -761,7 +797,7 @@ static void plan_release_device(molints_plan *p) {
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
-                    p->scratch, p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows};
+                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
     p->ctx = nullptr;
@@ -1281,12 +1317,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         // The scratch (about npacked doubles) is taken now.  If it does not fit the budget or
         // the device, AUTO falls back to the direct stores, which need no scratch; only an
         // explicit MOLINTS_OUTPUT_TWO_PHASE fails.
-        const int64_t held0 = p->bytes;
-        int src = dev_alloc(ctx, &p->scratch, (size_t)std::max<int64_t>(scratch_len, 1), &p->bytes);
+        int src = ctx_scratch(ctx, scratch_len);
         if (src && opts.output == MOLINTS_OUTPUT_AUTO) {
             cudaGetLastError();  // an out-of-memory status is not sticky; clear it
-            p->scratch = nullptr;
-            p->bytes = held0;
             p->two_phase = 0;
             region_h.clear();
             scratch_len = 0;
@@ -1295,6 +1328,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             plan_free(p);
             return src;
         }
+        p->scratch_need = scratch_len;
     }
     std::vector<QueueTask> tasks;
     std::vector<int> task_end(cps.size(), 0), cp_width(cps.size(), 32 * widen);
@@ -1623,7 +1657,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         Q.screen_cut = p->opts.screen_cutoff;
         Q.fp32_cut = p->opts.fp32_cutoff;
         if (p->two_phase && !jk.J) {
-            Q.scratch = p->scratch;
+            Q.scratch = ctx->scratch;
             Q.chunk_slot = p->chunk_slot + p->q_off[x][y];
         }
         // HGP: one warp per chunk, four per block; Rys: the launcher divides by its groups/block
@@ -1645,7 +1679,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         // second phase: the packed vector in order from the scratch blocks
         if (int rc = mark(launches, "gather_packed", 0, s)) return rc;
         const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, p->n_rows);
-        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, p->scratch, p->g_fn, p->g_pair,
+        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_fn, p->g_pair,
                                                              p->g_region, p->g_mol, p->g_rows, p->nmol,
                                                              p->n_rows);
         if (int rc = mark(launches, "gather_packed", 1, s)) return rc;
@@ -1672,16 +1706,31 @@ static void plan_occupancy(molints_plan *p) {
         }
 }
 
+static int plan_execute_impl(molints_plan *p, double *out_device);
+
 int molints_plan_execute(molints_plan *p, double *out_device) {
     if (!p || (!out_device && p->npacked > 0))
         return fail(p ? p->ctx : nullptr, MOLINTS_ERR_INVALID, "plan_execute: null argument");
     if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    // executes that use the context's shared scratch run one after another
+    const bool uses_scratch = p->two_phase && p->npacked > 0;
+    if (uses_scratch && ctx->scratch_ev_live) MI_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->scratch_ev, 0));
+    int rc = plan_execute_impl(p, out_device);
+    if (!rc && uses_scratch) {
+        MI_CUDA(ctx, cudaEventRecord(ctx->scratch_ev, ctx->stream));
+        ctx->scratch_ev_live = true;
+    }
+    return rc;
+}
+
+static int plan_execute_impl(molints_plan *p, double *out_device) {
+    molints_ctx *ctx = p->ctx;
     if (!p->use_graph || p->profiling) return plan_enqueue(p, out_device, true);
-    // CUDA graph: captured once per output pointer, then launched as a whole
+    // CUDA graph: captured once per output pointer (and scratch buffer), then launched whole
     cudaStream_t s = ctx->stream;
-    if (!p->gexec || p->graph_out != out_device) {
+    if (!p->gexec || p->graph_out != out_device || (p->two_phase && p->graph_gen != ctx->scratch_gen)) {
         if (p->gexec) {
             cudaGraphExecDestroy(p->gexec);
             p->gexec = nullptr;
@@ -1706,6 +1755,7 @@ int molints_plan_execute(molints_plan *p, double *out_device) {
             return cuda_fail(ctx, e, "cudaGraphInstantiate");
         }
         p->graph_out = out_device;
+        p->graph_gen = ctx->scratch_gen;
     }
     MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
     MI_CUDA(ctx, cudaGraphLaunch(p->gexec, s));

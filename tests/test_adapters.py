@@ -69,7 +69,9 @@ def test_coulomb_repulsion_known_answers(golden, oracle):
 
 
 @gpu
-def test_coulomb_pgbf_and_distance_sweep(golden):
+def test_coulomb_pgbf_and_distance_sweep(golden, oracle):
+    """The reference's pyquante2 values hold to its own rtol (about 1.5e-8: pyquante2's Boys
+    approximation), and the oracle's Huzinaga values to 1e-12."""
     _cuda()
     m = M.MolecularIntegrals()
     s = M.PGBF(1.0)
@@ -80,7 +82,13 @@ def test_coulomb_pgbf_and_distance_sweep(golden):
     assert abs(m.coulomb(c, c, c, c) - golden["coulomb"]["c,c,c,c"]["value"]) < 1e-8
     for g in golden["ss_distance_sweep"]:
         s3 = M.PGBF(1.0, (0.0, 0.0, g["r"]))
-        assert abs(m.coulomb_pgbf(s, s, s3, s3) - g["value"]) < 2e-9, g
+        v = m.coulomb_pgbf(s, s, s3, s3)
+        assert abs(v - g["value"]) <= 1.5e-8 * abs(g["value"]), g
+        o = (0.0, 0.0, 0.0)
+        with oracle.exact_boys():
+            ref = oracle.coulomb_prim((1.0, o, o), (1.0, o, o), (1.0, (0, 0, g["r"]), o),
+                                      (1.0, (0, 0, g["r"]), o)) * s.norm ** 4
+        assert abs(v - ref) < 1e-12, (g, v, ref)
 
 
 @gpu
