@@ -397,10 +397,13 @@ def run_ours(args):
 
 def measure_roofline(plans, groups, mols, out, stream, dev):
     """One serialised profiling pass of the FP64 plans (per-launch CUDA events on the launching
-    stream): per class kernel its device time over the whole batch and its algorithmic FLOP
-    (flops.py, summed over the molecules), the dominant kernel's FP64 roofline fraction
-    against the FP64 DGEMM peak measured here, and the DRAM traffic recorded by ncu for that
-    kernel (profiles/, scaled per launch) when present."""
+    stream), per kernel its device time over the whole batch.  The dominant kernel gets the
+    roofline: the gather pass of the two-phase output is HBM-bound (16 algorithmic bytes per
+    packed integral: one scratch read, one output write; peak = MEASURED_PEAKS.json hbm_gbs),
+    a class kernel FP64-bound (flops.py algorithmic FLOP over all primitive quartets; peak =
+    FP64 DGEMM measured here).  The top class kernel is reported beside it, also against the
+    FLOP of the primitive quartets it evaluates (after primitive-pair screening).  DRAM
+    traffic comes from an ncu capture recorded in profiles/ when one exists for the kernel."""
     from molints_b200 import flops as F
     per_tag = {}
     for g in groups:
@@ -408,8 +411,8 @@ def measure_roofline(plans, groups, mols, out, stream, dev):
             w, _ = F.workload(mols[i])
             for tag, d in w.items():
                 per_tag[tag] = per_tag.get(tag, 0.0) + d["flop"]
-    times = {}
-    nlaunch = {}
+    times, nlaunch, executed = {}, {}, {}
+    lv = {"s": 0, "p": 1, "d": 2, "f": 3}
     for p in plans:
         p.set_profiling(True)
         p.execute(out.data_ptr())
@@ -417,24 +420,49 @@ def measure_roofline(plans, groups, mols, out, stream, dev):
             times[name] = times.get(name, 0.0) + ms
             nlaunch[name] = nlaunch.get(name, 0) + 1
         p.set_profiling(False)
-    cls = {n: t for n, t in times.items() if n.startswith(("eri_", "rys_"))}
-    top = max(cls, key=cls.get)
-    flop = per_tag.get(top[4:], 0.0)
-    peak = measure_fp64_peak(dev)
-    ach = flop / (cls[top] * 1e-3) / 1e12
+        for tag, (nq, kq) in p.class_work().items():
+            la, lb, lc, ld = (lv[c] for c in tag)
+            executed[tag] = executed.get(tag, 0.0) + kq * F.per_prim_flops(la, lb, lc, ld) + \
+                nq * F.hrr_flops(la, lb, lc, ld)
     total_ms = sum(times.values())
-    traffic = None
+    peak64 = measure_fp64_peak(dev)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (copy)" if "hbm_gbs" in peaks else "fallback 6.65 TB/s"
+    traffic_db = {}
     tfile = ROOT / "profiles" / "dram_traffic_batch256.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("bytes_per_launch", {}).get(top)
-    return {"bound": "fp64", "kernel": top, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-            "frac": ach / peak, "traffic": traffic, "launches": nlaunch[top],
-            "kernel_ms_per_step": cls[top], "kernel_flop_per_step": flop,
-            "peak_source": "measured in this run: torch float64 8192^3 matmul (cuBLAS DGEMM); "
-                           "MEASURED_PEAKS.json has no FP64 figure",
-            "whole_step_tflops": sum(per_tag.values()) / (total_ms * 1e-3) / 1e12,
-            "serialised_ms": total_ms,
-            "share": {n: round(t / total_ms, 4) for n, t in sorted(times.items(), key=lambda x: -x[1])}}
+        traffic_db = json.loads(tfile.read_text()).get("bytes_per_integral", {})
+    n_eri = sum(p.npacked for p in plans)
+
+    def class_entry(name):
+        flop = per_tag.get(name[4:], 0.0)
+        ach = flop / (times[name] * 1e-3) / 1e12
+        ex = executed.get(name[4:], 0.0) / (times[name] * 1e-3) / 1e12
+        return {"bound": "fp64", "kernel": name, "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                "frac": ach / peak64, "executed_tflops": ex, "executed_frac": ex / peak64,
+                "launches": nlaunch[name], "kernel_ms_per_step": times[name],
+                "kernel_flop_per_step": flop, "executed_flop_per_step": executed.get(name[4:], 0.0),
+                "traffic": None,
+                "peak_source": "measured in this run: torch float64 8192^3 matmul (cuBLAS DGEMM); "
+                               "MEASURED_PEAKS.json has no FP64 figure"}
+    cls = [n for n in times if n.startswith(("eri_", "rys_"))]
+    top_cls = max(cls, key=times.get)
+    top = max(times, key=times.get)
+    if top == "gather_packed":
+        ach = 16.0 * n_eri / (times[top] * 1e-3) / 1e9
+        t = traffic_db.get(top)
+        roof = {"bound": "hbm", "kernel": top, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "launches": nlaunch[top], "kernel_ms_per_step": times[top],
+                "algorithmic_bytes_per_step": 16.0 * n_eri,
+                "traffic": None if t is None else t * n_eri / nlaunch[top], "peak_source": hbm_src}
+    else:
+        roof = class_entry(top)
+    roof["top_class_kernel"] = class_entry(top_cls)
+    roof["whole_step_tflops"] = sum(per_tag.values()) / (total_ms * 1e-3) / 1e12
+    roof["serialised_ms"] = total_ms
+    roof["share"] = {n: round(t / total_ms, 4) for n, t in sorted(times.items(), key=lambda x: -x[1])}
+    return roof
 
 
 def measure_fp64_peak(dev) -> float:

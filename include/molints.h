@@ -221,6 +221,12 @@ int molints_jk(molints_ctx *ctx, const molints_basis *basis, const molints_optio
  * out_device recaptures).  Not combined with profiling.  No reference counterpart. */
 int molints_plan_set_graph(molints_plan *plan, int enable);
 int molints_plan_stats(const molints_plan *plan, molints_stats *stats);
+/* Per class pair x >= y (entry x * MOLINTS_NUM_PAIR_CLASSES + y, n = MOLINTS_NUM_PAIR_CLASSES^2):
+ * the plan's shell quartets and the primitive quartets its kernels evaluate (the primitive
+ * pairs kept after prim_cutoff; screen_cutoff not applied), for work accounting.  Host only.
+ * No reference counterpart. */
+int molints_plan_class_work(const molints_plan *plan, int64_t *quartets, double *prim_quartets,
+                            int32_t n);
 int molints_plan_destroy(molints_plan *plan);
 
 /* Contracted Schwarz bounds Q_ab = sqrt(max |(ab|ab)|) of the plan's shell pairs (computed

@@ -2995,9 +2995,13 @@ __global__ void __launch_bounds__(128) eri_queue_ddpp(const EriQueue Q) {
             if constexpr (JK) {
                 jk_ddpp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
             } else if (Q.scratch) {
-                double *__restrict__ dst = Q.scratch + __ldg(&Q.chunk_slot[c]) + (long long)(base + kq) * 324;
+                // tiles of kScratchTile quartets, component-major: for each component the
+                // chunk's lanes store consecutive doubles
+                const long long u = __ldg(&Q.chunk_slot[c]) + base + kq;
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
+                    (u & ~(long long)(kScratchTile - 1)) * 324 + (u & (kScratchTile - 1));
 #pragma unroll
-                for (int x = 0; x < 324; ++x) dst[x] = res[x];
+                for (int x = 0; x < 324; ++x) dst[x * kScratchTile] = res[x];
             } else {
                 store_ddpp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
                             p == q, res);

@@ -124,8 +124,10 @@ struct molints_plan {
     long long *chunk_slot = nullptr;   // per chunk: scratch offset of its first quartet's block
     int2 *g_fn = nullptr;              // per function (all molecules): {shell in molecule, component}
     int *g_pair = nullptr;             // per molecule shell pair I >= J: pos << 5 | class << 1 | A == J
-    long long *g_region = nullptr;     // per (x, y, molecule): {scratch offset, first bra, first ket, kets}
-    long long *g_mol = nullptr;        // per molecule: {first function, first pair entry, packed offset, packed}
+    long long *g_region = nullptr;     // per (x, y, molecule): {scratch offset, first bra, first ket, kets, tile}
+    long long *g_mol = nullptr;        // per molecule: {first function, first pair entry, packed offset,
+                                       // first function-pair entry of g_col}
+    int2 *g_col = nullptr;             // per function pair of every molecule: gather_cols_kernel
     int2 *g_rows = nullptr;            // gather order: {molecule, row ij}, the rows of one shell pair together
     int64_t n_rows = 0;
     int64_t bytes = 0;
@@ -422,49 +424,80 @@ __device__ __forceinline__ long long untri_f(long long t) {
 
 constexpr int kGatherThreads = 256;
 
+// Per function pair (i >= j) of every molecule of a two-phase plan, what the gather needs to
+// place its entries, built once per plan on the device: x = list position << 4 | pair class of
+// the shell pair holding (i, j), y = component of the function in that pair's A << 16 |
+// component in its B.  Entry (m, ij) is at col[mol[4m+3] + ij]; rows[] lists each (m, ij)
+// exactly once.
+__global__ void gather_cols_kernel(int2 *__restrict__ col, const int2 *__restrict__ fn,
+                                   const int *__restrict__ pairs, const long long *__restrict__ mol,
+                                   const int2 *__restrict__ rows, long long nrows) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    const int2 mr = __ldg(&rows[r]);
+    const int m = mr.x;
+    const long long ij = mr.y;
+    const long long fb = __ldg(&mol[4 * m]), pb = __ldg(&mol[4 * m + 1]);
+    const long long i = untri_f(ij), j = ij - i * (i + 1) / 2;
+    const int2 fi = __ldg(&fn[fb + i]), fj = __ldg(&fn[fb + j]);
+    const int P = __ldg(&pairs[pb + (long long)fi.x * (fi.x + 1) / 2 + fj.x]);
+    const int ca = (P & 1) ? fj.y : fi.y, cb = (P & 1) ? fi.y : fj.y;
+    col[__ldg(&mol[4 * m + 3]) + ij] = make_int2(((P >> 5) << 4) | ((P >> 1) & 15), (ca << 16) | cb);
+}
+
 // Second phase of the two-phase output: the packed vector written row by row from the scratch
 // blocks.  A block of threads writes one row ij (function pair i >= j) whole, columns kl =
-// 0..ij in order, so the stores are coalesced; rows[] lists the rows shell pair by shell pair,
-// so the rows of one pair P, which read the same scratch blocks (P's bra row of each class
-// region, or P's column of the regions where P is the ket), run at the same time and find
-// them in L2.  Each entry comes from the block and component the direct path would have
-// stored it from: row ij >= column kl, shell pairs P (from ij) and Q (from kl); the quartet's
-// bra is the pair of the higher class, or of the later list position within a class (P for the
-// diagonal quartet P == Q); a pair's components are taken in its A, B orientation, with the
-// larger component first within a same-shell pair, as the direct store conditions pick.
+// 0..ij in order, so the stores are coalesced and so are the reads of the column descriptors;
+// rows[] lists the rows shell pair by shell pair, so the rows of one pair P, which read the same
+// scratch blocks (P's bra row of each class region, or P's column of the regions where P is the
+// ket), run at the same time and find them in L2.  The row's pair P fixes one class of each
+// region an entry can come from: the block stages those regions (P as bra, P as ket; one per
+// class of the other pair) in shared memory.  Each entry comes from the block and component the
+// direct path would have stored it from: the quartet's bra is the pair of the higher class, or
+// of the later list position within a class (P for the diagonal quartet P == Q); a pair's
+// components are taken in its A, B orientation, with the larger component first within a
+// same-shell pair, as the direct store conditions pick.
 __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
-    double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ fn,
-    const int *__restrict__ pairs, const long long *__restrict__ region, const long long *__restrict__ mol,
+    double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ col,
+    const long long *__restrict__ region, const long long *__restrict__ mol,
     const int2 *__restrict__ rows, int nmol, long long nrows) {
+    // [P as bra, P as ket][class of the other pair]: {scratch offset, first bra, first ket,
+    // kets, tile, block size}
+    __shared__ long long reg[2][kNumPairClasses][6];
     for (long long r = blockIdx.x; r < nrows; r += gridDim.x) {
         const int2 mr = __ldg(&rows[r]);
         const int m = mr.x;
         const long long ij = mr.y;
-        const long long fb = __ldg(&mol[4 * m]), pb = __ldg(&mol[4 * m + 1]);
+        const long long cbase = __ldg(&mol[4 * m + 3]);
         double *__restrict__ orow = out + __ldg(&mol[4 * m + 2]) + ij * (ij + 1) / 2;
-        const long long i = untri_f(ij), j = ij - i * (i + 1) / 2;
-        const int2 fi = __ldg(&fn[fb + i]), fj = __ldg(&fn[fb + j]);
-        const int P = __ldg(&pairs[pb + (long long)fi.x * (fi.x + 1) / 2 + fj.x]);
-        const int posP = P >> 5, clsP = (P >> 1) & 15;
-        const int pa = (P & 1) ? fj.y : fi.y, pbc = (P & 1) ? fi.y : fj.y;
-        long long k = untri_f(threadIdx.x), l = threadIdx.x - k * (k + 1) / 2;
+        const int2 pe = __ldg(&col[cbase + ij]);
+        const int posP = pe.x >> 4, clsP = pe.x & 15;
+        const int pa = pe.y >> 16, pbc = pe.y & 0xffff;
+        __syncthreads();  // the previous row's readers are done with reg
+        if (threadIdx.x < 2 * kNumPairClasses) {
+            const int o = threadIdx.x / kNumPairClasses, t = threadIdx.x % kNumPairClasses;
+            const int x = o == 0 ? clsP : t, y = o == 0 ? t : clsP;
+            if (x >= y) {
+                const long long *rg = region + kRegionFields * (((long long)x * kNumPairClasses + y) * nmol + m);
+                for (int f = 0; f < kRegionFields; ++f) reg[o][t][f] = __ldg(&rg[f]);
+                reg[o][t][5] = (long long)c_pair_na[x] * c_pair_nb[x] * c_pair_na[y] * c_pair_nb[y];
+            }
+        }
+        __syncthreads();
         for (long long kl = threadIdx.x; kl <= ij; kl += kGatherThreads) {
-            while (l > k) { l -= k + 1; ++k; }  // kl advanced by kGatherThreads since the last entry
-            const int2 fk = __ldg(&fn[fb + k]), fl = __ldg(&fn[fb + l]);
-            const int Q = __ldg(&pairs[pb + (long long)fk.x * (fk.x + 1) / 2 + fl.x]);
-            const int posQ = Q >> 5, clsQ = (Q >> 1) & 15;
-            const int qa = (Q & 1) ? fl.y : fk.y, qb = (Q & 1) ? fk.y : fl.y;
+            const int2 qe = __ldg(&col[cbase + kl]);
+            const int posQ = qe.x >> 4, clsQ = qe.x & 15;
+            const int qa = qe.y >> 16, qb = qe.y & 0xffff;
             const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
-            const int x = braP ? clsP : clsQ, y = braP ? clsQ : clsP;
+            const long long *rg = reg[braP ? 0 : 1][clsQ];
+            const int y = braP ? clsQ : clsP;
             const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
             const int ma = braP ? pa : qa, mb = braP ? pbc : qb, mc = braP ? qa : pa, md = braP ? qb : pbc;
-            const long long *rg = region + 4 * (((long long)x * kNumPairClasses + y) * nmol + m);
-            const long long db = bpos - __ldg(&rg[1]), dk = kpos - __ldg(&rg[2]);
-            const long long slot = (x == y) ? db * (db + 1) / 2 + dk : db * __ldg(&rg[3]) + dk;
-            const int na = c_pair_na[x], nb = c_pair_nb[x], nc = c_pair_na[y], nd = c_pair_nb[y];
-            const long long blk = (long long)na * nb * nc * nd;
-            orow[kl] = __ldg(&scratch[__ldg(&rg[0]) + slot * blk + ((ma * nb + mb) * nc + mc) * nd + md]);
-            l += kGatherThreads;
+            const long long db = bpos - rg[1], dk = kpos - rg[2];
+            const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
+            const int nb = c_pair_nb[braP ? clsP : clsQ], nc = c_pair_na[y], nd = c_pair_nb[y];
+            const long long tile = rg[4], u0 = slot & (tile - 1);  // tile: 1 or kScratchTile
+            orow[kl] = __ldg(&scratch[rg[0] + (slot - u0) * rg[5] + (((ma * nb + mb) * nc + mc) * nd + md) * tile + u0]);
         }
     }
 }
@@ -797,7 +830,7 @@ static void plan_release_device(molints_plan *p) {
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
-                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows};
+                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows, p->g_col};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
     p->ctx = nullptr;
@@ -1281,7 +1314,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         int ci = 0, pb0 = 0, pb1 = 0;
         std::vector<int4> raw;
         std::vector<unsigned char> bk;
-        std::vector<long long> slot;  // two-phase: scratch offset of each chunk's first block
+        std::vector<long long> slot;  // two-phase: region slot of each chunk's first quartet
         int64_t cnt[kBuckets] = {};
         int64_t base[kBuckets] = {};
         double total = 0.0;
@@ -1289,9 +1322,13 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<std::pair<int, int>> cps;
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) cps.push_back({x, y});
-    // two-phase scratch: per (class pair, molecule) a region of quartet blocks, bra-major
-    // (the triangle q <= p for equal classes); region_h[((x nc + y) nmol + m) 4 ..] =
-    // {offset in doubles, first bra pair, first ket pair, ket pairs}
+    // two-phase scratch: per (class pair, molecule) a region of quartet blocks in slot order,
+    // bra-major (the triangle q <= p for equal classes); region_h[((x nc + y) nmol + m) 5 ..] =
+    // {offset in doubles, first bra pair, first ket pair, ket pairs, tile}.  Quartet slot t,
+    // component x is at offset + (t - t % tile) * block + x * tile + t % tile: the HGP class
+    // kernels, whose lanes hold consecutive quartets, write tiles of kScratchTile quartets
+    // component-major (each component of a chunk is one coalesced run); the Rys kernels, whose
+    // thread groups write one quartet's block at a time, keep tile 1 (block after block).
     if (npair >= (1 << 26)) p->two_phase = 0;  // the gather's pair entries hold the position in 26 bits
     auto ncomp_of = [](int x, int y) {
         return (int64_t)ncart(kPairClassLa[x]) * ncart(kPairClassLb[x]) * ncart(kPairClassLa[y]) * ncart(kPairClassLb[y]);
@@ -1299,7 +1336,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     std::vector<long long> region_h;
     int64_t scratch_len = 0;
     if (p->two_phase) {
-        region_h.assign((size_t)kNumPairClasses * kNumPairClasses * nmol * 4, 0);
+        region_h.assign((size_t)kNumPairClasses * kNumPairClasses * nmol * kRegionFields, 0);
         for (const auto &cp : cps)
             for (int m = 0; m < nmol; ++m) {
                 const int x = cp.first, y = cp.second;
@@ -1307,12 +1344,15 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 range_of(x, m, b0, b1);
                 range_of(y, m, k0, k1);
                 const int64_t nb = b1 - b0, nk = k1 - k0;
-                long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * 4];
+                long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * kRegionFields];
+                const int64_t tile = p->method[x][y] == MOLINTS_METHOD_RYS ? 1 : kScratchTile;
+                const int64_t nslot = x == y ? nb * (nb + 1) / 2 : nb * nk;
                 rg[0] = scratch_len;
                 rg[1] = b0;
                 rg[2] = k0;
                 rg[3] = nk;
-                scratch_len += (x == y ? nb * (nb + 1) / 2 : nb * nk) * ncomp_of(x, y);
+                rg[4] = tile;
+                scratch_len += (nslot + tile - 1) / tile * tile * ncomp_of(x, y);
             }
         // The scratch (about npacked doubles) is taken now.  If it does not fit the budget or
         // the device, AUTO falls back to the direct stores, which need no scratch; only an
@@ -1422,9 +1462,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 T.raw.push_back(make_int4(pb, q0, n | (lg << 16), m));
                 T.bk.push_back((unsigned char)b);
                 if (p->two_phase) {
-                    const long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * 4];
+                    const long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * kRegionFields];
                     const long long db = pb - rg[1], dk = q0 - rg[2];
-                    T.slot.push_back(rg[0] + (x == y ? db * (db + 1) / 2 + dk : db * rg[3] + dk) * ncomp_of(x, y));
+                    T.slot.push_back(x == y ? db * (db + 1) / 2 + dk : db * rg[3] + dk);
                 }
                 ++cnt[b];
                 q0 += n;
@@ -1490,6 +1530,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         int2 *gfn = reinterpret_cast<int2 *>(stage + o_gfn);
         int *gpair = reinterpret_cast<int *>(stage + o_gpair);
         long long *gmol = reinterpret_cast<long long *>(stage + o_gmol);
+        long long cbase = 0;
         std::vector<int64_t> pbase(nmol + 1, 0);
         for (int m = 0, fb = 0; m < nmol; ++m) {
             pbase[m + 1] = pbase[m] + (int64_t)bases[m].nshell * (bases[m].nshell + 1) / 2;
@@ -1500,7 +1541,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             gmol[4 * m] = fb;
             gmol[4 * m + 1] = pbase[m];
             gmol[4 * m + 2] = (long long)p->mol_out_h[m];
-            gmol[4 * m + 3] = (long long)molints_npacked(mol_nbf[m]);
+            gmol[4 * m + 3] = cbase;
+            cbase += mol_nbf[m] * (mol_nbf[m] + 1) / 2;
             fb += (int)mol_nbf[m];
         }
         for (int k = 0; k < npair; ++k) {
@@ -1546,6 +1588,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         if (!rc) rc = dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_rows, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->g_col, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
     }
     if (rc) { plan_free(p); return rc; }
     if (tp && ((nq > 0 && (e = cudaMemcpyAsync(p->chunk_slot, stage + o_slot, (size_t)nq * sizeof(long long),
@@ -1562,6 +1605,11 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                                                        cudaMemcpyHostToDevice, s))))) {
         plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
+    }
+    if (tp && nrows_all > 0) {
+        gather_cols_kernel<<<(unsigned)((nrows_all + 255) / 256), 256, 0, s>>>(p->g_col, p->g_fn, p->g_pair,
+                                                                            p->g_mol, p->g_rows, nrows_all);
+        if ((e = cudaGetLastError())) { plan_free(p); return cuda_fail(ctx, e, "plan_create gather columns"); }
     }
     if ((e = cudaMemcpyAsync(p->pair_ab, stage + o_ab, npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, stage + o_info, npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
@@ -1659,6 +1707,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         if (p->two_phase && !jk.J) {
             Q.scratch = ctx->scratch;
             Q.chunk_slot = p->chunk_slot + p->q_off[x][y];
+            Q.region = p->g_region + ((size_t)x * kNumPairClasses + y) * p->nmol * kRegionFields;
         }
         // HGP: one warp per chunk, four per block; Rys: the launcher divides by its groups/block
         const int grid = rys ? occ * ctx->num_sms
@@ -1679,7 +1728,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         // second phase: the packed vector in order from the scratch blocks
         if (int rc = mark(launches, "gather_packed", 0, s)) return rc;
         const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, p->n_rows);
-        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_fn, p->g_pair,
+        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col,
                                                              p->g_region, p->g_mol, p->g_rows, p->nmol,
                                                              p->n_rows);
         if (int rc = mark(launches, "gather_packed", 1, s)) return rc;
@@ -1888,6 +1937,34 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) st->device_ms = ms;
     }
+    return MOLINTS_OK;
+}
+
+int molints_plan_class_work(const molints_plan *p, int64_t *quartets, double *prim_quartets, int32_t n) {
+    if (!p || !quartets || !prim_quartets || n != kNumPairClasses * kNumPairClasses) return MOLINTS_ERR_INVALID;
+    const int nc = kNumPairClasses;
+    for (int k = 0; k < n; ++k) { quartets[k] = 0; prim_quartets[k] = 0.0; }
+    // per (molecule, pair class): pair count, sum and sum of squares of kept primitive pairs
+    std::vector<double> cnt((size_t)std::max(p->nmol, 1) * nc, 0.0), sum(cnt.size(), 0.0), sq(cnt.size(), 0.0);
+    for (int c = 0; c < nc; ++c)
+        for (int k = p->class_start[c]; k < p->class_start[c + 1]; ++k) {
+            const size_t i = (size_t)p->pair_mol[k] * nc + c;
+            cnt[i] += 1.0;
+            sum[i] += p->npp_h[k];
+            sq[i] += (double)p->npp_h[k] * p->npp_h[k];
+        }
+    for (int m = 0; m < p->nmol; ++m)
+        for (int x = 0; x < nc; ++x)
+            for (int y = 0; y <= x; ++y) {
+                const size_t a = (size_t)m * nc + x, b = (size_t)m * nc + y;
+                if (x == y) {
+                    quartets[x * nc + y] += (int64_t)(cnt[a] * (cnt[a] + 1) / 2);
+                    prim_quartets[x * nc + y] += (sum[a] * sum[a] + sq[a]) / 2;
+                } else {
+                    quartets[x * nc + y] += (int64_t)(cnt[a] * cnt[b]);
+                    prim_quartets[x * nc + y] += sum[a] * sum[b];
+                }
+            }
     return MOLINTS_OK;
 }
 

@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = [
     "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
     "molints_release", "molints_serve_stats", "molints_shard_range", "molints_plan_create_shard",
     "molints_plan_set_graph", "molints_plan_jk", "molints_jk", "molints_one_e",
-    "molints_get_class_methods",
+    "molints_get_class_methods", "molints_plan_class_work",
 ]
 
 
@@ -122,6 +122,7 @@ def load_library(path: Path | str | None = None):
         "molints_plan_npacked": (I64, [P]),
         "molints_set_class_methods": (ctypes.c_int, [P, P, I32]),
         "molints_get_class_methods": (ctypes.c_int, [P, P, I32]),
+        "molints_plan_class_work": (ctypes.c_int, [P, P, P, I32]),
         "molints_serve_start": (ctypes.c_int, [P, I32, I64]),
         "molints_serve_stop": (ctypes.c_int, [P]),
         "molints_submit": (ctypes.c_int, [P, P, P, P]),
@@ -213,6 +214,23 @@ class Plan:
         st = Stats()
         self.engine._check(self.engine.lib.molints_plan_stats(self.h, ctypes.byref(st)))
         return st.as_dict()
+
+    def class_work(self) -> dict:
+        """{tag: (shell quartets, evaluated primitive quartets)} per class pair of the plan,
+        tags as 'ppps' (bra class then ket class, PAIR_CLASSES order)."""
+        n = NUM_PAIR_CLASSES * NUM_PAIR_CLASSES
+        q = np.zeros(n, dtype=np.int64)
+        k = np.zeros(n, dtype=np.float64)
+        self.engine._check(self.engine.lib.molints_plan_class_work(self.h, _ptr(q), _ptr(k), n))
+        L = "spdf"
+        out = {}
+        for x in range(NUM_PAIR_CLASSES):
+            for y in range(x + 1):
+                if q[x * NUM_PAIR_CLASSES + y]:
+                    (a, b), (c, d) = PAIR_CLASSES[x], PAIR_CLASSES[y]
+                    out[L[a] + L[b] + L[c] + L[d]] = (int(q[x * NUM_PAIR_CLASSES + y]),
+                                                      float(k[x * NUM_PAIR_CLASSES + y]))
+        return out
 
     def jk(self, D_ptr: int, J_ptr: int, K_ptr: int) -> None:
         """Queue J and K (n x n device arrays) for the symmetric device density at D_ptr."""

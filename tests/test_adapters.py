@@ -92,17 +92,24 @@ def test_coulomb_pgbf_and_distance_sweep(golden, oracle):
 
 
 @gpu
-def test_h2_basis_known_answers(golden):
+def test_h2_basis_known_answers(golden, oracle):
+    """H2/STO-3G: the reference's values (test/runtests.jl:41-52) to its rtol (about 1.5e-8:
+    they come from pyquante2), and the oracle's Huzinaga all_twoe_ints to 1e-12."""
     _cuda()
     m = M.MolecularIntegrals()
     b = M.Basis([M.Atom(a.atno, tuple(a.xyz)) for a in mi.h2()], "sto3g")
     assert len(b) == 2
     l, r = b
     h = golden["h2_sto3g_coulomb"]
-    assert abs(m.coulomb(l, l, l, l) - h["llll"]["value"]) < 1e-12
-    assert abs(m.coulomb(l, l, r, r) - h["llrr"]["value"]) < 1e-12
-    assert abs(m.coulomb(l, l, l, r) - h["lllr"]["value"]) < 1e-12
-    assert abs(m.coulomb(l, r, l, r) - h["lrlr"]["value"]) < 1e-12
+    with oracle.exact_boys():
+        huz = oracle.eri_packed_huzinaga(b.shells, nthreads=1)
+    for key, (f1, f2, f3, f4), ijkl in (("llll", (l, l, l, l), (0, 0, 0, 0)),
+                                         ("llrr", (l, l, r, r), (0, 0, 1, 1)),
+                                         ("lllr", (l, l, l, r), (0, 0, 0, 1)),
+                                         ("lrlr", (l, r, l, r), (0, 1, 0, 1))):
+        v = m.coulomb(f1, f2, f3, f4)
+        assert abs(v - h[key]["value"]) <= 1.5e-8 * h[key]["value"], key
+        assert abs(v - huz[M.packed_index(*ijkl)]) < 1e-12, key
     # test/runtests.jl:41-46
     assert abs(m.overlap(l, l) - 1.0) < 1e-12
     assert abs(m.overlap(l, r) - 0.6647387449282997) < 1e-12
@@ -111,11 +118,11 @@ def test_h2_basis_known_answers(golden):
     # all_twoe_ints over the basis by every method, and the 4-D form
     for meth in ("default", "hgp", "rys"):
         v = m.all_twoe_ints(b, meth)
-        assert abs(v[0] - h["llll"]["value"]) < 1e-12
+        assert np.max(np.abs(v - huz)) < 1e-12
         A = m.all_twoe_ints_4d(b, meth)
         assert A.shape == (2, 2, 2, 2)
-        assert abs(A[0, 0, 1, 1] - h["llrr"]["value"]) < 1e-12
-        assert abs(A[1, 0, 1, 0] - h["lrlr"]["value"]) < 1e-12
+        assert abs(A[0, 0, 1, 1] - huz[M.packed_index(0, 0, 1, 1)]) < 1e-12
+        assert abs(A[1, 0, 1, 0] - huz[M.packed_index(0, 1, 0, 1)]) < 1e-12
 
 
 @gpu
