@@ -65,9 +65,13 @@ enum molints_output { MOLINTS_OUTPUT_AUTO = 0, MOLINTS_OUTPUT_DIRECT = 1, MOLINT
 /* Plans of at least this many integrals take TWO_PHASE under MOLINTS_OUTPUT_AUTO. */
 #define MOLINTS_TWO_PHASE_MIN ((int64_t)1 << 25)
 
-/* Largest shell angular momentum the engine accepts (f = 3).  Class pairs with an f shell run
- * the Rys kernels (n <= 7 roots). */
-#define MOLINTS_LMAX 3
+/* Largest shell angular momentum the engine accepts (g = 4), as the reference's tables
+ * (shell_indices, src/Basis.jl:269-279).  Class pairs up to (ff|ff) run the generated HGP or Rys
+ * kernels (n <= 7 roots); every shell quartet with a g shell runs one generic Rys kernel (n <= 9
+ * roots, FP64, no screening), written for coverage rather than speed.  Plans with a g shell use
+ * the direct output and support neither sharding, J/K digestion nor molints_plan_schwarz
+ * (MOLINTS_ERR_UNSUPPORTED). */
+#define MOLINTS_LMAX 4
 /* Number of shell-pair classes, ordered by la+lb then la: ss ps pp ds dp fs dd fp df fd ff.
  * A pair is oriented with the larger L first, except that equal-L pairs and f-d pairs put the
  * tighter shell first (hence the class df). */
@@ -280,11 +284,13 @@ int molints_one_e(molints_ctx *ctx, const molints_basis *basis, int32_t natom,
  * blocking call); each request's vector is what molints_eri_packed would write for it.
  *
  * molints_serve_start gives the context a server of nslots slot workers (host threads, each
- * with its own engine context and stream on the context's device).  Requests queue in arrival
- * order; a free slot admits the head request once the server's HBM ledger -- resident result
- * vectors plus the pair tables of running plans -- has room for it under hbm_budget_bytes
- * (0 = no bound), so new requests join the ones already running and their kernels overlap on
- * the device.  A request larger than the whole budget fails with MOLINTS_ERR_BUDGET.
+ * with its own engine context and stream on the context's device).  A free slot admits the
+ * smallest queued request for which the server's HBM ledger -- resident result vectors plus
+ * the pair tables of running plans -- has room under hbm_budget_bytes (0 = no bound); a
+ * request that has waited 40 ms is admitted before any other (nothing else is admitted until it
+ * fits), so none starves.  New requests join the ones already running and their kernels
+ * overlap on the device.  A request larger than the whole budget fails with
+ * MOLINTS_ERR_BUDGET.
  * submit, poll, result, release and request_info may be called from any host thread. */
 typedef struct molints_request molints_request;
 

@@ -43,7 +43,7 @@ def sources():
         sys.path.pop(0)
     gen = gen_eri.generate()
     return ([CSRC / "molints.cu", CSRC / "noalloc.cu", CSRC / "serve.cu", CSRC / "one_e.cu",
-             CSRC / "generated" / "rys_tables.cu"] +
+             CSRC / "eri_generic.cu", CSRC / "generated" / "rys_tables.cu"] +
             sorted(gen))
 
 

@@ -100,7 +100,8 @@ struct EriQueue {
     const long long *region;
 };
 constexpr int kRegionFields = 5;
-constexpr int kScratchTile = 32;  // quartets per tile in the HGP regions (tile 1 for Rys)
+constexpr int kScratchTile = 4;   // quartets per tile in the HGP regions (tile 1 for Rys): a
+                                  // 32-byte sector holds one component of 4 quartets
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {
     const double2 *v = reinterpret_cast<const double2 *>(base + k);

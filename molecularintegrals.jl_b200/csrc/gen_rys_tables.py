@@ -1,9 +1,9 @@
-"""Generate the Rys quadrature tables (roots and weights for n = 1..7) as CUDA C.
+"""Generate the Rys quadrature tables (roots and weights for n = 1..9) as CUDA C.
 
 The Rys quadrature of order n for parameter X has nodes x_i = t_i^2 in (0,1) and weights W_i
 with sum_i W_i x_i^k = F_k(X) (the Boys function) for k = 0..2n-1.  The reference computes
 them for n <= 5 from fitted polynomials (Root1..Root5, src/Rys.jl:176-1478); here they are
-computed from the moments, for n <= 7, by published methods:
+computed from the moments, for n <= 9, by published methods:
 
   * the modified Chebyshev algorithm (Gautschi) turns the moments F_k(X) into the
     three-term recurrence of the orthogonal polynomials (done at 60 significant digits in
@@ -13,7 +13,7 @@ computed from the moments, for n <= 7, by published methods:
   * for 0 <= X < 100 each node and weight is fitted on unit intervals of X by a Chebyshev
     series of degree 15 (interpolation at Chebyshev points); for X >= 100 the measure's
     moments equal the half-range Gaussian's closely enough (checked: relative error of the
-    rule below 1e-16 for n <= 7), so x_i = h_i^2 / X and
+    rule below 1e-16 for n <= 9), so x_i = h_i^2 / X and
     W_i = g_i / sqrt(X) with h_i, g_i the positive nodes and weights of the 2n-point
     Gauss-Hermite rule.
 
@@ -34,7 +34,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "generated" / "rys_tables.cu"
 
-NMAX = 7
+NMAX = 9
 XMAX = 100         # Chebyshev fits cover [0, XMAX); asymptotic Hermite form above
 NCHEB = 16         # points / coefficients per interval (degree 15)
 DPS = 60

@@ -1591,8 +1591,8 @@ __global__ void __launch_bounds__(128) eri_queue_fdps(const EriQueue Q) {
             if constexpr (JK) {
                 jk_fdps(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
             } else if (Q.scratch) {
-                // tiles of kScratchTile quartets, component-major: for each component the
-                // chunk's lanes store consecutive doubles
+                // tiles of kScratchTile quartets, component-major: for each component, groups
+                // of kScratchTile lanes store whole 32-byte sectors
                 const long long u = __ldg(&Q.chunk_slot[c]) + base + kq;
                 double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
                     (u & ~(long long)(kScratchTile - 1)) * 180 + (u & (kScratchTile - 1));

@@ -133,6 +133,11 @@ struct molints_plan {
     int64_t bytes = 0;
     int n_launches = 0;
     int n_fp32_launches = 0;           // class-pair launches of the last execute that ran FP32
+    // shell quartets with a g shell (l = 4): computed by the generic kernel (eri_generic.cu)
+    int64_t n_gq = 0;
+    int4 *gq = nullptr;                // global shells (I, J, K, L), reference order
+    int *gq_mol = nullptr;
+    int *sh_L = nullptr, *sh_K = nullptr, *sh_fn = nullptr;
     double plan_ms[4] = {0, 0, 0, 0};  // plan creation phases (molints_stats.plan_ms)
     // CUDA graph of one execute (molints_plan_set_graph), valid for graph_out
     int use_graph = 0;
@@ -423,6 +428,7 @@ __device__ __forceinline__ long long untri_f(long long t) {
 }
 
 constexpr int kGatherThreads = 256;
+constexpr int kGatherUnroll = 8;
 
 // Per function pair (i >= j) of every molecule of a two-phase plan, what the gather needs to
 // place its entries, built once per plan on the device: x = list position << 4 | pair class of
@@ -484,20 +490,39 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
             }
         }
         __syncthreads();
-        for (long long kl = threadIdx.x; kl <= ij; kl += kGatherThreads) {
-            const int2 qe = __ldg(&col[cbase + kl]);
-            const int posQ = qe.x >> 4, clsQ = qe.x & 15;
-            const int qa = qe.y >> 16, qb = qe.y & 0xffff;
-            const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
-            const long long *rg = reg[braP ? 0 : 1][clsQ];
-            const int y = braP ? clsQ : clsP;
-            const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
-            const int ma = braP ? pa : qa, mb = braP ? pbc : qb, mc = braP ? qa : pa, md = braP ? qb : pbc;
-            const long long db = bpos - rg[1], dk = kpos - rg[2];
-            const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
-            const int nb = c_pair_nb[braP ? clsP : clsQ], nc = c_pair_na[y], nd = c_pair_nb[y];
-            const long long tile = rg[4], u0 = slot & (tile - 1);  // tile: 1 or kScratchTile
-            orow[kl] = __ldg(&scratch[rg[0] + (slot - u0) * rg[5] + (((ma * nb + mb) * nc + mc) * nd + md) * tile + u0]);
+        // kGatherUnroll entries per thread and pass, their loads issued before any is used (the
+        // pass is bound by the latency of the descriptor and scratch loads)
+        for (long long kl0 = threadIdx.x; kl0 <= ij; kl0 += kGatherUnroll * kGatherThreads) {
+            int2 qe[kGatherUnroll];
+#pragma unroll
+            for (int u = 0; u < kGatherUnroll; ++u) {
+                const long long kl = kl0 + u * kGatherThreads;
+                qe[u] = kl <= ij ? __ldg(&col[cbase + kl]) : make_int2(0, 0);
+            }
+            double v[kGatherUnroll];
+#pragma unroll
+            for (int u = 0; u < kGatherUnroll; ++u) {
+                const long long kl = kl0 + u * kGatherThreads;
+                const int posQ = qe[u].x >> 4, clsQ = qe[u].x & 15;
+                const int qa = qe[u].y >> 16, qb = qe[u].y & 0xffff;
+                const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
+                const long long *rg = reg[braP ? 0 : 1][clsQ];
+                const int y = braP ? clsQ : clsP;
+                const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
+                const int ma = braP ? pa : qa, mb = braP ? pbc : qb, mc = braP ? qa : pa, md = braP ? qb : pbc;
+                const long long db = bpos - rg[1], dk = kpos - rg[2];
+                const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
+                const int nb = c_pair_nb[braP ? clsP : clsQ], nc = c_pair_na[y], nd = c_pair_nb[y];
+                const long long tile = rg[4], u0 = slot & (tile - 1);  // tile: 1 or kScratchTile
+                v[u] = kl <= ij ? __ldg(&scratch[rg[0] + (slot - u0) * rg[5] +
+                                                 (((ma * nb + mb) * nc + mc) * nd + md) * tile + u0])
+                                : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kGatherUnroll; ++u) {
+                const long long kl = kl0 + u * kGatherThreads;
+                if (kl <= ij) orow[kl] = v[u];
+            }
         }
     }
 }
@@ -530,6 +555,22 @@ __global__ void boys_eval_kernel(BoysTab bt, int mmax, const double *__restrict_
     for (int m = 0; m < mmax; ++m) out[i * mmax + m] = F[m];
 }
 
+}  // namespace molints
+
+// ------------------------------------------------------------------ g shells (eri_generic.cu)
+namespace molints {
+struct GenQuartets {
+    const int4 *quartet;
+    const int *mol;
+    long long n;
+    const double *xyz;
+    const int *L, *nprim, *poff, *fn_off;
+    const double *expn, *ncoef;
+    const long long *mol_out;
+    double *out;
+    RysTab rys;
+};
+void launch_eri_generic(const GenQuartets &G, int grid, cudaStream_t s);
 }  // namespace molints
 
 // ------------------------------------------------------------------ helpers for noalloc.cu
@@ -830,7 +871,8 @@ static void plan_release_device(molints_plan *p) {
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
-                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows, p->g_col};
+                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows, p->g_col,
+                    p->gq, p->gq_mol, p->sh_L, p->sh_K, p->sh_fn};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
     p->ctx = nullptr;
@@ -1084,15 +1126,38 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     // bra pair's owned ket pairs are one contiguous run)
     struct PairRec { int cls, mol, npp, a, b, ref, ms; };
     std::vector<PairRec> pr;
+    // Shell pairs with a g shell stay out of the class-pair machinery: every shell quartet that
+    // holds one goes to the generic kernel, listed here in reference order (I >= J, K >= L,
+    // pair IJ >= pair KL).
+    std::vector<int4> gq_h;
+    std::vector<int> gq_mol_h;
     for (int m = 0; m < nmol; ++m) {
-        const int n = bases[m].nshell;
+        const int n = bases[m].nshell, s0 = shell_off[m];
+        bool has_g = false;
+        for (int i = 0; i < n; ++i) has_g = has_g || L[s0 + i] > kLmax;
+        if (has_g && nshards > 1) {
+            plan_free(p);
+            return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_create_shard: g shells are not sharded");
+        }
         for (int i = 0; i < n; ++i)
             for (int j = 0; j <= i; ++j) {
-                int a = shell_off[m] + i, bb = shell_off[m] + j;
+                int a = s0 + i, bb = s0 + j;
+                const bool g_ij = L[a] > kLmax || L[bb] > kLmax;
+                if (g_ij || has_g) {
+                    for (int k = 0; k <= i; ++k)
+                        for (int l = 0; l <= (k == i ? j : k); ++l)
+                            if (g_ij || L[s0 + k] > kLmax || L[s0 + l] > kLmax) {
+                                gq_h.push_back(make_int4(a, bb, s0 + k, s0 + l));
+                                gq_mol_h.push_back(m);
+                            }
+                }
+                if (g_ij) continue;
                 if (!a_first(a, bb)) std::swap(a, bb);
                 pr.push_back({pair_class_of(L[a], L[bb]), m, K[a] * K[bb], a, bb, i * (i + 1) / 2 + j, i});
             }
     }
+    p->n_gq = (int64_t)gq_h.size();
+    if (p->n_gq > 0) p->two_phase = 0;  // the gather would overwrite the generic kernel's entries
     const bool sharded = nshards > 1;
     auto order = [sharded](const PairRec &x, const PairRec &y) {
         if (x.cls != y.cls) return x.cls < y.cls;
@@ -1327,7 +1392,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     // {offset in doubles, first bra pair, first ket pair, ket pairs, tile}.  Quartet slot t,
     // component x is at offset + (t - t % tile) * block + x * tile + t % tile: the HGP class
     // kernels, whose lanes hold consecutive quartets, write tiles of kScratchTile quartets
-    // component-major (each component of a chunk is one coalesced run); the Rys kernels, whose
+    // component-major (a chunk's store of one component fills whole 32-byte sectors, four
+    // quartets each, instead of writing 8 bytes of one sector per lane); the Rys kernels, whose
     // thread groups write one quartet's block at a time, keep tile 1 (block after block).
     if (npair >= (1 << 26)) p->two_phase = 0;  // the gather's pair entries hold the position in 26 bits
     auto ncomp_of = [](int x, int y) {
@@ -1626,6 +1692,25 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
     }
+    if (p->n_gq > 0) {
+        // the generic kernel's shell data and quartet list (pageable sources: each copy is
+        // staged before the call returns)
+        rc = dev_alloc(ctx, &p->gq, (size_t)p->n_gq, &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->gq_mol, (size_t)p->n_gq, &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->sh_L, (size_t)ns, &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->sh_K, (size_t)ns, &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->sh_fn, (size_t)ns, &p->bytes);
+        if (rc) { plan_free(p); return rc; }
+        if ((e = cudaMemcpyAsync(p->gq, gq_h.data(), gq_h.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(p->gq_mol, gq_mol_h.data(), gq_mol_h.size() * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(p->sh_L, L.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(p->sh_K, K.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(p->sh_fn, fn_off.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+            (e = cudaStreamSynchronize(s))) {
+            plan_free(p);
+            return cuda_fail(ctx, e, "plan_create upload (g shells)");
+        }
+    }
     if (!sync_end) ctx->stage_busy = true;
     p->plan_ms[3] = ms_since(t_phase);
     ctx->plans.push_back(p);
@@ -1724,10 +1809,19 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         MI_CUDA(ctx, cudaEventRecord(ctx->join[i], ctx->side[i]));
         MI_CUDA(ctx, cudaStreamWaitEvent(s, ctx->join[i], 0));
     }
+    if (p->n_gq > 0) {
+        // shell quartets with a g shell (never two-phase plans; no J/K digestion)
+        GenQuartets G{p->gq, p->gq_mol, p->n_gq, p->sh_xyz, p->sh_L, p->sh_K, p->sh_poff, p->sh_fn,
+                      p->expn, p->ncoef, p->mol_out, out_device, ctx->rys};
+        if (int rc = mark(launches, "eri_generic", 0, s)) return rc;
+        launch_eri_generic(G, (int)std::min<int64_t>(p->n_gq, (int64_t)ctx->num_sms * 8), s);
+        if (int rc = mark(launches, "eri_generic", 1, s)) return rc;
+        ++launches;
+    }
     if (p->two_phase && !jk.J && p->npacked > 0) {
         // second phase: the packed vector in order from the scratch blocks
         if (int rc = mark(launches, "gather_packed", 0, s)) return rc;
-        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, p->n_rows);
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 4, p->n_rows);  // all resident
         gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col,
                                                              p->g_region, p->g_mol, p->g_rows, p->nmol,
                                                              p->n_rows);
@@ -1818,6 +1912,7 @@ int molints_plan_jk(molints_plan *p, const double *D_device, double *J_device, d
     if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     if (p->nmol != 1) return fail(ctx, MOLINTS_ERR_INVALID, "plan_jk: one molecule per plan");
+    if (p->n_gq > 0) return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_jk: g shells are not digested");
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
     const int64_t n = p->nbf0;
     const size_t bytes = (size_t)n * n * sizeof(double);
@@ -1888,6 +1983,7 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
     st->n_prim_pairs_kept = p->nprim_pair_kept;
     for (int k = 0; k < 4; ++k) st->plan_ms[k] = p->plan_ms[k];
     st->n_fp32_launches = p->n_fp32_launches;
+    st->n_shell_quartets += p->n_gq;
     // per (molecule, pair class): the pairs, gathered from the class-major list
     const int nc = kNumPairClasses;
     std::vector<std::vector<int>> by(std::max(p->nmol, 1) * nc);
@@ -1994,6 +2090,7 @@ int molints_plan_schwarz(molints_plan *p, double *out) {
     if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
     MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (p->n_gq > 0) return fail(ctx, MOLINTS_ERR_UNSUPPORTED, "plan_schwarz: g shells have no bounds");
     if (p->npair == 0) return MOLINTS_OK;
     if (!p->qcon) {
         int rc = dev_alloc(ctx, &p->qcon, (size_t)p->npair, &p->bytes);

@@ -1,11 +1,13 @@
 // serve.cu -- the serving form of the ERI engine: molints_submit / poll / result / release.
 //
 // A context's server is a set of slot workers (host threads), each with its own engine
-// context and stream on the same device.  Requests (a basis and options) wait in one FIFO
-// queue.  A free worker admits the request at the head of the queue as soon as the HBM budget
-// ledger can hold it -- its output vector plus its plan's pair tables -- so requests that
-// arrive while others are on the GPU join them: several plans execute at once on the workers'
-// streams and their kernels share the device (continuous batching).  A finished request keeps
+// context and stream on the same device.  Requests (a basis and options) wait in one queue.  A
+// free worker admits the smallest queued request that the HBM budget ledger can hold -- its
+// output vector plus its plan's pair tables -- or, once the oldest request has waited
+// kMaxWait, that one (then nothing else is admitted before it, so no request starves).
+// Requests that arrive while others are on the GPU join them: several plans execute at once on
+// the workers' streams and their kernels share the device (continuous batching).  Taking the
+// smallest first keeps small requests from queueing behind large ones when every slot is busy.  A finished request keeps
 // its packed ERI vector resident on the device until the caller releases it; its plan tables
 // are freed at completion.  The reference has no serving form; this is the batched,
 // asynchronous counterpart of all_twoe_ints (src/ERI.jl:104-112).
@@ -80,7 +82,27 @@ struct Server {
 
     void worker(int slot);
     void destroy_resources();
+    molints_request *pick() const;
 };
+
+// Seconds after which the oldest queued request is admitted before any smaller one.
+constexpr double kMaxWait = 0.040;
+
+// The request a free worker admits now, or nullptr (called with mu held): the oldest once it
+// has waited kMaxWait (if it does not fit, nothing is admitted until releases make room);
+// otherwise the smallest one that fits, the oldest among equals.
+molints_request *Server::pick() const {
+    if (queue.empty()) return nullptr;
+    auto fits = [&](const molints_request *r) {
+        return budget <= 0 || ledger + r->need_out + r->need_plan <= budget;
+    };
+    molints_request *h = queue.front();
+    if (now_s() - h->t_submit > kMaxWait) return fits(h) ? h : nullptr;
+    molints_request *best = nullptr;
+    for (molints_request *r : queue)
+        if (fits(r) && (!best || r->need_out < best->need_out)) best = r;
+    return best;
+}
 
 // Pool and free stream, once no request can reach them any more.
 void Server::destroy_resources() {
@@ -121,15 +143,10 @@ void Server::worker(int slot) {
         molints_request *r = nullptr;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv_work.wait(lk, [&] {
-                if (stop) return true;
-                if (queue.empty()) return false;
-                molints_request *h = queue.front();
-                return budget <= 0 || ledger + h->need_out + h->need_plan <= budget;
-            });
+            // woken by submits and releases; the timeout re-checks the oldest request's age
+            while (!stop && !(r = pick())) cv_work.wait_for(lk, std::chrono::milliseconds(5));
             if (stop) return;
-            r = queue.front();
-            queue.pop_front();
+            queue.erase(std::find(queue.begin(), queue.end(), r));
             ledger += r->need_out + r->need_plan;
             r->state = 1;
             r->slot = slot;

@@ -25,7 +25,7 @@ FP64, MIXED = 0, 1
 BOYS_REFERENCE, BOYS_EXACT = 0, 1
 METHOD_AUTO, METHOD_HGP, METHOD_RYS = 0, 1, 2
 CLASS_NO_FP32 = 4   # flag in a set_class_methods entry: MIXED plans run the FP64 kernel
-LMAX = 3
+LMAX = 4  # g shells: generic Rys kernel (molints.h MOLINTS_LMAX)
 # shell-pair classes in the engine's order (la+lb, then la): index -> (la, lb)
 PAIR_CLASSES = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (3, 0), (2, 2), (3, 1), (2, 3), (3, 2), (3, 3)]
 NUM_PAIR_CLASSES = len(PAIR_CLASSES)

@@ -242,7 +242,7 @@ static int64_t PFX(eri_packed_hgp_impl)(int nshell, const double *xyz, const int
     oracle_init();
     PFX(basis) b = {nshell, xyz, L, nprim, prim_off, expn, coef, 0, 0, 0, 0, 0};
     for (int s = 0; s < nshell; ++s)
-        if (L[s] < 0 || L[s] > 3 || nprim[s] < 1) return -1;
+        if (L[s] < 0 || L[s] > 4 || nprim[s] < 1) return -1;  /* shell_indices reach l = 4 */
     PFX(basis_prepare)(&b);
     int64_t npair = (int64_t)nshell * (nshell + 1) / 2;
     int64_t nquart = npair * (npair + 1) / 2;

@@ -57,15 +57,25 @@ def table_roots(tabs, n, X):
     return u, w
 
 
-@pytest.mark.parametrize("n", range(1, 8))
+@pytest.mark.parametrize("n", range(1, 10))
 def test_root_tables_against_long_double_solver(oracle, rys_tables, n):
-    assert rys_tables["kRysCheb"].size == XMAX * NCHEB * 7 * 8
+    """n <= 7 serve the class kernels up to (ff|ff), n = 8, 9 the g-shell kernel."""
+    assert rys_tables["kRysCheb"].size == XMAX * NCHEB * 9 * 10
     rng = np.random.default_rng(n)
     Xs = np.concatenate([[0.0, 1e-12, 0.5, 0.999999, 1.0, 29.99, 30.0, 99.999, 100.0, 150.0, 1e4],
                          rng.uniform(0, 100, 60), np.exp(rng.uniform(np.log(100), np.log(1e6), 10))])
+    if n >= 8:
+        # the long-double solver truncates its measure at X > 80, which costs 6e-14 in the
+        # smallest weights for n = 9; the tables are pinned to mpmath instead (fewer X: slow)
+        Xs = np.concatenate([Xs[:11], Xs[11:21], Xs[-3:]])
     for X in Xs:
         u, w = table_roots(rys_tables, n, X)
-        ru, rw = oracle.rys_roots(n, X)
+        if n >= 8:
+            mu, mw = oracle.rys_roots_mpmath(n, X)
+            ru = np.array([float(v) for v in mu])
+            rw = np.array([float(v) for v in mw])
+        else:
+            ru, rw = oracle.rys_roots(n, X)
         np.testing.assert_allclose(u, ru, rtol=2e-14, atol=0, err_msg=f"nodes n={n} X={X}")
         np.testing.assert_allclose(w, rw, rtol=2e-14, atol=1e-300, err_msg=f"weights n={n} X={X}")
         # the rule integrates the Boys moments: sum W u^k = F_k(X)
