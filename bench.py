@@ -604,14 +604,18 @@ def measure_config1(eng, dev, stream, fp32_cut, args):
     host = torch.empty(sh.npacked, dtype=torch.float64, pin_memory=True).numpy()
     e = E.Engine(dev.index)
     e.eri_packed(sh, out=host)
-    ts = []
+    ts, phases = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        e.eri_packed(sh, out=host)
+        _, st = e.eri_packed(sh, out=host, with_stats=True)
         ts.append(time.perf_counter() - t0)
+        phases.append(st["plan_ms"] + [st["device_ms"]])
     e.close()
+    ph = np.mean(np.array(phases), axis=0)
     res["e2e_fp64"] = {"value": sh.npacked / np.mean(ts), "ms": 1e3 * float(np.mean(ts)),
-                       "timing": "host wall clock around molints_eri_packed (host output)"}
+                       "timing": "host wall clock around molints_eri_packed (host output)",
+                       "plan_ms": {"tables": ph[0], "bound_pass": ph[1], "queues": ph[2], "upload": ph[3]},
+                       "execute_ms": ph[4]}
     return res
 
 

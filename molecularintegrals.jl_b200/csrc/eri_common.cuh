@@ -92,16 +92,14 @@ struct EriQueue {
     double fp32_cut;              // R_p R_q below this (MIXED kernels): FP32 VRR
     // two-phase output (scratch != nullptr): quartet (p, q0 + t) of chunk c (molecule m = its
     // w field) has slot u = chunk_slot[c] + t of its class pair's region for molecule m,
-    // region[m * kRegionFields ..] = {offset, first bra, first ket, kets, tile}; component x
-    // (ma, mb, mc, md row-major) goes to scratch[offset + (u - u % tile) * block + x * tile +
-    // u % tile].  A gather pass writes the packed vector from the scratch afterwards.
+    // region[m * kRegionFields ..] = {offset, first bra, first ket, kets}: its whole block
+    // (ma, mb, mc, md row-major) goes to scratch[offset + u * block size].  A gather pass
+    // writes the packed vector from the scratch afterwards.
     double *scratch;
     const long long *chunk_slot;
     const long long *region;
 };
-constexpr int kRegionFields = 5;
-constexpr int kScratchTile = 4;   // quartets per tile in the HGP regions (tile 1 for Rys): a
-                                  // 32-byte sector holds one component of 4 quartets
+constexpr int kRegionFields = 4;
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair *__restrict__ base, int k) {
     const double2 *v = reinterpret_cast<const double2 *>(base + k);

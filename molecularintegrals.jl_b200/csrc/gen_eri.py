@@ -47,6 +47,10 @@ HGP_MAX_VRR = 500
 # quartet is dominated by the FP64 prefactors and Boys function, so an FP32 VRR would only
 # add registers and divergence.  MIXED plans run them in FP64.
 MIXED_MIN_VRR = 40
+# Two-phase stores: classes with at most this many outputs per quartet have their HRR write the
+# chunk's blocks into shared memory (4 warps x 32 blocks; 40 doubles keep it under 48 KB) and
+# the warp copies them to the scratch as one contiguous run
+STAGE_MAX_OUT = 40
 
 
 # ------------------------------------------------------------------ AO tables
@@ -352,6 +356,29 @@ void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, do
     schwarz_kernel_{tag}<<<(np + 127) / 128, 128, 0, s>>>(P, B, p0, np, pbound, qout, full);
 }}
 """
+    if nout <= STAGE_MAX_OUT:
+        scratch_store = f"""            // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
+            // into shared memory, where they lie as in the scratch (consecutive slots); the warp
+            // then copies them out as one contiguous run
+            __shared__ double stg[4 * 32 * {nout}];
+            double *sb = stg + (threadIdx.x >> 5) * (32 * {nout});
+            if (lead) hrr_{tag}(Q.pairs, p, q, acc, sb + kq * {nout});
+            __syncwarp();
+            const int nlive = min(W, cnt - base);
+            double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
+                (__ldg(&Q.chunk_slot[c]) + base) * (long long){nout};
+            for (int t = lane; t < nlive * {nout}; t += 32) dst[t] = sb[t];
+            __syncwarp();"""
+    else:
+        scratch_store = f"""            // two-phase: each leader stores its quartet's whole block at its slot
+            if (lead) {{
+                double res[{nout}];
+                hrr_{tag}(Q.pairs, p, q, acc, res);
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
+                    (__ldg(&Q.chunk_slot[c]) + base + kq) * (long long){nout};
+#pragma unroll
+                for (int x = 0; x < {nout}; ++x) dst[x] = res[x];
+            }}"""
     if len(entries) >= MIXED_MIN_VRR:
         mixed_dispatch = ("    const bool jk = Q.jk.J != nullptr;\n"
                           "    if (mixed) {{ if (jk) eri_queue_{t}<1, 1><<<grid, 128, 0, s>>>(Q); "
@@ -512,19 +539,14 @@ __global__ void __launch_bounds__(128) eri_queue_{tag}(const EriQueue Q) {{
                 for (int x = 0; x < {nacc}; ++x) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], off);
             }}
         }}
-        if (live && s == 0) {{
+        const bool lead = live && s == 0;
+        if (!JK && Q.scratch) {{
+{scratch_store}
+        }} else if (lead) {{
             double res[{nout}];
             hrr_{tag}(Q.pairs, p, q, acc, res);
             if constexpr (JK) {{
                 jk_{tag}(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            }} else if (Q.scratch) {{
-                // tiles of kScratchTile quartets, component-major: for each component, groups
-                // of kScratchTile lanes store whole 32-byte sectors
-                const long long u = __ldg(&Q.chunk_slot[c]) + base + kq;
-                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
-                    (u & ~(long long)(kScratchTile - 1)) * {nout} + (u & (kScratchTile - 1));
-#pragma unroll
-                for (int x = 0; x < {nout}; ++x) dst[x * kScratchTile] = res[x];
             }} else {{
                 store_{tag}(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
                             p == q, res);

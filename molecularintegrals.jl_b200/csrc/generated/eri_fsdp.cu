@@ -1531,19 +1531,22 @@ __global__ void __launch_bounds__(128) eri_queue_fsdp(const EriQueue Q) {
                 for (int x = 0; x < 160; ++x) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], off);
             }
         }
-        if (live && s == 0) {
+        const bool lead = live && s == 0;
+        if (!JK && Q.scratch) {
+            // two-phase: each leader stores its quartet's whole block at its slot
+            if (lead) {
+                double res[180];
+                hrr_fsdp(Q.pairs, p, q, acc, res);
+                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
+                    (__ldg(&Q.chunk_slot[c]) + base + kq) * (long long)180;
+#pragma unroll
+                for (int x = 0; x < 180; ++x) dst[x] = res[x];
+            }
+        } else if (lead) {
             double res[180];
             hrr_fsdp(Q.pairs, p, q, acc, res);
             if constexpr (JK) {
                 jk_fsdp(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            } else if (Q.scratch) {
-                // tiles of kScratchTile quartets, component-major: for each component, groups
-                // of kScratchTile lanes store whole 32-byte sectors
-                const long long u = __ldg(&Q.chunk_slot[c]) + base + kq;
-                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
-                    (u & ~(long long)(kScratchTile - 1)) * 180 + (u & (kScratchTile - 1));
-#pragma unroll
-                for (int x = 0; x < 180; ++x) dst[x * kScratchTile] = res[x];
             } else {
                 store_fsdp(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
                             p == q, res);

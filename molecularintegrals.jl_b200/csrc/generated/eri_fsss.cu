@@ -224,19 +224,25 @@ __global__ void __launch_bounds__(128) eri_queue_fsss(const EriQueue Q) {
                 for (int x = 0; x < 10; ++x) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], off);
             }
         }
-        if (live && s == 0) {
+        const bool lead = live && s == 0;
+        if (!JK && Q.scratch) {
+            // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
+            // into shared memory, where they lie as in the scratch (consecutive slots); the warp
+            // then copies them out as one contiguous run
+            __shared__ double stg[4 * 32 * 10];
+            double *sb = stg + (threadIdx.x >> 5) * (32 * 10);
+            if (lead) hrr_fsss(Q.pairs, p, q, acc, sb + kq * 10);
+            __syncwarp();
+            const int nlive = min(W, cnt - base);
+            double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
+                (__ldg(&Q.chunk_slot[c]) + base) * (long long)10;
+            for (int t = lane; t < nlive * 10; t += 32) dst[t] = sb[t];
+            __syncwarp();
+        } else if (lead) {
             double res[10];
             hrr_fsss(Q.pairs, p, q, acc, res);
             if constexpr (JK) {
                 jk_fsss(Q.jk, __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]), p == q, res);
-            } else if (Q.scratch) {
-                // tiles of kScratchTile quartets, component-major: for each component, groups
-                // of kScratchTile lanes store whole 32-byte sectors
-                const long long u = __ldg(&Q.chunk_slot[c]) + base + kq;
-                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
-                    (u & ~(long long)(kScratchTile - 1)) * 10 + (u & (kScratchTile - 1));
-#pragma unroll
-                for (int x = 0; x < 10; ++x) dst[x * kScratchTile] = res[x];
             } else {
                 store_fsss(Q.out + __ldg(&Q.mol_out[ch.w]), __ldg(&Q.pairs.info[p]), __ldg(&Q.pairs.info[q]),
                             p == q, res);

@@ -124,10 +124,12 @@ struct molints_plan {
     long long *chunk_slot = nullptr;   // per chunk: scratch offset of its first quartet's block
     int2 *g_fn = nullptr;              // per function (all molecules): {shell in molecule, component}
     int *g_pair = nullptr;             // per molecule shell pair I >= J: pos << 5 | class << 1 | A == J
-    long long *g_region = nullptr;     // per (x, y, molecule): {scratch offset, first bra, first ket, kets, tile}
+    long long *g_region = nullptr;     // per (x, y, molecule): {scratch offset, first bra, first ket, kets}
     long long *g_mol = nullptr;        // per molecule: {first function, first pair entry, packed offset,
                                        // first function-pair entry of g_col}
     int2 *g_col = nullptr;             // per function pair of every molecule: gather_cols_kernel
+    int4 *g_units = nullptr;           // gather units: shell pairs, heaviest first (gather_packed_kernel)
+    int64_t n_units = 0;
     int2 *g_rows = nullptr;            // gather order: {molecule, row ij}, the rows of one shell pair together
     int64_t n_rows = 0;
     int64_t bytes = 0;
@@ -451,78 +453,92 @@ __global__ void gather_cols_kernel(int2 *__restrict__ col, const int2 *__restric
     col[__ldg(&mol[4 * m + 3]) + ij] = make_int2(((P >> 5) << 4) | ((P >> 1) & 15), (ca << 16) | cb);
 }
 
-// Second phase of the two-phase output: the packed vector written row by row from the scratch
-// blocks.  A block of threads writes one row ij (function pair i >= j) whole, columns kl =
-// 0..ij in order, so the stores are coalesced and so are the reads of the column descriptors;
-// rows[] lists the rows shell pair by shell pair, so the rows of one pair P, which read the same
-// scratch blocks (P's bra row of each class region, or P's column of the regions where P is the
-// ket), run at the same time and find them in L2.  The row's pair P fixes one class of each
-// region an entry can come from: the block stages those regions (P as bra, P as ket; one per
-// class of the other pair) in shared memory.  Each entry comes from the block and component the
-// direct path would have stored it from: the quartet's bra is the pair of the higher class, or
-// of the later list position within a class (P for the diagonal quartet P == Q); a pair's
-// components are taken in its A, B orientation, with the larger component first within a
-// same-shell pair, as the direct store conditions pick.
+// Second phase of the two-phase output: the packed vector written from the scratch blocks, one
+// shell pair P at a time.  A block of threads takes the next pair from units[] (heaviest first,
+// through an atomic counter) and writes all of P's rows (function pairs ij of P) column by
+// column: each thread takes a column kl, reads its descriptor once, and stores that column of
+// every row of P with kl <= ij.  The stores of one row are coalesced; the scratch entries of a
+// quartet (P, Q) for all of P's rows lie in one block, read by the same threads in the
+// same pass, so each scratch sector is fetched once.  Each entry comes from the block and
+// component the direct path would have stored it from: the quartet's bra is the pair of the
+// higher class, or of the later list position within a class (P for the diagonal quartet
+// P == Q); a pair's components are taken in its A, B orientation, with the larger component
+// first within a same-shell pair, as the direct store conditions pick.
+constexpr int kGatherMaxRows = 100;  // components of an (ff) pair
 __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
     double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ col,
     const long long *__restrict__ region, const long long *__restrict__ mol,
-    const int2 *__restrict__ rows, int nmol, long long nrows) {
+    const int4 *__restrict__ units, long long nunits, int *__restrict__ counter, int nmol) {
     // [P as bra, P as ket][class of the other pair]: {scratch offset, first bra, first ket,
-    // kets, tile, block size}
-    __shared__ long long reg[2][kNumPairClasses][6];
-    for (long long r = blockIdx.x; r < nrows; r += gridDim.x) {
-        const int2 mr = __ldg(&rows[r]);
-        const int m = mr.x;
-        const long long ij = mr.y;
+    // kets, block size}
+    __shared__ long long reg[2][kNumPairClasses][5];
+    __shared__ long long s_ij[kGatherMaxRows];
+    __shared__ int s_rc[kGatherMaxRows];
+    __shared__ long long s_unit;
+    for (;;) {
+        __syncthreads();  // the previous unit's readers are done with the shared tables
+        if (threadIdx.x == 0) s_unit = atomicAdd(counter, 1);
+        __syncthreads();
+        const long long u = s_unit;
+        if (u >= nunits) return;
+        const int4 un = __ldg(&units[u]);
+        const int m = un.x, fi0 = un.y, fj0 = un.z;
+        const int nI = un.w & 255, nJ = (un.w >> 8) & 255, same = (un.w >> 16) & 1;
         const long long cbase = __ldg(&mol[4 * m + 3]);
-        double *__restrict__ orow = out + __ldg(&mol[4 * m + 2]) + ij * (ij + 1) / 2;
-        const int2 pe = __ldg(&col[cbase + ij]);
+        double *__restrict__ obase = out + __ldg(&mol[4 * m + 2]);
+        // P's rows: ij, and the row's component index in P's A, B orientation
+        const int2 pe = __ldg(&col[cbase + (long long)fi0 * (fi0 + 1) / 2 + fj0]);
         const int posP = pe.x >> 4, clsP = pe.x & 15;
-        const int pa = pe.y >> 16, pbc = pe.y & 0xffff;
-        __syncthreads();  // the previous row's readers are done with reg
+        const int nbP = c_pair_nb[clsP];
+        int R = 0;
+        for (int a = 0; a < nI; ++a) R += same ? a + 1 : nJ;
+        for (int r = threadIdx.x; r < R; r += kGatherThreads) {
+            int a = 0, b = r;
+            if (same) { while (b > a) { b -= a + 1; ++a; } }
+            else { a = r / nJ; b = r - a * nJ; }
+            const long long i = fi0 + a, j = fj0 + b, ij = i * (i + 1) / 2 + j;
+            const int2 re = __ldg(&col[cbase + ij]);
+            s_ij[r] = ij;
+            s_rc[r] = (re.y >> 16) * nbP + (re.y & 0xffff);
+        }
         if (threadIdx.x < 2 * kNumPairClasses) {
             const int o = threadIdx.x / kNumPairClasses, t = threadIdx.x % kNumPairClasses;
             const int x = o == 0 ? clsP : t, y = o == 0 ? t : clsP;
             if (x >= y) {
                 const long long *rg = region + kRegionFields * (((long long)x * kNumPairClasses + y) * nmol + m);
                 for (int f = 0; f < kRegionFields; ++f) reg[o][t][f] = __ldg(&rg[f]);
-                reg[o][t][5] = (long long)c_pair_na[x] * c_pair_nb[x] * c_pair_na[y] * c_pair_nb[y];
+                reg[o][t][4] = (long long)c_pair_na[x] * c_pair_nb[x] * c_pair_na[y] * c_pair_nb[y];
             }
         }
         __syncthreads();
-        // kGatherUnroll entries per thread and pass, their loads issued before any is used (the
-        // pass is bound by the latency of the descriptor and scratch loads)
-        for (long long kl0 = threadIdx.x; kl0 <= ij; kl0 += kGatherUnroll * kGatherThreads) {
-            int2 qe[kGatherUnroll];
+        const long long ijmax = s_ij[R - 1];  // rows are in increasing ij
+        for (long long kl = threadIdx.x; kl <= ijmax; kl += kGatherThreads) {
+            const int2 qe = __ldg(&col[cbase + kl]);
+            const int posQ = qe.x >> 4, clsQ = qe.x & 15;
+            const int qa = qe.y >> 16, qb = qe.y & 0xffff;
+            const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
+            const long long *rg = reg[braP ? 0 : 1][clsQ];
+            const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
+            const long long db = bpos - rg[1], dk = kpos - rg[2];
+            const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
+            // component x = row part * rstride + column part
+            const int nq = c_pair_na[clsQ] * c_pair_nb[clsQ], qc = qa * c_pair_nb[clsQ] + qb;
+            const int nP = c_pair_na[clsP] * nbP;
+            const long long rstride = braP ? nq : 1, cpart = braP ? qc : (long long)qc * nP;
+            const double *__restrict__ src = scratch + rg[0] + slot * rg[4] + cpart;
+            const long long rs = rstride;
+            // rows with ij >= kl: a suffix of the increasing row list
+            int r0 = 0;
+            while (r0 < R && s_ij[r0] < kl) ++r0;
+            int r = r0;
+            for (; r + 4 <= R; r += 4) {
+                double v[4];
 #pragma unroll
-            for (int u = 0; u < kGatherUnroll; ++u) {
-                const long long kl = kl0 + u * kGatherThreads;
-                qe[u] = kl <= ij ? __ldg(&col[cbase + kl]) : make_int2(0, 0);
-            }
-            double v[kGatherUnroll];
+                for (int t = 0; t < 4; ++t) v[t] = __ldg(src + s_rc[r + t] * rs);
 #pragma unroll
-            for (int u = 0; u < kGatherUnroll; ++u) {
-                const long long kl = kl0 + u * kGatherThreads;
-                const int posQ = qe[u].x >> 4, clsQ = qe[u].x & 15;
-                const int qa = qe[u].y >> 16, qb = qe[u].y & 0xffff;
-                const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
-                const long long *rg = reg[braP ? 0 : 1][clsQ];
-                const int y = braP ? clsQ : clsP;
-                const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
-                const int ma = braP ? pa : qa, mb = braP ? pbc : qb, mc = braP ? qa : pa, md = braP ? qb : pbc;
-                const long long db = bpos - rg[1], dk = kpos - rg[2];
-                const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
-                const int nb = c_pair_nb[braP ? clsP : clsQ], nc = c_pair_na[y], nd = c_pair_nb[y];
-                const long long tile = rg[4], u0 = slot & (tile - 1);  // tile: 1 or kScratchTile
-                v[u] = kl <= ij ? __ldg(&scratch[rg[0] + (slot - u0) * rg[5] +
-                                                 (((ma * nb + mb) * nc + mc) * nd + md) * tile + u0])
-                                : 0.0;
+                for (int t = 0; t < 4; ++t) obase[s_ij[r + t] * (s_ij[r + t] + 1) / 2 + kl] = v[t];
             }
-#pragma unroll
-            for (int u = 0; u < kGatherUnroll; ++u) {
-                const long long kl = kl0 + u * kGatherThreads;
-                if (kl <= ij) orow[kl] = v[u];
-            }
+            for (; r < R; ++r) obase[s_ij[r] * (s_ij[r] + 1) / 2 + kl] = __ldg(src + s_rc[r] * rs);
         }
     }
 }
@@ -871,7 +887,7 @@ static void plan_release_device(molints_plan *p) {
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
-                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows, p->g_col,
+                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows, p->g_col, p->g_units,
                     p->gq, p->gq_mol, p->sh_L, p->sh_K, p->sh_fn};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
@@ -1223,7 +1239,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     rc = rc ? rc : dev_alloc(ctx, &p->bnd, (size_t)npair, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->pp_src, (size_t)nall, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)nall, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->counters, (size_t)nc2, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->counters, (size_t)nc2 + 1, &p->bytes);  // + the gather's
     rc = rc ? rc : dev_alloc(ctx, &p->mol_out, (size_t)std::max(nmol, 1), &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &pbound, (size_t)nall, &scratch);
     if (rc) {
@@ -1388,13 +1404,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     for (int x = 0; x < kNumPairClasses; ++x)
         for (int y = 0; y <= x; ++y) cps.push_back({x, y});
     // two-phase scratch: per (class pair, molecule) a region of quartet blocks in slot order,
-    // bra-major (the triangle q <= p for equal classes); region_h[((x nc + y) nmol + m) 5 ..] =
-    // {offset in doubles, first bra pair, first ket pair, ket pairs, tile}.  Quartet slot t,
-    // component x is at offset + (t - t % tile) * block + x * tile + t % tile: the HGP class
-    // kernels, whose lanes hold consecutive quartets, write tiles of kScratchTile quartets
-    // component-major (a chunk's store of one component fills whole 32-byte sectors, four
-    // quartets each, instead of writing 8 bytes of one sector per lane); the Rys kernels, whose
-    // thread groups write one quartet's block at a time, keep tile 1 (block after block).
+    // bra-major (the triangle q <= p for equal classes); region_h[((x nc + y) nmol + m) 4 ..] =
+    // {offset in doubles, first bra pair, first ket pair, ket pairs}.  Quartet slot t's block
+    // starts at offset + t * block.
     if (npair >= (1 << 26)) p->two_phase = 0;  // the gather's pair entries hold the position in 26 bits
     auto ncomp_of = [](int x, int y) {
         return (int64_t)ncart(kPairClassLa[x]) * ncart(kPairClassLb[x]) * ncart(kPairClassLa[y]) * ncart(kPairClassLb[y]);
@@ -1411,14 +1423,11 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 range_of(y, m, k0, k1);
                 const int64_t nb = b1 - b0, nk = k1 - k0;
                 long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * kRegionFields];
-                const int64_t tile = p->method[x][y] == MOLINTS_METHOD_RYS ? 1 : kScratchTile;
-                const int64_t nslot = x == y ? nb * (nb + 1) / 2 : nb * nk;
                 rg[0] = scratch_len;
                 rg[1] = b0;
                 rg[2] = k0;
                 rg[3] = nk;
-                rg[4] = tile;
-                scratch_len += (nslot + tile - 1) / tile * tile * ncomp_of(x, y);
+                scratch_len += (x == y ? nb * (nb + 1) / 2 : nb * nk) * ncomp_of(x, y);
             }
         // The scratch (about npacked doubles) is taken now.  If it does not fit the budget or
         // the device, AUTO falls back to the direct stores, which need no scratch; only an
@@ -1579,7 +1588,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     int64_t nrows_all = 0;
     for (int m = 0; m < nmol; ++m) nrows_all += mol_nbf[m] * (mol_nbf[m] + 1) / 2;
     const size_t o_grows = o_gmol + (tp ? al16((size_t)nmol * 4 * sizeof(long long)) : 0);
-    const size_t stage_bytes = o_grows + (tp ? al16((size_t)nrows_all * sizeof(int2)) : 0);
+    const size_t o_gunits = o_grows + (tp ? al16((size_t)nrows_all * sizeof(int2)) : 0);
+    const size_t stage_bytes = o_gunits + (tp ? al16((size_t)npe_all * sizeof(int4)) : 0);
     if ((rc = ctx_stage(ctx, stage_bytes))) { plan_free(p); return rc; }
     char *stage = ctx->stage;
     int4 *chunks = reinterpret_cast<int4 *>(stage);
@@ -1632,6 +1642,28 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                         }
                 }
         p->n_rows = nr;
+        // gather units: every shell pair I >= J of every molecule, heaviest first (rows x the
+        // last row's columns), so that the big pairs do not finish last
+        int4 *gu = reinterpret_cast<int4 *>(stage + o_gunits);
+        std::vector<std::pair<double, int64_t>> wk;
+        wk.reserve((size_t)npe_all);
+        std::vector<int4> u_h;
+        u_h.reserve((size_t)npe_all);
+        for (int m = 0; m < nmol; ++m)
+            for (int I = 0; I < bases[m].nshell; ++I)
+                for (int J = 0; J <= I; ++J) {
+                    const int gI = shell_off[m] + I, gJ = shell_off[m] + J;
+                    const int nI = ncart(L[gI]), nJ = ncart(L[gJ]);
+                    const int64_t li = fn_off[gI] + nI - 1, lj = I == J ? li : fn_off[gJ] + nJ - 1;
+                    const double rows = I == J ? nI * (nI + 1) / 2.0 : (double)nI * nJ;
+                    wk.push_back({rows * (double)(li * (li + 1) / 2 + lj + 1), (int64_t)u_h.size()});
+                    u_h.push_back(make_int4(m, fn_off[gI], fn_off[gJ], nI | (nJ << 8) | ((I == J) << 16)));
+                }
+        std::sort(wk.begin(), wk.end(), [](const std::pair<double, int64_t> &a, const std::pair<double, int64_t> &b) {
+            return a.first > b.first || (a.first == b.first && a.second < b.second);
+        });
+        for (size_t k = 0; k < wk.size(); ++k) gu[k] = u_h[wk[k].second];
+        p->n_units = (int64_t)wk.size();
     }
     std::memcpy(stage + o_info, info_h.data(), npair * sizeof(int4));
     std::memcpy(stage + o_bnd, p->bnd_h.data(), npair * sizeof(double2));
@@ -1655,6 +1687,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         if (!rc) rc = dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_rows, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->g_col, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
+        if (!rc) rc = dev_alloc(ctx, &p->g_units, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
     }
     if (rc) { plan_free(p); return rc; }
     if (tp && ((nq > 0 && (e = cudaMemcpyAsync(p->chunk_slot, stage + o_slot, (size_t)nq * sizeof(long long),
@@ -1667,6 +1700,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                                     cudaMemcpyHostToDevice, s)) ||
                (e = cudaMemcpyAsync(p->g_mol, stage + o_gmol, (size_t)nmol * 4 * sizeof(long long),
                                     cudaMemcpyHostToDevice, s)) ||
+               (npe_all > 0 && (e = cudaMemcpyAsync(p->g_units, stage + o_gunits, (size_t)npe_all * sizeof(int4),
+                                                     cudaMemcpyHostToDevice, s))) ||
                (nrows_all > 0 && (e = cudaMemcpyAsync(p->g_rows, stage + o_grows, (size_t)nrows_all * sizeof(int2),
                                                        cudaMemcpyHostToDevice, s))))) {
         plan_free(p);
@@ -1747,7 +1782,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         return err == cudaSuccess ? 0 : cuda_fail(ctx, err, "cudaEventRecord");
     };
     if (timing) MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
-    MI_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(int) * kNumPairClasses * kNumPairClasses, s));
+    MI_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(int) * (kNumPairClasses * kNumPairClasses + 1), s));
     if (p->npair > 0) {
         if (int rc = mark(launches, "build_pairs", 0, s)) return rc;
         build_pairs_kernel<<<build_pairs_blocks(p->npair), 128, 0, s>>>(
@@ -1821,10 +1856,11 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     if (p->two_phase && !jk.J && p->npacked > 0) {
         // second phase: the packed vector in order from the scratch blocks
         if (int rc = mark(launches, "gather_packed", 0, s)) return rc;
-        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 4, p->n_rows);  // all resident
-        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col,
-                                                             p->g_region, p->g_mol, p->g_rows, p->nmol,
-                                                             p->n_rows);
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, p->n_units);  // all resident
+        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col, p->g_region,
+                                                             p->g_mol, p->g_units, p->n_units,
+                                                             p->counters + kNumPairClasses * kNumPairClasses,
+                                                             p->nmol);
         if (int rc = mark(launches, "gather_packed", 1, s)) return rc;
         ++launches;
     }

@@ -407,7 +407,6 @@ __device__ __forceinline__ void rys_queue_body(const EriQueue &Q, const RysTab &
             group_sync<C::G>(gid);
             const bool dab = ib.z == ib.w, dcd = ik.z == ik.w, same = p == q;
             // two-phase output: the quartet's whole block, (bra component, ket component) row-major
-            // (tile 1: the region's blocks one after another)
             double *__restrict__ blk = (Q.scratch && !Q.jk.J)
                 ? Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
                       (__ldg(&Q.chunk_slot[c]) + (q - ch.y)) * (long long)(C::NAB * C::NCD)
