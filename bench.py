@@ -248,22 +248,16 @@ def flush_l2(buf):
     buf.add_(1.0)
 
 
-def timed_steps(plans, outs, stream, k, lanes=None):
-    """k steps, CUDA events around each step on `stream`; total ms.  Plan i executes into
-    outs[i % len(outs)]; with `lanes` (one stream per context, plan i on lanes[i % len]) the
-    lanes are forked from `stream` at the start of a step and joined back at its end, so one
-    plan's gather pass (HBM-bound) runs beside the next plan's class kernels."""
+def timed_steps(plans, out, stream, k):
+    """k steps (every plan executed into `out`), CUDA events around each step on the launching
+    stream; total ms."""
     import torch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(k)]
     for a, b in ev:
         a.record(stream)
-        for ln in lanes or ():
-            ln.wait_event(a)
-        for i, p in enumerate(plans):
-            p.execute(outs[i % len(outs)].data_ptr())
-        for ln in lanes or ():
-            stream.wait_stream(ln)
+        for p in plans:
+            p.execute(out.data_ptr())
         b.record(stream)
     torch.cuda.synchronize(stream.device)
     return sum(a.elapsed_time(b) for a, b in ev)
@@ -309,35 +303,24 @@ def run_ours(args):
     mine = order[rank::world]
     groups = make_groups(mols, mine)
     n_eri = sum(mols[i].npacked for i in mine)
-    # two contexts, each on its own stream, take the groups in turn: a context's two-phase
-    # scratch serves one execute at a time, and with two in flight one group's gather pass
-    # overlaps the next group's class kernels
-    engs = [eng, E.Engine(local)]
-    engs[1].set_class_methods(class_table)
-    lanes = [torch.cuda.Stream(dev) for _ in engs]
-    for e, ln in zip(engs, lanes):
-        e.set_stream(ln.cuda_stream)
     t0 = time.perf_counter()
-    plans64 = [engs[k % 2].plan_batch([mols[i] for i in g], boys=E.BOYS_EXACT) for k, g in enumerate(groups)]
+    plans64 = [eng.plan_batch([mols[i] for i in g], boys=E.BOYS_EXACT) for g in groups]
     t_plan64 = time.perf_counter() - t0
     t0 = time.perf_counter()
-    plansmx = [engs[k % 2].plan_batch([mols[i] for i in g], boys=E.BOYS_EXACT, precision=E.MIXED,
-                                      fp32_cutoff=fp32_cut, screen_cutoff=SCREEN_CUTOFF)
-               for k, g in enumerate(groups)]
+    plansmx = [eng.plan_batch([mols[i] for i in g], boys=E.BOYS_EXACT, precision=E.MIXED,
+                              fp32_cutoff=fp32_cut, screen_cutoff=SCREEN_CUTOFF) for g in groups]
     t_planmx = time.perf_counter() - t0
     for p in plans64 + plansmx:
         p.set_graph(True)
-    torch.cuda.synchronize(dev)
-    outs = [torch.empty(max(p.npacked for p in plans64), dtype=torch.float64, device=dev) for _ in engs]
-    out = outs[0]
+    out = torch.empty(max(p.npacked for p in plans64), dtype=torch.float64, device=dev)
     for plans in (plans64, plansmx):
-        timed_steps(plans, outs, stream, max(args.warmup, 3), lanes)
+        timed_steps(plans, out, stream, max(args.warmup, 3))
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
-        ms64 = timed_steps(plans64, outs, stream, args.steps, lanes)
-        msmx = timed_steps(plansmx, outs, stream, args.steps, lanes)
+        ms64 = timed_steps(plans64, out, stream, args.steps)
+        msmx = timed_steps(plansmx, out, stream, args.steps)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -359,15 +342,12 @@ def run_ours(args):
                    ("n_shell_quartets", "n_fp32_quartets", "n_screened", "n_fp32_launches")}
 
     roofline = measure_roofline(plans64, groups, mols, out, stream, dev)
-    for p in plans64 + plansmx:
-        p.close()
-    engs[1].close()
-    eng.set_stream(stream.cuda_stream)
-    del out, outs
-    torch.cuda.synchronize(dev)
-    torch.cuda.empty_cache()
     e2e = measure_e2e(eng, dev, stream, mols, groups, fp32_cut, min(args.steps, args.e2e_steps))
     plain = measure_plain_fp64(eng, dev, mols, mine) if "plain" in parts else None
+    for p in plans64 + plansmx:
+        p.close()
+    del out
+    torch.cuda.empty_cache()
 
     errors = measure_errors(eng, fp32_cut) if "errors" in parts and rank == 0 else None
     cfg1 = measure_config1(eng, dev, stream, fp32_cut, args) if "config1" in parts else None
@@ -392,8 +372,7 @@ def run_ours(args):
         cfg.update({"n_eri_per_step": int(n_all), "groups": len(groups), "fp32_cutoff": fp32_cut,
                     "boys": "exact", "mixed_quartets": mixed_stats,
                     "plan_create_s": {"fp64": t_plan64, "mixed": t_planmx},
-                    "cuda_graph": "one graph per batch plan",
-                    "contexts": "2 (groups taken in turn, each context on its own stream)"})
+                    "cuda_graph": "one graph per batch plan"})
         line = {
             "metric": METRIC, "value": valuemx, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": msmx / args.steps,
