@@ -48,9 +48,9 @@ HGP_MAX_VRR = 500
 # add registers and divergence.  MIXED plans run them in FP64.
 MIXED_MIN_VRR = 40
 # Two-phase stores: classes with at most this many outputs per quartet have their HRR write the
-# chunk's blocks into shared memory (4 warps x 32 blocks; 40 doubles keep it under 48 KB) and
+# chunk's blocks into dynamic shared memory (4 warps x 32 blocks x 8 B each: up to 162 KB) and
 # the warp copies them to the scratch as one contiguous run
-STAGE_MAX_OUT = 40
+STAGE_MAX_OUT = 162
 
 
 # ------------------------------------------------------------------ AO tables
@@ -357,10 +357,35 @@ void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, do
 }}
 """
     if nout <= STAGE_MAX_OUT:
+        sbytes = 4 * 32 * nout * 8
+        mixed_attr = (f"        cudaFuncSetAttribute(eri_queue_{tag}<1, 0>, "
+                      f"cudaFuncAttributeMaxDynamicSharedMemorySize, {sbytes});\n"
+                      if len(entries) >= MIXED_MIN_VRR else "")
+        stage_fn = (f"""
+// The dynamic shared memory of the two-phase staging ({sbytes} bytes), allowed once per device
+// (before any graph capture: the occupancy query of plan creation calls it first).
+static void eri_prepare_{tag}() {{
+    static bool done[64] = {{false}};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {{
+        cudaFuncSetAttribute(eri_queue_{tag}<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, {sbytes});
+{mixed_attr}        done[dev] = true;
+    }}
+}}
+""" if sbytes > 48 * 1024 else "")
+        stage_prep = (f"    // two-phase plans stage the chunk's blocks in {sbytes} bytes of dynamic shared memory\n"
+                      f"    const size_t smem = Q.scratch && !Q.jk.J ? {sbytes} : 0;" +
+                      (f"\n    if (smem) eri_prepare_{tag}();" if sbytes > 48 * 1024 else ""))
+        occ_prep = f"    eri_prepare_{tag}();" if sbytes > 48 * 1024 else ""
+    else:
+        stage_fn, occ_prep = "", ""
+        stage_prep = "    constexpr size_t smem = 0;"
+    if nout <= STAGE_MAX_OUT:
         scratch_store = f"""            // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
             // into shared memory, where they lie as in the scratch (consecutive slots); the warp
             // then copies them out as one contiguous run
-            __shared__ double stg[4 * 32 * {nout}];
+            extern __shared__ double stg[];  // 4 * 32 * {nout} doubles (launch_eri_{tag})
             double *sb = stg + (threadIdx.x >> 5) * (32 * {nout});
             if (lead) hrr_{tag}(Q.pairs, p, q, acc, sb + kq * {nout});
             __syncwarp();
@@ -382,15 +407,15 @@ void launch_schwarz_{tag}(const PairTab &P, const BoysTab &B, int p0, int np, do
     if len(entries) >= MIXED_MIN_VRR:
         mixed_dispatch = ("    const bool jk = Q.jk.J != nullptr;\n"
                           "    if (mixed) {{ if (jk) eri_queue_{t}<1, 1><<<grid, 128, 0, s>>>(Q); "
-                          "else eri_queue_{t}<1, 0><<<grid, 128, 0, s>>>(Q); }}\n"
+                          "else eri_queue_{t}<1, 0><<<grid, 128, smem, s>>>(Q); }}\n"
                           "    else if (jk) eri_queue_{t}<0, 1><<<grid, 128, 0, s>>>(Q);\n"
-                          "    else eri_queue_{t}<0, 0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
+                          "    else eri_queue_{t}<0, 0><<<grid, 128, smem, s>>>(Q);").format(t=tag)
         occ_dispatch = ("    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<1, 0>, 128, 0);\n"
                         "    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0, 0>, 128, 0);").format(t=tag)
     else:
         mixed_dispatch = ("    (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)\n"
                           "    if (Q.jk.J) eri_queue_{t}<0, 1><<<grid, 128, 0, s>>>(Q);\n"
-                          "    else eri_queue_{t}<0, 0><<<grid, 128, 0, s>>>(Q);").format(t=tag)
+                          "    else eri_queue_{t}<0, 0><<<grid, 128, smem, s>>>(Q);").format(t=tag)
         occ_dispatch = ("    (void)mixed;\n"
                         "    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_{t}<0, 0>, 128, 0);").format(t=tag)
     return f"""// Generated by gen_eri.py -- class ({'spdfg'[la]}{'spdfg'[lb]}|{'spdfg'[lc]}{'spdfg'[ld]}).  Do not edit.
@@ -556,13 +581,16 @@ __global__ void __launch_bounds__(128) eri_queue_{tag}(const EriQueue Q) {{
     }}
 }}
 
+{stage_fn}
 void launch_eri_{tag}(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {{
     if (Q.nchunks <= 0 || grid <= 0) return;
+{stage_prep}
 {mixed_dispatch}
 }}
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_{tag}(int mixed) {{
+{occ_prep}
     int n = 0;
 {occ_dispatch}
     return n;

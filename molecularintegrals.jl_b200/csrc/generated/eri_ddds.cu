@@ -2033,16 +2033,19 @@ __global__ void __launch_bounds__(128) eri_queue_ddds(const EriQueue Q) {
     }
 }
 
+
 void launch_eri_ddds(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
+    constexpr size_t smem = 0;
     const bool jk = Q.jk.J != nullptr;
-    if (mixed) { if (jk) eri_queue_ddds<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_ddds<1, 0><<<grid, 128, 0, s>>>(Q); }
+    if (mixed) { if (jk) eri_queue_ddds<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_ddds<1, 0><<<grid, 128, smem, s>>>(Q); }
     else if (jk) eri_queue_ddds<0, 1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_ddds<0, 0><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_ddds<0, 0><<<grid, 128, smem, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_ddds(int mixed) {
+
     int n = 0;
     if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ddds<1, 0>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ddds<0, 0>, 128, 0);

@@ -527,15 +527,18 @@ __global__ void __launch_bounds__(128) eri_queue_dpps(const EriQueue Q) {
         }
         const bool lead = live && s == 0;
         if (!JK && Q.scratch) {
-            // two-phase: each leader stores its quartet's whole block at its slot
-            if (lead) {
-                double res[54];
-                hrr_dpps(Q.pairs, p, q, acc, res);
-                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
-                    (__ldg(&Q.chunk_slot[c]) + base + kq) * (long long)54;
-#pragma unroll
-                for (int x = 0; x < 54; ++x) dst[x] = res[x];
-            }
+            // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
+            // into shared memory, where they lie as in the scratch (consecutive slots); the warp
+            // then copies them out as one contiguous run
+            extern __shared__ double stg[];  // 4 * 32 * 54 doubles (launch_eri_dpps)
+            double *sb = stg + (threadIdx.x >> 5) * (32 * 54);
+            if (lead) hrr_dpps(Q.pairs, p, q, acc, sb + kq * 54);
+            __syncwarp();
+            const int nlive = min(W, cnt - base);
+            double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
+                (__ldg(&Q.chunk_slot[c]) + base) * (long long)54;
+            for (int t = lane; t < nlive * 54; t += 32) dst[t] = sb[t];
+            __syncwarp();
         } else if (lead) {
             double res[54];
             hrr_dpps(Q.pairs, p, q, acc, res);
@@ -550,16 +553,34 @@ __global__ void __launch_bounds__(128) eri_queue_dpps(const EriQueue Q) {
     }
 }
 
+
+// The dynamic shared memory of the two-phase staging (55296 bytes), allowed once per device
+// (before any graph capture: the occupancy query of plan creation calls it first).
+static void eri_prepare_dpps() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(eri_queue_dpps<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 55296);
+        cudaFuncSetAttribute(eri_queue_dpps<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 55296);
+        done[dev] = true;
+    }
+}
+
 void launch_eri_dpps(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
+    // two-phase plans stage the chunk's blocks in 55296 bytes of dynamic shared memory
+    const size_t smem = Q.scratch && !Q.jk.J ? 55296 : 0;
+    if (smem) eri_prepare_dpps();
     const bool jk = Q.jk.J != nullptr;
-    if (mixed) { if (jk) eri_queue_dpps<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_dpps<1, 0><<<grid, 128, 0, s>>>(Q); }
+    if (mixed) { if (jk) eri_queue_dpps<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_dpps<1, 0><<<grid, 128, smem, s>>>(Q); }
     else if (jk) eri_queue_dpps<0, 1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_dpps<0, 0><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_dpps<0, 0><<<grid, 128, smem, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_dpps(int mixed) {
+    eri_prepare_dpps();
     int n = 0;
     if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpps<1, 0>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dpps<0, 0>, 128, 0);

@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(128) eri_queue_dsps(const EriQueue Q) {
             // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
             // into shared memory, where they lie as in the scratch (consecutive slots); the warp
             // then copies them out as one contiguous run
-            __shared__ double stg[4 * 32 * 18];
+            extern __shared__ double stg[];  // 4 * 32 * 18 doubles (launch_eri_dsps)
             double *sb = stg + (threadIdx.x >> 5) * (32 * 18);
             if (lead) hrr_dsps(Q.pairs, p, q, acc, sb + kq * 18);
             __syncwarp();
@@ -290,16 +290,20 @@ __global__ void __launch_bounds__(128) eri_queue_dsps(const EriQueue Q) {
     }
 }
 
+
 void launch_eri_dsps(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
+    // two-phase plans stage the chunk's blocks in 18432 bytes of dynamic shared memory
+    const size_t smem = Q.scratch && !Q.jk.J ? 18432 : 0;
     const bool jk = Q.jk.J != nullptr;
-    if (mixed) { if (jk) eri_queue_dsps<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_dsps<1, 0><<<grid, 128, 0, s>>>(Q); }
+    if (mixed) { if (jk) eri_queue_dsps<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_dsps<1, 0><<<grid, 128, smem, s>>>(Q); }
     else if (jk) eri_queue_dsps<0, 1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_dsps<0, 0><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_dsps<0, 0><<<grid, 128, smem, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_dsps(int mixed) {
+
     int n = 0;
     if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dsps<1, 0>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_dsps<0, 0>, 128, 0);

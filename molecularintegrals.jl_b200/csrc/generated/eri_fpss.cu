@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(128) eri_queue_fpss(const EriQueue Q) {
             // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
             // into shared memory, where they lie as in the scratch (consecutive slots); the warp
             // then copies them out as one contiguous run
-            __shared__ double stg[4 * 32 * 30];
+            extern __shared__ double stg[];  // 4 * 32 * 30 doubles (launch_eri_fpss)
             double *sb = stg + (threadIdx.x >> 5) * (32 * 30);
             if (lead) hrr_fpss(Q.pairs, p, q, acc, sb + kq * 30);
             __syncwarp();
@@ -411,16 +411,20 @@ __global__ void __launch_bounds__(128) eri_queue_fpss(const EriQueue Q) {
     }
 }
 
+
 void launch_eri_fpss(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
+    // two-phase plans stage the chunk's blocks in 30720 bytes of dynamic shared memory
+    const size_t smem = Q.scratch && !Q.jk.J ? 30720 : 0;
     const bool jk = Q.jk.J != nullptr;
-    if (mixed) { if (jk) eri_queue_fpss<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_fpss<1, 0><<<grid, 128, 0, s>>>(Q); }
+    if (mixed) { if (jk) eri_queue_fpss<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_fpss<1, 0><<<grid, 128, smem, s>>>(Q); }
     else if (jk) eri_queue_fpss<0, 1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_fpss<0, 0><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_fpss<0, 0><<<grid, 128, smem, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_fpss(int mixed) {
+
     int n = 0;
     if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fpss<1, 0>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fpss<0, 0>, 128, 0);

@@ -1046,15 +1046,18 @@ __global__ void __launch_bounds__(128) eri_queue_fsfs(const EriQueue Q) {
         }
         const bool lead = live && s == 0;
         if (!JK && Q.scratch) {
-            // two-phase: each leader stores its quartet's whole block at its slot
-            if (lead) {
-                double res[100];
-                hrr_fsfs(Q.pairs, p, q, acc, res);
-                double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
-                    (__ldg(&Q.chunk_slot[c]) + base + kq) * (long long)100;
-#pragma unroll
-                for (int x = 0; x < 100; ++x) dst[x] = res[x];
-            }
+            // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
+            // into shared memory, where they lie as in the scratch (consecutive slots); the warp
+            // then copies them out as one contiguous run
+            extern __shared__ double stg[];  // 4 * 32 * 100 doubles (launch_eri_fsfs)
+            double *sb = stg + (threadIdx.x >> 5) * (32 * 100);
+            if (lead) hrr_fsfs(Q.pairs, p, q, acc, sb + kq * 100);
+            __syncwarp();
+            const int nlive = min(W, cnt - base);
+            double *__restrict__ dst = Q.scratch + __ldg(&Q.region[ch.w * kRegionFields]) +
+                (__ldg(&Q.chunk_slot[c]) + base) * (long long)100;
+            for (int t = lane; t < nlive * 100; t += 32) dst[t] = sb[t];
+            __syncwarp();
         } else if (lead) {
             double res[100];
             hrr_fsfs(Q.pairs, p, q, acc, res);
@@ -1069,16 +1072,34 @@ __global__ void __launch_bounds__(128) eri_queue_fsfs(const EriQueue Q) {
     }
 }
 
+
+// The dynamic shared memory of the two-phase staging (102400 bytes), allowed once per device
+// (before any graph capture: the occupancy query of plan creation calls it first).
+static void eri_prepare_fsfs() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(eri_queue_fsfs<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 102400);
+        cudaFuncSetAttribute(eri_queue_fsfs<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 102400);
+        done[dev] = true;
+    }
+}
+
 void launch_eri_fsfs(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
+    // two-phase plans stage the chunk's blocks in 102400 bytes of dynamic shared memory
+    const size_t smem = Q.scratch && !Q.jk.J ? 102400 : 0;
+    if (smem) eri_prepare_fsfs();
     const bool jk = Q.jk.J != nullptr;
-    if (mixed) { if (jk) eri_queue_fsfs<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_fsfs<1, 0><<<grid, 128, 0, s>>>(Q); }
+    if (mixed) { if (jk) eri_queue_fsfs<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_fsfs<1, 0><<<grid, 128, smem, s>>>(Q); }
     else if (jk) eri_queue_fsfs<0, 1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_fsfs<0, 0><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_fsfs<0, 0><<<grid, 128, smem, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_fsfs(int mixed) {
+    eri_prepare_fsfs();
     int n = 0;
     if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fsfs<1, 0>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_fsfs<0, 0>, 128, 0);

@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(128) eri_queue_ppps(const EriQueue Q) {
             // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
             // into shared memory, where they lie as in the scratch (consecutive slots); the warp
             // then copies them out as one contiguous run
-            __shared__ double stg[4 * 32 * 27];
+            extern __shared__ double stg[];  // 4 * 32 * 27 doubles (launch_eri_ppps)
             double *sb = stg + (threadIdx.x >> 5) * (32 * 27);
             if (lead) hrr_ppps(Q.pairs, p, q, acc, sb + kq * 27);
             __syncwarp();
@@ -364,16 +364,20 @@ __global__ void __launch_bounds__(128) eri_queue_ppps(const EriQueue Q) {
     }
 }
 
+
 void launch_eri_ppps(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
+    // two-phase plans stage the chunk's blocks in 27648 bytes of dynamic shared memory
+    const size_t smem = Q.scratch && !Q.jk.J ? 27648 : 0;
     const bool jk = Q.jk.J != nullptr;
-    if (mixed) { if (jk) eri_queue_ppps<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_ppps<1, 0><<<grid, 128, 0, s>>>(Q); }
+    if (mixed) { if (jk) eri_queue_ppps<1, 1><<<grid, 128, 0, s>>>(Q); else eri_queue_ppps<1, 0><<<grid, 128, smem, s>>>(Q); }
     else if (jk) eri_queue_ppps<0, 1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_ppps<0, 0><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_ppps<0, 0><<<grid, 128, smem, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_ppps(int mixed) {
+
     int n = 0;
     if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ppps<1, 0>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_ppps<0, 0>, 128, 0);

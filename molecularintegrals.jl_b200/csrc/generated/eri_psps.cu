@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128) eri_queue_psps(const EriQueue Q) {
             // two-phase: the leaders' HRR writes the blocks of the chunk's quartets straight
             // into shared memory, where they lie as in the scratch (consecutive slots); the warp
             // then copies them out as one contiguous run
-            __shared__ double stg[4 * 32 * 9];
+            extern __shared__ double stg[];  // 4 * 32 * 9 doubles (launch_eri_psps)
             double *sb = stg + (threadIdx.x >> 5) * (32 * 9);
             if (lead) hrr_psps(Q.pairs, p, q, acc, sb + kq * 9);
             __syncwarp();
@@ -226,15 +226,19 @@ __global__ void __launch_bounds__(128) eri_queue_psps(const EriQueue Q) {
     }
 }
 
+
 void launch_eri_psps(const EriQueue &Q, int mixed, int grid, cudaStream_t s) {
     if (Q.nchunks <= 0 || grid <= 0) return;
+    // two-phase plans stage the chunk's blocks in 9216 bytes of dynamic shared memory
+    const size_t smem = Q.scratch && !Q.jk.J ? 9216 : 0;
     (void)mixed;  // no FP32 variant for this class (MIXED_MIN_VRR)
     if (Q.jk.J) eri_queue_psps<0, 1><<<grid, 128, 0, s>>>(Q);
-    else eri_queue_psps<0, 0><<<grid, 128, 0, s>>>(Q);
+    else eri_queue_psps<0, 0><<<grid, 128, smem, s>>>(Q);
 }
 
 // Resident blocks of 128 threads per SM for the queue kernel (sizes the persistent grid).
 int occupancy_eri_psps(int mixed) {
+
     int n = 0;
     (void)mixed;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, eri_queue_psps<0, 0>, 128, 0);

@@ -512,33 +512,48 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
         }
         __syncthreads();
         const long long ijmax = s_ij[R - 1];  // rows are in increasing ij
-        for (long long kl = threadIdx.x; kl <= ijmax; kl += kGatherThreads) {
-            const int2 qe = __ldg(&col[cbase + kl]);
-            const int posQ = qe.x >> 4, clsQ = qe.x & 15;
-            const int qa = qe.y >> 16, qb = qe.y & 0xffff;
-            const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
-            const long long *rg = reg[braP ? 0 : 1][clsQ];
-            const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
-            const long long db = bpos - rg[1], dk = kpos - rg[2];
-            const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
-            // component x = row part * rstride + column part
-            const int nq = c_pair_na[clsQ] * c_pair_nb[clsQ], qc = qa * c_pair_nb[clsQ] + qb;
-            const int nP = c_pair_na[clsP] * nbP;
-            const long long rstride = braP ? nq : 1, cpart = braP ? qc : (long long)qc * nP;
-            const double *__restrict__ src = scratch + rg[0] + slot * rg[4] + cpart;
-            const long long rs = rstride;
-            // rows with ij >= kl: a suffix of the increasing row list
-            int r0 = 0;
-            while (r0 < R && s_ij[r0] < kl) ++r0;
-            int r = r0;
-            for (; r + 4 <= R; r += 4) {
-                double v[4];
+        // two columns per thread and pass (kl and kl + kGatherThreads), their descriptor and
+        // scratch loads issued before their stores
+        for (long long kl0 = threadIdx.x; kl0 <= ijmax; kl0 += 2 * kGatherThreads) {
+            const double *src[2];
+            long long rs[2], kl[2];
+            int r0[2];
 #pragma unroll
-                for (int t = 0; t < 4; ++t) v[t] = __ldg(src + s_rc[r + t] * rs);
-#pragma unroll
-                for (int t = 0; t < 4; ++t) obase[s_ij[r + t] * (s_ij[r + t] + 1) / 2 + kl] = v[t];
+            for (int c = 0; c < 2; ++c) {
+                kl[c] = kl0 + c * kGatherThreads;
+                const bool on = kl[c] <= ijmax;
+                const int2 qe = on ? __ldg(&col[cbase + kl[c]]) : make_int2(clsP, 0);
+                const int posQ = on ? qe.x >> 4 : posP, clsQ = qe.x & 15;
+                const int qa = qe.y >> 16, qb = qe.y & 0xffff;
+                const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
+                const long long *rg = reg[braP ? 0 : 1][clsQ];
+                const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
+                const long long db = bpos - rg[1], dk = kpos - rg[2];
+                const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
+                // component x = row part * rstride + column part
+                const int nq = c_pair_na[clsQ] * c_pair_nb[clsQ], qc = qa * c_pair_nb[clsQ] + qb;
+                const int nP = c_pair_na[clsP] * nbP;
+                rs[c] = braP ? nq : 1;
+                src[c] = scratch + rg[0] + slot * rg[4] + (braP ? (long long)qc : (long long)qc * nP);
+                // rows with ij >= kl: a suffix of the increasing row list (none past ijmax)
+                int r = 0;
+                while (r < R && s_ij[r] < kl[c]) ++r;
+                r0[c] = on ? r : R;
             }
-            for (; r < R; ++r) obase[s_ij[r] * (s_ij[r] + 1) / 2 + kl] = __ldg(src + s_rc[r] * rs);
+            for (int r = min(r0[0], r0[1]); r < R; r += 4) {
+                double v[2][4];
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+#pragma unroll
+                    for (int t = 0; t < 4; ++t)
+                        v[c][t] = (r + t < R && r + t >= r0[c]) ? __ldg(src[c] + s_rc[r + t] * rs[c]) : 0.0;
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+#pragma unroll
+                    for (int t = 0; t < 4; ++t)
+                        if (r + t < R && r + t >= r0[c])
+                            obase[s_ij[r + t] * (s_ij[r + t] + 1) / 2 + kl[c]] = v[c][t];
+            }
         }
     }
 }
