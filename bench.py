@@ -482,21 +482,22 @@ def measure_fp64_peak(dev) -> float:
     return best
 
 
-def measure_e2e(eng, dev, stream, mols, groups, fp32_cut, steps, ring_doubles=64 * 2**20):
+def measure_e2e(eng, dev, stream, mols, groups, fp32_cut, steps, ring_doubles=32 * 2**20, ncopy=2):
     """The headline metric end to end through the public batch API: per group, the plan is
     created from the host basis arrays (normalisation, pair tables, device bound pass, work
     queues, uploads), executed, and its packed vectors are copied to pinned host memory through
-    a ring of two 512 MB pinned buffers on a copy stream (overlapped with the next group's
-    compute; two device outputs alternate).  Host wall clock around whole passes."""
+    a ring of four 256 MB pinned buffers on `ncopy` copy streams taking the chunks in turn
+    (overlapped with the next group's compute; two device outputs alternate).  Host wall clock
+    around whole passes."""
     import torch
     from molints_b200 import engine as E
     if steps <= 0:
         return None
     cap = max(sum(mols[i].npacked for i in g) for g in groups)
     outs = [torch.empty(cap, dtype=torch.float64, device=dev) for _ in range(2)]
-    ring = [torch.empty(ring_doubles, dtype=torch.float64, pin_memory=True) for _ in range(2)]
-    copy = torch.cuda.Stream(dev)
-    done = [torch.cuda.Event() for _ in range(2)]
+    ring = [torch.empty(ring_doubles, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+    copies = [torch.cuda.Stream(dev) for _ in range(ncopy)]
+    done = [[torch.cuda.Event() for _ in range(ncopy)] for _ in range(2)]
     computed = torch.cuda.Event()
     h2d = 0
     for g in groups:
@@ -511,24 +512,28 @@ def measure_e2e(eng, dev, stream, mols, groups, fp32_cut, steps, ring_doubles=64
         chunk = 0
         for gi, g in enumerate(groups):
             buf = outs[gi % 2]
-            stream.wait_event(done[gi % 2])  # the copies of group gi-2 have read this buffer
+            for ev in done[gi % 2]:
+                stream.wait_event(ev)  # the copies of group gi-2 have read this buffer
             plan = eng.plan_batch([mols[i] for i in g], boys=E.BOYS_EXACT, precision=E.MIXED,
                                   fp32_cutoff=fp32_cut, screen_cutoff=SCREEN_CUTOFF)
             plan.execute(buf.data_ptr())
             computed.record(stream)
-            copy.wait_event(computed)
-            with torch.cuda.stream(copy):
-                for off in range(0, plan.npacked, ring_doubles):
-                    n = min(ring_doubles, plan.npacked - off)
-                    ring[chunk % 2][:n].copy_(buf[off:off + n], non_blocking=True)
-                    chunk += 1
-            done[gi % 2].record(copy)
+            for cs in copies:
+                cs.wait_event(computed)
+            for off in range(0, plan.npacked, ring_doubles):
+                n = min(ring_doubles, plan.npacked - off)
+                with torch.cuda.stream(copies[chunk % ncopy]):
+                    ring[chunk % 4][:n].copy_(buf[off:off + n], non_blocking=True)
+                chunk += 1
+            for k, cs in enumerate(copies):
+                done[gi % 2][k].record(cs)
             plan.close()
         torch.cuda.synchronize(dev)
         walls.append(time.perf_counter() - t0)
     n = sum(mols[i].npacked for g in groups for i in g)
     return {"value": n * len(walls) / sum(walls), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 8 * n, "steps": len(walls), "seconds_per_step": walls,
+            "d2h_gbs": 8 * n / (sum(walls) / len(walls)) / 1e9,
             "timing": "host wall clock: plan creation from host arrays, execute, D2H of every "
                       "packed vector into pinned host memory (MIXED, same options as value)"}
 

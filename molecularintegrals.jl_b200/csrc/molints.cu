@@ -139,7 +139,8 @@ struct molints_plan {
     int64_t n_gq = 0;
     int4 *gq = nullptr;                // global shells (I, J, K, L), reference order
     int *gq_mol = nullptr;
-    int *sh_L = nullptr, *sh_K = nullptr, *sh_fn = nullptr;
+    int *sh_L = nullptr, *sh_K = nullptr, *sh_fn = nullptr;  // shells' L and primitive count (all
+                                                             // plans), first function (g plans)
     double plan_ms[4] = {0, 0, 0, 0};  // plan creation phases (molints_stats.plan_ms)
     // CUDA graph of one execute (molints_plan_set_graph), valid for graph_out
     int use_graph = 0;
@@ -363,6 +364,35 @@ class HostPool {
 
 // ------------------------------------------------------------------ device kernels
 namespace molints {
+
+// The normalised contraction coefficients of every shell, in place: raw coef x the primitive
+// norm (2a/pi)^(3/4) (4a)^(L/2) x the contracted norm 1/sqrt(S), S = sum_ij c_i c_j
+// (2 sqrt(a_i a_j) / (a_i + a_j))^(L + 3/2) the self-overlap of the shell's function (PGBF/CGBF
+// normalize!, src/Basis.jl:42-83; the component factor 1/sqrt((2I-1)!!(2J-1)!!(2K-1)!!) is
+// applied by the ERI kernels).  One thread per shell; a shell whose S is not positive sets
+// *bad (the plan is refused).
+__global__ void normalise_shells_kernel(int ns, const int *__restrict__ L, const int *__restrict__ K,
+                                        const int *__restrict__ poff, const double *__restrict__ expn,
+                                        double *__restrict__ coef, int *__restrict__ bad) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ns) return;
+    const int Ls = L[g], Ks = K[g], p0 = poff[g];
+    double S = 0.0;
+    for (int i = 0; i < Ks; ++i)
+        for (int j = 0; j < Ks; ++j) {
+            const double x = expn[p0 + i], y = expn[p0 + j];
+            S += coef[p0 + i] * coef[p0 + j] * pow(2.0 * sqrt(x * y) / (x + y), Ls + 1.5);
+        }
+    if (!(S > 0.0)) {
+        atomicExch(bad, 1);
+        return;
+    }
+    const double cn = 1.0 / sqrt(S);
+    for (int i = 0; i < Ks; ++i) {
+        const double a = expn[p0 + i];
+        coef[p0 + i] *= cn * pow(2.0 * a / 3.14159265358979323846, 0.75) * pow(4.0 * a, 0.5 * Ls);
+    }
+}
 
 __global__ void build_pairs_kernel(int npair, const int2 *__restrict__ pair_ab,
                                    const int4 *__restrict__ info, const int *__restrict__ pp_src,
@@ -1104,9 +1134,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             p->fp32[x][y] = opts.precision == MOLINTS_MIXED && has32 && !slower32;
         }
 
-    // Normalised coefficients: raw coef x (2a/pi)^(3/4) (4a)^(L/2) x CGBF norm; the component
-    // factor 1/sqrt((2I-1)!!(2J-1)!!(2K-1)!!) is applied by the generated kernels
-    // (PGBF/CGBF normalize!, src/Basis.jl:42-83).
+    // Shells of all molecules in one list, primitives in one array (raw coefficients: the
+    // device normalises them, normalise_shells_kernel).
     std::vector<double> xyz(3 * (size_t)std::max(ns, 1)), expn(std::max(nprim, 1)), ncoef(std::max(nprim, 1));
     std::vector<int> L(std::max(ns, 1)), K(std::max(ns, 1)), poff(std::max(ns, 1)), fn_off(std::max(ns, 1));
     for (int m = 0; m < nmol; ++m) {
@@ -1118,18 +1147,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             for (int k = 0; k < 3; ++k) xyz[3 * g + k] = b->xyz[3 * s + k];
             L[g] = Ls; K[g] = Ks; poff[g] = prim_base[m] + p0; fn_off[g] = f;
             f += ncart(Ls);
-            double S = 0;
-            for (int i = 0; i < Ks; ++i)
-                for (int j = 0; j < Ks; ++j) {
-                    const double x = b->expn[p0 + i], y = b->expn[p0 + j];
-                    S += b->coef[p0 + i] * b->coef[p0 + j] * std::pow(2 * std::sqrt(x * y) / (x + y), Ls + 1.5);
-                }
-            if (!(S > 0.0)) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: zero contracted function"); }
-            const double cn = 1.0 / std::sqrt(S);
             for (int i = 0; i < Ks; ++i) {
-                const double a = b->expn[p0 + i];
-                expn[poff[g] + i] = a;
-                ncoef[poff[g] + i] = b->coef[p0 + i] * cn * std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * Ls);
+                expn[poff[g] + i] = b->expn[p0 + i];
+                ncoef[poff[g] + i] = b->coef[p0 + i];  // raw here; normalised on the device
             }
         }
     }
@@ -1248,6 +1268,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     rc = rc ? rc : dev_alloc(ctx, &p->expn, (size_t)nprim, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->ncoef, (size_t)nprim, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->sh_poff, (size_t)ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_L, (size_t)ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_K, (size_t)ns, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->pair_ab, (size_t)npair, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->info, (size_t)npair, &p->bytes);
     rc = rc ? rc : dev_alloc(ctx, &p->geo, (size_t)npair, &p->bytes);
@@ -1271,12 +1293,21 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         (e = cudaMemcpyAsync(p->expn, expn.data(), (size_t)nprim * sizeof(double), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->ncoef, ncoef.data(), (size_t)nprim * sizeof(double), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->sh_poff, poff.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->sh_L, L.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(p->sh_K, K.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemsetAsync(p->counters + nc2, 0, sizeof(int), s)) ||
         (e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nall * sizeof(int), cudaMemcpyHostToDevice, s))) {
         dev_free(ctx, pbound); ctx->held -= scratch; plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
     }
+    // the raw coefficients become normalised ones in place; a shell with no positive
+    // self-overlap flags counters[nc2] (read back with the bounds)
+    if (ns > 0)
+        normalise_shells_kernel<<<(ns + 127) / 128, 128, 0, s>>>(ns, p->sh_L, p->sh_K, p->sh_poff, p->expn,
+                                                                 p->ncoef, p->counters + nc2);
+    int bad_shell = 0;
     if (npair > 0) {
         build_pairs_kernel<<<build_pairs_blocks(npair), 128, 0, s>>>(npair, p->pair_ab, p->info, p->pp_src,
                                                                p->sh_xyz, p->sh_poff, p->expn,
@@ -1290,12 +1321,14 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     if ((e = cudaGetLastError()) ||
         (nall > 0 && (e = cudaMemcpyAsync(pb_h.data(), pbound, nall * sizeof(double2),
                                           cudaMemcpyDeviceToHost, s))) ||
+        (e = cudaMemcpyAsync(&bad_shell, p->counters + nc2, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
         (e = cudaStreamSynchronize(s))) {
         dev_free(ctx, pbound); ctx->held -= scratch; plan_free(p);
         return cuda_fail(ctx, e, "plan_create bound pass");
     }
     dev_free(ctx, pbound);
     ctx->held -= scratch;
+    if (bad_shell) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: zero contracted function"); }
 
     p->plan_ms[1] = ms_since(t_phase);
     t_phase = clk::now();
@@ -1747,14 +1780,10 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         // staged before the call returns)
         rc = dev_alloc(ctx, &p->gq, (size_t)p->n_gq, &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->gq_mol, (size_t)p->n_gq, &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->sh_L, (size_t)ns, &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->sh_K, (size_t)ns, &p->bytes);
         if (!rc) rc = dev_alloc(ctx, &p->sh_fn, (size_t)ns, &p->bytes);
         if (rc) { plan_free(p); return rc; }
         if ((e = cudaMemcpyAsync(p->gq, gq_h.data(), gq_h.size() * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
             (e = cudaMemcpyAsync(p->gq_mol, gq_mol_h.data(), gq_mol_h.size() * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-            (e = cudaMemcpyAsync(p->sh_L, L.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-            (e = cudaMemcpyAsync(p->sh_K, K.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
             (e = cudaMemcpyAsync(p->sh_fn, fn_off.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
             (e = cudaStreamSynchronize(s))) {
             plan_free(p);

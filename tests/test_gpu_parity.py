@@ -359,9 +359,12 @@ def test_edge_cases(eng):
     assert v.shape == (1,) and v[0] == pytest.approx(2 / np.sqrt(np.pi) * np.sqrt(2.0 / 2), rel=1e-14)
     empty = mi.Shells.from_list([])
     assert eng.eri_packed(empty).shape == (0,)
+    # a g shell runs the generic kernel (tests/test_gpu_gshells.py); l = 5 is refused
     g_shell = mi.Shells.from_list([((0.0, 0.0, 0.0), 4, [(1.0, 1.0)])])
+    assert eng.eri_packed(g_shell).shape == (mi.Shells.from_list([((0.0, 0.0, 0.0), 4, [(1.0, 1.0)])]).npacked,)
+    h_shell = mi.Shells.from_list([((0.0, 0.0, 0.0), 5, [(1.0, 1.0)])])
     with pytest.raises(engine.MolintsError) as e:
-        eng.eri_packed(g_shell)
+        eng.eri_packed(h_shell)
     assert e.value.status == -2
     # one f shell: (ff|ff) on one centre, against the oracle
     f_shell = mi.Shells.from_list([((0.1, -0.2, 0.3), 3, [(1.3, 1.0)])])
