@@ -41,8 +41,6 @@ NMONO = 20           # monomials AB^(px,py,pz), px+py+pz <= 3
 # Classes with at least this many block entries and at most MIXED_MAX_ACC accumulators per
 # thread get an FP32 variant for MIXED quartets (stage-2 products summed in FP32 per batch).
 MIXED_MIN_NBLK = 32
-# Upper bound of the resident blocks of 128 threads a Rys queue kernel is compiled for.
-RYS_MIN_BLOCKS = 4
 MIXED_MAX_ACC = 24
 COL_MIN_NC = 16
 COL_MAX_NA = 48
@@ -202,10 +200,6 @@ def emit_class_pair(X, Y):
     koff, kterm = _flat_terms(t["ket"])
     smem_block = (128 // t["G"]) * t["smem_group"] * 8
     assert smem_block <= 227 * 1024, (tag, smem_block)
-    # resident blocks the shared memory allows (228 KB per SM, 1 KB reserved per block), at
-    # most RYS_MIN_BLOCKS: the register budget is capped to match, so registers do not cut the
-    # occupancy below what the shared memory allows
-    min_blocks = max(1, min(RYS_MIN_BLOCKS, (228 * 1024) // (smem_block + 1024)))
     diag = X == Y
     bound_kernel = bound_launch = ""
     if diag:
@@ -300,7 +294,7 @@ __device__ __forceinline__ RysClassTabs tabs_{tag}() {{
 }}
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, {min_blocks}) rys_queue_{tag}(const EriQueue Q, const RysTab R) {{
+__global__ void __launch_bounds__(128) rys_queue_{tag}(const EriQueue Q, const RysTab R) {{
     rys_queue_body<C_{tag}, MIXED>(Q, R, tabs_{tag}());
 }}
 {bound_kernel}

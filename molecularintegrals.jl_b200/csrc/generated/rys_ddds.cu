@@ -87,7 +87,7 @@ __device__ __forceinline__ RysClassTabs tabs_ddds() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_ddds(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_ddds(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_ddds, MIXED>(Q, R, tabs_ddds());
 }
 

@@ -97,7 +97,7 @@ __device__ __forceinline__ RysClassTabs tabs_ddpp() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_ddpp(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_ddpp(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_ddpp, MIXED>(Q, R, tabs_ddpp());
 }
 

@@ -78,7 +78,7 @@ __device__ __forceinline__ RysClassTabs tabs_ddps() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_ddps(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_ddps(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_ddps, MIXED>(Q, R, tabs_ddps());
 }
 

@@ -73,7 +73,7 @@ __device__ __forceinline__ RysClassTabs tabs_ddss() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_ddss(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_ddss(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_ddss, MIXED>(Q, R, tabs_ddss());
 }
 

@@ -107,7 +107,7 @@ __device__ __forceinline__ RysClassTabs tabs_dpdp() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dpdp(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dpdp(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dpdp, MIXED>(Q, R, tabs_dpdp());
 }
 

@@ -65,7 +65,7 @@ __device__ __forceinline__ RysClassTabs tabs_dpds() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dpds(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dpds(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dpds, MIXED>(Q, R, tabs_dpds());
 }
 

@@ -71,7 +71,7 @@ __device__ __forceinline__ RysClassTabs tabs_dppp() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dppp(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dppp(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dppp, MIXED>(Q, R, tabs_dppp());
 }
 

@@ -60,7 +60,7 @@ __device__ __forceinline__ RysClassTabs tabs_dpps() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dpps(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dpps(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dpps, MIXED>(Q, R, tabs_dpps());
 }
 

@@ -58,7 +58,7 @@ __device__ __forceinline__ RysClassTabs tabs_dpss() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dpss(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dpss(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dpss, MIXED>(Q, R, tabs_dpss());
 }
 

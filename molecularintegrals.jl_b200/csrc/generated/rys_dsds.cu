@@ -54,7 +54,7 @@ __device__ __forceinline__ RysClassTabs tabs_dsds() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dsds(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dsds(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dsds, MIXED>(Q, R, tabs_dsds());
 }
 

@@ -58,7 +58,7 @@ __device__ __forceinline__ RysClassTabs tabs_dspp() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dspp(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dspp(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dspp, MIXED>(Q, R, tabs_dspp());
 }
 

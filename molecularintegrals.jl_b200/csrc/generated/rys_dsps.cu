@@ -52,7 +52,7 @@ __device__ __forceinline__ RysClassTabs tabs_dsps() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dsps(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dsps(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dsps, MIXED>(Q, R, tabs_dsps());
 }
 

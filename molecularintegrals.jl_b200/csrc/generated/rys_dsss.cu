@@ -51,7 +51,7 @@ __device__ __forceinline__ RysClassTabs tabs_dsss() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_dsss(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_dsss(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_dsss, MIXED>(Q, R, tabs_dsss());
 }
 

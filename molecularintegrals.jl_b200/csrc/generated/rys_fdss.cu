@@ -89,7 +89,7 @@ __device__ __forceinline__ RysClassTabs tabs_fdss() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_fdss(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fdss(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fdss, MIXED>(Q, R, tabs_fdss());
 }
 

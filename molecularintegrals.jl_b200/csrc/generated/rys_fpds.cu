@@ -76,7 +76,7 @@ __device__ __forceinline__ RysClassTabs tabs_fpds() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_fpds(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fpds(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fpds, MIXED>(Q, R, tabs_fpds());
 }
 

@@ -85,7 +85,7 @@ __device__ __forceinline__ RysClassTabs tabs_fpfs() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 3) rys_queue_fpfs(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fpfs(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fpfs, MIXED>(Q, R, tabs_fpfs());
 }
 

@@ -84,7 +84,7 @@ __device__ __forceinline__ RysClassTabs tabs_fppp() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_fppp(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fppp(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fppp, MIXED>(Q, R, tabs_fppp());
 }
 

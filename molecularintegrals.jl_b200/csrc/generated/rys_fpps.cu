@@ -69,7 +69,7 @@ __device__ __forceinline__ RysClassTabs tabs_fpps() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_fpps(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fpps(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fpps, MIXED>(Q, R, tabs_fpps());
 }
 

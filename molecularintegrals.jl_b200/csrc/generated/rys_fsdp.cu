@@ -88,7 +88,7 @@ __device__ __forceinline__ RysClassTabs tabs_fsdp() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_fsdp(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fsdp(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fsdp, MIXED>(Q, R, tabs_fsdp());
 }
 

@@ -57,7 +57,7 @@ __device__ __forceinline__ RysClassTabs tabs_fsds() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_fsds(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fsds(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fsds, MIXED>(Q, R, tabs_fsds());
 }
 

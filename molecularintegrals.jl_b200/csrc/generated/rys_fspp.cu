@@ -62,7 +62,7 @@ __device__ __forceinline__ RysClassTabs tabs_fspp() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_fspp(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_fspp(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_fspp, MIXED>(Q, R, tabs_fspp());
 }
 

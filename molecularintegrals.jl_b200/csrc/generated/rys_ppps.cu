@@ -55,7 +55,7 @@ __device__ __forceinline__ RysClassTabs tabs_ppps() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_ppps(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_ppps(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_ppps, MIXED>(Q, R, tabs_ppps());
 }
 

@@ -53,7 +53,7 @@ __device__ __forceinline__ RysClassTabs tabs_ppss() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_ppss(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_ppss(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_ppss, MIXED>(Q, R, tabs_ppss());
 }
 

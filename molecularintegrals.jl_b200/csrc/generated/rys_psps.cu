@@ -50,7 +50,7 @@ __device__ __forceinline__ RysClassTabs tabs_psps() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_psps(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_psps(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_psps, MIXED>(Q, R, tabs_psps());
 }
 

@@ -50,7 +50,7 @@ __device__ __forceinline__ RysClassTabs tabs_psss() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_psss(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_psss(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_psss, MIXED>(Q, R, tabs_psss());
 }
 

@@ -50,7 +50,7 @@ __device__ __forceinline__ RysClassTabs tabs_ssss() {
 }
 
 template <int MIXED>
-__global__ void __launch_bounds__(128, 4) rys_queue_ssss(const EriQueue Q, const RysTab R) {
+__global__ void __launch_bounds__(128) rys_queue_ssss(const EriQueue Q, const RysTab R) {
     rys_queue_body<C_ssss, MIXED>(Q, R, tabs_ssss());
 }
 
