@@ -124,8 +124,10 @@ typedef struct molints_stats {
     double device_ms;         /* device time of the last execute (CUDA events) */
     int64_t n_prim_pairs;     /* primitive pairs of all shell pairs */
     int64_t n_prim_pairs_kept;/* primitive pairs left after prim_cutoff */
-    /* host wall time of plan creation, ms: [0] tables before the bound pass, [1] the bound
-     * pass (upload, kernels, read-back), [2] screening and work queues, [3] upload */
+    /* host wall time of plan creation, ms: [0] host tables (pair list, stage-1 primitive
+     * pairs, gather tables), [1] uploads and the device build up to its one read-back
+     * (normalisation, bound pass, screening, pair re-sort, work-queue sizes), [2] work-queue
+     * emission and ordering (launches), [3] the rest (g-shell quartet lists) */
     double plan_ms[4];
 } molints_stats;
 

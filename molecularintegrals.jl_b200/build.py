@@ -42,13 +42,13 @@ def sources():
     finally:
         sys.path.pop(0)
     gen = gen_eri.generate()
-    return ([CSRC / "molints.cu", CSRC / "noalloc.cu", CSRC / "serve.cu", CSRC / "one_e.cu",
+    return ([CSRC / "molints.cu", CSRC / "plan_build.cu", CSRC / "noalloc.cu", CSRC / "serve.cu", CSRC / "one_e.cu",
              CSRC / "eri_generic.cu", CSRC / "generated" / "rys_tables.cu"] +
             sorted(gen))
 
 
 def _deps(src: Path):
-    return [src, CSRC / "eri_common.cuh", CSRC / "rys_common.cuh", CSRC / "eri_dispatch.h",
+    return [src, CSRC / "eri_common.cuh", CSRC / "rys_common.cuh", CSRC / "eri_dispatch.h", CSRC / "plan_build.cuh",
             CSRC / "class_table.h", INCLUDE / "molints.h"]
 
 

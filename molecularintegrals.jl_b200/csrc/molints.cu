@@ -12,24 +12,19 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <chrono>
 #include <cmath>
-#include <condition_variable>
 #include <cstdio>
 #include <cstring>
-#include <deque>
-#include <functional>
-#include <mutex>
 #include <new>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "../../include/molints.h"
 #include "eri_common.cuh"
 #include "class_table.h"
 #include "eri_dispatch.h"
+#include "plan_build.cuh"
 
 using namespace molints;
 
@@ -72,10 +67,11 @@ struct molints_ctx {
     // the table molints_set_class_methods(NULL) restores: the tuned table of class_table.h on
     // the device it was measured on, all zero (HGP everywhere) elsewhere
     int32_t default_method[kNumPairClasses][kNumPairClasses] = {};
-    char *stage = nullptr;     // pinned host buffer of plan uploads (work queues, pair tables)
+    char *stage = nullptr;     // pinned host buffer of plan uploads (shells, stage-1 pair tables)
     size_t stage_bytes = 0;
-    cudaEvent_t stage_ev = nullptr;  // recorded after uploads that a plan creation left in flight
-    bool stage_busy = false;
+    // lane-split bound of the HGP work queues: a lane's share of a split quartet costs at most
+    // this many (ss|ss)-equivalent primitive quartets (hgp_split)
+    double lane_cost = 80.0;
     std::string err;
 };
 
@@ -97,9 +93,11 @@ struct molints_plan {
     double class_cost[kNumPairClasses][kNumPairClasses] = {};  // kept primitive quartets
     int method[kNumPairClasses][kNumPairClasses] = {};  // MOLINTS_METHOD_HGP or _RYS
     int fp32[kNumPairClasses][kNumPairClasses] = {};    // MIXED and this class's FP32 variant used
-    // host copies (final, screened order)
-    std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
+    // host copies (final, screened order): pair_mol from plan creation (the re-sort by kept
+    // count stays within each molecule's run), the rest fetched on first use (plan_host_tables)
     std::vector<int> pair_mol;         // canonical pair -> molecule
+    bool host_tables = false;
+    std::vector<int> pair_ref;         // canonical pair -> reference pair index i(i+1)/2+j
     std::vector<int> npp_h;            // kept primitive pairs per shell pair
     std::vector<double2> bnd_h;        // (Qabs, R) per shell pair
     // device buffers
@@ -197,28 +195,46 @@ int pair_class_of(int la, int lb) {
     return -1;
 }
 
-// Lane split of an HGP work-queue chunk whose bra pair has nb and ket pair nk kept primitive
-// pairs, in a class whose primitive quartet costs `cost` (kEriPrimCost; (ss|ss) ~ 1).  A lane
-// evaluates its quartet's primitive quartets one after another; a heavy quartet (six-primitive
-// core shells: 36 x 36) on one lane outlasts the rest of the launch.  Its primitive quartets
-// are therefore split over S = 2^lg lanes (S <= 32) -- ket primitives over Sj = 2^lgj of them
-// first (Sj <= nk), then bra primitives over S / Sj -- until a lane's share costs at most
-// kLaneCost.  Returns lg | lgj << 4, the chunk's split field.  A pure function of
-// (nb, nk, class): the same quartet gets the same split, and so the same rounding, in every
-// plan.
-constexpr double kLaneCost = 80.0;
-int hgp_split(int nb, int nk, double cost) {
-    int lg = 0, lgj = 0;
-    auto share = [&](int gj, int gi) {
-        return cost * (double)((nk + (1 << gj) - 1) >> gj) * (double)((nb + (1 << gi) - 1) >> gi);
-    };
-    while (lg < 5 && share(lgj, lg - lgj) > kLaneCost) {
-        if ((nk >> lgj) >= 2) ++lgj;
-        else if ((nb >> (lg - lgj)) < 2) break;
-        ++lg;
+// Stable LSD radix order of keys[0..n) over their low `bits` bits (8-bit digits): the
+// permutation position -> index, equal keys in index order.  O(n bits / 8).
+std::vector<uint32_t> radix_order(const std::vector<uint64_t> &keys, int bits) {
+    const size_t n = keys.size();
+    std::vector<uint64_t> k(keys), k2(n);
+    std::vector<uint32_t> v(n), v2(n);
+    for (size_t i = 0; i < n; ++i) v[i] = (uint32_t)i;
+    for (int sh = 0; sh < bits; sh += 8) {
+        size_t at[257] = {};
+        for (size_t i = 0; i < n; ++i) ++at[((k[i] >> sh) & 255) + 1];
+        if (at[1] == n) continue;  // every key has this digit 0
+        for (int d = 0; d < 256; ++d) at[d + 1] += at[d];
+        for (size_t i = 0; i < n; ++i) {
+            const size_t j = at[(k[i] >> sh) & 255]++;
+            k2[j] = k[i];
+            v2[j] = v[i];
+        }
+        k.swap(k2);
+        v.swap(v2);
     }
-    return lg | (lgj << 4);
+    return v;
 }
+
+// Bits needed to hold values 0..v.
+int bits_for(uint64_t v) {
+    int b = 0;
+    while (v >> b) ++b;
+    return b;
+}
+
+// Sub-buffers of one allocation: take<T>(n) returns the byte offset of n elements of T, each
+// sub-buffer 256-byte aligned (at least one element, so no two share an address).
+struct Carve {
+    size_t at = 0;
+    template <typename T> size_t take(long long count) {
+        const size_t o = at;
+        at += ((size_t)std::max<long long>(count, 1) * sizeof(T) + 255) & ~(size_t)255;
+        return o;
+    }
+};
 
 template <typename T>
 int dev_alloc(molints_ctx *ctx, T **p, size_t count, int64_t *tally) {
@@ -259,14 +275,9 @@ int ctx_scratch(molints_ctx *ctx, int64_t need) {
 }
 
 // The pinned upload buffer of the context, grown to at least `bytes` (a pinned source makes
-// the plan uploads asynchronous DMA at full link speed).  A plan creation that returns with its
-// uploads in flight marks the buffer busy; the next one waits for them before writing it.
+// the plan uploads asynchronous DMA at full link speed).  Plan creation synchronises on its
+// summary read-back after its last upload, so the buffer is free whenever a creation starts.
 int ctx_stage(molints_ctx *ctx, size_t bytes) {
-    if (ctx->stage_busy) {  // the previous plan's uploads may still read the buffer
-        cudaError_t e = cudaEventSynchronize(ctx->stage_ev);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "plan upload buffer");
-        ctx->stage_busy = false;
-    }
     if (ctx->stage_bytes >= bytes) return MOLINTS_OK;
     if (ctx->stage) cudaFreeHost(ctx->stage);
     ctx->stage = nullptr;
@@ -280,85 +291,6 @@ int ctx_stage(molints_ctx *ctx, size_t bytes) {
     ctx->stage_bytes = want;
     return MOLINTS_OK;
 }
-
-// Host worker threads shared by every context of the process (the serving slots create plans
-// concurrently and share them).  Created on first use and kept until the process exits, so a
-// plan creation pays no thread start-up.  run(n, fn) calls fn(0..n-1) on the workers and the
-// calling thread and returns when all calls are done; concurrent run()s from several threads
-// interleave on the same workers.
-class HostPool {
-  public:
-    static HostPool &instance() {
-        static HostPool *pool = new HostPool();  // never destroyed: its threads outlive main
-        return *pool;
-    }
-    void run(int n, const std::function<void(int)> &fn) {
-        if (n <= 0) return;
-        if (n == 1 || nthreads_ == 0) {
-            for (int i = 0; i < n; ++i) fn(i);
-            return;
-        }
-        Job job;
-        job.fn = &fn;
-        job.n = n;
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            jobs_.push_back(&job);
-        }
-        cv_.notify_all();
-        work(job);
-        std::unique_lock<std::mutex> lk(mu_);
-        auto it = std::find(jobs_.begin(), jobs_.end(), &job);
-        if (it != jobs_.end()) jobs_.erase(it);
-        // no worker can pick the job up any more; wait for those inside it
-        done_cv_.wait(lk, [&] { return job.users == 0 && job.done.load() == n; });
-    }
-
-  private:
-    struct Job {
-        const std::function<void(int)> *fn = nullptr;
-        int n = 0;
-        std::atomic<int> next{0}, done{0};
-        int users = 0;  // workers inside work(); guarded by mu_
-    };
-    static void work(Job &j) {
-        for (int i; (i = j.next.fetch_add(1)) < j.n;) {
-            (*j.fn)(i);
-            j.done.fetch_add(1);
-        }
-    }
-    HostPool() {
-        const unsigned hw = std::thread::hardware_concurrency();
-        nthreads_ = (int)std::min(15u, hw > 1 ? hw - 1 : 0u);
-        for (int t = 0; t < nthreads_; ++t) std::thread([this] { loop(); }).detach();
-    }
-    void loop() {
-        for (;;) {
-            Job *j = nullptr;
-            {
-                std::unique_lock<std::mutex> lk(mu_);
-                cv_.wait(lk, [&] { return !jobs_.empty(); });
-                j = jobs_.front();
-                if (j->next.load() >= j->n) {  // all calls handed out: move on
-                    jobs_.pop_front();
-                    continue;
-                }
-                ++j->users;
-            }
-            work(*j);
-            {
-                std::lock_guard<std::mutex> lk(mu_);
-                --j->users;
-                if (!jobs_.empty() && jobs_.front() == j && j->next.load() >= j->n) jobs_.pop_front();
-            }
-            done_cv_.notify_all();
-        }
-    }
-    std::mutex mu_;
-    std::condition_variable cv_, done_cv_;
-    std::deque<Job *> jobs_;
-    int nthreads_ = 0;
-};
 
 }  // namespace
 
@@ -753,7 +685,6 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
     for (int i = 0; ok && i < molints_ctx::kSide; ++i)
         ok = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&ctx->join[i], cudaEventDisableTiming) == cudaSuccess;
-    ok = ok && cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&ctx->scratch_ev, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         molints_destroy(ctx);
@@ -841,7 +772,6 @@ int molints_destroy(molints_ctx *ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
-    if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
     if (ctx->scratch_ev) cudaEventDestroy(ctx->scratch_ev);
     if (ctx->stage) cudaFreeHost(ctx->stage);
     delete ctx;
@@ -879,7 +809,15 @@ int molints_get_class_methods(const molints_ctx *ctx, int32_t *methods, int32_t 
 int molints_set_stream(molints_ctx *ctx, void *stream) {
     if (!ctx) return MOLINTS_ERR_INVALID;
     // NULL selects the context's own stream; the legacy default stream is cudaStreamLegacy.
-    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    cudaStream_t next = stream ? (cudaStream_t)stream : ctx->own_stream;
+    if (next != ctx->stream) {
+        // what the context left in flight on the old stream (a plan creation returns with its
+        // last kernels queued) comes before anything it launches on the new one
+        MI_CUDA(ctx, cudaSetDevice(ctx->device));
+        MI_CUDA(ctx, cudaEventRecord(ctx->fork, ctx->stream));
+        MI_CUDA(ctx, cudaStreamWaitEvent(next, ctx->fork, 0));
+    }
+    ctx->stream = next;
     return MOLINTS_OK;
 }
 
@@ -1026,11 +964,13 @@ static void shard_bounds(const molints_basis *b, int shard, int nshards, int *s_
     *hi = tri(tri(first_fn(*s_hi)));
 }
 
-// sync_end == false: return with the final uploads in flight on the context's stream (work
-// queued on that stream afterwards is ordered after them); molints_eri_packed uses it.
+// Plan creation synchronises the context's stream once, to read back the device build's
+// summary (work-queue sizes), and returns with the work-queue emission in flight on that
+// stream: work queued on it afterwards is ordered after it (molints_set_stream orders a new
+// stream after the old one).
 static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                             const molints_options *opts_in, int shard, int nshards,
-                            molints_plan **out, bool sync_end = true);
+                            molints_plan **out);
 
 int molints_plan_create_batch(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                               const molints_options *opts_in, molints_plan **out) {
@@ -1055,7 +995,7 @@ int molints_plan_create_shard(molints_ctx *ctx, const molints_basis *b, const mo
 
 static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis *bases,
                             const molints_options *opts_in, int shard, int nshards,
-                            molints_plan **out, bool sync_end) {
+                            molints_plan **out) {
     if (!ctx || !out || nmol < 0 || (nmol > 0 && !bases))
         return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: null argument");
     *out = nullptr;
@@ -1210,199 +1150,63 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     p->n_gq = (int64_t)gq_h.size();
     if (p->n_gq > 0) p->two_phase = 0;  // the gather would overwrite the generic kernel's entries
     const bool sharded = nshards > 1;
-    auto order = [sharded](const PairRec &x, const PairRec &y) {
-        if (x.cls != y.cls) return x.cls < y.cls;
-        if (x.mol != y.mol) return x.mol < y.mol;
-        if (sharded && x.ms != y.ms) return x.ms < y.ms;
-        return x.npp > y.npp;
-    };
-    std::stable_sort(pr.begin(), pr.end(), order);
+    {
+        // list order: class, molecule, (shard plans) highest shell, then primitive pairs
+        // descending; enumeration order among equals.  One stable radix pass per key byte.
+        int maxnpp = 0, maxms = 0;
+        for (const PairRec &r : pr) {
+            maxnpp = std::max(maxnpp, r.npp);
+            maxms = std::max(maxms, r.ms);
+        }
+        const int bn = bits_for((uint64_t)maxnpp), bs = sharded ? bits_for((uint64_t)maxms) : 0;
+        const int bm = bits_for((uint64_t)std::max(nmol - 1, 0)), bc = bits_for(kNumPairClasses - 1);
+        std::vector<uint64_t> key(pr.size());
+        for (size_t k = 0; k < pr.size(); ++k) {
+            const PairRec &r = pr[k];
+            key[k] = ((((uint64_t)r.cls << bm | (uint64_t)r.mol) << bs | (uint64_t)(sharded ? r.ms : 0)) << bn) |
+                     (uint64_t)(maxnpp - r.npp);
+        }
+        const std::vector<uint32_t> ord = radix_order(key, bc + bm + bs + bn);  // <= 4 + 31 + 31 + 16 bits
+        std::vector<PairRec> sorted(pr.size());
+        for (size_t k = 0; k < pr.size(); ++k) sorted[k] = pr[ord[k]];
+        pr.swap(sorted);
+    }
     const int npair = (int)pr.size();
     p->npair = npair;
 
-    std::vector<int2> ab_h(npair);
-    std::vector<int4> info_h(npair);
-    std::vector<int> src_h;
+    // ---- stage-1 pair tables (every primitive pair, list order) and the host-side structure
+    // of the list: class runs, and per (class, molecule) the molecule's run in the class (the
+    // pairs of a class are in molecule order)
     std::vector<int> cls_start(kNumPairClasses + 1, 0);
-    // kept primitive pairs of each pair, b_k and source in source order, flat: those of the
-    // pair at stage-1 position k are [kept_off[k], kept_off[k + 1])
-    std::vector<int64_t> kept_off;
-    std::vector<double> kept_b;
-    std::vector<int> kept_src;
-    std::vector<double> pbk_h;
-    auto fill_tables = [&](const std::vector<int> *stage1_pos) {
-        src_h.clear();
-        pbk_h.clear();
-        std::fill(cls_start.begin(), cls_start.end(), 0);
-        for (int k = 0; k < npair; ++k) {
-            ab_h[k] = make_int2(pr[k].a, pr[k].b);
-            const int off = (int)src_h.size();
-            if (stage1_pos) {
-                const int k1 = (*stage1_pos)[k];
-                for (int64_t x = kept_off[k1]; x < kept_off[k1 + 1]; ++x) {
-                    src_h.push_back(kept_src[x]);
-                    pbk_h.push_back(kept_b[x]);
-                }
-            } else {
-                for (int ia = 0; ia < K[pr[k].a]; ++ia)
-                    for (int ib = 0; ib < K[pr[k].b]; ++ib) src_h.push_back((ia << 8) | ib);
-            }
-            info_h[k] = make_int4(off, (int)src_h.size() - off, fn_off[pr[k].a], fn_off[pr[k].b]);
-            cls_start[pr[k].cls + 1] = k + 1;
-        }
-        for (int c = 1; c <= kNumPairClasses; ++c) cls_start[c] = std::max(cls_start[c], cls_start[c - 1]);
-    };
-    fill_tables(nullptr);
-    const int64_t nall = (int64_t)src_h.size();
+    int64_t nall = 0;
+    for (int k = 0; k < npair; ++k) nall += (int64_t)K[pr[k].a] * K[pr[k].b];
+    if (nall >= INT32_MAX) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: too many primitive pairs"); }
     p->nprim_pair_all = nall;
-
-    p->plan_ms[0] = ms_since(t_phase);
-    t_phase = clk::now();
-    cudaError_t e = cudaSetDevice(ctx->device);
-    if (e != cudaSuccess) { plan_free(p); return cuda_fail(ctx, e, "cudaSetDevice"); }
-    double2 *pbound = nullptr;
-    int64_t scratch = 0;
-    int rc = 0;
-    const int nc2 = kNumPairClasses * kNumPairClasses;
-    rc = rc ? rc : dev_alloc(ctx, &p->sh_xyz, (size_t)3 * ns, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->expn, (size_t)nprim, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->ncoef, (size_t)nprim, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->sh_poff, (size_t)ns, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->sh_L, (size_t)ns, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->sh_K, (size_t)ns, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->pair_ab, (size_t)npair, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->info, (size_t)npair, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->geo, (size_t)npair, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->bnd, (size_t)npair, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->pp_src, (size_t)nall, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)nall, &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &p->counters, (size_t)nc2 + 1, &p->bytes);  // + the gather's
-    rc = rc ? rc : dev_alloc(ctx, &p->mol_out, (size_t)std::max(nmol, 1), &p->bytes);
-    rc = rc ? rc : dev_alloc(ctx, &pbound, (size_t)nall, &scratch);
-    if (rc) {
-        if (pbound) { dev_free(ctx, pbound); ctx->held -= scratch; }
-        plan_free(p);
-        return rc;
-    }
-    cudaStream_t s = ctx->stream;
-    const double c0 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
-    std::vector<double2> pb_h(nall);
-    PairTab P{p->info, p->geo, p->pp, p->bnd};
-    BoysTab Bt = boys_of(ctx, opts.boys);
-    if ((e = cudaMemcpyAsync(p->sh_xyz, xyz.data(), 3 * (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->expn, expn.data(), (size_t)nprim * sizeof(double), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->ncoef, ncoef.data(), (size_t)nprim * sizeof(double), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->sh_poff, poff.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->sh_L, L.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->sh_K, K.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemsetAsync(p->counters + nc2, 0, sizeof(int), s)) ||
-        (e = cudaMemcpyAsync(p->pair_ab, ab_h.data(), npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->info, info_h.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->pp_src, src_h.data(), nall * sizeof(int), cudaMemcpyHostToDevice, s))) {
-        dev_free(ctx, pbound); ctx->held -= scratch; plan_free(p);
-        return cuda_fail(ctx, e, "plan_create upload");
-    }
-    // the raw coefficients become normalised ones in place; a shell with no positive
-    // self-overlap flags counters[nc2] (read back with the bounds)
-    if (ns > 0)
-        normalise_shells_kernel<<<(ns + 127) / 128, 128, 0, s>>>(ns, p->sh_L, p->sh_K, p->sh_poff, p->expn,
-                                                                 p->ncoef, p->counters + nc2);
-    int bad_shell = 0;
-    if (npair > 0) {
-        build_pairs_kernel<<<build_pairs_blocks(npair), 128, 0, s>>>(npair, p->pair_ab, p->info, p->pp_src,
-                                                               p->sh_xyz, p->sh_poff, p->expn,
-                                                               p->ncoef, c0, nullptr, p->pp, p->geo);
-        for (int c = 0; c < kNumPairClasses; ++c) {
-            const int n = cls_start[c + 1] - cls_start[c];
-            if (kSchwarzLaunchers[c]) kSchwarzLaunchers[c](P, Bt, cls_start[c], n, pbound, nullptr, 0, s);
-            else kRysBoundLaunchers[c](P, ctx->rys, cls_start[c], n, pbound, nullptr, 0, s);
-        }
-    }
-    if ((e = cudaGetLastError()) ||
-        (nall > 0 && (e = cudaMemcpyAsync(pb_h.data(), pbound, nall * sizeof(double2),
-                                          cudaMemcpyDeviceToHost, s))) ||
-        (e = cudaMemcpyAsync(&bad_shell, p->counters + nc2, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
-        (e = cudaStreamSynchronize(s))) {
-        dev_free(ctx, pbound); ctx->held -= scratch; plan_free(p);
-        return cuda_fail(ctx, e, "plan_create bound pass");
-    }
-    dev_free(ctx, pbound);
-    ctx->held -= scratch;
-    if (bad_shell) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: zero contracted function"); }
-
-    p->plan_ms[1] = ms_since(t_phase);
-    t_phase = clk::now();
-    // ---- stage 2: drop primitive pairs i with b_i * max Qabs (of the same molecule) below
-    // prim_cutoff -- each dropped term of any integral is below prim_cutoff by the Schwarz
-    // inequality -- and record each pair's bounds.
-    std::vector<double> qmax(std::max(nmol, 1), 0.0);
-    for (int k = 0; k < npair; ++k) {
-        double q = 0;
-        for (int x = 0; x < info_h[k].y; ++x) q += pb_h[info_h[k].x + x].x;
-        qmax[pr[k].mol] = std::max(qmax[pr[k].mol], q);
-    }
-    kept_off.assign(npair + 1, 0);
-    kept_b.resize(nall);
-    kept_src.resize(nall);
-    std::vector<double2> bnd1(npair);
-    int64_t nkept = 0;
-    for (int k = 0; k < npair; ++k) {
-        double qa = 0.0, wa = 0.0;
-        kept_off[k] = nkept;
-        for (int x = 0; x < info_h[k].y; ++x) {
-            const double2 bb = pb_h[info_h[k].x + x];
-            if (opts.prim_cutoff > 0.0 && bb.x * qmax[pr[k].mol] < opts.prim_cutoff) continue;
-            kept_b[nkept] = bb.x;
-            kept_src[nkept] = src_h[info_h[k].x + x];
-            ++nkept;
-            qa += bb.x;
-            wa += bb.y;
-        }
-        const double *A = &xyz[3 * pr[k].a], *Bc = &xyz[3 * pr[k].b];
-        const double dab = std::sqrt((A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
-                                     (A[2] - Bc[2]) * (A[2] - Bc[2]));
-        bnd1[k] = make_double2(qa, wa * std::pow(1.0 + dab, L[pr[k].b]));
-    }
-    kept_off[npair] = nkept;
-    p->nprim_pair_kept = nkept;
-    // re-sort by kept count, remembering each pair's stage-1 position
-    std::vector<int> pos1(npair);
-    for (int k = 0; k < npair; ++k) { pos1[k] = k; pr[k].npp = (int)(kept_off[k + 1] - kept_off[k]); }
-    std::vector<int> perm(npair);
-    for (int k = 0; k < npair; ++k) perm[k] = k;
-    std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return order(pr[x], pr[y]); });
-    {
-        std::vector<PairRec> pr2(npair);
-        for (int k = 0; k < npair; ++k) { pr2[k] = pr[perm[k]]; pos1[k] = perm[k]; }
-        pr.swap(pr2);
-    }
-    fill_tables(&pos1);
-    for (int c = 0; c <= kNumPairClasses; ++c) p->class_start[c] = cls_start[c];
-    p->pair_ref.resize(npair);
     p->pair_mol.resize(npair);
-    p->npp_h.resize(npair);
-    p->bnd_h.resize(npair);
     for (int k = 0; k < npair; ++k) {
-        p->pair_ref[k] = pr[k].ref;
         p->pair_mol[k] = pr[k].mol;
-        p->npp_h[k] = pr[k].npp;
-        p->bnd_h[k] = bnd1[pos1[k]];
+        cls_start[pr[k].cls + 1] = k + 1;
     }
-
-    // ---- work queues: per class pair, chunks of one bra pair and <= 32 ket pairs of the same
-    // molecule, ordered by decreasing estimated cost (kept primitive quartets x class weight)
+    for (int c = 1; c <= kNumPairClasses; ++c) cls_start[c] = std::max(cls_start[c], cls_start[c - 1]);
+    for (int c = 0; c <= kNumPairClasses; ++c) p->class_start[c] = cls_start[c];
+    const int cm_stride = nmol + 1;
+    std::vector<int> cm_start((size_t)kNumPairClasses * cm_stride);
+    for (int c = 0; c < kNumPairClasses; ++c) {
+        int k = cls_start[c];
+        for (int m = 0; m < nmol; ++m) {
+            cm_start[(size_t)c * cm_stride + m] = k;
+            while (k < cls_start[c + 1] && pr[k].mol == m) ++k;
+        }
+        cm_start[(size_t)c * cm_stride + nmol] = cls_start[c + 1];
+    }
     auto range_of = [&](int cls, int m, int &b0, int &b1) {
-        b0 = b1 = cls_start[cls];
-        // pairs of class cls are sorted by molecule: binary search the molecule's run
-        b0 = (int)(std::lower_bound(p->pair_mol.begin() + cls_start[cls], p->pair_mol.begin() + cls_start[cls + 1], m) -
-                   p->pair_mol.begin());
-        b1 = (int)(std::upper_bound(p->pair_mol.begin() + cls_start[cls], p->pair_mol.begin() + cls_start[cls + 1], m) -
-                   p->pair_mol.begin());
+        b0 = cm_start[(size_t)cls * cm_stride + m];
+        b1 = cm_start[(size_t)cls * cm_stride + m + 1];
     };
-    std::vector<int64_t> npp_prefix(npair + 1, 0);  // kept primitive pairs of pairs [0, k)
-    for (int k = 0; k < npair; ++k) npp_prefix[k + 1] = npp_prefix[k] + p->npp_h[k];
-    // chunk width: 32 ket pairs (one per lane), widened in steps of 32 for large batches so
-    // that the queues stay near kMaxChunks entries
+
+    // ---- work-queue shape per class pair: chunks of one bra pair and <= 32 ket pairs of the
+    // same molecule, widened in steps of 32 for large batches so that the queues stay near
+    // kMaxChunks entries
     constexpr double kMaxChunks = 4.0e6;
     double nchunk32 = 0.0;
     for (int x = 0; x < kNumPairClasses; ++x)
@@ -1431,27 +1235,47 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         }
         return std::max(1, std::min(8, (int)(nq / kRysMinChunks)));
     };
-    // Class pairs are independent, and so are the bra pairs of one class pair: the queues are
-    // built as tasks of consecutive bra pairs on the process's host worker threads.  Phase 1:
-    // each task's chunks, in (bra, ket) order, and its count per cost bucket.  Phase 2: every
-    // chunk goes straight to its place in the pinned upload buffer -- class pairs in order, in a
-    // class pair the heaviest bucket first, in a bucket the task and chunk order.
-    constexpr int kBuckets = 64;
-    // one cache-line-aligned record per task: the tasks run on different threads and each
-    // bumps its own vectors on every chunk (no line is shared between two tasks)
-    struct alignas(128) QueueTask {
-        int ci = 0, pb0 = 0, pb1 = 0;
-        std::vector<int4> raw;
-        std::vector<unsigned char> bk;
-        std::vector<long long> slot;  // two-phase: region slot of each chunk's first quartet
-        int64_t cnt[kBuckets] = {};
-        int64_t base[kBuckets] = {};
-        double total = 0.0;
-    };
-    std::vector<std::pair<int, int>> cps;
-    for (int x = 0; x < kNumPairClasses; ++x)
-        for (int y = 0; y <= x; ++y) cps.push_back({x, y});
-    // two-phase scratch: per (class pair, molecule) a region of quartet blocks in slot order,
+    QueueSetup S{};
+    {
+        int ci = 0, items = 0;
+        for (int x = 0; x < kNumPairClasses; ++x)
+            for (int y = 0; y <= x; ++y, ++ci) {
+                const bool hgp = p->method[x][y] != MOLINTS_METHOD_RYS;
+                const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
+                S.item_base[ci] = items;
+                S.cx[ci] = x;
+                S.cy[ci] = y;
+                S.hgp[ci] = hgp;
+                S.width[ci] = (hgp ? 32 : rys_width(x, y)) * widen;
+                S.pcost[ci] = (double)kEriPrimCost[x][y];
+                S.w[ci] = 1.0 + lsum * lsum;
+                items += cls_start[x + 1] - cls_start[x];
+            }
+        S.item_base[kNumClassPairs] = items;
+        for (int c = 0; c <= kNumPairClasses; ++c) S.cls_start[c] = cls_start[c];
+        S.nmol = nmol;
+        S.widen = widen;
+        S.lane_cost = ctx->lane_cost;
+        S.sharded = sharded;
+        S.shard_s0 = shard_s0;
+        S.shard_s1 = shard_s1;
+        for (int c = 0; c < kNumPairClasses; ++c) {
+            // shard plans (one molecule): a class's pairs are in highest-shell order
+            auto first_ms_at_least = [&](int v) {
+                return (int)(std::partition_point(pr.begin() + cls_start[c], pr.begin() + cls_start[c + 1],
+                                                  [v](const PairRec &r) { return r.ms < v; }) -
+                             pr.begin());
+            };
+            S.ps0[c] = sharded ? first_ms_at_least(shard_s0) : 0;
+            S.ps1[c] = sharded ? first_ms_at_least(shard_s1) : 0;
+        }
+    }
+    const int n_items = S.item_base[kNumClassPairs];
+
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) { plan_free(p); return cuda_fail(ctx, e, "cudaSetDevice"); }
+
+    // ---- two-phase scratch: per (class pair, molecule) a region of quartet blocks in slot order,
     // bra-major (the triangle q <= p for equal classes); region_h[((x nc + y) nmol + m) 4 ..] =
     // {offset in doubles, first bra pair, first ket pair, ket pairs}.  Quartet slot t's block
     // starts at offset + t * block.
@@ -1463,20 +1287,20 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     int64_t scratch_len = 0;
     if (p->two_phase) {
         region_h.assign((size_t)kNumPairClasses * kNumPairClasses * nmol * kRegionFields, 0);
-        for (const auto &cp : cps)
-            for (int m = 0; m < nmol; ++m) {
-                const int x = cp.first, y = cp.second;
-                int b0, b1, k0, k1;
-                range_of(x, m, b0, b1);
-                range_of(y, m, k0, k1);
-                const int64_t nb = b1 - b0, nk = k1 - k0;
-                long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * kRegionFields];
-                rg[0] = scratch_len;
-                rg[1] = b0;
-                rg[2] = k0;
-                rg[3] = nk;
-                scratch_len += (x == y ? nb * (nb + 1) / 2 : nb * nk) * ncomp_of(x, y);
-            }
+        for (int x = 0; x < kNumPairClasses; ++x)
+            for (int y = 0; y <= x; ++y)
+                for (int m = 0; m < nmol; ++m) {
+                    int b0, b1, k0, k1;
+                    range_of(x, m, b0, b1);
+                    range_of(y, m, k0, k1);
+                    const int64_t nb = b1 - b0, nk = k1 - k0;
+                    long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * kRegionFields];
+                    rg[0] = scratch_len;
+                    rg[1] = b0;
+                    rg[2] = k0;
+                    rg[3] = nk;
+                    scratch_len += (x == y ? nb * (nb + 1) / 2 : nb * nk) * ncomp_of(x, y);
+                }
         // The scratch (about npacked doubles) is taken now.  If it does not fit the budget or
         // the device, AUTO falls back to the direct stores, which need no scratch; only an
         // explicit MOLINTS_OUTPUT_TWO_PHASE fails.
@@ -1493,188 +1317,102 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         }
         p->scratch_need = scratch_len;
     }
-    std::vector<QueueTask> tasks;
-    std::vector<int> task_end(cps.size(), 0), cp_width(cps.size(), 32 * widen);
-    for (size_t ci = 0; ci < cps.size(); ++ci)
-        if (p->method[cps[ci].first][cps[ci].second] == MOLINTS_METHOD_RYS)
-            cp_width[ci] = rys_width(cps[ci].first, cps[ci].second) * widen;
-    for (size_t ci = 0; ci < cps.size(); ++ci) {
-        const int x = cps[ci].first, y = cps[ci].second;
-        const int b0 = cls_start[x], b1 = cls_start[x + 1];
-        const double nb = b1 - b0, nk = cls_start[y + 1] - cls_start[y];
-        // about kTaskChunks 32-ket chunks per task
-        constexpr double kTaskChunks = 1024.0;
-        const double est = (x == y ? nb * nb / 2.0 : nb * nk) / std::max(nmol, 1) / 32.0;
-        const int nt = b1 > b0 ? (int)std::max(1.0, std::min(std::min(nb, 256.0), std::ceil(est / kTaskChunks))) : 0;
-        for (int t = 0; t < nt; ++t) {
-            QueueTask T;
-            T.ci = (int)ci;
-            T.pb0 = b0 + (int)((int64_t)(b1 - b0) * t / nt);
-            T.pb1 = b0 + (int)((int64_t)(b1 - b0) * (t + 1) / nt);
-            const size_t guess = (size_t)(1.25 * est / nt) + 64;
-            T.raw.reserve(guess);
-            T.bk.reserve(guess);
-            if (p->two_phase) T.slot.reserve(guess);
-            tasks.push_back(std::move(T));
-        }
-        task_end[ci] = (int)tasks.size();
-    }
-    // heaviest first, bucketed by the binary exponent of the cost: an O(n) order that is all
-    // the load balance needs (a full sort of millions of chunks dominated batches)
-    auto bucket = [](double c) {
-        uint64_t bits;
-        std::memcpy(&bits, &c, sizeof bits);
-        const int e2 = c > 0.0 ? (int)((bits >> 52) & 0x7ff) - 1022 : 1;
-        return std::max(0, std::min(kBuckets - 1, kBuckets - 1 - (e2 + 8)));
-    };
-    auto build_task = [&](QueueTask &T) {
-        const int x = cps[T.ci].first, y = cps[T.ci].second;
-        const bool hgp = p->method[x][y] != MOLINTS_METHOD_RYS;
-        const int width = cp_width[T.ci];
-        const double pcost = kEriPrimCost[x][y];
-        const int lsum = kPairClassLa[x] + kPairClassLb[x] + kPairClassLa[y] + kPairClassLb[y];
-        const double w = 1.0 + lsum * lsum;
-        int mcur = -1, k0 = 0, k1 = 0;
-        double total = 0.0;            // accumulated here, stored once at the end
-        int64_t cnt[kBuckets] = {};
-        for (int pb = T.pb0; pb < T.pb1; ++pb) {
-            const int m = p->pair_mol[pb];
-            if (m != mcur) {
-                range_of(y, m, k0, k1);
-                mcur = m;
-            }
-            int kbeg = k0, kend = (x == y) ? pb + 1 : k1;
-            if (sharded) {
-                // quartet owner: the higher of the two pairs' max shells
-                const int mp = pr[pb].ms;
-                auto first_ms_at_least = [&](int v) {
-                    return (int)(std::partition_point(pr.begin() + k0, pr.begin() + k1,
-                                                      [v](const PairRec &r) { return r.ms < v; }) -
-                                 pr.begin());
-                };
-                if (mp >= shard_s1) continue;
-                if (x == y) {
-                    if (mp < shard_s0) continue;  // q <= pb in list order: owner is mp
-                } else if (mp >= shard_s0) {
-                    kend = first_ms_at_least(shard_s1);
-                } else {
-                    kbeg = first_ms_at_least(shard_s0);
-                    kend = first_ms_at_least(shard_s1);
-                }
-            }
-            const double wp = w * p->npp_h[pb];
-            bool heavy = hgp;  // this bra's remaining kets may still need a split
-            for (int q0 = kbeg; q0 < kend;) {
-                int n = std::min(width, kend - q0), lg = 0;
-                if (heavy) {
-                    // the kets of a molecule's class run are in descending primitive-pair
-                    // count, so the split only falls along the run: a chunk that starts
-                    // unsplit stays unsplit, and a split chunk ends where the split changes
-                    // (shard plans order by highest shell first; there a heavy ket inside
-                    // an unsplit chunk only runs unsplit)
-                    lg = hgp_split(p->npp_h[pb], p->npp_h[q0], pcost);
-                    n = std::min((32 >> (lg & 7)) * widen, kend - q0);
-                    if (lg)
-                        for (int k = 1; k < n; ++k)
-                            if (hgp_split(p->npp_h[pb], p->npp_h[q0 + k], pcost) != lg) { n = k; break; }
-                    heavy = lg != 0 || sharded;
-                }
-                const double cost = wp * (double)(npp_prefix[q0 + n] - npp_prefix[q0]);
-                total += cost;
-                const int b = bucket(cost);
-                T.raw.push_back(make_int4(pb, q0, n | (lg << 16), m));
-                T.bk.push_back((unsigned char)b);
-                if (p->two_phase) {
-                    const long long *rg = &region_h[(((size_t)x * kNumPairClasses + y) * nmol + m) * kRegionFields];
-                    const long long db = pb - rg[1], dk = q0 - rg[2];
-                    T.slot.push_back(x == y ? db * (db + 1) / 2 + dk : db * rg[3] + dk);
-                }
-                ++cnt[b];
-                q0 += n;
-            }
-        }
-        T.total = total;
-        std::memcpy(T.cnt, cnt, sizeof cnt);
-    };
-    HostPool &hp = HostPool::instance();
-    hp.run((int)tasks.size(), [&](int t) { build_task(tasks[t]); });
-    int64_t nq = 0;
-    for (size_t ci = 0, t0 = 0; ci < cps.size(); t0 = task_end[ci], ++ci) {
-        const int x = cps[ci].first, y = cps[ci].second;
-        p->q_off[x][y] = (int)nq;
-        double total = 0.0;
-        for (int b = 0; b < kBuckets; ++b)
-            for (size_t t = t0; t < (size_t)task_end[ci]; ++t) {
-                tasks[t].base[b] = nq;
-                nq += tasks[t].cnt[b];
-            }
-        for (size_t t = t0; t < (size_t)task_end[ci]; ++t) total += tasks[t].total;
-        p->q_len[x][y] = (int)(nq - p->q_off[x][y]);
-        p->class_cost[x][y] = total;
-    }
-    if (nq > INT32_MAX) { plan_free(p); return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: work queue too long"); }
-    // pinned upload buffer: chunks, then the final pair tables
-    auto al16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
-    const size_t o_info = al16((size_t)nq * sizeof(int4));
-    const size_t o_bnd = o_info + al16((size_t)npair * sizeof(int4));
-    const size_t o_ab = o_bnd + al16((size_t)npair * sizeof(double2));
-    const size_t o_src = o_ab + al16((size_t)npair * sizeof(int2));
-    const size_t o_pbk = o_src + al16((size_t)nkept * sizeof(int));
-    const size_t o_mol = o_pbk + al16((size_t)nkept * sizeof(double));
-    // two-phase: chunk slots and the gather tables (functions, shell pairs, regions, molecules)
-    int64_t nfn_all = 0, npe_all = 0;
+    const bool tp = p->two_phase != 0;
+    S.two_phase = tp;
+
+    // ---- pinned upload buffer: the summary read back after the device build, the plan's
+    // shells, the stage-1 block (laid out as in the device temporaries, one copy), the molecule
+    // offsets and the gather tables
+    int64_t nfn_all = 0, npe_all = 0, nrows_all = 0;
     for (int m = 0; m < nmol; ++m) {
         nfn_all += mol_nbf[m];
         npe_all += (int64_t)bases[m].nshell * (bases[m].nshell + 1) / 2;
+        nrows_all += mol_nbf[m] * (mol_nbf[m] + 1) / 2;
     }
-    const bool tp = p->two_phase != 0;
-    const size_t o_slot = o_mol + al16((size_t)std::max(nmol, 1) * sizeof(long long));
-    const size_t o_gfn = o_slot + (tp ? al16((size_t)nq * sizeof(long long)) : 0);
-    const size_t o_gpair = o_gfn + (tp ? al16((size_t)nfn_all * sizeof(int2)) : 0);
-    const size_t o_greg = o_gpair + (tp ? al16((size_t)npe_all * sizeof(int)) : 0);
-    const size_t o_gmol = o_greg + (tp ? al16(region_h.size() * sizeof(long long)) : 0);
-    int64_t nrows_all = 0;
-    for (int m = 0; m < nmol; ++m) nrows_all += mol_nbf[m] * (mol_nbf[m] + 1) / 2;
-    const size_t o_grows = o_gmol + (tp ? al16((size_t)nmol * 4 * sizeof(long long)) : 0);
-    const size_t o_gunits = o_grows + (tp ? al16((size_t)nrows_all * sizeof(int2)) : 0);
-    const size_t stage_bytes = o_gunits + (tp ? al16((size_t)npe_all * sizeof(int4)) : 0);
-    if ((rc = ctx_stage(ctx, stage_bytes))) { plan_free(p); return rc; }
+    // device temporaries of the build; the stage-1 block comes first
+    Carve tv;
+    const size_t t_ab1 = tv.take<int2>(npair), t_info1 = tv.take<int4>(npair), t_rec1 = tv.take<int4>(npair);
+    const size_t t_seg1 = tv.take<int>(npair), t_mol1 = tv.take<int>(npair);
+    const size_t t_cm = tv.take<int>(cm_start.size()), t_src1 = tv.take<int>(nall);
+    const size_t up_bytes = tv.at;
+    const size_t t_pbound = tv.take<double2>(nall), t_qmax = tv.take<unsigned long long>(nmol);
+    const size_t t_npp1 = tv.take<int>(npair), t_bnd1 = tv.take<double2>(npair);
+    const size_t t_key1 = tv.take<unsigned long long>(npair), t_key2 = tv.take<unsigned long long>(npair);
+    const size_t t_idx1 = tv.take<int>(npair), t_idx2 = tv.take<int>(npair);
+    const size_t t_prefix = tv.take<long long>((size_t)npair + 1), t_npp = tv.take<int>((size_t)npair + 1);
+    const size_t t_ms = tv.take<int>(npair);
+    const size_t t_cnt = tv.take<long long>((size_t)n_items + 1), t_cost = tv.take<double>(n_items);
+    const size_t t_off = tv.take<long long>((size_t)n_items + 1);
+    const size_t t_sum = tv.take<long long>(kNumClassPairs + 1), t_ccost = tv.take<double>(kNumClassPairs);
+    const size_t cub_bytes = std::max(plan_build_temp_bytes(npair), queue_count_temp_bytes(n_items));
+    const size_t t_cub = tv.take<char>(cub_bytes);
+    Carve sv;
+    // read back: class-pair chunk offsets, class-pair costs, kept primitive pairs, bad-shell flag
+    const size_t o_sum = sv.take<long long>(kNumClassPairs + 1), o_ccost = sv.take<double>(kNumClassPairs);
+    const size_t o_nkept = sv.take<long long>(1), o_bad = sv.take<int>(1);
+    const size_t o_up = sv.take<char>(up_bytes);
+    const size_t o_xyz = sv.take<double>(3 * (size_t)ns), o_expn = sv.take<double>(nprim);
+    const size_t o_coef = sv.take<double>(nprim), o_poff = sv.take<int>(ns), o_L = sv.take<int>(ns);
+    const size_t o_K = sv.take<int>(ns), o_mol = sv.take<long long>(nmol);
+    const size_t o_greg = sv.take<long long>(tp ? region_h.size() : 0), o_gfn = sv.take<int2>(tp ? nfn_all : 0);
+    const size_t o_gmol = sv.take<long long>(tp ? (size_t)nmol * 4 : 0), o_grows = sv.take<int2>(tp ? nrows_all : 0);
+    const size_t o_gunits = sv.take<int4>(tp ? npe_all : 0);
+    int rc = ctx_stage(ctx, sv.at);
+    if (rc) { plan_free(p); return rc; }
     char *stage = ctx->stage;
-    int4 *chunks = reinterpret_cast<int4 *>(stage);
-    long long *slots = tp ? reinterpret_cast<long long *>(stage + o_slot) : nullptr;
-    hp.run((int)tasks.size(), [&](int t) {
-        QueueTask &T = tasks[t];
-        for (size_t i = 0; i < T.raw.size(); ++i) {
-            const int64_t d = T.base[T.bk[i]]++;
-            chunks[d] = T.raw[i];
-            if (slots) slots[d] = T.slot[i];
+    {
+        char *up = stage + o_up;
+        int2 *ab1 = reinterpret_cast<int2 *>(up + t_ab1);
+        int4 *info1 = reinterpret_cast<int4 *>(up + t_info1), *rec1 = reinterpret_cast<int4 *>(up + t_rec1);
+        int *seg1 = reinterpret_cast<int *>(up + t_seg1), *mol1 = reinterpret_cast<int *>(up + t_mol1);
+        int *src1 = reinterpret_cast<int *>(up + t_src1);
+        int off = 0;
+        for (int k = 0; k < npair; ++k) {
+            const PairRec &r = pr[k];
+            const int m = r.mol;
+            ab1[k] = make_int2(r.a, r.b);
+            const int Ka = K[r.a], Kb = K[r.b];
+            info1[k] = make_int4(off, Ka * Kb, fn_off[r.a], fn_off[r.b]);
+            for (int ia = 0; ia < Ka; ++ia)
+                for (int ib = 0; ib < Kb; ++ib) src1[off++] = (ia << 8) | ib;
+            const int swapped = (r.a - shell_off[m]) != r.ms;  // A is the lower shell J
+            rec1[k] = make_int4(m, r.ref, r.cls | (swapped << 8), r.ms);
+            // the pair's run of equal (class, molecule[, ms]): the re-sort by kept count stays in it
+            const bool same = k > 0 && pr[k - 1].cls == r.cls && pr[k - 1].mol == m && (!sharded || pr[k - 1].ms == r.ms);
+            seg1[k] = same ? seg1[k - 1] : k;
+            mol1[k] = m;
         }
-    });
+        std::memcpy(up + t_cm, cm_start.data(), cm_start.size() * sizeof(int));
+    }
+    std::memcpy(stage + o_xyz, xyz.data(), 3 * (size_t)ns * sizeof(double));
+    std::memcpy(stage + o_expn, expn.data(), (size_t)nprim * sizeof(double));
+    std::memcpy(stage + o_coef, ncoef.data(), (size_t)nprim * sizeof(double));
+    std::memcpy(stage + o_poff, poff.data(), (size_t)ns * sizeof(int));
+    std::memcpy(stage + o_L, L.data(), (size_t)ns * sizeof(int));
+    std::memcpy(stage + o_K, K.data(), (size_t)ns * sizeof(int));
+    {
+        long long *mol_out_ll = reinterpret_cast<long long *>(stage + o_mol);
+        mol_out_ll[0] = 0;
+        for (int m = 0; m < nmol; ++m) mol_out_ll[m] = (long long)p->mol_out_h[m];
+    }
     if (tp) {
+        std::memcpy(stage + o_greg, region_h.data(), region_h.size() * sizeof(long long));
         int2 *gfn = reinterpret_cast<int2 *>(stage + o_gfn);
-        int *gpair = reinterpret_cast<int *>(stage + o_gpair);
         long long *gmol = reinterpret_cast<long long *>(stage + o_gmol);
-        long long cbase = 0;
-        std::vector<int64_t> pbase(nmol + 1, 0);
+        long long cbase = 0, pbase = 0;
         for (int m = 0, fb = 0; m < nmol; ++m) {
-            pbase[m + 1] = pbase[m] + (int64_t)bases[m].nshell * (bases[m].nshell + 1) / 2;
             for (int sl = 0; sl < bases[m].nshell; ++sl) {
                 const int g = shell_off[m] + sl;
                 for (int c = 0; c < ncart(L[g]); ++c) gfn[fb + fn_off[g] + c] = make_int2(sl, c);
             }
             gmol[4 * m] = fb;
-            gmol[4 * m + 1] = pbase[m];
+            gmol[4 * m + 1] = pbase;
             gmol[4 * m + 2] = (long long)p->mol_out_h[m];
             gmol[4 * m + 3] = cbase;
+            pbase += (int64_t)bases[m].nshell * (bases[m].nshell + 1) / 2;
             cbase += mol_nbf[m] * (mol_nbf[m] + 1) / 2;
             fb += (int)mol_nbf[m];
         }
-        for (int k = 0; k < npair; ++k) {
-            const int m = pr[k].mol;
-            const int swapped = (pr[k].a - shell_off[m]) != pr[k].ms;  // A is the lower shell J
-            gpair[pbase[m] + pr[k].ref] = (k << 5) | (pr[k].cls << 1) | swapped;
-        }
-        std::memcpy(stage + o_greg, region_h.data(), region_h.size() * sizeof(long long));
         // gather order: per molecule, shell pairs from the last, each pair's rows together
         int2 *grows = reinterpret_cast<int2 *>(stage + o_grows);
         int64_t nr = 0;
@@ -1707,73 +1445,220 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                     wk.push_back({rows * (double)(li * (li + 1) / 2 + lj + 1), (int64_t)u_h.size()});
                     u_h.push_back(make_int4(m, fn_off[gI], fn_off[gJ], nI | (nJ << 8) | ((I == J) << 16)));
                 }
-        std::sort(wk.begin(), wk.end(), [](const std::pair<double, int64_t> &a, const std::pair<double, int64_t> &b) {
-            return a.first > b.first || (a.first == b.first && a.second < b.second);
-        });
-        for (size_t k = 0; k < wk.size(); ++k) gu[k] = u_h[wk[k].second];
+        // by weight descending at float precision (24 bits: exponent and 15 mantissa bits), list
+        // order among equals
+        std::vector<uint64_t> wkey(wk.size());
+        for (size_t k = 0; k < wk.size(); ++k) {
+            const float f = (float)wk[k].first;
+            uint32_t fb;
+            std::memcpy(&fb, &f, sizeof fb);
+            wkey[k] = (uint64_t)((1u << 24) - 1 - (fb >> 7));
+        }
+        const std::vector<uint32_t> word = radix_order(wkey, 24);
+        for (size_t k = 0; k < wk.size(); ++k) gu[k] = u_h[wk[word[k]].second];
         p->n_units = (int64_t)wk.size();
     }
-    std::memcpy(stage + o_info, info_h.data(), npair * sizeof(int4));
-    std::memcpy(stage + o_bnd, p->bnd_h.data(), npair * sizeof(double2));
-    std::memcpy(stage + o_ab, ab_h.data(), npair * sizeof(int2));
-    if (nkept > 0) {
-        std::memcpy(stage + o_src, src_h.data(), nkept * sizeof(int));
-        std::memcpy(stage + o_pbk, pbk_h.data(), nkept * sizeof(double));
-    }
-    long long *mol_out_ll = reinterpret_cast<long long *>(stage + o_mol);
-    mol_out_ll[0] = 0;
-    for (int m = 0; m < nmol; ++m) mol_out_ll[m] = (long long)p->mol_out_h[m];
-    p->plan_ms[2] = ms_since(t_phase);
+    p->plan_ms[0] = ms_since(t_phase);
     t_phase = clk::now();
-    rc = dev_alloc(ctx, &p->chunks, (size_t)nq, &p->bytes);
-    if (!rc) rc = dev_alloc(ctx, &p->pbk, (size_t)std::max<int64_t>(nkept, 1), &p->bytes);
-    if (!rc && tp) {
-        rc = dev_alloc(ctx, &p->chunk_slot, (size_t)std::max<int64_t>(nq, 1), &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->g_fn, (size_t)std::max<int64_t>(nfn_all, 1), &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->g_pair, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->g_rows, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->g_col, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
-        if (!rc) rc = dev_alloc(ctx, &p->g_units, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
+
+    // ---- device: plan buffers, uploads, normalisation, bound pass, then the device build
+    const int nc2 = kNumPairClasses * kNumPairClasses;
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_xyz, (size_t)3 * ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->expn, (size_t)nprim, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->ncoef, (size_t)nprim, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_poff, (size_t)ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_L, (size_t)ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->sh_K, (size_t)ns, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->pair_ab, (size_t)npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->info, (size_t)npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->geo, (size_t)npair, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->bnd, (size_t)npair, &p->bytes);
+    // kept primitive pairs: at most nall (the count is known on the device only)
+    rc = rc ? rc : dev_alloc(ctx, &p->pp_src, (size_t)nall, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->pbk, (size_t)nall, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->pp, (size_t)nall, &p->bytes);
+    rc = rc ? rc : dev_alloc(ctx, &p->counters, (size_t)nc2 + 1, &p->bytes);  // + the gather's
+    rc = rc ? rc : dev_alloc(ctx, &p->mol_out, (size_t)std::max(nmol, 1), &p->bytes);
+    if (tp) {
+        rc = rc ? rc : dev_alloc(ctx, &p->g_fn, (size_t)std::max<int64_t>(nfn_all, 1), &p->bytes);
+        rc = rc ? rc : dev_alloc(ctx, &p->g_pair, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
+        rc = rc ? rc : dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
+        rc = rc ? rc : dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
+        rc = rc ? rc : dev_alloc(ctx, &p->g_rows, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
+        rc = rc ? rc : dev_alloc(ctx, &p->g_col, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
+        rc = rc ? rc : dev_alloc(ctx, &p->g_units, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
     }
-    if (rc) { plan_free(p); return rc; }
-    if (tp && ((nq > 0 && (e = cudaMemcpyAsync(p->chunk_slot, stage + o_slot, (size_t)nq * sizeof(long long),
-                                                cudaMemcpyHostToDevice, s))) ||
-               (nfn_all > 0 && (e = cudaMemcpyAsync(p->g_fn, stage + o_gfn, (size_t)nfn_all * sizeof(int2),
-                                                     cudaMemcpyHostToDevice, s))) ||
-               (npe_all > 0 && (e = cudaMemcpyAsync(p->g_pair, stage + o_gpair, (size_t)npe_all * sizeof(int),
-                                                     cudaMemcpyHostToDevice, s))) ||
-               (e = cudaMemcpyAsync(p->g_region, stage + o_greg, region_h.size() * sizeof(long long),
-                                    cudaMemcpyHostToDevice, s)) ||
-               (e = cudaMemcpyAsync(p->g_mol, stage + o_gmol, (size_t)nmol * 4 * sizeof(long long),
-                                    cudaMemcpyHostToDevice, s)) ||
-               (npe_all > 0 && (e = cudaMemcpyAsync(p->g_units, stage + o_gunits, (size_t)npe_all * sizeof(int4),
-                                                     cudaMemcpyHostToDevice, s))) ||
-               (nrows_all > 0 && (e = cudaMemcpyAsync(p->g_rows, stage + o_grows, (size_t)nrows_all * sizeof(int2),
-                                                       cudaMemcpyHostToDevice, s))))) {
-        plan_free(p);
+    int64_t temp_tally = 0;
+    char *tmp = nullptr;
+    rc = rc ? rc : dev_alloc(ctx, &tmp, tv.at, &temp_tally);
+    auto release_temp = [&]() {
+        if (tmp) dev_free(ctx, tmp);
+        ctx->held -= temp_tally;
+        tmp = nullptr;
+        temp_tally = 0;
+    };
+    if (rc) { release_temp(); plan_free(p); return rc; }
+    cudaStream_t s = ctx->stream;
+    auto h2d = [&](void *dst, size_t off, size_t bytes) {
+        return bytes ? cudaMemcpyAsync(dst, stage + off, bytes, cudaMemcpyHostToDevice, s) : cudaSuccess;
+    };
+    if ((e = h2d(tmp, o_up, up_bytes)) ||
+        (e = h2d(p->sh_xyz, o_xyz, 3 * (size_t)ns * sizeof(double))) ||
+        (e = h2d(p->expn, o_expn, (size_t)nprim * sizeof(double))) ||
+        (e = h2d(p->ncoef, o_coef, (size_t)nprim * sizeof(double))) ||
+        (e = h2d(p->sh_poff, o_poff, (size_t)ns * sizeof(int))) ||
+        (e = h2d(p->sh_L, o_L, (size_t)ns * sizeof(int))) ||
+        (e = h2d(p->sh_K, o_K, (size_t)ns * sizeof(int))) ||
+        (e = h2d(p->mol_out, o_mol, (size_t)nmol * sizeof(long long))) ||
+        (tp && ((e = h2d(p->g_region, o_greg, region_h.size() * sizeof(long long))) ||
+                (e = h2d(p->g_fn, o_gfn, (size_t)nfn_all * sizeof(int2))) ||
+                (e = h2d(p->g_mol, o_gmol, (size_t)nmol * 4 * sizeof(long long))) ||
+                (e = h2d(p->g_rows, o_grows, (size_t)nrows_all * sizeof(int2))) ||
+                (e = h2d(p->g_units, o_gunits, (size_t)npe_all * sizeof(int4))))) ||
+        (e = cudaMemsetAsync(p->counters + nc2, 0, sizeof(int), s)) ||
+        (e = cudaMemsetAsync(tmp + t_qmax, 0, (size_t)std::max(nmol, 1) * sizeof(unsigned long long), s)) ||
+        (e = cudaMemsetAsync(tmp + t_sum, 0, (kNumClassPairs + 1) * sizeof(long long), s)) ||
+        (e = cudaMemsetAsync(tmp + t_ccost, 0, kNumClassPairs * sizeof(double), s)) ||
+        (e = cudaMemsetAsync(tmp + t_prefix, 0, sizeof(long long), s))) {
+        release_temp(); plan_free(p);
         return cuda_fail(ctx, e, "plan_create upload");
+    }
+    // the raw coefficients become normalised ones in place; a shell with no positive
+    // self-overlap flags counters[nc2] (read back with the summary)
+    if (ns > 0)
+        normalise_shells_kernel<<<(ns + 127) / 128, 128, 0, s>>>(ns, p->sh_L, p->sh_K, p->sh_poff, p->expn,
+                                                                 p->ncoef, p->counters + nc2);
+    PlanBuildArgs A{};
+    A.npair = npair;
+    A.nall = (int)nall;
+    A.prim_cutoff = opts.prim_cutoff;
+    A.ab1 = reinterpret_cast<const int2 *>(tmp + t_ab1);
+    A.info1 = reinterpret_cast<const int4 *>(tmp + t_info1);
+    A.src1 = reinterpret_cast<const int *>(tmp + t_src1);
+    A.rec1 = reinterpret_cast<const int4 *>(tmp + t_rec1);
+    A.seg1 = reinterpret_cast<const int *>(tmp + t_seg1);
+    A.pbound = reinterpret_cast<const double2 *>(tmp + t_pbound);
+    A.xyz = p->sh_xyz;
+    A.sh_L = p->sh_L;
+    A.qmax = reinterpret_cast<unsigned long long *>(tmp + t_qmax);
+    A.npp1 = reinterpret_cast<int *>(tmp + t_npp1);
+    A.bnd1 = reinterpret_cast<double2 *>(tmp + t_bnd1);
+    A.key1 = reinterpret_cast<unsigned long long *>(tmp + t_key1);
+    A.key2 = reinterpret_cast<unsigned long long *>(tmp + t_key2);
+    A.idx1 = reinterpret_cast<int *>(tmp + t_idx1);
+    A.idx2 = reinterpret_cast<int *>(tmp + t_idx2);
+    A.npp_prefix = reinterpret_cast<long long *>(tmp + t_prefix);
+    A.npp = reinterpret_cast<int *>(tmp + t_npp);
+    A.ms = reinterpret_cast<int *>(tmp + t_ms);
+    A.pair_ab = p->pair_ab;
+    A.info = p->info;
+    A.bnd = p->bnd;
+    A.pp_src = p->pp_src;
+    A.pbk = p->pbk;
+    A.g_pair = tp ? p->g_pair : nullptr;
+    A.g_mol = tp ? p->g_mol : nullptr;
+    QueueArgs QA{};
+    QA.n_items = n_items;
+    QA.npp = A.npp;
+    QA.mol = reinterpret_cast<const int *>(tmp + t_mol1);
+    QA.cm_start = reinterpret_cast<const int *>(tmp + t_cm);
+    QA.ms = A.ms;
+    QA.npp_prefix = A.npp_prefix;
+    QA.region = tp ? p->g_region : nullptr;
+    QA.cnt = reinterpret_cast<long long *>(tmp + t_cnt);
+    QA.cost = reinterpret_cast<double *>(tmp + t_cost);
+    QA.off = reinterpret_cast<long long *>(tmp + t_off);
+    QA.summary = reinterpret_cast<long long *>(tmp + t_sum);
+    QA.class_cost = reinterpret_cast<double *>(tmp + t_ccost);
+    if (npair > 0) {
+        const double c0 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
+        build_pairs_kernel<<<build_pairs_blocks(npair), 128, 0, s>>>(npair, A.ab1, A.info1, A.src1, p->sh_xyz,
+                                                                     p->sh_poff, p->expn, p->ncoef, c0, nullptr,
+                                                                     p->pp, p->geo);
+        PairTab P1{A.info1, p->geo, p->pp, p->bnd};
+        BoysTab Bt = boys_of(ctx, opts.boys);
+        double2 *pbound = reinterpret_cast<double2 *>(tmp + t_pbound);
+        for (int c = 0; c < kNumPairClasses; ++c) {
+            const int n = cls_start[c + 1] - cls_start[c];
+            if (kSchwarzLaunchers[c]) kSchwarzLaunchers[c](P1, Bt, cls_start[c], n, pbound, nullptr, 0, s);
+            else kRysBoundLaunchers[c](P1, ctx->rys, cls_start[c], n, pbound, nullptr, 0, s);
+        }
+        if ((e = cudaGetLastError()) || (e = plan_build_pairs(A, tmp + t_cub, cub_bytes, s)) ||
+            (e = queue_count(S, QA, tmp + t_cub, cub_bytes, s))) {
+            release_temp(); plan_free(p);
+            return cuda_fail(ctx, e, "plan_create device build");
+        }
+    }
+    if ((e = cudaGetLastError()) ||
+        (e = cudaMemcpyAsync(stage + o_sum, tmp + t_sum, (kNumClassPairs + 1) * sizeof(long long),
+                             cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(stage + o_ccost, tmp + t_ccost, kNumClassPairs * sizeof(double),
+                             cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(stage + o_nkept, A.npp_prefix + npair, sizeof(long long), cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(stage + o_bad, p->counters + nc2, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaStreamSynchronize(s))) {
+        release_temp(); plan_free(p);
+        return cuda_fail(ctx, e, "plan_create bound pass");
+    }
+    if (*reinterpret_cast<const int *>(stage + o_bad)) {
+        release_temp(); plan_free(p);
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: zero contracted function");
+    }
+    const long long *qsum = reinterpret_cast<const long long *>(stage + o_sum);
+    const double *qcost = reinterpret_cast<const double *>(stage + o_ccost);
+    p->nprim_pair_kept = *reinterpret_cast<const long long *>(stage + o_nkept);
+    const long long nq = qsum[kNumClassPairs];
+    if (nq > INT32_MAX) {
+        release_temp(); plan_free(p);
+        return fail(ctx, MOLINTS_ERR_INVALID, "plan_create: work queue too long");
+    }
+    for (int ci = 0; ci < kNumClassPairs; ++ci) {
+        const int x = S.cx[ci], y = S.cy[ci];
+        p->q_off[x][y] = (int)qsum[ci];
+        p->q_len[x][y] = (int)(qsum[ci + 1] - qsum[ci]);
+        p->class_cost[x][y] = qcost[ci];
+    }
+    p->plan_ms[1] = ms_since(t_phase);
+    t_phase = clk::now();
+
+    // ---- the chunks, emitted in (class pair, bra, ket) order and placed by a stable sort on
+    // (class pair, cost bucket): class pairs in order, heaviest bucket first
+    rc = dev_alloc(ctx, &p->chunks, (size_t)std::max<long long>(nq, 1), &p->bytes);
+    if (!rc && tp) rc = dev_alloc(ctx, &p->chunk_slot, (size_t)std::max<long long>(nq, 1), &p->bytes);
+    Carve ev;
+    const size_t e_raw = ev.take<int4>(nq), e_key1 = ev.take<unsigned short>(nq), e_key2 = ev.take<unsigned short>(nq);
+    const size_t e_idx1 = ev.take<int>(nq), e_idx2 = ev.take<int>(nq), e_slot = ev.take<long long>(tp ? nq : 0);
+    const size_t emit_cub = queue_emit_temp_bytes(nq);
+    const size_t e_cub = ev.take<char>(emit_cub);
+    char *etmp = nullptr;
+    if (!rc && nq > 0) rc = dev_alloc(ctx, &etmp, ev.at, &temp_tally);
+    if (rc) { release_temp(); plan_free(p); return rc; }
+    if (nq > 0) {
+        QueueEmitArgs E{};
+        E.raw = reinterpret_cast<int4 *>(etmp + e_raw);
+        E.key1 = reinterpret_cast<unsigned short *>(etmp + e_key1);
+        E.key2 = reinterpret_cast<unsigned short *>(etmp + e_key2);
+        E.idx1 = reinterpret_cast<int *>(etmp + e_idx1);
+        E.idx2 = reinterpret_cast<int *>(etmp + e_idx2);
+        E.raw_slot = tp ? reinterpret_cast<long long *>(etmp + e_slot) : nullptr;
+        E.chunks = p->chunks;
+        E.chunk_slot = tp ? p->chunk_slot : nullptr;
+        E.nq = nq;
+        e = queue_emit(S, QA, E, etmp + e_cub, emit_cub, s);
+        dev_free(ctx, etmp);
+        if (e != cudaSuccess) { release_temp(); plan_free(p); return cuda_fail(ctx, e, "plan_create work queues"); }
     }
     if (tp && nrows_all > 0) {
         gather_cols_kernel<<<(unsigned)((nrows_all + 255) / 256), 256, 0, s>>>(p->g_col, p->g_fn, p->g_pair,
                                                                             p->g_mol, p->g_rows, nrows_all);
-        if ((e = cudaGetLastError())) { plan_free(p); return cuda_fail(ctx, e, "plan_create gather columns"); }
+        if ((e = cudaGetLastError())) { release_temp(); plan_free(p); return cuda_fail(ctx, e, "plan_create gather columns"); }
     }
-    if ((e = cudaMemcpyAsync(p->pair_ab, stage + o_ab, npair * sizeof(int2), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->info, stage + o_info, npair * sizeof(int4), cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemcpyAsync(p->bnd, stage + o_bnd, npair * sizeof(double2), cudaMemcpyHostToDevice, s)) ||
-        (nkept > 0 && (e = cudaMemcpyAsync(p->pp_src, stage + o_src, nkept * sizeof(int),
-                                           cudaMemcpyHostToDevice, s))) ||
-        (nkept > 0 && (e = cudaMemcpyAsync(p->pbk, stage + o_pbk, nkept * sizeof(double),
-                                           cudaMemcpyHostToDevice, s))) ||
-        (nq > 0 && (e = cudaMemcpyAsync(p->chunks, chunks, (size_t)nq * sizeof(int4),
-                                        cudaMemcpyHostToDevice, s))) ||
-        (e = cudaMemcpyAsync(p->mol_out, mol_out_ll, std::max(nmol, 1) * sizeof(long long),
-                             cudaMemcpyHostToDevice, s)) ||
-        (sync_end ? (e = cudaStreamSynchronize(s)) : (e = cudaEventRecord(ctx->stage_ev, s)))) {
+    release_temp();
+    p->plan_ms[2] = ms_since(t_phase);
+    t_phase = clk::now();
+    if ((e = cudaGetLastError())) {
         plan_free(p);
-        return cuda_fail(ctx, e, "plan_create upload");
+        return cuda_fail(ctx, e, "plan_create work queues");
     }
     if (p->n_gq > 0) {
         // the generic kernel's shell data and quartet list (pageable sources: each copy is
@@ -1790,7 +1675,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             return cuda_fail(ctx, e, "plan_create upload (g shells)");
         }
     }
-    if (!sync_end) ctx->stage_busy = true;
     p->plan_ms[3] = ms_since(t_phase);
     ctx->plans.push_back(p);
     *out = p;
@@ -2052,10 +1936,43 @@ int molints_plan_set_graph(molints_plan *p, int enable) {
     return MOLINTS_OK;
 }
 
+// The host copies of the final pair tables that the statistics and the Schwarz read-out use.
+// Plan creation builds the tables on the device only; they are fetched on first use.
+static int plan_host_tables(const molints_plan *cp) {
+    molints_plan *p = const_cast<molints_plan *>(cp);
+    if (p->host_tables) return MOLINTS_OK;
+    molints_ctx *ctx = p->ctx;
+    const int n = p->npair;
+    std::vector<int2> ab(n);
+    std::vector<int4> info(n);
+    p->bnd_h.resize(n);
+    MI_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (n > 0) {
+        MI_CUDA(ctx, cudaMemcpyAsync(ab.data(), p->pair_ab, n * sizeof(int2), cudaMemcpyDeviceToHost, ctx->stream));
+        MI_CUDA(ctx, cudaMemcpyAsync(info.data(), p->info, n * sizeof(int4), cudaMemcpyDeviceToHost, ctx->stream));
+        MI_CUDA(ctx, cudaMemcpyAsync(p->bnd_h.data(), p->bnd, n * sizeof(double2), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+        MI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    std::vector<int> first(std::max(p->nmol, 1), 0);  // first global shell of each molecule
+    for (int m = 1; m < p->nmol; ++m) first[m] = first[m - 1] + p->mol_nshell[m - 1];
+    p->pair_ref.resize(n);
+    p->npp_h.resize(n);
+    for (int k = 0; k < n; ++k) {
+        const int f = first[p->pair_mol[k]];
+        const int i = std::max(ab[k].x, ab[k].y) - f, j = std::min(ab[k].x, ab[k].y) - f;
+        p->pair_ref[k] = i * (i + 1) / 2 + j;
+        p->npp_h[k] = info[k].y;
+    }
+    p->host_tables = true;
+    return MOLINTS_OK;
+}
+
 int molints_plan_stats(const molints_plan *p, molints_stats *st) {
     if (!p || !st) return MOLINTS_ERR_INVALID;
     if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
     molints_ctx *ctx = p->ctx;
+    if (int rc = plan_host_tables(p)) return rc;
     std::memset(st, 0, sizeof(*st));
     st->n_eri = p->npacked;
     st->n_kernel_launches = p->n_launches;
@@ -2118,6 +2035,8 @@ int molints_plan_stats(const molints_plan *p, molints_stats *st) {
 
 int molints_plan_class_work(const molints_plan *p, int64_t *quartets, double *prim_quartets, int32_t n) {
     if (!p || !quartets || !prim_quartets || n != kNumPairClasses * kNumPairClasses) return MOLINTS_ERR_INVALID;
+    if (!p->ctx) return MOLINTS_ERR_INVALID;  // its context was destroyed first
+    if (int rc = plan_host_tables(p)) return rc;
     const int nc = kNumPairClasses;
     for (int k = 0; k < n; ++k) { quartets[k] = 0; prim_quartets[k] = 0.0; }
     // per (molecule, pair class): pair count, sum and sum of squares of kept primitive pairs
@@ -2189,6 +2108,7 @@ int molints_plan_schwarz(molints_plan *p, double *out) {
     MI_CUDA(ctx, cudaMemcpyAsync(q.data(), p->qcon, p->npair * sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->stream));
     MI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (int rc = plan_host_tables(p)) return rc;
     std::vector<int64_t> base(std::max(p->nmol, 1), 0);
     for (int m = 1; m < p->nmol; ++m)
         base[m] = base[m - 1] + (int64_t)p->mol_nshell[m - 1] * (p->mol_nshell[m - 1] + 1) / 2;
@@ -2203,7 +2123,7 @@ int molints_eri_packed(molints_ctx *ctx, const molints_basis *b, const molints_o
     if (nbf < 0) return fail(ctx, MOLINTS_ERR_INVALID, "eri_packed: malformed basis");
     if (!out && molints_npacked(nbf) > 0) return fail(ctx, MOLINTS_ERR_INVALID, "eri_packed: null output");
     molints_plan *p = nullptr;
-    int rc = plan_create_impl(ctx, 1, b, opts, 0, 1, &p, false);
+    int rc = plan_create_impl(ctx, 1, b, opts, 0, 1, &p);
     if (rc) return rc;
     if (p->npacked == 0) {
         if (stats) rc = molints_plan_stats(p, stats);
