@@ -288,6 +288,9 @@ def run_ours(args):
         eng, [mi.config3_molecule(m) for m in range(1, 16, 2)] + [mi.config4_request(r) for r in range(4)],
         fp32_cutoff=fp32_cut)
     eng.set_class_methods(class_table)
+    # then the work-queue schedule (lane split, chunk lengths) with that table
+    schedule, sched_trials = AT.tune_schedule(eng, [mi.config3_molecule(m) for m in range(1, 16, 2)])
+    eng.set_schedule(schedule)
     eng.set_stream(stream.cuda_stream)
     t_tune = time.perf_counter() - t_tune
     tuned = {"seconds": t_tune, "fp32_cutoff": fp32_cut, "fp32_cutoff_tuning": [t for _, t in tunes],
@@ -295,7 +298,8 @@ def run_ours(args):
                                    if class_table[AT._class_index(t)] & 3 == E.METHOD_RYS),
              "fp32_classes": sorted(t for t in class_timings
                                     if not class_table[AT._class_index(t)] & E.CLASS_NO_FP32),
-             "timings_ms": class_timings}
+             "timings_ms": class_timings, "schedule": schedule,
+             "schedule_trials": [[{k: v for k, v in sc.items()}, round(ms, 3)] for sc, ms in sched_trials]}
 
     # ---- the headline: the 256-molecule batch, molecules sharded over ranks by size
     mols = mi.config3(NMOL)
@@ -356,7 +360,8 @@ def run_ours(args):
     jk = measure_jk(eng, stream, dev, mi.config1()) if "jk" in parts else None
     serving = None
     if "serve" in parts:
-        serving = measure_serving(local, fp32_cut, args.serve_window, rank, class_table=class_table)
+        serving = measure_serving(local, fp32_cut, args.serve_window, rank, class_table=class_table,
+                                  schedule=schedule)
     cpu = None
     if rank == 0 and world == 1 and "cpu" in parts:
         smp = cpu_sample()
@@ -634,7 +639,7 @@ def plan_phases(ph):
 
 
 def measure_serving(device, fp32_cut, window_s, rank, rate=200.0, nslots=8,
-                    budget=150 * 10**9, class_table=None):
+                    budget=150 * 10**9, class_table=None, schedule=None):
     """The serving stream: Poisson arrivals (mean `rate` per s over `window_s` s) of
     synthetic molecules with 20-285 cartesian functions, l <= 3 (f shells on heavy atoms
     half the time), submitted to the engine's server as they arrive.  The server admits them
@@ -655,6 +660,8 @@ def measure_serving(device, fp32_cut, window_s, rank, rate=200.0, nslots=8,
     try:
         if class_table:
             srv.set_class_methods(class_table)
+        if schedule:
+            srv.set_schedule(schedule)
         srv.serve_start(nslots=nslots, hbm_budget_bytes=budget)
         # warm-up: kernel attributes and the result pool, grown by the largest requests
         big = sorted(mols, key=lambda m: -m.npacked)[:4 * nslots]

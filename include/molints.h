@@ -168,6 +168,28 @@ int molints_get_class_methods(const molints_ctx *ctx, int32_t *methods, int32_t 
  * method (or the entry is AUTO); a plan whose options force the other method ignores it. */
 #define MOLINTS_CLASS_NO_FP32 4
 
+/* Work-queue schedule of the plans a context creates (no reference counterpart: the
+ * reference evaluates one shell quartet at a time).  Plans created after the call use it.
+ *   lane_cost     HGP lane split: a quartet's primitive quartets are spread over up to 32
+ *                 lanes until one lane's share costs at most lane_cost (ss|ss)-equivalents
+ *                 (default 80)
+ *   hgp_widen     ket pairs of an unsplit HGP chunk, in units of 32 (one per lane) (default 1;
+ *                 very large batches widen further to bound the queue length)
+ *   rys_chunks    Rys chunks are as long as keeps about this many chunks in a class queue
+ *                 (default 4096)
+ *   rys_max_width the longest Rys chunk, in ket pairs (default 8)
+ * On a B200 the defaults are the shipped tuned values (autotune.tune_schedule); s == NULL
+ * restores them. */
+typedef struct molints_schedule {
+    double lane_cost;
+    int32_t hgp_widen;
+    int32_t rys_chunks;
+    int32_t rys_max_width;
+    int32_t reserved;
+} molints_schedule;
+int molints_set_schedule(molints_ctx *ctx, const molints_schedule *s);
+int molints_get_schedule(const molints_ctx *ctx, molints_schedule *s);
+
 /* Set the CUDA stream (a cudaStream_t passed as void*) the context launches on.
  * NULL selects the context's own (non-blocking) stream; to launch on the legacy default
  * stream pass cudaStreamLegacy ((void*)0x1). */

@@ -1,4 +1,5 @@
-"""Autotuning of the mixed-precision cutoff.
+"""Autotuning: the mixed-precision cutoff, the per-class method table and the work-queue
+schedule.
 
 ``tune_fp32_cutoff`` runs the FP64 path once and the MIXED path over a ladder of cutoffs on
 the device, and returns the largest cutoff whose max abs error against FP64 stays below
@@ -126,3 +127,68 @@ def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95
         timings[tag] = t
         table[_class_index(tag)] = entry
     return table, timings
+
+
+# Values tried per schedule knob (molints_schedule), in the order the knobs are tuned.
+SCHEDULE_GRID = (
+    ("lane_cost", (20.0, 40.0, 80.0, 160.0, 320.0)),
+    ("hgp_widen", (1, 2, 4)),
+    ("rys_chunks", (1024, 4096, 16384)),
+    ("rys_max_width", (4, 8, 16)),
+)
+
+
+def tune_schedule(engine, molecules, repeats: int = 3, margin: float = 0.99, precision=None,
+                  grid=SCHEDULE_GRID):
+    """The work-queue schedule (engine.set_schedule) that runs a batch plan over `molecules`
+    fastest: one pass of coordinate descent over `grid` from the context's current schedule,
+    each knob set to the value with the shortest execute (CUDA events around the whole
+    execute, median of `repeats` after one warm-up) while the others keep their best values so
+    far; a value replaces the current one only when faster by `margin`.  The context's
+    schedule is restored.  Returns (best, trials) with trials = [(schedule, ms), ...]."""
+    import torch
+    from . import engine as E
+    mols = list(molecules)
+    dev = torch.device("cuda", engine.device)
+    out = torch.empty(max(sum(m.npacked for m in mols), 1), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    prec = E.FP64 if precision is None else precision
+    saved = engine.schedule()
+    trials = []
+
+    def run(sched):
+        engine.set_schedule(sched)
+        plan = engine.plan_batch(mols, boys=E.BOYS_EXACT, precision=prec)
+        try:
+            plan.execute(out.data_ptr())
+            ts = []
+            for _ in range(repeats):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                plan.execute(out.data_ptr())
+                b.record(stream)
+                b.synchronize()
+                ts.append(a.elapsed_time(b))
+        finally:
+            plan.close()
+        ms = float(np.median(ts))
+        trials.append((dict(sched), ms))
+        return ms
+
+    engine.set_stream(stream.cuda_stream)
+    try:
+        best = dict(saved)
+        best_ms = run(best)
+        for key, values in grid:
+            for v in values:
+                if v == best[key]:
+                    continue
+                cand = dict(best, **{key: v})
+                ms = run(cand)
+                if ms < margin * best_ms:
+                    best, best_ms = cand, ms
+    finally:
+        engine.set_schedule(saved)
+        engine.set_stream(None)
+    return best, trials
+

@@ -19,4 +19,6 @@ static const int32_t kTunedClassMethods[11][11] = {
     {5, 5, 6, 6, 6, 6, 6, 6, 6, 6, 0},
     {5, 2, 6, 6, 6, 6, 6, 6, 6, 6, 6},
 };
+// work-queue schedule: lane_cost, hgp_widen, rys_chunks, rys_max_width (built-in values)
+static const double kTunedSchedule[4] = {80.0, 1.0, 4096.0, 8.0};
 }  // namespace molints

@@ -69,9 +69,9 @@ struct molints_ctx {
     int32_t default_method[kNumPairClasses][kNumPairClasses] = {};
     char *stage = nullptr;     // pinned host buffer of plan uploads (shells, stage-1 pair tables)
     size_t stage_bytes = 0;
-    // lane-split bound of the HGP work queues: a lane's share of a split quartet costs at most
-    // this many (ss|ss)-equivalent primitive quartets (hgp_split)
-    double lane_cost = 80.0;
+    // work-queue schedule of the plans it creates (molints_set_schedule)
+    molints_schedule sched{};
+    molints_schedule default_sched{};  // what molints_set_schedule(NULL) restores
     std::string err;
 };
 
@@ -128,8 +128,6 @@ struct molints_plan {
     int2 *g_col = nullptr;             // per function pair of every molecule: gather_cols_kernel
     int4 *g_units = nullptr;           // gather units: shell pairs, heaviest first (gather_packed_kernel)
     int64_t n_units = 0;
-    int2 *g_rows = nullptr;            // gather order: {molecule, row ij}, the rows of one shell pair together
-    int64_t n_rows = 0;
     int64_t bytes = 0;
     int n_launches = 0;
     int n_fp32_launches = 0;           // class-pair launches of the last execute that ran FP32
@@ -397,16 +395,19 @@ constexpr int kGatherUnroll = 8;
 // Per function pair (i >= j) of every molecule of a two-phase plan, what the gather needs to
 // place its entries, built once per plan on the device: x = list position << 4 | pair class of
 // the shell pair holding (i, j), y = component of the function in that pair's A << 16 |
-// component in its B.  Entry (m, ij) is at col[mol[4m+3] + ij]; rows[] lists each (m, ij)
-// exactly once.
+// component in its B.  Entry (m, ij) is at col[mol[4m+3] + ij]; thread r takes entry r, of the
+// molecule m with mol[4m+3] <= r < mol[4(m+1)+3] (the molecules' entries follow one another).
 __global__ void gather_cols_kernel(int2 *__restrict__ col, const int2 *__restrict__ fn,
                                    const int *__restrict__ pairs, const long long *__restrict__ mol,
-                                   const int2 *__restrict__ rows, long long nrows) {
+                                   int nmol, long long nrows) {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrows) return;
-    const int2 mr = __ldg(&rows[r]);
-    const int m = mr.x;
-    const long long ij = mr.y;
+    int m = 0, hi = nmol;  // last m with mol[4m+3] <= r
+    while (hi - m > 1) {
+        const int mid = (m + hi) >> 1;
+        if (__ldg(&mol[4 * mid + 3]) <= r) m = mid; else hi = mid;
+    }
+    const long long ij = r - __ldg(&mol[4 * m + 3]);
     const long long fb = __ldg(&mol[4 * m]), pb = __ldg(&mol[4 * m + 1]);
     const long long i = untri_f(ij), j = ij - i * (i + 1) / 2;
     const int2 fi = __ldg(&fn[fb + i]), fj = __ldg(&fn[fb + j]);
@@ -636,6 +637,15 @@ int basis_ncoef(const molints_basis *b, std::vector<double> &ncoef, std::string 
 // The AUTO method table of src, given to dst (the serving slots inherit their owner's table).
 void ctx_copy_methods(molints_ctx *dst, const molints_ctx *src) {
     std::memcpy(dst->class_method, src->class_method, sizeof(dst->class_method));
+    dst->sched = src->sched;
+}
+
+// The schedule of contexts on devices without a tuned one.
+constexpr molints_schedule kBuiltinSchedule = {80.0, 1, 4096, 8, 0};
+
+bool schedule_ok(const molints_schedule &s) {
+    return s.lane_cost > 0.0 && s.lane_cost <= 1e6 && s.hgp_widen >= 1 && s.hgp_widen <= 64 &&
+           s.rys_chunks >= 1 && s.rys_max_width >= 1 && s.rys_max_width <= 64;
 }
 }  // namespace molints
 
@@ -699,10 +709,15 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
         ctx->num_sms = 1;
     {
         cudaDeviceProp prop;
+        ctx->default_sched = kBuiltinSchedule;
         if (cudaGetDeviceProperties(&prop, device) == cudaSuccess &&
-            std::strncmp(prop.name, kTunedDevice, std::strlen(kTunedDevice)) == 0)
+            std::strncmp(prop.name, kTunedDevice, std::strlen(kTunedDevice)) == 0) {
             std::memcpy(ctx->default_method, kTunedClassMethods, sizeof(ctx->default_method));
+            ctx->default_sched = {kTunedSchedule[0], (int32_t)kTunedSchedule[1], (int32_t)kTunedSchedule[2],
+                                  (int32_t)kTunedSchedule[3], 0};
+        }
         std::memcpy(ctx->class_method, ctx->default_method, sizeof(ctx->class_method));
+        ctx->sched = ctx->default_sched;
     }
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
@@ -806,6 +821,26 @@ int molints_get_class_methods(const molints_ctx *ctx, int32_t *methods, int32_t 
     return MOLINTS_OK;
 }
 
+int molints_set_schedule(molints_ctx *ctx, const molints_schedule *s) {
+    if (!ctx) return MOLINTS_ERR_INVALID;
+    if (!s) {
+        ctx->sched = ctx->default_sched;
+        return MOLINTS_OK;
+    }
+    if (!schedule_ok(*s))
+        return fail(ctx, MOLINTS_ERR_INVALID,
+                    "set_schedule: lane_cost in (0, 1e6], hgp_widen and rys_max_width in [1, 64], rys_chunks >= 1");
+    ctx->sched = *s;
+    ctx->sched.reserved = 0;
+    return MOLINTS_OK;
+}
+
+int molints_get_schedule(const molints_ctx *ctx, molints_schedule *s) {
+    if (!ctx || !s) return MOLINTS_ERR_INVALID;
+    *s = ctx->sched;
+    return MOLINTS_OK;
+}
+
 int molints_set_stream(molints_ctx *ctx, void *stream) {
     if (!ctx) return MOLINTS_ERR_INVALID;
     // NULL selects the context's own stream; the legacy default stream is cudaStreamLegacy.
@@ -870,7 +905,7 @@ static void plan_release_device(molints_plan *p) {
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
-                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_rows, p->g_col, p->g_units,
+                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_col, p->g_units,
                     p->gq, p->gq_mol, p->sh_L, p->sh_K, p->sh_fn};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
@@ -1219,11 +1254,13 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 nchunk32 += (x == y) ? nb * (nb + 1) / 64.0 + nb : nb * (nk / 32.0 + 1.0);
             }
     const int widen = std::max(1, (int)std::ceil(nchunk32 / kMaxChunks));
+    const int hgp_widen = std::max(widen, (int)ctx->sched.hgp_widen);
     // A Rys group computes a chunk's quartets one after another.  Its chunks are as long as
-    // keeps about kRysMinChunks chunks in the class queue (1..8 ket pairs): the large classes
-    // have few quartets (e.g. 231 (ff|ff) quartets for six f shells) and need one group per
-    // quartet, while the many small quartets of the low classes amortise the queue atomic.
-    constexpr double kRysMinChunks = 4096.0;
+    // keeps about rys_chunks chunks in the class queue (1..rys_max_width ket pairs): the large
+    // classes have few quartets (e.g. 231 (ff|ff) quartets for six f shells) and need one group
+    // per quartet, while the many small quartets of the low classes amortise the queue atomic.
+    const double rys_chunks = ctx->sched.rys_chunks;
+    const int rys_max_width = ctx->sched.rys_max_width;
     auto rys_width = [&](int x, int y) {
         double nq = 0.0;
         for (int m = 0; m < nmol; ++m) {
@@ -1233,7 +1270,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             const double nb = b1 - b0, nk = k1 - k0;
             nq += (x == y) ? nb * (nb + 1) / 2 : nb * nk;
         }
-        return std::max(1, std::min(8, (int)(nq / kRysMinChunks)));
+        return std::max(1, std::min(rys_max_width, (int)(nq / rys_chunks)));
     };
     QueueSetup S{};
     {
@@ -1246,7 +1283,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
                 S.cx[ci] = x;
                 S.cy[ci] = y;
                 S.hgp[ci] = hgp;
-                S.width[ci] = (hgp ? 32 : rys_width(x, y)) * widen;
+                S.width[ci] = hgp ? 32 * hgp_widen : rys_width(x, y) * widen;
                 S.pcost[ci] = (double)kEriPrimCost[x][y];
                 S.w[ci] = 1.0 + lsum * lsum;
                 items += cls_start[x + 1] - cls_start[x];
@@ -1254,8 +1291,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         S.item_base[kNumClassPairs] = items;
         for (int c = 0; c <= kNumPairClasses; ++c) S.cls_start[c] = cls_start[c];
         S.nmol = nmol;
-        S.widen = widen;
-        S.lane_cost = ctx->lane_cost;
+        S.widen = hgp_widen;
+        S.lane_cost = ctx->sched.lane_cost;
         S.sharded = sharded;
         S.shard_s0 = shard_s0;
         S.shard_s1 = shard_s1;
@@ -1333,8 +1370,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     Carve tv;
     const size_t t_ab1 = tv.take<int2>(npair), t_info1 = tv.take<int4>(npair), t_rec1 = tv.take<int4>(npair);
     const size_t t_seg1 = tv.take<int>(npair), t_mol1 = tv.take<int>(npair);
-    const size_t t_cm = tv.take<int>(cm_start.size()), t_src1 = tv.take<int>(nall);
+    const size_t t_cm = tv.take<int>(cm_start.size());
     const size_t up_bytes = tv.at;
+    const size_t t_src1 = tv.take<int>(nall);
     const size_t t_pbound = tv.take<double2>(nall), t_qmax = tv.take<unsigned long long>(nmol);
     const size_t t_npp1 = tv.take<int>(npair), t_bnd1 = tv.take<double2>(npair);
     const size_t t_key1 = tv.take<unsigned long long>(npair), t_key2 = tv.take<unsigned long long>(npair);
@@ -1355,7 +1393,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     const size_t o_coef = sv.take<double>(nprim), o_poff = sv.take<int>(ns), o_L = sv.take<int>(ns);
     const size_t o_K = sv.take<int>(ns), o_mol = sv.take<long long>(nmol);
     const size_t o_greg = sv.take<long long>(tp ? region_h.size() : 0), o_gfn = sv.take<int2>(tp ? nfn_all : 0);
-    const size_t o_gmol = sv.take<long long>(tp ? (size_t)nmol * 4 : 0), o_grows = sv.take<int2>(tp ? nrows_all : 0);
+    const size_t o_gmol = sv.take<long long>(tp ? (size_t)nmol * 4 : 0);
     const size_t o_gunits = sv.take<int4>(tp ? npe_all : 0);
     int rc = ctx_stage(ctx, sv.at);
     if (rc) { plan_free(p); return rc; }
@@ -1365,16 +1403,13 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         int2 *ab1 = reinterpret_cast<int2 *>(up + t_ab1);
         int4 *info1 = reinterpret_cast<int4 *>(up + t_info1), *rec1 = reinterpret_cast<int4 *>(up + t_rec1);
         int *seg1 = reinterpret_cast<int *>(up + t_seg1), *mol1 = reinterpret_cast<int *>(up + t_mol1);
-        int *src1 = reinterpret_cast<int *>(up + t_src1);
-        int off = 0;
+        int off = 0;  // the primitive pairs themselves are listed on the device (plan_stage1_src)
         for (int k = 0; k < npair; ++k) {
             const PairRec &r = pr[k];
             const int m = r.mol;
             ab1[k] = make_int2(r.a, r.b);
-            const int Ka = K[r.a], Kb = K[r.b];
-            info1[k] = make_int4(off, Ka * Kb, fn_off[r.a], fn_off[r.b]);
-            for (int ia = 0; ia < Ka; ++ia)
-                for (int ib = 0; ib < Kb; ++ib) src1[off++] = (ia << 8) | ib;
+            info1[k] = make_int4(off, r.npp, fn_off[r.a], fn_off[r.b]);
+            off += r.npp;
             const int swapped = (r.a - shell_off[m]) != r.ms;  // A is the lower shell J
             rec1[k] = make_int4(m, r.ref, r.cls | (swapped << 8), r.ms);
             // the pair's run of equal (class, molecule[, ms]): the re-sort by kept count stays in it
@@ -1413,21 +1448,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
             cbase += mol_nbf[m] * (mol_nbf[m] + 1) / 2;
             fb += (int)mol_nbf[m];
         }
-        // gather order: per molecule, shell pairs from the last, each pair's rows together
-        int2 *grows = reinterpret_cast<int2 *>(stage + o_grows);
-        int64_t nr = 0;
-        for (int m = 0; m < nmol; ++m)
-            for (int I = bases[m].nshell - 1; I >= 0; --I)
-                for (int J = I; J >= 0; --J) {
-                    const int gI = shell_off[m] + I, gJ = shell_off[m] + J;
-                    for (int ci = 0; ci < ncart(L[gI]); ++ci)
-                        for (int cj = 0; cj < ncart(L[gJ]); ++cj) {
-                            const int64_t fi = fn_off[gI] + ci, fj = fn_off[gJ] + cj;
-                            if (fj > fi) continue;
-                            grows[nr++] = make_int2(m, (int)(fi * (fi + 1) / 2 + fj));
-                        }
-                }
-        p->n_rows = nr;
         // gather units: every shell pair I >= J of every molecule, heaviest first (rows x the
         // last row's columns), so that the big pairs do not finish last
         int4 *gu = reinterpret_cast<int4 *>(stage + o_gunits);
@@ -1484,7 +1504,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         rc = rc ? rc : dev_alloc(ctx, &p->g_pair, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
-        rc = rc ? rc : dev_alloc(ctx, &p->g_rows, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_col, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_units, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
     }
@@ -1513,7 +1532,6 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         (tp && ((e = h2d(p->g_region, o_greg, region_h.size() * sizeof(long long))) ||
                 (e = h2d(p->g_fn, o_gfn, (size_t)nfn_all * sizeof(int2))) ||
                 (e = h2d(p->g_mol, o_gmol, (size_t)nmol * 4 * sizeof(long long))) ||
-                (e = h2d(p->g_rows, o_grows, (size_t)nrows_all * sizeof(int2))) ||
                 (e = h2d(p->g_units, o_gunits, (size_t)npe_all * sizeof(int4))))) ||
         (e = cudaMemsetAsync(p->counters + nc2, 0, sizeof(int), s)) ||
         (e = cudaMemsetAsync(tmp + t_qmax, 0, (size_t)std::max(nmol, 1) * sizeof(unsigned long long), s)) ||
@@ -1572,6 +1590,10 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     QA.class_cost = reinterpret_cast<double *>(tmp + t_ccost);
     if (npair > 0) {
         const double c0 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
+        if ((e = plan_stage1_src(npair, A.ab1, A.info1, p->sh_K, const_cast<int *>(A.src1), s))) {
+            release_temp(); plan_free(p);
+            return cuda_fail(ctx, e, "plan_create pair list");
+        }
         build_pairs_kernel<<<build_pairs_blocks(npair), 128, 0, s>>>(npair, A.ab1, A.info1, A.src1, p->sh_xyz,
                                                                      p->sh_poff, p->expn, p->ncoef, c0, nullptr,
                                                                      p->pp, p->geo);
@@ -1650,7 +1672,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     }
     if (tp && nrows_all > 0) {
         gather_cols_kernel<<<(unsigned)((nrows_all + 255) / 256), 256, 0, s>>>(p->g_col, p->g_fn, p->g_pair,
-                                                                            p->g_mol, p->g_rows, nrows_all);
+                                                                            p->g_mol, nmol, nrows_all);
         if ((e = cudaGetLastError())) { release_temp(); plan_free(p); return cuda_fail(ctx, e, "plan_create gather columns"); }
     }
     release_temp();

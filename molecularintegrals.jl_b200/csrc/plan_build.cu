@@ -12,6 +12,18 @@ constexpr int kThreads = 256;
 
 inline unsigned blocks_for(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
+__global__ void pair_src_kernel(int npair, const int2 *__restrict__ ab1, const int4 *__restrict__ info1,
+                                const int *__restrict__ sh_K, int *__restrict__ src1) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= npair) return;
+    const int4 in = info1[k];
+    const int kb = sh_K[ab1[k].y];
+    for (int x = 0, ia = 0, ib = 0; x < in.y; ++x) {
+        src1[in.x + x] = (ia << 8) | ib;
+        if (++ib == kb) { ib = 0; ++ia; }
+    }
+}
+
 // max over a molecule's pairs of Qabs = sum_k b_k (every primitive pair), summed in list order
 // as the screening needs it.  The sums are >= 0, so their bit patterns order like the values.
 __global__ void pair_qmax_kernel(PlanBuildArgs A) {
@@ -207,6 +219,13 @@ __global__ void queue_place_kernel(QueueEmitArgs E) {
 }
 
 }  // namespace
+
+cudaError_t plan_stage1_src(int npair, const int2 *ab1, const int4 *info1, const int *sh_K, int *src1,
+                            cudaStream_t s) {
+    if (npair <= 0) return cudaSuccess;
+    pair_src_kernel<<<blocks_for(npair), kThreads, 0, s>>>(npair, ab1, info1, sh_K, src1);
+    return cudaGetLastError();
+}
 
 size_t plan_build_temp_bytes(int npair) {
     size_t a = 0, b = 0;

@@ -102,6 +102,11 @@ struct PlanBuildArgs {
     const long long *g_mol;        // two-phase: per molecule {.., first pair entry, ..}
 };
 
+// Stage-1 primitive-pair list: pair k's K_A x K_B entries (ia << 8) | ib, A's primitive
+// outer, at info1[k].x.
+cudaError_t plan_stage1_src(int npair, const int2 *ab1, const int4 *info1, const int *sh_K, int *src1,
+                            cudaStream_t s);
+
 // Screening, re-sort and final pair tables.  temp: CUB scratch of at least
 // plan_build_temp_bytes(npair) bytes.
 cudaError_t plan_build_pairs(const PlanBuildArgs &A, void *temp, size_t temp_bytes, cudaStream_t s);

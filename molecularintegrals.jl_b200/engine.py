@@ -44,7 +44,8 @@ EXPORTED_SYMBOLS = [
     "molints_result", "molints_result_copy", "molints_request_info", "molints_request_error",
     "molints_release", "molints_serve_stats", "molints_shard_range", "molints_plan_create_shard",
     "molints_plan_set_graph", "molints_plan_jk", "molints_jk", "molints_one_e",
-    "molints_get_class_methods", "molints_plan_class_work",
+    "molints_get_class_methods", "molints_plan_class_work", "molints_set_schedule",
+    "molints_get_schedule",
 ]
 
 
@@ -86,6 +87,17 @@ class Stats(ctypes.Structure):
         return d
 
 
+class Schedule(ctypes.Structure):
+    """molints_schedule: the work-queue knobs of the plans a context creates."""
+    _fields_ = [("lane_cost", ctypes.c_double), ("hgp_widen", ctypes.c_int32),
+                ("rys_chunks", ctypes.c_int32), ("rys_max_width", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+    KEYS = ("lane_cost", "hgp_widen", "rys_chunks", "rys_max_width")
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k in self.KEYS}
+
+
 _lib = None
 
 
@@ -122,6 +134,8 @@ def load_library(path: Path | str | None = None):
         "molints_plan_npacked": (I64, [P]),
         "molints_set_class_methods": (ctypes.c_int, [P, P, I32]),
         "molints_get_class_methods": (ctypes.c_int, [P, P, I32]),
+        "molints_set_schedule": (ctypes.c_int, [P, P]),
+        "molints_get_schedule": (ctypes.c_int, [P, P]),
         "molints_plan_class_work": (ctypes.c_int, [P, P, P, I32]),
         "molints_serve_start": (ctypes.c_int, [P, I32, I64]),
         "molints_serve_stop": (ctypes.c_int, [P]),
@@ -401,6 +415,24 @@ class Engine:
         for (x, y), m in dict(table).items():
             arr[x * NUM_PAIR_CLASSES + y] = m
         self._check(self.lib.molints_set_class_methods(self.ctx, _ptr(arr), arr.size))
+
+    def set_schedule(self, sched: dict | None = None):
+        """Work-queue schedule of the plans created afterwards: a dict with any of lane_cost,
+        hgp_widen, rys_chunks, rys_max_width (the others keep their current values); None
+        restores the library's default (the tuned one on a B200)."""
+        if sched is None:
+            self._check(self.lib.molints_set_schedule(self.ctx, None))
+            return
+        cur = self.schedule()
+        cur.update(sched)
+        sc = Schedule(**{k: cur[k] for k in Schedule.KEYS})
+        self._check(self.lib.molints_set_schedule(self.ctx, ctypes.byref(sc)))
+
+    def schedule(self) -> dict:
+        """The context's current work-queue schedule."""
+        sc = Schedule()
+        self._check(self.lib.molints_get_schedule(self.ctx, ctypes.byref(sc)))
+        return sc.as_dict()
 
     def class_methods(self) -> dict:
         """The context's current table as {(x, y): entry} for x >= y."""
