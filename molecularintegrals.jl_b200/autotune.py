@@ -131,7 +131,7 @@ def tune_class_methods(engine, molecules, repeats: int = 3, margin: float = 0.95
 
 # Values tried per schedule knob (molints_schedule), in the order the knobs are tuned.
 SCHEDULE_GRID = (
-    ("lane_cost", (20.0, 40.0, 80.0, 160.0, 320.0)),
+    ("lane_cost", (40.0, 80.0, 160.0, 320.0, 640.0, 1280.0)),
     ("hgp_widen", (1, 2, 4)),
     ("rys_chunks", (1024, 4096, 16384)),
     ("rys_max_width", (4, 8, 16)),
