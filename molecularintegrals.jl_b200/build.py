@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import argparse
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -47,9 +48,25 @@ def sources():
             sorted(gen))
 
 
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
 def _deps(src: Path):
-    return [src, CSRC / "eri_common.cuh", CSRC / "rys_common.cuh", CSRC / "eri_dispatch.h", CSRC / "plan_build.cuh",
-            CSRC / "class_table.h", INCLUDE / "molints.h"]
+    """src and every project header it includes, directly or through other headers (quoted
+    includes, resolved against the including file's folder, then csrc/ and include/)."""
+    seen, todo = [], [src]
+    while todo:
+        f = todo.pop()
+        if f in seen or not f.exists():
+            continue
+        seen.append(f)
+        for name in _INCLUDE_RE.findall(f.read_text(errors="replace")):
+            for base in (f.parent, CSRC, INCLUDE):
+                cand = (base / name).resolve()
+                if cand.exists():
+                    todo.append(cand)
+                    break
+    return seen
 
 
 def _compile(src: Path, force: bool):

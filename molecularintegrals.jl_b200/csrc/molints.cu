@@ -426,12 +426,16 @@ __global__ void gather_cols_kernel(int2 *__restrict__ col, const int2 *__restric
 // component the direct path would have stored it from: the quartet's bra is the pair of the
 // higher class, or of the later list position within a class (P for the diagonal quartet
 // P == Q); a pair's components are taken in its A, B orientation, with the larger component
-// first within a same-shell pair, as the direct store conditions pick.
+// first within a same-shell pair, as the direct store conditions pick.  With quartet
+// screening, the entries of a screened quartet are written as 0 without reading the scratch:
+// two-phase plans that screen end each bra's ket run after its last unscreened ket, so no
+// chunk computes the rest.
 constexpr int kGatherMaxRows = 100;  // components of an (ff) pair
 __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
     double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ col,
     const long long *__restrict__ region, const long long *__restrict__ mol,
-    const int4 *__restrict__ units, long long nunits, int *__restrict__ counter, int nmol) {
+    const int4 *__restrict__ units, long long nunits, int *__restrict__ counter, int nmol,
+    const double2 *__restrict__ bnd, double screen_cut) {
     // [P as bra, P as ket][class of the other pair]: {scratch offset, first bra, first ket,
     // kets, block size}
     __shared__ long long reg[2][kNumPairClasses][5];
@@ -453,6 +457,7 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
         const int2 pe = __ldg(&col[cbase + (long long)fi0 * (fi0 + 1) / 2 + fj0]);
         const int posP = pe.x >> 4, clsP = pe.x & 15;
         const int nbP = c_pair_nb[clsP];
+        const double qP = screen_cut > 0.0 ? __ldg(&bnd[posP]).x : 0.0;
         int R = 0;
         for (int a = 0; a < nI; ++a) R += same ? a + 1 : nJ;
         for (int r = threadIdx.x; r < R; r += kGatherThreads) {
@@ -481,12 +486,16 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
             const double *src[2];
             long long rs[2], kl[2];
             int r0[2];
+            bool zero[2];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 kl[c] = kl0 + c * kGatherThreads;
                 const bool on = kl[c] <= ijmax;
                 const int2 qe = on ? __ldg(&col[cbase + kl[c]]) : make_int2(clsP, 0);
                 const int posQ = on ? qe.x >> 4 : posP, clsQ = qe.x & 15;
+                // a screened quartet (the class kernels' test, Qabs_P Qabs_Q < screen_cut) is 0;
+                // its block is not read (no chunk may have computed it)
+                zero[c] = screen_cut > 0.0 && qP * __ldg(&bnd[posQ]).x < screen_cut;
                 const int qa = qe.y >> 16, qb = qe.y & 0xffff;
                 const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
                 const long long *rg = reg[braP ? 0 : 1][clsQ];
@@ -509,7 +518,7 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
                 for (int c = 0; c < 2; ++c)
 #pragma unroll
                     for (int t = 0; t < 4; ++t)
-                        v[c][t] = (r + t < R && r + t >= r0[c]) ? __ldg(src[c] + s_rc[r + t] * rs[c]) : 0.0;
+                        v[c][t] = (r + t < R && r + t >= r0[c] && !zero[c]) ? __ldg(src[c] + s_rc[r + t] * rs[c]) : 0.0;
 #pragma unroll
                 for (int c = 0; c < 2; ++c)
 #pragma unroll
@@ -1356,6 +1365,9 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     }
     const bool tp = p->two_phase != 0;
     S.two_phase = tp;
+    S.screen_sort = !sharded && opts.screen_cutoff > 0.0;
+    S.screen_trunc = tp && S.screen_sort;
+    S.screen_cut = opts.screen_cutoff;
 
     // ---- pinned upload buffer: the summary read back after the device build, the plan's
     // shells, the stage-1 block (laid out as in the device temporaries, one copy), the molecule
@@ -1550,6 +1562,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     A.npair = npair;
     A.nall = (int)nall;
     A.prim_cutoff = opts.prim_cutoff;
+    A.screen_sort = S.screen_sort;
     A.ab1 = reinterpret_cast<const int2 *>(tmp + t_ab1);
     A.info1 = reinterpret_cast<const int4 *>(tmp + t_info1);
     A.src1 = reinterpret_cast<const int *>(tmp + t_src1);
@@ -1583,6 +1596,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     QA.ms = A.ms;
     QA.npp_prefix = A.npp_prefix;
     QA.region = tp ? p->g_region : nullptr;
+    QA.bnd = p->bnd;
     QA.cnt = reinterpret_cast<long long *>(tmp + t_cnt);
     QA.cost = reinterpret_cast<double *>(tmp + t_cost);
     QA.off = reinterpret_cast<long long *>(tmp + t_off);
@@ -1810,7 +1824,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col, p->g_region,
                                                              p->g_mol, p->g_units, p->n_units,
                                                              p->counters + kNumPairClasses * kNumPairClasses,
-                                                             p->nmol);
+                                                             p->nmol, p->bnd, p->opts.screen_cutoff);
         if (int rc = mark(launches, "gather_packed", 1, s)) return rc;
         ++launches;
     }

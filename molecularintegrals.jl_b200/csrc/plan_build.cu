@@ -38,7 +38,8 @@ __global__ void pair_qmax_kernel(PlanBuildArgs A) {
 // Per stage-1 pair: primitive pairs kept (b_k * max Qabs of the molecule >= prim_cutoff; each
 // dropped term of any integral is below prim_cutoff by the Schwarz inequality), the pair's
 // bounds Qabs = sum of kept b_k and R = (1 + |AB|)^lb sum of kept w_k, and its sort key:
-// (class, molecule[, ms]) run first, then kept count descending.
+// (class, molecule[, ms]) run first, then kept count descending (plans that screen quartets:
+// Qabs bucket descending, then kept count descending).
 __global__ void pair_screen_kernel(PlanBuildArgs A) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= A.npair) return;
@@ -62,7 +63,10 @@ __global__ void pair_screen_kernel(PlanBuildArgs A) {
     for (int l = 0; l < A.sh_L[ab.y]; ++l) f *= dab1;
     A.npp1[k] = kept;
     A.bnd1[k] = make_double2(qa, wa * f);
-    A.key1[k] = ((unsigned long long)A.seg1[k] << 20) | (unsigned long long)(0xFFFFF - kept);
+    const unsigned long long within =
+        A.screen_sort ? ((unsigned long long)(255 - qabs_bucket(qa)) << 12) | (unsigned long long)(0xFFF - min(kept, 0xFFF))
+                      : (unsigned long long)(0xFFFFF - kept);
+    A.key1[k] = ((unsigned long long)A.seg1[k] << 20) | within;
     A.idx1[k] = k;
 }
 
@@ -102,12 +106,30 @@ __global__ void pair_tables_kernel(PlanBuildArgs A) {
 
 // ---- work queues
 
+// Two-phase plans that screen quartets: the end of bra pb's ket run [kbeg, kend) after its last ket q
+// with Qabs_pb Qabs_q >= screen_cut (kbeg if there is none).  The run is in Qabs-bucket order,
+// descending, so the kets screened by their bucket's upper bound alone form a suffix, found by
+// bisection; the last unscreened ket lies just before it.  The quartets past the end are
+// screened: the gather writes their zeros.
+__device__ int unscreened_end(const QueueSetup &S, const QueueArgs &A, int pb, int kbeg, int kend) {
+    const double qp = A.bnd[pb].x;
+    int lo = kbeg, hi = kend;  // first q with qabs_bucket_hi(q) * qp < cut, in [kbeg, kend]
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (qabs_bucket_hi(qabs_bucket(A.bnd[mid].x)) * qp < S.screen_cut) hi = mid; else lo = mid + 1;
+    }
+    int e = lo;
+    while (e > kbeg && qp * A.bnd[e - 1].x < S.screen_cut) --e;
+    return e;
+}
+
 // The chunks of one item: bra pair pb of class pair ci against its ket run, in ket order.
 // Chunks hold one bra pair and up to `width` ket pairs of the same molecule.  HGP chunks whose
 // quartets are split over lanes (hgp_split) hold (32 >> lg) * widen ket pairs and end where the
 // split changes: the kets of a molecule's class run are in descending kept count, so the split
-// only falls along the run and a chunk that starts unsplit stays unsplit (shard plans order by
-// highest shell first and test every chunk).
+// only falls along the run and a chunk that starts unsplit stays unsplit (shard plans, ordered
+// by highest shell first, and plans that screen quartets, ordered by Qabs bucket first, test
+// every ket).
 template <class Emit>
 __device__ void walk_item(const QueueSetup &S, const QueueArgs &A, int ci, int pb, Emit &&emit) {
     const int x = S.cx[ci], y = S.cy[ci];
@@ -127,18 +149,21 @@ __device__ void walk_item(const QueueSetup &S, const QueueArgs &A, int ci, int p
             kend = S.ps1[y];
         }
     }
+    if (S.screen_trunc && kend > kbeg) kend = unscreened_end(S, A, pb, kbeg, kend);
     const int nb = A.npp[pb];
     const double wp = S.w[ci] * nb, pcost = S.pcost[ci];
-    bool heavy = S.hgp[ci] != 0;  // this bra's remaining kets may still need a split
+    // this bra's remaining kets may still need a split (in Qabs order the kept counts do not
+    // descend along the run: every chunk is tested)
+    bool heavy = S.hgp[ci] != 0;
     for (int q0 = kbeg; q0 < kend;) {
         int n = min(S.width[ci], kend - q0), lg = 0;
         if (heavy) {
             lg = hgp_split(nb, A.npp[q0], pcost, S.lane_cost);
             n = min((32 >> (lg & 7)) * S.widen, kend - q0);
-            if (lg)
+            if (lg || S.sharded || S.screen_sort)
                 for (int k = 1; k < n; ++k)
                     if (hgp_split(nb, A.npp[q0 + k], pcost, S.lane_cost) != lg) { n = k; break; }
-            heavy = lg != 0 || S.sharded;
+            heavy = lg != 0 || S.sharded || S.screen_sort;
         }
         const double cost = wp * (double)(A.npp_prefix[q0 + n] - A.npp_prefix[q0]);
         emit(q0, n, lg, m, cost);

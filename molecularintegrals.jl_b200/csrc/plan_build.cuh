@@ -51,6 +51,28 @@ __host__ __device__ inline int cost_bucket(double c) {
     return b < 0 ? 0 : (b > kCostBuckets - 1 ? kCostBuckets - 1 : b);
 }
 
+// Bucket of a pair's Schwarz factor Qabs for the screening order: a factor of 16 in Qabs per
+// bucket.  With Qabs = f 2^e (f in [0.5, 1), so Qabs < 2^e), the bucket is
+// (e + kQabsBias) / 4 clamped to [1, 255], and 0 for Qabs = 0.  Plans that screen quartets
+// order each (class, molecule) run of pairs by bucket, descending, so that a bra's unscreened
+// kets come first; within a bucket the kept count descends, which keeps a chunk's lanes
+// alike.
+constexpr int kQabsBias = 640;
+__host__ __device__ inline int qabs_bucket(double q) {
+    if (!(q > 0.0)) return 0;
+    int e2 = 0;
+    frexp(q, &e2);
+    const int b = (e2 + kQabsBias) >> 2;
+    return b < 1 ? 1 : (b > 255 ? 255 : b);
+}
+
+// Upper bound of the Qabs values in a bucket (infinite for the top one).
+__host__ __device__ inline double qabs_bucket_hi(int b) {
+    if (b <= 0) return 0.0;
+    if (b >= 255) return HUGE_VAL;
+    return ldexp(1.0, 4 * b + 3 - kQabsBias);  // e <= 4b + 3 - kQabsBias
+}
+
 // What the queue kernels need per class pair (x, y <= x), in the host's class-pair order
 // (x outer, y inner): a plain struct passed by value.
 struct QueueSetup {
@@ -67,6 +89,13 @@ struct QueueSetup {
     int sharded, shard_s0, shard_s1;    // shard plans: owned highest-shell range [s0, s1)
     int ps0[kNumPairClasses], ps1[kNumPairClasses];  // first pair of each class with ms >= s0 / s1
     int two_phase;
+    // Quartet screening (Qabs_p Qabs_q < screen_cut written as 0): the pair runs are in
+    // Qabs-bucket order (screen_sort; direct and two-phase plans alike, so that their quartets
+    // have the same bra and sum alike), and in two-phase plans each bra's ket run ends after
+    // its last unscreened ket (screen_trunc): the gather writes the zeros of the quartets no
+    // chunk holds.
+    int screen_sort, screen_trunc;
+    double screen_cut;
 };
 
 // Device arrays of one device plan build (all owned by the caller).
@@ -74,6 +103,7 @@ struct PlanBuildArgs {
     int npair;
     int nall;                      // stage-1 primitive pairs
     double prim_cutoff;
+    int screen_sort;               // order runs by Qabs bucket (descending), then kept count
     // stage 1 (pair order by class, molecule[, ms], all-primitive count)
     const int2 *ab1;               // global shells (A, B)
     const int4 *info1;             // {first primitive pair, count, first function of A, of B}
@@ -123,6 +153,7 @@ struct QueueArgs {
     const int *ms;                 // shard plans
     const long long *npp_prefix;
     const long long *region;       // two-phase: per (x, y, molecule) 4 fields, else null
+    const double2 *bnd;            // per final pair (Qabs, R): the screening order's cut
     long long *cnt;                // n_items + 1
     double *cost;                  // n_items
     long long *off;                // n_items + 1

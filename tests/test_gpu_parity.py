@@ -152,31 +152,37 @@ def test_auto_output_falls_back_to_direct_under_budget():
 def test_two_phase_output_equals_direct(eng):
     """The two-phase output (quartet blocks into a class-major scratch, then the packed vector
     gathered in order) gives the direct path's vector bit for bit: HGP and Rys classes (an f
-    molecule), FP64 and MIXED, a batch plan over several molecules, every entry written (NaN
-    sentinel), and J/K digested from a two-phase plan."""
+    molecule), FP64, MIXED and MIXED with quartet screening (whose two-phase plans order the
+    pairs by Schwarz factor and leave the screened quartets to the gather), a batch plan over
+    several molecules, every entry written (NaN sentinel), and J/K digested from a two-phase
+    plan."""
     import torch
     from molints_b200 import engine
     TP, DIR = engine.OUTPUT_TWO_PHASE, engine.OUTPUT_DIRECT
     for sh in (mi.config2(), _f_molecule(7), _rand_basis(105, 2)):
-        for prec, cut in ((engine.FP64, 0.0), (engine.MIXED, 1e-3)):
-            a = eng.eri_packed(sh, precision=prec, fp32_cutoff=cut, output=DIR)
-            b = eng.eri_packed(sh, precision=prec, fp32_cutoff=cut, output=TP)
+        for prec, cut, scut in ((engine.FP64, 0.0, 0.0), (engine.MIXED, 1e-3, 0.0), (engine.MIXED, 1e-3, 1e-8)):
+            a = eng.eri_packed(sh, precision=prec, fp32_cutoff=cut, screen_cutoff=scut, output=DIR)
+            b = eng.eri_packed(sh, precision=prec, fp32_cutoff=cut, screen_cutoff=scut, output=TP)
             assert np.array_equal(a, b)
-    mols = [mi.config2(), mi.config0(), _rand_basis(106, 2), _f_molecule(8)]
-    outs = []
-    for mode in (DIR, TP):
-        plan = eng.plan_batch(mols, output=mode)
-        out = torch.full((plan.npacked,), float("nan"), dtype=torch.float64, device="cuda")
-        torch.cuda.synchronize()
-        eng.set_stream(torch.cuda.current_stream().cuda_stream)
-        try:
-            plan.execute(out.data_ptr())
+            if scut > 0.0:
+                assert (a == 0.0).sum() > 0
+    mols = [mi.config2(), mi.config0(), _rand_basis(106, 2), _f_molecule(8), mi.config3_molecule(6)]
+    for scut in (0.0, 1e-9):
+        outs = []
+        for mode in (DIR, TP):
+            plan = eng.plan_batch(mols, output=mode, precision=engine.MIXED if scut else engine.FP64,
+                                  fp32_cutoff=1e-3 if scut else 0.0, screen_cutoff=scut)
+            out = torch.full((plan.npacked,), float("nan"), dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
-        finally:
-            eng.set_stream(None)
-        outs.append(out.cpu().numpy())
-        plan.close()
-    assert not np.isnan(outs[1]).any() and np.array_equal(outs[0], outs[1])
+            eng.set_stream(torch.cuda.current_stream().cuda_stream)
+            try:
+                plan.execute(out.data_ptr())
+                torch.cuda.synchronize()
+            finally:
+                eng.set_stream(None)
+            outs.append(out.cpu().numpy())
+            plan.close()
+        assert not np.isnan(outs[1]).any() and np.array_equal(outs[0], outs[1])
     sh = _f_molecule(9)
     n = sh.nbf
     rng = np.random.default_rng(3)
