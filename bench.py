@@ -9,7 +9,7 @@ molecules: every group's plan executed (one CUDA graph per plan) into a device o
 than L2.
 
   value      MIXED: FP32 variants below the tuned fp32_cutoff where they measured faster, and
-             Schwarz screening at screen_cutoff 1e-10 (each screened integral is below 1e-10
+             Schwarz screening at screen_cutoff 5e-10 (each screened integral is below 5e-10
              by the Schwarz inequality); max abs error against the oracle is reported beside it
   fp64       the plain FP64 path on the same plans' molecules (no screening)
   e2e        the same metric through the public batch API from host arrays: plan creation from
@@ -48,7 +48,10 @@ NMOL = 256
 WORKLOAD = ("batch256: 256 synthetic molecules (seeds 3000+m, 4-40 atoms, l<=2, K in {1,3,6,7}, "
             "15-330 cart. functions, 4.91e10 unique integrals)")
 GROUP_CAP = 1.5e9          # output doubles per batch plan
-SCREEN_CUTOFF = 1e-10      # MIXED: quartets whose Schwarz bound is below this are written as 0
+# MIXED: quartets whose Schwarz bound Qabs_P Qabs_Q is below this are written as 0, so each
+# screened integral is off by less than 5e-10; with the FP32 cutoff tuned to an error of at most
+# 2.5e-10, the MIXED error stays below the 1e-9 target
+SCREEN_CUTOFF = 5e-10
 # The CPU sample: the batch molecules among its first eight with fewer than 150 functions and
 # more than 40 (m = 1, 2, 4: 130, 82 and 67 functions, both recipes, 44.6 M integrals)
 CPU_SAMPLE = (1, 2, 4)
@@ -348,6 +351,8 @@ def run_ours(args):
                    ("n_shell_quartets", "n_fp32_quartets", "n_screened", "n_fp32_launches")}
 
     roofline = measure_roofline(plans64, groups, mols, out, stream, dev)
+    tmx, _, _ = profile_pass(plansmx, out)
+    roofline["mixed_kernel_ms_per_step"] = {n: round(t, 3) for n, t in sorted(tmx.items(), key=lambda x: -x[1])}
     e2e = measure_e2e(eng, dev, stream, mols, groups, fp32_cut, min(args.steps, args.e2e_steps))
     plain = measure_plain_fp64(eng, dev, mols, mine) if "plain" in parts else None
     for p in plans64 + plansmx:
@@ -385,7 +390,7 @@ def run_ours(args):
             "metric": METRIC, "value": valuemx, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": msmx / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (FP32 VRR below the tuned cutoff where faster; Schwarz screening 1e-10)",
+            "dtype": f"f64 (FP32 VRR below the tuned cutoff where faster; Schwarz screening {SCREEN_CUTOFF:g})",
             "data": "synthetic", "config": cfg,
             "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
                      "mixed_over_fp64": valuemx / value64},
@@ -401,6 +406,27 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def profile_pass(plans, out):
+    """One serialised profiling execute of each plan: per kernel its summed device time (ms,
+    per-launch CUDA events on the launching stream) and launches, and per class pair the FLOP
+    of the primitive quartets its kernels evaluate."""
+    from molints_b200 import flops as F
+    times, nlaunch, executed = {}, {}, {}
+    lv = {"s": 0, "p": 1, "d": 2, "f": 3}
+    for p in plans:
+        p.set_profiling(True)
+        p.execute(out.data_ptr())
+        for name, ms in p.launch_times():
+            times[name] = times.get(name, 0.0) + ms
+            nlaunch[name] = nlaunch.get(name, 0) + 1
+        p.set_profiling(False)
+        for tag, (nq, kq) in p.class_work().items():
+            la, lb, lc, ld = (lv[c] for c in tag)
+            executed[tag] = executed.get(tag, 0.0) + kq * F.per_prim_flops(la, lb, lc, ld) + \
+                nq * F.hrr_flops(la, lb, lc, ld)
+    return times, nlaunch, executed
 
 
 def measure_roofline(plans, groups, mols, out, stream, dev):
@@ -419,19 +445,7 @@ def measure_roofline(plans, groups, mols, out, stream, dev):
             w, _ = F.workload(mols[i])
             for tag, d in w.items():
                 per_tag[tag] = per_tag.get(tag, 0.0) + d["flop"]
-    times, nlaunch, executed = {}, {}, {}
-    lv = {"s": 0, "p": 1, "d": 2, "f": 3}
-    for p in plans:
-        p.set_profiling(True)
-        p.execute(out.data_ptr())
-        for name, ms in p.launch_times():
-            times[name] = times.get(name, 0.0) + ms
-            nlaunch[name] = nlaunch.get(name, 0) + 1
-        p.set_profiling(False)
-        for tag, (nq, kq) in p.class_work().items():
-            la, lb, lc, ld = (lv[c] for c in tag)
-            executed[tag] = executed.get(tag, 0.0) + kq * F.per_prim_flops(la, lb, lc, ld) + \
-                nq * F.hrr_flops(la, lb, lc, ld)
+    times, nlaunch, executed = profile_pass(plans, out)
     total_ms = sum(times.values())
     peak64 = measure_fp64_peak(dev)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -776,8 +790,9 @@ def run_case(args):
     eng = E.Engine(0)
     stream = torch.cuda.current_stream()
     eng.set_stream(stream.cuda_stream)
-    plan = eng.plan_batch(mols, method=method, precision=E.MIXED if args.mixed > 0 else E.FP64,
-                          fp32_cutoff=args.mixed, boys=E.BOYS_EXACT)
+    mixed = args.mixed > 0 or args.screen > 0
+    plan = eng.plan_batch(mols, method=method, precision=E.MIXED if mixed else E.FP64,
+                          fp32_cutoff=args.mixed, screen_cutoff=args.screen, boys=E.BOYS_EXACT)
     out = torch.empty(max(plan.npacked, 1), dtype=torch.float64, device="cuda")
     for k in range(args.repeat):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -813,6 +828,7 @@ def main():
     ap.add_argument("--nh", type=int, default=16)
     ap.add_argument("--method", default="auto", choices=["auto", "hgp", "rys"])
     ap.add_argument("--mixed", type=float, default=0.0, help="FP32 cutoff of --case (0: plain FP64)")
+    ap.add_argument("--screen", type=float, default=0.0, help="quartet screening cutoff of --case (0: none)")
     ap.add_argument("--repeat", type=int, default=3)
     args = ap.parse_args()
     if args.case:

@@ -178,6 +178,9 @@ int molints_get_class_methods(const molints_ctx *ctx, int32_t *methods, int32_t 
  *   rys_chunks    Rys chunks are as long as keeps about this many chunks in a class queue
  *                 (default 4096)
  *   rys_max_width the longest Rys chunk, in ket pairs (default 8)
+ *   gather_blocks resident blocks per SM of the two-phase output's gather pass, in [1, 16]
+ *                 (0 = default 5): its persistent grid is this many blocks per SM.  Fewer
+ *                 blocks trade warps for L1 space per block.
  * On a B200 the defaults are the shipped tuned values (autotune.tune_schedule); s == NULL
  * restores them. */
 typedef struct molints_schedule {
@@ -185,7 +188,7 @@ typedef struct molints_schedule {
     int32_t hgp_widen;
     int32_t rys_chunks;
     int32_t rys_max_width;
-    int32_t reserved;
+    int32_t gather_blocks;
 } molints_schedule;
 int molints_set_schedule(molints_ctx *ctx, const molints_schedule *s);
 int molints_get_schedule(const molints_ctx *ctx, molints_schedule *s);

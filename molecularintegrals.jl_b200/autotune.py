@@ -135,6 +135,7 @@ SCHEDULE_GRID = (
     ("hgp_widen", (1, 2, 4)),
     ("rys_chunks", (1024, 4096, 16384)),
     ("rys_max_width", (4, 8, 16)),
+    ("gather_blocks", (3, 4, 5, 6, 8)),
 )
 
 

@@ -719,14 +719,16 @@ def emit_class_table(path: Path):
              f"static const int32_t kTunedClassMethods[{n}][{n}] = {{"]
     for x in range(n):
         lines.append("    {" + ", ".join(str(v) for v in tab[x]) + "},")
-    # work-queue schedule (molints_schedule: lane_cost, hgp_widen, rys_chunks, rys_max_width),
-    # the built-in one where the tuner's result has none
-    sc = d.get("schedule", {"lane_cost": 80.0, "hgp_widen": 1, "rys_chunks": 4096, "rys_max_width": 8})
+    # work-queue schedule (molints_schedule: lane_cost, hgp_widen, rys_chunks, rys_max_width,
+    # gather_blocks), the built-in values where the tuner's result has none
+    sc = dict({"lane_cost": 80.0, "hgp_widen": 1, "rys_chunks": 4096, "rys_max_width": 8, "gather_blocks": 5},
+              **d.get("schedule", {}))
+    keys = ("lane_cost", "hgp_widen", "rys_chunks", "rys_max_width", "gather_blocks")
     lines += ["};",
-              "// work-queue schedule: lane_cost, hgp_widen, rys_chunks, rys_max_width"
+              "// work-queue schedule: " + ", ".join(keys)
               + (f" ({d['schedule_source']})" if "schedule_source" in d else " (built-in values)"),
-              "static const double kTunedSchedule[4] = {" +
-              ", ".join(repr(float(sc[k])) for k in ("lane_cost", "hgp_widen", "rys_chunks", "rys_max_width")) + "};",
+              f"static const double kTunedSchedule[{len(keys)}] = {{" +
+              ", ".join(repr(float(sc[k])) for k in keys) + "};",
               "}  // namespace molints", ""]
     return "\n".join(lines)
 

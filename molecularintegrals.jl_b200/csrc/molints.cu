@@ -117,6 +117,7 @@ struct molints_plan {
     // two-phase output (molints_output): the class kernels store whole quartet blocks into a
     // class-major scratch, a gather pass writes the packed vector in order from it
     int two_phase = 0;
+    int gather_blocks = 0;             // the context's schedule at creation: gather blocks per SM
     int64_t scratch_need = 0;          // doubles of the context's scratch an execute uses: per
                                        // (class pair, molecule) a region of quartet blocks
     long long *chunk_slot = nullptr;   // per chunk: scratch offset of its first quartet's block
@@ -126,6 +127,7 @@ struct molints_plan {
     long long *g_mol = nullptr;        // per molecule: {first function, first pair entry, packed offset,
                                        // first function-pair entry of g_col}
     int2 *g_col = nullptr;             // per function pair of every molecule: gather_cols_kernel
+    double *g_colq = nullptr;          // beside g_col when quartets are screened: Qabs of its pair
     int4 *g_units = nullptr;           // gather units: shell pairs, heaviest first (gather_packed_kernel)
     int64_t n_units = 0;
     int64_t bytes = 0;
@@ -390,14 +392,15 @@ __device__ __forceinline__ long long untri_f(long long t) {
 }
 
 constexpr int kGatherThreads = 256;
-constexpr int kGatherUnroll = 8;
 
 // Per function pair (i >= j) of every molecule of a two-phase plan, what the gather needs to
 // place its entries, built once per plan on the device: x = list position << 4 | pair class of
 // the shell pair holding (i, j), y = component of the function in that pair's A << 16 |
-// component in its B.  Entry (m, ij) is at col[mol[4m+3] + ij]; thread r takes entry r, of the
-// molecule m with mol[4m+3] <= r < mol[4(m+1)+3] (the molecules' entries follow one another).
-__global__ void gather_cols_kernel(int2 *__restrict__ col, const int2 *__restrict__ fn,
+// component in its B; colq (plans that screen quartets) the pair's Qabs.  Entry (m, ij) is at
+// col[mol[4m+3] + ij]; thread r takes entry r, of the molecule m with
+// mol[4m+3] <= r < mol[4(m+1)+3] (the molecules' entries follow one another).
+__global__ void gather_cols_kernel(int2 *__restrict__ col, double *__restrict__ colq,
+                                   const double2 *__restrict__ bnd, const int2 *__restrict__ fn,
                                    const int *__restrict__ pairs, const long long *__restrict__ mol,
                                    int nmol, long long nrows) {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -414,6 +417,7 @@ __global__ void gather_cols_kernel(int2 *__restrict__ col, const int2 *__restric
     const int P = __ldg(&pairs[pb + (long long)fi.x * (fi.x + 1) / 2 + fj.x]);
     const int ca = (P & 1) ? fj.y : fi.y, cb = (P & 1) ? fi.y : fj.y;
     col[__ldg(&mol[4 * m + 3]) + ij] = make_int2(((P >> 5) << 4) | ((P >> 1) & 15), (ca << 16) | cb);
+    if (colq) colq[__ldg(&mol[4 * m + 3]) + ij] = __ldg(&bnd[P >> 5]).x;
 }
 
 // Second phase of the two-phase output: the packed vector written from the scratch blocks, one
@@ -431,15 +435,80 @@ __global__ void gather_cols_kernel(int2 *__restrict__ col, const int2 *__restric
 // two-phase plans that screen end each bra's ket run after its last unscreened ket, so no
 // chunk computes the rest.
 constexpr int kGatherMaxRows = 100;  // components of an (ff) pair
+
+// The columns of one shell pair P for the gather: NC columns per thread and pass (kl,
+// kl + kGatherThreads, ...), their descriptor loads first, then the scratch loads of NR rows of
+// each column (NC * NR in flight), then their stores.  RMAX > 0: P has at most RMAX rows, known
+// at compile time (RMAX <= NR: one row step per pass, no loop).  (Measured on B200: NC = 2,
+// NR = 4 with the small pairs' copies specialised beats more columns or rows per pass and
+// prefetching the next pass's descriptors, which cost occupancy.)
+template <int NC, int NR, int RMAX>
+__device__ __forceinline__ void gather_pair_columns(
+    double *__restrict__ obase, const double *__restrict__ scratch, const int2 *__restrict__ col,
+    const double *__restrict__ colq, long long cbase, const long long (*reg)[kNumPairClasses][5],
+    const long long *s_ij, const long long *s_tri, const int *s_rc, int R, int posP, int clsP,
+    double qP, double screen_cut) {
+    if (RMAX == 1) R = 1;
+    const long long ijmax = s_ij[R - 1];  // rows are in increasing ij
+    const int nP = c_pair_na[clsP] * c_pair_nb[clsP];
+    for (long long kl0 = threadIdx.x; kl0 <= ijmax; kl0 += NC * kGatherThreads) {
+        const double *src[NC];
+        long long kl[NC];
+        int r0[NC], rs[NC];
+        bool zero[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            kl[c] = kl0 + c * kGatherThreads;
+            const bool on = kl[c] <= ijmax;
+            const int2 qe = on ? __ldg(&col[cbase + kl[c]]) : make_int2(clsP, 0);
+            // a screened quartet (the class kernels' test, Qabs_P Qabs_Q < screen_cut) is 0;
+            // its block is not read (no chunk may have computed it)
+            zero[c] = on && screen_cut > 0.0 && qP * __ldg(&colq[cbase + kl[c]]) < screen_cut;
+            const int posQ = on ? qe.x >> 4 : posP, clsQ = qe.x & 15;
+            const int qa = qe.y >> 16, qb = qe.y & 0xffff;
+            const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
+            const long long *rg = reg[braP ? 0 : 1][clsQ];
+            const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
+            const long long db = bpos - rg[1], dk = kpos - rg[2];
+            const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
+            // component x = row part * rstride + column part
+            const int nq = c_pair_na[clsQ] * c_pair_nb[clsQ], qc = qa * c_pair_nb[clsQ] + qb;
+            rs[c] = braP ? nq : 1;
+            src[c] = scratch + rg[0] + slot * rg[4] + (braP ? qc : qc * nP);
+            // rows with ij >= kl: a suffix of the increasing row list (none past ijmax)
+            int r = 0;
+            while (r < R && s_ij[r] < kl[c]) ++r;
+            r0[c] = on ? r : R;
+        }
+        int rmin = r0[0];
+#pragma unroll
+        for (int c = 1; c < NC; ++c) rmin = min(rmin, r0[c]);
+        for (int r = rmin; r < R; r += NR) {
+            double v[NC][NR];
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+#pragma unroll
+                for (int t = 0; t < NR; ++t)
+                    v[c][t] = (r + t < R && r + t >= r0[c] && !zero[c]) ? __ldg(src[c] + s_rc[r + t] * rs[c]) : 0.0;
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+#pragma unroll
+                for (int t = 0; t < NR; ++t)
+                    if (r + t < R && r + t >= r0[c]) obase[s_tri[r + t] + kl[c]] = v[c][t];
+            if (RMAX > 0 && RMAX <= NR) break;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
     double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ col,
-    const long long *__restrict__ region, const long long *__restrict__ mol,
+    const double *__restrict__ colq, const long long *__restrict__ region, const long long *__restrict__ mol,
     const int4 *__restrict__ units, long long nunits, int *__restrict__ counter, int nmol,
     const double2 *__restrict__ bnd, double screen_cut) {
     // [P as bra, P as ket][class of the other pair]: {scratch offset, first bra, first ket,
     // kets, block size}
     __shared__ long long reg[2][kNumPairClasses][5];
-    __shared__ long long s_ij[kGatherMaxRows];
+    __shared__ long long s_ij[kGatherMaxRows], s_tri[kGatherMaxRows];
     __shared__ int s_rc[kGatherMaxRows];
     __shared__ long long s_unit;
     for (;;) {
@@ -453,7 +522,8 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
         const int nI = un.w & 255, nJ = (un.w >> 8) & 255, same = (un.w >> 16) & 1;
         const long long cbase = __ldg(&mol[4 * m + 3]);
         double *__restrict__ obase = out + __ldg(&mol[4 * m + 2]);
-        // P's rows: ij, and the row's component index in P's A, B orientation
+        // P's rows: ij, the row's first packed index tri(ij), and the row's component index in
+        // P's A, B orientation
         const int2 pe = __ldg(&col[cbase + (long long)fi0 * (fi0 + 1) / 2 + fj0]);
         const int posP = pe.x >> 4, clsP = pe.x & 15;
         const int nbP = c_pair_nb[clsP];
@@ -467,6 +537,7 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
             const long long i = fi0 + a, j = fj0 + b, ij = i * (i + 1) / 2 + j;
             const int2 re = __ldg(&col[cbase + ij]);
             s_ij[r] = ij;
+            s_tri[r] = ij * (ij + 1) / 2;
             s_rc[r] = (re.y >> 16) * nbP + (re.y & 0xffff);
         }
         if (threadIdx.x < 2 * kNumPairClasses) {
@@ -479,54 +550,16 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
             }
         }
         __syncthreads();
-        const long long ijmax = s_ij[R - 1];  // rows are in increasing ij
-        // two columns per thread and pass (kl and kl + kGatherThreads), their descriptor and
-        // scratch loads issued before their stores
-        for (long long kl0 = threadIdx.x; kl0 <= ijmax; kl0 += 2 * kGatherThreads) {
-            const double *src[2];
-            long long rs[2], kl[2];
-            int r0[2];
-            bool zero[2];
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                kl[c] = kl0 + c * kGatherThreads;
-                const bool on = kl[c] <= ijmax;
-                const int2 qe = on ? __ldg(&col[cbase + kl[c]]) : make_int2(clsP, 0);
-                const int posQ = on ? qe.x >> 4 : posP, clsQ = qe.x & 15;
-                // a screened quartet (the class kernels' test, Qabs_P Qabs_Q < screen_cut) is 0;
-                // its block is not read (no chunk may have computed it)
-                zero[c] = screen_cut > 0.0 && qP * __ldg(&bnd[posQ]).x < screen_cut;
-                const int qa = qe.y >> 16, qb = qe.y & 0xffff;
-                const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
-                const long long *rg = reg[braP ? 0 : 1][clsQ];
-                const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
-                const long long db = bpos - rg[1], dk = kpos - rg[2];
-                const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
-                // component x = row part * rstride + column part
-                const int nq = c_pair_na[clsQ] * c_pair_nb[clsQ], qc = qa * c_pair_nb[clsQ] + qb;
-                const int nP = c_pair_na[clsP] * nbP;
-                rs[c] = braP ? nq : 1;
-                src[c] = scratch + rg[0] + slot * rg[4] + (braP ? (long long)qc : (long long)qc * nP);
-                // rows with ij >= kl: a suffix of the increasing row list (none past ijmax)
-                int r = 0;
-                while (r < R && s_ij[r] < kl[c]) ++r;
-                r0[c] = on ? r : R;
-            }
-            for (int r = min(r0[0], r0[1]); r < R; r += 4) {
-                double v[2][4];
-#pragma unroll
-                for (int c = 0; c < 2; ++c)
-#pragma unroll
-                    for (int t = 0; t < 4; ++t)
-                        v[c][t] = (r + t < R && r + t >= r0[c] && !zero[c]) ? __ldg(src[c] + s_rc[r + t] * rs[c]) : 0.0;
-#pragma unroll
-                for (int c = 0; c < 2; ++c)
-#pragma unroll
-                    for (int t = 0; t < 4; ++t)
-                        if (r + t < R && r + t >= r0[c])
-                            obase[s_ij[r + t] * (s_ij[r + t] + 1) / 2 + kl[c]] = v[c][t];
-            }
-        }
+        // pairs of one or a few rows (ss, sp) are most of the units: their copies have no row loop
+        if (R == 1)
+            gather_pair_columns<2, 1, 1>(obase, scratch, col, colq, cbase, reg, s_ij, s_tri, s_rc, R, posP, clsP,
+                                         qP, screen_cut);
+        else if (R <= 4)
+            gather_pair_columns<2, 4, 4>(obase, scratch, col, colq, cbase, reg, s_ij, s_tri, s_rc, R, posP, clsP,
+                                         qP, screen_cut);
+        else
+            gather_pair_columns<2, 4, 0>(obase, scratch, col, colq, cbase, reg, s_ij, s_tri, s_rc, R, posP, clsP,
+                                         qP, screen_cut);
     }
 }
 
@@ -650,11 +683,13 @@ void ctx_copy_methods(molints_ctx *dst, const molints_ctx *src) {
 }
 
 // The schedule of contexts on devices without a tuned one.
-constexpr molints_schedule kBuiltinSchedule = {80.0, 1, 4096, 8, 0};
+constexpr molints_schedule kBuiltinSchedule = {80.0, 1, 4096, 8, 5};
+constexpr int kGatherBlocksDefault = 5;
 
 bool schedule_ok(const molints_schedule &s) {
     return s.lane_cost > 0.0 && s.lane_cost <= 1e6 && s.hgp_widen >= 1 && s.hgp_widen <= 64 &&
-           s.rys_chunks >= 1 && s.rys_max_width >= 1 && s.rys_max_width <= 64;
+           s.rys_chunks >= 1 && s.rys_max_width >= 1 && s.rys_max_width <= 64 && s.gather_blocks >= 0 &&
+           s.gather_blocks <= 16;
 }
 }  // namespace molints
 
@@ -723,7 +758,7 @@ int molints_create(molints_ctx **out, int device, int64_t budget, uint32_t flags
             std::strncmp(prop.name, kTunedDevice, std::strlen(kTunedDevice)) == 0) {
             std::memcpy(ctx->default_method, kTunedClassMethods, sizeof(ctx->default_method));
             ctx->default_sched = {kTunedSchedule[0], (int32_t)kTunedSchedule[1], (int32_t)kTunedSchedule[2],
-                                  (int32_t)kTunedSchedule[3], 0};
+                                  (int32_t)kTunedSchedule[3], (int32_t)kTunedSchedule[4]};
         }
         std::memcpy(ctx->class_method, ctx->default_method, sizeof(ctx->class_method));
         ctx->sched = ctx->default_sched;
@@ -838,9 +873,10 @@ int molints_set_schedule(molints_ctx *ctx, const molints_schedule *s) {
     }
     if (!schedule_ok(*s))
         return fail(ctx, MOLINTS_ERR_INVALID,
-                    "set_schedule: lane_cost in (0, 1e6], hgp_widen and rys_max_width in [1, 64], rys_chunks >= 1");
+                    "set_schedule: lane_cost in (0, 1e6], hgp_widen and rys_max_width in [1, 64], rys_chunks >= 1, "
+                    "gather_blocks in [0, 16]");
     ctx->sched = *s;
-    ctx->sched.reserved = 0;
+    if (ctx->sched.gather_blocks == 0) ctx->sched.gather_blocks = kGatherBlocksDefault;
     return MOLINTS_OK;
 }
 
@@ -914,8 +950,8 @@ static void plan_release_device(molints_plan *p) {
     p->prof_ev.clear();
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
-                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_col, p->g_units,
-                    p->gq, p->gq_mol, p->sh_L, p->sh_K, p->sh_fn};
+                    p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_col, p->g_colq,
+                    p->g_units, p->gq, p->gq_mol, p->sh_L, p->sh_K, p->sh_fn};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
     p->ctx = nullptr;
@@ -1302,6 +1338,7 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         S.nmol = nmol;
         S.widen = hgp_widen;
         S.lane_cost = ctx->sched.lane_cost;
+        p->gather_blocks = ctx->sched.gather_blocks;
         S.sharded = sharded;
         S.shard_s0 = shard_s0;
         S.shard_s1 = shard_s1;
@@ -1517,6 +1554,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         rc = rc ? rc : dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_col, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
+        if (opts.screen_cutoff > 0.0)
+            rc = rc ? rc : dev_alloc(ctx, &p->g_colq, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_units, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
     }
     int64_t temp_tally = 0;
@@ -1685,7 +1724,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         if (e != cudaSuccess) { release_temp(); plan_free(p); return cuda_fail(ctx, e, "plan_create work queues"); }
     }
     if (tp && nrows_all > 0) {
-        gather_cols_kernel<<<(unsigned)((nrows_all + 255) / 256), 256, 0, s>>>(p->g_col, p->g_fn, p->g_pair,
+        gather_cols_kernel<<<(unsigned)((nrows_all + 255) / 256), 256, 0, s>>>(p->g_col, p->g_colq, p->bnd,
+                                                                            p->g_fn, p->g_pair,
                                                                             p->g_mol, nmol, nrows_all);
         if ((e = cudaGetLastError())) { release_temp(); plan_free(p); return cuda_fail(ctx, e, "plan_create gather columns"); }
     }
@@ -1820,8 +1860,12 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     if (p->two_phase && !jk.J && p->npacked > 0) {
         // second phase: the packed vector in order from the scratch blocks
         if (int rc = mark(launches, "gather_packed", 0, s)) return rc;
-        const int grid = (int)std::min<long long>((long long)ctx->num_sms * 8, p->n_units);  // all resident
-        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col, p->g_region,
+        // a persistent grid of gather_blocks blocks per SM; blocks beyond what the kernel's
+        // registers let reside (five at 44 registers) start as others finish, and find the
+        // unit list done
+        const int gb = p->gather_blocks > 0 ? p->gather_blocks : kGatherBlocksDefault;
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * gb, p->n_units);
+        gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col, p->g_colq, p->g_region,
                                                              p->g_mol, p->g_units, p->n_units,
                                                              p->counters + kNumPairClasses * kNumPairClasses,
                                                              p->nmol, p->bnd, p->opts.screen_cutoff);

@@ -91,8 +91,8 @@ class Schedule(ctypes.Structure):
     """molints_schedule: the work-queue knobs of the plans a context creates."""
     _fields_ = [("lane_cost", ctypes.c_double), ("hgp_widen", ctypes.c_int32),
                 ("rys_chunks", ctypes.c_int32), ("rys_max_width", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
-    KEYS = ("lane_cost", "hgp_widen", "rys_chunks", "rys_max_width")
+                ("gather_blocks", ctypes.c_int32)]
+    KEYS = ("lane_cost", "hgp_widen", "rys_chunks", "rys_max_width", "gather_blocks")
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k in self.KEYS}
@@ -418,7 +418,8 @@ class Engine:
 
     def set_schedule(self, sched: dict | None = None):
         """Work-queue schedule of the plans created afterwards: a dict with any of lane_cost,
-        hgp_widen, rys_chunks, rys_max_width (the others keep their current values); None
+        hgp_widen, rys_chunks, rys_max_width, gather_blocks (the others keep their current
+        values); None
         restores the library's default (the tuned one on a B200)."""
         if sched is None:
             self._check(self.lib.molints_set_schedule(self.ctx, None))

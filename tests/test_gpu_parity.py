@@ -487,27 +487,32 @@ def test_class_method_table(eng):
 
 
 def test_schedule_knobs_keep_results(eng, oracle):
-    """The work-queue schedule changes how quartets are grouped and split over lanes, not
-    what is computed: extreme schedules give the default's integrals within the FP64 bar, on a
-    d molecule (HGP lane splits) and an f molecule (Rys chunks), and every slot is written."""
+    """The work-queue schedule changes how quartets are grouped and split over lanes and how
+    many gather blocks share an SM, not what is computed: extreme schedules give the default's
+    integrals within the FP64 bar, on a d molecule (HGP lane splits) and an f molecule (Rys
+    chunks), with direct stores and the two-phase gather, and every slot is written."""
     from molints_b200 import engine
     default = eng.schedule()
-    assert set(default) == {"lane_cost", "hgp_widen", "rys_chunks", "rys_max_width"}
+    assert set(default) == {"lane_cost", "hgp_widen", "rys_chunks", "rys_max_width", "gather_blocks"}
     mols = [mi.config2(), _f_molecule(21, nheavy=2, nh=1)]
     refs = [eng.eri_packed(sh, boys=engine.BOYS_EXACT) for sh in mols]
     try:
-        for sched in ({"lane_cost": 20.0, "hgp_widen": 4, "rys_chunks": 1, "rys_max_width": 16},
-                      {"lane_cost": 1e6, "hgp_widen": 1, "rys_chunks": 1 << 30, "rys_max_width": 1}):
+        for sched in ({"lane_cost": 20.0, "hgp_widen": 4, "rys_chunks": 1, "rys_max_width": 16, "gather_blocks": 1},
+                      {"lane_cost": 1e6, "hgp_widen": 1, "rys_chunks": 1 << 30, "rys_max_width": 1,
+                       "gather_blocks": 16}):
             eng.set_schedule(sched)
             assert eng.schedule() == {k: (float(v) if k == "lane_cost" else v) for k, v in sched.items()}
             for sh, ref in zip(mols, refs):
-                got = eng.eri_packed(sh, boys=engine.BOYS_EXACT)
-                assert not np.isnan(got).any()
-                assert np.max(np.abs(got - ref)) < TOL_FP64
+                for out in (engine.OUTPUT_DIRECT, engine.OUTPUT_TWO_PHASE):
+                    got = eng.eri_packed(sh, boys=engine.BOYS_EXACT, output=out)
+                    assert not np.isnan(got).any()
+                    assert np.max(np.abs(got - ref)) < TOL_FP64
         with pytest.raises(engine.MolintsError):
             eng.set_schedule({"hgp_widen": 0})
         with pytest.raises(engine.MolintsError):
             eng.set_schedule({"lane_cost": -1.0})
+        with pytest.raises(engine.MolintsError):
+            eng.set_schedule({"gather_blocks": 17})
     finally:
         eng.set_schedule(None)
     assert eng.schedule() == default
