@@ -118,6 +118,7 @@ struct molints_plan {
     // class-major scratch, a gather pass writes the packed vector in order from it
     int two_phase = 0;
     int gather_blocks = 0;             // the context's schedule at creation: gather blocks per SM
+    int screen_trunc = 0;              // ket runs end at the last unscreened ket (quartet screening)
     int64_t scratch_need = 0;          // doubles of the context's scratch an execute uses: per
                                        // (class pair, molecule) a region of quartet blocks
     long long *chunk_slot = nullptr;   // per chunk: scratch offset of its first quartet's block
@@ -432,7 +433,7 @@ __global__ void gather_cols_kernel(int2 *__restrict__ col, double *__restrict__ 
 // P == Q); a pair's components are taken in its A, B orientation, with the larger component
 // first within a same-shell pair, as the direct store conditions pick.  With quartet
 // screening, the entries of a screened quartet are written as 0 without reading the scratch:
-// two-phase plans that screen end each bra's ket run after its last unscreened ket, so no
+// plans that screen end each bra's ket run after its last unscreened ket, so no
 // chunk computes the rest.
 constexpr int kGatherMaxRows = 100;  // components of an (ff) pair
 
@@ -1403,7 +1404,8 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
     const bool tp = p->two_phase != 0;
     S.two_phase = tp;
     S.screen_sort = !sharded && opts.screen_cutoff > 0.0;
-    S.screen_trunc = tp && S.screen_sort;
+    S.screen_trunc = S.screen_sort;
+    p->screen_trunc = S.screen_trunc;
     S.screen_cut = opts.screen_cutoff;
 
     // ---- pinned upload buffer: the summary read back after the device build, the plan's
@@ -1787,6 +1789,11 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     };
     if (timing) MI_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
     MI_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(int) * (kNumPairClasses * kNumPairClasses + 1), s));
+    // direct plans that screen quartets: the screened quartets past each bra's last unscreened
+    // ket are in no chunk, so their zeros come from clearing the whole output first (a
+    // streaming write instead of scattered 8-byte stores); two-phase plans' gather writes them
+    if (p->screen_trunc && !p->two_phase && !jk.J && p->npacked > 0)
+        MI_CUDA(ctx, cudaMemsetAsync(out_device, 0, (size_t)p->npacked * sizeof(double), s));
     if (p->npair > 0) {
         if (int rc = mark(launches, "build_pairs", 0, s)) return rc;
         build_pairs_kernel<<<build_pairs_blocks(p->npair), 128, 0, s>>>(

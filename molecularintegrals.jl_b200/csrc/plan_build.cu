@@ -106,11 +106,11 @@ __global__ void pair_tables_kernel(PlanBuildArgs A) {
 
 // ---- work queues
 
-// Two-phase plans that screen quartets: the end of bra pb's ket run [kbeg, kend) after its last ket q
+// Plans that screen quartets: the end of bra pb's ket run [kbeg, kend) after its last ket q
 // with Qabs_pb Qabs_q >= screen_cut (kbeg if there is none).  The run is in Qabs-bucket order,
 // descending, so the kets screened by their bucket's upper bound alone form a suffix, found by
 // bisection; the last unscreened ket lies just before it.  The quartets past the end are
-// screened: the gather writes their zeros.
+// screened: their zeros come from the gather or from the cleared output.
 __device__ int unscreened_end(const QueueSetup &S, const QueueArgs &A, int pb, int kbeg, int kend) {
     const double qp = A.bnd[pb].x;
     int lo = kbeg, hi = kend;  // first q with qabs_bucket_hi(q) * qp < cut, in [kbeg, kend]

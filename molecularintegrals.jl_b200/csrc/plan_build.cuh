@@ -90,10 +90,9 @@ struct QueueSetup {
     int ps0[kNumPairClasses], ps1[kNumPairClasses];  // first pair of each class with ms >= s0 / s1
     int two_phase;
     // Quartet screening (Qabs_p Qabs_q < screen_cut written as 0): the pair runs are in
-    // Qabs-bucket order (screen_sort; direct and two-phase plans alike, so that their quartets
-    // have the same bra and sum alike), and in two-phase plans each bra's ket run ends after
-    // its last unscreened ket (screen_trunc): the gather writes the zeros of the quartets no
-    // chunk holds.
+    // Qabs-bucket order (screen_sort) and each bra's ket run ends after its last unscreened
+    // ket (screen_trunc); the zeros of the quartets no chunk holds come from the gather
+    // (two-phase plans) or from clearing the output before the class kernels (direct plans).
     int screen_sort, screen_trunc;
     double screen_cut;
 };
