@@ -433,8 +433,8 @@ __global__ void gather_cols_kernel(int2 *__restrict__ col, double *__restrict__ 
 // P == Q); a pair's components are taken in its A, B orientation, with the larger component
 // first within a same-shell pair, as the direct store conditions pick.  With quartet
 // screening, the entries of a screened quartet are written as 0 without reading the scratch:
-// plans that screen end each bra's ket run after its last unscreened ket, so no
-// chunk computes the rest.
+// plans that screen end each bra's ket run after its last unscreened ket, so no chunk computes
+// the rest.
 constexpr int kGatherMaxRows = 100;  // components of an (ff) pair
 
 // The columns of one shell pair P for the gather: NC columns per thread and pass (kl,
@@ -1791,7 +1791,9 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
     MI_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(int) * (kNumPairClasses * kNumPairClasses + 1), s));
     // direct plans that screen quartets: the screened quartets past each bra's last unscreened
     // ket are in no chunk, so their zeros come from clearing the whole output first (a
-    // streaming write instead of scattered 8-byte stores); two-phase plans' gather writes them
+    // streaming write instead of scattered 8-byte stores).  Two-phase plans' gather writes them
+    // (measured on B200: clearing first and leaving them out of the gather cost more than the
+    // gather's zero stores, which are coalesced)
     if (p->screen_trunc && !p->two_phase && !jk.J && p->npacked > 0)
         MI_CUDA(ctx, cudaMemsetAsync(out_device, 0, (size_t)p->npacked * sizeof(double), s));
     if (p->npair > 0) {
