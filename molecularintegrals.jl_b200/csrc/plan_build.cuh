@@ -51,18 +51,21 @@ __host__ __device__ inline int cost_bucket(double c) {
     return b < 0 ? 0 : (b > kCostBuckets - 1 ? kCostBuckets - 1 : b);
 }
 
-// Bucket of a pair's Schwarz factor Qabs for the screening order: a factor of 16 in Qabs per
+// Bucket of a pair's Schwarz factor Qabs for the screening order: a factor of 256 in Qabs per
 // bucket.  With Qabs = f 2^e (f in [0.5, 1), so Qabs < 2^e), the bucket is
-// (e + kQabsBias) / 4 clamped to [1, 255], and 0 for Qabs = 0.  Plans that screen quartets
+// (e + kQabsBias) / 8 clamped to [1, 255], and 0 for Qabs = 0.  Plans that screen quartets
 // order each (class, molecule) run of pairs by bucket, descending, so that a bra's unscreened
-// kets come first; within a bucket the kept count descends, which keeps a chunk's lanes
-// alike.
-constexpr int kQabsBias = 640;
+// kets come first; within a bucket the kept count descends, which keeps a chunk's lanes alike
+// and its lane split constant.  Wider buckets leave more screened quartets inside the runs,
+// narrower ones cut more chunks where the split changes (measured on B200 over the eight
+// largest groups of the 256-molecule batch, MIXED: factors 4 / 16 / 256 / 65536 / 2^32 per
+// bucket, 60.8 / 55.9 / 54.2 / 54.7 / 56.3 ms per execute).
+constexpr int kQabsBias = 1280;
 __host__ __device__ inline int qabs_bucket(double q) {
     if (!(q > 0.0)) return 0;
     int e2 = 0;
     frexp(q, &e2);
-    const int b = (e2 + kQabsBias) >> 2;
+    const int b = (e2 + kQabsBias) >> 3;
     return b < 1 ? 1 : (b > 255 ? 255 : b);
 }
 
@@ -70,7 +73,7 @@ __host__ __device__ inline int qabs_bucket(double q) {
 __host__ __device__ inline double qabs_bucket_hi(int b) {
     if (b <= 0) return 0.0;
     if (b >= 255) return HUGE_VAL;
-    return ldexp(1.0, 4 * b + 3 - kQabsBias);  // e <= 4b + 3 - kQabsBias
+    return ldexp(1.0, 8 * b + 7 - kQabsBias);  // e <= 8b + 7 - kQabsBias
 }
 
 // What the queue kernels need per class pair (x, y <= x), in the host's class-pair order
