@@ -104,7 +104,14 @@ typedef struct molints_options {
                                 FP32 (FP64 Boys, prefactors, contraction and HRR); R_ab =
                                 (1+|A-B|)^lb sum_i sqrt(max |[e0|e0]_ii|) bounds the VRR
                                 output block the HRR combines */
-    double screen_cutoff;    /* quartets with B below this are written as 0 */
+    double screen_cutoff;    /* quartets with B below this are written as 0, and their work
+                                is skipped: such plans order each class's pairs by Qabs and
+                                end each bra's ket run after its last unscreened ket (a direct
+                                output is cleared with one memset first, a two-phase one gets
+                                the zeros from the gather).  The bra/ket roles of some
+                                same-class quartets then differ from an unscreened plan's, so
+                                the kept integrals agree with it to rounding, not bit for bit.
+                                Shard plans keep the per-quartet test only. */
     double prim_cutoff;      /* primitive pairs i with b_i * max_cd Qabs_cd below this are
                                 dropped, b_i = sqrt(max |(a_i b_i|a_i b_i)|); each dropped
                                 contribution is below prim_cutoff.  Default 1e-18. */
