@@ -465,17 +465,23 @@ __device__ __forceinline__ void gather_pair_columns(
             // a screened quartet (the class kernels' test, Qabs_P Qabs_Q < screen_cut) is 0;
             // its block is not read (no chunk may have computed it)
             zero[c] = on && screen_cut > 0.0 && qP * __ldg(&colq[cbase + kl[c]]) < screen_cut;
-            const int posQ = on ? qe.x >> 4 : posP, clsQ = qe.x & 15;
-            const int qa = qe.y >> 16, qb = qe.y & 0xffff;
-            const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
-            const long long *rg = reg[braP ? 0 : 1][clsQ];
-            const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
-            const long long db = bpos - rg[1], dk = kpos - rg[2];
-            const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
-            // component x = row part * rstride + column part
-            const int nq = c_pair_na[clsQ] * c_pair_nb[clsQ], qc = qa * c_pair_nb[clsQ] + qb;
-            rs[c] = braP ? nq : 1;
-            src[c] = scratch + rg[0] + slot * rg[4] + (braP ? qc : qc * nP);
+            src[c] = scratch;
+            rs[c] = 0;
+            if (!zero[c]) {
+                // the column's scratch block and component (skipped for screened columns, most
+                // of a screened plan's)
+                const int posQ = on ? qe.x >> 4 : posP, clsQ = qe.x & 15;
+                const int qa = qe.y >> 16, qb = qe.y & 0xffff;
+                const bool braP = clsP > clsQ || (clsP == clsQ && posP >= posQ);
+                const long long *rg = reg[braP ? 0 : 1][clsQ];
+                const int bpos = braP ? posP : posQ, kpos = braP ? posQ : posP;
+                const long long db = bpos - rg[1], dk = kpos - rg[2];
+                const long long slot = (clsP == clsQ) ? db * (db + 1) / 2 + dk : db * rg[3] + dk;
+                // component x = row part * rstride + column part
+                const int nq = c_pair_na[clsQ] * c_pair_nb[clsQ], qc = qa * c_pair_nb[clsQ] + qb;
+                rs[c] = braP ? nq : 1;
+                src[c] = scratch + rg[0] + slot * rg[4] + (braP ? qc : qc * nP);
+            }
             // rows with ij >= kl: a suffix of the increasing row list (none past ijmax)
             int r = 0;
             while (r < R && s_ij[r] < kl[c]) ++r;
