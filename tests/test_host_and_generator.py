@@ -25,6 +25,62 @@ def _header_functions():
     return sorted(set(re.findall(r"\b(molints_[a-z_0-9]+)\s*\(", text)))
 
 
+def _header_structs():
+    """{struct name: [(field, C type, array length or 0), ...]} of the typedef'd structs that
+    cross the C ABI by value, read from include/molints.h."""
+    text = (ROOT / "include" / "molints.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for name, body in re.findall(r"typedef struct (molints_\w+) \{(.*?)\} \1;", text, flags=re.S):
+        fields = []
+        for decl in filter(None, (d.strip() for d in body.split(";"))):
+            m = re.match(r"(?:const\s+)?(\w+)\s*(\*?)\s*(\w+)(?:\[(\d+)\])?$", " ".join(decl.split()))
+            assert m, decl
+            ctype = m.group(1) + ("*" if m.group(2) else "")
+            fields.append((m.group(3), ctype, int(m.group(4) or 0)))
+        out[name] = fields
+    return out
+
+
+def test_ctypes_structs_match_header():
+    """The Python binding's structures have the header's fields, in order, with the same C
+    types and the same size, so that every struct passed through the C ABI lines up."""
+    from molints_b200 import engine
+    ctype_of = {"int32_t": ctypes.c_int32, "int64_t": ctypes.c_int64, "double": ctypes.c_double}
+    mirrors = {"molints_basis": engine.Basis, "molints_options": engine.Options,
+               "molints_stats": engine.Stats, "molints_schedule": engine.Schedule}
+    structs = _header_structs()
+    assert set(mirrors) <= set(structs), sorted(structs)
+    for cname, py in mirrors.items():
+        want = structs[cname]
+        got = py._fields_
+        assert [f for f, _, _ in want] == [f for f, _ in got], cname
+        for (f, ct, n), (_, pt) in zip(want, got):
+            exp = ctypes.c_void_p if ct.endswith("*") else ctype_of[ct]
+            if n:
+                exp = exp * n
+            assert ctypes.sizeof(pt) == ctypes.sizeof(exp), (cname, f)
+            assert getattr(pt, "_type_", pt) == getattr(exp, "_type_", exp), (cname, f)
+            if n:
+                assert pt._length_ == n, (cname, f)
+
+
+def test_julia_shim_structs_match_header():
+    """The Julia ccall shim of INTEGRATION.md declares MolintsBasis and MolintsOptions with the
+    header's fields, in order, with matching types (isbits structs pass by Ref as the C structs)."""
+    text = (ROOT / "INTEGRATION.md").read_text()
+    jl = {"Int32": "int32_t", "Int64": "int64_t", "Float64": "double"}
+    structs = _header_structs()
+    for jname, cname in (("MolintsBasis", "molints_basis"), ("MolintsOptions", "molints_options")):
+        body = re.search(r"struct %s\n(.*?)\nend" % jname, text, flags=re.S).group(1)
+        body = re.sub(r"#[^\n]*", "", body)
+        fields = re.findall(r"(\w+)::(Ptr\{\w+\}|\w+)", body)
+        want = structs[cname]
+        assert [f for f, _ in fields] == [f for f, _, _ in want], jname
+        for (f, jt), (_, ct, _) in zip(fields, want):
+            assert (jt.startswith("Ptr{") and ct.endswith("*")) or jl.get(jt) == ct, (jname, f, jt, ct)
+
+
 @pytest.fixture(scope="module")
 def lib():
     from molints_b200 import engine
