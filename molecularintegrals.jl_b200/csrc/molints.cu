@@ -129,6 +129,9 @@ struct molints_plan {
                                        // first function-pair entry of g_col}
     int2 *g_col = nullptr;             // per function pair of every molecule: gather_cols_kernel
     double *g_colq = nullptr;          // beside g_col when quartets are screened: Qabs of its pair
+    double *g_qmax = nullptr;          // per molecule when quartets are screened: a bound of every
+                                       // pair's Qabs (the largest sum of b_k over all its
+                                       // primitive pairs)
     int4 *g_units = nullptr;           // gather units: shell pairs, heaviest first (gather_packed_kernel)
     int64_t n_units = 0;
     int64_t bytes = 0;
@@ -511,7 +514,7 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
     double *__restrict__ out, const double *__restrict__ scratch, const int2 *__restrict__ col,
     const double *__restrict__ colq, const long long *__restrict__ region, const long long *__restrict__ mol,
     const int4 *__restrict__ units, long long nunits, int *__restrict__ counter, int nmol,
-    const double2 *__restrict__ bnd, double screen_cut) {
+    const double2 *__restrict__ bnd, const double *__restrict__ qmax, double screen_cut) {
     // [P as bra, P as ket][class of the other pair]: {scratch offset, first bra, first ket,
     // kets, block size}
     __shared__ long long reg[2][kNumPairClasses][5];
@@ -557,6 +560,16 @@ __global__ void __launch_bounds__(kGatherThreads) gather_packed_kernel(
             }
         }
         __syncthreads();
+        if (screen_cut > 0.0 && qP * __ldg(&qmax[m]) < screen_cut) {
+            // every quartet of P is screened (Qabs_P times the molecule's largest Qabs is below
+            // the cutoff): its rows are zeros, written as contiguous runs with no descriptor or
+            // scratch loads
+            for (int r = 0; r < R; ++r) {
+                const long long t0 = s_tri[r], n = s_ij[r] + 1;
+                for (long long k = threadIdx.x; k < n; k += kGatherThreads) obase[t0 + k] = 0.0;
+            }
+            continue;
+        }
         // pairs of one or a few rows (ss, sp) are most of the units: their copies have no row loop
         if (R == 1)
             gather_pair_columns<2, 1, 1>(obase, scratch, col, colq, cbase, reg, s_ij, s_tri, s_rc, R, posP, clsP,
@@ -958,7 +971,7 @@ static void plan_release_device(molints_plan *p) {
     void *bufs[] = {p->sh_xyz, p->expn, p->ncoef, p->sh_poff, p->pair_ab, p->info, p->pp_src, p->pbk,
                     p->geo, p->pp, p->bnd, p->chunks, p->counters, p->mol_out, p->qcon,
                     p->chunk_slot, p->g_fn, p->g_pair, p->g_region, p->g_mol, p->g_col, p->g_colq,
-                    p->g_units, p->gq, p->gq_mol, p->sh_L, p->sh_K, p->sh_fn};
+                    p->g_qmax, p->g_units, p->gq, p->gq_mol, p->sh_L, p->sh_K, p->sh_fn};
     for (void *b : bufs) dev_free(p->ctx, b);
     p->ctx->held -= p->bytes;
     p->ctx = nullptr;
@@ -1562,8 +1575,10 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         rc = rc ? rc : dev_alloc(ctx, &p->g_region, region_h.size(), &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_mol, (size_t)nmol * 4, &p->bytes);
         rc = rc ? rc : dev_alloc(ctx, &p->g_col, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
-        if (opts.screen_cutoff > 0.0)
+        if (opts.screen_cutoff > 0.0) {
             rc = rc ? rc : dev_alloc(ctx, &p->g_colq, (size_t)std::max<int64_t>(nrows_all, 1), &p->bytes);
+            rc = rc ? rc : dev_alloc(ctx, &p->g_qmax, (size_t)std::max(nmol, 1), &p->bytes);
+        }
         rc = rc ? rc : dev_alloc(ctx, &p->g_units, (size_t)std::max<int64_t>(npe_all, 1), &p->bytes);
     }
     int64_t temp_tally = 0;
@@ -1735,7 +1750,10 @@ static int plan_create_impl(molints_ctx *ctx, int32_t nmol, const molints_basis 
         gather_cols_kernel<<<(unsigned)((nrows_all + 255) / 256), 256, 0, s>>>(p->g_col, p->g_colq, p->bnd,
                                                                             p->g_fn, p->g_pair,
                                                                             p->g_mol, nmol, nrows_all);
-        if ((e = cudaGetLastError())) { release_temp(); plan_free(p); return cuda_fail(ctx, e, "plan_create gather columns"); }
+        e = cudaGetLastError();
+        if (!e && p->g_qmax)  // the molecules' Qabs bounds (doubles as bits) outlive the build
+            e = cudaMemcpyAsync(p->g_qmax, tmp + t_qmax, (size_t)nmol * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (e) { release_temp(); plan_free(p); return cuda_fail(ctx, e, "plan_create gather columns"); }
     }
     release_temp();
     p->plan_ms[2] = ms_since(t_phase);
@@ -1883,7 +1901,7 @@ static int plan_enqueue(molints_plan *p, double *out_device, bool timing, JKOut 
         gather_packed_kernel<<<grid, kGatherThreads, 0, s>>>(out_device, ctx->scratch, p->g_col, p->g_colq, p->g_region,
                                                              p->g_mol, p->g_units, p->n_units,
                                                              p->counters + kNumPairClasses * kNumPairClasses,
-                                                             p->nmol, p->bnd, p->opts.screen_cutoff);
+                                                             p->nmol, p->bnd, p->g_qmax, p->opts.screen_cutoff);
         if (int rc = mark(launches, "gather_packed", 1, s)) return rc;
         ++launches;
     }
