@@ -395,6 +395,7 @@ def run_ours(args):
             "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
                      "mixed_over_fp64": valuemx / value64},
             "plain_fp64_per_molecule": plain,
+            "mixed_over_plain_fp64_per_molecule": None if plain is None else valuemx / plain["value"],
             "max_abs_err_vs_oracle": errors,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "config1": cfg1, "serving_config4": serving, "jk_config1": jk,
@@ -574,7 +575,8 @@ def measure_plain_fp64(eng, dev, mols, mine):
     dt = time.perf_counter() - t0
     n = sum(mols[i].npacked for i in mine)
     return {"value": n / dt, "unit": UNIT, "seconds": dt,
-            "note": "molints_eri_packed per molecule (FP64, default options), device output"}
+            "note": "molints_eri_packed per molecule (FP64, default options), device output, "
+                    "plan creation included (host wall clock)"}
 
 
 def measure_errors(eng, fp32_cut):
