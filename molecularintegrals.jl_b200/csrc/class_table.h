@@ -19,6 +19,6 @@ static const int32_t kTunedClassMethods[11][11] = {
     {5, 5, 6, 6, 6, 6, 6, 6, 6, 6, 0},
     {5, 2, 6, 6, 6, 6, 6, 6, 6, 6, 6},
 };
-// work-queue schedule: lane_cost, hgp_widen, rys_chunks, rys_max_width, gather_blocks (autotune.tune_schedule on B200 (bench.py): a batch plan over 8 molecules of the 256-molecule batch, 57.3 ms with the built-in schedule, 53.9 ms with this one)
-static const double kTunedSchedule[5] = {320.0, 1.0, 4096.0, 8.0, 5.0};
+// work-queue schedule: lane_cost, hgp_widen, rys_chunks, rys_max_width, gather_blocks (autotune.tune_schedule on B200 (bench.py): a batch plan over 8 molecules of the 256-molecule batch, 54.8 ms with lane_cost 320 and 5 gather blocks per SM, 53.0 ms with this one)
+static const double kTunedSchedule[5] = {640.0, 1.0, 4096.0, 8.0, 4.0};
 }  // namespace molints
