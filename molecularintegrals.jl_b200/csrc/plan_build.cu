@@ -106,23 +106,6 @@ __global__ void pair_tables_kernel(PlanBuildArgs A) {
 
 // ---- work queues
 
-// Plans that screen quartets: the end of bra pb's ket run [kbeg, kend) after its last ket q
-// with Qabs_pb Qabs_q >= screen_cut (kbeg if there is none).  The run is in Qabs-bucket order,
-// descending, so the kets screened by their bucket's upper bound alone form a suffix, found by
-// bisection; the last unscreened ket lies just before it.  The quartets past the end are
-// screened: their zeros come from the gather or from the cleared output.
-__device__ int unscreened_end(const QueueSetup &S, const QueueArgs &A, int pb, int kbeg, int kend) {
-    const double qp = A.bnd[pb].x;
-    int lo = kbeg, hi = kend;  // first q with qabs_bucket_hi(q) * qp < cut, in [kbeg, kend]
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (qabs_bucket_hi(qabs_bucket(A.bnd[mid].x)) * qp < S.screen_cut) hi = mid; else lo = mid + 1;
-    }
-    int e = lo;
-    while (e > kbeg && qp * A.bnd[e - 1].x < S.screen_cut) --e;
-    return e;
-}
-
 // The chunks of one item: bra pair pb of class pair ci against its ket run, in ket order.
 // Chunks hold one bra pair and up to `width` ket pairs of the same molecule.  HGP chunks whose
 // quartets are split over lanes (hgp_split) hold (32 >> lg) * widen ket pairs and end where the
@@ -149,7 +132,7 @@ __device__ void walk_item(const QueueSetup &S, const QueueArgs &A, int ci, int p
             kend = S.ps1[y];
         }
     }
-    if (S.screen_trunc && kend > kbeg) kend = unscreened_end(S, A, pb, kbeg, kend);
+    if (S.screen_trunc && kend > kbeg) kend = unscreened_end(A.bnd, S.screen_cut, pb, kbeg, kend);
     const int nb = A.npp[pb];
     const double wp = S.w[ci] * nb, pcost = S.pcost[ci];
     // this bra's remaining kets may still need a split (in Qabs order the kept counts do not

@@ -76,6 +76,23 @@ __host__ __device__ inline double qabs_bucket_hi(int b) {
     return ldexp(1.0, 8 * b + 7 - kQabsBias);  // e <= 8b + 7 - kQabsBias
 }
 
+// Plans that screen quartets: the end of bra pb's ket run [kbeg, kend) after its last ket q
+// with Qabs_pb Qabs_q >= cut (kbeg if there is none); bnd[k].x = Qabs of pair k.  The run is in
+// Qabs-bucket order, descending, so the kets screened by their bucket's upper bound alone form a
+// suffix, found by bisection; the last unscreened ket lies just before it.  The quartets past
+// the end are screened: their zeros come from the gather or from the cleared output.
+__host__ __device__ inline int unscreened_end(const double2 *bnd, double cut, int pb, int kbeg, int kend) {
+    const double qp = bnd[pb].x;
+    int lo = kbeg, hi = kend;  // first q with qabs_bucket_hi(q) * qp < cut, in [kbeg, kend]
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (qabs_bucket_hi(qabs_bucket(bnd[mid].x)) * qp < cut) hi = mid; else lo = mid + 1;
+    }
+    int e = lo;
+    while (e > kbeg && qp * bnd[e - 1].x < cut) --e;
+    return e;
+}
+
 // What the queue kernels need per class pair (x, y <= x), in the host's class-pair order
 // (x outer, y inner): a plain struct passed by value.
 struct QueueSetup {

@@ -5,6 +5,8 @@ The work-queue emission relies on three properties of them:
 - the Schwarz-factor bucket is non-decreasing in Qabs, so a run sorted by bucket (descending)
   has its screened kets, by the bucket bound alone, as a suffix (bisection in unscreened_end);
 - every Qabs lies below its bucket's upper bound, so that suffix is screened exactly;
+- in a run so sorted, the bisection on the bucket bound plus a short scan back ends a bra's
+  ket run exactly after its last unscreened ket (no unscreened quartet is left out);
 - a ket whose quartet with the bra needs no HGP lane split implies the same for every ket
   with fewer primitive pairs, so that in a run of descending counts a chunk that starts
   unsplit stays unsplit (splits above zero need not be monotone in the count: the walk tests
@@ -63,6 +65,34 @@ int main() {
                     split_below = split_below || lg != 0;
                 }
             }
+    // the truncation of a bra's ket run: runs sorted as the plan sorts them (bucket descending,
+    // any order within a bucket) end exactly after their last unscreened ket
+    std::uniform_int_distribution<int> len(1, 400);
+    std::uniform_real_distribution<double> lq(-25.0, 3.0), u01(0.0, 1.0);
+    const double cuts[] = {1e-12, 5e-10, 1e-6, 1e-2};
+    for (int trial = 0; trial < 4000; ++trial) {
+        const int n = len(rng);
+        std::vector<std::pair<int, double>> v(n);
+        for (auto &e : v) {
+            const double x = u01(rng) < 0.05 ? 0.0 : std::pow(10.0, lq(rng));
+            e = {qabs_bucket(x), x};
+        }
+        std::shuffle(v.begin(), v.end(), rng);
+        std::stable_sort(v.begin(), v.end(), [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+            return a.first > b.first;
+        });
+        std::vector<double2> bnd(n);
+        for (int k = 0; k < n; ++k) bnd[k] = make_double2(v[k].second, 0.0);
+        const int pb = std::uniform_int_distribution<int>(0, n - 1)(rng);
+        const int kbeg = std::uniform_int_distribution<int>(0, pb)(rng);
+        const int kend = trial % 2 ? pb + 1 : n;  // equal classes: kets up to the bra itself
+        const double cut = cuts[trial % 4];
+        int want = kbeg;
+        for (int k = kbeg; k < kend; ++k)
+            if (!(bnd[pb].x * bnd[k].x < cut)) want = k + 1;
+        const int got = unscreened_end(bnd.data(), cut, pb, kbeg, kend);
+        if (got != want) { ++bad; std::printf("run end %d, want %d (n %d)\n", got, want, n); }
+    }
     std::printf("%zu values, %d failures\n", q.size(), bad);
     return bad != 0;
 }
