@@ -395,7 +395,9 @@ def run_ours(args):
             "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
                      "mixed_over_fp64": valuemx / value64},
             "plain_fp64_per_molecule": plain,
-            "mixed_over_plain_fp64_per_molecule": None if plain is None else valuemx / plain["value"],
+            # rank 0's own molecules at N > 1: the ratio is stated for one GPU only
+            "mixed_over_plain_fp64_per_molecule": (valuemx / plain["value"]
+                                                   if plain is not None and world == 1 else None),
             "max_abs_err_vs_oracle": errors,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "config1": cfg1, "serving_config4": serving, "jk_config1": jk,
